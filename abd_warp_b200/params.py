@@ -1,0 +1,93 @@
+"""Simulation parameters.
+
+The reference reads its physics constants from module globals (const_params.py:24-44)
+and ignores the values in ``AffineBodySimulator.simulator_args`` (abd.py:107-121).
+Here every constant is a field of :class:`SimParams`, passed by value to the CUDA
+library and to the oracle, so one object fixes the physics of a run.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field, asdict
+
+SOLVER_BICGSTAB = 0
+SOLVER_PCG = 1
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+
+@dataclass
+class SimParams:
+    dt: float = 0.01                 # const_params.py:24
+    dhat: float = 1e-3               # barrier distance; d2hat = dhat^2 (const_params.py:33-34)
+    kappa: float = 1e6               # barrier stiffness (const_params.py:35)
+    stiffness: float = 1e7           # orthogonality stiffness (const_params.py:27)
+    gravity: float = -9.8            # y component (const_params.py:32)
+    tol: float = 1e-6                # Newton stop: g.g < tol (abd.py:265-268)
+    c1: float = 1e-4                 # Armijo constant (const_params.py:28)
+    alpha_min: float = 1e-3          # line-search floor (const_params.py:29)
+    max_iter: int = 100              # Newton iteration cap (abd.py:114)
+    armijo_sign: int = -1            # -1: E1 < E0 - c1 a dq.g ; +1: reference form abd.py:156
+    ground_enabled: bool = False     # vertex-ground plane contact (culling.py:54-82)
+    ground: float = -0.5             # plane height (const_params.py:36)
+    psd_ee: bool = False             # contact_psd 0 only: clamp EE eigenvalues too (ee_ipc.py:33-36)
+    contact_psd: int = 1             # 1: PSD-project the barrier Hessian (mu_k = B' lam_k, clamped);
+                                     # 0: reference form, clamp lam_k then scale by B' < 0
+                                     #    (pt_ipc.py:166, 266-269)
+    enable_pt: bool = True           # const_params.py:41-43
+    enable_ee: bool = True
+    enable_vg: bool = True
+    solver: int = SOLVER_BICGSTAB    # reference solver: bicgstab (abd.py:244)
+    cg_tol: float = 1e-10            # relative residual of the Newton linear solve
+    cg_max_iter: int = 2000
+    precision: int = PRECISION_FP64
+    refine_tol: float = 1e-10        # mixed precision: FP64 refinement target
+
+    @property
+    def d2hat(self) -> float:
+        return self.dhat * self.dhat
+
+    def to_c(self) -> "CParams":
+        c = CParams()
+        c.dt = self.dt
+        c.dhat = self.dhat
+        c.d2hat = self.d2hat
+        c.kappa = self.kappa
+        c.stiffness = self.stiffness
+        c.gravity = self.gravity
+        c.tol = self.tol
+        c.c1 = self.c1
+        c.alpha_min = self.alpha_min
+        c.ground = self.ground
+        c.cg_tol = self.cg_tol
+        c.refine_tol = self.refine_tol
+        c.max_iter = self.max_iter
+        c.armijo_sign = self.armijo_sign
+        c.ground_enabled = int(self.ground_enabled)
+        c.psd_ee = int(self.psd_ee)
+        c.enable_pt = int(self.enable_pt)
+        c.enable_ee = int(self.enable_ee)
+        c.enable_vg = int(self.enable_vg)
+        c.solver = self.solver
+        c.cg_max_iter = self.cg_max_iter
+        c.precision = self.precision
+        c.contact_psd = self.contact_psd
+        return c
+
+    def as_dict(self):
+        return asdict(self)
+
+
+class CParams(ctypes.Structure):
+    """Mirror of ``abd_params`` in include/abd_b200.h (and of the oracle's copy)."""
+    _fields_ = [
+        ("dt", ctypes.c_double), ("dhat", ctypes.c_double), ("d2hat", ctypes.c_double),
+        ("kappa", ctypes.c_double), ("stiffness", ctypes.c_double), ("gravity", ctypes.c_double),
+        ("tol", ctypes.c_double), ("c1", ctypes.c_double), ("alpha_min", ctypes.c_double),
+        ("ground", ctypes.c_double), ("cg_tol", ctypes.c_double), ("refine_tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int), ("armijo_sign", ctypes.c_int), ("ground_enabled", ctypes.c_int),
+        ("psd_ee", ctypes.c_int), ("enable_pt", ctypes.c_int), ("enable_ee", ctypes.c_int),
+        ("enable_vg", ctypes.c_int), ("solver", ctypes.c_int), ("cg_max_iter", ctypes.c_int),
+        ("precision", ctypes.c_int), ("contact_psd", ctypes.c_int),
+    ]

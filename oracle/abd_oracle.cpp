@@ -1,0 +1,1389 @@
+// CPU FP64 oracle: a restatement of the reference ABD implicit contact step.
+//
+// TEST INFRASTRUCTURE ONLY.  Loaded by tests/, __graft_entry__.smoke() and bench.py's
+// CPU-baseline leg as the checker; the product path (abd_warp_b200/, libabd_b200.so) never
+// links or calls it.
+//
+// Follows, function by function (citations are to the reference project's files):
+//   step / line search / ccd driver ........ abd/abd.py:124-362
+//   inertia + orthogonality ................ abd/orthogonal_energy.py:24-135
+//   barrier ................................ abd/ipcsk/barrier.py:3-49
+//   PT / EE / VG gradient + Hessian ........ abd/ipcsk/pt_ipc.py:111-287, ee_ipc.py:13-218,
+//                                            vg_ipc.py:4-34, put.py:25-66
+//   contact energy ......................... abd/ipcsk/energy.py:9-48
+//   distance geometry + eigensystem ........ abd/psd/vf.py:3-71, psd/ee.py:5-163,
+//                                            psd/hl.py:15-39,155-195
+//   CCD .................................... abd/ccd.py:9-195, abd/cubic_roots.py:6-193
+//   culling (intended cull_ semantics) ..... abd/culling.py:32-99, abd/culling2.py:32-280
+// with the corrections of the reference's evident defects: PT/EE lists used consistently,
+// per-body-pair culling instead of the hard-wired pair (0,1), the full coupled Hessian,
+// capacity-free lists, per-body mass / I0, fixed (Dirichlet) bodies, and the Armijo sign
+// selectable (armijo_sign = -1 correct, +1 the reference's form).
+//
+// Parity pin: the per-pair math is checked against oracle/np_ref.py and the reference's
+// known-answer fixtures (tests/golden).  Whole-step trajectories cannot be checked
+// against the reference itself (it does not run without Warp and abdtk): the step-level
+// parity of this oracle is unpinned with respect to the reference's own execution.
+//
+// Build: oracle/Makefile  (g++ -O2 -fopenmp -ffp-contract=off).  No FMA contraction, so
+// elementwise arithmetic matches the CUDA build (nvcc -fmad=false) bit for bit where the
+// operation order is the same.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <omp.h>
+
+namespace {
+
+struct Params {
+  double dt, dhat, d2hat, kappa, stiffness, gravity, tol, c1, alpha_min, ground, cg_tol, refine_tol;
+  int max_iter, armijo_sign, ground_enabled, psd_ee, enable_pt, enable_ee, enable_vg, solver,
+      cg_max_iter, precision, contact_psd;
+};
+
+struct V3 {
+  double x, y, z;
+};
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator*(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline double comp(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+struct Box {
+  float lo[3], hi[3];
+};
+inline bool overlap(const Box& a, const Box& b) {
+  for (int k = 0; k < 3; ++k)
+    if (a.lo[k] > b.hi[k] || b.lo[k] > a.hi[k]) return false;
+  return true;
+}
+
+struct Cand {
+  int I, J, pair, pi, pj;  // vec5i (I, J, ij index, prim of I, prim of J)
+};
+
+struct Oracle {
+  int n, V, T, E;
+  std::vector<int> voff, toff, eoff, tris, edges, fixed;
+  std::vector<double> x0, mass, I0;
+  Params prm;
+  // states, [n][9] row-major A (row k = a_k) and [n][3] p
+  std::vector<double> A, p, Ak, pk, Adot, pdot, A0, p0;
+  std::vector<double> dq, g;  // [n][12]
+  std::vector<double> x, xk, xview;
+  // assembled system
+  std::vector<double> diag;       // [n][144]
+  std::vector<double> off;        // [npairs][144], block (I,J) with I<J
+  std::vector<int> ij;            // [npairs][2]
+  // stats
+  int stat_newton = 0, stat_lin = 0, stat_ls = 0, stat_pt = 0, stat_ee = 0, stat_vg = 0, stat_ij = 0,
+      stat_active = 0;
+  double stat_alpha = 0, stat_toi = 0, stat_energy = 0;
+};
+
+// ---------------------------------------------------------------------------------------
+// transform + boxes (abd.py:305-324, culling2.py:32-79, 229-280)
+// ---------------------------------------------------------------------------------------
+void transform(const Oracle& o, const double* A, const double* p, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < o.n; ++b) {
+    const double* a = A + 9 * b;
+    for (int v = o.voff[b]; v < o.voff[b + 1]; ++v) {
+      const double r0 = o.x0[3 * v], r1 = o.x0[3 * v + 1], r2 = o.x0[3 * v + 2];
+      for (int j = 0; j < 3; ++j)
+        out[3 * v + j] = ((a[0 * 3 + j] * r0 + a[1 * 3 + j] * r1) + a[2 * 3 + j] * r2) + p[3 * b + j];
+    }
+  }
+}
+
+struct Boxes {
+  std::vector<Box> pt, ed, tr, body;
+};
+
+void static_boxes(const Oracle& o, const double* y, Boxes& bx) {
+  const double dh = o.prm.dhat, dhh = o.prm.dhat * 0.5;
+  bx.pt.resize(o.V);
+  bx.ed.resize(o.E);
+  bx.tr.resize(o.T);
+  bx.body.resize(o.n);
+  const float dhf = (float)dh;
+#pragma omp parallel for schedule(static)
+  for (int v = 0; v < o.V; ++v)
+    for (int k = 0; k < 3; ++k) {
+      float c = (float)y[3 * v + k];
+      bx.pt[v].lo[k] = c - dhf;
+      bx.pt[v].hi[k] = c + dhf;
+    }
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < o.E; ++e) {
+    const int a = o.edges[2 * e], b = o.edges[2 * e + 1];
+    for (int k = 0; k < 3; ++k) {
+      double lo = std::min(y[3 * a + k], y[3 * b + k]);
+      double hi = std::max(y[3 * a + k], y[3 * b + k]);
+      bx.ed[e].lo[k] = (float)(lo - dhh);
+      bx.ed[e].hi[k] = (float)(hi + dhh);
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < o.T; ++t) {
+    const int a = o.tris[3 * t], b = o.tris[3 * t + 1], c = o.tris[3 * t + 2];
+    for (int k = 0; k < 3; ++k) {
+      double lo = std::min(std::min(y[3 * a + k], y[3 * b + k]), y[3 * c + k]);
+      double hi = std::max(std::max(y[3 * a + k], y[3 * b + k]), y[3 * c + k]);
+      bx.tr[t].lo[k] = (float)(lo - 0.0);
+      bx.tr[t].hi[k] = (float)(hi + 0.0);
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < o.n; ++b) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int v = o.voff[b]; v < o.voff[b + 1]; ++v)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], y[3 * v + k]);
+        hi[k] = std::max(hi[k], y[3 * v + k]);
+      }
+    for (int k = 0; k < 3; ++k) {
+      bx.body[b].lo[k] = (float)(lo[k] - dhh);
+      bx.body[b].hi[k] = (float)(hi[k] + dhh);
+    }
+  }
+}
+
+// swept boxes: the static (dilated) boxes at x united with the undilated boxes at xk
+void swept_boxes(const Oracle& o, const double* x, const double* xk, Boxes& bx) {
+  static_boxes(o, x, bx);
+  auto grow = [](Box& b, int k, double lo, double hi) {
+    b.lo[k] = std::min(b.lo[k], (float)lo);
+    b.hi[k] = std::max(b.hi[k], (float)hi);
+  };
+#pragma omp parallel for schedule(static)
+  for (int v = 0; v < o.V; ++v)
+    for (int k = 0; k < 3; ++k) grow(bx.pt[v], k, xk[3 * v + k], xk[3 * v + k]);
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < o.E; ++e) {
+    const int a = o.edges[2 * e], b = o.edges[2 * e + 1];
+    for (int k = 0; k < 3; ++k)
+      grow(bx.ed[e], k, std::min(xk[3 * a + k], xk[3 * b + k]), std::max(xk[3 * a + k], xk[3 * b + k]));
+  }
+#pragma omp parallel for schedule(static)
+  for (int t = 0; t < o.T; ++t) {
+    const int a = o.tris[3 * t], b = o.tris[3 * t + 1], c = o.tris[3 * t + 2];
+    for (int k = 0; k < 3; ++k)
+      grow(bx.tr[t], k, std::min(std::min(xk[3 * a + k], xk[3 * b + k]), xk[3 * c + k]),
+           std::max(std::max(xk[3 * a + k], xk[3 * b + k]), xk[3 * c + k]));
+  }
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < o.n; ++b) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int v = o.voff[b]; v < o.voff[b + 1]; ++v)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], xk[3 * v + k]);
+        hi[k] = std::max(hi[k], xk[3 * v + k]);
+      }
+    for (int k = 0; k < 3; ++k) grow(bx.body[b], k, lo[k], hi[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// culling: body pairs (culling2.py:213-227), primitive pairs (culling.py:85-99),
+// vertex-ground (culling.py:64-82)
+// ---------------------------------------------------------------------------------------
+struct Lists {
+  std::vector<int> ij;      // [m][2], I < J
+  std::vector<Cand> pt, ee;
+  std::vector<int> vg;      // [k][2] (body, global vertex)
+};
+
+void cull(const Oracle& o, const Boxes& bx, Lists& L) {
+  L.ij.clear();
+  for (int I = 0; I < o.n; ++I)
+    for (int J = I + 1; J < o.n; ++J)
+      if (overlap(bx.body[I], bx.body[J])) {
+        L.ij.push_back(I);
+        L.ij.push_back(J);
+      }
+  const int m = (int)L.ij.size() / 2;
+  std::vector<std::vector<Cand>> ptp(m), eep(m);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int q = 0; q < m; ++q) {
+    const int I = L.ij[2 * q], J = L.ij[2 * q + 1];
+    // primitives of each body that can touch the other body's box (exact prefilter:
+    // every primitive box lies inside its body box)
+    auto near = [&](const std::vector<Box>& bs, int lo, int hi, const Box& other) {
+      std::vector<int> r;
+      for (int i = lo; i < hi; ++i)
+        if (overlap(bs[i], other)) r.push_back(i);
+      return r;
+    };
+    // a point box (+-dhat) is not inside its body box (+-dhat/2): triangles are
+    // prefiltered by the union of the near points' boxes instead
+    auto unite = [&](const std::vector<int>& ids) {
+      Box u;
+      for (int k = 0; k < 3; ++k) {
+        u.lo[k] = INFINITY;
+        u.hi[k] = -INFINITY;
+      }
+      for (int i : ids)
+        for (int k = 0; k < 3; ++k) {
+          u.lo[k] = std::min(u.lo[k], bx.pt[i].lo[k]);
+          u.hi[k] = std::max(u.hi[k], bx.pt[i].hi[k]);
+        }
+      return u;
+    };
+    if (o.prm.enable_pt) {
+      std::vector<int> pI = near(bx.pt, o.voff[I], o.voff[I + 1], bx.body[J]);
+      if (!pI.empty()) {
+        std::vector<int> tJ = near(bx.tr, o.toff[J], o.toff[J + 1], unite(pI));
+        for (int a : pI)
+          for (int t : tJ)
+            if (overlap(bx.pt[a], bx.tr[t])) ptp[q].push_back({I, J, q, a - o.voff[I], t - o.toff[J]});
+      }
+      std::vector<int> pJ = near(bx.pt, o.voff[J], o.voff[J + 1], bx.body[I]);
+      if (!pJ.empty()) {
+        std::vector<int> tI = near(bx.tr, o.toff[I], o.toff[I + 1], unite(pJ));
+        for (int a : pJ)
+          for (int t : tI)
+            if (overlap(bx.pt[a], bx.tr[t])) ptp[q].push_back({J, I, q, a - o.voff[J], t - o.toff[I]});
+      }
+    }
+    if (o.prm.enable_ee) {
+      std::vector<int> eI = near(bx.ed, o.eoff[I], o.eoff[I + 1], bx.body[J]);
+      std::vector<int> eJ = near(bx.ed, o.eoff[J], o.eoff[J + 1], bx.body[I]);
+      for (int a : eI)
+        for (int b : eJ)
+          if (overlap(bx.ed[a], bx.ed[b])) eep[q].push_back({I, J, q, a - o.eoff[I], b - o.eoff[J]});
+    }
+  }
+  L.pt.clear();
+  L.ee.clear();
+  for (int q = 0; q < m; ++q) {
+    L.pt.insert(L.pt.end(), ptp[q].begin(), ptp[q].end());
+    L.ee.insert(L.ee.end(), eep[q].begin(), eep[q].end());
+  }
+  L.vg.clear();
+  if (o.prm.ground_enabled && o.prm.enable_vg) {
+    const float g32 = (float)o.prm.ground;
+    Box gq;
+    gq.lo[0] = gq.lo[1] = gq.lo[2] = -1e3f;
+    gq.hi[0] = 1e3f;
+    gq.hi[1] = g32;
+    gq.hi[2] = 1e3f;
+    for (int b = 0; b < o.n; ++b) {
+      if (!((double)bx.body[b].lo[1] < 0.5 * o.prm.dhat + o.prm.ground)) continue;
+      for (int v = o.voff[b]; v < o.voff[b + 1]; ++v)
+        if (overlap(bx.pt[v], gq)) {
+          L.vg.push_back(b);
+          L.vg.push_back(v);
+        }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// per-primitive geometry (psd/vf.py, psd/ee.py, psd/hl.py, ccd.py:44-54)
+// ---------------------------------------------------------------------------------------
+inline void solve22(V3 e0, V3 e1, V3 e2, double& beta, double& gamma) {
+  const double a = dot(e0, e0), b = dot(e0, e1), d = dot(e1, e1);
+  const double det = a * d - b * b;
+  const double s = 1.0 / det;
+  const double i00 = d * s, i01 = -b * s, i10 = -b * s, i11 = a * s;
+  const double r0 = dot(e0, e2), r1 = dot(e1, e2);
+  beta = i00 * r0 + i01 * r1;
+  gamma = i10 * r0 + i11 * r1;
+}
+
+struct Geo {
+  V3 e0, e1p, e2p;
+  double alpha, beta, gamma;
+};
+
+// type 0: point-triangle (x0 point; x1,x2,x3 triangle); type 1: edge-edge
+inline Geo geometry(int type, V3 x0, V3 x1, V3 x2, V3 x3) {
+  Geo G;
+  V3 e0, e1, e2;
+  if (type == 0) {
+    e0 = x1 - x2;
+    e1 = x3 - x2;
+    e2 = x0 - x2;
+  } else {
+    e0 = x1 - x0;
+    e1 = x3 - x2;
+    e2 = x2 - x0;
+  }
+  G.alpha = dot(e0, e1) / dot(e0, e0);
+  G.e0 = e0;
+  G.e1p = e1 - G.alpha * e0;
+  solve22(e0, e1, e2, G.beta, G.gamma);
+  G.e2p = (e2 - G.beta * e0) - G.gamma * e1;
+  return G;
+}
+
+inline bool valid_root(int type, double beta, double gamma) {
+  if (type == 0) return 0.0 < beta && beta < 1.0 && 0.0 < gamma && gamma < 1.0 && 0.0 < beta + gamma &&
+                        beta + gamma < 1.0;
+  return 0.0 < beta && beta < 1.0 && 0.0 < -gamma && -gamma < 1.0;
+}
+
+inline double signed_distance(V3 e0p, V3 e1p, V3 e2p) {
+  V3 n = cross(e0p, e1p);
+  return dot(e2p, n) / std::sqrt(dot(n, n));
+}
+
+inline double barrier(double d, const Params& P) {
+  if (d < P.d2hat) {
+    const double s = d / P.d2hat;
+    return P.kappa * -std::pow(s - 1.0, 2.0) * std::log(s);
+  }
+  return 0.0;
+}
+inline double barrier_d1(double d, const Params& P) {
+  if (d < P.d2hat)
+    return P.kappa * (P.d2hat - d) * (2.0 * std::log(d / P.d2hat) + (d - P.d2hat) / d) / (P.d2hat * P.d2hat);
+  return 0.0;
+}
+inline double barrier_d2(double d, const Params& P) {
+  if (d < P.d2hat)
+    return -P.kappa *
+           (2.0 * std::log(d / P.d2hat) + (d - P.d2hat) / d + (d - P.d2hat) * (2.0 / d + P.d2hat / (d * d))) /
+           (P.d2hat * P.d2hat);
+  return 0.0;
+}
+
+// Contact gradient (24) and Hessian blocks (3 x 12x12) of one PT/EE pair
+// (pt_ipc.py:111-185, 194-246; ee_ipc.py:381-475).  Returns false when inactive.
+bool contact_gh(int type, const V3 xs[4], const V3 rs[4], const Params& P, double& d2out, double g24[24],
+                double Hi[144], double Hj[144], double Hij[144]) {
+  Geo G = geometry(type, xs[0], xs[1], xs[2], xs[3]);
+  const bool valid = valid_root(type, G.beta, G.gamma);
+  double d2;
+  if (type == 0) {
+    const double l = signed_distance(G.e0, G.e1p, G.e2p);
+    d2 = l * l;
+  } else {
+    d2 = dot(G.e2p, G.e2p);
+  }
+  d2out = d2;
+  if (!(d2 < P.d2hat && valid)) return false;
+  const double l = signed_distance(G.e0, G.e1p, G.e2p);
+  const double e0pn = dot(G.e0, G.e0), e1pn = dot(G.e1p, G.e1p), e2pn = dot(G.e2p, G.e2p);
+  const double f12 = std::sqrt(1.0 + 4.0 * (e1pn / e2pn));
+  const double f02 = std::sqrt(1.0 + 4.0 * (e0pn / e2pn));
+  double lam[5];
+  lam[0] = -l / (2.0 * e1pn) * (1.0 + f12);
+  lam[1] = -l / (2.0 * e1pn) * (1.0 - f12);
+  lam[2] = -l / (2.0 * e0pn) * (1.0 + f02);
+  lam[3] = -l / (2.0 * e0pn) * (1.0 - f02);
+  double om[4];
+  for (int k = 0; k < 4; ++k) om[k] = lam[k] / (lam[k] - l / e2pn);
+  double Q[5][9];
+  std::memset(Q, 0, sizeof(Q));
+  for (int k = 0; k < 2; ++k) {
+    V3 t = om[k] * G.e1p;
+    Q[k][3] = G.e2p.x; Q[k][4] = G.e2p.y; Q[k][5] = G.e2p.z;
+    Q[k][6] = t.x; Q[k][7] = t.y; Q[k][8] = t.z;
+  }
+  for (int k = 2; k < 4; ++k) {
+    V3 t = om[k] * G.e0;
+    Q[k][0] = G.e2p.x; Q[k][1] = G.e2p.y; Q[k][2] = G.e2p.z;
+    Q[k][6] = t.x; Q[k][7] = t.y; Q[k][8] = t.z;
+  }
+  {
+    V3 gl2 = G.e2p * l;
+    gl2 = {gl2.x / e2pn, gl2.y / e2pn, gl2.z / e2pn};
+    V3 q4 = (gl2 * 2.0) * l;
+    Q[4][6] = q4.x; Q[4][7] = q4.y; Q[4][8] = q4.z;
+  }
+  for (int k = 0; k < 4; ++k) lam[k] = lam[k] * 2.0 * l;
+  lam[4] = 2.0;
+  const double Bp = barrier_d1(d2, P), Bpp = barrier_d2(d2, P);
+  double q4n = 0.0;
+  for (int i = 0; i < 9; ++i) q4n += Q[4][i] * Q[4][i];
+  if (P.contact_psd == 1) {
+    // projected barrier Hessian: eigenvalues of B' Hc + B'' q4 q4^T on the (orthogonal)
+    // eigenvectors q_k, clamped at zero; the B'' term is folded into the fifth pair
+    for (int k = 0; k < 4; ++k) lam[k] = std::max(Bp * lam[k], 0.0);
+    lam[4] = std::max(Bp * 2.0 + Bpp * q4n, 0.0);
+  } else if (type == 0 || P.psd_ee) {
+    for (int k = 0; k < 4; ++k) lam[k] = std::max(lam[k], 0.0);
+  }
+  // D (3x4): dcvfdx_s / dceedx_s
+  double D[3][4];
+  if (type == 0) {
+    const double al = G.alpha, be = G.beta, ga = G.gamma;
+    double t[3][4] = {{0.0, 1.0, -1.0, 0.0}, {0.0, -al, al - 1.0, 1.0}, {1.0, -be, be + ga - 1.0, -ga}};
+    std::memcpy(D, t, sizeof(D));
+  } else {
+    const double al = G.alpha, be = G.beta, ga = G.gamma;
+    double t[3][4] = {{-1.0, 1.0, 0.0, 0.0}, {al, -al, -1.0, 1.0}, {be - 1.0, -be, ga + 1.0, -ga}};
+    std::memcpy(D, t, sizeof(D));
+  }
+  // Hc = Q diag(lam) diag(1/|q|^2) Q^T   (QLQinv)
+  double qn[5];
+  for (int k = 0; k < 5; ++k) {
+    double s = 0.0;
+    for (int i = 0; i < 9; ++i) s += Q[k][i] * Q[k][i];
+    qn[k] = 1.0 / s;
+  }
+  double Hc[9][9];
+  for (int a = 0; a < 9; ++a)
+    for (int b = 0; b < 9; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < 5; ++k) s += (Q[k][a] * lam[k]) * (qn[k] * Q[k][b]);
+      Hc[a][b] = s;
+    }
+  // Hx = (D kron I)^T Hc (D kron I)  (dcTHldc), g12 = (D kron I)^T q4
+  double Hx[12][12], g12[12];
+  for (int j = 0; j < 4; ++j)
+    for (int a = 0; a < 3; ++a) {
+      double s = 0.0;
+      for (int i = 0; i < 3; ++i) s += D[i][j] * Q[4][3 * i + a];
+      g12[3 * j + a] = s;
+    }
+  {
+    double T1[9][12];  // Hc (D kron I)
+    for (int a = 0; a < 9; ++a)
+      for (int l2 = 0; l2 < 4; ++l2)
+        for (int b = 0; b < 3; ++b) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += Hc[a][3 * k + b] * D[k][l2];
+          T1[a][3 * l2 + b] = s;
+        }
+    for (int j = 0; j < 4; ++j)
+      for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 12; ++c) {
+          double s = 0.0;
+          for (int i = 0; i < 3; ++i) s += D[i][j] * T1[3 * i + a][c];
+          Hx[3 * j + a][c] = s;
+        }
+  }
+  double H12[12][12];
+  for (int a = 0; a < 12; ++a)
+    for (int b = 0; b < 12; ++b)
+      H12[a][b] = (P.contact_psd == 1) ? Hx[a][b] : Hx[a][b] * Bp + g12[a] * g12[b] * Bpp;
+  // body Jacobians: vertex v -> weights w_v = (1, r_v); PT: v0 in I, v1..3 in J;
+  // EE: v0,v1 in I, v2,v3 in J
+  const int nI = (type == 0) ? 1 : 2;
+  double w[4][4];
+  for (int v = 0; v < 4; ++v) {
+    w[v][0] = 1.0;
+    w[v][1] = rs[v].x;
+    w[v][2] = rs[v].y;
+    w[v][3] = rs[v].z;
+  }
+  // gradient: g_I[3m+a] = sum_{v in I} w_v[m] g12[3v+a] * B'
+  for (int m = 0; m < 4; ++m)
+    for (int a = 0; a < 3; ++a) {
+      double sI = 0.0, sJ = 0.0;
+      for (int v = 0; v < nI; ++v) sI += w[v][m] * g12[3 * v + a];
+      for (int v = nI; v < 4; ++v) sJ += w[v][m] * g12[3 * v + a];
+      g24[3 * m + a] = sI * Bp;
+      g24[12 + 3 * m + a] = sJ * Bp;
+    }
+  for (int m = 0; m < 4; ++m)
+    for (int a = 0; a < 3; ++a)
+      for (int n2 = 0; n2 < 4; ++n2)
+        for (int b = 0; b < 3; ++b) {
+          double sII = 0.0, sJJ = 0.0, sIJ = 0.0;
+          for (int u = 0; u < 4; ++u)
+            for (int v = 0; v < 4; ++v) {
+              const double h = w[u][m] * H12[3 * u + a][3 * v + b] * w[v][n2];
+              const bool uI = u < nI, vI = v < nI;
+              if (uI && vI) sII += h;
+              else if (!uI && !vI) sJJ += h;
+              else if (uI && !vI) sIJ += h;
+            }
+          Hi[(3 * m + a) * 12 + 3 * n2 + b] = sII;
+          Hj[(3 * m + a) * 12 + 3 * n2 + b] = sJJ;
+          Hij[(3 * m + a) * 12 + 3 * n2 + b] = sIJ;
+        }
+  return true;
+}
+
+inline void fetch(const Oracle& o, const double* y, const Cand& c, int type, V3 xs[4], V3 rs[4]) {
+  int ids[4];
+  if (type == 0) {
+    ids[0] = o.voff[c.I] + c.pi;
+    const int t = o.toff[c.J] + c.pj;
+    ids[1] = o.tris[3 * t];
+    ids[2] = o.tris[3 * t + 1];
+    ids[3] = o.tris[3 * t + 2];
+  } else {
+    const int ea = o.eoff[c.I] + c.pi, eb = o.eoff[c.J] + c.pj;
+    ids[0] = o.edges[2 * ea];
+    ids[1] = o.edges[2 * ea + 1];
+    ids[2] = o.edges[2 * eb];
+    ids[3] = o.edges[2 * eb + 1];
+  }
+  for (int k = 0; k < 4; ++k) {
+    xs[k] = {y[3 * ids[k]], y[3 * ids[k] + 1], y[3 * ids[k] + 2]};
+    rs[k] = {o.x0[3 * ids[k]], o.x0[3 * ids[k] + 1], o.x0[3 * ids[k] + 2]};
+  }
+}
+
+// contact energy of one candidate (ipcsk/energy.py:9-48)
+inline double contact_energy(int type, const V3 xs[4], const Params& P) {
+  Geo G = geometry(type, xs[0], xs[1], xs[2], xs[3]);
+  if (!valid_root(type, G.beta, G.gamma)) return 0.0;
+  double d2;
+  if (type == 0) {
+    d2 = dot(G.e2p, G.e2p);
+  } else {
+    const double d = signed_distance(G.e0, G.e1p, G.e2p);
+    d2 = d * d;
+  }
+  return barrier(d2, P);
+}
+
+// ---------------------------------------------------------------------------------------
+// inertia + orthogonality (orthogonal_energy.py:24-135)
+// ---------------------------------------------------------------------------------------
+inline V3 row(const double* A, int k) { return {A[3 * k], A[3 * k + 1], A[3 * k + 2]}; }
+
+void tilde(const Oracle& o, int b, double At[9], double pt[3]) {
+  const double dt = o.prm.dt;
+  for (int k = 0; k < 9; ++k) At[k] = o.A0[9 * b + k] + dt * o.Adot[9 * b + k];
+  const double gv[3] = {0.0, o.prm.gravity, 0.0};
+  for (int k = 0; k < 3; ++k) pt[k] = (o.p0[3 * b + k] + dt * o.pdot[3 * b + k]) + (dt * dt) * gv[k];
+}
+
+double inertia_energy(const Oracle& o, int b, const double* Ak, const double* pk) {
+  double At[9], pt[3];
+  tilde(o, b, At, pt);
+  const double* a = Ak + 9 * b;
+  double eo = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double t = dot(row(a, i), row(a, j)) - (i == j ? 1.0 : 0.0);
+      eo += t * t;
+    }
+  eo = eo * o.prm.stiffness;
+  V3 d0 = V3{pk[3 * b], pk[3 * b + 1], pk[3 * b + 2]} - V3{pt[0], pt[1], pt[2]};
+  V3 d1 = row(a, 0) - row(At, 0), d2 = row(a, 1) - row(At, 1), d3 = row(a, 2) - row(At, 2);
+  const double nm = dot(d0, d0) * o.mass[b] + (dot(d1, d1) + dot(d2, d2) + dot(d3, d3)) * o.I0[b];
+  return eo * o.prm.dt * o.prm.dt + 0.5 * nm;
+}
+
+void inertia_gh(const Oracle& o, int b, double g12[12], double H[144]) {
+  const double dt = o.prm.dt, ks = o.prm.stiffness;
+  const double* a = o.A.data() + 9 * b;
+  double At[9], pt[3];
+  tilde(o, b, At, pt);
+  for (int k = 0; k < 3; ++k) g12[k] = 0.0;
+  for (int ii = 1; ii < 4; ++ii) {
+    const int i = ii - 1;
+    V3 gr = V3{-a[3 * i], -a[3 * i + 1], -a[3 * i + 2]};
+    for (int j = 0; j < 3; ++j) gr = gr + dot(row(a, i), row(a, j)) * row(a, j);
+    gr = (gr * 4.0) * ks;
+    gr = (dt * dt) * gr;
+    g12[3 * ii] = gr.x;
+    g12[3 * ii + 1] = gr.y;
+    g12[3 * ii + 2] = gr.z;
+  }
+  const double m = o.mass[b], I0 = o.I0[b];
+  for (int k = 0; k < 3; ++k) g12[k] += (o.p[3 * b + k] - pt[k]) * m;
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) g12[3 * (r + 1) + k] += (a[3 * r + k] - At[3 * r + k]) * I0;
+  std::memset(H, 0, sizeof(double) * 144);
+  for (int ii = 0; ii < 4; ++ii)
+    for (int jj = 0; jj < 4; ++jj) {
+      double dh[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      const double mm = (ii != jj) ? 0.0 : (ii == 0 ? m : I0);
+      for (int k = 0; k < 3; ++k) dh[k][k] = mm;
+      if (ii > 0 && jj > 0) {
+        const int i = ii - 1, j = jj - 1;
+        double h[3][3];
+        if (i == j) {
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) h[r][c] = 0.0;
+          for (int k = 0; k < 3; ++k)
+            for (int r = 0; r < 3; ++r)
+              for (int c = 0; c < 3; ++c) h[r][c] += a[3 * k + r] * a[3 * k + c];
+          const double ti = dot(row(a, i), row(a, i)) - 1.0;
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) h[r][c] += (a[3 * i + r] * a[3 * i + c] + (r == c ? ti : 0.0));
+        } else {
+          const double tj = dot(row(a, j), row(a, i));
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) h[r][c] = a[3 * j + r] * a[3 * i + c] + (r == c ? tj : 0.0);
+        }
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) dh[r][c] = dh[r][c] + ((h[r][c] * 4.0) * ks) * dt * dt;
+      }
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) H[(3 * ii + r) * 12 + 3 * jj + c] = dh[r][c];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// assembly: g, diagonal blocks, off-diagonal blocks per body pair (put.py:25-66)
+// ---------------------------------------------------------------------------------------
+void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
+  const int n = o.n, m = (int)L.ij.size() / 2;
+  o.ij = L.ij;
+  o.g.assign(12 * n, 0.0);
+  o.diag.assign(144 * n, 0.0);
+  o.off.assign(144 * (size_t)m, 0.0);
+  std::vector<double> gb(12), Hb(144);
+  for (int b = 0; b < n; ++b) {
+    if (o.fixed[b]) continue;
+    inertia_gh(o, b, gb.data(), Hb.data());
+    for (int k = 0; k < 12; ++k) o.g[12 * b + k] += gb[k];
+    for (int k = 0; k < 144; ++k) o.diag[144 * b + k] += Hb[k];
+  }
+  struct Res {
+    bool active;
+    double g[24], Hi[144], Hj[144], Hij[144];
+  };
+  int active = 0;
+  for (int type = 0; type < 2; ++type) {
+    const std::vector<Cand>& C = type == 0 ? L.pt : L.ee;
+    const int nc = (int)C.size();
+    std::vector<Res> R(nc);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < nc; ++i) {
+      V3 xs[4], rs[4];
+      fetch(o, y, C[i], type, xs, rs);
+      double d2;
+      R[i].active = contact_gh(type, xs, rs, o.prm, d2, R[i].g, R[i].Hi, R[i].Hj, R[i].Hij);
+    }
+    for (int i = 0; i < nc; ++i) {
+      if (!R[i].active) continue;
+      ++active;
+      const int I = C[i].I, J = C[i].J, q = C[i].pair;
+      for (int k = 0; k < 12; ++k) {
+        o.g[12 * I + k] += R[i].g[k];
+        o.g[12 * J + k] += R[i].g[12 + k];
+      }
+      for (int k = 0; k < 144; ++k) {
+        o.diag[144 * I + k] += R[i].Hi[k];
+        o.diag[144 * J + k] += R[i].Hj[k];
+      }
+      double* blk = &o.off[144 * (size_t)q];
+      if (I < J) {
+        for (int k = 0; k < 144; ++k) blk[k] += R[i].Hij[k];
+      } else {
+        for (int r = 0; r < 12; ++r)
+          for (int c = 0; c < 12; ++c) blk[c * 12 + r] += R[i].Hij[r * 12 + c];
+      }
+    }
+  }
+  // vertex-ground terms (vg_ipc.py:4-34)
+  for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
+    const int b = L.vg[k], v = L.vg[k + 1];
+    const double d = y[3 * v + 1] - o.prm.ground;
+    const double d2b = barrier_d2(d * d, o.prm), db = barrier_d1(d * d, o.prm);
+    const double th[4] = {1.0, o.x0[3 * v], o.x0[3 * v + 1], o.x0[3 * v + 2]};
+    for (int ii = 0; ii < 4; ++ii) {
+      o.g[12 * b + 3 * ii + 1] += ((d * 2.0) * th[ii]) * db;
+      for (int jj = 0; jj < 4; ++jj)
+        o.diag[144 * b + (3 * ii + 1) * 12 + 3 * jj + 1] += (((th[ii] * th[jj]) * d2b) * 4.0) * d * d;
+    }
+  }
+  // Dirichlet rows/columns of fixed bodies
+  for (int b = 0; b < n; ++b) {
+    if (!o.fixed[b]) continue;
+    for (int k = 0; k < 12; ++k) o.g[12 * b + k] = 0.0;
+    for (int k = 0; k < 144; ++k) o.diag[144 * b + k] = (k % 13 == 0) ? 1.0 : 0.0;
+  }
+  for (int q = 0; q < m; ++q)
+    if (o.fixed[L.ij[2 * q]] || o.fixed[L.ij[2 * q + 1]])
+      std::fill(o.off.begin() + 144 * (size_t)q, o.off.begin() + 144 * (size_t)(q + 1), 0.0);
+  o.stat_active = active;
+}
+
+// ---------------------------------------------------------------------------------------
+// linear solve H dq = g: block-Jacobi preconditioned BiCGSTAB (reference solver choice,
+// abd.py:244) or PCG
+// ---------------------------------------------------------------------------------------
+double ddot(const std::vector<double>& a, const std::vector<double>& b) {
+  // fixed chunking: deterministic for any thread count
+  const size_t N = a.size(), CH = 4096, nch = (N + CH - 1) / CH;
+  std::vector<double> part(nch, 0.0);
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < (long)nch; ++c) {
+    double s = 0.0;
+    for (size_t i = c * CH; i < std::min(N, (c + 1) * CH); ++i) s += a[i] * b[i];
+    part[c] = s;
+  }
+  double s = 0.0;
+  for (double v : part) s += v;
+  return s;
+}
+
+void spmv(const Oracle& o, const std::vector<double>& xv, std::vector<double>& yv) {
+  const int n = o.n, m = (int)o.ij.size() / 2;
+  yv.assign(12 * n, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < n; ++b)
+    for (int r = 0; r < 12; ++r) {
+      double s = 0.0;
+      for (int c = 0; c < 12; ++c) s += o.diag[144 * b + r * 12 + c] * xv[12 * b + c];
+      yv[12 * b + r] = s;
+    }
+  for (int q = 0; q < m; ++q) {
+    const int I = o.ij[2 * q], J = o.ij[2 * q + 1];
+    const double* B = &o.off[144 * (size_t)q];
+    for (int r = 0; r < 12; ++r) {
+      double s = 0.0, t = 0.0;
+      for (int c = 0; c < 12; ++c) {
+        s += B[r * 12 + c] * xv[12 * J + c];
+        t += B[c * 12 + r] * xv[12 * I + c];
+      }
+      yv[12 * I + r] += s;
+      yv[12 * J + r] += t;
+    }
+  }
+}
+
+// inverse of a 12x12 block by Gauss-Jordan with partial pivoting
+void inv12(const double* Ain, double* out) {
+  double a[12][24];
+  for (int r = 0; r < 12; ++r)
+    for (int c = 0; c < 12; ++c) {
+      a[r][c] = Ain[r * 12 + c];
+      a[r][12 + c] = (r == c) ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < 12; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 12; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+    if (piv != c)
+      for (int k = 0; k < 24; ++k) std::swap(a[c][k], a[piv][k]);
+    const double inv = 1.0 / a[c][c];
+    for (int k = 0; k < 24; ++k) a[c][k] *= inv;
+    for (int r = 0; r < 12; ++r) {
+      if (r == c) continue;
+      const double f = a[r][c];
+      if (f != 0.0)
+        for (int k = 0; k < 24; ++k) a[r][k] -= f * a[c][k];
+    }
+  }
+  for (int r = 0; r < 12; ++r)
+    for (int c = 0; c < 12; ++c) out[r * 12 + c] = a[r][12 + c];
+}
+
+int solve(Oracle& o) {
+  const int n = o.n, N = 12 * n;
+  std::vector<double> Minv(144 * (size_t)n);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < n; ++b) inv12(&o.diag[144 * b], &Minv[144 * b]);
+  auto prec = [&](const std::vector<double>& v, std::vector<double>& out) {
+    out.resize(N);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < n; ++b)
+      for (int r = 0; r < 12; ++r) {
+        double s = 0.0;
+        for (int c = 0; c < 12; ++c) s += Minv[144 * b + r * 12 + c] * v[12 * b + c];
+        out[12 * b + r] = s;
+      }
+  };
+  std::vector<double>& x = o.dq;
+  const std::vector<double>& bvec = o.g;
+  const double bnorm = std::sqrt(ddot(bvec, bvec));
+  if (bnorm == 0.0) {
+    std::fill(x.begin(), x.end(), 0.0);
+    return 0;
+  }
+  const double thr = o.prm.cg_tol * bnorm;
+  std::vector<double> r(N), Ax;
+  spmv(o, x, Ax);
+  for (int i = 0; i < N; ++i) r[i] = bvec[i] - Ax[i];
+  if (std::sqrt(ddot(r, r)) <= thr) return 0;
+  int it = 0;
+  if (o.prm.solver == 1) {  // PCG
+    std::vector<double> z, pv, Ap;
+    prec(r, z);
+    pv = z;
+    double rz = ddot(r, z);
+    for (it = 1; it <= o.prm.cg_max_iter; ++it) {
+      spmv(o, pv, Ap);
+      const double alpha = rz / ddot(pv, Ap);
+      for (int i = 0; i < N; ++i) {
+        x[i] += alpha * pv[i];
+        r[i] -= alpha * Ap[i];
+      }
+      if (std::sqrt(ddot(r, r)) <= thr) break;
+      prec(r, z);
+      const double rzn = ddot(r, z);
+      const double beta = rzn / rz;
+      for (int i = 0; i < N; ++i) pv[i] = z[i] + beta * pv[i];
+      rz = rzn;
+    }
+    return std::min(it, o.prm.cg_max_iter);
+  }
+  // BiCGSTAB, right preconditioned
+  std::vector<double> rh = r, pv(N, 0.0), v(N, 0.0), y, s(N), z, t;
+  double rho_old = 1.0, alpha = 1.0, omega = 1.0;
+  for (it = 1; it <= o.prm.cg_max_iter; ++it) {
+    const double rho = ddot(rh, r);
+    if (rho == 0.0) break;
+    if (it == 1) {
+      pv = r;
+    } else {
+      const double beta = (rho / rho_old) * (alpha / omega);
+      for (int i = 0; i < N; ++i) pv[i] = r[i] + beta * (pv[i] - omega * v[i]);
+    }
+    prec(pv, y);
+    spmv(o, y, v);
+    alpha = rho / ddot(rh, v);
+    for (int i = 0; i < N; ++i) s[i] = r[i] - alpha * v[i];
+    if (std::sqrt(ddot(s, s)) <= thr) {
+      for (int i = 0; i < N; ++i) x[i] += alpha * y[i];
+      break;
+    }
+    prec(s, z);
+    spmv(o, z, t);
+    omega = ddot(t, s) / ddot(t, t);
+    for (int i = 0; i < N; ++i) {
+      x[i] += alpha * y[i] + omega * z[i];
+      r[i] = s[i] - omega * t[i];
+    }
+    if (std::sqrt(ddot(r, r)) <= thr) break;
+    rho_old = rho;
+  }
+  return std::min(it, o.prm.cg_max_iter);
+}
+
+// ---------------------------------------------------------------------------------------
+// CCD (ccd.py:56-195, cubic_roots.py:6-193)
+// ---------------------------------------------------------------------------------------
+const double X_ERROR = 1e-10;
+inline double evaluate(const double c[4], double x) { return c[0] + x * (c[1] + x * (c[2] + x * c[3])); }
+inline double multi_sign(double a, double b) { return b < 0.0 ? -a : a; }
+inline bool diff_sign(double y0, double yr) { return y0 * yr < 0.0; }
+
+double find_closed(const double coef[4], const double deriv[4], double x0, double x1, double y0, double y1) {
+  (void)y1;
+  double xr = (x0 + x1) / 2.0;
+  double yr = evaluate(coef, xr);
+  double xb0 = x0, xb1 = x1;
+  if (x1 - x0 <= X_ERROR * 2.0) return xr;
+  for (;;) {
+    if (diff_sign(y0, yr)) xb1 = xr;
+    else xb0 = xr;
+    const double dy = evaluate(deriv, xr);
+    const double dx = yr / dy;
+    const double xn = xr - dx;
+    if (xn > xb0 && xn < xb1) {
+      const double step = std::fabs(xr - xn);
+      xr = xn;
+      if (step > X_ERROR) yr = evaluate(coef, xr);
+      else break;
+    } else {
+      xr = (xb0 + xb1) / 2.0;
+      yr = evaluate(coef, xr);
+      if (xb0 == xr || xb1 == xr || xb1 - xb0 <= 2.0 * X_ERROR) break;
+    }
+  }
+  return xr;
+}
+
+int quadratic_roots(const double coef[3], double x0, double x1, double roots[2]) {
+  roots[0] = roots[1] = 0.0;
+  const double c = coef[0], b = coef[1], a = coef[2];
+  const double delta = b * b - 4.0 * a * c;
+  int ret = 0;
+  if (delta > 0.0) {
+    const double d = std::sqrt(delta);
+    const double q = -(b + multi_sign(d, b)) * 0.5;
+    const double rv0 = q / a, rv1 = c / q;
+    const double xa = rv0 < rv1 ? rv0 : rv1, xb = rv0 > rv1 ? rv0 : rv1;
+    if (xa >= x0 && xa <= x1) roots[ret++] = xa;
+    if (xb >= x0 && xb <= x1) roots[ret++] = xb;
+  } else if (delta < 0.0) {
+    ret = 0;
+  } else {
+    const double r0 = -0.5 * b / a;
+    roots[0] = r0;
+    if (r0 >= x0 && r0 <= x1) ret = 1;
+  }
+  return ret;
+}
+
+int cubic_roots(const double coef[4], double x0, double x1, double roots[3]) {
+  roots[0] = roots[1] = roots[2] = 0.0;
+  const double y0 = evaluate(coef, x0), y1 = evaluate(coef, x1);
+  const double a = coef[3] * 3.0, b_2 = coef[2], c = coef[1];
+  const double deriv[4] = {c, 2.0 * b_2, a, 0.0};
+  const double delta_4 = b_2 * b_2 - a * c;
+  auto deflate_solve = [&](double lo) {
+    double dp[3];
+    dp[2] = coef[3];
+    for (int i = 2; i > 0; --i) dp[i - 1] = coef[i] + roots[0] * dp[i];
+    double qr[2];
+    const int r = quadratic_roots(dp, lo, x1, qr);
+    roots[1] = qr[0];
+    roots[2] = qr[1];
+    return r + 1;
+  };
+  if (delta_4 > 0.0) {
+    const double d_2 = std::sqrt(delta_4);
+    const double q = -(b_2 + multi_sign(d_2, b_2));
+    const double rv0 = q / a, rv1 = c / q;
+    const double xa = rv0 < rv1 ? rv0 : rv1, xb = rv0 > rv1 ? rv0 : rv1;
+    if (diff_sign(y0, y1)) {
+      if (xa >= x1 || xb <= x0 || (xa <= x0 && xb >= x1)) {
+        roots[0] = find_closed(coef, deriv, x0, x1, y0, y1);
+        return 1;
+      }
+    } else {
+      if (xa >= x1 || xb <= x0 || (xa <= x0 && xb >= x1)) return 0;
+    }
+    if (xa > x0) {
+      const double ya = evaluate(coef, xa);
+      if (diff_sign(y0, ya)) {
+        roots[0] = find_closed(coef, deriv, x0, xa, y0, ya);
+        if (diff_sign(ya, y1) || (xb < x1 && diff_sign(ya, evaluate(coef, xb)))) return deflate_solve(xa);
+        return 1;
+      }
+      if (xb < x1) {
+        const double yb = evaluate(coef, xb);
+        if (diff_sign(ya, yb)) {
+          roots[0] = find_closed(coef, deriv, xa, xb, ya, yb);
+          if (diff_sign(yb, y1)) return deflate_solve(xb);
+          return 1;
+        }
+        if (diff_sign(yb, y1)) {
+          roots[0] = find_closed(coef, deriv, xb, x1, yb, y1);
+          return 1;
+        }
+      } else if (diff_sign(ya, y1)) {
+        roots[0] = find_closed(coef, deriv, xa, x1, ya, y1);
+        return 1;
+      }
+    } else {
+      const double yb = evaluate(coef, xb);
+      if (diff_sign(y0, yb)) {
+        roots[0] = find_closed(coef, deriv, x0, xb, y0, yb);
+        if (diff_sign(yb, y1)) return deflate_solve(xb);
+        return 1;
+      }
+      if (diff_sign(yb, y1)) {
+        roots[0] = find_closed(coef, deriv, xb, x1, yb, y1);
+        return 1;
+      }
+    }
+    return 0;
+  }
+  if (diff_sign(y0, y1)) {
+    roots[0] = find_closed(coef, deriv, x0, x1, y0, y1);
+    return 1;
+  }
+  return 0;
+}
+
+inline void cubic_binomial(const double a[3], const double b[3], double out[4]) {
+  out[0] = b[0] * b[1] * b[2];
+  out[1] = a[0] * b[1] * b[2] + b[0] * b[1] * a[2] + b[0] * a[1] * b[2];
+  out[2] = a[0] * a[1] * b[2] + a[0] * b[1] * a[2] + b[0] * a[1] * a[2];
+  out[3] = a[0] * a[1] * a[2];
+}
+
+// det(b + t a) of 3x3 matrices (row-major m[r][c])
+void det_polynomial(const double a[3][3], const double b[3][3], double out[4]) {
+  static const int P[6][3][2] = {{{0, 0}, {1, 1}, {2, 2}}, {{0, 1}, {1, 2}, {2, 0}}, {{0, 2}, {1, 0}, {2, 1}},
+                                 {{0, 0}, {1, 2}, {2, 1}}, {{0, 1}, {1, 0}, {2, 2}}, {{0, 2}, {1, 1}, {2, 0}}};
+  double pos[4] = {0, 0, 0, 0}, neg[4] = {0, 0, 0, 0};
+  for (int t = 0; t < 6; ++t) {
+    double av[3], bv[3], cb[4];
+    for (int k = 0; k < 3; ++k) {
+      av[k] = a[P[t][k][0]][P[t][k][1]];
+      bv[k] = b[P[t][k][0]][P[t][k][1]];
+    }
+    cubic_binomial(av, bv, cb);
+    double* dst = t < 3 ? pos : neg;
+    for (int k = 0; k < 4; ++k) dst[k] = dst[k] + cb[k];
+  }
+  for (int k = 0; k < 4; ++k) out[k] = pos[k] - neg[k];
+}
+
+// columns = the three points (wp.mat33(v0, v1, v2) is column-wise)
+inline void cols(V3 p, V3 q, V3 r, double m[3][3]) {
+  m[0][0] = p.x; m[1][0] = p.y; m[2][0] = p.z;
+  m[0][1] = q.x; m[1][1] = q.y; m[2][1] = q.z;
+  m[0][2] = r.x; m[1][2] = r.y; m[2][2] = r.z;
+}
+
+double collision_time(int type, const V3 a0[4], const V3 a1[4]) {
+  double A[4][3][3], B[4][3][3];
+  const int sel[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+  for (int k = 0; k < 4; ++k) {
+    cols(a1[sel[k][0]], a1[sel[k][1]], a1[sel[k][2]], A[k]);
+    cols(a0[sel[k][0]], a0[sel[k][1]], a0[sel[k][2]], B[k]);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) A[k][r][c] -= B[k][r][c];
+  }
+  double d[4][4];
+  for (int k = 0; k < 4; ++k) det_polynomial(A[k], B[k], d[k]);
+  double coef[4];
+  for (int k = 0; k < 4; ++k) coef[k] = ((d[0][k] - d[1][k]) + d[2][k]) - d[3][k];
+  double roots[3];
+  const int nr = cubic_roots(coef, 0.0, 1.0, roots);
+  double root = 1.0;
+  bool ok = false;
+  for (int i = 0; i < nr; ++i) {
+    root = roots[i];
+    V3 pt[4];
+    for (int k = 0; k < 4; ++k) pt[k] = a0[k] * (1.0 - root) + a1[k] * root;  // wp.lerp
+    Geo G = geometry(type, pt[0], pt[1], pt[2], pt[3]);
+    ok = valid_root(type, G.beta, G.gamma);
+    if (ok) break;
+  }
+  return ok ? root : 1.0;
+}
+
+// ---------------------------------------------------------------------------------------
+// driver (abd.py:124-362)
+// ---------------------------------------------------------------------------------------
+void update_qk(Oracle& o, double alpha) {
+  for (int b = 0; b < o.n; ++b) {
+    for (int k = 0; k < 3; ++k) o.pk[3 * b + k] = o.p[3 * b + k] - o.dq[12 * b + k] * alpha;
+    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < 3; ++k) o.Ak[9 * b + 3 * r + k] = o.A[9 * b + 3 * r + k] - o.dq[12 * b + 3 * (r + 1) + k] * alpha;
+  }
+}
+
+void update_q(Oracle& o, double alpha) {
+  for (int b = 0; b < o.n; ++b) {
+    for (int k = 0; k < 3; ++k) o.p[3 * b + k] = o.p[3 * b + k] - o.dq[12 * b + k] * alpha;
+    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < 3; ++k) o.A[9 * b + 3 * r + k] = o.A[9 * b + 3 * r + k] - o.dq[12 * b + 3 * (r + 1) + k] * alpha;
+  }
+}
+
+double energy_at(Oracle& o, const double* y, const double* Akp, const double* pkp) {
+  Boxes bx;
+  Lists L;
+  static_boxes(o, y, bx);
+  cull(o, bx, L);
+  double ec = 0.0;
+  for (int type = 0; type < 2; ++type) {
+    const std::vector<Cand>& C = type == 0 ? L.pt : L.ee;
+    const int nc = (int)C.size();
+    std::vector<double> e(nc);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nc; ++i) {
+      V3 xs[4], rs[4];
+      fetch(o, y, C[i], type, xs, rs);
+      e[i] = contact_energy(type, xs, o.prm);
+    }
+    for (int i = 0; i < nc; ++i) ec += e[i];
+  }
+  for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
+    const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
+    ec += barrier(d * d, o.prm);
+  }
+  double ei = 0.0;
+  for (int b = 0; b < o.n; ++b)
+    if (!o.fixed[b]) ei += inertia_energy(o, b, Akp, pkp);
+  return ec + ei;
+}
+
+double compute_energy(Oracle& o, double alpha) {
+  update_qk(o, alpha);
+  transform(o, o.Ak.data(), o.pk.data(), o.xk.data());
+  return energy_at(o, o.xk.data(), o.Ak.data(), o.pk.data());
+}
+
+double ccd_toi(Oracle& o, const double* x, const double* xk, double* raw) {
+  Boxes bx;
+  Lists L;
+  swept_boxes(o, x, xk, bx);
+  cull(o, bx, L);
+  double toi = 1.0;
+  for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
+    const int v = L.vg[k + 1];
+    const double d1 = xk[3 * v + 1] - o.prm.ground;
+    double t = 1.0;
+    if (d1 < 0) {
+      const double d0 = x[3 * v + 1] - o.prm.ground;
+      t = d0 / (d0 - d1);
+    }
+    if (t < 1.0) toi = std::min(toi, t);
+  }
+  for (int type = 0; type < 2; ++type) {
+    const std::vector<Cand>& C = type == 0 ? L.pt : L.ee;
+    const int nc = (int)C.size();
+    double tmin = 1.0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(min : tmin)
+    for (int i = 0; i < nc; ++i) {
+      V3 a0[4], a1[4], rs[4];
+      fetch(o, x, C[i], type, a0, rs);
+      fetch(o, xk, C[i], type, a1, rs);
+      const double t = collision_time(type, a0, a1);
+      if (t < 1.0) tmin = std::min(tmin, t);
+    }
+    toi = std::min(toi, tmin);
+  }
+  if (raw) *raw = toi;
+  double t = std::max(0.0, std::min(1.0, toi));
+  if (t < 1.0) t *= 0.9;
+  return t;
+}
+
+void step(Oracle& o) {
+  const int n = o.n;
+  o.A = o.A0;
+  o.p = o.p0;
+  o.Ak = o.A0;
+  o.pk = o.p0;
+  double E0 = compute_energy(o, 0.0);
+  int it = 0, lin = 0, ls = 0;
+  for (;;) {
+    transform(o, o.A.data(), o.p.data(), o.x.data());
+    o.xk = o.x;
+    Boxes bx;
+    Lists L;
+    static_boxes(o, o.x.data(), bx);
+    cull(o, bx, L);
+    if (it == 0) {
+      o.stat_pt = (int)L.pt.size();
+      o.stat_ee = (int)L.ee.size();
+      o.stat_vg = (int)L.vg.size() / 2;
+      o.stat_ij = (int)L.ij.size() / 2;
+    }
+    assemble(o, o.x.data(), bx, L);
+    lin += solve(o);
+    // CCD (abd.py:278-303)
+    update_qk(o, 1.0);
+    transform(o, o.Ak.data(), o.pk.data(), o.xk.data());
+    const double alpha_cap = ccd_toi(o, o.x.data(), o.xk.data(), &o.stat_toi);
+    // line search (abd.py:146-160)
+    const double qTg = ddot(o.dq, o.g);
+    double alpha = alpha_cap, E1;
+    for (;;) {
+      E1 = compute_energy(o, alpha);
+      ++ls;
+      const bool wolfe = E1 < E0 + o.prm.armijo_sign * o.prm.c1 * alpha * qTg;
+      if (wolfe || alpha < o.prm.alpha_min) break;
+      alpha *= 0.5;
+    }
+    E0 = E1;
+    update_q(o, alpha);
+    ++it;
+    o.stat_alpha = alpha;
+    const double gTg = ddot(o.g, o.g);
+    if (gTg < o.prm.tol || it >= o.prm.max_iter) break;
+  }
+  for (int b = 0; b < n; ++b) {
+    for (int k = 0; k < 3; ++k) {
+      o.pdot[3 * b + k] = (o.p[3 * b + k] - o.p0[3 * b + k]) / o.prm.dt;
+      o.p0[3 * b + k] = o.p[3 * b + k];
+    }
+    for (int k = 0; k < 9; ++k) {
+      o.Adot[9 * b + k] = (o.A[9 * b + k] - o.A0[9 * b + k]) / o.prm.dt;
+      o.A0[9 * b + k] = o.A[9 * b + k];
+    }
+  }
+  transform(o, o.A0.data(), o.p0.data(), o.xview.data());
+  o.stat_newton = it;
+  o.stat_lin = lin;
+  o.stat_ls = ls;
+  o.stat_energy = E0;
+}
+
+}  // namespace
+
+// =======================================================================================
+// C ABI for the tests (ctypes)
+// =======================================================================================
+extern "C" {
+
+struct orc_info {
+  int newton_iters, linear_iters, ls_trials, n_pt, n_ee, n_vg, n_ij, n_active;
+  double alpha, toi, energy;
+};
+
+void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const double* x0, const int* tris,
+                 const int* edges, const double* mass, const double* I0, const int* fixed, const Params* prm) {
+  Oracle* o = new Oracle();
+  o->n = n;
+  o->voff.assign(voff, voff + n + 1);
+  o->toff.assign(toff, toff + n + 1);
+  o->eoff.assign(eoff, eoff + n + 1);
+  o->V = o->voff[n];
+  o->T = o->toff[n];
+  o->E = o->eoff[n];
+  o->x0.assign(x0, x0 + 3 * (size_t)o->V);
+  o->tris.assign(tris, tris + 3 * (size_t)o->T);
+  o->edges.assign(edges, edges + 2 * (size_t)o->E);
+  o->mass.assign(mass, mass + n);
+  o->I0.assign(I0, I0 + n);
+  o->fixed.assign(fixed, fixed + n);
+  o->prm = *prm;
+  for (auto* v : {&o->A, &o->Ak, &o->Adot, &o->A0}) v->assign(9 * (size_t)n, 0.0);
+  for (auto* v : {&o->p, &o->pk, &o->pdot, &o->p0}) v->assign(3 * (size_t)n, 0.0);
+  o->dq.assign(12 * (size_t)n, 0.0);
+  o->g.assign(12 * (size_t)n, 0.0);
+  o->x.assign(3 * (size_t)o->V, 0.0);
+  o->xk = o->x;
+  o->xview = o->x;
+  return o;
+}
+
+void orc_destroy(void* h) { delete (Oracle*)h; }
+void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
+void orc_set_threads(int t) { omp_set_num_threads(t); }
+int orc_max_threads() { return omp_get_max_threads(); }
+
+void orc_set_state(void* h, const double* A0, const double* p0, const double* Adot, const double* pdot,
+                   const double* dq) {
+  Oracle* o = (Oracle*)h;
+  std::copy(A0, A0 + 9 * o->n, o->A0.begin());
+  std::copy(p0, p0 + 3 * o->n, o->p0.begin());
+  std::copy(Adot, Adot + 9 * o->n, o->Adot.begin());
+  std::copy(pdot, pdot + 3 * o->n, o->pdot.begin());
+  o->A = o->A0;
+  o->p = o->p0;
+  if (dq) std::copy(dq, dq + 12 * o->n, o->dq.begin());
+  else std::fill(o->dq.begin(), o->dq.end(), 0.0);
+}
+
+void orc_get_state(void* h, double* A0, double* p0, double* Adot, double* pdot, double* dq, double* xview) {
+  Oracle* o = (Oracle*)h;
+  if (A0) std::copy(o->A0.begin(), o->A0.end(), A0);
+  if (p0) std::copy(o->p0.begin(), o->p0.end(), p0);
+  if (Adot) std::copy(o->Adot.begin(), o->Adot.end(), Adot);
+  if (pdot) std::copy(o->pdot.begin(), o->pdot.end(), pdot);
+  if (dq) std::copy(o->dq.begin(), o->dq.end(), dq);
+  if (xview) std::copy(o->xview.begin(), o->xview.end(), xview);
+}
+
+int orc_step(void* h, orc_info* info) {
+  Oracle* o = (Oracle*)h;
+  step(*o);
+  if (info) {
+    info->newton_iters = o->stat_newton;
+    info->linear_iters = o->stat_lin;
+    info->ls_trials = o->stat_ls;
+    info->n_pt = o->stat_pt;
+    info->n_ee = o->stat_ee;
+    info->n_vg = o->stat_vg;
+    info->n_ij = o->stat_ij;
+    info->n_active = o->stat_active;
+    info->alpha = o->stat_alpha;
+    info->toi = o->stat_toi;
+    info->energy = o->stat_energy;
+  }
+  return 0;
+}
+
+void orc_transform(void* h, const double* A, const double* p, double* x) { transform(*(Oracle*)h, A, p, x); }
+
+// Culling lists.  mode 0: static boxes at y0; mode 1: swept boxes y0 -> y1.
+// Returns the counts in counts[4] = {ij, pt, ee, vg}; lists are written up to their caps.
+void orc_collision_set(void* h, int mode, const double* y0, const double* y1, int* ij, int* pt, int* ee, int* vg,
+                       int cap, int* counts) {
+  Oracle* o = (Oracle*)h;
+  Boxes bx;
+  Lists L;
+  if (mode == 0) static_boxes(*o, y0, bx);
+  else swept_boxes(*o, y0, y1, bx);
+  cull(*o, bx, L);
+  counts[0] = (int)L.ij.size() / 2;
+  counts[1] = (int)L.pt.size();
+  counts[2] = (int)L.ee.size();
+  counts[3] = (int)L.vg.size() / 2;
+  for (int i = 0; i < std::min(cap, counts[0]); ++i) {
+    ij[2 * i] = L.ij[2 * i];
+    ij[2 * i + 1] = L.ij[2 * i + 1];
+  }
+  for (int i = 0; i < std::min(cap, counts[1]); ++i) std::memcpy(pt + 5 * i, &L.pt[i], 5 * sizeof(int));
+  for (int i = 0; i < std::min(cap, counts[2]); ++i) std::memcpy(ee + 5 * i, &L.ee[i], 5 * sizeof(int));
+  for (int i = 0; i < std::min(cap, counts[3]); ++i) {
+    vg[2 * i] = L.vg[2 * i];
+    vg[2 * i + 1] = L.vg[2 * i + 1];
+  }
+}
+
+// Gradient and Hessian at the state set by orc_set_state with A, p overridden.  Outputs
+// g [n*12], diag [n*144], off [cap*144] (block (I,J) of ij pair q, I<J), ij [cap*2];
+// returns the number of body pairs.
+int orc_gh(void* h, const double* A, const double* p, double* g, double* diag, double* off, int* ij, int cap,
+           int* n_active) {
+  Oracle* o = (Oracle*)h;
+  std::copy(A, A + 9 * o->n, o->A.begin());
+  std::copy(p, p + 3 * o->n, o->p.begin());
+  transform(*o, o->A.data(), o->p.data(), o->x.data());
+  Boxes bx;
+  Lists L;
+  static_boxes(*o, o->x.data(), bx);
+  cull(*o, bx, L);
+  assemble(*o, o->x.data(), bx, L);
+  std::copy(o->g.begin(), o->g.end(), g);
+  std::copy(o->diag.begin(), o->diag.end(), diag);
+  const int m = (int)L.ij.size() / 2;
+  for (int q = 0; q < std::min(m, cap); ++q) {
+    std::copy(o->off.begin() + 144 * (size_t)q, o->off.begin() + 144 * (size_t)(q + 1), off + 144 * (size_t)q);
+    ij[2 * q] = L.ij[2 * q];
+    ij[2 * q + 1] = L.ij[2 * q + 1];
+  }
+  if (n_active) *n_active = o->stat_active;
+  return m;
+}
+
+// Energy at trial DOFs (Ak, pk) against the state set by orc_set_state.
+double orc_energy(void* h, const double* Ak, const double* pk) {
+  Oracle* o = (Oracle*)h;
+  std::vector<double> y(3 * (size_t)o->V);
+  transform(*o, Ak, pk, y.data());
+  return energy_at(*o, y.data(), Ak, pk);
+}
+
+// CCD step bound between DOFs (A, p) and (A1, p1): returns the capped alpha; raw toi too.
+double orc_ccd(void* h, const double* A, const double* p, const double* A1, const double* p1, double* raw) {
+  Oracle* o = (Oracle*)h;
+  std::vector<double> x(3 * (size_t)o->V), xk(3 * (size_t)o->V);
+  transform(*o, A, p, x.data());
+  transform(*o, A1, p1, xk.data());
+  return ccd_toi(*o, x.data(), xk.data(), raw);
+}
+
+// Per-pair contact terms for KATs: type 0 PT, 1 EE.  Returns active flag.
+int orc_contact_gh(int type, const double* xs12, const double* rs12, const Params* prm, double* d2, double* g24,
+                   double* Hi, double* Hj, double* Hij) {
+  V3 xs[4], rs[4];
+  for (int k = 0; k < 4; ++k) {
+    xs[k] = {xs12[3 * k], xs12[3 * k + 1], xs12[3 * k + 2]};
+    rs[k] = {rs12[3 * k], rs12[3 * k + 1], rs12[3 * k + 2]};
+  }
+  return contact_gh(type, xs, rs, *prm, *d2, g24, Hi, Hj, Hij) ? 1 : 0;
+}
+
+double orc_contact_energy(int type, const double* xs12, const Params* prm) {
+  V3 xs[4];
+  for (int k = 0; k < 4; ++k) xs[k] = {xs12[3 * k], xs12[3 * k + 1], xs12[3 * k + 2]};
+  return contact_energy(type, xs, *prm);
+}
+
+double orc_collision_time(int type, const double* p0_12, const double* p1_12) {
+  V3 a0[4], a1[4];
+  for (int k = 0; k < 4; ++k) {
+    a0[k] = {p0_12[3 * k], p0_12[3 * k + 1], p0_12[3 * k + 2]};
+    a1[k] = {p1_12[3 * k], p1_12[3 * k + 1], p1_12[3 * k + 2]};
+  }
+  return collision_time(type, a0, a1);
+}
+
+int orc_cubic_roots(const double* coef, double x0, double x1, double* roots) {
+  return cubic_roots(coef, x0, x1, roots);
+}
+
+// Solve with the system assembled by the last orc_gh; dq is the warm start, overwritten.
+int orc_solve(void* h, double* dq) {
+  Oracle* o = (Oracle*)h;
+  std::copy(dq, dq + 12 * o->n, o->dq.begin());
+  const int it = solve(*o);
+  std::copy(o->dq.begin(), o->dq.end(), dq);
+  return it;
+}
+
+}  // extern "C"
