@@ -1,0 +1,211 @@
+// Internal declarations shared by the CUDA translation units of libabd_b200.so.
+//
+// Build flags: -gencode arch=compute_100a,code=sm_100a -fmad=false.  Contraction of
+// multiply-add into FMA is off so that the FP64 elementwise arithmetic rounds exactly
+// like the CPU oracle; the heavy stages are memory- or latency-bound, not FMA-bound.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/abd_b200.h"
+
+namespace abd {
+
+// ---------------------------------------------------------------------------------------
+// status bits written by kernels into the simulator's device status word
+// ---------------------------------------------------------------------------------------
+enum : int {
+  ST_PT_OVERFLOW = 1,      // PT candidate list capacity exceeded (host grows and reruns)
+  ST_EE_OVERFLOW = 2,      // EE candidate list capacity exceeded
+  ST_PAIR_OVERFLOW = 4,    // body-pair capacity exceeded
+  ST_STACK_OVERFLOW = 8,   // BVH traversal stack exceeded (should not happen)
+  ST_SOLVER_NOCONV = 16,   // Krylov solve hit cg_max_iter
+  ST_NAN = 32,             // non-finite value in the Newton system
+  ST_VG_OVERFLOW = 64,     // VG list capacity exceeded
+};
+
+constexpr int kTraversalStack = 64;
+
+// ---------------------------------------------------------------------------------------
+// small vector helpers (FP64)
+// ---------------------------------------------------------------------------------------
+struct d3 {
+  double x, y, z;
+};
+__host__ __device__ inline d3 mk(double x, double y, double z) { return {x, y, z}; }
+__host__ __device__ inline d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__host__ __device__ inline d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__host__ __device__ inline d3 operator*(d3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__host__ __device__ inline d3 operator*(double s, d3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__host__ __device__ inline double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ inline d3 cross(d3 a, d3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ inline d3 ld3(const double* p) { return {p[0], p[1], p[2]}; }
+
+// f32 axis-aligned box, 32 B (one sector)
+struct __align__(16) Box {
+  float lo[3];
+  float pad0;
+  float hi[3];
+  float pad1;
+};
+
+__device__ inline bool overlap(const Box& a, const Box& b) {
+  return !(a.lo[0] > b.hi[0] || b.lo[0] > a.hi[0] || a.lo[1] > b.hi[1] || b.lo[1] > a.hi[1] ||
+           a.lo[2] > b.hi[2] || b.lo[2] > a.hi[2]);
+}
+
+__device__ inline Box load_box(const Box* p) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+  float4 a = __ldg(q), b = __ldg(q + 1);
+  Box r;
+  r.lo[0] = a.x; r.lo[1] = a.y; r.lo[2] = a.z; r.pad0 = 0.f;
+  r.hi[0] = b.x; r.hi[1] = b.y; r.hi[2] = b.z; r.pad1 = 0.f;
+  return r;
+}
+// L1-bypassing load for boxes written by other CTAs of the same kernel (refit)
+__device__ inline Box load_box_cg(const Box* p) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+  float4 a = __ldcg(q), b = __ldcg(q + 1);
+  Box r;
+  r.lo[0] = a.x; r.lo[1] = a.y; r.lo[2] = a.z; r.pad0 = 0.f;
+  r.hi[0] = b.x; r.hi[1] = b.y; r.hi[2] = b.z; r.pad1 = 0.f;
+  return r;
+}
+__device__ inline void store_box(Box* p, const Box& b) {
+  float4* q = reinterpret_cast<float4*>(p);
+  q[0] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
+  q[1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
+}
+
+// order-preserving encoding of a non-negative double for atomicMin on 64-bit integers
+__device__ inline unsigned long long dkey(double v) { return (unsigned long long)__double_as_longlong(v); }
+
+// ---------------------------------------------------------------------------------------
+// LBVH over the primitives of every body (one tree per primitive kind; each body's
+// primitives form a subtree whose root is body_root[b])
+// ---------------------------------------------------------------------------------------
+struct Tree {
+  int N = 0;              // leaves (primitives)
+  int* child = nullptr;   // [N-1][2] node ids: internal 0..N-2, leaf = N-1+sorted position
+  int* parent = nullptr;  // [2N-1]
+  int* leaf_prim = nullptr;   // [N] sorted position -> primitive index
+  int* prim_leaf = nullptr;   // [N] primitive index -> sorted position
+  int* body_root = nullptr;   // [n] node id of the body's subtree, -1 if the body has none
+  int* flags = nullptr;       // [N-1] refit arrival counters
+  Box* box = nullptr;         // [2N-1]
+};
+
+// ---------------------------------------------------------------------------------------
+// the simulator
+// ---------------------------------------------------------------------------------------
+struct Sim {
+  cudaStream_t stream = 0;
+  abd_params prm{};
+  int n = 0, V = 0, T = 0, E = 0;
+  int max_body_v = 0, max_body_t = 0, max_body_e = 0;
+  long long launches = 0;
+  int host_status = 0;   // status bits raised on the host (solver non-convergence)
+
+  // mesh (device)
+  int *voff = nullptr, *toff = nullptr, *eoff = nullptr;
+  int *vbody = nullptr, *tbody = nullptr, *ebody = nullptr;
+  int *tris = nullptr, *edges = nullptr;
+  double *x0 = nullptr, *mass = nullptr, *I0 = nullptr;
+  int* fixed = nullptr;
+  Tree tri_tree, edge_tree;
+
+  // positions
+  double *x = nullptr, *xk = nullptr;
+  Box* body_box = nullptr;  // [n]
+
+  // body pairs
+  int W = 0;                       // mask words per row
+  uint32_t* pair_mask = nullptr;   // [n][W]
+  int *row_ptr = nullptr, *upper_ptr = nullptr;  // [n+1]
+  int cap_pairs = 0, cap_adj = 0;
+  int2* ij = nullptr;              // [cap_pairs]
+  int *adj_col = nullptr, *adj_pair = nullptr;   // [cap_adj]
+  int n_pairs = 0, n_adj = 0;      // host copies after a culling pass
+
+  // candidate lists
+  int cap_pt = 0, cap_ee = 0, cap_vg = 0;
+  int *pt_list = nullptr, *ee_list = nullptr, *vg_list = nullptr;  // [cap][5], [cap][5], [cap][2]
+  int* pair_cand = nullptr;        // [cap_pairs][4] PT base, PT count, EE base, EE count
+
+  // per-pair scratch of the contact assembly
+  double *offdiag = nullptr;       // [cap_pairs][2][144]: H_IJ, H_JI
+  double *pdiag = nullptr;         // [cap_pairs][2][144]: contributions to diag I, diag J
+  double *pgrad = nullptr;         // [cap_pairs][2][12]
+  int* pair_active = nullptr;      // [cap_pairs] active contacts of the pair
+  double* pair_val = nullptr;      // [cap_pairs] energy or toi per pair
+  double* body_val = nullptr;      // [n]
+
+  // Newton system
+  double *g = nullptr, *dq = nullptr, *diag = nullptr, *Minv = nullptr;  // [n][12], [n][144]
+  float *diag32 = nullptr, *off32 = nullptr, *Minv32 = nullptr;          // mixed precision copies
+  // Krylov work vectors [n][12]
+  double *r = nullptr, *rh = nullptr, *pv = nullptr, *v = nullptr, *y = nullptr, *s = nullptr, *z = nullptr,
+         *t = nullptr, *ddq = nullptr;
+  double* partials = nullptr;      // reduction partials [kRedSlots][kRedBlocks]
+  double* scal = nullptr;          // solver scalars
+  int* dstat = nullptr;            // device: [0] status, [1..] counters
+  int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
+  double* hval = nullptr;          // pinned host scalars
+  unsigned long long* dmin = nullptr;  // device min accumulators
+};
+
+constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
+constexpr int kRedSlots = 8;
+
+// dstat layout
+enum : int {
+  DS_STATUS = 0,
+  DS_PT_COUNT = 1,
+  DS_EE_COUNT = 2,
+  DS_VG_COUNT = 3,
+  DS_ACTIVE = 4,
+  DS_SOLVER_DONE = 5,
+  DS_SOLVER_ITERS = 6,
+  DS_NSLOTS = 16
+};
+
+// ---------------------------------------------------------------------------------------
+// launchers (each returns cudaError_t of the launch)
+// ---------------------------------------------------------------------------------------
+// lbvh.cu
+cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body_dev, const double* centroid_dev,
+                       const int* prim_off_host);
+cudaError_t radix_sort_pairs(Sim& s, unsigned long long* keys, int* vals, unsigned long long* keys_tmp,
+                             int* vals_tmp, int N, int key_bits);
+cudaError_t refit(Sim& s, Tree& tr);
+
+// broad.cu
+cudaError_t transform(Sim& s, const double* A, const double* p, double* x);
+cudaError_t prim_boxes(Sim& s, const double* y0, const double* y1);
+cudaError_t body_boxes(Sim& s, const double* y0, const double* y1);
+cudaError_t body_pairs(Sim& s, bool* overflow);
+
+// narrow.cu
+enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS = 3 };
+cudaError_t narrow(Sim& s, int mode, const double* y0, const double* y1);
+cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y);
+cudaError_t body_energy(Sim& s, const abd_states& st, const double* Ak, const double* pk, const double* y);
+cudaError_t body_vg_toi(Sim& s, const double* y0, const double* y1);
+cudaError_t vg_list(Sim& s, const double* y0);
+cudaError_t sum_energy(Sim& s, double* out_dev);
+cudaError_t min_toi(Sim& s, double* out_dev);
+cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
+cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
+                        double* pout);
+cudaError_t finish_step(Sim& s, const abd_states& st, double* xview);
+cudaError_t dot_partials(Sim& s, const double* a, const double* b, int slot);
+cudaError_t finish_dot(Sim& s, int slot, double* out_dev);
+
+// solver.cu
+cudaError_t block_inverse(Sim& s);
+int krylov_solve(Sim& s, double* x, int* iters);  // returns ABD status
+
+}  // namespace abd

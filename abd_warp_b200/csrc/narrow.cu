@@ -1,0 +1,834 @@
+// Narrow phase and per-body terms.
+//
+// One CTA per body pair {I, J} (I < J) walks the LBVH subtrees of the other body for
+//   PT: every point of I against J's triangles, every point of J against I's triangles,
+//   EE: every edge of I against J's edges,
+// which is the reference's intended per-body-pair culling (cull_ / intersection_prims,
+// abd/culling.py:32-52, 85-99) with the same float32 box predicate.  The pass mode decides
+// what is done with each candidate:
+//   LISTS / GH: candidates are written as contiguous, deterministically ordered per-pair
+//       segments of the PT and EE lists (vec5i rows, as the reference's lists); GH then
+//       evaluates the contacts of the segment (pt_ipc.py:111-190, ee_ipc.py:381-430) and
+//       reduces them, in candidate order, into the pair's off-diagonal 12x12 block and its
+//       contributions to the two diagonal blocks and gradients (put.py:25-66).  The
+//       reduction replaces the reference's float atomics with a fixed-order sum, so the
+//       assembled system is bitwise reproducible.
+//   ENERGY: sum of barrier energies of the candidates (ipcsk/energy.py:9-48).
+//   CCD: minimum time of impact over the candidates (ccd.py:20-40, 133-186).
+// Per-body CTAs add inertia / orthogonality (orthogonal_energy.py:24-135) and the
+// vertex-ground terms (vg_ipc.py:4-34, culling.py:54-82, ccd.py:9-18, energy.py:24-33).
+#include <cuda_runtime.h>
+
+#include "abd_common.cuh"
+#include "abd_geometry.cuh"
+
+namespace abd {
+
+namespace {
+
+constexpr int NT = 128;          // threads per pair CTA
+constexpr int NW = NT / 32;
+constexpr int NOUT = 456;        // 144 off-diagonal + 2 x 144 diagonal + 2 x 12 gradient
+constexpr int NACC = (NOUT + 31) / 32;
+
+inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+struct NarrowArgs {
+  int mode;
+  abd_params prm;
+  int n_pairs;
+  const int2* ij;
+  const int *voff, *toff, *eoff, *tris, *edges;
+  const double *y0, *y1, *x0;
+  Tree tri, edge;
+  int *pt_list, *ee_list;
+  int cap_pt, cap_ee;
+  int* pair_cand;
+  int* dstat;
+  double *offdiag, *pdiag, *pgrad, *pair_val;
+  int* pair_active;
+};
+
+__device__ inline Box point_box(const double* y0, const double* y1, int v, float dhf) {
+  Box B;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float c = (float)y0[3 * v + k];
+    B.lo[k] = c - dhf;
+    B.hi[k] = c + dhf;
+    if (y1) {
+      const float c1 = (float)y1[3 * v + k];
+      B.lo[k] = fminf(B.lo[k], c1);
+      B.hi[k] = fmaxf(B.hi[k], c1);
+    }
+  }
+  return B;
+}
+
+// Stack traversal of the subtree rooted at `root`; calls f(prim) for every leaf whose box
+// overlaps q, in a fixed depth-first order.
+template <class F>
+__device__ inline void traverse(const Tree& tr, int root, const Box& q, int* dstat, F&& f) {
+  if (root < 0) return;
+  const int L0 = tr.N - 1;
+  if (root >= L0) {
+    if (overlap(load_box(&tr.box[root]), q)) f(__ldg(&tr.leaf_prim[root - L0]));
+    return;
+  }
+  if (!overlap(load_box(&tr.box[root]), q)) return;
+  int stack[kTraversalStack];
+  int sp = 0;
+  stack[sp++] = root;
+  while (sp > 0) {
+    const int node = stack[--sp];
+    const int c0 = __ldg(&tr.child[2 * node]), c1 = __ldg(&tr.child[2 * node + 1]);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = h ? c1 : c0;
+      if (!overlap(load_box(&tr.box[c]), q)) continue;
+      if (c >= L0) {
+        f(__ldg(&tr.leaf_prim[c - L0]));
+      } else if (sp < kTraversalStack) {
+        stack[sp++] = c;
+      } else {
+        atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
+      }
+    }
+  }
+}
+
+struct PairInfo {
+  int I, J, nPT1, nPT2, nEE;
+};
+
+__device__ inline PairInfo pair_info(const NarrowArgs& a, int p) {
+  PairInfo P;
+  const int2 ij = a.ij[p];
+  P.I = ij.x;
+  P.J = ij.y;
+  P.nPT1 = a.prm.enable_pt ? a.voff[P.I + 1] - a.voff[P.I] : 0;
+  P.nPT2 = a.prm.enable_pt ? a.voff[P.J + 1] - a.voff[P.J] : 0;
+  P.nEE = a.prm.enable_ee ? a.eoff[P.I + 1] - a.eoff[P.I] : 0;
+  return P;
+}
+
+// Visit every candidate of item k: f(type, pointOrEdgeBody, primA_global, primB_global)
+template <class F>
+__device__ inline void visit_item(const NarrowArgs& a, const PairInfo& P, int k, F&& f) {
+  const float dhf = (float)a.prm.dhat;
+  if (k < P.nPT1 + P.nPT2) {
+    const bool first = k < P.nPT1;
+    const int body = first ? P.I : P.J, other = first ? P.J : P.I;
+    const int v = a.voff[body] + (first ? k : k - P.nPT1);
+    const Box q = point_box(a.y0, a.y1, v, dhf);
+    traverse(a.tri, __ldg(&a.tri.body_root[other]), q, a.dstat, [&](int t) { f(0, first ? 0 : 1, v, t); });
+  } else {
+    const int e = a.eoff[P.I] + (k - P.nPT1 - P.nPT2);
+    const Box q = load_box(&a.edge.box[(a.edge.N - 1) + __ldg(&a.edge.prim_leaf[e])]);
+    traverse(a.edge, __ldg(&a.edge.body_root[P.J]), q, a.dstat, [&](int eb) { f(1, 0, e, eb); });
+  }
+}
+
+// global vertex ids of a candidate: PT (point v, triangle t), EE (edge a, edge b)
+__device__ inline void cand_vertices(const NarrowArgs& a, int type, int pa, int pb, int ids[4]) {
+  if (type == 0) {
+    ids[0] = pa;
+    ids[1] = __ldg(&a.tris[3 * pb]);
+    ids[2] = __ldg(&a.tris[3 * pb + 1]);
+    ids[3] = __ldg(&a.tris[3 * pb + 2]);
+  } else {
+    ids[0] = __ldg(&a.edges[2 * pa]);
+    ids[1] = __ldg(&a.edges[2 * pa + 1]);
+    ids[2] = __ldg(&a.edges[2 * pb]);
+    ids[3] = __ldg(&a.edges[2 * pb + 1]);
+  }
+}
+
+__device__ inline void fetch(const double* y, const int ids[4], d3 xs[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) xs[k] = mk(__ldg(&y[3 * ids[k]]), __ldg(&y[3 * ids[k] + 1]), __ldg(&y[3 * ids[k] + 2]));
+}
+
+// block-wide exclusive scan of one int per thread; returns the total
+__device__ inline int block_scan(int v, int* sh, int& excl) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int w = 0; w < NW; ++w) {
+      const int c = sh[w];
+      sh[w] = acc;
+      acc += c;
+    }
+    sh[NW] = acc;
+  }
+  __syncthreads();
+  excl = sh[warp] + x - v;
+  const int total = sh[NW];
+  __syncthreads();
+  return total;
+}
+
+__global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
+  const int p = blockIdx.x;
+  if (p >= a.n_pairs) return;
+  const PairInfo P = pair_info(a, p);
+  const int items = P.nPT1 + P.nPT2 + P.nEE;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ int sh[NW + 1];
+  __shared__ double shd[NT];
+
+  if (a.mode == NARROW_ENERGY || a.mode == NARROW_CCD) {
+    const bool ccd = a.mode == NARROW_CCD;
+    double acc = ccd ? 1.0 : 0.0;
+    for (int k = tid; k < items; k += NT) {
+      visit_item(a, P, k, [&](int type, int, int pa, int pb) {
+        int ids[4];
+        cand_vertices(a, type, pa, pb, ids);
+        d3 xs[4];
+        fetch(a.y0, ids, xs);
+        if (ccd) {
+          d3 x1[4];
+          fetch(a.y1, ids, x1);
+          const double t = collision_time(type, xs, x1);
+          if (t < 1.0) acc = fmin(acc, t);
+        } else {
+          acc += contact_energy(type, xs, a.prm);
+        }
+      });
+    }
+    shd[tid] = acc;
+    __syncthreads();
+    for (int s = NT / 2; s > 0; s >>= 1) {
+      if (tid < s) shd[tid] = ccd ? fmin(shd[tid], shd[tid + s]) : shd[tid] + shd[tid + s];
+      __syncthreads();
+    }
+    if (tid == 0) a.pair_val[p] = shd[0];
+    return;
+  }
+
+  // ---- LISTS / GH: two passes over the candidates (count, then write in order) ----
+  int cpt = 0, cee = 0;
+  for (int k = tid; k < items; k += NT)
+    visit_item(a, P, k, [&](int type, int, int, int) {
+      if (type == 0) ++cpt;
+      else ++cee;
+    });
+  int opt, oee;
+  const int tpt = block_scan(cpt, sh, opt);
+  const int tee = block_scan(cee, sh, oee);
+  __shared__ int base_pt, base_ee, ok;
+  if (tid == 0) {
+    base_pt = atomicAdd(&a.dstat[DS_PT_COUNT], tpt);
+    base_ee = atomicAdd(&a.dstat[DS_EE_COUNT], tee);
+    ok = 1;
+    if (base_pt + tpt > a.cap_pt) {
+      atomicOr(&a.dstat[DS_STATUS], ST_PT_OVERFLOW);
+      ok = 0;
+    }
+    if (base_ee + tee > a.cap_ee) {
+      atomicOr(&a.dstat[DS_STATUS], ST_EE_OVERFLOW);
+      ok = 0;
+    }
+    a.pair_cand[4 * p + 0] = base_pt;
+    a.pair_cand[4 * p + 1] = tpt;
+    a.pair_cand[4 * p + 2] = base_ee;
+    a.pair_cand[4 * p + 3] = tee;
+  }
+  __syncthreads();
+  if (!ok) {
+    if (tid == 0 && a.mode == NARROW_GH) a.pair_active[p] = 0;
+    return;
+  }
+  {
+    int wpt = base_pt + opt, wee = base_ee + oee;
+    for (int k = tid; k < items; k += NT)
+      visit_item(a, P, k, [&](int type, int swap, int pa, int pb) {
+        // (I, J, pair, local prim of I, local prim of J) with I the point's / first edge's body
+        int* row = type == 0 ? &a.pt_list[5 * (size_t)wpt++] : &a.ee_list[5 * (size_t)wee++];
+        const int bI = swap ? P.J : P.I, bJ = swap ? P.I : P.J;
+        row[0] = bI;
+        row[1] = bJ;
+        row[2] = p;
+        row[3] = type == 0 ? pa - a.voff[bI] : pa - a.eoff[bI];
+        row[4] = type == 0 ? pb - a.toff[bJ] : pb - a.eoff[bJ];
+      });
+  }
+  if (a.mode != NARROW_GH) return;
+  __syncthreads();  // the pair's list segment, written by this CTA, is now visible to it
+
+  // ---- GH: contacts of the segment, in candidate order ----
+  __shared__ int act[NT];
+  __shared__ double ush[NW][5][24];
+  __shared__ double red[NW][NOUT];
+  double accv[NACC];
+#pragma unroll
+  for (int j = 0; j < NACC; ++j) accv[j] = 0.0;
+  const int total = tpt + tee;
+  int nact_total = 0;
+  for (int c0 = 0; c0 < total; c0 += NT) {
+    const int c = c0 + tid;
+    int is_act = 0;
+    if (c < total) {
+      const int type = c < tpt ? 0 : 1;
+      const int* row = type == 0 ? &a.pt_list[5 * (size_t)(base_pt + c)] : &a.ee_list[5 * (size_t)(base_ee + c - tpt)];
+      const int pa = (type == 0 ? a.voff[row[0]] : a.eoff[row[0]]) + row[3];
+      const int pb = (type == 0 ? a.toff[row[1]] : a.eoff[row[1]]) + row[4];
+      int ids[4];
+      cand_vertices(a, type, pa, pb, ids);
+      d3 xs[4];
+      fetch(a.y0, ids, xs);
+      Geo G;
+      double d2;
+      is_act = contact_active(type, xs, a.prm, &G, &d2) ? 1 : 0;
+    }
+    int pos;
+    const int nact = block_scan(is_act, sh, pos);
+    if (is_act) act[pos] = c;
+    __syncthreads();
+    nact_total += nact;
+    for (int ai = warp; ai < nact; ai += NW) {
+      const int cc = act[ai];
+      const int type = cc < tpt ? 0 : 1;
+      const int* row =
+          type == 0 ? &a.pt_list[5 * (size_t)(base_pt + cc)] : &a.ee_list[5 * (size_t)(base_ee + cc - tpt)];
+      const int swap = row[0] != P.I;  // point / first vertex group belongs to body J
+      const int pa = (type == 0 ? a.voff[row[0]] : a.eoff[row[0]]) + row[3];
+      const int pb = (type == 0 ? a.toff[row[1]] : a.eoff[row[1]]) + row[4];
+      int ids[4];
+      cand_vertices(a, type, pa, pb, ids);
+      d3 xs[4];
+      fetch(a.y0, ids, xs);
+      Geo G;
+      double d2;
+      contact_active(type, xs, a.prm, &G, &d2);
+      ContactScalars C;
+      contact_scalars(type, G, d2, a.prm, C);
+      if (lane < 24) {
+        const int side = lane / 12, m = (lane % 12) / 3, comp = lane % 3;
+        const int group = side ^ swap;  // vertex group whose body is this side
+        const int v0 = type == 0 ? (group ? 1 : 0) : (group ? 2 : 0);
+        const int v1 = type == 0 ? (group ? 4 : 1) : (group ? 4 : 2);
+        double dw[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          double sacc = 0.0;
+          for (int v = v0; v < v1; ++v) {
+            const double w = m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]);
+            sacc += C.D[i][v] * w;
+          }
+          dw[i] = sacc;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          ush[warp][k][lane] = dw[0] * C.q[k][comp] + dw[1] * C.q[k][3 + comp] + dw[2] * C.q[k][6 + comp];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < NACC; ++j) {
+        const int e = lane + 32 * j;
+        if (e >= NOUT) break;
+        double v = 0.0;
+        if (e < 432) {
+          const int blk = e / 144, r = (e % 144) / 12, cidx = e % 12;
+          const int ra = blk == 2 ? 12 + r : r;
+          const int cb = blk == 1 ? cidx : 12 + cidx;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) v += C.coef[k] * (ush[warp][k][ra] * ush[warp][k][cb]);
+        } else {
+          v = C.gscale * ush[warp][4][e - 432];
+        }
+        accv[j] += v;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    a.pair_active[p] = nact_total;
+    if (nact_total) atomicAdd(&a.dstat[DS_ACTIVE], nact_total);
+  }
+  if (nact_total == 0) return;
+#pragma unroll
+  for (int j = 0; j < NACC; ++j) {
+    const int e = lane + 32 * j;
+    if (e < NOUT) red[warp][e] = accv[j];
+  }
+  __syncthreads();
+  for (int e = tid; e < NOUT; e += NT) {
+    double v = red[0][e];
+    for (int w = 1; w < NW; ++w) v += red[w][e];
+    if (e < 144) {
+      a.offdiag[(size_t)p * 288 + e] = v;
+      a.offdiag[(size_t)p * 288 + 144 + (e % 12) * 12 + e / 12] = v;
+    } else if (e < 432) {
+      a.pdiag[(size_t)p * 288 + (e - 144)] = v;
+    } else {
+      a.pgrad[(size_t)p * 24 + (e - 432)] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// per-body kernels
+// ---------------------------------------------------------------------------------------
+struct BodyArgs {
+  abd_params prm;
+  int n;
+  const int* voff;
+  const double *x0, *mass, *I0;
+  const int* fixed;
+  abd_states st;
+  const double *A, *p, *y, *y1;
+  const Box* body_box;
+  const int *row_ptr, *adj_pair, *pair_active;
+  const int2* ij;
+  const double *pdiag, *pgrad;
+  double *diag, *g, *body_val;
+  int* dstat;
+  int* vg_list;
+  int cap_vg;
+};
+
+__device__ inline void tilde(const BodyArgs& a, int b, double At[9], double pt[3]) {
+  const double dt = a.prm.dt;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) At[k] = a.st.A0[9 * b + k] + dt * a.st.Adot[9 * b + k];
+  const double gv[3] = {0.0, a.prm.gravity, 0.0};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) pt[k] = (a.st.p0[3 * b + k] + dt * a.st.pdot[3 * b + k]) + (dt * dt) * gv[k];
+}
+
+// does vertex v of body b take part in the vertex-ground terms (culling.py:64-82)?
+__device__ inline bool vg_candidate(const BodyArgs& a, const Box& bb, const double* y0, const double* y1, int v) {
+  if (!((double)bb.lo[1] < 0.5 * a.prm.dhat + a.prm.ground)) return false;
+  const Box q = point_box(y0, y1, v, (float)a.prm.dhat);
+  Box g;
+  g.lo[0] = g.lo[1] = g.lo[2] = -1e3f;
+  g.hi[0] = 1e3f;
+  g.hi[1] = (float)a.prm.ground;
+  g.hi[2] = 1e3f;
+  return overlap(q, g);
+}
+
+constexpr int BT = 160;
+
+__global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
+  const int b = blockIdx.x, t = threadIdx.x;
+  const bool fixed = a.fixed[b] != 0;
+  const double dt = a.prm.dt, ks = a.prm.stiffness;
+  const double* A = a.A + 9 * b;
+  double val = 0.0;
+  // vertex-ground partial sums: g (4 y-components) and H (4x4 yy-components)
+  __shared__ double vred[20][128];
+  const bool vg_on = a.prm.ground_enabled && a.prm.enable_vg && !fixed;
+  if (vg_on) {
+    double acc[20];
+#pragma unroll
+    for (int k = 0; k < 20; ++k) acc[k] = 0.0;
+    if (t < 128) {
+      const Box bb = load_box(&a.body_box[b]);
+      for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
+        if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
+        const double d = a.y[3 * v + 1] - a.prm.ground;
+        const double d2b = barrier_d2(d * d, a.prm), db = barrier_d1(d * d, a.prm);
+        const double th[4] = {1.0, a.x0[3 * v], a.x0[3 * v + 1], a.x0[3 * v + 2]};
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+          acc[ii] += ((d * 2.0) * th[ii]) * db;
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) acc[4 + 4 * ii + jj] += (((th[ii] * th[jj]) * d2b) * 4.0) * d * d;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 20; ++k) vred[k][t] = acc[k];
+    }
+    __syncthreads();
+    for (int s = 64; s > 0; s >>= 1) {
+      if (t < s)
+#pragma unroll
+        for (int k = 0; k < 20; ++k) vred[k][t] += vred[k][t + s];
+      __syncthreads();
+    }
+  }
+  if (t >= 156) return;
+  if (!fixed) {
+    double At[9], pt[3];
+    tilde(a, b, At, pt);
+    if (t < 144) {
+      const int r = t / 12, c = t % 12, ii = r / 3, jj = c / 3, rr = r % 3, cc = c % 3;
+      const double m = (ii != jj) ? 0.0 : (ii == 0 ? a.mass[b] : a.I0[b]);
+      double dh = rr == cc ? m : 0.0;
+      if (ii > 0 && jj > 0) {
+        const int i = ii - 1, j = jj - 1;
+        double h;
+        if (i == j) {
+          h = 0.0;
+          for (int k = 0; k < 3; ++k) h += A[3 * k + rr] * A[3 * k + cc];
+          const double ti = (A[3 * i] * A[3 * i] + A[3 * i + 1] * A[3 * i + 1] + A[3 * i + 2] * A[3 * i + 2]) - 1.0;
+          h += (A[3 * i + rr] * A[3 * i + cc] + (rr == cc ? ti : 0.0));
+        } else {
+          const double tj = A[3 * j] * A[3 * i] + A[3 * j + 1] * A[3 * i + 1] + A[3 * j + 2] * A[3 * i + 2];
+          h = A[3 * j + rr] * A[3 * i + cc] + (rr == cc ? tj : 0.0);
+        }
+        dh = dh + ((h * 4.0) * ks) * dt * dt;
+      }
+      val = dh;
+      if (vg_on && rr == 1 && cc == 1) val += vred[4 + 4 * ii + jj][0];
+    } else {
+      const int k = t - 144, m = k / 3, comp = k % 3;
+      if (m == 0) {
+        val = 0.0 + (a.p[3 * b + comp] - pt[comp]) * a.mass[b];
+      } else {
+        const int i = m - 1;
+        double gr = -A[3 * i + comp];
+        for (int j = 0; j < 3; ++j) {
+          const double dj = A[3 * i] * A[3 * j] + A[3 * i + 1] * A[3 * j + 1] + A[3 * i + 2] * A[3 * j + 2];
+          gr = gr + dj * A[3 * j + comp];
+        }
+        gr = (gr * 4.0) * ks;
+        gr = (dt * dt) * gr;
+        val = gr + (A[3 * i + comp] - At[3 * i + comp]) * a.I0[b];
+      }
+      if (vg_on && comp == 1) val += vred[m][0];
+    }
+    // contact contributions of the body's pairs, in adjacency (increasing neighbour) order
+    for (int k = a.row_ptr[b]; k < a.row_ptr[b + 1]; ++k) {
+      const int pr = a.adj_pair[k];
+      if (a.pair_active[pr] <= 0) continue;
+      const int side = a.ij[pr].x == b ? 0 : 1;
+      val += t < 144 ? a.pdiag[(size_t)pr * 288 + side * 144 + t] : a.pgrad[(size_t)pr * 24 + side * 12 + (t - 144)];
+    }
+    if (!isfinite(val)) atomicOr(&a.dstat[DS_STATUS], ST_NAN);
+  } else {
+    val = (t < 144 && (t % 13) == 0) ? 1.0 : 0.0;
+  }
+  if (t < 144) a.diag[(size_t)b * 144 + t] = val;
+  else a.g[(size_t)b * 12 + (t - 144)] = val;
+}
+
+__global__ void __launch_bounds__(128) k_body_energy(BodyArgs a) {
+  const int b = blockIdx.x, t = threadIdx.x;
+  __shared__ double red[128];
+  double acc = 0.0;
+  if (a.prm.ground_enabled && a.prm.enable_vg) {
+    const Box bb = load_box(&a.body_box[b]);
+    for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
+      if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
+      const double d = a.y[3 * v + 1] - a.prm.ground;
+      acc += barrier(d * d, a.prm);
+    }
+  }
+  red[t] = acc;
+  __syncthreads();
+  for (int s = 64; s > 0; s >>= 1) {
+    if (t < s) red[t] += red[t + s];
+    __syncthreads();
+  }
+  if (t == 0) {
+    double e = red[0];
+    if (!a.fixed[b]) {
+      double At[9], pt[3];
+      tilde(a, b, At, pt);
+      const double* K = a.A + 9 * b;  // trial DOFs Ak
+      double eo = 0.0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          const double tt = (K[3 * i] * K[3 * j] + K[3 * i + 1] * K[3 * j + 1] + K[3 * i + 2] * K[3 * j + 2]) -
+                            (i == j ? 1.0 : 0.0);
+          eo += tt * tt;
+        }
+      eo = eo * a.prm.stiffness;
+      const double* pk = a.p + 3 * b;
+      double d0[3], d1[3], d2[3], d3v[3];
+      for (int k = 0; k < 3; ++k) {
+        d0[k] = pk[k] - pt[k];
+        d1[k] = K[k] - At[k];
+        d2[k] = K[3 + k] - At[3 + k];
+        d3v[k] = K[6 + k] - At[6 + k];
+      }
+      auto dd = [](const double* u) { return u[0] * u[0] + u[1] * u[1] + u[2] * u[2]; };
+      const double nm = dd(d0) * a.mass[b] + (dd(d1) + dd(d2) + dd(d3v)) * a.I0[b];
+      e += eo * a.prm.dt * a.prm.dt + 0.5 * nm;
+    }
+    a.body_val[b] = e;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_body_vg_toi(BodyArgs a) {
+  const int b = blockIdx.x, t = threadIdx.x;
+  __shared__ double red[128];
+  double acc = 1.0;
+  if (a.prm.ground_enabled && a.prm.enable_vg) {
+    const Box bb = load_box(&a.body_box[b]);
+    for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
+      if (!vg_candidate(a, bb, a.y, a.y1, v)) continue;
+      const double d1 = a.y1[3 * v + 1] - a.prm.ground;
+      double tt = 1.0;
+      if (d1 < 0) {
+        const double d0 = a.y[3 * v + 1] - a.prm.ground;
+        tt = d0 / (d0 - d1);
+      }
+      if (tt < 1.0) acc = fmin(acc, tt);
+    }
+  }
+  red[t] = acc;
+  __syncthreads();
+  for (int s = 64; s > 0; s >>= 1) {
+    if (t < s) red[t] = fmin(red[t], red[t + s]);
+    __syncthreads();
+  }
+  if (t == 0) a.body_val[b] = red[0];
+}
+
+__global__ void k_vg_list(BodyArgs a) {
+  const int b = blockIdx.x;
+  const Box bb = load_box(&a.body_box[b]);
+  for (int v = a.voff[b] + threadIdx.x; v < a.voff[b + 1]; v += blockDim.x) {
+    if (!vg_candidate(a, bb, a.y, a.y1, v)) continue;
+    const int pos = atomicAdd(&a.dstat[DS_VG_COUNT], 1);
+    if (pos < a.cap_vg) {
+      a.vg_list[2 * pos] = b;
+      a.vg_list[2 * pos + 1] = v;
+    } else {
+      atomicOr(&a.dstat[DS_STATUS], ST_VG_OVERFLOW);
+    }
+  }
+}
+
+// deterministic single-CTA reduction of pair and body values (sum or min)
+__global__ void __launch_bounds__(1024) k_reduce_vals(const double* pv, int np, const double* bv, int nb, int is_min,
+                                                      double* out) {
+  __shared__ double red[1024];
+  const int t = threadIdx.x;
+  double acc = is_min ? 1.0 : 0.0;
+  for (int i = t; i < np; i += 1024) acc = is_min ? fmin(acc, pv[i]) : acc + pv[i];
+  for (int i = t; i < nb; i += 1024) acc = is_min ? fmin(acc, bv[i]) : acc + bv[i];
+  red[t] = acc;
+  __syncthreads();
+  for (int s = 512; s > 0; s >>= 1) {
+    if (t < s) red[t] = is_min ? fmin(red[t], red[t + s]) : red[t] + red[t + s];
+    __syncthreads();
+  }
+  if (t == 0) *out = red[0];
+}
+
+__global__ void k_export_off(int np, const int* pair_active, const double* offdiag, const int2* ij, double* out,
+                             int* ijout, int cap) {
+  const int p = blockIdx.x;
+  if (p >= np || p >= cap) return;
+  for (int e = threadIdx.x; e < 144; e += blockDim.x)
+    out[(size_t)p * 144 + e] = pair_active[p] > 0 ? offdiag[(size_t)p * 288 + e] : 0.0;
+  if (threadIdx.x == 0 && ijout) {
+    ijout[2 * p] = ij[p].x;
+    ijout[2 * p + 1] = ij[p].y;
+  }
+}
+
+__global__ void k_update_dofs(int n, const double* A, const double* p, const double* dq, double alpha, double* Ao,
+                              double* po) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) po[3 * b + k] = p[3 * b + k] - dq[12 * b + k] * alpha;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Ao[9 * b + 3 * r + k] = A[9 * b + 3 * r + k] - dq[12 * b + 3 * (r + 1) + k] * alpha;
+}
+
+__global__ void k_finish(int n, double dt, abd_states st) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  for (int k = 0; k < 3; ++k) {
+    st.pdot[3 * b + k] = (st.p[3 * b + k] - st.p0[3 * b + k]) / dt;
+    st.p0[3 * b + k] = st.p[3 * b + k];
+  }
+  for (int k = 0; k < 9; ++k) {
+    st.Adot[9 * b + k] = (st.A[9 * b + k] - st.A0[9 * b + k]) / dt;
+    st.A0[9 * b + k] = st.A[9 * b + k];
+  }
+}
+
+__global__ void k_dot_partials(int N, const double* a, const double* b, double* part) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < N; i += kRedBlocks * 256) acc += a[i] * b[i];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void k_finish_dot(const double* part, double* out) {
+  __shared__ double red[512];
+  const int t = threadIdx.x;
+  red[t] = t < kRedBlocks ? part[t] : 0.0;
+  __syncthreads();
+  for (int s = 256; s > 0; s >>= 1) {
+    if (t < s) red[t] += red[t + s];
+    __syncthreads();
+  }
+  if (t == 0) *out = red[0];
+}
+
+NarrowArgs narrow_args(Sim& s, int mode, const double* y0, const double* y1) {
+  NarrowArgs a;
+  a.mode = mode;
+  a.prm = s.prm;
+  a.n_pairs = s.n_pairs;
+  a.ij = s.ij;
+  a.voff = s.voff;
+  a.toff = s.toff;
+  a.eoff = s.eoff;
+  a.tris = s.tris;
+  a.edges = s.edges;
+  a.y0 = y0;
+  a.y1 = y1;
+  a.x0 = s.x0;
+  a.tri = s.tri_tree;
+  a.edge = s.edge_tree;
+  a.pt_list = s.pt_list;
+  a.ee_list = s.ee_list;
+  a.cap_pt = s.cap_pt;
+  a.cap_ee = s.cap_ee;
+  a.pair_cand = s.pair_cand;
+  a.dstat = s.dstat;
+  a.offdiag = s.offdiag;
+  a.pdiag = s.pdiag;
+  a.pgrad = s.pgrad;
+  a.pair_val = s.pair_val;
+  a.pair_active = s.pair_active;
+  return a;
+}
+
+BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* p, const double* y, const double* y1) {
+  BodyArgs a;
+  a.prm = s.prm;
+  a.n = s.n;
+  a.voff = s.voff;
+  a.x0 = s.x0;
+  a.mass = s.mass;
+  a.I0 = s.I0;
+  a.fixed = s.fixed;
+  if (st) a.st = *st;
+  else a.st = abd_states{};
+  a.A = A;
+  a.p = p;
+  a.y = y;
+  a.y1 = y1;
+  a.body_box = s.body_box;
+  a.row_ptr = s.row_ptr;
+  a.adj_pair = s.adj_pair;
+  a.pair_active = s.pair_active;
+  a.ij = s.ij;
+  a.pdiag = s.pdiag;
+  a.pgrad = s.pgrad;
+  a.diag = s.diag;
+  a.g = s.g;
+  a.body_val = s.body_val;
+  a.dstat = s.dstat;
+  a.vg_list = s.vg_list;
+  a.cap_vg = s.cap_vg;
+  return a;
+}
+
+}  // namespace
+
+cudaError_t narrow(Sim& s, int mode, const double* y0, const double* y1) {
+  if (s.n_pairs == 0) return cudaSuccess;
+  k_narrow<<<s.n_pairs, NT, 0, s.stream>>>(narrow_args(s, mode, y0, y1));
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y) {
+  k_body_gh<<<s.n, BT, 0, s.stream>>>(body_args(s, &st, A, p, y, nullptr));
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t body_energy(Sim& s, const abd_states& st, const double* Ak, const double* pk, const double* y) {
+  k_body_energy<<<s.n, 128, 0, s.stream>>>(body_args(s, &st, Ak, pk, y, nullptr));
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t body_vg_toi(Sim& s, const double* y0, const double* y1) {
+  k_body_vg_toi<<<s.n, 128, 0, s.stream>>>(body_args(s, nullptr, nullptr, nullptr, y0, y1));
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t vg_list(Sim& s, const double* y0) {
+  if (!(s.prm.ground_enabled && s.prm.enable_vg)) return cudaSuccess;
+  k_vg_list<<<s.n, 128, 0, s.stream>>>(body_args(s, nullptr, nullptr, nullptr, y0, nullptr));
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t vg_list_swept(Sim& s, const double* y0, const double* y1) {
+  if (!(s.prm.ground_enabled && s.prm.enable_vg)) return cudaSuccess;
+  k_vg_list<<<s.n, 128, 0, s.stream>>>(body_args(s, nullptr, nullptr, nullptr, y0, y1));
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t sum_energy(Sim& s, double* out) {
+  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.pair_val, s.n_pairs, s.body_val, s.n, 0, out);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t min_toi(Sim& s, double* out) {
+  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.pair_val, s.n_pairs, s.body_val, s.n, 1, out);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap) {
+  const int np = s.n_pairs < cap ? s.n_pairs : cap;
+  if (np == 0) return cudaSuccess;
+  k_export_off<<<np, 128, 0, s.stream>>>(s.n_pairs, s.pair_active, s.offdiag, s.ij, off_dev, ij_dev, cap);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
+                        double* pout) {
+  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, dq, alpha, Aout, pout);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t finish_step(Sim& s, const abd_states& st, double* xview) {
+  k_finish<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, s.prm.dt, st);
+  ++s.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !xview) return e;
+  return transform(s, st.A0, st.p0, xview);
+}
+
+cudaError_t dot_partials(Sim& s, const double* a, const double* b, int slot) {
+  k_dot_partials<<<kRedBlocks, 256, 0, s.stream>>>(12 * s.n, a, b, s.partials + slot * kRedBlocks);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t finish_dot(Sim& s, int slot, double* out) {
+  k_finish_dot<<<1, 512, 0, s.stream>>>(s.partials + slot * kRedBlocks, out);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+}  // namespace abd

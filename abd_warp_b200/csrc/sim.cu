@@ -1,0 +1,512 @@
+// Host orchestration and the C ABI (include/abd_b200.h).
+//
+// abd_step follows AffineBodySimulator.step (abd/abd.py:212-276) with the corrections of the
+// reference's defects: PT / EE lists used consistently in the energy and in CCD, the full
+// coupled Hessian (diagonal + both off-diagonal blocks of every contacting body pair),
+// capacity-checked lists that grow and rerun instead of writing out of bounds, and the
+// Armijo sign selectable.  Device work is issued on one stream; the host synchronises only
+// to read list counts, energies, the time of impact and the solver's convergence flags.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "abd_common.cuh"
+
+namespace abd {
+cudaError_t vg_list_swept(Sim& s, const double* y0, const double* y1);
+}
+
+struct abd_sim {
+  abd::Sim s;
+};
+
+namespace {
+
+using abd::Sim;
+
+#define CK(x)                                  \
+  do {                                         \
+    if ((x) != cudaSuccess) return ABD_ERR_CUDA; \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1));
+}
+
+template <class T>
+cudaError_t upload(T** p, const T* host, size_t count, cudaStream_t st) {
+  cudaError_t e = dalloc(p, count);
+  if (e != cudaSuccess || count == 0) return e;
+  return cudaMemcpyAsync(*p, host, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+}
+
+void free_tree(abd::Tree& t) {
+  for (void* q : {(void*)t.child, (void*)t.parent, (void*)t.leaf_prim, (void*)t.prim_leaf, (void*)t.body_root,
+                  (void*)t.flags, (void*)t.box})
+    if (q) cudaFree(q);
+  t = abd::Tree{};
+}
+
+int grow_pairs(Sim& s, int need) {
+  const int cap = std::max(need + need / 2, 2 * s.cap_pairs);
+  const int cap_adj = 2 * cap;
+  for (void* q : {(void*)s.ij, (void*)s.adj_col, (void*)s.adj_pair, (void*)s.pair_cand, (void*)s.offdiag,
+                  (void*)s.pdiag, (void*)s.pgrad, (void*)s.pair_active, (void*)s.pair_val})
+    if (q) cudaFree(q);
+  s.cap_pairs = cap;
+  s.cap_adj = cap_adj;
+  if (dalloc(&s.ij, cap) || dalloc(&s.adj_col, cap_adj) || dalloc(&s.adj_pair, cap_adj) ||
+      dalloc(&s.pair_cand, 4 * (size_t)cap) || dalloc(&s.offdiag, 288 * (size_t)cap) ||
+      dalloc(&s.pdiag, 288 * (size_t)cap) || dalloc(&s.pgrad, 24 * (size_t)cap) || dalloc(&s.pair_active, cap) ||
+      dalloc(&s.pair_val, cap))
+    return ABD_ERR_OVERFLOW;
+  return ABD_OK;
+}
+
+int grow_lists(Sim& s, int need_pt, int need_ee) {
+  if (need_pt > s.cap_pt) {
+    cudaFree(s.pt_list);
+    s.cap_pt = std::max(need_pt + need_pt / 2, 2 * s.cap_pt);
+    if (dalloc(&s.pt_list, 5 * (size_t)s.cap_pt)) return ABD_ERR_OVERFLOW;
+  }
+  if (need_ee > s.cap_ee) {
+    cudaFree(s.ee_list);
+    s.cap_ee = std::max(need_ee + need_ee / 2, 2 * s.cap_ee);
+    if (dalloc(&s.ee_list, 5 * (size_t)s.cap_ee)) return ABD_ERR_OVERFLOW;
+  }
+  return ABD_OK;
+}
+
+// Boxes, body pairs and the narrow pass of `mode` on positions y0 (static) or y0 -> y1
+// (swept).  Grows the capacities and reruns as needed.
+int culling(abd_sim* h, const double* y0, const double* y1, int mode) {
+  Sim& s = h->s;
+  CK(abd::prim_boxes(s, y0, y1));
+  CK(abd::body_boxes(s, y0, y1));
+  for (int tries = 0;; ++tries) {
+    bool ovf = false;
+    CK(abd::body_pairs(s, &ovf));
+    if (!ovf) break;
+    if (tries > 4) return ABD_ERR_OVERFLOW;
+    int st = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
+    if (st) return st;
+  }
+  const bool lists = mode == abd::NARROW_GH || mode == abd::NARROW_LISTS;
+  for (int tries = 0;; ++tries) {
+    if (lists) CK(cudaMemsetAsync(s.dstat + abd::DS_PT_COUNT, 0, 4 * sizeof(int), s.stream));
+    CK(abd::narrow(s, mode, y0, y1));
+    if (!lists) break;
+    CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    const int bits = s.hstat[abd::DS_STATUS];
+    if (!(bits & (abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW))) break;
+    if (tries > 4) return ABD_ERR_OVERFLOW;
+    int st = grow_lists(s, s.hstat[abd::DS_PT_COUNT], s.hstat[abd::DS_EE_COUNT]);
+    if (st) return st;
+    const int clear = bits & ~(abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW);
+    CK(cudaMemcpyAsync(s.dstat + abd::DS_STATUS, &clear, sizeof(int), cudaMemcpyHostToDevice, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+  }
+  return ABD_OK;
+}
+
+int read_scalar(Sim& s, const double* dev, double* out) {
+  CK(cudaMemcpyAsync(s.hval, dev, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  *out = s.hval[0];
+  return ABD_OK;
+}
+
+// E(Ak, pk): barrier over the culling lists at xk + inertia (compute_energy, abd.py:133-141)
+int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* pk, double* E) {
+  Sim& s = h->s;
+  CK(abd::transform(s, Ak, pk, s.xk));
+  int r = culling(h, s.xk, nullptr, abd::NARROW_ENERGY);
+  if (r) return r;
+  CK(abd::body_energy(s, st, Ak, pk, s.xk));
+  CK(abd::sum_energy(s, s.scal + 8));
+  return read_scalar(s, s.scal + 8, E);
+}
+
+// CCD bound between positions x (at A, p) and xk (at A1, p1) (ccd, abd.py:278-303)
+int ccd_at(abd_sim* h, const double* x, const double* xk, double* alpha, double* raw) {
+  Sim& s = h->s;
+  int r = culling(h, x, xk, abd::NARROW_CCD);
+  if (r) return r;
+  CK(abd::body_vg_toi(s, x, xk));
+  CK(abd::min_toi(s, s.scal + 9));
+  double toi;
+  r = read_scalar(s, s.scal + 9, &toi);
+  if (r) return r;
+  if (raw) *raw = toi;
+  double t = std::max(0.0, std::min(1.0, toi));
+  if (t < 1.0) t *= 0.9;
+  *alpha = t;
+  return ABD_OK;
+}
+
+int gh_at(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active) {
+  Sim& s = h->s;
+  CK(abd::transform(s, A, p, s.x));
+  int r = culling(h, s.x, nullptr, abd::NARROW_GH);
+  if (r) return r;
+  CK(abd::body_gh(s, st, A, p, s.x));
+  if (n_active) *n_active = s.hstat[abd::DS_ACTIVE];  // mirrored by culling after the narrow pass
+  return ABD_OK;
+}
+
+int take_status(abd_sim* h) {
+  Sim& s = h->s;
+  int bits = 0;
+  if (cudaMemcpyAsync(s.hstat + 21, s.dstat + abd::DS_STATUS, sizeof(int), cudaMemcpyDeviceToHost, s.stream) ==
+          cudaSuccess &&
+      cudaStreamSynchronize(s.stream) == cudaSuccess)
+    bits = s.hstat[21];
+  cudaMemsetAsync(s.dstat + abd::DS_STATUS, 0, sizeof(int), s.stream);
+  bits |= s.host_status;
+  s.host_status = 0;
+  return bits;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* abd_status_string(int code) {
+  switch (code) {
+    case ABD_OK: return "ok";
+    case ABD_ERR_CUDA: return "CUDA runtime error";
+    case ABD_ERR_INVALID: return "invalid argument";
+    case ABD_ERR_OVERFLOW: return "capacity could not be grown";
+    case ABD_ERR_DEVICE: return "device-side error";
+    default: return "unknown status";
+  }
+}
+
+int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream, abd_sim** out) {
+  if (!d || !prm || !out || d->n_bodies <= 0 || !d->vert_off || !d->tri_off || !d->edge_off || !d->x0 ||
+      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed)
+    return ABD_ERR_INVALID;
+  const int n = d->n_bodies;
+  const int V = d->vert_off[n], T = d->tri_off[n], E = d->edge_off[n];
+  if (V <= 0 || T < 0 || E < 0) return ABD_ERR_INVALID;
+  for (int b = 0; b < n; ++b)
+    if (d->vert_off[b + 1] < d->vert_off[b] || d->tri_off[b + 1] < d->tri_off[b] ||
+        d->edge_off[b + 1] < d->edge_off[b])
+      return ABD_ERR_INVALID;
+  std::vector<int> vbody(V), tbody(T), ebody(E);
+  for (int b = 0; b < n; ++b) {
+    for (int v = d->vert_off[b]; v < d->vert_off[b + 1]; ++v) vbody[v] = b;
+    for (int t = d->tri_off[b]; t < d->tri_off[b + 1]; ++t) {
+      tbody[t] = b;
+      for (int k = 0; k < 3; ++k) {
+        const int v = d->tris[3 * t + k];
+        if (v < d->vert_off[b] || v >= d->vert_off[b + 1]) return ABD_ERR_INVALID;
+      }
+    }
+    for (int e = d->edge_off[b]; e < d->edge_off[b + 1]; ++e) {
+      ebody[e] = b;
+      for (int k = 0; k < 2; ++k) {
+        const int v = d->edges[2 * e + k];
+        if (v < d->vert_off[b] || v >= d->vert_off[b + 1]) return ABD_ERR_INVALID;
+      }
+    }
+  }
+  abd_sim* h = new (std::nothrow) abd_sim();
+  if (!h) return ABD_ERR_OVERFLOW;
+  Sim& s = h->s;
+  s.stream = (cudaStream_t)stream;
+  s.prm = *prm;
+  s.n = n;
+  s.V = V;
+  s.T = T;
+  s.E = E;
+  // rest-space centroids for the Morton keys
+  std::vector<double> tc(3 * (size_t)T), ec(3 * (size_t)E);
+  for (int t = 0; t < T; ++t)
+    for (int k = 0; k < 3; ++k)
+      tc[3 * t + k] = (d->x0[3 * d->tris[3 * t] + k] + d->x0[3 * d->tris[3 * t + 1] + k] +
+                       d->x0[3 * d->tris[3 * t + 2] + k]) /
+                      3.0;
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < 3; ++k) ec[3 * e + k] = 0.5 * (d->x0[3 * d->edges[2 * e] + k] + d->x0[3 * d->edges[2 * e + 1] + k]);
+  double *tcd = nullptr, *ecd = nullptr;
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+    return e == cudaSuccess;
+  };
+  ok(upload(&s.voff, d->vert_off, n + 1, s.stream));
+  ok(upload(&s.toff, d->tri_off, n + 1, s.stream));
+  ok(upload(&s.eoff, d->edge_off, n + 1, s.stream));
+  ok(upload(&s.vbody, vbody.data(), V, s.stream));
+  ok(upload(&s.tbody, tbody.data(), T, s.stream));
+  ok(upload(&s.ebody, ebody.data(), E, s.stream));
+  ok(upload(&s.tris, d->tris, 3 * (size_t)T, s.stream));
+  ok(upload(&s.edges, d->edges, 2 * (size_t)E, s.stream));
+  ok(upload(&s.x0, d->x0, 3 * (size_t)V, s.stream));
+  ok(upload(&s.mass, d->mass, n, s.stream));
+  ok(upload(&s.I0, d->I0, n, s.stream));
+  ok(upload(&s.fixed, d->fixed, n, s.stream));
+  ok(upload(&tcd, tc.data(), tc.size(), s.stream));
+  ok(upload(&ecd, ec.data(), ec.size(), s.stream));
+  if (e == cudaSuccess) ok(abd::build_tree(s, s.tri_tree, T, s.tbody, tcd, d->tri_off));
+  if (e == cudaSuccess) ok(abd::build_tree(s, s.edge_tree, E, s.ebody, ecd, d->edge_off));
+  s.W = (n + 31) / 32;
+  ok(dalloc(&s.x, 3 * (size_t)V));
+  ok(dalloc(&s.xk, 3 * (size_t)V));
+  ok(dalloc(&s.body_box, n));
+  ok(dalloc(&s.pair_mask, (size_t)n * s.W));
+  ok(dalloc(&s.row_ptr, n + 1));
+  ok(dalloc(&s.upper_ptr, n + 1));
+  ok(dalloc(&s.body_val, n));
+  for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq}) ok(dalloc(v, 12 * (size_t)n));
+  ok(dalloc(&s.diag, 144 * (size_t)n));
+  ok(dalloc(&s.Minv, 144 * (size_t)n));
+  ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
+  ok(dalloc(&s.scal, 16));
+  ok(dalloc(&s.dstat, abd::DS_NSLOTS));
+  ok(dalloc(&s.dmin, 4));
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 8 * sizeof(double), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat, 0, sizeof(int) * abd::DS_NSLOTS, s.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+  if (tcd) cudaFree(tcd);
+  if (ecd) cudaFree(ecd);
+  if (e != cudaSuccess) {
+    abd_sim_destroy(h);
+    return ABD_ERR_CUDA;
+  }
+  s.cap_pairs = 0;
+  int r = grow_pairs(s, std::max(256, 4 * n));
+  s.cap_pt = 0;
+  s.cap_ee = 0;
+  if (!r) r = grow_lists(s, std::max(1 << 14, V / 4), std::max(1 << 14, E / 4));
+  s.cap_vg = std::max(1024, V);
+  if (!r && dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) r = ABD_ERR_OVERFLOW;
+  if (r) {
+    abd_sim_destroy(h);
+    return r;
+  }
+  *out = h;
+  return ABD_OK;
+}
+
+int abd_sim_destroy(abd_sim* h) {
+  if (!h) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  cudaStreamSynchronize(s.stream);
+  free_tree(s.tri_tree);
+  free_tree(s.edge_tree);
+  void* bufs[] = {s.voff, s.toff, s.eoff, s.vbody, s.tbody, s.ebody, s.tris, s.edges, s.x0, s.mass, s.I0,
+                  s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
+                  s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
+                  s.pair_active, s.pair_val, s.body_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
+                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin};
+  for (void* q : bufs)
+    if (q) cudaFree(q);
+  if (s.hstat) cudaFreeHost(s.hstat);
+  if (s.hval) cudaFreeHost(s.hval);
+  delete h;
+  return ABD_OK;
+}
+
+int abd_sim_set_params(abd_sim* h, const abd_params* prm) {
+  if (!h || !prm) return ABD_ERR_INVALID;
+  h->s.prm = *prm;
+  return ABD_OK;
+}
+
+int abd_sim_set_stream(abd_sim* h, void* stream) {
+  if (!h) return ABD_ERR_INVALID;
+  h->s.stream = (cudaStream_t)stream;
+  return ABD_OK;
+}
+
+int abd_sim_reset(abd_sim* h) {
+  if (!h) return ABD_ERR_INVALID;
+  CK(cudaMemsetAsync(h->s.dq, 0, sizeof(double) * 12 * h->s.n, h->s.stream));
+  return ABD_OK;
+}
+
+static int copy_vec(abd_sim* h, double* dst, const double* src) {
+  if (!h || !dst || !src) return ABD_ERR_INVALID;
+  CK(cudaMemcpyAsync(dst, src, sizeof(double) * 12 * h->s.n, cudaMemcpyDeviceToDevice, h->s.stream));
+  CK(cudaStreamSynchronize(h->s.stream));
+  return ABD_OK;
+}
+int abd_sim_get_dq(abd_sim* h, double* dst) { return h ? copy_vec(h, dst, h->s.dq) : ABD_ERR_INVALID; }
+int abd_sim_set_dq(abd_sim* h, const double* src) {
+  return h ? copy_vec(h, h->s.dq, src) : ABD_ERR_INVALID;
+}
+int abd_sim_get_g(abd_sim* h, double* dst) { return h ? copy_vec(h, dst, h->s.g) : ABD_ERR_INVALID; }
+
+int abd_sim_sizes(const abd_sim* h, int* n, int* V, int* T, int* E) {
+  if (!h) return ABD_ERR_INVALID;
+  if (n) *n = h->s.n;
+  if (V) *V = h->s.V;
+  if (T) *T = h->s.T;
+  if (E) *E = h->s.E;
+  return ABD_OK;
+}
+
+long long abd_launch_count(const abd_sim* h) { return h ? h->s.launches : 0; }
+
+int abd_take_status(abd_sim* h, int* status) {
+  if (!h || !status) return ABD_ERR_INVALID;
+  *status = take_status(h);
+  return ABD_OK;
+}
+
+int abd_update_mesh_vertex(abd_sim* h, const double* A, const double* p, double* x) {
+  if (!h || !A || !p || !x) return ABD_ERR_INVALID;
+  CK(abd::transform(h->s, A, p, x));
+  return ABD_OK;
+}
+
+int abd_collision_set(abd_sim* h, const double* y0, const double* y1, int counts[4]) {
+  if (!h || !y0 || !counts) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  int r = culling(h, y0, y1, abd::NARROW_LISTS);
+  if (r) return r;
+  for (int tries = 0;; ++tries) {
+    CK(cudaMemsetAsync(s.dstat + abd::DS_VG_COUNT, 0, sizeof(int), s.stream));
+    CK(y1 ? abd::vg_list_swept(s, y0, y1) : abd::vg_list(s, y0));
+    CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    if (s.hstat[abd::DS_VG_COUNT] <= s.cap_vg) break;
+    if (tries > 2) return ABD_ERR_OVERFLOW;
+    cudaFree(s.vg_list);
+    s.cap_vg = 2 * s.hstat[abd::DS_VG_COUNT];
+    if (dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) return ABD_ERR_OVERFLOW;
+  }
+  counts[0] = s.n_pairs;
+  counts[1] = s.hstat[abd::DS_PT_COUNT];
+  counts[2] = s.hstat[abd::DS_EE_COUNT];
+  counts[3] = s.hstat[abd::DS_VG_COUNT];
+  return ABD_OK;
+}
+
+int abd_export_lists(abd_sim* h, int* ij, int* pt, int* ee, int* vg, int cap) {
+  if (!h || cap < 0) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  const int npt = s.hstat[abd::DS_PT_COUNT], nee = s.hstat[abd::DS_EE_COUNT], nvg = s.hstat[abd::DS_VG_COUNT];
+  if (ij) CK(cudaMemcpyAsync(ij, s.ij, sizeof(int2) * std::min(cap, s.n_pairs), cudaMemcpyDeviceToDevice, s.stream));
+  if (pt) CK(cudaMemcpyAsync(pt, s.pt_list, sizeof(int) * 5 * std::min(cap, npt), cudaMemcpyDeviceToDevice, s.stream));
+  if (ee) CK(cudaMemcpyAsync(ee, s.ee_list, sizeof(int) * 5 * std::min(cap, nee), cudaMemcpyDeviceToDevice, s.stream));
+  if (vg) CK(cudaMemcpyAsync(vg, s.vg_list, sizeof(int) * 2 * std::min(cap, nvg), cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  return ABD_OK;
+}
+
+int abd_ipc_gh(abd_sim* h, const abd_states* st, const double* A, const double* p, int* n_active) {
+  if (!h || !st || !A || !p) return ABD_ERR_INVALID;
+  return gh_at(h, *st, A, p, n_active ? n_active : nullptr);
+}
+
+int abd_export_system(abd_sim* h, double* g, double* diag, double* off, int* ij, int cap, int* n_pairs) {
+  if (!h) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  if (g) CK(cudaMemcpyAsync(g, s.g, sizeof(double) * 12 * s.n, cudaMemcpyDeviceToDevice, s.stream));
+  if (diag) CK(cudaMemcpyAsync(diag, s.diag, sizeof(double) * 144 * s.n, cudaMemcpyDeviceToDevice, s.stream));
+  if (off) CK(abd::export_system(s, off, ij, cap));
+  CK(cudaStreamSynchronize(s.stream));
+  if (n_pairs) *n_pairs = s.n_pairs;
+  return ABD_OK;
+}
+
+int abd_solve(abd_sim* h, double* dq, int* iters) {
+  if (!h || !dq) return ABD_ERR_INVALID;
+  CK(abd::block_inverse(h->s));
+  return abd::krylov_solve(h->s, dq, iters);
+}
+
+int abd_compute_energy(abd_sim* h, const abd_states* st, const double* Ak, const double* pk, double* E) {
+  if (!h || !st || !Ak || !pk || !E) return ABD_ERR_INVALID;
+  return energy_at(h, *st, Ak, pk, E);
+}
+
+int abd_ccd(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
+            double* raw) {
+  if (!h || !A || !p || !A1 || !p1 || !alpha) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  CK(abd::transform(s, A, p, s.x));
+  CK(abd::transform(s, A1, p1, s.xk));
+  return ccd_at(h, s.x, s.xk, alpha, raw);
+}
+
+int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
+  if (!h || !stp) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  const abd_states& st = *stp;
+  const abd_params& P = s.prm;
+  const size_t nA = sizeof(double) * 9 * s.n, np = sizeof(double) * 3 * s.n;
+  // q <- q0 (abd.py:124-128)
+  CK(cudaMemcpyAsync(st.A, st.A0, nA, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaMemcpyAsync(st.p, st.p0, np, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaMemcpyAsync(st.Ak, st.A0, nA, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, s.stream));
+  abd_step_info inf{};
+  int r;
+  double E0;
+  CK(abd::update_dofs(s, st.A, st.p, s.dq, 0.0, st.Ak, st.pk));
+  if ((r = energy_at(h, st, st.Ak, st.pk, &E0))) return r;
+  int it = 0;
+  for (;;) {
+    int nact = 0;
+    if ((r = gh_at(h, st, st.A, st.p, &nact))) return r;
+    if (it == 0) {
+      inf.n_pt = s.hstat[abd::DS_PT_COUNT];
+      inf.n_ee = s.hstat[abd::DS_EE_COUNT];
+      inf.n_ij = s.n_pairs;
+    }
+    inf.n_active = nact;
+    int lin = 0;
+    CK(abd::block_inverse(s));
+    if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
+    inf.linear_iters += lin;
+    // CCD bound (abd.py:278-303)
+    CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
+    CK(abd::transform(s, st.Ak, st.pk, s.xk));
+    double alpha;
+    if ((r = ccd_at(h, s.x, s.xk, &alpha, &inf.toi))) return r;
+    // dq.g and g.g (abd.py:148, 265)
+    CK(abd::dot_partials(s, s.dq, s.g, 7));
+    CK(abd::finish_dot(s, 7, s.scal + 10));
+    CK(abd::dot_partials(s, s.g, s.g, 7));
+    CK(abd::finish_dot(s, 7, s.scal + 11));
+    CK(cudaMemcpyAsync(s.hval + 2, s.scal + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    const double qTg = s.hval[2], gTg = s.hval[3];
+    // backtracking line search (abd.py:146-160)
+    double E1 = E0;
+    for (;;) {
+      CK(abd::update_dofs(s, st.A, st.p, s.dq, alpha, st.Ak, st.pk));
+      if ((r = energy_at(h, st, st.Ak, st.pk, &E1))) return r;
+      ++inf.ls_trials;
+      const bool wolfe = E1 < E0 + P.armijo_sign * P.c1 * alpha * qTg;
+      if (wolfe || alpha < P.alpha_min) break;
+      alpha *= 0.5;
+    }
+    E0 = E1;
+    CK(abd::update_dofs(s, st.A, st.p, s.dq, alpha, st.A, st.p));
+    ++it;
+    inf.alpha = alpha;
+    if (gTg < P.tol || it >= P.max_iter) break;
+  }
+  CK(abd::finish_step(s, st, x_view));
+  inf.newton_iters = it;
+  inf.energy = E0;
+  inf.status = take_status(h);
+  inf.n_vg = 0;
+  if (info) *info = inf;
+  return (inf.status & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,273 @@
+"""``AffineBodySimulator``: the reference's simulator API (abd/abd.py:16-333) on the B200
+library.
+
+Construction mirrors ``AffineBodySimulator(config_file)`` / ``BaseSimulator.__init__``
+(abd/abd.py:21-95, simulator/base.py:31-45): the config JSON names a scene JSON whose
+``objects`` become :class:`AffineMesh` bodies.  Unlike the reference, the physics keys of the
+config (``dt, dhat, kappa, stiffness, tol, max_iter`` and any other :class:`SimParams` field)
+are honoured (the reference ignores them, abd/abd.py:107-121).  Scenes can also be passed
+directly as a list of bodies.
+
+All arrays live on one CUDA device as float64 torch tensors.  ``step()`` runs the whole
+Newton time step inside libabd_b200.so; the stage methods (``collision_set``,
+``compute_energy``, ``ccd``, ``gradient_hessian``, ``solve``) expose the pieces for testing.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+from . import _lib
+from .affine_body import AffineMesh, Scene, WarpMesh, affine_body_states_empty
+from .params import SimParams
+from .scenes import flatten_bodies
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class AffineBodySimulator:
+    """One scene of affine bodies on the GPU.
+
+    Attributes (as in the reference): ``scene``, ``n_bodies``, ``states``
+    (:class:`AffineBodyStates`), ``meshes`` (list of :class:`WarpMesh` views), ``highlight``
+    (numpy bool per body), plus ``g`` / ``dq`` properties, ``params`` and ``last_info``.
+    """
+
+    def __init__(self, config_file: str | None = None, bodies=None, params: SimParams | None = None,
+                 device: str = "cuda"):
+        import torch
+        self.torch = torch
+        self.params = params if params is not None else SimParams()
+        if config_file is not None:
+            with open(config_file) as f:
+                config = json.load(f)
+            for k, v in config.items():
+                if hasattr(self.params, k) and not k.startswith("_"):
+                    setattr(self.params, k, v)
+            scene_file = config["scene"]
+            if not os.path.isabs(scene_file):
+                scene_file = os.path.join(os.path.dirname(os.path.abspath(config_file)), scene_file)
+            self.scene = Scene(AffineMesh, scene_config_file=scene_file)
+        else:
+            if bodies is None:
+                raise ValueError("pass config_file or bodies")
+            self.scene = Scene(AffineMesh, objects=list(bodies))
+        bodies = self.scene.kinetic_objects
+        self.n_bodies = n = len(bodies)
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise _lib.AbdError("AffineBodySimulator runs on a CUDA device only")
+        self.flat = flat = flatten_bodies(bodies)
+        self.n_verts = int(flat["voff"][-1])
+        L = _lib.load()
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.states = affine_body_states_empty(n, dev)
+        self.states.mass.copy_(torch.as_tensor(flat["mass"]))
+        self.states.I0.copy_(torch.as_tensor(flat["I0"]))
+        self.x0 = torch.as_tensor(flat["x0"], **f64)
+        self.x = torch.zeros_like(self.x0)
+        self.xk = torch.zeros_like(self.x0)
+        self.x_view = torch.zeros_like(self.x0)
+        self.meshes = []
+        for i, b in enumerate(bodies):
+            v0, v1 = int(flat["voff"][i]), int(flat["voff"][i + 1])
+            self.meshes.append(WarpMesh(
+                id=i, x0=self.x0[v0:v1], x=self.x[v0:v1], xk=self.xk[v0:v1], x_view=self.x_view[v0:v1],
+                triangles=torch.as_tensor(b.F, dtype=torch.int32, device=dev),
+                edges=torch.as_tensor(b.edges, dtype=torch.int32, device=dev)))
+        self.highlight = np.zeros(n, dtype=bool)
+        self.last_info = None
+        # C ABI scene description (host arrays are copied by abd_sim_create)
+        self._host = {k: np.ascontiguousarray(flat[k], dtype=np.int32 if k in ("voff", "toff", "eoff", "tris", "edges", "fixed") else np.float64)
+                      for k in ("voff", "toff", "eoff", "x0", "tris", "edges", "mass", "I0", "fixed")}
+        hp = {k: v.ctypes.data_as(ctypes.c_void_p) for k, v in self._host.items()}
+        desc = _lib.SceneDesc(n, hp["voff"], hp["toff"], hp["eoff"], hp["x0"], hp["tris"], hp["edges"],
+                              hp["mass"], hp["I0"], hp["fixed"])
+        self._cprm = self.params.to_c()
+        h = ctypes.c_void_p()
+        torch.cuda.set_device(dev)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(L.abd_sim_create(ctypes.byref(desc), ctypes.byref(self._cprm), stream, ctypes.byref(h)),
+                   "abd_sim_create")
+        self._h = h
+        self._L = L
+        self.reset()
+
+    # ------------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.torch.cuda.synchronize(self.device)
+            self._L.abd_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params: SimParams):
+        self.params = params
+        self._cprm = params.to_c()
+        _lib.check(self._L.abd_sim_set_params(self._h, ctypes.byref(self._cprm)), "abd_sim_set_params")
+
+    def _cstates(self):
+        s = self.states
+        return _lib.States(*[_ptr(t) for t in (s.A, s.p, s.Ak, s.pk, s.Adot, s.pdot, s.A0, s.p0)])
+
+    def gather(self, field):
+        """Stack a per-body field of the scene objects (simulator/base.py:78-79)."""
+        return np.array([getattr(ko, field) for ko in self.scene.kinetic_objects])
+
+    def reset(self):
+        """Initial states from the scene, dq = 0, meshes at their initial pose
+        (abd/abd.py:97-104)."""
+        t = self.torch
+        s = self.states
+        s.A0.copy_(t.as_tensor(self.gather("A")))
+        s.p0.copy_(t.as_tensor(self.gather("p")))
+        s.pdot.copy_(t.as_tensor(self.gather("pdot")))
+        s.Adot.copy_(t.as_tensor(self.gather("Adot")))
+        s.A.copy_(s.A0)
+        s.p.copy_(s.p0)
+        s.Ak.copy_(s.A0)
+        s.pk.copy_(s.p0)
+        _lib.check(self._L.abd_sim_reset(self._h), "abd_sim_reset")
+        self.update_mesh_vertex("x")
+        self.xk.copy_(self.x)
+        self.x_view.copy_(self.x)
+
+    # ------------------------------------------------------------------ the time step
+    def step(self, frame: int = 1):
+        """One implicit time step (abd/abd.py:212-276); updates ``states`` in place and
+        ``x_view`` to the new positions."""
+        info = _lib.StepInfo()
+        cst = self._cstates()
+        _lib.check(self._L.abd_step(self._h, ctypes.byref(cst), _ptr(self.x_view), ctypes.byref(info)), "abd_step")
+        self.last_info = info.as_dict()
+        return self.last_info
+
+    # ------------------------------------------------------------------ stages
+    def update_mesh_vertex(self, field: str = "x"):
+        """``x = p + sum_k r_k a_k`` into ``x`` / ``xk`` / ``x_view`` from (A, p) / (Ak, pk) /
+        (A0, p0) (abd/abd.py:305-324).  Returns the per-axis minimum."""
+        s = self.states
+        A, p = {"x": (s.A, s.p), "xk": (s.Ak, s.pk), "x_view": (s.A0, s.p0)}[field]
+        out = getattr(self, field)
+        _lib.check(self._L.abd_update_mesh_vertex(self._h, _ptr(A), _ptr(p), _ptr(out)), "abd_update_mesh_vertex")
+        return out.min(dim=0).values
+
+    def transform(self, A, p):
+        out = self.torch.empty_like(self.x0)
+        _lib.check(self._L.abd_update_mesh_vertex(self._h, _ptr(A.contiguous()), _ptr(p.contiguous()), _ptr(out)),
+                   "abd_update_mesh_vertex")
+        return out
+
+    def _lists(self, y0, y1):
+        t = self.torch
+        counts = (ctypes.c_int * 4)()
+        _lib.check(self._L.abd_collision_set(self._h, _ptr(y0), _ptr(y1) if y1 is not None else None, counts),
+                   "abd_collision_set")
+        cap = max(1, max(counts))
+        i32 = dict(dtype=t.int32, device=self.device)
+        ij, pt, ee, vg = (t.zeros((cap, 2), **i32), t.zeros((cap, 5), **i32), t.zeros((cap, 5), **i32),
+                          t.zeros((cap, 2), **i32))
+        _lib.check(self._L.abd_export_lists(self._h, _ptr(ij), _ptr(pt), _ptr(ee), _ptr(vg), cap), "abd_export_lists")
+        return ij[:counts[0]], pt[:counts[1]], ee[:counts[2]], vg[:counts[3]]
+
+    def collision_set(self, y=None):
+        """Culling on positions ``y`` (default ``xk``): ``(ij, ee, pt, vg)`` as the reference
+        returns them (abd/abd.py:187-207); pt/ee rows are (I, J, pair, prim of I, prim of J)."""
+        y = self.xk if y is None else y
+        ij, pt, ee, vg = self._lists(y.contiguous(), None)
+        return ij, ee, pt, vg
+
+    def trajectory_intersection_set(self, y0=None, y1=None):
+        """Culling on the swept boxes x -> xk: ``(ij, pt, ee, vg)`` (abd/abd.py:170-185)."""
+        y0 = self.x if y0 is None else y0
+        y1 = self.xk if y1 is None else y1
+        ij, pt, ee, vg = self._lists(y0.contiguous(), y1.contiguous())
+        return ij, pt, ee, vg
+
+    def gradient_hessian(self, A=None, p=None):
+        """Assemble g and the block system at DOFs (A, p) (default the current ones):
+        returns dict(g [n,12], diag [n,12,12], off [m,12,12], ij [m,2], n_active)."""
+        t = self.torch
+        s = self.states
+        A = s.A if A is None else A.contiguous()
+        p = s.p if p is None else p.contiguous()
+        na = ctypes.c_int(0)
+        cst = self._cstates()
+        _lib.check(self._L.abd_ipc_gh(self._h, ctypes.byref(cst), _ptr(A), _ptr(p), ctypes.byref(na)), "abd_ipc_gh")
+        n = self.n_bodies
+        npairs = ctypes.c_int(0)
+        g = t.zeros((n, 12), dtype=t.float64, device=self.device)
+        diag = t.zeros((n, 12, 12), dtype=t.float64, device=self.device)
+        _lib.check(self._L.abd_export_system(self._h, _ptr(g), _ptr(diag), None, None, 0, ctypes.byref(npairs)),
+                   "abd_export_system")
+        m = npairs.value
+        off = t.zeros((max(m, 1), 12, 12), dtype=t.float64, device=self.device)
+        ij = t.zeros((max(m, 1), 2), dtype=t.int32, device=self.device)
+        _lib.check(self._L.abd_export_system(self._h, None, None, _ptr(off), _ptr(ij), m, ctypes.byref(npairs)),
+                   "abd_export_system")
+        return {"g": g, "diag": diag, "off": off[:m], "ij": ij[:m], "n_active": na.value}
+
+    def solve(self, dq0=None):
+        """Solve the last assembled system H dq = g, warm-started from dq0 (default: the
+        simulator's dq).  Returns (dq, iterations)."""
+        t = self.torch
+        dq = (self.dq if dq0 is None else dq0).contiguous().clone()
+        it = ctypes.c_int(0)
+        _lib.check(self._L.abd_solve(self._h, _ptr(dq), ctypes.byref(it)), "abd_solve")
+        return dq, it.value
+
+    def compute_energy(self, Ak=None, pk=None):
+        """Total energy at trial DOFs (default Ak, pk) (abd/abd.py:133-141)."""
+        s = self.states
+        Ak = s.Ak if Ak is None else Ak.contiguous()
+        pk = s.pk if pk is None else pk.contiguous()
+        E = ctypes.c_double(0)
+        cst = self._cstates()
+        _lib.check(self._L.abd_compute_energy(self._h, ctypes.byref(cst), _ptr(Ak), _ptr(pk), ctypes.byref(E)),
+                   "abd_compute_energy")
+        return E.value
+
+    def ccd(self, A, p, A1, p1):
+        """Step bound between two DOF sets (abd/abd.py:278-303): (alpha, raw toi)."""
+        a = ctypes.c_double(0)
+        raw = ctypes.c_double(0)
+        _lib.check(self._L.abd_ccd(self._h, _ptr(A.contiguous()), _ptr(p.contiguous()), _ptr(A1.contiguous()),
+                                   _ptr(p1.contiguous()), ctypes.byref(a), ctypes.byref(raw)), "abd_ccd")
+        return a.value, raw.value
+
+    # ------------------------------------------------------------------ dq / g
+    @property
+    def dq(self):
+        """The warm-started Newton step (reference ``sim.dq``), [n, 12] float64."""
+        t = self.torch
+        out = t.empty((self.n_bodies, 12), dtype=t.float64, device=self.device)
+        _lib.check(self._L.abd_sim_get_dq(self._h, _ptr(out)), "abd_sim_get_dq")
+        return out
+
+    @dq.setter
+    def dq(self, value):
+        t = self.torch
+        v = value.to(self.device, t.float64).contiguous()
+        _lib.check(self._L.abd_sim_set_dq(self._h, _ptr(v)), "abd_sim_set_dq")
+
+    @property
+    def g(self):
+        """The last assembled gradient (reference ``sim.g``), [n, 12] float64."""
+        t = self.torch
+        out = t.empty((self.n_bodies, 12), dtype=t.float64, device=self.device)
+        _lib.check(self._L.abd_sim_get_g(self._h, _ptr(out)), "abd_sim_get_g")
+        return out
+
+    def launch_count(self) -> int:
+        return int(self._L.abd_launch_count(self._h))

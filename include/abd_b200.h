@@ -1,0 +1,152 @@
+/*
+ * abd_b200.h - C ABI of the B200 (sm_100a) affine-body-dynamics implicit contact step.
+ *
+ * This is the drop-in boundary below the Python mirror of the reference's simulator API
+ * (abd_warp_b200/simulator.py).  The reference (Luke-Skycrawler/abd-warp) is Python on
+ * NVIDIA Warp and has no FFI of its own; each entry point below replaces the reference
+ * function or Warp library call named beside it (paths are within the reference project).
+ *
+ * Conventions
+ *  - All arrays named *_dev are device pointers on the simulator's device; everything else
+ *    is host memory.  No entry point takes framework (torch) types.
+ *  - Body state layout follows AffineBodyStates (abd/affine_body.py:7-21): A is [n][3][3]
+ *    row-major with row k the DOF vector a_k, p is [n][3]; a rest vertex r maps to
+ *    x = p + r0 a0 + r1 a1 + r2 a2 (abd/abd.py:313-316).  Gradients and Newton steps are
+ *    [n][4][3] = per body (p, a0, a1, a2), as the reference's g / dq (abd/abd.py:49-50).
+ *  - Calls are asynchronous on the simulator's stream unless they return a host value
+ *    (counts, energies, step info), in which case they synchronise that stream.
+ *  - Return value: ABD_OK or an ABD_ERR_* code; abd_status_string() describes it.
+ *    A simulator whose call returned ABD_ERR_CUDA should be destroyed.
+ */
+#ifndef ABD_B200_H
+#define ABD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  ABD_OK = 0,
+  ABD_ERR_CUDA = 1,      /* a CUDA runtime call failed */
+  ABD_ERR_INVALID = 2,   /* bad argument (NULL pointer, size out of range, bad mesh index) */
+  ABD_ERR_OVERFLOW = 3,  /* a capacity could not be grown (out of device memory) */
+  ABD_ERR_DEVICE = 4     /* a kernel reported an internal error (traversal stack, NaN) */
+};
+
+/* Physics and solver parameters; the reference's module constants
+ * (abd/const_params.py:24-44) and simulator_args (abd/abd.py:107-121) as one struct. */
+typedef struct abd_params {
+  double dt, dhat, d2hat, kappa, stiffness, gravity, tol, c1, alpha_min, ground, cg_tol, refine_tol;
+  int max_iter;       /* Newton iteration cap (abd.py:114) */
+  int armijo_sign;    /* -1: E1 < E0 - c1 a dq.g (default); +1: the reference's form (abd.py:156) */
+  int ground_enabled; /* vertex-ground plane contact at y = ground (culling.py:54-82, vg_ipc.py) */
+  int psd_ee;         /* contact_psd == 0 only: clamp EE eigenvalues as PT does */
+  int enable_pt, enable_ee, enable_vg; /* const_params.py:41-43 */
+  int solver;         /* 0: block-Jacobi BiCGSTAB (abd.py:244 uses bicgstab), 1: block-Jacobi PCG */
+  int cg_max_iter;
+  int precision;      /* 0: FP64 throughout; 1: FP32 Krylov solve inside FP64 refinement */
+  int contact_psd;    /* 1: PSD projection of the barrier Hessian; 0: the reference's form */
+} abd_params;
+
+/* Scene description (host arrays, copied at creation).  Bodies are concatenated:
+ * vertices of body b are [vert_off[b], vert_off[b+1]) etc.  Replaces the per-body WarpMesh
+ * arrays (abd/affine_body.py:42-51, 84-97). */
+typedef struct abd_scene_desc {
+  int n_bodies;
+  const int* vert_off;  /* [n+1] */
+  const int* tri_off;   /* [n+1] */
+  const int* edge_off;  /* [n+1] */
+  const double* x0;     /* [V][3] rest positions (body frame) */
+  const int* tris;      /* [T][3] global vertex indices */
+  const int* edges;     /* [E][2] global vertex indices */
+  const double* mass;   /* [n] */
+  const double* I0;     /* [n] */
+  const int* fixed;     /* [n] 1 = Dirichlet body (its DOFs never move) */
+} abd_scene_desc;
+
+/* Device pointers to the caller-owned body states (AffineBodyStates, affine_body.py:7-21). */
+typedef struct abd_states {
+  double *A, *p, *Ak, *pk, *Adot, *pdot, *A0, *p0;
+} abd_states;
+
+/* Counters of one time step. */
+typedef struct abd_step_info {
+  int newton_iters, linear_iters, ls_trials, n_pt, n_ee, n_vg, n_ij, n_active;
+  double alpha, toi, energy;
+  int status;          /* device status bits seen during the step (0 = clean) */
+  int refine_iters;    /* precision == 1: FP64 refinement sweeps */
+} abd_step_info;
+
+typedef struct abd_sim abd_sim;
+
+/* Create a simulator for one scene on the current CUDA device; stream may be NULL (legacy
+ * default stream).  Builds the per-body LBVHs (Morton codes, radix sort, Karras build).
+ * Replaces AffineBodySimulator.__init__'s device setup (abd/abd.py:21-95). */
+int abd_sim_create(const abd_scene_desc* scene, const abd_params* prm, void* stream, abd_sim** out);
+int abd_sim_destroy(abd_sim* sim);
+int abd_sim_set_params(abd_sim* sim, const abd_params* prm);
+int abd_sim_set_stream(abd_sim* sim, void* stream);
+/* Zero the warm-started Newton step dq (AffineBodySimulator.reset, abd/abd.py:97-104). */
+int abd_sim_reset(abd_sim* sim);
+/* Copy the simulator's warm-started Newton step dq [n][12] / last gradient g [n][12]
+ * (the reference's sim.dq / sim.g, abd/abd.py:49-50) to or from device buffers. */
+int abd_sim_get_dq(abd_sim* sim, double* dst_dev);
+int abd_sim_set_dq(abd_sim* sim, const double* src_dev);
+int abd_sim_get_g(abd_sim* sim, double* dst_dev);
+int abd_sim_sizes(const abd_sim* sim, int* n_bodies, int* n_verts, int* n_tris, int* n_edges);
+
+/* One implicit time step (AffineBodySimulator.step, abd/abd.py:212-276): Newton on
+ * inertia + orthogonality + IPC barrier energy with CCD-bounded backtracking line search,
+ * then q0 <- q, qdot <- (q - q0)/dt and x_view_dev <- transform(q0).  x_view_dev may be NULL. */
+int abd_step(abd_sim* sim, const abd_states* st, double* x_view_dev, abd_step_info* info);
+
+/* x = p + sum_k r_k a_k for every vertex (update_mesh_vertex, abd/abd.py:305-324). */
+int abd_update_mesh_vertex(abd_sim* sim, const double* A_dev, const double* p_dev, double* x_dev);
+
+/* Broad + narrow culling on positions y0_dev (collision_set, abd/abd.py:187-207) or, when
+ * y1_dev is not NULL, on the swept boxes y0 -> y1 (trajectory_intersection_set,
+ * abd/abd.py:170-185).  counts[4] = {body pairs, PT, EE, VG} (host); the lists stay in the
+ * simulator for abd_export_lists. */
+int abd_collision_set(abd_sim* sim, const double* y0_dev, const double* y1_dev, int counts[4]);
+/* Copy the last culling lists into device buffers of capacity cap rows:
+ * ij [cap][2] (I < J), pt [cap][5] and ee [cap][5] as (I, J, pair, local prim of I, local
+ * prim of J) like the reference's vec5i lists (culling.py:85-99), vg [cap][2] (body,
+ * global vertex).  Any pointer may be NULL. */
+int abd_export_lists(abd_sim* sim, int* ij_dev, int* pt_dev, int* ee_dev, int* vg_dev, int cap);
+
+/* Gradient and Hessian at body DOFs (A_dev, p_dev) with prediction from st->A0/p0/Adot/pdot
+ * (inertia: orthogonal_energy.py:17-22, contacts: ipc.py:54-62 -> pt_ipc / ee_ipc / vg_ipc,
+ * assembly: put.py + bsr_set_from_triplets, abd/abd.py:240-243).  n_active (host, may be
+ * NULL) receives the number of active PT + EE contacts. */
+int abd_ipc_gh(abd_sim* sim, const abd_states* st, const double* A_dev, const double* p_dev, int* n_active);
+/* Copy the last assembled system: g [n][12], diagonal blocks [n][12][12], off-diagonal blocks
+ * [cap][12][12] (block (I,J), I < J, of body pair q in ij order) and ij [cap][2].
+ * n_pairs (host) receives the number of body pairs. */
+int abd_export_system(abd_sim* sim, double* g_dev, double* diag_dev, double* off_dev, int* ij_dev, int cap,
+                      int* n_pairs);
+
+/* Solve H dq = g of the last assembled system, dq_dev the warm start, overwritten
+ * (warp.optim.linear.bicgstab call, abd/abd.py:244).  iters (host) may be NULL. */
+int abd_solve(abd_sim* sim, double* dq_dev, int* iters);
+
+/* Total energy at trial DOFs (Ak_dev, pk_dev) with prediction from st (compute_energy,
+ * abd/abd.py:133-141: IPC barrier ipcsk/energy.py:9-48 + inertia orthogonal_energy.py:24-32). */
+int abd_compute_energy(abd_sim* sim, const abd_states* st, const double* Ak_dev, const double* pk_dev, double* E);
+
+/* CCD step bound between DOFs (A, p) and (A1, p1) (ccd, abd/abd.py:278-303; toi_vg ccd.py:9-18,
+ * cubic CCD ccd.py:56-186 / cubic_roots.py:95-193 in place of abdtk).  alpha (host) gets
+ * clamp(toi, 0, 1) * (0.9 if < 1), raw_toi (host, may be NULL) the unclamped minimum. */
+int abd_ccd(abd_sim* sim, const double* A_dev, const double* p_dev, const double* A1_dev, const double* p1_dev,
+            double* alpha, double* raw_toi);
+
+/* Device status bits accumulated since the last call (and cleared). */
+int abd_take_status(abd_sim* sim, int* status);
+const char* abd_status_string(int code);
+
+/* Number of kernel launches the simulator has issued since creation. */
+long long abd_launch_count(const abd_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABD_B200_H */

@@ -340,7 +340,8 @@ inline double signed_distance(V3 e0p, V3 e1p, V3 e2p) {
 inline double barrier(double d, const Params& P) {
   if (d < P.d2hat) {
     const double s = d / P.d2hat;
-    return P.kappa * -std::pow(s - 1.0, 2.0) * std::log(s);
+    const double t = s - 1.0;  // pow(s - 1, 2.0) as its correctly rounded value
+    return P.kappa * -(t * t) * std::log(s);
   }
   return 0.0;
 }
@@ -866,7 +867,7 @@ double find_closed(const double coef[4], const double deriv[4], double x0, doubl
   double yr = evaluate(coef, xr);
   double xb0 = x0, xb1 = x1;
   if (x1 - x0 <= X_ERROR * 2.0) return xr;
-  for (;;) {
+  for (int guard = 0; guard < 4096; ++guard) {
     if (diff_sign(y0, yr)) xb1 = xr;
     else xb0 = xr;
     const double dy = evaluate(deriv, xr);

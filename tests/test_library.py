@@ -1,0 +1,48 @@
+"""The C ABI library loads and exports every entry point include/abd_b200.h declares
+(no compute calls: these run without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "abd_b200.h")
+LIB = os.path.join(ROOT, "abd_warp_b200", "libabd_b200.so")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(abd_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "abd_step" in names and "abd_sim_create" in names
+    assert len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(LIB):
+        pytest.skip("libabd_b200.so not built")
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_matches_header():
+    from abd_warp_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libabd_b200.so not built")
+    assert set(_lib.exported_symbols()) <= set(declared_functions())
+
+
+def test_status_strings():
+    from abd_warp_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libabd_b200.so not built")
+    L = _lib.load()
+    assert L.abd_status_string(0) == b"ok"
+    assert L.abd_status_string(3) == b"capacity could not be grown"

@@ -1,0 +1,33 @@
+import numpy as np
+import pytest
+
+from abd_warp_b200 import meshes, scenes
+
+
+@pytest.mark.parametrize("level,counts", [(2, (162, 320, 480)), (3, (642, 1280, 1920))])
+def test_icosphere_counts(level, counts):
+    V, F = meshes.icosphere_mesh(level, 0.3)
+    E = meshes.unique_edges(F)
+    assert (V.shape[0], F.shape[0], E.shape[0]) == counts
+
+
+def test_cube_mass_properties():
+    V, F = meshes.cube_mesh(0.5)
+    m, com, I0 = meshes.mass_properties(V, F, 1000.0)
+    assert m == pytest.approx(1000 * 0.125)
+    assert np.allclose(com, 0)
+    assert I0 == pytest.approx(1000 * 0.5 ** 5 / 12)
+    assert meshes.unique_edges(F).shape[0] == 18
+
+
+@pytest.mark.parametrize("idx,sizes", [(0, (2, 16, 24, 36)), (1, (65, 10376, 20492, 30738)),
+                                       (4, (17, 2600, 5132, 7698))])
+def test_config_sizes(idx, sizes):
+    bodies, prm, steps = scenes.make_config(idx)
+    f = scenes.flatten_bodies(bodies)
+    assert (f["n"], f["voff"][-1], f["toff"][-1], f["eoff"][-1]) == sizes
+
+
+def test_config0_initial_separation():
+    bodies, prm, _ = scenes.make_config(0)
+    assert bodies[1].vertices_world()[:, 1].min() > 0.5 + prm.dhat
