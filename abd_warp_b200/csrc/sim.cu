@@ -490,7 +490,8 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
       CK(abd::update_dofs(s, st.A, st.p, s.dq, alpha, st.Ak, st.pk));
       if ((r = energy_at(h, st, st.Ak, st.pk, &E1))) return r;
       ++inf.ls_trials;
-      const bool wolfe = E1 < E0 + P.armijo_sign * P.c1 * alpha * qTg;
+      const bool wolfe = E1 < E0 + P.armijo_sign * P.c1 * alpha * qTg ||
+                         std::fabs(E1 - E0) <= P.ls_noise_floor * std::fabs(E0);
       if (wolfe || alpha < P.alpha_min) break;
       alpha *= 0.5;
     }

@@ -27,6 +27,8 @@ class SimParams:
     tol: float = 1e-6                # Newton stop: g.g < tol (abd.py:265-268)
     c1: float = 1e-4                 # Armijo constant (const_params.py:28)
     alpha_min: float = 1e-3          # line-search floor (const_params.py:29)
+    ls_noise_floor: float = 1e-12    # also accept a trial when |E1 - E0| <= floor |E0|: below the
+                                     # energies' rounding error the Armijo test is noise
     max_iter: int = 100              # Newton iteration cap (abd.py:114)
     armijo_sign: int = -1            # -1: E1 < E0 - c1 a dq.g ; +1: reference form abd.py:156
     ground_enabled: bool = False     # vertex-ground plane contact (culling.py:54-82)
@@ -62,6 +64,7 @@ class SimParams:
         c.ground = self.ground
         c.cg_tol = self.cg_tol
         c.refine_tol = self.refine_tol
+        c.ls_noise_floor = self.ls_noise_floor
         c.max_iter = self.max_iter
         c.armijo_sign = self.armijo_sign
         c.ground_enabled = int(self.ground_enabled)
@@ -86,6 +89,7 @@ class CParams(ctypes.Structure):
         ("kappa", ctypes.c_double), ("stiffness", ctypes.c_double), ("gravity", ctypes.c_double),
         ("tol", ctypes.c_double), ("c1", ctypes.c_double), ("alpha_min", ctypes.c_double),
         ("ground", ctypes.c_double), ("cg_tol", ctypes.c_double), ("refine_tol", ctypes.c_double),
+        ("ls_noise_floor", ctypes.c_double),
         ("max_iter", ctypes.c_int), ("armijo_sign", ctypes.c_int), ("ground_enabled", ctypes.c_int),
         ("psd_ee", ctypes.c_int), ("enable_pt", ctypes.c_int), ("enable_ee", ctypes.c_int),
         ("enable_vg", ctypes.c_int), ("solver", ctypes.c_int), ("cg_max_iter", ctypes.c_int),

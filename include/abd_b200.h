@@ -37,6 +37,7 @@ enum {
  * (abd/const_params.py:24-44) and simulator_args (abd/abd.py:107-121) as one struct. */
 typedef struct abd_params {
   double dt, dhat, d2hat, kappa, stiffness, gravity, tol, c1, alpha_min, ground, cg_tol, refine_tol;
+  double ls_noise_floor; /* line search also accepts |E1 - E0| <= ls_noise_floor |E0| (0: off) */
   int max_iter;       /* Newton iteration cap (abd.py:114) */
   int armijo_sign;    /* -1: E1 < E0 - c1 a dq.g (default); +1: the reference's form (abd.py:156) */
   int ground_enabled; /* vertex-ground plane contact at y = ground (culling.py:54-82, vg_ipc.py) */

@@ -33,6 +33,7 @@ def lib():
         L.orc_destroy.argtypes = [v]
         L.orc_set_params.argtypes = [v, v]
         L.orc_set_threads.argtypes = [i]
+        L.orc_set_reverse_sums.argtypes = [i]
         L.orc_max_threads.restype = i
         L.orc_set_state.argtypes = [v] * 6
         L.orc_get_state.argtypes = [v] * 7
@@ -204,6 +205,11 @@ def cubic_roots(coef, x0, x1):
     roots = np.zeros(3)
     n = lib().orc_cubic_roots(_p(coef), x0, x1, _p(roots))
     return n, roots
+
+
+def set_reverse_sums(flag: bool):
+    """Test hook: sum contact energies in reverse order (perturbs rounding only)."""
+    lib().orc_set_reverse_sums(int(flag))
 
 
 def set_threads(t: int):

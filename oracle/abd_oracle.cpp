@@ -38,8 +38,12 @@
 
 namespace {
 
+// test hook: 1 sums contact energies in reverse candidate order (changes rounding only)
+int g_reverse_sums = 0;
+
 struct Params {
   double dt, dhat, d2hat, kappa, stiffness, gravity, tol, c1, alpha_min, ground, cg_tol, refine_tol;
+  double ls_noise_floor;
   int max_iter, armijo_sign, ground_enabled, psd_ee, enable_pt, enable_ee, enable_vg, solver,
       cg_max_iter, precision, contact_psd;
 };
@@ -1076,7 +1080,10 @@ double energy_at(Oracle& o, const double* y, const double* Akp, const double* pk
       fetch(o, y, C[i], type, xs, rs);
       e[i] = contact_energy(type, xs, o.prm);
     }
-    for (int i = 0; i < nc; ++i) ec += e[i];
+    if (g_reverse_sums)
+      for (int i = nc - 1; i >= 0; --i) ec += e[i];
+    else
+      for (int i = 0; i < nc; ++i) ec += e[i];
   }
   for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
     const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
@@ -1163,7 +1170,8 @@ void step(Oracle& o) {
     for (;;) {
       E1 = compute_energy(o, alpha);
       ++ls;
-      const bool wolfe = E1 < E0 + o.prm.armijo_sign * o.prm.c1 * alpha * qTg;
+      const bool wolfe = E1 < E0 + o.prm.armijo_sign * o.prm.c1 * alpha * qTg ||
+                         std::fabs(E1 - E0) <= o.prm.ls_noise_floor * std::fabs(E0);
       if (wolfe || alpha < o.prm.alpha_min) break;
       alpha *= 0.5;
     }
@@ -1233,6 +1241,7 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
 void orc_destroy(void* h) { delete (Oracle*)h; }
 void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
 void orc_set_threads(int t) { omp_set_num_threads(t); }
+void orc_set_reverse_sums(int r) { g_reverse_sums = r; }
 int orc_max_threads() { return omp_get_max_threads(); }
 
 void orc_set_state(void* h, const double* A0, const double* p0, const double* Adot, const double* pdot,
