@@ -149,6 +149,14 @@ struct Sim {
   // Krylov work vectors [n][12]
   double *r = nullptr, *rh = nullptr, *pv = nullptr, *v = nullptr, *y = nullptr, *s = nullptr, *z = nullptr,
          *t = nullptr, *ddq = nullptr;
+  // preconditioner clusters (contact-coupled bodies, <= cluster_max each)
+  int ncl = 0, max_cl = 1;
+  int *cl_ptr = nullptr, *cl_body = nullptr;     // [ncl+1], [n]
+  long long* cl_off = nullptr;                   // [ncl+1] offsets into cl_inv (doubles)
+  double* cl_inv = nullptr;                      // dense inverses of the cluster systems
+  size_t cap_cl_inv = 0;
+  float* pair_w = nullptr;                       // [cap_pairs] coupling weights
+  double* zb = nullptr;                          // [n][12] scratch (M^-1 b)
   double* partials = nullptr;      // reduction partials [kRedSlots][kRedBlocks]
   double* scal = nullptr;          // solver scalars
   int* dstat = nullptr;            // device: [0] status, [1..] counters
@@ -158,7 +166,7 @@ struct Sim {
 };
 
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
-constexpr int kRedSlots = 8;
+constexpr int kRedSlots = 12;
 
 // dstat layout
 enum : int {
@@ -205,7 +213,7 @@ cudaError_t dot_partials(Sim& s, const double* a, const double* b, int slot);
 cudaError_t finish_dot(Sim& s, int slot, double* out_dev);
 
 // solver.cu
-cudaError_t block_inverse(Sim& s);
+int build_preconditioner(Sim& s);                 // returns ABD status
 int krylov_solve(Sim& s, double* x, int* iters);  // returns ABD status
 
 }  // namespace abd

@@ -56,14 +56,14 @@ int grow_pairs(Sim& s, int need) {
   const int cap = std::max(need + need / 2, 2 * s.cap_pairs);
   const int cap_adj = 2 * cap;
   for (void* q : {(void*)s.ij, (void*)s.adj_col, (void*)s.adj_pair, (void*)s.pair_cand, (void*)s.offdiag,
-                  (void*)s.pdiag, (void*)s.pgrad, (void*)s.pair_active, (void*)s.pair_val})
+                  (void*)s.pdiag, (void*)s.pgrad, (void*)s.pair_active, (void*)s.pair_val, (void*)s.pair_w})
     if (q) cudaFree(q);
   s.cap_pairs = cap;
   s.cap_adj = cap_adj;
   if (dalloc(&s.ij, cap) || dalloc(&s.adj_col, cap_adj) || dalloc(&s.adj_pair, cap_adj) ||
       dalloc(&s.pair_cand, 4 * (size_t)cap) || dalloc(&s.offdiag, 288 * (size_t)cap) ||
       dalloc(&s.pdiag, 288 * (size_t)cap) || dalloc(&s.pgrad, 24 * (size_t)cap) || dalloc(&s.pair_active, cap) ||
-      dalloc(&s.pair_val, cap))
+      dalloc(&s.pair_val, cap) || dalloc(&s.pair_w, cap))
     return ABD_ERR_OVERFLOW;
   return ABD_OK;
 }
@@ -265,7 +265,11 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.row_ptr, n + 1));
   ok(dalloc(&s.upper_ptr, n + 1));
   ok(dalloc(&s.body_val, n));
-  for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq}) ok(dalloc(v, 12 * (size_t)n));
+  for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq, &s.zb})
+    ok(dalloc(v, 12 * (size_t)n));
+  ok(dalloc(&s.cl_ptr, n + 1));
+  ok(dalloc(&s.cl_body, n));
+  ok(dalloc(&s.cl_off, n + 1));
   ok(dalloc(&s.diag, 144 * (size_t)n));
   ok(dalloc(&s.Minv, 144 * (size_t)n));
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
@@ -308,7 +312,8 @@ int abd_sim_destroy(abd_sim* h) {
                   s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
                   s.pair_active, s.pair_val, s.body_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
-                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin};
+                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin,
+                  s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_w};
   for (void* q : bufs)
     if (q) cudaFree(q);
   if (s.hstat) cudaFreeHost(s.hstat);
@@ -423,7 +428,8 @@ int abd_export_system(abd_sim* h, double* g, double* diag, double* off, int* ij,
 
 int abd_solve(abd_sim* h, double* dq, int* iters) {
   if (!h || !dq) return ABD_ERR_INVALID;
-  CK(abd::block_inverse(h->s));
+  int r = abd::build_preconditioner(h->s);
+  if (r) return r;
   return abd::krylov_solve(h->s, dq, iters);
 }
 
@@ -468,7 +474,7 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     }
     inf.n_active = nact;
     int lin = 0;
-    CK(abd::block_inverse(s));
+    if ((r = abd::build_preconditioner(s))) return r;
     if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
     inf.linear_iters += lin;
     // CCD bound (abd.py:278-303)
@@ -477,10 +483,10 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     double alpha;
     if ((r = ccd_at(h, s.x, s.xk, &alpha, &inf.toi))) return r;
     // dq.g and g.g (abd.py:148, 265)
-    CK(abd::dot_partials(s, s.dq, s.g, 7));
-    CK(abd::finish_dot(s, 7, s.scal + 10));
-    CK(abd::dot_partials(s, s.g, s.g, 7));
-    CK(abd::finish_dot(s, 7, s.scal + 11));
+    CK(abd::dot_partials(s, s.dq, s.g, 10));
+    CK(abd::finish_dot(s, 10, s.scal + 10));
+    CK(abd::dot_partials(s, s.g, s.g, 11));
+    CK(abd::finish_dot(s, 11, s.scal + 11));
     CK(cudaMemcpyAsync(s.hval + 2, s.scal + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     CK(cudaStreamSynchronize(s.stream));
     const double qTg = s.hval[2], gTg = s.hval[3];

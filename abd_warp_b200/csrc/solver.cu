@@ -1,14 +1,28 @@
 // Newton linear solve H dq = g on the block-sparse (12x12 per body pair) system.
 //
 // Replaces warp.optim.linear.bicgstab(hess, g, dq, 1e-4) and warp.sparse's BSR product
-// (abd/abd.py:243-244).  Block-Jacobi preconditioned BiCGSTAB (the reference's solver
-// choice) or PCG, FP64.  The SpMV is warp per block row: 24 lanes cover the 12 rows x 2
-// half-rows of each 12x12 block, the row's blocks are the body's diagonal block and the
-// off-diagonal blocks of its active body pairs in adjacency order.  Dot products are fused
-// into the vector kernels as per-CTA partials on a fixed grid of kRedBlocks CTAs and summed
-// in a fixed order, so the solve is bitwise reproducible.  Convergence is decided on the
-// device (iteration-tagged flags); the host checks every kCheckEvery iterations.
+// (abd/abd.py:243-244).
+//
+// Preconditioner: contact-cluster block Jacobi.  Barrier stiffness between touching bodies is
+// 1e8-1e10 times their mass, so a per-body block Jacobi leaves the Krylov method facing that
+// condition number.  Bodies coupled by active contacts are grouped (union-find on the host,
+// strongest coupling first, at most cluster_max bodies); each cluster's dense system is
+// assembled and inverted in shared memory by one CTA (Gauss-Jordan, SPD, no pivoting), and
+// applied as a dense product.  Clusters of one body reduce to the per-body 12x12 block.
+//
+// Krylov: PCG (default; the projected Hessian is SPD) or right-preconditioned BiCGSTAB (the
+// reference's choice).  Convergence is measured in the preconditioned norm,
+// r^T M^-1 r <= tol^2 b^T M^-1 b, which stays resolvable in FP64 although the plain residual
+// of such stiff systems has a rounding floor near eps * cond.  The SpMV is warp per block row
+// (24 lanes = 12 rows x 2 half-rows).  Dot products are per-CTA partials on a fixed grid of
+// kRedBlocks CTAs summed in a fixed order, so the solve is bitwise reproducible.  The host
+// checks the device-side convergence flags every kCheckEvery iterations.
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <numeric>
+#include <utility>
+#include <vector>
 
 #include "abd_common.cuh"
 
@@ -16,11 +30,13 @@ namespace abd {
 
 namespace {
 
-constexpr int WPB = 8;          // warps (body rows) per CTA
+constexpr int WPB = 8;          // warps (body rows) per CTA of the row kernels
 constexpr int kCheckEvery = 8;  // iterations launched between host checks
+constexpr int AT = 128;         // threads of the cluster kernels
+constexpr int kMaxCluster = 12; // bodies per cluster: 144 x 144 doubles fit in shared memory
 
 // slots of Sim::partials
-enum { SL_R2 = 0, SL_RHR = 1, SL_RHV = 2, SL_S2 = 3, SL_TS = 4, SL_TT = 5, SL_B2 = 6, SL_X = 7 };
+enum { SL_RZ0 = 0, SL_RZ1 = 1, SL_PAP = 2, SL_BZ = 3, SL_RHR = 4, SL_RHV = 5, SL_SZ = 6, SL_TS = 7, SL_TT = 8 };
 // Sim::scal layout
 enum { SC_RHO0 = 0, SC_RHO1 = 1, SC_ALPHA = 2, SC_OMEGA = 3, SC_THR2 = 4 };
 // dstat slots used by the solver
@@ -28,9 +44,13 @@ enum { DS_R_DONE = 10, DS_S_DONE = 11 };
 
 struct SolverArgs {
   int n;
-  const double *diag, *offdiag, *Minv;
+  const double *diag, *offdiag;
   const int *row_ptr, *adj_col, *adj_pair, *pair_active, *fixed;
   const int2* ij;
+  int ncl;
+  const int *cl_ptr, *cl_body;
+  const long long* cl_off;
+  double* cl_inv;
   double* part;
   double* scal;
   int* dstat;
@@ -59,10 +79,10 @@ __device__ inline void cta_scalars(const double* part, const int* slots, int ns,
   __syncthreads();
 }
 
-// per-CTA partial of two dot products: each warp passes its lane values (lanes 0..11)
+// per-CTA partial of two dot products (every thread passes its own contribution)
 __device__ inline void cta_partials(double d0, double d1, double* part, int slot0, int slot1) {
-  __shared__ double w[WPB][2];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double w[32][2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     d0 += __shfl_xor_sync(0xffffffffu, d0, o);
@@ -75,13 +95,14 @@ __device__ inline void cta_partials(double d0, double d1, double* part, int slot
   __syncthreads();
   if (threadIdx.x == 0) {
     double a = 0.0, b = 0.0;
-    for (int k = 0; k < WPB; ++k) {
+    for (int k = 0; k < nw; ++k) {
       a += w[k][0];
       b += w[k][1];
     }
     if (slot0 >= 0) part[slot0 * kRedBlocks + blockIdx.x] = a;
     if (slot1 >= 0) part[slot1 * kRedBlocks + blockIdx.x] = b;
   }
+  __syncthreads();
 }
 
 // y_b (lanes 0..11 hold row lane) = (A x)_b for block row b
@@ -112,29 +133,98 @@ __device__ inline double row_product(const SolverArgs& a, int b, const double* x
   return acc;  // valid on lanes 0..11
 }
 
-// lanes 0..11: (Minv_b v_b)[lane]
-__device__ inline double block_apply(const double* M, int b, const double* v) {
-  const int lane = threadIdx.x & 31;
-  double acc = 0.0;
-  if (lane < 24) {
-    const int r = lane % 12, h = lane / 12;
-    const double* B = M + (size_t)b * 144 + r * 12 + 6 * h;
-    const double* vb = v + (size_t)b * 12 + 6 * h;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) acc += B[c] * vb[c];
-  }
-  acc += __shfl_down_sync(0xffffffffu, acc, 12);
-  return acc;
-}
-
-#define FOR_BODIES(b)                                                                      \
-  for (int b = blockIdx.x * WPB + (int)(threadIdx.x >> 5); b < a.n; b += kRedBlocks * WPB)
+#define FOR_BODIES(b) for (int b = blockIdx.x * WPB + (int)(threadIdx.x >> 5); b < a.n; b += kRedBlocks * WPB)
 
 __device__ inline bool solver_done(const int* dstat) {
   return ((volatile const int*)dstat)[DS_R_DONE] != 0 || ((volatile const int*)dstat)[DS_S_DONE] != 0;
 }
 
-// ---- shared setup: r = b - A x, rh = r, p = v = 0; partials r.r, rh.r ----
+// ---- preconditioner setup: assemble and invert each cluster's dense block system ----
+__global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, int c1, const int* body_cl) {
+  extern __shared__ double K[];
+  for (int c = c0 + blockIdx.x; c < c1; c += gridDim.x) {
+    const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
+    for (int e = threadIdx.x; e < D * D; e += AT) K[e] = 0.0;
+    __syncthreads();
+    // block row of every member: its diagonal block and the blocks of active pairs whose
+    // other body is in the same cluster
+    for (int e = threadIdx.x; e < s * 144; e += AT) {
+      const int li = e / 144, rc = e % 144;
+      const int b = a.cl_body[base + li];
+      K[(size_t)(12 * li + rc / 12) * D + 12 * li + rc % 12] = a.diag[(size_t)b * 144 + rc];
+    }
+    if (s > 1) {
+      for (int li = 0; li < s; ++li) {
+        const int b = a.cl_body[base + li];
+        for (int k = a.row_ptr[b]; k < a.row_ptr[b + 1]; ++k) {
+          const int pr = a.adj_pair[k];
+          if (a.pair_active[pr] <= 0) continue;
+          const int J = a.adj_col[k];
+          if (body_cl[J] != c || a.fixed[J] || a.fixed[b]) continue;
+          int lj = 0;
+          while (a.cl_body[base + lj] != J) ++lj;  // members are few (<= kMaxCluster)
+          const int side = a.ij[pr].x == b ? 0 : 1;
+          const double* O = a.offdiag + (size_t)pr * 288 + side * 144;
+          for (int rc = threadIdx.x; rc < 144; rc += AT)
+            K[(size_t)(12 * li + rc / 12) * D + 12 * lj + rc % 12] = O[rc];
+        }
+      }
+    }
+    __syncthreads();
+    // in-place Gauss-Jordan inverse (SPD: no pivoting), same operation order as the oracle
+    __shared__ double f[12 * kMaxCluster];
+    for (int k = 0; k < D; ++k) {
+      const double p = K[(size_t)k * D + k];
+      __syncthreads();
+      const double ip = 1.0 / p;
+      if (threadIdx.x == 0) K[(size_t)k * D + k] = 1.0;
+      __syncthreads();
+      for (int j = threadIdx.x; j < D; j += AT) K[(size_t)k * D + j] *= ip;
+      for (int i = threadIdx.x; i < D; i += AT) f[i] = (i == k) ? 0.0 : K[(size_t)i * D + k];
+      __syncthreads();
+      for (int i = threadIdx.x; i < D; i += AT)
+        if (i != k) K[(size_t)i * D + k] = 0.0;
+      __syncthreads();
+      for (int e = threadIdx.x; e < D * D; e += AT) {
+        const int i = e / D, j = e % D;
+        const double fi = f[i];
+        if (i != k && fi != 0.0) K[e] -= fi * K[(size_t)k * D + j];
+      }
+      __syncthreads();
+    }
+    double* out = a.cl_inv + a.cl_off[c];
+    for (int e = threadIdx.x; e < D * D; e += AT) out[e] = K[e];
+    __syncthreads();
+  }
+}
+
+// out = M^-1 in (cluster by cluster); partial in.out into slot (if >= 0); also copies out
+// into copy (if not null)
+__global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out,
+                                              double* copy, int slot) {
+  if (it_guard && solver_done(a.dstat)) return;
+  __shared__ double vs[12 * kMaxCluster];
+  double d0 = 0.0;
+  for (int c = blockIdx.x; c < a.ncl; c += gridDim.x) {
+    const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
+    for (int i = threadIdx.x; i < D; i += AT) vs[i] = in[(size_t)a.cl_body[base + i / 12] * 12 + i % 12];
+    __syncthreads();
+    const double* Kc = a.cl_inv + a.cl_off[c];
+    for (int i = threadIdx.x; i < D; i += AT) {
+      double acc = 0.0;
+      const double* row = Kc + (size_t)i * D;
+      for (int j = 0; j < D; ++j) acc += row[j] * vs[j];
+      const size_t gi = (size_t)a.cl_body[base + i / 12] * 12 + i % 12;
+      out[gi] = acc;
+      if (copy) copy[gi] = acc;
+      d0 += vs[i] * acc;
+    }
+    __syncthreads();
+  }
+  if (slot >= 0) cta_partials(d0, 0.0, a.part, slot, -1);
+}
+
+// ---- r = b - A x (+ rh = r, p = v = 0 for BiCGSTAB) ----
 __global__ void __launch_bounds__(256) k_residual(SolverArgs a, const double* bvec, const double* x, double* r,
                                                   double* rh, double* pv, double* v) {
   const int lane = threadIdx.x & 31;
@@ -151,31 +241,90 @@ __global__ void __launch_bounds__(256) k_residual(SolverArgs a, const double* bv
       d0 += ri * ri;
     }
   }
-  cta_partials(d0, d0, a.part, SL_R2, SL_RHR);
+  cta_partials(d0, 0.0, a.part, SL_RHR, -1);
 }
 
-__global__ void __launch_bounds__(256) k_norm2(SolverArgs a, const double* u, int slot) {
+// ---- PCG ----
+// K1: converged if r.z <= thr^2; else Ap = A p with partial p.Ap
+__global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, int it, const double* pv, double* Ap) {
+  if (solver_done(a.dstat)) return;
+  const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
+  const int slots[1] = {rz};
+  double sc[1];
+  cta_scalars(a.part, slots, 1, sc);
+  if (!(sc[0] > a.scal[SC_THR2])) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.dstat[DS_R_DONE] = it;
+      a.dstat[DS_SOLVER_ITERS] = it - 1;
+    }
+    return;
+  }
   const int lane = threadIdx.x & 31;
   double d0 = 0.0;
   FOR_BODIES(b) {
+    const double yi = row_product(a, b, pv);
     if (lane < 12) {
-      const double ui = u[(size_t)b * 12 + lane];
-      d0 += ui * ui;
+      const size_t i = (size_t)b * 12 + lane;
+      Ap[i] = yi;
+      d0 += pv[i] * yi;
     }
   }
-  cta_partials(d0, 0.0, a.part, slot, -1);
+  cta_partials(d0, 0.0, a.part, SL_PAP, -1);
 }
 
-// ---- BiCGSTAB ----
-// K1: rho = rh.r; p = r + beta (p - omega v); y = M p
-__global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, int it, const double* r, double* pv, const double* v,
-                                                double* y) {
+// K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature)
+__global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, int it, const double* pv, const double* Ap, double* x,
+                                               double* r) {
   if (solver_done(a.dstat)) return;
-  const int slots[2] = {SL_R2, SL_RHR};
+  const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
+  const int slots[2] = {rz, SL_PAP};
   double sc[2];
   cta_scalars(a.part, slots, 2, sc);
-  const double thr2 = a.scal[SC_THR2];
-  if (sc[0] <= thr2) {
+  if (!(sc[1] > 0.0)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.dstat[DS_R_DONE] = it;
+      a.dstat[DS_SOLVER_ITERS] = it - 1;
+    }
+    return;
+  }
+  const double alpha = sc[0] / sc[1];
+  const int lane = threadIdx.x & 31;
+  FOR_BODIES(b) {
+    if (lane < 12) {
+      const size_t i = (size_t)b * 12 + lane;
+      x[i] += alpha * pv[i];
+      r[i] -= alpha * Ap[i];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.dstat[DS_SOLVER_ITERS] = it;
+}
+
+// K3 (after z = M r with partial r.z into the new slot): beta = rz_new / rz_old; p = z + beta p
+__global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, int it, const double* z, double* pv) {
+  if (solver_done(a.dstat)) return;
+  const int rz_old = (it & 1) ? SL_RZ0 : SL_RZ1, rz_new = (it & 1) ? SL_RZ1 : SL_RZ0;
+  const int slots[2] = {rz_new, rz_old};
+  double sc[2];
+  cta_scalars(a.part, slots, 2, sc);
+  if (!(sc[0] > a.scal[SC_THR2])) return;  // converged: K1 of the next iteration stops
+  const double beta = sc[0] / sc[1];
+  const int lane = threadIdx.x & 31;
+  FOR_BODIES(b) {
+    if (lane < 12) {
+      const size_t i = (size_t)b * 12 + lane;
+      pv[i] = z[i] + beta * pv[i];
+    }
+  }
+}
+
+// ---- BiCGSTAB (right preconditioned) ----
+// K1: converged if r.M^-1 r small; rho = rh.r; p = r + beta (p - omega v)
+__global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, int it, const double* r, double* pv, const double* v) {
+  if (solver_done(a.dstat)) return;
+  const int slots[2] = {SL_RZ0, SL_RHR};
+  double sc[2];
+  cta_scalars(a.part, slots, 2, sc);
+  if (!(sc[0] > a.scal[SC_THR2]) || sc[1] == 0.0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.dstat[DS_R_DONE] = it;
       a.dstat[DS_SOLVER_ITERS] = it - 1;
@@ -192,14 +341,11 @@ __global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, int it, const doub
       const size_t i = (size_t)b * 12 + lane;
       pv[i] = it == 1 ? r[i] : r[i] + beta * (pv[i] - omega * v[i]);
     }
-    __syncwarp();
-    const double yi = block_apply(a.Minv, b, pv);
-    if (lane < 12) y[(size_t)b * 12 + lane] = yi;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.scal[it & 1] = rho;
 }
 
-// K2 / K5: out = A in; partials in2.out (slot0), out.out (slot1)
+// out = A in; partials w0.out (slot0), w1.out (slot1)
 __global__ void __launch_bounds__(256) k_spmv(SolverArgs a, const double* in, double* out, const double* w0, int slot0,
                                               const double* w1, int slot1) {
   if (solver_done(a.dstat)) return;
@@ -217,7 +363,7 @@ __global__ void __launch_bounds__(256) k_spmv(SolverArgs a, const double* in, do
   cta_partials(d0, d1, a.part, slot0, slot1);
 }
 
-// K3: alpha = rho / rh.v; s = r - alpha v; partial s.s
+// K3: alpha = rho / rh.v; s = r - alpha v
 __global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, int it, const double* r, const double* v, double* s) {
   if (solver_done(a.dstat)) return;
   const int slots[1] = {SL_RHV};
@@ -225,49 +371,38 @@ __global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, int it, const doub
   cta_scalars(a.part, slots, 1, sc);
   const double alpha = a.scal[it & 1] / sc[0];
   const int lane = threadIdx.x & 31;
-  double d0 = 0.0;
   FOR_BODIES(b) {
     if (lane < 12) {
       const size_t i = (size_t)b * 12 + lane;
-      const double si = r[i] - alpha * v[i];
-      s[i] = si;
-      d0 += si * si;
+      s[i] = r[i] - alpha * v[i];
     }
   }
-  cta_partials(d0, 0.0, a.part, SL_S2, -1);
   if (blockIdx.x == 0 && threadIdx.x == 0) a.scal[SC_ALPHA] = alpha;
 }
 
-// K4: if |s| small: x += alpha y and stop; else z = M s
-__global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, int it, const double* y, const double* s, double* z,
-                                                double* x) {
+// K4 (after z = M s with partial s.z): if small, x += alpha y and stop
+__global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, int it, const double* y, double* x) {
   const volatile int* ds = a.dstat;
   if (ds[DS_R_DONE] != 0 || (ds[DS_S_DONE] != 0 && ds[DS_S_DONE] != it)) return;
-  const int slots[1] = {SL_S2};
+  const int slots[1] = {SL_SZ};
   double sc[1];
   cta_scalars(a.part, slots, 1, sc);
+  if (sc[0] > a.scal[SC_THR2]) return;
   const double alpha = a.scal[SC_ALPHA];
   const int lane = threadIdx.x & 31;
-  if (sc[0] <= a.scal[SC_THR2]) {
-    FOR_BODIES(b) {
-      if (lane < 12) {
-        const size_t i = (size_t)b * 12 + lane;
-        x[i] += alpha * y[i];
-      }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      a.dstat[DS_S_DONE] = it;
-      a.dstat[DS_SOLVER_ITERS] = it;
-    }
-    return;
-  }
   FOR_BODIES(b) {
-    const double zi = block_apply(a.Minv, b, s);
-    if (lane < 12) z[(size_t)b * 12 + lane] = zi;
+    if (lane < 12) {
+      const size_t i = (size_t)b * 12 + lane;
+      x[i] += alpha * y[i];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.dstat[DS_S_DONE] = it;
+    a.dstat[DS_SOLVER_ITERS] = it;
   }
 }
 
-// K6: omega = t.s / t.t; x += alpha y + omega z; r = s - omega t; partials r.r, rh.r
+// K6: omega = t.s / t.t; x += alpha y + omega z; r = s - omega t; partial rh.r
 __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, int it, const double* y, const double* z,
                                                 const double* s, const double* t, const double* rh, double* x,
                                                 double* r) {
@@ -278,157 +413,35 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, int it, const doub
   const double omega = sc[0] / sc[1];
   const double alpha = a.scal[SC_ALPHA];
   const int lane = threadIdx.x & 31;
-  double d0 = 0.0, d1 = 0.0;
+  double d1 = 0.0;
   FOR_BODIES(b) {
     if (lane < 12) {
       const size_t i = (size_t)b * 12 + lane;
       x[i] += alpha * y[i] + omega * z[i];
       const double ri = s[i] - omega * t[i];
       r[i] = ri;
-      d0 += ri * ri;
       d1 += rh[i] * ri;
     }
   }
-  cta_partials(d0, d1, a.part, SL_R2, SL_RHR);
+  cta_partials(0.0, d1, a.part, -1, SL_RHR);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scal[SC_OMEGA] = omega;
     a.dstat[DS_SOLVER_ITERS] = it;
   }
 }
 
-// ---- PCG ----
-// init: z = M r, p = z; partials r.z (SL_RHR), r.r (SL_R2 kept from k_residual)
-__global__ void __launch_bounds__(256) k_pcg_init(SolverArgs a, const double* r, double* z, double* pv) {
-  const int lane = threadIdx.x & 31;
-  double d0 = 0.0;
-  FOR_BODIES(b) {
-    const double zi = block_apply(a.Minv, b, r);
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      z[i] = zi;
-      pv[i] = zi;
-      d0 += r[i] * zi;
-    }
+__global__ void k_pair_weights(int np, const int2* ij, const int* pair_active, const int* fixed,
+                               const double* offdiag, float* w) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  float out = 0.f;
+  if (pair_active[p] > 0 && !fixed[ij[p].x] && !fixed[ij[p].y]) {
+    double f = 0.0;
+    const double* O = offdiag + (size_t)p * 288;
+    for (int k = 0; k < 144; ++k) f += O[k] * O[k];
+    out = (float)sqrt(f);
   }
-  cta_partials(d0, 0.0, a.part, SL_RHR, -1);
-}
-
-// K1: convergence check on r.r, then Ap = A p with partial p.Ap
-__global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, int it, const double* pv, double* Ap) {
-  if (solver_done(a.dstat)) return;
-  const int slots[1] = {SL_R2};
-  double sc[1];
-  cta_scalars(a.part, slots, 1, sc);
-  if (sc[0] <= a.scal[SC_THR2]) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      a.dstat[DS_R_DONE] = it;
-      a.dstat[DS_SOLVER_ITERS] = it - 1;
-    }
-    return;
-  }
-  const int lane = threadIdx.x & 31;
-  double d0 = 0.0;
-  FOR_BODIES(b) {
-    const double yi = row_product(a, b, pv);
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      Ap[i] = yi;
-      d0 += pv[i] * yi;
-    }
-  }
-  cta_partials(d0, 0.0, a.part, SL_RHV, -1);
-}
-
-// K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap; z = M r; partials r.z (new), r.r
-__global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, int it, const double* pv, const double* Ap, double* x,
-                                               double* r, double* z) {
-  if (solver_done(a.dstat)) return;
-  const int rz_old = (it & 1) ? SL_RHR : SL_TS, rz_new = (it & 1) ? SL_TS : SL_RHR;
-  const int slots[2] = {rz_old, SL_RHV};
-  double sc[2];
-  cta_scalars(a.part, slots, 2, sc);
-  const double alpha = sc[0] / sc[1];
-  const int lane = threadIdx.x & 31;
-  double d0 = 0.0, d1 = 0.0;
-  FOR_BODIES(b) {
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      x[i] += alpha * pv[i];
-      r[i] -= alpha * Ap[i];
-    }
-    __syncwarp();
-    const double zi = block_apply(a.Minv, b, r);
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      z[i] = zi;
-      d0 += r[i] * zi;
-      d1 += r[i] * r[i];
-    }
-  }
-  cta_partials(d0, d1, a.part, rz_new, SL_R2);
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.dstat[DS_SOLVER_ITERS] = it;
-}
-
-// K3: beta = rz_new / rz_old; p = z + beta p
-__global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, int it, const double* z, double* pv) {
-  if (solver_done(a.dstat)) return;
-  const int rz_old = (it & 1) ? SL_RHR : SL_TS, rz_new = (it & 1) ? SL_TS : SL_RHR;
-  const int slots[3] = {rz_new, rz_old, SL_R2};
-  double sc[3];
-  cta_scalars(a.part, slots, 3, sc);
-  if (sc[2] <= a.scal[SC_THR2]) return;  // converged: K1 of the next iteration stops
-  const double beta = sc[0] / sc[1];
-  const int lane = threadIdx.x & 31;
-  FOR_BODIES(b) {
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      pv[i] = z[i] + beta * pv[i];
-    }
-  }
-}
-
-// ---- block inverse by Gauss-Jordan with partial pivoting (one CTA of 144 threads per body) ----
-__global__ void __launch_bounds__(144) k_block_inverse(int n, const double* diag, double* Minv) {
-  const int b = blockIdx.x, t = threadIdx.x;
-  __shared__ double m[12][24];
-  __shared__ double f[12];
-  __shared__ int piv;
-  {
-    const int r = t / 12, c = t % 12;
-    m[r][c] = diag[(size_t)b * 144 + t];
-    m[r][12 + c] = r == c ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  for (int c = 0; c < 12; ++c) {
-    if (t == 0) {
-      int pr = c;
-      for (int r = c + 1; r < 12; ++r)
-        if (fabs(m[r][c]) > fabs(m[pr][c])) pr = r;
-      piv = pr;
-    }
-    __syncthreads();
-    if (piv != c && t < 24) {
-      const double tmp = m[c][t];
-      m[c][t] = m[piv][t];
-      m[piv][t] = tmp;
-    }
-    __syncthreads();
-    const double inv = 1.0 / m[c][c];
-    __syncthreads();
-    if (t < 24) m[c][t] *= inv;
-    __syncthreads();
-    if (t < 12) f[t] = m[t][c];
-    __syncthreads();
-    for (int e = t; e < 288; e += 144) {
-      const int r = e / 24, k = e % 24;
-      if (r != c && f[r] != 0.0) m[r][k] -= f[r] * m[c][k];
-    }
-    __syncthreads();
-  }
-  {
-    const int r = t / 12, c = t % 12;
-    Minv[(size_t)b * 144 + t] = m[r][12 + c];
-  }
+  w[p] = out;
 }
 
 SolverArgs solver_args(Sim& s) {
@@ -436,13 +449,17 @@ SolverArgs solver_args(Sim& s) {
   a.n = s.n;
   a.diag = s.diag;
   a.offdiag = s.offdiag;
-  a.Minv = s.Minv;
   a.row_ptr = s.row_ptr;
   a.adj_col = s.adj_col;
   a.adj_pair = s.adj_pair;
   a.pair_active = s.pair_active;
   a.fixed = s.fixed;
   a.ij = s.ij;
+  a.ncl = s.ncl;
+  a.cl_ptr = s.cl_ptr;
+  a.cl_body = s.cl_body;
+  a.cl_off = s.cl_off;
+  a.cl_inv = s.cl_inv;
   a.part = s.partials;
   a.scal = s.scal;
   a.dstat = s.dstat;
@@ -451,10 +468,95 @@ SolverArgs solver_args(Sim& s) {
 
 }  // namespace
 
-cudaError_t block_inverse(Sim& s) {
-  k_block_inverse<<<s.n, 144, 0, s.stream>>>(s.n, s.diag, s.Minv);
+// Clusters (host union-find on the coupling weights of the last assembled system) and their
+// dense inverses.  Same clustering rule as the oracle: strongest coupling first (float
+// Frobenius norm of H_IJ, ties by pair index), merged while at most cluster_max bodies.
+int build_preconditioner(Sim& s) {
+  const int n = s.n, np = s.n_pairs;
+  const int cap = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
+  std::vector<int> parent(n), size(n, 1);
+  std::iota(parent.begin(), parent.end(), 0);
+  if (cap > 1 && np > 0) {
+    k_pair_weights<<<(np + 255) / 256, 256, 0, s.stream>>>(np, s.ij, s.pair_active, s.fixed, s.offdiag, s.pair_w);
+    ++s.launches;
+    std::vector<float> w(np);
+    std::vector<int2> ij(np);
+    if (cudaMemcpyAsync(w.data(), s.pair_w, sizeof(float) * np, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+        cudaMemcpyAsync(ij.data(), s.ij, sizeof(int2) * np, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+        cudaStreamSynchronize(s.stream) != cudaSuccess)
+      return ABD_ERR_CUDA;
+    std::vector<int> order;
+    for (int p = 0; p < np; ++p)
+      if (w[p] > 0.f) order.push_back(p);
+    std::sort(order.begin(), order.end(), [&](int x, int y) { return w[x] > w[y] || (w[x] == w[y] && x < y); });
+    auto find = [&](int x) {
+      while (parent[x] != x) x = parent[x] = parent[parent[x]];
+      return x;
+    };
+    for (int p : order) {
+      const int a = find(ij[p].x), b = find(ij[p].y);
+      if (a == b || size[a] + size[b] > cap) continue;
+      if (a < b) {
+        parent[b] = a;
+        size[a] += size[b];
+      } else {
+        parent[a] = b;
+        size[b] += size[a];
+      }
+    }
+    for (int b = 0; b < n; ++b) parent[b] = find(b);
+  }
+  // clusters ordered by their first body, members in increasing order
+  std::vector<int> first(n, -1), cl_ptr(1, 0), cl_body, body_cl(n);
+  std::vector<std::vector<int>> members;
+  for (int b = 0; b < n; ++b) {
+    const int r = parent[b];
+    if (first[r] < 0) {
+      first[r] = (int)members.size();
+      members.push_back({});
+    }
+    members[first[r]].push_back(b);
+  }
+  std::vector<long long> cl_off(1, 0);
+  int max_cl = 1;
+  std::vector<int> big;  // clusters with more than one body
+  for (size_t c = 0; c < members.size(); ++c) {
+    for (int b : members[c]) {
+      cl_body.push_back(b);
+      body_cl[b] = (int)c;
+    }
+    cl_ptr.push_back((int)cl_body.size());
+    const long long d = 12LL * (long long)members[c].size();
+    cl_off.push_back(cl_off.back() + d * d);
+    max_cl = std::max(max_cl, (int)members[c].size());
+  }
+  s.ncl = (int)members.size();
+  s.max_cl = max_cl;
+  const size_t need = (size_t)cl_off.back();
+  if (need > s.cap_cl_inv) {
+    if (s.cl_inv) cudaFree(s.cl_inv);
+    s.cap_cl_inv = std::max(need, 2 * s.cap_cl_inv);
+    if (cudaMalloc(&s.cl_inv, sizeof(double) * s.cap_cl_inv) != cudaSuccess) return ABD_ERR_OVERFLOW;
+  }
+  // body -> cluster map rides in the scratch vector zb (as ints) during the setup kernel
+  int* body_cl_dev = reinterpret_cast<int*>(s.zb);
+  if (cudaMemcpyAsync(s.cl_ptr, cl_ptr.data(), sizeof(int) * cl_ptr.size(), cudaMemcpyHostToDevice, s.stream) ||
+      cudaMemcpyAsync(s.cl_body, cl_body.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s.stream) ||
+      cudaMemcpyAsync(s.cl_off, cl_off.data(), sizeof(long long) * cl_off.size(), cudaMemcpyHostToDevice,
+                      s.stream) ||
+      cudaMemcpyAsync(body_cl_dev, body_cl.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s.stream))
+    return ABD_ERR_CUDA;
+  SolverArgs a = solver_args(s);
+  const size_t smem = sizeof(double) * 144 * (size_t)max_cl * max_cl;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  const int grid = std::min(s.ncl, 4 * 148);
+  k_cluster_inverse<<<grid, AT, smem, s.stream>>>(a, 0, s.ncl, body_cl_dev);
   ++s.launches;
-  return cudaGetLastError();
+  // the host vectors must outlive the asynchronous copies
+  if (cudaStreamSynchronize(s.stream) != cudaSuccess) return ABD_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
 // Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.
@@ -463,48 +565,51 @@ int krylov_solve(Sim& s, double* x, int* iters_out) {
   const double* bvec = s.g;
   cudaStream_t st = s.stream;
   const bool pcg = s.prm.solver == 1;
-  // |b|^2 and the initial residual
-  k_norm2<<<kRedBlocks, 256, 0, st>>>(a, bvec, SL_B2);
+  // b^T M^-1 b sets the threshold
+  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
   k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
                                          pcg ? nullptr : s.v);
   s.launches += 2;
-  if (finish_dot(s, SL_B2, s.scal + SC_THR2) != cudaSuccess) return ABD_ERR_CUDA;
+  if (finish_dot(s, SL_BZ, s.scal + SC_THR2) != cudaSuccess) return ABD_ERR_CUDA;
   if (cudaMemcpyAsync(s.hval, s.scal + SC_THR2, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return ABD_ERR_CUDA;
-  const double b2 = s.hval[0];
-  if (b2 == 0.0) {
+  const double bz = s.hval[0];
+  if (!(bz > 0.0)) {
     cudaMemsetAsync(x, 0, sizeof(double) * 12 * s.n, st);
     if (iters_out) *iters_out = 0;
     return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
   }
-  const double thr2 = (s.prm.cg_tol * s.prm.cg_tol) * b2;
+  const double thr2 = (s.prm.cg_tol * s.prm.cg_tol) * bz;
   double hs[5] = {1.0, 1.0, 1.0, 1.0, thr2};  // rho (both parities), alpha, omega, thr^2
   cudaMemcpyAsync(s.scal, hs, sizeof(hs), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st);
   cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st);
-  if (pcg) {
-    k_pcg_init<<<kRedBlocks, 256, 0, st>>>(a, s.r, s.z, s.pv);
-    ++s.launches;
-  }
+  // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
+  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
+  ++s.launches;
   const int maxit = s.prm.cg_max_iter;
   int it = 1;
-  int status = ABD_OK;
   for (;;) {
     for (int k = 0; k < kCheckEvery && it <= maxit; ++k, ++it) {
       if (pcg) {
+        const int rz_new = (it & 1) ? SL_RZ1 : SL_RZ0;
         k_pcg_1<<<kRedBlocks, 256, 0, st>>>(a, it, s.pv, s.v);
-        k_pcg_2<<<kRedBlocks, 256, 0, st>>>(a, it, s.pv, s.v, x, s.r, s.z);
+        k_pcg_2<<<kRedBlocks, 256, 0, st>>>(a, it, s.pv, s.v, x, s.r);
+        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.z, nullptr, rz_new);
         k_pcg_3<<<kRedBlocks, 256, 0, st>>>(a, it, s.z, s.pv);
-        s.launches += 3;
+        s.launches += 4;
       } else {
-        k_bicg_1<<<kRedBlocks, 256, 0, st>>>(a, it, s.r, s.pv, s.v, s.y);
+        k_bicg_1<<<kRedBlocks, 256, 0, st>>>(a, it, s.r, s.pv, s.v);
+        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.pv, s.y, nullptr, -1);
         k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
         k_bicg_3<<<kRedBlocks, 256, 0, st>>>(a, it, s.r, s.v, s.s);
-        k_bicg_4<<<kRedBlocks, 256, 0, st>>>(a, it, s.y, s.s, s.z, x);
+        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
+        k_bicg_4<<<kRedBlocks, 256, 0, st>>>(a, it, s.y, x);
         k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
         k_bicg_6<<<kRedBlocks, 256, 0, st>>>(a, it, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-        s.launches += 6;
+        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
+        s.launches += 9;
       }
     }
     if (cudaGetLastError() != cudaSuccess) return ABD_ERR_CUDA;
@@ -518,7 +623,7 @@ int krylov_solve(Sim& s, double* x, int* iters_out) {
     }
   }
   if (iters_out) *iters_out = s.hstat[20];
-  return status;
+  return ABD_OK;
 }
 
 }  // namespace abd

@@ -29,7 +29,8 @@ class SimParams:
     alpha_min: float = 1e-3          # line-search floor (const_params.py:29)
     ls_noise_floor: float = 1e-12    # also accept a trial when |E1 - E0| <= floor |E0|: below the
                                      # energies' rounding error the Armijo test is noise
-    max_iter: int = 100              # Newton iteration cap (abd.py:114)
+    max_iter: int = 10               # Newton iteration cap: the value step() reads (const_params.py:25
+                                     # via abd.py:1); simulator_args' 100 (abd.py:114) is never used
     armijo_sign: int = -1            # -1: E1 < E0 - c1 a dq.g ; +1: reference form abd.py:156
     ground_enabled: bool = False     # vertex-ground plane contact (culling.py:54-82)
     ground: float = -0.5             # plane height (const_params.py:36)
@@ -40,8 +41,11 @@ class SimParams:
     enable_pt: bool = True           # const_params.py:41-43
     enable_ee: bool = True
     enable_vg: bool = True
-    solver: int = SOLVER_BICGSTAB    # reference solver: bicgstab (abd.py:244)
-    cg_tol: float = 1e-10            # relative residual of the Newton linear solve
+    solver: int = SOLVER_PCG         # the reference calls bicgstab (abd.py:244); the projected
+                                     # Hessian is SPD, so CG is the default
+    precond: int = 1                 # 1: contact-cluster block Jacobi; 0: per-body 12x12 blocks
+    cluster_max: int = 12            # bodies per preconditioner cluster
+    cg_tol: float = 1e-10            # stop when r^T M^-1 r <= cg_tol^2 b^T M^-1 b
     cg_max_iter: int = 2000
     precision: int = PRECISION_FP64
     refine_tol: float = 1e-10        # mixed precision: FP64 refinement target
@@ -76,6 +80,8 @@ class SimParams:
         c.cg_max_iter = self.cg_max_iter
         c.precision = self.precision
         c.contact_psd = self.contact_psd
+        c.precond = self.precond
+        c.cluster_max = self.cluster_max
         return c
 
     def as_dict(self):
@@ -93,5 +99,6 @@ class CParams(ctypes.Structure):
         ("max_iter", ctypes.c_int), ("armijo_sign", ctypes.c_int), ("ground_enabled", ctypes.c_int),
         ("psd_ee", ctypes.c_int), ("enable_pt", ctypes.c_int), ("enable_ee", ctypes.c_int),
         ("enable_vg", ctypes.c_int), ("solver", ctypes.c_int), ("cg_max_iter", ctypes.c_int),
-        ("precision", ctypes.c_int), ("contact_psd", ctypes.c_int),
+        ("precision", ctypes.c_int), ("contact_psd", ctypes.c_int), ("precond", ctypes.c_int),
+        ("cluster_max", ctypes.c_int),
     ]

@@ -62,6 +62,8 @@ class AffineBodySimulator:
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise _lib.AbdError("AffineBodySimulator runs on a CUDA device only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.flat = flat = flatten_bodies(bodies)
         self.n_verts = int(flat["voff"][-1])
         L = _lib.load()

@@ -43,10 +43,12 @@ typedef struct abd_params {
   int ground_enabled; /* vertex-ground plane contact at y = ground (culling.py:54-82, vg_ipc.py) */
   int psd_ee;         /* contact_psd == 0 only: clamp EE eigenvalues as PT does */
   int enable_pt, enable_ee, enable_vg; /* const_params.py:41-43 */
-  int solver;         /* 0: block-Jacobi BiCGSTAB (abd.py:244 uses bicgstab), 1: block-Jacobi PCG */
+  int solver;         /* 0: preconditioned BiCGSTAB (abd.py:244 uses bicgstab), 1: PCG (default) */
   int cg_max_iter;
   int precision;      /* 0: FP64 throughout; 1: FP32 Krylov solve inside FP64 refinement */
   int contact_psd;    /* 1: PSD projection of the barrier Hessian; 0: the reference's form */
+  int precond;        /* 1: contact-cluster block Jacobi (clusters of <= cluster_max bodies); 0: per body */
+  int cluster_max;    /* 1..12 */
 } abd_params;
 
 /* Scene description (host arrays, copied at creation).  Bodies are concatenated:

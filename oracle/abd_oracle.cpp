@@ -45,7 +45,7 @@ struct Params {
   double dt, dhat, d2hat, kappa, stiffness, gravity, tol, c1, alpha_min, ground, cg_tol, refine_tol;
   double ls_noise_floor;
   int max_iter, armijo_sign, ground_enabled, psd_ee, enable_pt, enable_ee, enable_vg, solver,
-      cg_max_iter, precision, contact_psd;
+      cg_max_iter, precision, contact_psd, precond, cluster_max;
 };
 
 struct V3 {
@@ -775,61 +775,177 @@ void inv12(const double* Ain, double* out) {
     for (int c = 0; c < 12; ++c) out[r * 12 + c] = a[r][12 + c];
 }
 
+// In-place Gauss-Jordan inverse without pivoting of an SPD matrix (row-major N x N).
+void inv_spd_inplace(std::vector<double>& a, int N) {
+  for (int k = 0; k < N; ++k) {
+    const double p = a[(size_t)k * N + k];
+    a[(size_t)k * N + k] = 1.0;
+    const double ip = 1.0 / p;
+    for (int j = 0; j < N; ++j) a[(size_t)k * N + j] *= ip;
+    for (int i = 0; i < N; ++i) {
+      if (i == k) continue;
+      const double f = a[(size_t)i * N + k];
+      a[(size_t)i * N + k] = 0.0;
+      if (f != 0.0)
+        for (int j = 0; j < N; ++j) a[(size_t)i * N + j] -= f * a[(size_t)k * N + j];
+    }
+  }
+}
+
+// Contact clusters for the preconditioner: union-find over free body pairs with active
+// contacts, strongest coupling (Frobenius norm of the off-diagonal block, as float) first,
+// ties by pair index, merged only while the cluster stays within cluster_max bodies.
+// Clusters list their bodies in increasing order and are ordered by their first body.
+void build_clusters(const Oracle& o, std::vector<int>& cl_ptr, std::vector<int>& cl_body) {
+  const int n = o.n, m = (int)o.ij.size() / 2;
+  std::vector<std::pair<float, int>> w;
+  for (int q = 0; q < m; ++q) {
+    const int I = o.ij[2 * q], J = o.ij[2 * q + 1];
+    if (o.fixed[I] || o.fixed[J]) continue;
+    double f = 0.0;
+    for (int k = 0; k < 144; ++k) f += o.off[144 * (size_t)q + k] * o.off[144 * (size_t)q + k];
+    if (f > 0.0) w.push_back({(float)std::sqrt(f), q});
+  }
+  std::sort(w.begin(), w.end(), [](const std::pair<float, int>& a, const std::pair<float, int>& b) {
+    return a.first > b.first || (a.first == b.first && a.second < b.second);
+  });
+  std::vector<int> parent(n), size(n, 1);
+  for (int b = 0; b < n; ++b) parent[b] = b;
+  auto find = [&](int x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  };
+  const int cap = o.prm.precond == 1 ? std::max(1, o.prm.cluster_max) : 1;
+  for (auto& e : w) {
+    const int a = find(o.ij[2 * e.second]), b = find(o.ij[2 * e.second + 1]);
+    if (a == b || size[a] + size[b] > cap) continue;
+    if (a < b) {
+      parent[b] = a;
+      size[a] += size[b];
+    } else {
+      parent[a] = b;
+      size[b] += size[a];
+    }
+  }
+  std::vector<int> root_first(n, -1), order;
+  std::vector<std::vector<int>> members;
+  for (int b = 0; b < n; ++b) {
+    const int r = find(b);
+    if (root_first[r] < 0) {
+      root_first[r] = (int)members.size();
+      members.push_back({});
+    }
+    members[root_first[r]].push_back(b);
+  }
+  cl_ptr.assign(1, 0);
+  cl_body.clear();
+  for (auto& mb : members) {
+    cl_body.insert(cl_body.end(), mb.begin(), mb.end());
+    cl_ptr.push_back((int)cl_body.size());
+  }
+}
+
 int solve(Oracle& o) {
-  const int n = o.n, N = 12 * n;
-  std::vector<double> Minv(144 * (size_t)n);
-#pragma omp parallel for schedule(static)
-  for (int b = 0; b < n; ++b) inv12(&o.diag[144 * b], &Minv[144 * b]);
-  auto prec = [&](const std::vector<double>& v, std::vector<double>& out) {
-    out.resize(N);
-#pragma omp parallel for schedule(static)
-    for (int b = 0; b < n; ++b)
-      for (int r = 0; r < 12; ++r) {
-        double s = 0.0;
-        for (int c = 0; c < 12; ++c) s += Minv[144 * b + r * 12 + c] * v[12 * b + c];
-        out[12 * b + r] = s;
+  const int n = o.n, N = 12 * n, m = (int)o.ij.size() / 2;
+  // preconditioner: dense inverse of every cluster's block system
+  std::vector<int> cl_ptr, cl_body;
+  build_clusters(o, cl_ptr, cl_body);
+  const int ncl = (int)cl_ptr.size() - 1;
+  std::vector<size_t> cl_off(ncl + 1, 0);
+  for (int c = 0; c < ncl; ++c) {
+    const size_t s = cl_ptr[c + 1] - cl_ptr[c];
+    cl_off[c + 1] = cl_off[c] + 144 * s * s;
+  }
+  std::vector<double> Kinv(cl_off[ncl]);
+  std::vector<int> where(n, -1);
+  for (int c = 0; c < ncl; ++c)
+    for (int k = cl_ptr[c]; k < cl_ptr[c + 1]; ++k) where[cl_body[k]] = k - cl_ptr[c];
+  std::vector<int> body_cl(n);
+  for (int c = 0; c < ncl; ++c)
+    for (int k = cl_ptr[c]; k < cl_ptr[c + 1]; ++k) body_cl[cl_body[k]] = c;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < ncl; ++c) {
+    const int s = cl_ptr[c + 1] - cl_ptr[c], D = 12 * s;
+    std::vector<double> K((size_t)D * D, 0.0);
+    for (int a = 0; a < s; ++a) {
+      const int b = cl_body[cl_ptr[c] + a];
+      for (int r = 0; r < 12; ++r)
+        for (int cc = 0; cc < 12; ++cc) K[(size_t)(12 * a + r) * D + 12 * a + cc] = o.diag[144 * b + r * 12 + cc];
+    }
+    if (s > 1)
+      for (int q = 0; q < m; ++q) {
+        const int I = o.ij[2 * q], J = o.ij[2 * q + 1];
+        if (body_cl[I] != c || body_cl[J] != c) continue;
+        const int a = where[I], b = where[J];
+        for (int r = 0; r < 12; ++r)
+          for (int cc = 0; cc < 12; ++cc) {
+            const double v = o.off[144 * (size_t)q + r * 12 + cc];
+            K[(size_t)(12 * a + r) * D + 12 * b + cc] = v;
+            K[(size_t)(12 * b + cc) * D + 12 * a + r] = v;
+          }
       }
+    inv_spd_inplace(K, D);
+    std::copy(K.begin(), K.end(), Kinv.begin() + cl_off[c]);
+  }
+  auto prec = [&](const std::vector<double>& v, std::vector<double>& out) {
+    out.assign(N, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < ncl; ++c) {
+      const int s = cl_ptr[c + 1] - cl_ptr[c], D = 12 * s;
+      const double* K = &Kinv[cl_off[c]];
+      for (int i = 0; i < D; ++i) {
+        double acc = 0.0;
+        for (int j = 0; j < D; ++j) acc += K[(size_t)i * D + j] * v[12 * cl_body[cl_ptr[c] + j / 12] + j % 12];
+        out[12 * cl_body[cl_ptr[c] + i / 12] + i % 12] = acc;
+      }
+    }
   };
   std::vector<double>& x = o.dq;
   const std::vector<double>& bvec = o.g;
-  const double bnorm = std::sqrt(ddot(bvec, bvec));
-  if (bnorm == 0.0) {
+  std::vector<double> zb;
+  prec(bvec, zb);
+  const double bz = ddot(bvec, zb);
+  if (!(bz > 0.0)) {
     std::fill(x.begin(), x.end(), 0.0);
     return 0;
   }
-  const double thr = o.prm.cg_tol * bnorm;
+  const double thr2 = o.prm.cg_tol * o.prm.cg_tol * bz;
   std::vector<double> r(N), Ax;
   spmv(o, x, Ax);
   for (int i = 0; i < N; ++i) r[i] = bvec[i] - Ax[i];
-  if (std::sqrt(ddot(r, r)) <= thr) return 0;
   int it = 0;
-  if (o.prm.solver == 1) {  // PCG
+  if (o.prm.solver == 1) {  // PCG, converged when r^T M^-1 r <= tol^2 b^T M^-1 b
     std::vector<double> z, pv, Ap;
     prec(r, z);
-    pv = z;
     double rz = ddot(r, z);
+    if (rz <= thr2) return 0;
+    pv = z;
     for (it = 1; it <= o.prm.cg_max_iter; ++it) {
       spmv(o, pv, Ap);
-      const double alpha = rz / ddot(pv, Ap);
+      const double pAp = ddot(pv, Ap);
+      if (!(pAp > 0.0)) break;
+      const double alpha = rz / pAp;
       for (int i = 0; i < N; ++i) {
         x[i] += alpha * pv[i];
         r[i] -= alpha * Ap[i];
       }
-      if (std::sqrt(ddot(r, r)) <= thr) break;
       prec(r, z);
       const double rzn = ddot(r, z);
+      if (rzn <= thr2) break;
       const double beta = rzn / rz;
       for (int i = 0; i < N; ++i) pv[i] = z[i] + beta * pv[i];
       rz = rzn;
     }
     return std::min(it, o.prm.cg_max_iter);
   }
-  // BiCGSTAB, right preconditioned
-  std::vector<double> rh = r, pv(N, 0.0), v(N, 0.0), y, s(N), z, t;
+  // BiCGSTAB, right preconditioned; converged in the preconditioned norm of s / r
+  std::vector<double> rh = r, pv(N, 0.0), v(N, 0.0), y, s(N), z, t, zz;
+  prec(r, zz);
+  if (ddot(r, zz) <= thr2) return 0;
   double rho_old = 1.0, alpha = 1.0, omega = 1.0;
   for (it = 1; it <= o.prm.cg_max_iter; ++it) {
     const double rho = ddot(rh, r);
-    if (rho == 0.0) break;
+    if (rho == 0.0 || !std::isfinite(rho)) break;
     if (it == 1) {
       pv = r;
     } else {
@@ -840,18 +956,19 @@ int solve(Oracle& o) {
     spmv(o, y, v);
     alpha = rho / ddot(rh, v);
     for (int i = 0; i < N; ++i) s[i] = r[i] - alpha * v[i];
-    if (std::sqrt(ddot(s, s)) <= thr) {
+    prec(s, z);
+    if (ddot(s, z) <= thr2) {
       for (int i = 0; i < N; ++i) x[i] += alpha * y[i];
       break;
     }
-    prec(s, z);
     spmv(o, z, t);
     omega = ddot(t, s) / ddot(t, t);
     for (int i = 0; i < N; ++i) {
       x[i] += alpha * y[i] + omega * z[i];
       r[i] = s[i] - omega * t[i];
     }
-    if (std::sqrt(ddot(r, r)) <= thr) break;
+    prec(r, zz);
+    if (ddot(r, zz) <= thr2) break;
     rho_old = rho;
   }
   return std::min(it, o.prm.cg_max_iter);
