@@ -620,12 +620,14 @@ __global__ void __launch_bounds__(1024) k_reduce_vals(const double* pv, int np, 
   if (t == 0) *out = red[0];
 }
 
-__global__ void k_export_off(int np, const int* pair_active, const double* offdiag, const int2* ij, double* out,
-                             int* ijout, int cap) {
+// exported blocks follow the solver's view: pairs without active contacts or touching a fixed
+// (Dirichlet) body have no coupling block
+__global__ void k_export_off(int np, const int* pair_active, const int* fixed, const double* offdiag, const int2* ij,
+                             double* out, int* ijout, int cap) {
   const int p = blockIdx.x;
   if (p >= np || p >= cap) return;
-  for (int e = threadIdx.x; e < 144; e += blockDim.x)
-    out[(size_t)p * 144 + e] = pair_active[p] > 0 ? offdiag[(size_t)p * 288 + e] : 0.0;
+  const bool live = pair_active[p] > 0 && !fixed[ij[p].x] && !fixed[ij[p].y];
+  for (int e = threadIdx.x; e < 144; e += blockDim.x) out[(size_t)p * 144 + e] = live ? offdiag[(size_t)p * 288 + e] : 0.0;
   if (threadIdx.x == 0 && ijout) {
     ijout[2 * p] = ij[p].x;
     ijout[2 * p + 1] = ij[p].y;
@@ -799,7 +801,7 @@ cudaError_t min_toi(Sim& s, double* out) {
 cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap) {
   const int np = s.n_pairs < cap ? s.n_pairs : cap;
   if (np == 0) return cudaSuccess;
-  k_export_off<<<np, 128, 0, s.stream>>>(s.n_pairs, s.pair_active, s.offdiag, s.ij, off_dev, ij_dev, cap);
+  k_export_off<<<np, 128, 0, s.stream>>>(s.n_pairs, s.pair_active, s.fixed, s.offdiag, s.ij, off_dev, ij_dev, cap);
   ++s.launches;
   return cudaGetLastError();
 }
