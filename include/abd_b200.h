@@ -142,6 +142,19 @@ int abd_compute_energy(abd_sim* sim, const abd_states* st, const double* Ak_dev,
 int abd_ccd(abd_sim* sim, const double* A_dev, const double* p_dev, const double* A1_dev, const double* p1_dev,
             double* alpha, double* raw_toi);
 
+/* Inertia + orthogonality energy of n_bodies bodies at trial DOFs (Ak, pk), with the
+ * prediction from st->A0 / p0 / Adot / pdot, written to E_dev (one double).  No counterpart in
+ * the reference: it is the body part of abd_compute_energy, made for callers that may not
+ * allocate device memory while running (fixed-budget real-time loops, plug-ins whose host
+ * application owns all device memory).  It allocates nothing; its only scratch is a
+ * fixed array inside the library (4096 doubles, so n_bodies <= 1,048,576, else
+ * ABD_ERR_INVALID).  All calls share that array: calls that overlap on the GPU race.  The
+ * first call on a device looks up the array's address (make it before any stream capture).
+ * Fixed bodies contribute nothing.  Runs on `stream` (NULL: legacy default stream). */
+int abd_inertia_energy_noalloc(const abd_params* prm, int n_bodies, const abd_states* st, const double* Ak_dev,
+                               const double* pk_dev, const double* mass_dev, const double* I0_dev,
+                               const int* fixed_dev, double* E_dev, void* stream);
+
 /* Device status bits accumulated since the last call (and cleared). */
 int abd_take_status(abd_sim* sim, int* status);
 const char* abd_status_string(int code);
