@@ -96,6 +96,11 @@ struct Tree {
   int* body_root = nullptr;   // [n] node id of the body's subtree, -1 if the body has none
   int* flags = nullptr;       // [N-1] refit arrival counters
   Box* box = nullptr;         // [2N-1]
+  // per-body bottom-up refit schedule: the internal nodes of body b's subtree grouped by
+  // height, order[lvl[body_lvl[b] + h - 1] .. lvl[body_lvl[b] + h]) for h = 1..heights
+  int* order = nullptr;       // [N-1]
+  int* lvl = nullptr;         // [sum over bodies of (heights + 1)]
+  int* body_lvl = nullptr;    // [n+1]
 };
 
 // ---------------------------------------------------------------------------------------
@@ -195,6 +200,10 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x);
 cudaError_t prim_boxes(Sim& s, const double* y0, const double* y1);
 cudaError_t body_boxes(Sim& s, const double* y0, const double* y1);
 cudaError_t body_pairs(Sim& s, bool* overflow);
+// fused per-body broad phase: optional transform (A != null: y0 = x(A, p); A1 != null:
+// y1 = x(A1, p1)), body boxes, leaf boxes and the subtree refits of both trees
+cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A1, const double* p1, double* y0,
+                       double* y1);
 
 // narrow.cu
 enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS = 3 };

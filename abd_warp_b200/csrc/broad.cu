@@ -200,7 +200,313 @@ __global__ void k_fill_adj(int n, int W, const uint32_t* __restrict__ mask, cons
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// fused per-body broad phase: one CTA per body
+// ---------------------------------------------------------------------------------------
+constexpr int BB = 256;
+
+struct BroadArgs {
+  int n, V, T, E;
+  const int *voff, *toff, *eoff, *tris, *edges;
+  const double* x0;
+  const double *A, *p, *A1, *p1;
+  double *y0, *y1;
+  double dhh;
+  Box* body_box;
+  const int *tri_leaf, *edge_leaf;
+  Box *tri_box, *edge_box;
+  const int *tri_child, *edge_child, *tri_order, *edge_order, *tri_lvl, *edge_lvl, *tri_blvl, *edge_blvl;
+};
+
+__device__ inline void refit_level(const int* child, const int* order, int k0, int k1, Box* box) {
+  for (int k = k0 + (int)threadIdx.x; k < k1; k += BB) {
+    const int node = order[k];
+    const Box a = load_box_cg(&box[child[2 * node]]);
+    const Box b = load_box_cg(&box[child[2 * node + 1]]);
+    Box u;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      u.lo[c] = fminf(a.lo[c], b.lo[c]);
+      u.hi[c] = fmaxf(a.hi[c], b.hi[c]);
+    }
+    store_box(&box[node], u);
+  }
+}
+
+__global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
+  const int b = blockIdx.x;
+  __shared__ double red[12][BB / 32];
+  const int v0 = a.voff[b], v1 = a.voff[b + 1];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double lo1[3] = {INFINITY, INFINITY, INFINITY}, hi1[3] = {-INFINITY, -INFINITY, -INFINITY};
+  const bool swept = a.y1 != nullptr;
+  // vertices: transform (same arithmetic as k_transform) and bounds
+  for (int v = v0 + threadIdx.x; v < v1; v += BB) {
+    double y[3], z[3];
+    if (a.A) {
+      const double r0 = a.x0[3 * v], r1 = a.x0[3 * v + 1], r2 = a.x0[3 * v + 2];
+      const double* m = a.A + 9 * b;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        y[j] = ((m[j] * r0 + m[3 + j] * r1) + m[6 + j] * r2) + a.p[3 * b + j];
+        a.y0[3 * v + j] = y[j];
+      }
+      if (swept && a.A1) {
+        const double* m1 = a.A1 + 9 * b;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          z[j] = ((m1[j] * r0 + m1[3 + j] * r1) + m1[6 + j] * r2) + a.p1[3 * b + j];
+          a.y1[3 * v + j] = z[j];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) y[j] = a.y0[3 * v + j];
+    }
+    if (swept && !a.A1) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) z[j] = a.y1[3 * v + j];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      lo[j] = fmin(lo[j], y[j]);
+      hi[j] = fmax(hi[j], y[j]);
+      if (swept) {
+        lo1[j] = fmin(lo1[j], z[j]);
+        hi1[j] = fmax(hi1[j], z[j]);
+      }
+    }
+  }
+  // body box: warp then CTA reduction of the float64 bounds (min/max are exact)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[j] = fmin(lo[j], __shfl_xor_sync(0xffffffffu, lo[j], o));
+      hi[j] = fmax(hi[j], __shfl_xor_sync(0xffffffffu, hi[j], o));
+      lo1[j] = fmin(lo1[j], __shfl_xor_sync(0xffffffffu, lo1[j], o));
+      hi1[j] = fmax(hi1[j], __shfl_xor_sync(0xffffffffu, hi1[j], o));
+    }
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      red[j][warp] = lo[j];
+      red[3 + j][warp] = hi[j];
+      red[6 + j][warp] = lo1[j];
+      red[9 + j][warp] = hi1[j];
+    }
+  __syncthreads();  // also makes this CTA's y0 / y1 writes visible to all its threads
+  if (threadIdx.x == 0) {
+    Box B;
+    for (int j = 0; j < 3; ++j) {
+      double l = red[j][0], h = red[3 + j][0], l1 = red[6 + j][0], h1 = red[9 + j][0];
+      for (int w = 1; w < BB / 32; ++w) {
+        l = fmin(l, red[j][w]);
+        h = fmax(h, red[3 + j][w]);
+        l1 = fmin(l1, red[6 + j][w]);
+        h1 = fmax(h1, red[9 + j][w]);
+      }
+      B.lo[j] = (float)(l - a.dhh);
+      B.hi[j] = (float)(h + a.dhh);
+      if (swept) {
+        B.lo[j] = fminf(B.lo[j], (float)l1);
+        B.hi[j] = fmaxf(B.hi[j], (float)h1);
+      }
+    }
+    store_box(&a.body_box[b], B);
+  }
+  // leaf boxes (same rounding as k_edge_boxes / k_tri_boxes)
+  for (int e = a.eoff[b] + threadIdx.x; e < a.eoff[b + 1]; e += BB) {
+    const int i0 = a.edges[2 * e], i1 = a.edges[2 * e + 1];
+    Box B;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double u = a.y0[3 * i0 + k], w = a.y0[3 * i1 + k];
+      B.lo[k] = (float)(fmin(u, w) - a.dhh);
+      B.hi[k] = (float)(fmax(u, w) + a.dhh);
+      if (swept) {
+        const double u1 = a.y1[3 * i0 + k], w1 = a.y1[3 * i1 + k];
+        B.lo[k] = fminf(B.lo[k], (float)fmin(u1, w1));
+        B.hi[k] = fmaxf(B.hi[k], (float)fmax(u1, w1));
+      }
+    }
+    store_box(&a.edge_box[(a.E - 1) + a.edge_leaf[e]], B);
+  }
+  for (int t = a.toff[b] + threadIdx.x; t < a.toff[b + 1]; t += BB) {
+    const int i0 = a.tris[3 * t], i1 = a.tris[3 * t + 1], i2 = a.tris[3 * t + 2];
+    Box B;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double u = a.y0[3 * i0 + k], w = a.y0[3 * i1 + k], q = a.y0[3 * i2 + k];
+      B.lo[k] = (float)(fmin(fmin(u, w), q) - 0.0);
+      B.hi[k] = (float)(fmax(fmax(u, w), q) + 0.0);
+      if (swept) {
+        const double u1 = a.y1[3 * i0 + k], w1 = a.y1[3 * i1 + k], q1 = a.y1[3 * i2 + k];
+        B.lo[k] = fminf(B.lo[k], (float)fmin(fmin(u1, w1), q1));
+        B.hi[k] = fmaxf(B.hi[k], (float)fmax(fmax(u1, w1), q1));
+      }
+    }
+    store_box(&a.tri_box[(a.T - 1) + a.tri_leaf[t]], B);
+  }
+  __syncthreads();
+  // refit the body's subtrees of both trees, one height level at a time
+  const int te0 = a.tri_blvl[b], te1 = a.tri_blvl[b + 1];
+  const int ee0 = a.edge_blvl[b], ee1 = a.edge_blvl[b + 1];
+  const int ht = te1 - te0 - 1, he = ee1 - ee0 - 1;
+  const int H = ht > he ? ht : he;
+  for (int h = 1; h <= H; ++h) {
+    if (h <= ht) refit_level(a.tri_child, a.tri_order, a.tri_lvl[te0 + h - 1], a.tri_lvl[te0 + h], a.tri_box);
+    if (h <= he) refit_level(a.edge_child, a.edge_order, a.edge_lvl[ee0 + h - 1], a.edge_lvl[ee0 + h], a.edge_box);
+    __syncthreads();
+  }
+}
+
+// Body pairs for n <= kSmallPairs in one CTA: the same outputs as the multi-kernel path
+// (sorted ij list, CSR adjacency in increasing neighbour order, pair index of every entry).
+constexpr int kSmallPairs = 4096;
+constexpr int PT = 1024;
+
+// dynamic shared memory: float bx[n][6], int cnt[n], int up[n]
+__global__ void __launch_bounds__(PT) k_body_pairs_small(int n, const Box* __restrict__ body_box, int* row_ptr,
+                                                          int* upper_ptr, int cap_pairs, int cap_adj, int2* ij,
+                                                          int* adj_col, int* adj_pair) {
+  extern __shared__ float smem_pairs[];
+  float(*bx)[6] = reinterpret_cast<float(*)[6]>(smem_pairs);
+  int* cnt = reinterpret_cast<int*>(smem_pairs + 6 * (size_t)n);
+  int* up = cnt + n;
+  __shared__ int wsum[2][PT / 32];
+  for (int i = threadIdx.x; i < n; i += PT) {
+    const Box B = load_box(&body_box[i]);
+    for (int c = 0; c < 3; ++c) {
+      bx[i][c] = B.lo[c];
+      bx[i][3 + c] = B.hi[c];
+    }
+  }
+  __syncthreads();
+  auto ov = [&](int I, int J) {
+    return !(bx[I][0] > bx[J][3] || bx[J][0] > bx[I][3] || bx[I][1] > bx[J][4] || bx[J][1] > bx[I][4] ||
+             bx[I][2] > bx[J][5] || bx[J][2] > bx[I][5]);
+  };
+  for (int I = threadIdx.x; I < n; I += PT) {
+    int full = 0, upper = 0;
+    for (int J = 0; J < n; ++J)
+      if (J != I && ov(I, J)) {
+        ++full;
+        if (J > I) ++upper;
+      }
+    cnt[I] = full;
+    up[I] = upper;
+  }
+  __syncthreads();
+  // exclusive scans of cnt and up (rows strided over threads: chunked by thread)
+  const int per = (n + PT - 1) / PT;
+  const int r0 = threadIdx.x * per, r1 = min(n, r0 + per);
+  int s0 = 0, s1 = 0;
+  for (int i = r0; i < r1; ++i) {
+    s0 += cnt[i];
+    s1 += up[i];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x0 = s0, x1 = s1;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+    if (lane >= o) {
+      x0 += y0;
+      x1 += y1;
+    }
+  }
+  if (lane == 31) {
+    wsum[0][warp] = x0;
+    wsum[1][warp] = x1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int a0 = 0, a1 = 0;
+    for (int w = 0; w < PT / 32; ++w) {
+      const int c0 = wsum[0][w], c1 = wsum[1][w];
+      wsum[0][w] = a0;
+      wsum[1][w] = a1;
+      a0 += c0;
+      a1 += c1;
+    }
+    row_ptr[n] = a0;
+    upper_ptr[n] = a1;
+  }
+  __syncthreads();
+  int e0 = wsum[0][warp] + x0 - s0, e1 = wsum[1][warp] + x1 - s1;
+  for (int i = r0; i < r1; ++i) {
+    const int c0 = cnt[i], c1 = up[i];
+    cnt[i] = e0;
+    up[i] = e1;
+    row_ptr[i] = e0;
+    upper_ptr[i] = e1;
+    e0 += c0;
+    e1 += c1;
+  }
+  __syncthreads();
+  for (int I = threadIdx.x; I < n; I += PT) {
+    int pos = cnt[I], u = up[I];
+    for (int J = 0; J < n; ++J) {
+      if (J == I || !ov(I, J)) continue;
+      int pr;
+      if (J > I) {
+        pr = u++;
+        if (pr < cap_pairs) ij[pr] = make_int2(I, J);
+      } else {
+        int rank = 0;  // upper neighbours of J below I
+        for (int K = J + 1; K < I; ++K)
+          if (ov(J, K)) ++rank;
+        pr = up[J] + rank;
+      }
+      if (pos < cap_adj) {
+        adj_col[pos] = J;
+        adj_pair[pos] = pr;
+      }
+      ++pos;
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A1, const double* p1, double* y0,
+                       double* y1) {
+  BroadArgs a;
+  a.n = s.n;
+  a.V = s.V;
+  a.T = s.T;
+  a.E = s.E;
+  a.voff = s.voff;
+  a.toff = s.toff;
+  a.eoff = s.eoff;
+  a.tris = s.tris;
+  a.edges = s.edges;
+  a.x0 = s.x0;
+  a.A = A;
+  a.p = p;
+  a.A1 = A1;
+  a.p1 = p1;
+  a.y0 = y0;
+  a.y1 = y1;
+  a.dhh = s.prm.dhat * 0.5;
+  a.body_box = s.body_box;
+  a.tri_leaf = s.tri_tree.prim_leaf;
+  a.edge_leaf = s.edge_tree.prim_leaf;
+  a.tri_box = s.tri_tree.box;
+  a.edge_box = s.edge_tree.box;
+  a.tri_child = s.tri_tree.child;
+  a.edge_child = s.edge_tree.child;
+  a.tri_order = s.tri_tree.order;
+  a.edge_order = s.edge_tree.order;
+  a.tri_lvl = s.tri_tree.lvl;
+  a.edge_lvl = s.edge_tree.lvl;
+  a.tri_blvl = s.tri_tree.body_lvl;
+  a.edge_blvl = s.edge_tree.body_lvl;
+  k_body_broad<<<s.n, BB, 0, s.stream>>>(a);
+  ++s.launches;
+  return cudaGetLastError();
+}
 
 cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
   if (s.V == 0) return cudaSuccess;
@@ -237,13 +543,23 @@ cudaError_t body_boxes(Sim& s, const double* y0, const double* y1) {
 // Synchronises the stream to read the counts; *overflow is set when a capacity is short.
 cudaError_t body_pairs(Sim& s, bool* overflow) {
   const int n = s.n, W = s.W;
-  k_pair_mask<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.body_box, s.pair_mask);
-  k_row_counts<<<blocks(n, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr);
-  k_scan_excl<<<1, 1024, 0, s.stream>>>(s.row_ptr, n, s.row_ptr + n);
-  k_scan_excl<<<1, 1024, 0, s.stream>>>(s.upper_ptr, n, s.upper_ptr + n);
-  k_fill_adj<<<blocks(n, 128), 128, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj,
-                                                   s.ij, s.adj_col, s.adj_pair);
-  s.launches += 5;
+  if (n <= kSmallPairs) {
+    const size_t smem = sizeof(float) * 6 * (size_t)n + sizeof(int) * 2 * (size_t)n;
+    cudaError_t e = cudaFuncSetAttribute(k_body_pairs_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(float) * 6 * kSmallPairs + sizeof(int) * 2 * kSmallPairs));
+    if (e != cudaSuccess) return e;
+    k_body_pairs_small<<<1, PT, smem, s.stream>>>(n, s.body_box, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj, s.ij,
+                                                  s.adj_col, s.adj_pair);
+    ++s.launches;
+  } else {
+    k_pair_mask<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.body_box, s.pair_mask);
+    k_row_counts<<<blocks(n, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr);
+    k_scan_excl<<<1, 1024, 0, s.stream>>>(s.row_ptr, n, s.row_ptr + n);
+    k_scan_excl<<<1, 1024, 0, s.stream>>>(s.upper_ptr, n, s.upper_ptr + n);
+    k_fill_adj<<<blocks(n, 128), 128, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr, s.cap_pairs,
+                                                     s.cap_adj, s.ij, s.adj_col, s.adj_pair);
+    s.launches += 5;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   cudaMemcpyAsync(s.hstat + 16, s.upper_ptr + n, sizeof(int), cudaMemcpyDeviceToHost, s.stream);

@@ -9,7 +9,9 @@
 // once and only the boxes are refit per culling pass.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <utility>
+#include <vector>
 
 #include "abd_common.cuh"
 #include "abd_scan.cuh"
@@ -266,7 +268,16 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body, const doub
   TRY(cudaMalloc(&tr.box, sizeof(Box) * nodes));
   TRY(cudaMemsetAsync(tr.body_root, 0xff, sizeof(int) * n, s.stream));
   TRY(cudaMemsetAsync(tr.parent, 0xff, sizeof(int) * nodes, s.stream));
-  if (N == 0) return cudaSuccess;
+  if (N == 0) {
+    std::vector<int> zeros(2 * (size_t)n + 1, 0), bl(n + 1);
+    for (int b = 0; b <= n; ++b) bl[b] = 2 * b;  // every body: an empty schedule [0, 0]
+    TRY(cudaMalloc(&tr.order, sizeof(int)));
+    TRY(cudaMalloc(&tr.lvl, sizeof(int) * zeros.size()));
+    TRY(cudaMalloc(&tr.body_lvl, sizeof(int) * bl.size()));
+    TRY(cudaMemcpy(tr.lvl, zeros.data(), sizeof(int) * zeros.size(), cudaMemcpyHostToDevice));
+    TRY(cudaMemcpy(tr.body_lvl, bl.data(), sizeof(int) * bl.size(), cudaMemcpyHostToDevice));
+    return cudaSuccess;
+  }
   const int* off = (prim_body == s.tbody) ? s.toff : s.eoff;
   float* lohi = nullptr;
   unsigned long long *keys = nullptr, *ktmp = nullptr;
@@ -289,6 +300,64 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body, const doub
   k_body_roots<<<blocks((N > n ? N : n), 256), 256, 0, s.stream>>>(N, n, off, lo_hi, tr.body_root);
   k_inverse_perm<<<blocks(N, 256), 256, 0, s.stream>>>(N, tr.leaf_prim, tr.prim_leaf);
   s.launches += 2;
+  // per-body refit schedule (host, once): node heights, then each body's internal nodes
+  // grouped by height.  Karras node i spans [i, j] or [j, i], so a body's subtree nodes are
+  // exactly the internal nodes whose span lies inside the body's leaf range.
+  {
+    const int M = N - 1;
+    std::vector<int> child(2 * (size_t)(M > 0 ? M : 1)), span(2 * (size_t)(M > 0 ? M : 1)), offh(n + 1);
+    if (M > 0) {
+      TRY(cudaMemcpyAsync(child.data(), tr.child, sizeof(int) * 2 * M, cudaMemcpyDeviceToHost, s.stream));
+      TRY(cudaMemcpyAsync(span.data(), lo_hi, sizeof(int) * 2 * M, cudaMemcpyDeviceToHost, s.stream));
+    }
+    TRY(cudaMemcpyAsync(offh.data(), off, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s.stream));
+    TRY(cudaStreamSynchronize(s.stream));
+    std::vector<int> byspan(M), height(M, 0), owner(M, -1);
+    for (int i = 0; i < M; ++i) byspan[i] = i;
+    std::sort(byspan.begin(), byspan.end(), [&](int a, int b) {
+      return span[2 * a + 1] - span[2 * a] < span[2 * b + 1] - span[2 * b];
+    });
+    for (int i : byspan) {
+      int h = 0;
+      for (int c = 0; c < 2; ++c) {
+        const int ch = child[2 * i + c];
+        if (ch < M) h = std::max(h, height[ch]);
+      }
+      height[i] = h + 1;
+      const int lo = span[2 * i], hi = span[2 * i + 1];
+      const int b = int(std::upper_bound(offh.begin(), offh.end(), lo) - offh.begin()) - 1;
+      if (b >= 0 && b < n && hi < offh[b + 1]) owner[i] = b;
+    }
+    std::vector<int> order, lvl, body_lvl(n + 1, 0);
+    std::vector<std::vector<int>> per(n);
+    for (int i = 0; i < M; ++i)
+      if (owner[i] >= 0) per[owner[i]].push_back(i);
+    for (int b = 0; b < n; ++b) {
+      std::vector<int>& v = per[b];
+      std::stable_sort(v.begin(), v.end(), [&](int a, int c) { return height[a] < height[c]; });
+      body_lvl[b] = (int)lvl.size();
+      lvl.push_back((int)order.size());
+      int h = 1;
+      for (size_t k = 0; k < v.size(); ++k) {
+        while (height[v[k]] > h) {
+          lvl.push_back((int)order.size());
+          ++h;
+        }
+        order.push_back(v[k]);
+      }
+      lvl.push_back((int)order.size());
+    }
+    body_lvl[n] = (int)lvl.size();
+    TRY(cudaMalloc(&tr.order, sizeof(int) * std::max<size_t>(1, order.size())));
+    TRY(cudaMalloc(&tr.lvl, sizeof(int) * lvl.size()));
+    TRY(cudaMalloc(&tr.body_lvl, sizeof(int) * body_lvl.size()));
+    if (!order.empty())
+      TRY(cudaMemcpyAsync(tr.order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, s.stream));
+    TRY(cudaMemcpyAsync(tr.lvl, lvl.data(), sizeof(int) * lvl.size(), cudaMemcpyHostToDevice, s.stream));
+    TRY(cudaMemcpyAsync(tr.body_lvl, body_lvl.data(), sizeof(int) * body_lvl.size(), cudaMemcpyHostToDevice,
+                        s.stream));
+    TRY(cudaStreamSynchronize(s.stream));
+  }
   cudaFreeAsync(lohi, s.stream);
   cudaFreeAsync(keys, s.stream);
   cudaFreeAsync(ktmp, s.stream);

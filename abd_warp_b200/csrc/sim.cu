@@ -47,7 +47,7 @@ cudaError_t upload(T** p, const T* host, size_t count, cudaStream_t st) {
 
 void free_tree(abd::Tree& t) {
   for (void* q : {(void*)t.child, (void*)t.parent, (void*)t.leaf_prim, (void*)t.prim_leaf, (void*)t.body_root,
-                  (void*)t.flags, (void*)t.box})
+                  (void*)t.flags, (void*)t.box, (void*)t.order, (void*)t.lvl, (void*)t.body_lvl})
     if (q) cudaFree(q);
   t = abd::Tree{};
 }
@@ -84,10 +84,12 @@ int grow_lists(Sim& s, int need_pt, int need_ee) {
 
 // Boxes, body pairs and the narrow pass of `mode` on positions y0 (static) or y0 -> y1
 // (swept).  Grows the capacities and reruns as needed.
-int culling(abd_sim* h, const double* y0, const double* y1, int mode) {
+// A != null: y0 (and y1 when A1 != null) are computed from the DOFs inside the broad-phase
+// kernel; otherwise y0 / y1 are given positions.
+int culling(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* y0,
+            double* y1, int mode) {
   Sim& s = h->s;
-  CK(abd::prim_boxes(s, y0, y1));
-  CK(abd::body_boxes(s, y0, y1));
+  CK(abd::body_broad(s, A, p, A1, p1, y0, y1));
   for (int tries = 0;; ++tries) {
     bool ovf = false;
     CK(abd::body_pairs(s, &ovf));
@@ -125,20 +127,20 @@ int read_scalar(Sim& s, const double* dev, double* out) {
 // E(Ak, pk): barrier over the culling lists at xk + inertia (compute_energy, abd.py:133-141)
 int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* pk, double* E) {
   Sim& s = h->s;
-  CK(abd::transform(s, Ak, pk, s.xk));
-  int r = culling(h, s.xk, nullptr, abd::NARROW_ENERGY);
+  int r = culling(h, Ak, pk, nullptr, nullptr, s.xk, nullptr, abd::NARROW_ENERGY);
   if (r) return r;
   CK(abd::body_energy(s, st, Ak, pk, s.xk));
   CK(abd::sum_energy(s, s.scal + 8));
   return read_scalar(s, s.scal + 8, E);
 }
 
-// CCD bound between positions x (at A, p) and xk (at A1, p1) (ccd, abd.py:278-303)
-int ccd_at(abd_sim* h, const double* x, const double* xk, double* alpha, double* raw) {
+// CCD bound between DOFs (A, p) and (A1, p1) (ccd, abd.py:278-303); positions land in x, xk
+int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
+           double* raw) {
   Sim& s = h->s;
-  int r = culling(h, x, xk, abd::NARROW_CCD);
+  int r = culling(h, A, p, A1, p1, s.x, s.xk, abd::NARROW_CCD);
   if (r) return r;
-  CK(abd::body_vg_toi(s, x, xk));
+  CK(abd::body_vg_toi(s, s.x, s.xk));
   CK(abd::min_toi(s, s.scal + 9));
   double toi;
   r = read_scalar(s, s.scal + 9, &toi);
@@ -152,8 +154,7 @@ int ccd_at(abd_sim* h, const double* x, const double* xk, double* alpha, double*
 
 int gh_at(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active) {
   Sim& s = h->s;
-  CK(abd::transform(s, A, p, s.x));
-  int r = culling(h, s.x, nullptr, abd::NARROW_GH);
+  int r = culling(h, A, p, nullptr, nullptr, s.x, nullptr, abd::NARROW_GH);
   if (r) return r;
   CK(abd::body_gh(s, st, A, p, s.x));
   if (n_active) *n_active = s.hstat[abd::DS_ACTIVE];  // mirrored by culling after the narrow pass
@@ -378,7 +379,8 @@ int abd_update_mesh_vertex(abd_sim* h, const double* A, const double* p, double*
 int abd_collision_set(abd_sim* h, const double* y0, const double* y1, int counts[4]) {
   if (!h || !y0 || !counts) return ABD_ERR_INVALID;
   Sim& s = h->s;
-  int r = culling(h, y0, y1, abd::NARROW_LISTS);
+  int r = culling(h, nullptr, nullptr, nullptr, nullptr, const_cast<double*>(y0), const_cast<double*>(y1),
+                  abd::NARROW_LISTS);
   if (r) return r;
   for (int tries = 0;; ++tries) {
     CK(cudaMemsetAsync(s.dstat + abd::DS_VG_COUNT, 0, sizeof(int), s.stream));
@@ -441,10 +443,7 @@ int abd_compute_energy(abd_sim* h, const abd_states* st, const double* Ak, const
 int abd_ccd(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
             double* raw) {
   if (!h || !A || !p || !A1 || !p1 || !alpha) return ABD_ERR_INVALID;
-  Sim& s = h->s;
-  CK(abd::transform(s, A, p, s.x));
-  CK(abd::transform(s, A1, p1, s.xk));
-  return ccd_at(h, s.x, s.xk, alpha, raw);
+  return ccd_at(h, A, p, A1, p1, alpha, raw);
 }
 
 int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
@@ -479,9 +478,8 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     inf.linear_iters += lin;
     // CCD bound (abd.py:278-303)
     CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
-    CK(abd::transform(s, st.Ak, st.pk, s.xk));
     double alpha;
-    if ((r = ccd_at(h, s.x, s.xk, &alpha, &inf.toi))) return r;
+    if ((r = ccd_at(h, st.A, st.p, st.Ak, st.pk, &alpha, &inf.toi))) return r;
     // dq.g and g.g (abd.py:148, 265)
     CK(abd::dot_partials(s, s.dq, s.g, 10));
     CK(abd::finish_dot(s, 10, s.scal + 10));
