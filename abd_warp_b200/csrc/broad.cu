@@ -216,6 +216,7 @@ struct BroadArgs {
   const int *tri_leaf, *edge_leaf;
   Box *tri_box, *edge_box;
   const int *tri_child, *edge_child, *tri_order, *edge_order, *tri_lvl, *edge_lvl, *tri_blvl, *edge_blvl;
+  int smem_refit;
 };
 
 __device__ inline void refit_level(const int* child, const int* order, int k0, int k1, Box* box) {
@@ -231,6 +232,46 @@ __device__ inline void refit_level(const int* child, const int* order, int k0, i
     }
     store_box(&box[node], u);
   }
+}
+
+// Refit one body's subtree in shared memory: leaves [s0, s0 + cnt) are loaded from global,
+// internal nodes (global ids in [s0, s0 + cnt)) are combined level by level with local ids,
+// then written back.  Local ids: internal id - s0, leaf cnt + position - s0.
+__device__ inline void refit_smem(const int* child, const int* order, const int* lvl, int l0, int l1, int s0,
+                                  int cnt, int N, Box* box, float* sb) {
+  if (cnt <= 1) return;  // a single leaf is its own root
+  const int L0 = N - 1;
+  for (int k = threadIdx.x; k < cnt; k += BB) {
+    const Box B = load_box_cg(&box[L0 + s0 + k]);
+    float* d = sb + 6 * (size_t)(cnt + k);
+    d[0] = B.lo[0]; d[1] = B.lo[1]; d[2] = B.lo[2];
+    d[3] = B.hi[0]; d[4] = B.hi[1]; d[5] = B.hi[2];
+  }
+  __syncthreads();
+  const int H = l1 - l0 - 1;
+  for (int h = 1; h <= H; ++h) {
+    for (int k = lvl[l0 + h - 1] + (int)threadIdx.x; k < lvl[l0 + h]; k += BB) {
+      const int node = order[k];
+      int c0 = child[2 * node], c1 = child[2 * node + 1];
+      c0 = c0 >= L0 ? cnt + (c0 - L0 - s0) : c0 - s0;
+      c1 = c1 >= L0 ? cnt + (c1 - L0 - s0) : c1 - s0;
+      const float* p = sb + 6 * (size_t)c0;
+      const float* q = sb + 6 * (size_t)c1;
+      float* d = sb + 6 * (size_t)(node - s0);
+      d[0] = fminf(p[0], q[0]); d[1] = fminf(p[1], q[1]); d[2] = fminf(p[2], q[2]);
+      d[3] = fmaxf(p[3], q[3]); d[4] = fmaxf(p[4], q[4]); d[5] = fmaxf(p[5], q[5]);
+    }
+    __syncthreads();
+  }
+  for (int k = lvl[l0] + (int)threadIdx.x; k < lvl[l1 - 1]; k += BB) {
+    const int node = order[k];
+    const float* d = sb + 6 * (size_t)(node - s0);
+    Box B;
+    B.lo[0] = d[0]; B.lo[1] = d[1]; B.lo[2] = d[2];
+    B.hi[0] = d[3]; B.hi[1] = d[4]; B.hi[2] = d[5];
+    store_box(&box[node], B);
+  }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
@@ -350,7 +391,15 @@ __global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
     store_box(&a.tri_box[(a.T - 1) + a.tri_leaf[t]], B);
   }
   __syncthreads();
-  // refit the body's subtrees of both trees, one height level at a time
+  if (a.smem_refit) {
+    extern __shared__ float sbox[];  // [2 * cnt][6]: internal nodes, then leaves (local ids)
+    refit_smem(a.edge_child, a.edge_order, a.edge_lvl, a.edge_blvl[b], a.edge_blvl[b + 1], a.eoff[b],
+               a.eoff[b + 1] - a.eoff[b], a.E, a.edge_box, sbox);
+    refit_smem(a.tri_child, a.tri_order, a.tri_lvl, a.tri_blvl[b], a.tri_blvl[b + 1], a.toff[b],
+               a.toff[b + 1] - a.toff[b], a.T, a.tri_box, sbox);
+    return;
+  }
+  // refit the body's subtrees of both trees in global memory, one height level at a time
   const int te0 = a.tri_blvl[b], te1 = a.tri_blvl[b + 1];
   const int ee0 = a.edge_blvl[b], ee1 = a.edge_blvl[b + 1];
   const int ht = te1 - te0 - 1, he = ee1 - ee0 - 1;
@@ -359,112 +408,6 @@ __global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
     if (h <= ht) refit_level(a.tri_child, a.tri_order, a.tri_lvl[te0 + h - 1], a.tri_lvl[te0 + h], a.tri_box);
     if (h <= he) refit_level(a.edge_child, a.edge_order, a.edge_lvl[ee0 + h - 1], a.edge_lvl[ee0 + h], a.edge_box);
     __syncthreads();
-  }
-}
-
-// Body pairs for n <= kSmallPairs in one CTA: the same outputs as the multi-kernel path
-// (sorted ij list, CSR adjacency in increasing neighbour order, pair index of every entry).
-constexpr int kSmallPairs = 4096;
-constexpr int PT = 1024;
-
-// dynamic shared memory: float bx[n][6], int cnt[n], int up[n]
-__global__ void __launch_bounds__(PT) k_body_pairs_small(int n, const Box* __restrict__ body_box, int* row_ptr,
-                                                          int* upper_ptr, int cap_pairs, int cap_adj, int2* ij,
-                                                          int* adj_col, int* adj_pair) {
-  extern __shared__ float smem_pairs[];
-  float(*bx)[6] = reinterpret_cast<float(*)[6]>(smem_pairs);
-  int* cnt = reinterpret_cast<int*>(smem_pairs + 6 * (size_t)n);
-  int* up = cnt + n;
-  __shared__ int wsum[2][PT / 32];
-  for (int i = threadIdx.x; i < n; i += PT) {
-    const Box B = load_box(&body_box[i]);
-    for (int c = 0; c < 3; ++c) {
-      bx[i][c] = B.lo[c];
-      bx[i][3 + c] = B.hi[c];
-    }
-  }
-  __syncthreads();
-  auto ov = [&](int I, int J) {
-    return !(bx[I][0] > bx[J][3] || bx[J][0] > bx[I][3] || bx[I][1] > bx[J][4] || bx[J][1] > bx[I][4] ||
-             bx[I][2] > bx[J][5] || bx[J][2] > bx[I][5]);
-  };
-  for (int I = threadIdx.x; I < n; I += PT) {
-    int full = 0, upper = 0;
-    for (int J = 0; J < n; ++J)
-      if (J != I && ov(I, J)) {
-        ++full;
-        if (J > I) ++upper;
-      }
-    cnt[I] = full;
-    up[I] = upper;
-  }
-  __syncthreads();
-  // exclusive scans of cnt and up (rows strided over threads: chunked by thread)
-  const int per = (n + PT - 1) / PT;
-  const int r0 = threadIdx.x * per, r1 = min(n, r0 + per);
-  int s0 = 0, s1 = 0;
-  for (int i = r0; i < r1; ++i) {
-    s0 += cnt[i];
-    s1 += up[i];
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x0 = s0, x1 = s1;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
-    if (lane >= o) {
-      x0 += y0;
-      x1 += y1;
-    }
-  }
-  if (lane == 31) {
-    wsum[0][warp] = x0;
-    wsum[1][warp] = x1;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int a0 = 0, a1 = 0;
-    for (int w = 0; w < PT / 32; ++w) {
-      const int c0 = wsum[0][w], c1 = wsum[1][w];
-      wsum[0][w] = a0;
-      wsum[1][w] = a1;
-      a0 += c0;
-      a1 += c1;
-    }
-    row_ptr[n] = a0;
-    upper_ptr[n] = a1;
-  }
-  __syncthreads();
-  int e0 = wsum[0][warp] + x0 - s0, e1 = wsum[1][warp] + x1 - s1;
-  for (int i = r0; i < r1; ++i) {
-    const int c0 = cnt[i], c1 = up[i];
-    cnt[i] = e0;
-    up[i] = e1;
-    row_ptr[i] = e0;
-    upper_ptr[i] = e1;
-    e0 += c0;
-    e1 += c1;
-  }
-  __syncthreads();
-  for (int I = threadIdx.x; I < n; I += PT) {
-    int pos = cnt[I], u = up[I];
-    for (int J = 0; J < n; ++J) {
-      if (J == I || !ov(I, J)) continue;
-      int pr;
-      if (J > I) {
-        pr = u++;
-        if (pr < cap_pairs) ij[pr] = make_int2(I, J);
-      } else {
-        int rank = 0;  // upper neighbours of J below I
-        for (int K = J + 1; K < I; ++K)
-          if (ov(J, K)) ++rank;
-        pr = up[J] + rank;
-      }
-      if (pos < cap_adj) {
-        adj_col[pos] = J;
-        adj_pair[pos] = pr;
-      }
-      ++pos;
-    }
   }
 }
 
@@ -503,7 +446,15 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
   a.edge_lvl = s.edge_tree.lvl;
   a.tri_blvl = s.tri_tree.body_lvl;
   a.edge_blvl = s.edge_tree.body_lvl;
-  k_body_broad<<<s.n, BB, 0, s.stream>>>(a);
+  // shared-memory refit when the largest body subtree fits (2 boxes of 24 B per primitive)
+  const int maxp = s.max_body_t > s.max_body_e ? s.max_body_t : s.max_body_e;
+  const size_t smem = 2 * sizeof(float) * 6 * (size_t)maxp;
+  a.smem_refit = smem <= 200 * 1024;
+  if (a.smem_refit && smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_body_broad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_body_broad<<<s.n, BB, a.smem_refit ? smem : 0, s.stream>>>(a);
   ++s.launches;
   return cudaGetLastError();
 }
@@ -543,23 +494,13 @@ cudaError_t body_boxes(Sim& s, const double* y0, const double* y1) {
 // Synchronises the stream to read the counts; *overflow is set when a capacity is short.
 cudaError_t body_pairs(Sim& s, bool* overflow) {
   const int n = s.n, W = s.W;
-  if (n <= kSmallPairs) {
-    const size_t smem = sizeof(float) * 6 * (size_t)n + sizeof(int) * 2 * (size_t)n;
-    cudaError_t e = cudaFuncSetAttribute(k_body_pairs_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(float) * 6 * kSmallPairs + sizeof(int) * 2 * kSmallPairs));
-    if (e != cudaSuccess) return e;
-    k_body_pairs_small<<<1, PT, smem, s.stream>>>(n, s.body_box, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj, s.ij,
-                                                  s.adj_col, s.adj_pair);
-    ++s.launches;
-  } else {
-    k_pair_mask<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.body_box, s.pair_mask);
-    k_row_counts<<<blocks(n, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr);
-    k_scan_excl<<<1, 1024, 0, s.stream>>>(s.row_ptr, n, s.row_ptr + n);
-    k_scan_excl<<<1, 1024, 0, s.stream>>>(s.upper_ptr, n, s.upper_ptr + n);
-    k_fill_adj<<<blocks(n, 128), 128, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr, s.cap_pairs,
-                                                     s.cap_adj, s.ij, s.adj_col, s.adj_pair);
-    s.launches += 5;
-  }
+  k_pair_mask<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.body_box, s.pair_mask);
+  k_row_counts<<<blocks(n, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr);
+  k_scan_excl<<<1, 1024, 0, s.stream>>>(s.row_ptr, n, s.row_ptr + n);
+  k_scan_excl<<<1, 1024, 0, s.stream>>>(s.upper_ptr, n, s.upper_ptr + n);
+  k_fill_adj<<<blocks(n, 128), 128, 0, s.stream>>>(n, W, s.pair_mask, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj,
+                                                   s.ij, s.adj_col, s.adj_pair);
+  s.launches += 5;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   cudaMemcpyAsync(s.hstat + 16, s.upper_ptr + n, sizeof(int), cudaMemcpyDeviceToHost, s.stream);

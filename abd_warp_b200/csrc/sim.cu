@@ -201,6 +201,12 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
         d->edge_off[b + 1] < d->edge_off[b])
       return ABD_ERR_INVALID;
   std::vector<int> vbody(V), tbody(T), ebody(E);
+  int max_v = 0, max_t = 0, max_e = 0;
+  for (int b = 0; b < n; ++b) {
+    max_v = std::max(max_v, d->vert_off[b + 1] - d->vert_off[b]);
+    max_t = std::max(max_t, d->tri_off[b + 1] - d->tri_off[b]);
+    max_e = std::max(max_e, d->edge_off[b + 1] - d->edge_off[b]);
+  }
   for (int b = 0; b < n; ++b) {
     for (int v = d->vert_off[b]; v < d->vert_off[b + 1]; ++v) vbody[v] = b;
     for (int t = d->tri_off[b]; t < d->tri_off[b + 1]; ++t) {
@@ -227,6 +233,9 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   s.V = V;
   s.T = T;
   s.E = E;
+  s.max_body_v = max_v;
+  s.max_body_t = max_t;
+  s.max_body_e = max_e;
   // rest-space centroids for the Morton keys
   std::vector<double> tc(3 * (size_t)T), ec(3 * (size_t)E);
   for (int t = 0; t < T; ++t)
