@@ -68,6 +68,7 @@ def load():
         "abd_step": ([P, P, P, P], c_int),
         "abd_update_mesh_vertex": ([P, P, P, P], c_int),
         "abd_collision_set": ([P, P, P, P], c_int),
+        "abd_collision_set_dofs": ([P, P, P, P, P, P], c_int),
         "abd_export_lists": ([P, P, P, P, P, c_int], c_int),
         "abd_ipc_gh": ([P, P, P, P, P], c_int),
         "abd_export_system": ([P, P, P, P, P, c_int, P], c_int),
@@ -91,7 +92,7 @@ def exported_symbols():
     load()
     return ["abd_sim_create", "abd_sim_destroy", "abd_sim_set_params", "abd_sim_set_stream", "abd_sim_reset",
             "abd_sim_get_dq", "abd_sim_set_dq", "abd_sim_get_g", "abd_sim_sizes", "abd_step", "abd_update_mesh_vertex",
-            "abd_collision_set", "abd_export_lists", "abd_ipc_gh", "abd_export_system", "abd_solve",
+            "abd_collision_set", "abd_collision_set_dofs", "abd_export_lists", "abd_ipc_gh", "abd_export_system", "abd_solve",
             "abd_compute_energy", "abd_ccd", "abd_take_status", "abd_status_string", "abd_launch_count"]
 
 

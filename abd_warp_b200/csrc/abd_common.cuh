@@ -23,6 +23,7 @@ enum : int {
   ST_SOLVER_NOCONV = 16,   // Krylov solve hit cg_max_iter
   ST_NAN = 32,             // non-finite value in the Newton system
   ST_VG_OVERFLOW = 64,     // VG list capacity exceeded
+  ST_ACT_OVERFLOW = 128,   // active-pair list capacity exceeded (host grows and reruns)
 };
 
 constexpr int kTraversalStack = 64;
@@ -80,6 +81,63 @@ __device__ inline void store_box(Box* p, const Box& b) {
   q[1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
 }
 
+// Leaf boxes with the reference's rounding (culling2.py:32-79, 229-280): edges take the FP64
+// min / max of their end points, dilate by dhat/2 in FP64 and round to FP32; triangles are
+// not dilated.  Swept boxes (y1 != null) add the undilated FP32 box at y1.
+__device__ inline Box edge_leaf_box(const int* __restrict__ edges, const double* __restrict__ y0,
+                                    const double* __restrict__ y1, int e, double dhh) {
+  const int i0 = __ldg(&edges[2 * e]), i1 = __ldg(&edges[2 * e + 1]);
+  Box B;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double u = y0[3 * i0 + k], w = y0[3 * i1 + k];
+    B.lo[k] = (float)(fmin(u, w) - dhh);
+    B.hi[k] = (float)(fmax(u, w) + dhh);
+    if (y1) {
+      const double u1 = y1[3 * i0 + k], w1 = y1[3 * i1 + k];
+      B.lo[k] = fminf(B.lo[k], (float)fmin(u1, w1));
+      B.hi[k] = fmaxf(B.hi[k], (float)fmax(u1, w1));
+    }
+  }
+  B.pad0 = B.pad1 = 0.f;
+  return B;
+}
+__device__ inline Box tri_leaf_box(const int* __restrict__ tris, const double* __restrict__ y0,
+                                   const double* __restrict__ y1, int t) {
+  const int i0 = __ldg(&tris[3 * t]), i1 = __ldg(&tris[3 * t + 1]), i2 = __ldg(&tris[3 * t + 2]);
+  Box B;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double u = y0[3 * i0 + k], w = y0[3 * i1 + k], q = y0[3 * i2 + k];
+    B.lo[k] = (float)(fmin(fmin(u, w), q) - 0.0);
+    B.hi[k] = (float)(fmax(fmax(u, w), q) + 0.0);
+    if (y1) {
+      const double u1 = y1[3 * i0 + k], w1 = y1[3 * i1 + k], q1 = y1[3 * i2 + k];
+      B.lo[k] = fminf(B.lo[k], (float)fmin(fmin(u1, w1), q1));
+      B.hi[k] = fmaxf(B.hi[k], (float)fmax(fmax(u1, w1), q1));
+    }
+  }
+  B.pad0 = B.pad1 = 0.f;
+  return B;
+}
+// Point boxes: the FP32 position dilated by FP32 dhat (culling2.py:32-45); swept adds y1.
+__device__ inline Box point_box(const double* y0, const double* y1, int v, float dhf) {
+  Box B;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float c = (float)y0[3 * v + k];
+    B.lo[k] = c - dhf;
+    B.hi[k] = c + dhf;
+    if (y1) {
+      const float c1 = (float)y1[3 * v + k];
+      B.lo[k] = fminf(B.lo[k], c1);
+      B.hi[k] = fmaxf(B.hi[k], c1);
+    }
+  }
+  B.pad0 = B.pad1 = 0.f;
+  return B;
+}
+
 // order-preserving encoding of a non-negative double for atomicMin on 64-bit integers
 __device__ inline unsigned long long dkey(double v) { return (unsigned long long)__double_as_longlong(v); }
 
@@ -94,8 +152,11 @@ struct Tree {
   int* leaf_prim = nullptr;   // [N] sorted position -> primitive index
   int* prim_leaf = nullptr;   // [N] primitive index -> sorted position
   int* body_root = nullptr;   // [n] node id of the body's subtree, -1 if the body has none
-  int* flags = nullptr;       // [N-1] refit arrival counters
-  Box* box = nullptr;         // [2N-1]
+  Box* box = nullptr;         // [2N-1] world boxes: internal nodes (refit), then leaves
+  // [N-1] internal node boxes in the body's rest frame (the refit of the rest positions);
+  // when the positions are x = A^T r + p, a node's world box is bounded by the affine image
+  // of its rest box, which the traversal computes from the body's DOFs instead of a refit
+  Box* rest = nullptr;
   // per-body bottom-up refit schedule: the internal nodes of body b's subtree grouped by
   // height, order[lvl[body_lvl[b] + h - 1] .. lvl[body_lvl[b] + h]) for h = 1..heights
   int* order = nullptr;       // [N-1]
@@ -129,11 +190,23 @@ struct Sim {
   // body pairs
   int W = 0;                       // mask words per row
   uint32_t* pair_mask = nullptr;   // [n][W]
+  int* pair_wpre = nullptr;        // [n][W] popcounts, then per-row exclusive prefix
   int *row_ptr = nullptr, *upper_ptr = nullptr;  // [n+1]
   int cap_pairs = 0, cap_adj = 0;
   int2* ij = nullptr;              // [cap_pairs]
   int *adj_col = nullptr, *adj_pair = nullptr;   // [cap_adj]
-  int n_pairs = 0, n_adj = 0;      // host copies after a culling pass
+  int n_pairs = 0, n_adj = 0;      // host copies, valid after a read of dstat
+  // active pairs (contacts, both bodies free) with their coupling weight, for the
+  // preconditioner's clustering on the host: int4 (pair, I, J, weight bits)
+  int cap_act = 0;
+  int4* act_pairs = nullptr;       // device [cap_act]
+  int4* hact = nullptr;            // pinned [cap_act]
+
+  // per-body work chunks of the energy / CCD narrow passes: (body, first item) with items
+  // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
+  int nch = 0;
+  int2* chunk = nullptr;           // [nch]
+  double* chunk_val = nullptr;     // [nch] energy sum or minimum time of impact
 
   // candidate lists
   int cap_pt = 0, cap_ee = 0, cap_vg = 0;
@@ -160,17 +233,19 @@ struct Sim {
   long long* cl_off = nullptr;                   // [ncl+1] offsets into cl_inv (doubles)
   double* cl_inv = nullptr;                      // dense inverses of the cluster systems
   size_t cap_cl_inv = 0;
-  float* pair_w = nullptr;                       // [cap_pairs] coupling weights
   double* zb = nullptr;                          // [n][12] scratch (M^-1 b)
   double* partials = nullptr;      // reduction partials [kRedSlots][kRedBlocks]
   double* scal = nullptr;          // solver scalars
   int* dstat = nullptr;            // device: [0] status, [1..] counters
   int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
+  void* hstage = nullptr;          // pinned staging of the preconditioner's cluster tables
+  size_t cap_hstage = 0;
   double* hval = nullptr;          // pinned host scalars
   unsigned long long* dmin = nullptr;  // device min accumulators
 };
 
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
+constexpr int kChunk = 128;       // items per chunk of the energy / CCD narrow passes
 constexpr int kRedSlots = 12;
 
 // dstat layout
@@ -182,6 +257,9 @@ enum : int {
   DS_ACTIVE = 4,
   DS_SOLVER_DONE = 5,
   DS_SOLVER_ITERS = 6,
+  DS_NPAIRS = 7,     // body pairs of the last culling pass
+  DS_NADJ = 8,       // adjacency entries (2 x pairs)
+  DS_NACTP = 9,      // active pairs appended by pair_weights
   DS_NSLOTS = 16
 };
 
@@ -193,26 +271,32 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body_dev, const 
                        const int* prim_off_host);
 cudaError_t radix_sort_pairs(Sim& s, unsigned long long* keys, int* vals, unsigned long long* keys_tmp,
                              int* vals_tmp, int N, int key_bits);
-cudaError_t refit(Sim& s, Tree& tr);
 
 // broad.cu
 cudaError_t transform(Sim& s, const double* A, const double* p, double* x);
-cudaError_t prim_boxes(Sim& s, const double* y0, const double* y1);
-cudaError_t body_boxes(Sim& s, const double* y0, const double* y1);
-cudaError_t body_pairs(Sim& s, bool* overflow);
-// fused per-body broad phase: optional transform (A != null: y0 = x(A, p); A1 != null:
-// y1 = x(A1, p1)), body boxes, leaf boxes and the subtree refits of both trees
+cudaError_t body_pairs(Sim& s);
+// fused per-body broad phase: body boxes (static, or swept when y1 != null) and leaf boxes.
+// A != null: y0 = x(A, p) (and y1 = x(A1, p1) when A1 != null) are computed here and the
+// traversal bounds internal nodes by the affine images of their rest boxes; A == null: y0 /
+// y1 are given positions and the body subtrees are refit level by level.
 cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A1, const double* p1, double* y0,
                        double* y1);
+// rest-frame internal node boxes of both trees (once, at creation)
+cudaError_t rest_boxes(Sim& s);
 
 // narrow.cu
 enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS = 3 };
-cudaError_t narrow(Sim& s, int mode, const double* y0, const double* y1);
+// A != null: internal node boxes are the affine images of the rest boxes under (A, p) (united
+// with (A1, p1) when swept); A == null: the refit boxes.  y0 / y1 are the positions.
+cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
+                   const double* y0, const double* y1);
 cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y);
 cudaError_t body_energy(Sim& s, const abd_states& st, const double* Ak, const double* pk, const double* y);
 cudaError_t body_vg_toi(Sim& s, const double* y0, const double* y1);
 cudaError_t vg_list(Sim& s, const double* y0);
 cudaError_t sum_energy(Sim& s, double* out_dev);
+// active pairs with their coupling weights (device list + count in dstat DS_NACTP)
+cudaError_t pair_weights(Sim& s);
 cudaError_t min_toi(Sim& s, double* out_dev);
 cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,

@@ -6,7 +6,8 @@
 // Sorting by body first makes every body's primitives a contiguous key range, and in a
 // binary radix tree the keys sharing the body prefix form one subtree: body_root[b].
 // Affine motion keeps the rest-space hierarchy spatially coherent, so the topology is built
-// once and only the boxes are refit per culling pass.
+// once.  The rest-frame boxes of the internal nodes are computed once as well (rest_boxes,
+// broad.cu); under motion by DOFs a node's world box is bounded by their affine image.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -197,26 +198,6 @@ __global__ void k_inverse_perm(int N, const int* leaf_prim, int* prim_leaf) {
   if (i < N) prim_leaf[leaf_prim[i]] = i;
 }
 
-__global__ void k_refit(int N, const int* child, const int* parent, int* flags, Box* box) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= N) return;
-  int cur = parent[N - 1 + k];
-  // at most N-1 ancestors; the bound guarantees termination
-  for (int guard = 0; cur >= 0 && guard < N; ++guard) {
-    __threadfence();
-    if (atomicAdd(&flags[cur], 1) == 0) return;
-    const Box a = load_box_cg(&box[child[2 * cur]]);
-    const Box b = load_box_cg(&box[child[2 * cur + 1]]);
-    Box u;
-    for (int c = 0; c < 3; ++c) {
-      u.lo[c] = fminf(a.lo[c], b.lo[c]);
-      u.hi[c] = fmaxf(a.hi[c], b.hi[c]);
-    }
-    store_box(&box[cur], u);
-    cur = parent[cur];
-  }
-}
-
 inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -264,7 +245,7 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body, const doub
   TRY(cudaMalloc(&tr.leaf_prim, sizeof(int) * (size_t)(N > 0 ? N : 1)));
   TRY(cudaMalloc(&tr.prim_leaf, sizeof(int) * (size_t)(N > 0 ? N : 1)));
   TRY(cudaMalloc(&tr.body_root, sizeof(int) * (size_t)n));
-  TRY(cudaMalloc(&tr.flags, sizeof(int) * (size_t)(N > 1 ? N - 1 : 1)));
+  TRY(cudaMalloc(&tr.rest, sizeof(Box) * (size_t)(N > 1 ? N - 1 : 1)));
   TRY(cudaMalloc(&tr.box, sizeof(Box) * nodes));
   TRY(cudaMemsetAsync(tr.body_root, 0xff, sizeof(int) * n, s.stream));
   TRY(cudaMemsetAsync(tr.parent, 0xff, sizeof(int) * nodes, s.stream));
@@ -364,15 +345,6 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body, const doub
   cudaFreeAsync(vtmp, s.stream);
   cudaFreeAsync(lo_hi, s.stream);
 #undef TRY
-  return cudaGetLastError();
-}
-
-cudaError_t refit(Sim& s, Tree& tr) {
-  if (tr.N <= 1) return cudaSuccess;
-  cudaError_t e = cudaMemsetAsync(tr.flags, 0, sizeof(int) * (tr.N - 1), s.stream);
-  if (e != cudaSuccess) return e;
-  k_refit<<<blocks(tr.N, 256), 256, 0, s.stream>>>(tr.N, tr.child, tr.parent, tr.flags, tr.box);
-  ++s.launches;
   return cudaGetLastError();
 }
 

@@ -36,10 +36,16 @@ inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t);
 struct NarrowArgs {
   int mode;
   abd_params prm;
-  int n_pairs;
+  int n, cap_adj;
   const int2* ij;
+  const int *row_ptr, *adj_col;
+  const Box* body_box;
+  const int2* chunk;
+  double* chunk_val;
   const int *voff, *toff, *eoff, *tris, *edges;
   const double *y0, *y1, *x0;
+  const double *A, *p, *A1, *p1;  // DOFs of y0 / y1 (affine node boxes), or null
+  int affine;
   Tree tri, edge;
   int *pt_list, *ee_list;
   int cap_pt, cap_ee;
@@ -49,33 +55,79 @@ struct NarrowArgs {
   int* pair_active;
 };
 
-__device__ inline Box point_box(const double* y0, const double* y1, int v, float dhf) {
-  Box B;
+// Conservative world box of an internal node of a body moving by x = A^T r + p, from its
+// rest-frame box R: centre and half extents map to p + A^T c and |A|^T h.  Computed in
+// FP32 from FP32 copies m = (A row-major, p) of the DOFs; every rounding error of that
+// (operand conversion, the products and sums, the rest box's own rounding) stays below
+// 2^-21 (|p_j| + sum_k |A_kj| max(|R.lo_k|, |R.hi_k|)), so a margin of 2^-16 of that plus the
+// leaf dilation `pad` (rounded up) keeps every leaf box of the subtree inside the result.
+__device__ inline Box affine_box(const Box& R, const float* m, float pad) {
+  float c[3], h[3], e[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const float c = (float)y0[3 * v + k];
-    B.lo[k] = c - dhf;
-    B.hi[k] = c + dhf;
-    if (y1) {
-      const float c1 = (float)y1[3 * v + k];
-      B.lo[k] = fminf(B.lo[k], c1);
-      B.hi[k] = fmaxf(B.hi[k], c1);
-    }
+    c[k] = 0.5f * (R.lo[k] + R.hi[k]);
+    h[k] = 0.5f * (R.hi[k] - R.lo[k]);
+    e[k] = fmaxf(fabsf(R.lo[k]), fabsf(R.hi[k]));
   }
+  Box B;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const float a0 = m[j], a1 = m[3 + j], a2 = m[6 + j];
+    const float cw = __fmaf_rn(a2, c[2], __fmaf_rn(a1, c[1], __fmaf_rn(a0, c[0], m[9 + j])));
+    const float hw = __fmaf_rn(fabsf(a2), h[2], __fmaf_rn(fabsf(a1), h[1], fabsf(a0) * h[0]));
+    const float sc = __fmaf_rn(fabsf(a2), e[2], __fmaf_rn(fabsf(a1), e[1], __fmaf_rn(fabsf(a0), e[0], fabsf(m[9 + j]))));
+    const float w = hw + __fmaf_rn(sc, 0x1p-16f, pad);
+    B.lo[j] = cw - w;
+    B.hi[j] = cw + w;
+  }
+  B.pad0 = B.pad1 = 0.f;
   return B;
 }
+
+// Per-CTA view of one body's subtree boxes.  Refit mode (m0 == null): the stored boxes.
+// Affine mode: internal nodes are the affine images of their rest boxes under the body's
+// DOFs at y0 (m0) and, when swept, y1 (m1); leaves are computed from the positions.
+struct NodeBoxes {
+  const Tree* tr;
+  const float *m0, *m1;
+  float pad;
+  const int* prims;   // tris or edges
+  int tri;            // 1: triangle tree, 0: edge tree
+  const double *y0, *y1;
+  double dhh;
+  __device__ inline Box internal(int node) const {
+    if (!m0) return load_box(&tr->box[node]);
+    const Box R = load_box(&tr->rest[node]);
+    Box B = affine_box(R, m0, pad);
+    if (m1) {
+      const Box B1 = affine_box(R, m1, pad);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        B.lo[k] = fminf(B.lo[k], B1.lo[k]);
+        B.hi[k] = fmaxf(B.hi[k], B1.hi[k]);
+      }
+    }
+    return B;
+  }
+  __device__ inline Box leaf(int node, int prim) const {
+    if (!m0) return load_box(&tr->box[node]);
+    return tri ? tri_leaf_box(prims, y0, y1, prim) : edge_leaf_box(prims, y0, y1, prim, dhh);
+  }
+};
 
 // Stack traversal of the subtree rooted at `root`; calls f(prim) for every leaf whose box
 // overlaps q, in a fixed depth-first order.
 template <class F>
-__device__ inline void traverse(const Tree& tr, int root, const Box& q, int* dstat, F&& f) {
+__device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int* dstat, F&& f) {
   if (root < 0) return;
+  const Tree& tr = *nb.tr;
   const int L0 = tr.N - 1;
   if (root >= L0) {
-    if (overlap(load_box(&tr.box[root]), q)) f(__ldg(&tr.leaf_prim[root - L0]));
+    const int prim = __ldg(&tr.leaf_prim[root - L0]);
+    if (overlap(nb.leaf(root, prim), q)) f(prim);
     return;
   }
-  if (!overlap(load_box(&tr.box[root]), q)) return;
+  if (!overlap(nb.internal(root), q)) return;
   int stack[kTraversalStack];
   int sp = 0;
   stack[sp++] = root;
@@ -85,13 +137,12 @@ __device__ inline void traverse(const Tree& tr, int root, const Box& q, int* dst
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int c = h ? c1 : c0;
-      if (!overlap(load_box(&tr.box[c]), q)) continue;
       if (c >= L0) {
-        f(__ldg(&tr.leaf_prim[c - L0]));
-      } else if (sp < kTraversalStack) {
-        stack[sp++] = c;
-      } else {
-        atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
+        const int prim = __ldg(&tr.leaf_prim[c - L0]);
+        if (overlap(nb.leaf(c, prim), q)) f(prim);
+      } else if (overlap(nb.internal(c), q)) {
+        if (sp < kTraversalStack) stack[sp++] = c;
+        else atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
       }
     }
   }
@@ -99,6 +150,7 @@ __device__ inline void traverse(const Tree& tr, int root, const Box& q, int* dst
 
 struct PairInfo {
   int I, J, nPT1, nPT2, nEE;
+  const float* dof;  // shared [2 bodies][2 times][12] FP32 DOFs (I, J), or null
 };
 
 __device__ inline PairInfo pair_info(const NarrowArgs& a, int p) {
@@ -109,7 +161,23 @@ __device__ inline PairInfo pair_info(const NarrowArgs& a, int p) {
   P.nPT1 = a.prm.enable_pt ? a.voff[P.I + 1] - a.voff[P.I] : 0;
   P.nPT2 = a.prm.enable_pt ? a.voff[P.J + 1] - a.voff[P.J] : 0;
   P.nEE = a.prm.enable_ee ? a.eoff[P.I + 1] - a.eoff[P.I] : 0;
+  P.dof = nullptr;
   return P;
+}
+
+// tree boxes of one body: m = its FP32 DOFs [y0: 12][y1: 12] in shared memory, or null
+__device__ inline NodeBoxes node_boxes(const NarrowArgs& a, const Tree* tr, bool tri, const float* m) {
+  NodeBoxes nb;
+  nb.tr = tr;
+  nb.m0 = m;
+  nb.m1 = m && a.y1 ? m + 12 : nullptr;
+  nb.pad = __double2float_ru(0.5 * a.prm.dhat);
+  nb.prims = tri ? a.tris : a.edges;
+  nb.tri = tri;
+  nb.y0 = a.y0;
+  nb.y1 = a.y1;
+  nb.dhh = 0.5 * a.prm.dhat;
+  return nb;
 }
 
 // Visit every candidate of item k: f(type, pointOrEdgeBody, primA_global, primB_global)
@@ -121,11 +189,14 @@ __device__ inline void visit_item(const NarrowArgs& a, const PairInfo& P, int k,
     const int body = first ? P.I : P.J, other = first ? P.J : P.I;
     const int v = a.voff[body] + (first ? k : k - P.nPT1);
     const Box q = point_box(a.y0, a.y1, v, dhf);
-    traverse(a.tri, __ldg(&a.tri.body_root[other]), q, a.dstat, [&](int t) { f(0, first ? 0 : 1, v, t); });
+    traverse(node_boxes(a, &a.tri, true, P.dof ? P.dof + 24 * (first ? 1 : 0) : nullptr),
+             __ldg(&a.tri.body_root[other]), q, a.dstat, [&](int t) { f(0, first ? 0 : 1, v, t); });
   } else {
     const int e = a.eoff[P.I] + (k - P.nPT1 - P.nPT2);
-    const Box q = load_box(&a.edge.box[(a.edge.N - 1) + __ldg(&a.edge.prim_leaf[e])]);
-    traverse(a.edge, __ldg(&a.edge.body_root[P.J]), q, a.dstat, [&](int eb) { f(1, 0, e, eb); });
+    const Box q = P.dof ? edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat)
+                        : load_box(&a.edge.box[(a.edge.N - 1) + __ldg(&a.edge.prim_leaf[e])]);
+    traverse(node_boxes(a, &a.edge, false, P.dof ? P.dof + 24 : nullptr), __ldg(&a.edge.body_root[P.J]), q,
+             a.dstat, [&](int eb) { f(1, 0, e, eb); });
   }
 }
 
@@ -176,42 +247,29 @@ __device__ inline int block_scan(int v, int* sh, int& excl) {
   return total;
 }
 
+// One CTA per body pair (grid = pair capacity): candidate lists, and for GH the pair's
+// contact assembly.  MODE is a template parameter so that the list pass is not held to the
+// register budget of the assembly.
+template <int MODE>
 __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
   const int p = blockIdx.x;
-  if (p >= a.n_pairs) return;
-  const PairInfo P = pair_info(a, p);
+  // pair count of this pass (device); an overflowed pass is rerun by the host
+  if (p >= a.dstat[DS_NPAIRS] || (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW)) return;
+  PairInfo P = pair_info(a, p);
   const int items = P.nPT1 + P.nPT2 + P.nEE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ int sh[NW + 1];
-  __shared__ double shd[NT];
-
-  if (a.mode == NARROW_ENERGY || a.mode == NARROW_CCD) {
-    const bool ccd = a.mode == NARROW_CCD;
-    double acc = ccd ? 1.0 : 0.0;
-    for (int k = tid; k < items; k += NT) {
-      visit_item(a, P, k, [&](int type, int, int pa, int pb) {
-        int ids[4];
-        cand_vertices(a, type, pa, pb, ids);
-        d3 xs[4];
-        fetch(a.y0, ids, xs);
-        if (ccd) {
-          d3 x1[4];
-          fetch(a.y1, ids, x1);
-          const double t = collision_time(type, xs, x1);
-          if (t < 1.0) acc = fmin(acc, t);
-        } else {
-          acc += contact_energy(type, xs, a.prm);
-        }
-      });
+  __shared__ float sdof[2][2][12];  // [I, J][y0, y1][A row-major, p]
+  if (a.affine) {
+    if (tid < 48) {
+      const int side = tid / 24, t = (tid / 12) & 1, c = tid % 12;
+      const int b = side ? P.J : P.I;
+      const double* A = t ? a.A1 : a.A;
+      const double* q = t ? a.p1 : a.p;
+      if (!t || a.y1) sdof[side][t][c] = (float)(c < 9 ? A[9 * b + c] : q[3 * b + c - 9]);
     }
-    shd[tid] = acc;
     __syncthreads();
-    for (int s = NT / 2; s > 0; s >>= 1) {
-      if (tid < s) shd[tid] = ccd ? fmin(shd[tid], shd[tid + s]) : shd[tid] + shd[tid + s];
-      __syncthreads();
-    }
-    if (tid == 0) a.pair_val[p] = shd[0];
-    return;
+    P.dof = &sdof[0][0][0];
   }
 
   // ---- LISTS / GH: two passes over the candidates (count, then write in order) ----
@@ -244,7 +302,7 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
   }
   __syncthreads();
   if (!ok) {
-    if (tid == 0 && a.mode == NARROW_GH) a.pair_active[p] = 0;
+    if (tid == 0 && MODE == NARROW_GH) a.pair_active[p] = 0;
     return;
   }
   {
@@ -261,7 +319,7 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
         row[4] = type == 0 ? pb - a.toff[bJ] : pb - a.eoff[bJ];
       });
   }
-  if (a.mode != NARROW_GH) return;
+  if constexpr (MODE != NARROW_GH) return;
   __syncthreads();  // the pair's list segment, written by this CTA, is now visible to it
 
   // ---- GH: contacts of the segment, in candidate order ----
@@ -374,6 +432,116 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
       a.pgrad[(size_t)p * 24 + (e - 432)] = v;
     }
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// energy / CCD passes: one CTA per chunk of one body's points and edges
+// ---------------------------------------------------------------------------------------
+constexpr int CT = kChunk;  // threads per chunk CTA
+constexpr int NBB = 64;     // neighbours staged per batch
+
+// Which body of a pair {I, J} queries the other's edge tree for the EE candidates: the one
+// with more edges (ties: the higher index), so that a body with few edges and many
+// neighbours (a ground box) does not serialise them.  The candidate set does not depend on
+// the choice (the box predicate is symmetric).
+__device__ inline bool ee_owner(int I, int nEI, int J, int nEJ) { return nEI > nEJ || (nEI == nEJ && I > J); }
+
+// Body I's points against the triangle trees of all its neighbours J (PT pairs (I, J); the
+// pairs (J, I) come from J's chunks), and its edges against the edge trees of the neighbours
+// it owns the EE candidates with -- the same candidates as the per-pair kernel, each query
+// box built once.  A query is only traversed into J's tree when it overlaps J's body box,
+// which contains every leaf box of J.  The (query, neighbour) combinations of a batch are
+// spread over the CTA's threads, so a chunk with few queries and many neighbours stays
+// parallel.  ENERGY sums the barrier energies (ipcsk/energy.py:9-48), CCD takes the minimum
+// time of impact (ccd.py:20-40, 133-186); both in a fixed order per chunk.
+template <int MODE>
+__global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
+  constexpr bool ccd = MODE == NARROW_CCD;
+  const int c = blockIdx.x, tid = threadIdx.x;
+  const int2 ch = a.chunk[c];
+  const int I = ch.x;
+  const int nEI = a.eoff[I + 1] - a.eoff[I];
+  const int nV = a.prm.enable_pt ? a.voff[I + 1] - a.voff[I] : 0;
+  const int nE = a.prm.enable_ee ? nEI : 0;
+  const int Q = max(0, min(CT, nV + nE - ch.y));
+  __shared__ Box qbox[CT];
+  __shared__ int qprim[CT];  // point id, or ~edge id
+  __shared__ Box nbox[NBB];
+  __shared__ float ndof[NBB][24];
+  __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB];
+  __shared__ double red[CT];
+  if (tid < Q) {
+    const int k = ch.y + tid;
+    if (k < nV) {
+      const int v = a.voff[I] + k;
+      qprim[tid] = v;
+      qbox[tid] = point_box(a.y0, a.y1, v, (float)a.prm.dhat);
+    } else {
+      const int e = a.eoff[I] + (k - nV);
+      qprim[tid] = ~e;
+      qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
+    }
+  }
+  double acc = ccd ? 1.0 : 0.0;
+  const bool ok = !(a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW);  // an overflowed pass is rerun
+  const int r0 = a.row_ptr[I], r1 = min(a.row_ptr[I + 1], a.cap_adj);
+  for (int b0 = (ok && Q > 0) ? r0 : r1; b0 < r1; b0 += NBB) {
+    const int nb = min(NBB, r1 - b0);
+    __syncthreads();
+    if (tid < nb) {
+      const int J = a.adj_col[b0 + tid];
+      nJ[tid] = J;
+      nbox[tid] = load_box(&a.body_box[J]);
+      ntri[tid] = a.tri.body_root[J];
+      nedge[tid] = a.edge.body_root[J];
+      nown[tid] = ee_owner(I, nEI, J, a.eoff[J + 1] - a.eoff[J]);
+    }
+    for (int e = tid; e < 24 * nb; e += CT) {
+      const int j = e / 24, t = (e / 12) & 1, cc = e % 12;
+      const int J = a.adj_col[b0 + j];
+      const double* A = t ? a.A1 : a.A;
+      const double* pp = t ? a.p1 : a.p;
+      if (!t || a.y1) ndof[j][cc + 12 * t] = (float)(cc < 9 ? A[9 * J + cc] : pp[3 * J + cc - 9]);
+    }
+    __syncthreads();
+    for (int it = tid; it < Q * nb; it += CT) {
+      const int q = it % Q, j = it / Q;
+      const int qp = qprim[q];
+      const bool pt = qp >= 0;
+      if (!pt && !nown[j]) continue;
+      const Box qb = qbox[q];
+      if (!overlap(qb, nbox[j])) continue;
+      auto visit = [&](int type, int pa, int pb) {
+        int ids[4];
+        cand_vertices(a, type, pa, pb, ids);
+        d3 xs[4];
+        fetch(a.y0, ids, xs);
+        if constexpr (ccd) {
+          d3 x1[4];
+          fetch(a.y1, ids, x1);
+          const double t = collision_time(type, xs, x1);
+          if (t < 1.0) acc = fmin(acc, t);
+        } else {
+          acc += contact_energy(type, xs, a.prm);
+        }
+      };
+      if (pt) {
+        traverse(node_boxes(a, &a.tri, true, ndof[j]), ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); });
+      } else {
+        // EE candidates are evaluated with the edge of the lower body first, as the per-pair lists
+        const bool lower = I < nJ[j];
+        traverse(node_boxes(a, &a.edge, false, ndof[j]), nedge[j], qb, a.dstat,
+                 [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); });
+      }
+    }
+  }
+  red[tid] = acc;
+  __syncthreads();
+  for (int st = CT / 2; st > 0; st >>= 1) {
+    if (tid < st) red[tid] = ccd ? fmin(red[tid], red[tid + st]) : red[tid] + red[tid + st];
+    __syncthreads();
+  }
+  if (tid == 0) a.chunk_val[c] = red[0];
 }
 
 // ---------------------------------------------------------------------------------------
@@ -499,8 +667,10 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
       }
       if (vg_on && comp == 1) val += vred[m][0];
     }
-    // contact contributions of the body's pairs, in adjacency (increasing neighbour) order
-    for (int k = a.row_ptr[b]; k < a.row_ptr[b + 1]; ++k) {
+    // contact contributions of the body's pairs, in adjacency (increasing neighbour) order;
+    // skipped when the pair lists of this pass overflowed (the host reruns the pass)
+    const int k1 = (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW) ? a.row_ptr[b] : a.row_ptr[b + 1];
+    for (int k = a.row_ptr[b]; k < k1; ++k) {
       const int pr = a.adj_pair[k];
       if (a.pair_active[pr] <= 0) continue;
       const int side = a.ij[pr].x == b ? 0 : 1;
@@ -603,7 +773,7 @@ __global__ void k_vg_list(BodyArgs a) {
   }
 }
 
-// deterministic single-CTA reduction of pair and body values (sum or min)
+// deterministic single-CTA reduction of chunk and body values (sum or min)
 __global__ void __launch_bounds__(1024) k_reduce_vals(const double* pv, int np, const double* bv, int nb, int is_min,
                                                       double* out) {
   __shared__ double red[1024];
@@ -684,12 +854,24 @@ __global__ void k_finish_dot(const double* part, double* out) {
   if (t == 0) *out = red[0];
 }
 
-NarrowArgs narrow_args(Sim& s, int mode, const double* y0, const double* y1) {
+NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
+                       const double* y0, const double* y1) {
   NarrowArgs a;
+  a.A = A;
+  a.p = p;
+  a.A1 = A1;
+  a.p1 = p1;
+  a.affine = A && p && (!y1 || (A1 && p1));
   a.mode = mode;
   a.prm = s.prm;
-  a.n_pairs = s.n_pairs;
+  a.n = s.n;
+  a.cap_adj = s.cap_adj;
   a.ij = s.ij;
+  a.row_ptr = s.row_ptr;
+  a.adj_col = s.adj_col;
+  a.body_box = s.body_box;
+  a.chunk = s.chunk;
+  a.chunk_val = s.chunk_val;
   a.voff = s.voff;
   a.toff = s.toff;
   a.eoff = s.eoff;
@@ -747,9 +929,19 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
 
 }  // namespace
 
-cudaError_t narrow(Sim& s, int mode, const double* y0, const double* y1) {
-  if (s.n_pairs == 0) return cudaSuccess;
-  k_narrow<<<s.n_pairs, NT, 0, s.stream>>>(narrow_args(s, mode, y0, y1));
+cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
+                   const double* y0, const double* y1) {
+  const NarrowArgs a = narrow_args(s, mode, A, p, A1, p1, y0, y1);
+  if (mode == NARROW_ENERGY || mode == NARROW_CCD) {
+    if (!a.affine) return cudaErrorInvalidValue;  // energy and CCD always run at DOFs
+    if (s.nch == 0) return cudaSuccess;
+    if (mode == NARROW_ENERGY) k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
+    else k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+  } else {
+    if (s.cap_pairs == 0) return cudaSuccess;
+    if (mode == NARROW_GH) k_narrow<NARROW_GH><<<s.cap_pairs, NT, 0, s.stream>>>(a);
+    else k_narrow<NARROW_LISTS><<<s.cap_pairs, NT, 0, s.stream>>>(a);
+  }
   ++s.launches;
   return cudaGetLastError();
 }
@@ -787,13 +979,13 @@ cudaError_t vg_list_swept(Sim& s, const double* y0, const double* y1) {
 }
 
 cudaError_t sum_energy(Sim& s, double* out) {
-  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.pair_val, s.n_pairs, s.body_val, s.n, 0, out);
+  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.chunk_val, s.nch, s.body_val, s.n, 0, out);
   ++s.launches;
   return cudaGetLastError();
 }
 
 cudaError_t min_toi(Sim& s, double* out) {
-  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.pair_val, s.n_pairs, s.body_val, s.n, 1, out);
+  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.chunk_val, s.nch, s.body_val, s.n, 1, out);
   ++s.launches;
   return cudaGetLastError();
 }

@@ -47,7 +47,7 @@ cudaError_t upload(T** p, const T* host, size_t count, cudaStream_t st) {
 
 void free_tree(abd::Tree& t) {
   for (void* q : {(void*)t.child, (void*)t.parent, (void*)t.leaf_prim, (void*)t.prim_leaf, (void*)t.body_root,
-                  (void*)t.flags, (void*)t.box, (void*)t.order, (void*)t.lvl, (void*)t.body_lvl})
+                  (void*)t.rest, (void*)t.box, (void*)t.order, (void*)t.lvl, (void*)t.body_lvl})
     if (q) cudaFree(q);
   t = abd::Tree{};
 }
@@ -56,14 +56,32 @@ int grow_pairs(Sim& s, int need) {
   const int cap = std::max(need + need / 2, 2 * s.cap_pairs);
   const int cap_adj = 2 * cap;
   for (void* q : {(void*)s.ij, (void*)s.adj_col, (void*)s.adj_pair, (void*)s.pair_cand, (void*)s.offdiag,
-                  (void*)s.pdiag, (void*)s.pgrad, (void*)s.pair_active, (void*)s.pair_val, (void*)s.pair_w})
+                  (void*)s.pdiag, (void*)s.pgrad, (void*)s.pair_active, (void*)s.pair_val})
     if (q) cudaFree(q);
   s.cap_pairs = cap;
   s.cap_adj = cap_adj;
   if (dalloc(&s.ij, cap) || dalloc(&s.adj_col, cap_adj) || dalloc(&s.adj_pair, cap_adj) ||
       dalloc(&s.pair_cand, 4 * (size_t)cap) || dalloc(&s.offdiag, 288 * (size_t)cap) ||
       dalloc(&s.pdiag, 288 * (size_t)cap) || dalloc(&s.pgrad, 24 * (size_t)cap) || dalloc(&s.pair_active, cap) ||
-      dalloc(&s.pair_val, cap) || dalloc(&s.pair_w, cap))
+      dalloc(&s.pair_val, cap))
+    return ABD_ERR_OVERFLOW;
+  // zeroed so that the body ids of a pass that overflowed are still valid indices
+  if (cudaMemsetAsync(s.ij, 0, sizeof(int2) * cap, s.stream) ||
+      cudaMemsetAsync(s.adj_col, 0, sizeof(int) * cap_adj, s.stream) ||
+      cudaMemsetAsync(s.adj_pair, 0, sizeof(int) * cap_adj, s.stream))
+    return ABD_ERR_CUDA;
+  return ABD_OK;
+}
+
+int grow_act(Sim& s, int need) {
+  if (need <= s.cap_act) return ABD_OK;
+  if (s.act_pairs) cudaFree(s.act_pairs);
+  if (s.hact) cudaFreeHost(s.hact);
+  s.act_pairs = nullptr;
+  s.hact = nullptr;
+  s.cap_act = std::max(need + need / 2, 2 * s.cap_act);
+  if (dalloc(&s.act_pairs, s.cap_act) ||
+      cudaHostAlloc((void**)&s.hact, sizeof(int4) * s.cap_act, cudaHostAllocDefault) != cudaSuccess)
     return ABD_ERR_OVERFLOW;
   return ABD_OK;
 }
@@ -83,68 +101,99 @@ int grow_lists(Sim& s, int need_pt, int need_ee) {
 }
 
 // Boxes, body pairs and the narrow pass of `mode` on positions y0 (static) or y0 -> y1
-// (swept).  Grows the capacities and reruns as needed.
+// (swept), all asynchronous: counts and overflow bits stay in dstat until the caller's next
+// read (sync_read), after which overflow() grows what was short and asks for a rerun.
 // A != null: y0 (and y1 when A1 != null) are computed from the DOFs inside the broad-phase
 // kernel; otherwise y0 / y1 are given positions.
 int culling(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* y0,
             double* y1, int mode) {
   Sim& s = h->s;
   CK(abd::body_broad(s, A, p, A1, p1, y0, y1));
-  for (int tries = 0;; ++tries) {
-    bool ovf = false;
-    CK(abd::body_pairs(s, &ovf));
-    if (!ovf) break;
-    if (tries > 4) return ABD_ERR_OVERFLOW;
-    int st = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
-    if (st) return st;
-  }
-  const bool lists = mode == abd::NARROW_GH || mode == abd::NARROW_LISTS;
-  for (int tries = 0;; ++tries) {
-    if (lists) CK(cudaMemsetAsync(s.dstat + abd::DS_PT_COUNT, 0, 4 * sizeof(int), s.stream));
-    CK(abd::narrow(s, mode, y0, y1));
-    if (!lists) break;
-    CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-    CK(cudaStreamSynchronize(s.stream));
-    const int bits = s.hstat[abd::DS_STATUS];
-    if (!(bits & (abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW))) break;
-    if (tries > 4) return ABD_ERR_OVERFLOW;
-    int st = grow_lists(s, s.hstat[abd::DS_PT_COUNT], s.hstat[abd::DS_EE_COUNT]);
-    if (st) return st;
-    const int clear = bits & ~(abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW);
-    CK(cudaMemcpyAsync(s.dstat + abd::DS_STATUS, &clear, sizeof(int), cudaMemcpyHostToDevice, s.stream));
-    CK(cudaStreamSynchronize(s.stream));
-  }
+  CK(abd::body_pairs(s));
+  if (mode == abd::NARROW_GH || mode == abd::NARROW_LISTS)  // PT, EE, VG and active counters
+    CK(cudaMemsetAsync(s.dstat + abd::DS_PT_COUNT, 0, 4 * sizeof(int), s.stream));
+  CK(abd::narrow(s, mode, A, p, A1, p1, y0, y1));
   return ABD_OK;
 }
 
-int read_scalar(Sim& s, const double* dev, double* out) {
-  CK(cudaMemcpyAsync(s.hval, dev, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+// One synchronisation: the dstat mirror plus `nd` doubles from `dev` into hval (and, when
+// act is set, the active-pair list into hact).  Updates the host pair counts.
+int sync_read(Sim& s, const double* dev, int nd, bool act = false) {
+  CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+  if (nd > 0) CK(cudaMemcpyAsync(s.hval, dev, nd * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  if (act && s.cap_act > 0)
+    CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
   CK(cudaStreamSynchronize(s.stream));
-  *out = s.hval[0];
+  s.n_pairs = s.hstat[abd::DS_NPAIRS];
+  s.n_adj = s.hstat[abd::DS_NADJ];
   return ABD_OK;
 }
+
+constexpr int kRerun = -1;
+
+// After sync_read: grow every capacity whose overflow bit is set and clear those bits.
+// Returns kRerun when the pass has to be rerun, 0 when it is complete, or an ABD error.
+int overflow(Sim& s) {
+  const int bits = s.hstat[abd::DS_STATUS];
+  const int mask = abd::ST_PAIR_OVERFLOW | abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW | abd::ST_VG_OVERFLOW |
+                   abd::ST_ACT_OVERFLOW;
+  if (!(bits & mask)) return 0;
+  int r = ABD_OK;
+  if (bits & abd::ST_PAIR_OVERFLOW) r = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
+  else if (bits & (abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW))
+    r = grow_lists(s, s.hstat[abd::DS_PT_COUNT], s.hstat[abd::DS_EE_COUNT]);
+  if (!r && (bits & abd::ST_VG_OVERFLOW) && s.hstat[abd::DS_VG_COUNT] > s.cap_vg) {
+    cudaFree(s.vg_list);
+    s.vg_list = nullptr;
+    s.cap_vg = 2 * s.hstat[abd::DS_VG_COUNT];
+    if (dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) r = ABD_ERR_OVERFLOW;
+  }
+  if (!r && (bits & abd::ST_ACT_OVERFLOW)) r = grow_act(s, s.hstat[abd::DS_NACTP]);
+  if (r) return r;
+  const int clear = bits & ~mask;
+  s.hstat[abd::DS_STATUS] = clear;
+  CK(cudaMemcpyAsync(s.dstat + abd::DS_STATUS, &s.hstat[abd::DS_STATUS], sizeof(int), cudaMemcpyHostToDevice,
+                     s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  return kRerun;
+}
+
+constexpr int kMaxReruns = 6;
 
 // E(Ak, pk): barrier over the culling lists at xk + inertia (compute_energy, abd.py:133-141)
 int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* pk, double* E) {
   Sim& s = h->s;
-  int r = culling(h, Ak, pk, nullptr, nullptr, s.xk, nullptr, abd::NARROW_ENERGY);
-  if (r) return r;
-  CK(abd::body_energy(s, st, Ak, pk, s.xk));
-  CK(abd::sum_energy(s, s.scal + 8));
-  return read_scalar(s, s.scal + 8, E);
+  for (int tries = 0;; ++tries) {
+    int r = culling(h, Ak, pk, nullptr, nullptr, s.xk, nullptr, abd::NARROW_ENERGY);
+    if (r) return r;
+    CK(abd::body_energy(s, st, Ak, pk, s.xk));
+    CK(abd::sum_energy(s, s.scal + 8));
+    if ((r = sync_read(s, s.scal + 8, 1))) return r;
+    if ((r = overflow(s)) > 0) return r;
+    if (r == 0) break;
+    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
+  }
+  *E = s.hval[0];
+  return ABD_OK;
 }
 
-// CCD bound between DOFs (A, p) and (A1, p1) (ccd, abd.py:278-303); positions land in x, xk
+// CCD bound between DOFs (A, p) and (A1, p1) (ccd, abd.py:278-303); positions land in x, xk.
+// The scalars scal[10], scal[11] (dq.g, g.g of the step) ride along in the same read into
+// hval[1], hval[2].
 int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
            double* raw) {
   Sim& s = h->s;
-  int r = culling(h, A, p, A1, p1, s.x, s.xk, abd::NARROW_CCD);
-  if (r) return r;
-  CK(abd::body_vg_toi(s, s.x, s.xk));
-  CK(abd::min_toi(s, s.scal + 9));
-  double toi;
-  r = read_scalar(s, s.scal + 9, &toi);
-  if (r) return r;
+  for (int tries = 0;; ++tries) {
+    int r = culling(h, A, p, A1, p1, s.x, s.xk, abd::NARROW_CCD);
+    if (r) return r;
+    CK(abd::body_vg_toi(s, s.x, s.xk));
+    CK(abd::min_toi(s, s.scal + 9));
+    if ((r = sync_read(s, s.scal + 9, 3))) return r;
+    if ((r = overflow(s)) > 0) return r;
+    if (r == 0) break;
+    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
+  }
+  const double toi = s.hval[0];
   if (raw) *raw = toi;
   double t = std::max(0.0, std::min(1.0, toi));
   if (t < 1.0) t *= 0.9;
@@ -152,12 +201,20 @@ int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const
   return ABD_OK;
 }
 
+// Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner
 int gh_at(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active) {
   Sim& s = h->s;
-  int r = culling(h, A, p, nullptr, nullptr, s.x, nullptr, abd::NARROW_GH);
-  if (r) return r;
-  CK(abd::body_gh(s, st, A, p, s.x));
-  if (n_active) *n_active = s.hstat[abd::DS_ACTIVE];  // mirrored by culling after the narrow pass
+  for (int tries = 0;; ++tries) {
+    int r = culling(h, A, p, nullptr, nullptr, s.x, nullptr, abd::NARROW_GH);
+    if (r) return r;
+    CK(abd::body_gh(s, st, A, p, s.x));
+    CK(abd::pair_weights(s));
+    if ((r = sync_read(s, nullptr, 0, true))) return r;
+    if ((r = overflow(s)) > 0) return r;
+    if (r == 0) break;
+    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
+  }
+  if (n_active) *n_active = s.hstat[abd::DS_ACTIVE];
   return ABD_OK;
 }
 
@@ -272,6 +329,19 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.xk, 3 * (size_t)V));
   ok(dalloc(&s.body_box, n));
   ok(dalloc(&s.pair_mask, (size_t)n * s.W));
+  ok(dalloc(&s.pair_wpre, (size_t)n * s.W));
+  {
+    // energy / CCD work chunks: kChunk items (points, then edges) of one body each
+    std::vector<int2> ch;
+    for (int b = 0; b < n; ++b) {
+      const int items = (d->vert_off[b + 1] - d->vert_off[b]) + (d->edge_off[b + 1] - d->edge_off[b]);
+      for (int i = 0; i < items; i += abd::kChunk) ch.push_back(make_int2(b, i));
+    }
+    s.nch = (int)ch.size();
+    ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
+    ok(dalloc(&s.chunk_val, ch.size()));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // ch is a host temporary
+  }
   ok(dalloc(&s.row_ptr, n + 1));
   ok(dalloc(&s.upper_ptr, n + 1));
   ok(dalloc(&s.body_val, n));
@@ -288,6 +358,10 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.dmin, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 8 * sizeof(double), cudaHostAllocDefault);
+  // preconditioner tables: cl_ptr, cl_body, body_cl (ints), cl_off (8-byte aligned long longs)
+  s.cap_hstage = sizeof(int) * (3 * (size_t)n + 2) + sizeof(long long) * ((size_t)n + 2);
+  if (e == cudaSuccess) e = cudaHostAlloc(&s.hstage, s.cap_hstage, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = abd::rest_boxes(s);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat, 0, sizeof(int) * abd::DS_NSLOTS, s.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
@@ -299,6 +373,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   }
   s.cap_pairs = 0;
   int r = grow_pairs(s, std::max(256, 4 * n));
+  if (!r) r = grow_act(s, std::max(1024, n));
   s.cap_pt = 0;
   s.cap_ee = 0;
   if (!r) r = grow_lists(s, std::max(1 << 14, V / 4), std::max(1 << 14, E / 4));
@@ -323,11 +398,12 @@ int abd_sim_destroy(abd_sim* h) {
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
                   s.pair_active, s.pair_val, s.body_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin,
-                  s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_w};
+                  s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
+                  s.chunk_val};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  if (s.hstat) cudaFreeHost(s.hstat);
-  if (s.hval) cudaFreeHost(s.hval);
+  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact})
+    if (q) cudaFreeHost(q);
   delete h;
   return ABD_OK;
 }
@@ -385,28 +461,44 @@ int abd_update_mesh_vertex(abd_sim* h, const double* A, const double* p, double*
   return ABD_OK;
 }
 
-int abd_collision_set(abd_sim* h, const double* y0, const double* y1, int counts[4]) {
-  if (!h || !y0 || !counts) return ABD_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+
+// lists (culling in LISTS mode) plus the VG list; counts = {pairs, PT, EE, VG}
+int cull_lists(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* y0,
+               double* y1, int counts[4]) {
   Sim& s = h->s;
-  int r = culling(h, nullptr, nullptr, nullptr, nullptr, const_cast<double*>(y0), const_cast<double*>(y1),
-                  abd::NARROW_LISTS);
-  if (r) return r;
   for (int tries = 0;; ++tries) {
-    CK(cudaMemsetAsync(s.dstat + abd::DS_VG_COUNT, 0, sizeof(int), s.stream));
+    int r = culling(h, A, p, A1, p1, y0, y1, abd::NARROW_LISTS);
+    if (r) return r;
     CK(y1 ? abd::vg_list_swept(s, y0, y1) : abd::vg_list(s, y0));
-    CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-    CK(cudaStreamSynchronize(s.stream));
-    if (s.hstat[abd::DS_VG_COUNT] <= s.cap_vg) break;
-    if (tries > 2) return ABD_ERR_OVERFLOW;
-    cudaFree(s.vg_list);
-    s.cap_vg = 2 * s.hstat[abd::DS_VG_COUNT];
-    if (dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) return ABD_ERR_OVERFLOW;
+    if ((r = sync_read(s, nullptr, 0))) return r;
+    if ((r = overflow(s)) > 0) return r;
+    if (r == 0) break;
+    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
   }
   counts[0] = s.n_pairs;
   counts[1] = s.hstat[abd::DS_PT_COUNT];
   counts[2] = s.hstat[abd::DS_EE_COUNT];
   counts[3] = s.hstat[abd::DS_VG_COUNT];
   return ABD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int abd_collision_set(abd_sim* h, const double* y0, const double* y1, int counts[4]) {
+  if (!h || !y0 || !counts) return ABD_ERR_INVALID;
+  return cull_lists(h, nullptr, nullptr, nullptr, nullptr, const_cast<double*>(y0), const_cast<double*>(y1), counts);
+}
+
+int abd_collision_set_dofs(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1,
+                           int counts[4]) {
+  if (!h || !A || !p || !counts || (!A1) != (!p1)) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  return cull_lists(h, A, p, A1, p1, s.x, A1 ? s.xk : nullptr, counts);
 }
 
 int abd_export_lists(abd_sim* h, int* ij, int* pt, int* ee, int* vg, int cap) {
@@ -485,18 +577,16 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     if ((r = abd::build_preconditioner(s))) return r;
     if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
     inf.linear_iters += lin;
-    // CCD bound (abd.py:278-303)
-    CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
-    double alpha;
-    if ((r = ccd_at(h, st.A, st.p, st.Ak, st.pk, &alpha, &inf.toi))) return r;
-    // dq.g and g.g (abd.py:148, 265)
+    // dq.g and g.g (abd.py:148, 265), read back together with the CCD bound
     CK(abd::dot_partials(s, s.dq, s.g, 10));
     CK(abd::finish_dot(s, 10, s.scal + 10));
     CK(abd::dot_partials(s, s.g, s.g, 11));
     CK(abd::finish_dot(s, 11, s.scal + 11));
-    CK(cudaMemcpyAsync(s.hval + 2, s.scal + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    CK(cudaStreamSynchronize(s.stream));
-    const double qTg = s.hval[2], gTg = s.hval[3];
+    // CCD bound (abd.py:278-303)
+    CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
+    double alpha;
+    if ((r = ccd_at(h, st.A, st.p, st.Ak, st.pk, &alpha, &inf.toi))) return r;
+    const double qTg = s.hval[1], gTg = s.hval[2];
     // backtracking line search (abd.py:146-160)
     double E1 = E0;
     for (;;) {

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 #include <utility>
 #include <vector>
@@ -430,18 +431,40 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, int it, const doub
   }
 }
 
-__global__ void k_pair_weights(int np, const int2* ij, const int* pair_active, const int* fixed,
-                               const double* offdiag, float* w) {
+// Active pairs of the last GH pass (contacts, both bodies free) with the Frobenius norm of
+// their coupling block, appended to a list in any order (the host sorts it)
+__global__ void k_pair_weights(int cap_pairs, const int* dstat_np, const int2* ij, const int* pair_active,
+                               const int* fixed, const double* offdiag, int cap_act, int4* act, int* dstat) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
-  float out = 0.f;
-  if (pair_active[p] > 0 && !fixed[ij[p].x] && !fixed[ij[p].y]) {
-    double f = 0.0;
-    const double* O = offdiag + (size_t)p * 288;
-    for (int k = 0; k < 144; ++k) f += O[k] * O[k];
-    out = (float)sqrt(f);
+  if (p >= cap_pairs || p >= *dstat_np) return;
+  if (!(pair_active[p] > 0 && !fixed[ij[p].x] && !fixed[ij[p].y])) return;
+  double f = 0.0;
+  const double* O = offdiag + (size_t)p * 288;
+  for (int k = 0; k < 144; ++k) f += O[k] * O[k];
+  const float w = (float)sqrt(f);
+  if (!(w > 0.f)) return;
+  const int pos = atomicAdd(&dstat[DS_NACTP], 1);
+  if (pos < cap_act) act[pos] = make_int4(p, ij[p].x, ij[p].y, __float_as_int(w));
+  else atomicOr(&dstat[DS_STATUS], ST_ACT_OVERFLOW);
+}
+
+// Threshold thr^2 = tol^2 b^T M^-1 b and the recurrence scalars; b = 0 gives x = 0 and ends
+// the solve before its first iteration
+__global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, double* x) {
+  __shared__ double bz;
+  if (threadIdx.x < 32) {
+    const double v = sum_partials(a.part + SL_BZ * kRedBlocks);
+    if (threadIdx.x == 0) bz = v;
   }
-  w[p] = out;
+  __syncthreads();
+  const double b = bz;
+  if (!(b > 0.0))
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < 12 * a.n; i += kRedBlocks * 256) x[i] = 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
+    a.scal[SC_THR2] = tol2 * b;
+    if (!(b > 0.0)) a.dstat[DS_R_DONE] = 1;
+  }
 }
 
 SolverArgs solver_args(Sim& s) {
@@ -468,33 +491,45 @@ SolverArgs solver_args(Sim& s) {
 
 }  // namespace
 
-// Clusters (host union-find on the coupling weights of the last assembled system) and their
-// dense inverses.  Same clustering rule as the oracle: strongest coupling first (float
-// Frobenius norm of H_IJ, ties by pair index), merged while at most cluster_max bodies.
+cudaError_t pair_weights(Sim& s) {
+  cudaError_t e = cudaMemsetAsync(s.dstat + DS_NACTP, 0, sizeof(int), s.stream);
+  if (e != cudaSuccess || s.cap_pairs == 0) return e;
+  k_pair_weights<<<(s.cap_pairs + 255) / 256, 256, 0, s.stream>>>(s.cap_pairs, s.dstat + DS_NPAIRS, s.ij,
+                                                                  s.pair_active, s.fixed, s.offdiag, s.cap_act,
+                                                                  s.act_pairs, s.dstat);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+// Clusters and their dense inverses, from the active-pair list the host read at its last
+// sync (s.hact, count in the dstat mirror).  Same clustering rule as the oracle: greedy
+// union-find, strongest coupling first (FP32 Frobenius norm of H_IJ, ties by pair index), at
+// most cluster_max bodies per cluster.  Tables go up through pinned staging without a sync.
 int build_preconditioner(Sim& s) {
-  const int n = s.n, np = s.n_pairs;
+  const int n = s.n;
   const int cap = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
   std::vector<int> parent(n), size(n, 1);
   std::iota(parent.begin(), parent.end(), 0);
-  if (cap > 1 && np > 0) {
-    k_pair_weights<<<(np + 255) / 256, 256, 0, s.stream>>>(np, s.ij, s.pair_active, s.fixed, s.offdiag, s.pair_w);
-    ++s.launches;
-    std::vector<float> w(np);
-    std::vector<int2> ij(np);
-    if (cudaMemcpyAsync(w.data(), s.pair_w, sizeof(float) * np, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
-        cudaMemcpyAsync(ij.data(), s.ij, sizeof(int2) * np, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
-        cudaStreamSynchronize(s.stream) != cudaSuccess)
-      return ABD_ERR_CUDA;
-    std::vector<int> order;
-    for (int p = 0; p < np; ++p)
-      if (w[p] > 0.f) order.push_back(p);
-    std::sort(order.begin(), order.end(), [&](int x, int y) { return w[x] > w[y] || (w[x] == w[y] && x < y); });
+  const int nact = std::min(s.hstat[DS_NACTP], s.cap_act);
+  if (cap > 1 && nact > 0) {
+    std::vector<int> order(nact);
+    std::iota(order.begin(), order.end(), 0);
+    const int4* L = s.hact;
+    auto weight = [&](int k) {
+      float f;
+      std::memcpy(&f, &L[k].w, sizeof(float));
+      return f;
+    };
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+      const float wx = weight(x), wy = weight(y);
+      return wx > wy || (wx == wy && L[x].x < L[y].x);
+    });
     auto find = [&](int x) {
       while (parent[x] != x) x = parent[x] = parent[parent[x]];
       return x;
     };
-    for (int p : order) {
-      const int a = find(ij[p].x), b = find(ij[p].y);
+    for (int k : order) {
+      const int a = find(L[k].y), b = find(L[k].z);
       if (a == b || size[a] + size[b] > cap) continue;
       if (a < b) {
         parent[b] = a;
@@ -507,32 +542,38 @@ int build_preconditioner(Sim& s) {
     for (int b = 0; b < n; ++b) parent[b] = find(b);
   }
   // clusters ordered by their first body, members in increasing order
-  std::vector<int> first(n, -1), cl_ptr(1, 0), cl_body, body_cl(n);
-  std::vector<std::vector<int>> members;
+  int* cl_ptr = reinterpret_cast<int*>(s.hstage);          // [n+1]
+  int* cl_body = cl_ptr + (n + 1);                          // [n]
+  int* body_cl = cl_body + n;                               // [n]
+  long long* cl_off = reinterpret_cast<long long*>(body_cl + n + ((3 * n + 1) & 1));  // [n+1], 8-aligned
+  std::vector<int> first(n, -1), csize;
   for (int b = 0; b < n; ++b) {
     const int r = parent[b];
     if (first[r] < 0) {
-      first[r] = (int)members.size();
-      members.push_back({});
+      first[r] = (int)csize.size();
+      csize.push_back(0);
     }
-    members[first[r]].push_back(b);
+    ++csize[first[r]];
   }
-  std::vector<long long> cl_off(1, 0);
+  const int ncl = (int)csize.size();
+  cl_ptr[0] = 0;
+  cl_off[0] = 0;
   int max_cl = 1;
-  std::vector<int> big;  // clusters with more than one body
-  for (size_t c = 0; c < members.size(); ++c) {
-    for (int b : members[c]) {
-      cl_body.push_back(b);
-      body_cl[b] = (int)c;
-    }
-    cl_ptr.push_back((int)cl_body.size());
-    const long long d = 12LL * (long long)members[c].size();
-    cl_off.push_back(cl_off.back() + d * d);
-    max_cl = std::max(max_cl, (int)members[c].size());
+  for (int c = 0; c < ncl; ++c) {
+    cl_ptr[c + 1] = cl_ptr[c] + csize[c];
+    const long long d = 12LL * csize[c];
+    cl_off[c + 1] = cl_off[c] + d * d;
+    max_cl = std::max(max_cl, csize[c]);
   }
-  s.ncl = (int)members.size();
+  std::vector<int> fill(ncl, 0);
+  for (int b = 0; b < n; ++b) {
+    const int c = first[parent[b]];
+    cl_body[cl_ptr[c] + fill[c]++] = b;
+    body_cl[b] = c;
+  }
+  s.ncl = ncl;
   s.max_cl = max_cl;
-  const size_t need = (size_t)cl_off.back();
+  const size_t need = (size_t)cl_off[ncl];
   if (need > s.cap_cl_inv) {
     if (s.cl_inv) cudaFree(s.cl_inv);
     s.cap_cl_inv = std::max(need, 2 * s.cap_cl_inv);
@@ -540,11 +581,10 @@ int build_preconditioner(Sim& s) {
   }
   // body -> cluster map rides in the scratch vector zb (as ints) during the setup kernel
   int* body_cl_dev = reinterpret_cast<int*>(s.zb);
-  if (cudaMemcpyAsync(s.cl_ptr, cl_ptr.data(), sizeof(int) * cl_ptr.size(), cudaMemcpyHostToDevice, s.stream) ||
-      cudaMemcpyAsync(s.cl_body, cl_body.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s.stream) ||
-      cudaMemcpyAsync(s.cl_off, cl_off.data(), sizeof(long long) * cl_off.size(), cudaMemcpyHostToDevice,
-                      s.stream) ||
-      cudaMemcpyAsync(body_cl_dev, body_cl.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s.stream))
+  if (cudaMemcpyAsync(s.cl_ptr, cl_ptr, sizeof(int) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
+      cudaMemcpyAsync(s.cl_body, cl_body, sizeof(int) * n, cudaMemcpyHostToDevice, s.stream) ||
+      cudaMemcpyAsync(s.cl_off, cl_off, sizeof(long long) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
+      cudaMemcpyAsync(body_cl_dev, body_cl, sizeof(int) * n, cudaMemcpyHostToDevice, s.stream))
     return ABD_ERR_CUDA;
   SolverArgs a = solver_args(s);
   const size_t smem = sizeof(double) * 144 * (size_t)max_cl * max_cl;
@@ -554,8 +594,6 @@ int build_preconditioner(Sim& s) {
   const int grid = std::min(s.ncl, 4 * 148);
   k_cluster_inverse<<<grid, AT, smem, s.stream>>>(a, 0, s.ncl, body_cl_dev);
   ++s.launches;
-  // the host vectors must outlive the asynchronous copies
-  if (cudaStreamSynchronize(s.stream) != cudaSuccess) return ABD_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
@@ -570,21 +608,10 @@ int krylov_solve(Sim& s, double* x, int* iters_out) {
   k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
                                          pcg ? nullptr : s.v);
   s.launches += 2;
-  if (finish_dot(s, SL_BZ, s.scal + SC_THR2) != cudaSuccess) return ABD_ERR_CUDA;
-  if (cudaMemcpyAsync(s.hval, s.scal + SC_THR2, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return ABD_ERR_CUDA;
-  const double bz = s.hval[0];
-  if (!(bz > 0.0)) {
-    cudaMemsetAsync(x, 0, sizeof(double) * 12 * s.n, st);
-    if (iters_out) *iters_out = 0;
-    return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
-  }
-  const double thr2 = (s.prm.cg_tol * s.prm.cg_tol) * bz;
-  double hs[5] = {1.0, 1.0, 1.0, 1.0, thr2};  // rho (both parities), alpha, omega, thr^2
-  cudaMemcpyAsync(s.scal, hs, sizeof(hs), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st);
   cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st);
+  k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x);
+  ++s.launches;
   // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
   k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
   ++s.launches;

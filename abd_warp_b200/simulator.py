@@ -171,11 +171,15 @@ class AffineBodySimulator:
                    "abd_update_mesh_vertex")
         return out
 
-    def _lists(self, y0, y1):
+    def _lists(self, y0, y1, dofs=None):
         t = self.torch
         counts = (ctypes.c_int * 4)()
-        _lib.check(self._L.abd_collision_set(self._h, _ptr(y0), _ptr(y1) if y1 is not None else None, counts),
-                   "abd_collision_set")
+        if dofs is None:
+            _lib.check(self._L.abd_collision_set(self._h, _ptr(y0), _ptr(y1) if y1 is not None else None, counts),
+                       "abd_collision_set")
+        else:
+            A, p, A1, p1 = (None if v is None else _ptr(v.contiguous()) for v in dofs)
+            _lib.check(self._L.abd_collision_set_dofs(self._h, A, p, A1, p1, counts), "abd_collision_set_dofs")
         cap = max(1, max(counts))
         i32 = dict(dtype=t.int32, device=self.device)
         ij, pt, ee, vg = (t.zeros((cap, 2), **i32), t.zeros((cap, 5), **i32), t.zeros((cap, 5), **i32),
@@ -196,6 +200,11 @@ class AffineBodySimulator:
         y1 = self.xk if y1 is None else y1
         ij, pt, ee, vg = self._lists(y0.contiguous(), y1.contiguous())
         return ij, pt, ee, vg
+
+    def collision_set_dofs(self, A, p, A1=None, p1=None):
+        """Culling at DOFs as the time step runs it: positions ``transform(A, p)`` (swept to
+        ``transform(A1, p1)`` when given) land in ``x`` / ``xk``; returns ``(ij, pt, ee, vg)``."""
+        return self._lists(None, None, (A, p, A1, p1))
 
     def gradient_hessian(self, A=None, p=None):
         """Assemble g and the block system at DOFs (A, p) (default the current ones):

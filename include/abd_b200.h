@@ -111,6 +111,14 @@ int abd_update_mesh_vertex(abd_sim* sim, const double* A_dev, const double* p_de
  * abd/abd.py:170-185).  counts[4] = {body pairs, PT, EE, VG} (host); the lists stay in the
  * simulator for abd_export_lists. */
 int abd_collision_set(abd_sim* sim, const double* y0_dev, const double* y1_dev, int counts[4]);
+/* The same culling at DOFs, the form the time step uses: positions x = transform(A, p) (and
+ * xk = transform(A1, p1) for the swept boxes when A1_dev / p1_dev are not NULL) are computed
+ * into the simulator's x / xk, and the tree's internal boxes are bounded by the affine
+ * images of their rest-frame boxes instead of a refit.  Lists and counts as
+ * abd_collision_set (update_mesh_vertex + collision_set / trajectory_intersection_set,
+ * abd/abd.py:170-207, as step and ccd call them at abd.py:226-227, 278-280). */
+int abd_collision_set_dofs(abd_sim* sim, const double* A_dev, const double* p_dev, const double* A1_dev,
+                           const double* p1_dev, int counts[4]);
 /* Copy the last culling lists into device buffers of capacity cap rows:
  * ij [cap][2] (I < J), pt [cap][5] and ee [cap][5] as (I, J, pair, local prim of I, local
  * prim of J) like the reference's vec5i lists (culling.py:85-99), vg [cap][2] (body,

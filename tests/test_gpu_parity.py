@@ -94,6 +94,26 @@ def test_culling_sets_bitexact(scene_state, swept):
         assert len(ref["pt"]) + len(ref["ee"]) > 0
 
 
+@pytest.mark.parametrize("swept", [False, True])
+def test_culling_sets_dofs_bitexact(scene_state, swept):
+    """Culling at DOFs (internal node boxes bounded by affine images of rest boxes) finds
+    exactly the oracle's pair sets on the positions those DOFs give."""
+    name, bodies, prm, o, st, sim = scene_state
+    import torch
+    rng = np.random.default_rng(1)
+    A = st["A0"] + 1e-3 * rng.normal(size=st["A0"].shape)
+    p = st["p0"] + 1e-3 * rng.normal(size=st["p0"].shape)
+    A1 = A + 3 * prm.dt * st["Adot"] if swept else None
+    p1 = p + 3 * prm.dt * st["pdot"] + np.array([0, -0.02, 0]) if swept else None
+    ref = o.collision_set(o.transform(A, p), o.transform(A1, p1) if swept else None)
+    cu = lambda v: None if v is None else torch.as_tensor(v, device="cuda")
+    ij, pt, ee, vg = sim.collision_set_dofs(cu(A), cu(p), cu(A1), cu(p1))
+    np.testing.assert_array_equal(ij.cpu().numpy(), ref["ij"])
+    got = {"pt": pt.cpu().numpy(), "ee": ee.cpu().numpy(), "vg": vg.cpu().numpy()}
+    for k in ("pt", "ee", "vg"):
+        np.testing.assert_array_equal(_sorted_rows(got[k]), _sorted_rows(ref[k]), err_msg=f"{name} {k}")
+
+
 def test_gradient_hessian(scene_state):
     name, bodies, prm, o, st, sim = scene_state
     import torch
