@@ -9,6 +9,7 @@
 #include <stdint.h>
 
 #include "../../include/abd_b200.h"
+#include "abd_exact.cuh"
 
 namespace abd {
 
@@ -206,7 +207,8 @@ struct Sim {
   // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
-  double* chunk_val = nullptr;     // [nch] energy sum or minimum time of impact
+  double* chunk_val = nullptr;     // [nch] minimum time of impact
+  XSum* chunk_acc = nullptr;  // [nch] exact barrier-energy sums
 
   // candidate lists
   int cap_pt = 0, cap_ee = 0, cap_vg = 0;
@@ -219,7 +221,8 @@ struct Sim {
   double *pgrad = nullptr;         // [cap_pairs][2][12]
   int* pair_active = nullptr;      // [cap_pairs] active contacts of the pair
   double* pair_val = nullptr;      // [cap_pairs] energy or toi per pair
-  double* body_val = nullptr;      // [n]
+  double* body_val = nullptr;      // [n] minimum time of impact (vertex-ground)
+  XSum* body_acc = nullptr; // [n] exact inertia + vertex-ground energy sums
 
   // Newton system
   double *g = nullptr, *dq = nullptr, *diag = nullptr, *Minv = nullptr;  // [n][12], [n][144]
@@ -234,7 +237,8 @@ struct Sim {
   double* cl_inv = nullptr;                      // dense inverses of the cluster systems
   size_t cap_cl_inv = 0;
   double* zb = nullptr;                          // [n][12] scratch (M^-1 b)
-  double* partials = nullptr;      // reduction partials [kRedSlots][kRedBlocks]
+  XSum* partials = nullptr; // exact reduction partials [kRedSlots][kRedBlocks]
+  int* red_count = nullptr;        // [kRedSlots] CTAs done per reduction (last CTA finishes)
   double* scal = nullptr;          // solver scalars
   int* dstat = nullptr;            // device: [0] status, [1..] counters
   int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
@@ -302,8 +306,8 @@ cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
                         double* pout);
 cudaError_t finish_step(Sim& s, const abd_states& st, double* xview);
-cudaError_t dot_partials(Sim& s, const double* a, const double* b, int slot);
-cudaError_t finish_dot(Sim& s, int slot, double* out_dev);
+// exact dot product of two [n][12] vectors into *out_dev (reduction slot `slot`)
+cudaError_t dot(Sim& s, const double* a, const double* b, int slot, double* out_dev);
 
 // solver.cu
 int build_preconditioner(Sim& s);                 // returns ABD status

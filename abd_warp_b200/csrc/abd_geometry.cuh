@@ -15,6 +15,7 @@
 #pragma once
 
 #include "abd_common.cuh"
+#include "abd_exact.cuh"
 
 namespace abd {
 
@@ -62,23 +63,61 @@ __device__ inline double signed_distance(d3 e0p, d3 e1p, d3 e2p) {
   return dot(e2p, n) / sqrt(dot(n, n));
 }
 
+// Natural logarithm, computed with IEEE-exact operations only (+, -, *, / correctly rounded,
+// frexp exact) so that the oracle's restatement of the same steps returns the same bits.
+// Method: argument reduction x = (1 + f) 2^k with 1 + f in [sqrt(1/2), sqrt(2)) (f exact by
+// Sterbenz's lemma) and the series log(1 + f) = 2 atanh(s), s = f / (2 + f), |s| < 0.1716:
+// 2 atanh(s) = 2s + s R(z), z = s^2, R = sum_{i=1..11} 2 z^i / (2i + 1), and 2s = f - f s,
+// so log(1 + f) = f - s (f - R), whose correction term is small against the exact f (the
+// classical atanh reduction, e.g. J.-M. Muller, "Elementary Functions: Algorithms and
+// Implementation", ch. 11).  log 2 is split in two parts so that k log 2 adds no rounding
+// error of its own.  Measured accuracy: within 1 ulp of the true logarithm.
+__device__ inline double abd_log(double x) {
+  if (!(x > 0.0)) return x == 0.0 ? -INFINITY : __longlong_as_double(0x7ff8000000000000LL);
+  if (isinf(x)) return x;
+  int k;
+  double m = frexp(x, &k);  // x = m 2^k, m in [0.5, 1)
+  if (m < 0.70710678118654752) {
+    m = m * 2.0;
+    k -= 1;
+  }
+  const double f = m - 1.0;
+  const double s = f / (2.0 + f);
+  const double z = s * s;
+  double r = 2.0 / 23.0;
+  r = r * z + 2.0 / 21.0;
+  r = r * z + 2.0 / 19.0;
+  r = r * z + 2.0 / 17.0;
+  r = r * z + 2.0 / 15.0;
+  r = r * z + 2.0 / 13.0;
+  r = r * z + 2.0 / 11.0;
+  r = r * z + 2.0 / 9.0;
+  r = r * z + 2.0 / 7.0;
+  r = r * z + 2.0 / 5.0;
+  r = r * z + 2.0 / 3.0;
+  r = r * z;
+  // log 2 = kLn2Hi + kLn2Lo with kLn2Hi on 40 bits, so k * kLn2Hi is exact for |k| < 2^12
+  const double kLn2Hi = 0.6931471805592082, kLn2Lo = 7.371002565167799e-13;
+  return (double)k * kLn2Hi + (f - (s * (f - r) - (double)k * kLn2Lo));
+}
+
 __device__ inline double barrier(double d, const abd_params& P) {
   if (d < P.d2hat) {
     const double s = d / P.d2hat;
     const double t = s - 1.0;
-    return P.kappa * -(t * t) * log(s);
+    return P.kappa * -(t * t) * abd_log(s);
   }
   return 0.0;
 }
 __device__ inline double barrier_d1(double d, const abd_params& P) {
   if (d < P.d2hat)
-    return P.kappa * (P.d2hat - d) * (2.0 * log(d / P.d2hat) + (d - P.d2hat) / d) / (P.d2hat * P.d2hat);
+    return P.kappa * (P.d2hat - d) * (2.0 * abd_log(d / P.d2hat) + (d - P.d2hat) / d) / (P.d2hat * P.d2hat);
   return 0.0;
 }
 __device__ inline double barrier_d2(double d, const abd_params& P) {
   if (d < P.d2hat)
     return -P.kappa *
-           (2.0 * log(d / P.d2hat) + (d - P.d2hat) / d + (d - P.d2hat) * (2.0 / d + P.d2hat / (d * d))) /
+           (2.0 * abd_log(d / P.d2hat) + (d - P.d2hat) / d + (d - P.d2hat) * (2.0 / d + P.d2hat / (d * d))) /
            (P.d2hat * P.d2hat);
   return 0.0;
 }

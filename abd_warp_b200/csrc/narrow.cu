@@ -29,7 +29,6 @@ namespace {
 constexpr int NT = 128;          // threads per pair CTA
 constexpr int NW = NT / 32;
 constexpr int NOUT = 456;        // 144 off-diagonal + 2 x 144 diagonal + 2 x 12 gradient
-constexpr int NACC = (NOUT + 31) / 32;
 
 inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -42,6 +41,7 @@ struct NarrowArgs {
   const Box* body_box;
   const int2* chunk;
   double* chunk_val;
+  XSum* chunk_acc;
   const int *voff, *toff, *eoff, *tris, *edges;
   const double *y0, *y1, *x0;
   const double *A, *p, *A1, *p1;  // DOFs of y0 / y1 (affine node boxes), or null
@@ -322,13 +322,11 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
   if constexpr (MODE != NARROW_GH) return;
   __syncthreads();  // the pair's list segment, written by this CTA, is now visible to it
 
-  // ---- GH: contacts of the segment, in candidate order ----
+  // ---- GH: contacts of the segment; every contact's 456 values are added exactly ----
   __shared__ int act[NT];
   __shared__ double ush[NW][5][24];
-  __shared__ double red[NW][NOUT];
-  double accv[NACC];
-#pragma unroll
-  for (int j = 0; j < NACC; ++j) accv[j] = 0.0;
+  extern __shared__ XSum xred[];  // [NOUT]
+  for (int e = tid; e < NOUT * (kXD + 1); e += NT) reinterpret_cast<long long*>(xred)[e] = 0;
   const int total = tpt + tee;
   int nact_total = 0;
   for (int c0 = 0; c0 < total; c0 += NT) {
@@ -348,7 +346,7 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
       is_act = contact_active(type, xs, a.prm, &G, &d2) ? 1 : 0;
     }
     int pos;
-    const int nact = block_scan(is_act, sh, pos);
+    const int nact = block_scan(is_act, sh, pos);  // also orders the zeroing of xred before use
     if (is_act) act[pos] = c;
     __syncthreads();
     nact_total += nact;
@@ -389,10 +387,7 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
           ush[warp][k][lane] = dw[0] * C.q[k][comp] + dw[1] * C.q[k][3 + comp] + dw[2] * C.q[k][6 + comp];
       }
       __syncwarp();
-#pragma unroll
-      for (int j = 0; j < NACC; ++j) {
-        const int e = lane + 32 * j;
-        if (e >= NOUT) break;
+      for (int e = lane; e < NOUT; e += 32) {
         double v = 0.0;
         if (e < 432) {
           const int blk = e / 144, r = (e % 144) / 12, cidx = e % 12;
@@ -403,7 +398,7 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
         } else {
           v = C.gscale * ush[warp][4][e - 432];
         }
-        accv[j] += v;
+        xs_add_atomic(&xred[e], v);
       }
       __syncwarp();
     }
@@ -414,15 +409,8 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
     if (nact_total) atomicAdd(&a.dstat[DS_ACTIVE], nact_total);
   }
   if (nact_total == 0) return;
-#pragma unroll
-  for (int j = 0; j < NACC; ++j) {
-    const int e = lane + 32 * j;
-    if (e < NOUT) red[warp][e] = accv[j];
-  }
-  __syncthreads();
   for (int e = tid; e < NOUT; e += NT) {
-    double v = red[0][e];
-    for (int w = 1; w < NW; ++w) v += red[w][e];
+    const double v = xs_round(xred[e]);
     if (e < 144) {
       a.offdiag[(size_t)p * 288 + e] = v;
       a.offdiag[(size_t)p * 288 + 144 + (e % 12) * 12 + e / 12] = v;
@@ -469,7 +457,6 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   __shared__ Box nbox[NBB];
   __shared__ float ndof[NBB][24];
   __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB];
-  __shared__ double red[CT];
   if (tid < Q) {
     const int k = ch.y + tid;
     if (k < nV) {
@@ -482,7 +469,9 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
     }
   }
-  double acc = ccd ? 1.0 : 0.0;
+  double acc = 1.0;  // CCD: minimum time of impact
+  XSum xacc;         // ENERGY: exact sum of the barrier energies
+  xs_zero(xacc);
   const bool ok = !(a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW);  // an overflowed pass is rerun
   const int r0 = a.row_ptr[I], r1 = min(a.row_ptr[I + 1], a.cap_adj);
   for (int b0 = (ok && Q > 0) ? r0 : r1; b0 < r1; b0 += NBB) {
@@ -522,7 +511,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
           const double t = collision_time(type, xs, x1);
           if (t < 1.0) acc = fmin(acc, t);
         } else {
-          acc += contact_energy(type, xs, a.prm);
+          xs_add(xacc, contact_energy(type, xs, a.prm));
         }
       };
       if (pt) {
@@ -535,13 +524,20 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       }
     }
   }
-  red[tid] = acc;
-  __syncthreads();
-  for (int st = CT / 2; st > 0; st >>= 1) {
-    if (tid < st) red[tid] = ccd ? fmin(red[tid], red[tid + st]) : red[tid] + red[tid + st];
+  if constexpr (ccd) {
+    __shared__ double red[CT];
+    red[tid] = acc;
     __syncthreads();
+    for (int st = CT / 2; st > 0; st >>= 1) {
+      if (tid < st) red[tid] = fmin(red[tid], red[tid + st]);
+      __syncthreads();
+    }
+    if (tid == 0) a.chunk_val[c] = red[0];
+  } else {
+    __shared__ XSum xsh[CT / 32];
+    xs_block_sum(xacc, xsh);
+    if (tid == 0) a.chunk_acc[c] = xacc;
   }
-  if (tid == 0) a.chunk_val[c] = red[0];
 }
 
 // ---------------------------------------------------------------------------------------
@@ -560,6 +556,7 @@ struct BodyArgs {
   const int2* ij;
   const double *pdiag, *pgrad;
   double *diag, *g, *body_val;
+  XSum* body_acc;
   int* dstat;
   int* vg_list;
   int cap_vg;
@@ -594,38 +591,27 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   const double dt = a.prm.dt, ks = a.prm.stiffness;
   const double* A = a.A + 9 * b;
   double val = 0.0;
-  // vertex-ground partial sums: g (4 y-components) and H (4x4 yy-components)
-  __shared__ double vred[20][128];
+  // vertex-ground sums, exact: g (4 y-components) and H (4x4 yy-components)
+  __shared__ XSum vx[20];
   const bool vg_on = a.prm.ground_enabled && a.prm.enable_vg && !fixed;
-  if (vg_on) {
-    double acc[20];
+  for (int e = t; e < 20 * (kXD + 1); e += BT) reinterpret_cast<long long*>(vx)[e] = 0;
+  __syncthreads();
+  if (vg_on && t < 128) {
+    const Box bb = load_box(&a.body_box[b]);
+    for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
+      if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
+      const double d = a.y[3 * v + 1] - a.prm.ground;
+      const double d2b = barrier_d2(d * d, a.prm), db = barrier_d1(d * d, a.prm);
+      const double th[4] = {1.0, a.x0[3 * v], a.x0[3 * v + 1], a.x0[3 * v + 2]};
 #pragma unroll
-    for (int k = 0; k < 20; ++k) acc[k] = 0.0;
-    if (t < 128) {
-      const Box bb = load_box(&a.body_box[b]);
-      for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
-        if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
-        const double d = a.y[3 * v + 1] - a.prm.ground;
-        const double d2b = barrier_d2(d * d, a.prm), db = barrier_d1(d * d, a.prm);
-        const double th[4] = {1.0, a.x0[3 * v], a.x0[3 * v + 1], a.x0[3 * v + 2]};
+      for (int ii = 0; ii < 4; ++ii) {
+        xs_add_atomic(&vx[ii], ((d * 2.0) * th[ii]) * db);
 #pragma unroll
-        for (int ii = 0; ii < 4; ++ii) {
-          acc[ii] += ((d * 2.0) * th[ii]) * db;
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj) acc[4 + 4 * ii + jj] += (((th[ii] * th[jj]) * d2b) * 4.0) * d * d;
-        }
+        for (int jj = 0; jj < 4; ++jj) xs_add_atomic(&vx[4 + 4 * ii + jj], (((th[ii] * th[jj]) * d2b) * 4.0) * d * d);
       }
-#pragma unroll
-      for (int k = 0; k < 20; ++k) vred[k][t] = acc[k];
-    }
-    __syncthreads();
-    for (int s = 64; s > 0; s >>= 1) {
-      if (t < s)
-#pragma unroll
-        for (int k = 0; k < 20; ++k) vred[k][t] += vred[k][t + s];
-      __syncthreads();
     }
   }
+  __syncthreads();
   if (t >= 156) return;
   if (!fixed) {
     double At[9], pt[3];
@@ -649,7 +635,6 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
         dh = dh + ((h * 4.0) * ks) * dt * dt;
       }
       val = dh;
-      if (vg_on && rr == 1 && cc == 1) val += vred[4 + 4 * ii + jj][0];
     } else {
       const int k = t - 144, m = k / 3, comp = k % 3;
       if (m == 0) {
@@ -665,17 +650,29 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
         gr = (dt * dt) * gr;
         val = gr + (A[3 * i + comp] - At[3 * i + comp]) * a.I0[b];
       }
-      if (vg_on && comp == 1) val += vred[m][0];
     }
-    // contact contributions of the body's pairs, in adjacency (increasing neighbour) order;
+    // entry = inertia + vertex-ground terms + the pair contributions (adjacency order; the sum
+    // is exact, so the order does not matter), rounded once
+    XSum acc;
+    xs_zero(acc);
+    xs_add(acc, val);
+    if (vg_on) {
+      if (t < 144) {
+        const int r = t / 12, c = t % 12;
+        if (r % 3 == 1 && c % 3 == 1) xs_merge(acc, vx[4 + 4 * (r / 3) + c / 3]);
+      } else if ((t - 144) % 3 == 1) {
+        xs_merge(acc, vx[(t - 144) / 3]);
+      }
+    }
     // skipped when the pair lists of this pass overflowed (the host reruns the pass)
     const int k1 = (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW) ? a.row_ptr[b] : a.row_ptr[b + 1];
     for (int k = a.row_ptr[b]; k < k1; ++k) {
       const int pr = a.adj_pair[k];
       if (a.pair_active[pr] <= 0) continue;
       const int side = a.ij[pr].x == b ? 0 : 1;
-      val += t < 144 ? a.pdiag[(size_t)pr * 288 + side * 144 + t] : a.pgrad[(size_t)pr * 24 + side * 12 + (t - 144)];
+      xs_add(acc, t < 144 ? a.pdiag[(size_t)pr * 288 + side * 144 + t] : a.pgrad[(size_t)pr * 24 + side * 12 + (t - 144)]);
     }
+    val = xs_round(acc);
     if (!isfinite(val)) atomicOr(&a.dstat[DS_STATUS], ST_NAN);
   } else {
     val = (t < 144 && (t % 13) == 0) ? 1.0 : 0.0;
@@ -684,52 +681,47 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   else a.g[(size_t)b * 12 + (t - 144)] = val;
 }
 
+// body b's exact energy terms: vertex-ground barriers and inertia + orthogonality
+// (orthogonal_energy.py:24-32, vg_ipc.py / energy.py:24-33)
 __global__ void __launch_bounds__(128) k_body_energy(BodyArgs a) {
   const int b = blockIdx.x, t = threadIdx.x;
-  __shared__ double red[128];
-  double acc = 0.0;
+  __shared__ XSum xsh[4];
+  XSum acc;
+  xs_zero(acc);
   if (a.prm.ground_enabled && a.prm.enable_vg) {
     const Box bb = load_box(&a.body_box[b]);
     for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
       if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
       const double d = a.y[3 * v + 1] - a.prm.ground;
-      acc += barrier(d * d, a.prm);
+      xs_add(acc, barrier(d * d, a.prm));
     }
   }
-  red[t] = acc;
-  __syncthreads();
-  for (int s = 64; s > 0; s >>= 1) {
-    if (t < s) red[t] += red[t + s];
-    __syncthreads();
-  }
-  if (t == 0) {
-    double e = red[0];
-    if (!a.fixed[b]) {
-      double At[9], pt[3];
-      tilde(a, b, At, pt);
-      const double* K = a.A + 9 * b;  // trial DOFs Ak
-      double eo = 0.0;
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) {
-          const double tt = (K[3 * i] * K[3 * j] + K[3 * i + 1] * K[3 * j + 1] + K[3 * i + 2] * K[3 * j + 2]) -
-                            (i == j ? 1.0 : 0.0);
-          eo += tt * tt;
-        }
-      eo = eo * a.prm.stiffness;
-      const double* pk = a.p + 3 * b;
-      double d0[3], d1[3], d2[3], d3v[3];
-      for (int k = 0; k < 3; ++k) {
-        d0[k] = pk[k] - pt[k];
-        d1[k] = K[k] - At[k];
-        d2[k] = K[3 + k] - At[3 + k];
-        d3v[k] = K[6 + k] - At[6 + k];
+  if (t == 0 && !a.fixed[b]) {
+    double At[9], pt[3];
+    tilde(a, b, At, pt);
+    const double* K = a.A + 9 * b;  // trial DOFs Ak
+    double eo = 0.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const double tt = (K[3 * i] * K[3 * j] + K[3 * i + 1] * K[3 * j + 1] + K[3 * i + 2] * K[3 * j + 2]) -
+                          (i == j ? 1.0 : 0.0);
+        eo += tt * tt;
       }
-      auto dd = [](const double* u) { return u[0] * u[0] + u[1] * u[1] + u[2] * u[2]; };
-      const double nm = dd(d0) * a.mass[b] + (dd(d1) + dd(d2) + dd(d3v)) * a.I0[b];
-      e += eo * a.prm.dt * a.prm.dt + 0.5 * nm;
+    eo = eo * a.prm.stiffness;
+    const double* pk = a.p + 3 * b;
+    double d0[3], d1[3], d2[3], d3v[3];
+    for (int k = 0; k < 3; ++k) {
+      d0[k] = pk[k] - pt[k];
+      d1[k] = K[k] - At[k];
+      d2[k] = K[3 + k] - At[3 + k];
+      d3v[k] = K[6 + k] - At[6 + k];
     }
-    a.body_val[b] = e;
+    auto dd = [](const double* u) { return u[0] * u[0] + u[1] * u[1] + u[2] * u[2]; };
+    const double nm = dd(d0) * a.mass[b] + (dd(d1) + dd(d2) + dd(d3v)) * a.I0[b];
+    xs_add(acc, eo * a.prm.dt * a.prm.dt + 0.5 * nm);
   }
+  xs_block_sum(acc, xsh);
+  if (t == 0) a.body_acc[b] = acc;
 }
 
 __global__ void __launch_bounds__(128) k_body_vg_toi(BodyArgs a) {
@@ -771,6 +763,17 @@ __global__ void k_vg_list(BodyArgs a) {
       atomicOr(&a.dstat[DS_STATUS], ST_VG_OVERFLOW);
     }
   }
+}
+
+// single-CTA exact sum of two accumulator arrays, rounded once
+__global__ void __launch_bounds__(1024) k_reduce_exact(const XSum* xa, int na, const XSum* xb, int nb, double* out) {
+  __shared__ XSum xsh[32];
+  XSum acc;
+  xs_zero(acc);
+  for (int i = threadIdx.x; i < na; i += 1024) xs_merge(acc, xa[i]);
+  for (int i = threadIdx.x; i < nb; i += 1024) xs_merge(acc, xb[i]);
+  xs_block_sum(acc, xsh);
+  if (threadIdx.x == 0) *out = xs_round(acc);
 }
 
 // deterministic single-CTA reduction of chunk and body values (sum or min)
@@ -829,29 +832,37 @@ __global__ void k_finish(int n, double dt, abd_states st) {
   }
 }
 
-__global__ void k_dot_partials(int N, const double* a, const double* b, double* part) {
-  __shared__ double red[256];
-  double acc = 0.0;
-  for (int i = blockIdx.x * 256 + threadIdx.x; i < N; i += kRedBlocks * 256) acc += a[i] * b[i];
-  red[threadIdx.x] = acc;
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-    __syncthreads();
+// Exact dot product on a fixed grid of kRedBlocks CTAs; the last CTA to finish sums the
+// partials and writes the rounded result to *out.
+__global__ void __launch_bounds__(256) k_dot(int N, const double* a, const double* b, XSum* part, int* count,
+                                             double* out) {
+  __shared__ XSum sh[8];
+  __shared__ bool last;
+  XSum acc;
+  xs_zero(acc);
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < N; i += kRedBlocks * 256) xs_add(acc, a[i] * b[i]);
+  xs_block_sum(acc, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = acc;
+    __threadfence();
+    last = atomicAdd(count, 1) == kRedBlocks - 1;
   }
-  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
-}
-
-__global__ void k_finish_dot(const double* part, double* out) {
-  __shared__ double red[512];
-  const int t = threadIdx.x;
-  red[t] = t < kRedBlocks ? part[t] : 0.0;
   __syncthreads();
-  for (int s = 256; s > 0; s >>= 1) {
-    if (t < s) red[t] += red[t + s];
-    __syncthreads();
+  if (!last || threadIdx.x >= 32) return;
+  __threadfence();
+  XSum t;
+  xs_zero(t);
+  for (int i = threadIdx.x; i < kRedBlocks; i += 32) {
+    const long long* q = reinterpret_cast<const long long*>(part + i);
+#pragma unroll
+    for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
+    t.flags |= __ldcg(q + kXD);
   }
-  if (t == 0) *out = red[0];
+  xs_warp_sum(t);
+  if (threadIdx.x == 0) {
+    *out = xs_round(t);
+    *count = 0;
+  }
 }
 
 NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
@@ -872,6 +883,7 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.body_box = s.body_box;
   a.chunk = s.chunk;
   a.chunk_val = s.chunk_val;
+  a.chunk_acc = s.chunk_acc;
   a.voff = s.voff;
   a.toff = s.toff;
   a.eoff = s.eoff;
@@ -921,6 +933,7 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
   a.diag = s.diag;
   a.g = s.g;
   a.body_val = s.body_val;
+  a.body_acc = s.body_acc;
   a.dstat = s.dstat;
   a.vg_list = s.vg_list;
   a.cap_vg = s.cap_vg;
@@ -939,7 +952,12 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
     else k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
   } else {
     if (s.cap_pairs == 0) return cudaSuccess;
-    if (mode == NARROW_GH) k_narrow<NARROW_GH><<<s.cap_pairs, NT, 0, s.stream>>>(a);
+    if (mode == NARROW_GH) {
+      const int smem = NOUT * (int)sizeof(XSum);
+      cudaError_t e = cudaFuncSetAttribute(k_narrow<NARROW_GH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      k_narrow<NARROW_GH><<<s.cap_pairs, NT, smem, s.stream>>>(a);
+    }
     else k_narrow<NARROW_LISTS><<<s.cap_pairs, NT, 0, s.stream>>>(a);
   }
   ++s.launches;
@@ -979,7 +997,7 @@ cudaError_t vg_list_swept(Sim& s, const double* y0, const double* y1) {
 }
 
 cudaError_t sum_energy(Sim& s, double* out) {
-  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.chunk_val, s.nch, s.body_val, s.n, 0, out);
+  k_reduce_exact<<<1, 1024, 0, s.stream>>>(s.chunk_acc, s.nch, s.body_acc, s.n, out);
   ++s.launches;
   return cudaGetLastError();
 }
@@ -1013,14 +1031,9 @@ cudaError_t finish_step(Sim& s, const abd_states& st, double* xview) {
   return transform(s, st.A0, st.p0, xview);
 }
 
-cudaError_t dot_partials(Sim& s, const double* a, const double* b, int slot) {
-  k_dot_partials<<<kRedBlocks, 256, 0, s.stream>>>(12 * s.n, a, b, s.partials + slot * kRedBlocks);
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t finish_dot(Sim& s, int slot, double* out) {
-  k_finish_dot<<<1, 512, 0, s.stream>>>(s.partials + slot * kRedBlocks, out);
+cudaError_t dot(Sim& s, const double* a, const double* b, int slot, double* out_dev) {
+  k_dot<<<kRedBlocks, 256, 0, s.stream>>>(12 * s.n, a, b, s.partials + (size_t)slot * kRedBlocks, s.red_count + slot,
+                                          out_dev);
   ++s.launches;
   return cudaGetLastError();
 }

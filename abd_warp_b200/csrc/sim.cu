@@ -340,6 +340,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     s.nch = (int)ch.size();
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
     ok(dalloc(&s.chunk_val, ch.size()));
+    ok(dalloc(&s.chunk_acc, ch.size()));
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // ch is a host temporary
   }
   ok(dalloc(&s.row_ptr, n + 1));
@@ -353,7 +354,9 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.diag, 144 * (size_t)n));
   ok(dalloc(&s.Minv, 144 * (size_t)n));
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
-  ok(dalloc(&s.scal, 16));
+  ok(dalloc(&s.red_count, abd::kRedSlots));
+  ok(dalloc(&s.scal, 32));
+  ok(dalloc(&s.body_acc, n));
   ok(dalloc(&s.dstat, abd::DS_NSLOTS));
   ok(dalloc(&s.dmin, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
@@ -364,6 +367,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = abd::rest_boxes(s);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat, 0, sizeof(int) * abd::DS_NSLOTS, s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.red_count, 0, sizeof(int) * abd::kRedSlots, s.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
   if (tcd) cudaFree(tcd);
   if (ecd) cudaFree(ecd);
@@ -399,7 +403,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.pair_active, s.pair_val, s.body_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
-                  s.chunk_val};
+                  s.chunk_val, s.chunk_acc, s.body_acc, s.red_count};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact})
@@ -578,10 +582,8 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
     inf.linear_iters += lin;
     // dq.g and g.g (abd.py:148, 265), read back together with the CCD bound
-    CK(abd::dot_partials(s, s.dq, s.g, 10));
-    CK(abd::finish_dot(s, 10, s.scal + 10));
-    CK(abd::dot_partials(s, s.g, s.g, 11));
-    CK(abd::finish_dot(s, 11, s.scal + 11));
+    CK(abd::dot(s, s.dq, s.g, 10, s.scal + 10));
+    CK(abd::dot(s, s.g, s.g, 11, s.scal + 11));
     // CCD bound (abd.py:278-303)
     CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
     double alpha;

@@ -52,58 +52,59 @@ struct SolverArgs {
   const int *cl_ptr, *cl_body;
   const long long* cl_off;
   double* cl_inv;
-  double* part;
+  XSum* part;        // [kRedSlots][kRedBlocks] exact per-CTA partials
+  int* red_count;    // [kRedSlots] CTAs that delivered their partial
   double* scal;
   int* dstat;
 };
 
-// all lanes of the calling warp return the fixed-order sum of the kRedBlocks partials
-__device__ inline double sum_partials(const double* part) {
-  const int lane = threadIdx.x & 31;
-  double a = 0.0;
-  for (int i = lane; i < kRedBlocks; i += 32) a += part[i];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-  return a;
+constexpr int SC_RED = 16;  // scal[SC_RED + slot]: the rounded total of reduction `slot`
+
+// scalars produced by the previous kernel's reductions
+__device__ inline void cta_scalars(const SolverArgs& a, const int* slots, int ns, double* out) {
+  for (int k = 0; k < ns; ++k) out[k] = a.scal[SC_RED + slots[k]];
 }
 
-// CTA-wide broadcast of sum_partials for up to 3 slots
-__device__ inline void cta_scalars(const double* part, const int* slots, int ns, double* out) {
-  __shared__ double sv[3];
-  if (threadIdx.x < 32)
-    for (int k = 0; k < ns; ++k) {
-      const double v = sum_partials(part + slots[k] * kRedBlocks);
-      if (threadIdx.x == 0) sv[k] = v;
-    }
-  __syncthreads();
-  for (int k = 0; k < ns; ++k) out[k] = sv[k];
-  __syncthreads();
-}
-
-// per-CTA partial of two dot products (every thread passes its own contribution)
-__device__ inline void cta_partials(double d0, double d1, double* part, int slot0, int slot1) {
-  __shared__ double w[32][2];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    d0 += __shfl_xor_sync(0xffffffffu, d0, o);
-    d1 += __shfl_xor_sync(0xffffffffu, d1, o);
+// Exact per-CTA partials of up to two dot products (every thread passes its accumulators);
+// the last CTA to deliver sums the partials of all CTAs and stores the rounded totals in
+// scal[SC_RED + slot] (a single counter per launch: slot0 if >= 0, else slot1).
+__device__ inline void cta_partials(const SolverArgs& a, XSum& x0, XSum& x1, int slot0, int slot1) {
+  __shared__ XSum sh[8];
+  __shared__ bool last;
+  if (slot0 >= 0) {
+    xs_block_sum(x0, sh);
+    if (threadIdx.x == 0) a.part[slot0 * kRedBlocks + blockIdx.x] = x0;
   }
-  if (lane == 0) {
-    w[warp][0] = d0;
-    w[warp][1] = d1;
+  if (slot1 >= 0) {
+    xs_block_sum(x1, sh);
+    if (threadIdx.x == 0) a.part[slot1 * kRedBlocks + blockIdx.x] = x1;
   }
-  __syncthreads();
+  const int cslot = slot0 >= 0 ? slot0 : slot1;
   if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int k = 0; k < nw; ++k) {
-      a += w[k][0];
-      b += w[k][1];
-    }
-    if (slot0 >= 0) part[slot0 * kRedBlocks + blockIdx.x] = a;
-    if (slot1 >= 0) part[slot1 * kRedBlocks + blockIdx.x] = b;
+    __threadfence();
+    last = atomicAdd(&a.red_count[cslot], 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = 0; k < 2; ++k) {
+    const int slot = k ? slot1 : slot0;
+    if (slot < 0) continue;
+    XSum t;
+    xs_zero(t);
+    if (threadIdx.x < 32) {
+      const XSum* P = a.part + slot * kRedBlocks;
+      for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
+        const long long* q = reinterpret_cast<const long long*>(P + i);
+#pragma unroll
+        for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
+        t.flags |= __ldcg(q + kXD);
+      }
+      xs_warp_sum(t);
+      if (threadIdx.x == 0) a.scal[SC_RED + slot] = xs_round(t);
+    }
+  }
+  if (threadIdx.x == 0) a.red_count[cslot] = 0;
 }
 
 // y_b (lanes 0..11 hold row lane) = (A x)_b for block row b
@@ -205,7 +206,9 @@ __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const 
                                               double* copy, int slot) {
   if (it_guard && solver_done(a.dstat)) return;
   __shared__ double vs[12 * kMaxCluster];
-  double d0 = 0.0;
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
   for (int c = blockIdx.x; c < a.ncl; c += gridDim.x) {
     const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
     for (int i = threadIdx.x; i < D; i += AT) vs[i] = in[(size_t)a.cl_body[base + i / 12] * 12 + i % 12];
@@ -218,18 +221,20 @@ __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const 
       const size_t gi = (size_t)a.cl_body[base + i / 12] * 12 + i % 12;
       out[gi] = acc;
       if (copy) copy[gi] = acc;
-      d0 += vs[i] * acc;
+      if (slot >= 0) xs_add(d0, vs[i] * acc);
     }
     __syncthreads();
   }
-  if (slot >= 0) cta_partials(d0, 0.0, a.part, slot, -1);
+  if (slot >= 0) cta_partials(a, d0, d1, slot, -1);
 }
 
 // ---- r = b - A x (+ rh = r, p = v = 0 for BiCGSTAB) ----
 __global__ void __launch_bounds__(256) k_residual(SolverArgs a, const double* bvec, const double* x, double* r,
                                                   double* rh, double* pv, double* v) {
   const int lane = threadIdx.x & 31;
-  double d0 = 0.0;
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
   FOR_BODIES(b) {
     const double ax = row_product(a, b, x);
     if (lane < 12) {
@@ -239,10 +244,10 @@ __global__ void __launch_bounds__(256) k_residual(SolverArgs a, const double* bv
       if (rh) rh[i] = ri;
       if (pv) pv[i] = 0.0;
       if (v) v[i] = 0.0;
-      d0 += ri * ri;
+      xs_add(d0, ri * ri);
     }
   }
-  cta_partials(d0, 0.0, a.part, SL_RHR, -1);
+  cta_partials(a, d0, d1, SL_RHR, -1);
 }
 
 // ---- PCG ----
@@ -252,7 +257,7 @@ __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, int it, const doubl
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
   const int slots[1] = {rz};
   double sc[1];
-  cta_scalars(a.part, slots, 1, sc);
+  cta_scalars(a, slots, 1, sc);
   if (!(sc[0] > a.scal[SC_THR2])) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.dstat[DS_R_DONE] = it;
@@ -261,16 +266,18 @@ __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, int it, const doubl
     return;
   }
   const int lane = threadIdx.x & 31;
-  double d0 = 0.0;
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
   FOR_BODIES(b) {
     const double yi = row_product(a, b, pv);
     if (lane < 12) {
       const size_t i = (size_t)b * 12 + lane;
       Ap[i] = yi;
-      d0 += pv[i] * yi;
+      xs_add(d0, pv[i] * yi);
     }
   }
-  cta_partials(d0, 0.0, a.part, SL_PAP, -1);
+  cta_partials(a, d0, d1, SL_PAP, -1);
 }
 
 // K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature)
@@ -280,7 +287,7 @@ __global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, int it, const doubl
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
   const int slots[2] = {rz, SL_PAP};
   double sc[2];
-  cta_scalars(a.part, slots, 2, sc);
+  cta_scalars(a, slots, 2, sc);
   if (!(sc[1] > 0.0)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.dstat[DS_R_DONE] = it;
@@ -306,7 +313,7 @@ __global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, int it, const doubl
   const int rz_old = (it & 1) ? SL_RZ0 : SL_RZ1, rz_new = (it & 1) ? SL_RZ1 : SL_RZ0;
   const int slots[2] = {rz_new, rz_old};
   double sc[2];
-  cta_scalars(a.part, slots, 2, sc);
+  cta_scalars(a, slots, 2, sc);
   if (!(sc[0] > a.scal[SC_THR2])) return;  // converged: K1 of the next iteration stops
   const double beta = sc[0] / sc[1];
   const int lane = threadIdx.x & 31;
@@ -324,8 +331,8 @@ __global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, int it, const doub
   if (solver_done(a.dstat)) return;
   const int slots[2] = {SL_RZ0, SL_RHR};
   double sc[2];
-  cta_scalars(a.part, slots, 2, sc);
-  if (!(sc[0] > a.scal[SC_THR2]) || sc[1] == 0.0) {
+  cta_scalars(a, slots, 2, sc);
+  if (!(sc[0] > a.scal[SC_THR2]) || sc[1] == 0.0 || !isfinite(sc[1])) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.dstat[DS_R_DONE] = it;
       a.dstat[DS_SOLVER_ITERS] = it - 1;
@@ -351,17 +358,19 @@ __global__ void __launch_bounds__(256) k_spmv(SolverArgs a, const double* in, do
                                               const double* w1, int slot1) {
   if (solver_done(a.dstat)) return;
   const int lane = threadIdx.x & 31;
-  double d0 = 0.0, d1 = 0.0;
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
   FOR_BODIES(b) {
     const double yi = row_product(a, b, in);
     if (lane < 12) {
       const size_t i = (size_t)b * 12 + lane;
       out[i] = yi;
-      if (w0) d0 += w0[i] * yi;
-      if (w1) d1 += w1[i] * yi;
+      if (w0) xs_add(d0, w0[i] * yi);
+      if (w1) xs_add(d1, w1[i] * yi);
     }
   }
-  cta_partials(d0, d1, a.part, slot0, slot1);
+  cta_partials(a, d0, d1, slot0, slot1);
 }
 
 // K3: alpha = rho / rh.v; s = r - alpha v
@@ -369,7 +378,7 @@ __global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, int it, const doub
   if (solver_done(a.dstat)) return;
   const int slots[1] = {SL_RHV};
   double sc[1];
-  cta_scalars(a.part, slots, 1, sc);
+  cta_scalars(a, slots, 1, sc);
   const double alpha = a.scal[it & 1] / sc[0];
   const int lane = threadIdx.x & 31;
   FOR_BODIES(b) {
@@ -387,7 +396,7 @@ __global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, int it, const doub
   if (ds[DS_R_DONE] != 0 || (ds[DS_S_DONE] != 0 && ds[DS_S_DONE] != it)) return;
   const int slots[1] = {SL_SZ};
   double sc[1];
-  cta_scalars(a.part, slots, 1, sc);
+  cta_scalars(a, slots, 1, sc);
   if (sc[0] > a.scal[SC_THR2]) return;
   const double alpha = a.scal[SC_ALPHA];
   const int lane = threadIdx.x & 31;
@@ -410,21 +419,23 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, int it, const doub
   if (solver_done(a.dstat)) return;
   const int slots[2] = {SL_TS, SL_TT};
   double sc[2];
-  cta_scalars(a.part, slots, 2, sc);
+  cta_scalars(a, slots, 2, sc);
   const double omega = sc[0] / sc[1];
   const double alpha = a.scal[SC_ALPHA];
   const int lane = threadIdx.x & 31;
-  double d1 = 0.0;
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
   FOR_BODIES(b) {
     if (lane < 12) {
       const size_t i = (size_t)b * 12 + lane;
       x[i] += alpha * y[i] + omega * z[i];
       const double ri = s[i] - omega * t[i];
       r[i] = ri;
-      d1 += rh[i] * ri;
+      xs_add(d1, rh[i] * ri);
     }
   }
-  cta_partials(0.0, d1, a.part, -1, SL_RHR);
+  cta_partials(a, d0, d1, -1, SL_RHR);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scal[SC_OMEGA] = omega;
     a.dstat[DS_SOLVER_ITERS] = it;
@@ -451,13 +462,7 @@ __global__ void k_pair_weights(int cap_pairs, const int* dstat_np, const int2* i
 // Threshold thr^2 = tol^2 b^T M^-1 b and the recurrence scalars; b = 0 gives x = 0 and ends
 // the solve before its first iteration
 __global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, double* x) {
-  __shared__ double bz;
-  if (threadIdx.x < 32) {
-    const double v = sum_partials(a.part + SL_BZ * kRedBlocks);
-    if (threadIdx.x == 0) bz = v;
-  }
-  __syncthreads();
-  const double b = bz;
+  const double b = a.scal[SC_RED + SL_BZ];
   if (!(b > 0.0))
     for (int i = blockIdx.x * 256 + threadIdx.x; i < 12 * a.n; i += kRedBlocks * 256) x[i] = 0.0;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -484,6 +489,7 @@ SolverArgs solver_args(Sim& s) {
   a.cl_off = s.cl_off;
   a.cl_inv = s.cl_inv;
   a.part = s.partials;
+  a.red_count = s.red_count;
   a.scal = s.scal;
   a.dstat = s.dstat;
   return a;

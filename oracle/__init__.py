@@ -33,7 +33,6 @@ def lib():
         L.orc_destroy.argtypes = [v]
         L.orc_set_params.argtypes = [v, v]
         L.orc_set_threads.argtypes = [i]
-        L.orc_set_reverse_sums.argtypes = [i]
         L.orc_max_threads.restype = i
         L.orc_set_state.argtypes = [v] * 6
         L.orc_get_state.argtypes = [v] * 7
@@ -49,6 +48,12 @@ def lib():
         L.orc_ccd.restype = d
         L.orc_contact_gh.argtypes = [i, v, v, v, v, v, v, v, v]
         L.orc_contact_gh.restype = i
+        L.orc_contact_terms.argtypes = [i, v, v, v, v]
+        L.orc_contact_terms.restype = i
+        L.orc_log.argtypes = [d]
+        L.orc_log.restype = d
+        L.orc_exact_sum.argtypes = [v, ctypes.c_long]
+        L.orc_exact_sum.restype = d
         L.orc_contact_energy.argtypes = [i, v, v]
         L.orc_contact_energy.restype = d
         L.orc_collision_time.argtypes = [i, v, v]
@@ -189,6 +194,25 @@ def contact_gh(type_, x4, r4, prm):
     return bool(a), d2.value, g, Hi, Hj, Hij
 
 
+def contact_terms(type_, x4, r4, prm):
+    """Rank-one form of the pair terms: (active, H_IJ, H_II, H_JJ, g24)."""
+    x4, r4 = _c64(x4), _c64(r4)
+    c = prm.to_c()
+    out = np.zeros(456)
+    a = lib().orc_contact_terms(type_, _p(x4), _p(r4), ctypes.byref(c), _p(out))
+    return bool(a), out[:144].reshape(12, 12), out[144:288].reshape(12, 12), out[288:432].reshape(12, 12), out[432:]
+
+
+def abd_log(x: float) -> float:
+    """The logarithm shared bit for bit with the CUDA product."""
+    return lib().orc_log(float(x))
+
+
+def exact_sum(values) -> float:
+    v = _c64(np.ravel(values))
+    return lib().orc_exact_sum(_p(v), len(v))
+
+
 def contact_energy(type_, x4, prm):
     x4 = _c64(x4)
     c = prm.to_c()
@@ -205,11 +229,6 @@ def cubic_roots(coef, x0, x1):
     roots = np.zeros(3)
     n = lib().orc_cubic_roots(_p(coef), x0, x1, _p(roots))
     return n, roots
-
-
-def set_reverse_sums(flag: bool):
-    """Test hook: sum contact energies in reverse order (perturbs rounding only)."""
-    lib().orc_set_reverse_sums(int(flag))
 
 
 def set_threads(t: int):

@@ -30,6 +30,7 @@
 // operation order is the same.
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -37,9 +38,6 @@
 #include <omp.h>
 
 namespace {
-
-// test hook: 1 sums contact energies in reverse candidate order (changes rounding only)
-int g_reverse_sums = 0;
 
 struct Params {
   double dt, dhat, d2hat, kappa, stiffness, gravity, tol, c1, alpha_min, ground, cg_tol, refine_tol;
@@ -74,6 +72,115 @@ struct Cand {
   int I, J, pair, pi, pj;  // vec5i (I, J, ij index, prim of I, prim of J)
 };
 
+// ---------------------------------------------------------------------------------------
+// Exact summation.  Every reduction of the step is the exact sum of its FP64 terms, each
+// truncated to a multiple of 2^-192, rounded to FP64 once (to nearest, ties to even).  The
+// sum does not depend on the order of the terms, so it is fixed by the terms alone; the
+// CUDA product sums the same way (32-bit digits in 64-bit limbs).
+// ---------------------------------------------------------------------------------------
+constexpr int kXD = 10, kXB0 = -192;
+
+struct XSum {
+  long long d[kXD] = {};
+  int flags = 0;  // 1 NaN, 2 +inf, 4 -inf, 8 out of range
+
+  void add(double x) {
+    uint64_t bits;
+    std::memcpy(&bits, &x, 8);
+    const int ex = (int)((bits >> 52) & 0x7ff);
+    const uint64_t frac = bits & 0xfffffffffffffULL;
+    const bool neg = (bits >> 63) != 0;
+    if (ex == 0x7ff) {
+      flags |= frac ? 1 : (neg ? 4 : 2);
+      return;
+    }
+    uint64_t m = ex ? (frac | (1ULL << 52)) : frac;
+    int sft = (ex ? ex : 1) - 1075 - kXB0;
+    if (sft < 0) {
+      if (sft <= -64) return;
+      m >>= -sft;
+      sft = 0;
+    }
+    if (!m) return;
+    const int j = sft >> 5;
+    const unsigned __int128 v = (unsigned __int128)m << (sft & 31);
+    const uint64_t u[3] = {(uint64_t)v & 0xffffffffULL, (uint64_t)(v >> 32) & 0xffffffffULL, (uint64_t)(v >> 64)};
+    const int top = u[2] ? 2 : (u[1] ? 1 : 0);
+    if (j + top >= kXD) {
+      flags |= 8;
+      return;
+    }
+    for (int k = 0; k < 3 && j + k < kXD; ++k) d[j + k] += neg ? -(long long)u[k] : (long long)u[k];
+  }
+  void merge(const XSum& o) {
+    for (int i = 0; i < kXD; ++i) d[i] += o.d[i];
+    flags |= o.flags;
+  }
+  double round() const {
+    if (flags & (1 | 8)) return std::nan("");
+    if (flags & 2) return (flags & 4) ? std::nan("") : INFINITY;
+    if (flags & 4) return -INFINITY;
+    long long e[kXD + 1];
+    for (int i = 0; i < kXD; ++i) e[i] = d[i];
+    e[kXD] = 0;
+    auto carry = [&]() {
+      for (int i = 0; i < kXD; ++i) {
+        const long long c = e[i] >> 32;  // floor division by 2^32
+        e[i] -= c * 4294967296LL;
+        e[i + 1] += c;
+      }
+    };
+    carry();
+    const bool neg = e[kXD] < 0;
+    if (neg) {
+      for (int i = 0; i <= kXD; ++i) e[i] = -e[i];
+      carry();
+    }
+    int h = -1;
+    for (int i = 0; i <= kXD; ++i)
+      if (e[i] != 0) h = i;
+    if (h < 0) return 0.0;
+    const uint64_t t2 = (uint64_t)e[h], t1 = h >= 1 ? (uint64_t)e[h - 1] : 0, t0 = h >= 2 ? (uint64_t)e[h - 2] : 0;
+    bool sticky = false;
+    for (int i = 0; i < h - 2; ++i) sticky = sticky || e[i] != 0;
+    const unsigned __int128 w = ((unsigned __int128)t2 << 64) | ((unsigned __int128)t1 << 32) | t0;
+    const int msb = 127 - __builtin_clzll(t2);  // t2 != 0
+    const int drop = msb - 52;
+    uint64_t mant = (uint64_t)(w >> drop);
+    const unsigned __int128 rem = w & ((((unsigned __int128)1) << drop) - 1);
+    const unsigned __int128 half = ((unsigned __int128)1) << (drop - 1);
+    if (rem > half || (rem == half && (sticky || (mant & 1)))) ++mant;
+    const double r = std::ldexp((double)mant, drop + 32 * (h - 2) + kXB0);
+    return neg ? -r : r;
+  }
+};
+
+// Natural logarithm from IEEE-exact operations only, so that it returns the same bits as
+// the CUDA product's: x = (1 + f) 2^k with 1 + f in [sqrt(1/2), sqrt(2)), f exact;
+// log(1 + f) = 2 atanh(s), s = f / (2 + f), = f - s (f - R) with R = sum_{i=1..11}
+// 2 s^(2i) / (2i + 1) in Horner form (the atanh reduction as in J.-M. Muller, "Elementary
+// Functions", ch. 11), and log 2 split in a 40-bit head and a tail.
+inline double abd_log(double x) {
+  if (!(x > 0.0)) return x == 0.0 ? -INFINITY : std::nan("");
+  if (std::isinf(x)) return x;
+  int k;
+  double m = std::frexp(x, &k);
+  if (m < 0.70710678118654752) {
+    m = m * 2.0;
+    k -= 1;
+  }
+  const double f = m - 1.0;
+  const double s = f / (2.0 + f);
+  const double z = s * s;
+  const double c[10] = {2.0 / 21.0, 2.0 / 19.0, 2.0 / 17.0, 2.0 / 15.0, 2.0 / 13.0,
+                        2.0 / 11.0, 2.0 / 9.0,  2.0 / 7.0,  2.0 / 5.0,  2.0 / 3.0};
+  double r = 2.0 / 23.0;
+  for (int i = 0; i < 10; ++i) r = r * z + c[i];
+  r = r * z;
+  const double ln2_hi = 0.6931471805592082, ln2_lo = 7.371002565167799e-13;  // ln2_hi: 40 bits
+  return (double)k * ln2_hi + (f - (s * (f - r) - (double)k * ln2_lo));
+}
+
 struct Oracle {
   int n, V, T, E;
   std::vector<int> voff, toff, eoff, tris, edges, fixed;
@@ -87,6 +194,8 @@ struct Oracle {
   std::vector<double> diag;       // [n][144]
   std::vector<double> off;        // [npairs][144], block (I,J) with I<J
   std::vector<int> ij;            // [npairs][2]
+  std::vector<int> pact;          // [npairs] active contacts
+  std::vector<int> adj_ptr, adj;  // per body (neighbour, pair, side), neighbours increasing
   // stats
   int stat_newton = 0, stat_lin = 0, stat_ls = 0, stat_pt = 0, stat_ee = 0, stat_vg = 0, stat_ij = 0,
       stat_active = 0;
@@ -345,19 +454,19 @@ inline double barrier(double d, const Params& P) {
   if (d < P.d2hat) {
     const double s = d / P.d2hat;
     const double t = s - 1.0;  // pow(s - 1, 2.0) as its correctly rounded value
-    return P.kappa * -(t * t) * std::log(s);
+    return P.kappa * -(t * t) * abd_log(s);
   }
   return 0.0;
 }
 inline double barrier_d1(double d, const Params& P) {
   if (d < P.d2hat)
-    return P.kappa * (P.d2hat - d) * (2.0 * std::log(d / P.d2hat) + (d - P.d2hat) / d) / (P.d2hat * P.d2hat);
+    return P.kappa * (P.d2hat - d) * (2.0 * abd_log(d / P.d2hat) + (d - P.d2hat) / d) / (P.d2hat * P.d2hat);
   return 0.0;
 }
 inline double barrier_d2(double d, const Params& P) {
   if (d < P.d2hat)
     return -P.kappa *
-           (2.0 * std::log(d / P.d2hat) + (d - P.d2hat) / d + (d - P.d2hat) * (2.0 / d + P.d2hat / (d * d))) /
+           (2.0 * abd_log(d / P.d2hat) + (d - P.d2hat) / d + (d - P.d2hat) * (2.0 / d + P.d2hat / (d * d))) /
            (P.d2hat * P.d2hat);
   return 0.0;
 }
@@ -512,6 +621,113 @@ bool contact_gh(int type, const V3 xs[4], const V3 rs[4], const Params& P, doubl
   return true;
 }
 
+// The same contact's gradient and Hessian as 5 rank-one terms (the form the assembly sums):
+//   H = sum_k coef[k] u_k u_k^T,  g = B' u_4,
+// u_k (24: the pair's first body, then its second) = W^T (D kron I3)^T q_k with q_k the
+// eigenvectors of the c-space Hessian of l^2 (q_4 = grad l^2), D = dc/dx (3x4, frozen
+// alpha, beta, gamma) and W the vertex weights [1, r_v].  Mathematically identical to
+// contact_gh (which follows the reference's matrix products); the assembly uses this form
+// and its operation order.  `swap`: the candidate's first vertex group (point / first edge)
+// belongs to the pair's second body.  out[456]: H_IJ (144), H_II (144), H_JJ (144), g (24).
+bool contact_terms(int type, const V3 xs[4], const V3 rs[4], int swap, const Params& P, double out[456]) {
+  Geo G = geometry(type, xs[0], xs[1], xs[2], xs[3]);
+  const bool valid = valid_root(type, G.beta, G.gamma);
+  double d2;
+  if (type == 0) {
+    const double l = signed_distance(G.e0, G.e1p, G.e2p);
+    d2 = l * l;
+  } else {
+    d2 = dot(G.e2p, G.e2p);
+  }
+  if (!(d2 < P.d2hat && valid)) return false;
+  const double l = signed_distance(G.e0, G.e1p, G.e2p);
+  const double e0pn = dot(G.e0, G.e0), e1pn = dot(G.e1p, G.e1p), e2pn = dot(G.e2p, G.e2p);
+  const double f12 = std::sqrt(1.0 + 4.0 * (e1pn / e2pn));
+  const double f02 = std::sqrt(1.0 + 4.0 * (e0pn / e2pn));
+  double lam[5];
+  lam[0] = -l / (2.0 * e1pn) * (1.0 + f12);
+  lam[1] = -l / (2.0 * e1pn) * (1.0 - f12);
+  lam[2] = -l / (2.0 * e0pn) * (1.0 + f02);
+  lam[3] = -l / (2.0 * e0pn) * (1.0 - f02);
+  double om[4];
+  for (int k = 0; k < 4; ++k) om[k] = lam[k] / (lam[k] - l / e2pn);
+  double q[5][9];
+  std::memset(q, 0, sizeof(q));
+  for (int k = 0; k < 2; ++k) {
+    V3 t = om[k] * G.e1p;
+    q[k][3] = G.e2p.x; q[k][4] = G.e2p.y; q[k][5] = G.e2p.z;
+    q[k][6] = t.x; q[k][7] = t.y; q[k][8] = t.z;
+  }
+  for (int k = 2; k < 4; ++k) {
+    V3 t = om[k] * G.e0;
+    q[k][0] = G.e2p.x; q[k][1] = G.e2p.y; q[k][2] = G.e2p.z;
+    q[k][6] = t.x; q[k][7] = t.y; q[k][8] = t.z;
+  }
+  {
+    V3 gl2 = G.e2p * l;
+    gl2 = {gl2.x / e2pn, gl2.y / e2pn, gl2.z / e2pn};
+    V3 q4 = (gl2 * 2.0) * l;
+    q[4][6] = q4.x; q[4][7] = q4.y; q[4][8] = q4.z;
+  }
+  for (int k = 0; k < 4; ++k) lam[k] = lam[k] * 2.0 * l;
+  lam[4] = 2.0;
+  double qn[5];
+  for (int k = 0; k < 5; ++k) {
+    double sq = 0.0;
+    for (int i = 0; i < 9; ++i) sq += q[k][i] * q[k][i];
+    qn[k] = sq;
+  }
+  const double Bp = barrier_d1(d2, P), Bpp = barrier_d2(d2, P);
+  double coef[5];
+  if (P.contact_psd == 1) {
+    for (int k = 0; k < 4; ++k) coef[k] = std::fmax(Bp * lam[k], 0.0) / qn[k];
+    coef[4] = std::fmax(Bp * 2.0 + Bpp * qn[4], 0.0) / qn[4];
+  } else {
+    const bool clamp = (type == 0) || P.psd_ee;
+    for (int k = 0; k < 4; ++k) coef[k] = Bp * (clamp ? std::fmax(lam[k], 0.0) : lam[k]) / qn[k];
+    coef[4] = Bp * 2.0 / qn[4] + Bpp;
+  }
+  const double al = G.alpha, be = G.beta, ga = G.gamma;
+  double D[3][4];
+  if (type == 0) {
+    const double t[3][4] = {{0.0, 1.0, -1.0, 0.0}, {0.0, -al, al - 1.0, 1.0}, {1.0, -be, be + ga - 1.0, -ga}};
+    std::memcpy(D, t, sizeof(D));
+  } else {
+    const double t[3][4] = {{-1.0, 1.0, 0.0, 0.0}, {al, -al, -1.0, 1.0}, {be - 1.0, -be, ga + 1.0, -ga}};
+    std::memcpy(D, t, sizeof(D));
+  }
+  double u[5][24];
+  for (int e = 0; e < 24; ++e) {
+    const int side = e / 12, m = (e % 12) / 3, c = e % 3;
+    const int group = side ^ swap;
+    const int v0 = type == 0 ? (group ? 1 : 0) : (group ? 2 : 0);
+    const int v1 = type == 0 ? (group ? 4 : 1) : (group ? 4 : 2);
+    double dw[3];
+    for (int i = 0; i < 3; ++i) {
+      double sacc = 0.0;
+      for (int v = v0; v < v1; ++v) {
+        const double w = m == 0 ? 1.0 : (m == 1 ? rs[v].x : (m == 2 ? rs[v].y : rs[v].z));
+        sacc += D[i][v] * w;
+      }
+      dw[i] = sacc;
+    }
+    for (int k = 0; k < 5; ++k) u[k][e] = dw[0] * q[k][c] + dw[1] * q[k][3 + c] + dw[2] * q[k][6 + c];
+  }
+  for (int e = 0; e < 456; ++e) {
+    double v = 0.0;
+    if (e < 432) {
+      const int blk = e / 144, r = (e % 144) / 12, c = e % 12;
+      const int ra = blk == 2 ? 12 + r : r;
+      const int cb = blk == 1 ? c : 12 + c;
+      for (int k = 0; k < 5; ++k) v += coef[k] * (u[k][ra] * u[k][cb]);
+    } else {
+      v = Bp * u[4][e - 432];
+    }
+    out[e] = v;
+  }
+  return true;
+}
+
 inline void fetch(const Oracle& o, const double* y, const Cand& c, int type, V3 xs[4], V3 rs[4]) {
   int ids[4];
   if (type == 0) {
@@ -636,68 +852,109 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
   o.g.assign(12 * n, 0.0);
   o.diag.assign(144 * n, 0.0);
   o.off.assign(144 * (size_t)m, 0.0);
-  std::vector<double> gb(12), Hb(144);
-  for (int b = 0; b < n; ++b) {
-    if (o.fixed[b]) continue;
-    inertia_gh(o, b, gb.data(), Hb.data());
-    for (int k = 0; k < 12; ++k) o.g[12 * b + k] += gb[k];
-    for (int k = 0; k < 144; ++k) o.diag[144 * b + k] += Hb[k];
+  o.pact.assign(m, 0);
+  // adjacency: body -> (neighbour, pair, side), neighbours increasing
+  o.adj_ptr.assign(n + 1, 0);
+  for (int q = 0; q < m; ++q) {
+    ++o.adj_ptr[L.ij[2 * q] + 1];
+    ++o.adj_ptr[L.ij[2 * q + 1] + 1];
   }
-  struct Res {
-    bool active;
-    double g[24], Hi[144], Hj[144], Hij[144];
+  for (int b = 0; b < n; ++b) o.adj_ptr[b + 1] += o.adj_ptr[b];
+  o.adj.assign(3 * (size_t)o.adj_ptr[n], 0);
+  {
+    std::vector<std::vector<std::array<int, 3>>> rows(n);
+    for (int q = 0; q < m; ++q) {
+      const int I = L.ij[2 * q], J = L.ij[2 * q + 1];
+      rows[I].push_back({J, q, 0});
+      rows[J].push_back({I, q, 1});
+    }
+    for (int b = 0; b < n; ++b) {
+      std::sort(rows[b].begin(), rows[b].end());
+      for (size_t k = 0; k < rows[b].size(); ++k)
+        for (int t = 0; t < 3; ++t) o.adj[3 * (size_t)(o.adj_ptr[b] + k) + t] = rows[b][k][t];
+    }
+  }
+  // contact terms of every active candidate
+  struct Act {
+    int pair;
+    double v[456];
   };
+  std::vector<Act> acts;
   int active = 0;
   for (int type = 0; type < 2; ++type) {
     const std::vector<Cand>& C = type == 0 ? L.pt : L.ee;
     const int nc = (int)C.size();
-    std::vector<Res> R(nc);
+    std::vector<Act> R(nc);
+    std::vector<char> on(nc, 0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int i = 0; i < nc; ++i) {
       V3 xs[4], rs[4];
       fetch(o, y, C[i], type, xs, rs);
-      double d2;
-      R[i].active = contact_gh(type, xs, rs, o.prm, d2, R[i].g, R[i].Hi, R[i].Hj, R[i].Hij);
+      const int swap = C[i].I != L.ij[2 * C[i].pair];
+      on[i] = contact_terms(type, xs, rs, swap, o.prm, R[i].v) ? 1 : 0;
+      R[i].pair = C[i].pair;
     }
-    for (int i = 0; i < nc; ++i) {
-      if (!R[i].active) continue;
-      ++active;
-      const int I = C[i].I, J = C[i].J, q = C[i].pair;
-      for (int k = 0; k < 12; ++k) {
-        o.g[12 * I + k] += R[i].g[k];
-        o.g[12 * J + k] += R[i].g[12 + k];
+    for (int i = 0; i < nc; ++i)
+      if (on[i]) {
+        acts.push_back(R[i]);
+        ++o.pact[R[i].pair];
+        ++active;
       }
-      for (int k = 0; k < 144; ++k) {
-        o.diag[144 * I + k] += R[i].Hi[k];
-        o.diag[144 * J + k] += R[i].Hj[k];
-      }
-      double* blk = &o.off[144 * (size_t)q];
-      if (I < J) {
-        for (int k = 0; k < 144; ++k) blk[k] += R[i].Hij[k];
-      } else {
-        for (int r = 0; r < 12; ++r)
-          for (int c = 0; c < 12; ++c) blk[c * 12 + r] += R[i].Hij[r * 12 + c];
+  }
+  // per pair: exact sums of its contacts, rounded (H_IJ, contributions to diag I / J, g I / J)
+  std::vector<double> pdiag(288 * (size_t)m, 0.0), pgrad(24 * (size_t)m, 0.0);
+  {
+    std::vector<std::vector<int>> by_pair(m);
+    for (size_t k = 0; k < acts.size(); ++k) by_pair[acts[k].pair].push_back((int)k);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int q = 0; q < m; ++q) {
+      if (by_pair[q].empty()) continue;
+      std::vector<XSum> acc(456);
+      for (int k : by_pair[q])
+        for (int e = 0; e < 456; ++e) acc[e].add(acts[k].v[e]);
+      for (int e = 0; e < 456; ++e) {
+        const double v = acc[e].round();
+        if (e < 144) o.off[144 * (size_t)q + e] = v;
+        else if (e < 432) pdiag[288 * (size_t)q + (e - 144)] = v;
+        else pgrad[24 * (size_t)q + (e - 432)] = v;
       }
     }
   }
-  // vertex-ground terms (vg_ipc.py:4-34)
-  for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
-    const int b = L.vg[k], v = L.vg[k + 1];
-    const double d = y[3 * v + 1] - o.prm.ground;
-    const double d2b = barrier_d2(d * d, o.prm), db = barrier_d1(d * d, o.prm);
-    const double th[4] = {1.0, o.x0[3 * v], o.x0[3 * v + 1], o.x0[3 * v + 2]};
-    for (int ii = 0; ii < 4; ++ii) {
-      o.g[12 * b + 3 * ii + 1] += ((d * 2.0) * th[ii]) * db;
-      for (int jj = 0; jj < 4; ++jj)
-        o.diag[144 * b + (3 * ii + 1) * 12 + 3 * jj + 1] += (((th[ii] * th[jj]) * d2b) * 4.0) * d * d;
-    }
-  }
-  // Dirichlet rows/columns of fixed bodies
+  // per body: inertia + vertex-ground terms + the rounded pair contributions, summed exactly
+  std::vector<std::vector<int>> vg_of(n);
+  for (size_t k = 0; k + 1 < L.vg.size(); k += 2) vg_of[L.vg[k]].push_back(L.vg[k + 1]);
+#pragma omp parallel for schedule(dynamic, 4)
   for (int b = 0; b < n; ++b) {
-    if (!o.fixed[b]) continue;
-    for (int k = 0; k < 12; ++k) o.g[12 * b + k] = 0.0;
-    for (int k = 0; k < 144; ++k) o.diag[144 * b + k] = (k % 13 == 0) ? 1.0 : 0.0;
+    if (o.fixed[b]) {
+      for (int k = 0; k < 12; ++k) o.g[12 * b + k] = 0.0;
+      for (int k = 0; k < 144; ++k) o.diag[144 * b + k] = (k % 13 == 0) ? 1.0 : 0.0;
+      continue;
+    }
+    std::vector<XSum> acc(156);
+    double gb[12], Hb[144];
+    inertia_gh(o, b, gb, Hb);
+    for (int k = 0; k < 144; ++k) acc[k].add(Hb[k]);
+    for (int k = 0; k < 12; ++k) acc[144 + k].add(gb[k]);
+    if (o.prm.ground_enabled && o.prm.enable_vg)  // vertex-ground terms (vg_ipc.py:4-34)
+      for (int v : vg_of[b]) {
+        const double d = y[3 * v + 1] - o.prm.ground;
+        const double d2b = barrier_d2(d * d, o.prm), db = barrier_d1(d * d, o.prm);
+        const double th[4] = {1.0, o.x0[3 * v], o.x0[3 * v + 1], o.x0[3 * v + 2]};
+        for (int ii = 0; ii < 4; ++ii) {
+          acc[144 + 3 * ii + 1].add(((d * 2.0) * th[ii]) * db);
+          for (int jj = 0; jj < 4; ++jj) acc[(3 * ii + 1) * 12 + 3 * jj + 1].add((((th[ii] * th[jj]) * d2b) * 4.0) * d * d);
+        }
+      }
+    for (int k = o.adj_ptr[b]; k < o.adj_ptr[b + 1]; ++k) {
+      const int q = o.adj[3 * (size_t)k + 1], side = o.adj[3 * (size_t)k + 2];
+      if (o.pact[q] <= 0) continue;
+      for (int e = 0; e < 144; ++e) acc[e].add(pdiag[288 * (size_t)q + 144 * side + e]);
+      for (int e = 0; e < 12; ++e) acc[144 + e].add(pgrad[24 * (size_t)q + 12 * side + e]);
+    }
+    for (int k = 0; k < 144; ++k) o.diag[144 * b + k] = acc[k].round();
+    for (int k = 0; k < 12; ++k) o.g[12 * b + k] = acc[144 + k].round();
   }
+  // pairs touching a fixed (Dirichlet) body have no coupling block
   for (int q = 0; q < m; ++q)
     if (o.fixed[L.ij[2 * q]] || o.fixed[L.ij[2 * q + 1]])
       std::fill(o.off.begin() + 144 * (size_t)q, o.off.begin() + 144 * (size_t)(q + 1), 0.0);
@@ -709,43 +966,48 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
 // abd.py:244) or PCG
 // ---------------------------------------------------------------------------------------
 double ddot(const std::vector<double>& a, const std::vector<double>& b) {
-  // fixed chunking: deterministic for any thread count
-  const size_t N = a.size(), CH = 4096, nch = (N + CH - 1) / CH;
-  std::vector<double> part(nch, 0.0);
-#pragma omp parallel for schedule(static)
-  for (long c = 0; c < (long)nch; ++c) {
-    double s = 0.0;
-    for (size_t i = c * CH; i < std::min(N, (c + 1) * CH); ++i) s += a[i] * b[i];
-    part[c] = s;
+  // exact sum of the products (order-independent), rounded once
+  const long N = (long)a.size();
+  XSum total;
+#pragma omp parallel
+  {
+    XSum part;
+#pragma omp for schedule(static) nowait
+    for (long i = 0; i < N; ++i) part.add(a[i] * b[i]);
+#pragma omp critical
+    total.merge(part);
   }
-  double s = 0.0;
-  for (double v : part) s += v;
-  return s;
+  return total.round();
 }
 
+// y = H x, block row by block row: the row of body b sums its diagonal block and the blocks
+// of its active pairs with free neighbours in increasing neighbour order, columns 0..5 and
+// 6..11 separately, then adds the two halves (the CUDA product's per-row order).
 void spmv(const Oracle& o, const std::vector<double>& xv, std::vector<double>& yv) {
-  const int n = o.n, m = (int)o.ij.size() / 2;
+  const int n = o.n;
   yv.assign(12 * n, 0.0);
 #pragma omp parallel for schedule(static)
   for (int b = 0; b < n; ++b)
     for (int r = 0; r < 12; ++r) {
-      double s = 0.0;
-      for (int c = 0; c < 12; ++c) s += o.diag[144 * b + r * 12 + c] * xv[12 * b + c];
-      yv[12 * b + r] = s;
-    }
-  for (int q = 0; q < m; ++q) {
-    const int I = o.ij[2 * q], J = o.ij[2 * q + 1];
-    const double* B = &o.off[144 * (size_t)q];
-    for (int r = 0; r < 12; ++r) {
-      double s = 0.0, t = 0.0;
-      for (int c = 0; c < 12; ++c) {
-        s += B[r * 12 + c] * xv[12 * J + c];
-        t += B[c * 12 + r] * xv[12 * I + c];
+      double acc[2];
+      for (int h = 0; h < 2; ++h) {
+        double a = 0.0;
+        for (int c = 0; c < 6; ++c) a += o.diag[144 * b + r * 12 + 6 * h + c] * xv[12 * b + 6 * h + c];
+        if (!o.fixed[b])
+          for (int k = o.adj_ptr[b]; k < o.adj_ptr[b + 1]; ++k) {
+            const int J = o.adj[3 * (size_t)k], q = o.adj[3 * (size_t)k + 1], side = o.adj[3 * (size_t)k + 2];
+            if (o.pact[q] <= 0 || o.fixed[J]) continue;
+            const double* B = &o.off[144 * (size_t)q];
+            for (int c = 0; c < 6; ++c) {
+              const int col = 6 * h + c;
+              const double O = side == 0 ? B[r * 12 + col] : B[col * 12 + r];
+              a += O * xv[12 * J + col];
+            }
+          }
+        acc[h] = a;
       }
-      yv[12 * I + r] += s;
-      yv[12 * J + r] += t;
+      yv[12 * b + r] = acc[0] + acc[1];
     }
-  }
 }
 
 // inverse of a 12x12 block by Gauss-Jordan with partial pivoting
@@ -923,7 +1185,10 @@ int solve(Oracle& o) {
     for (it = 1; it <= o.prm.cg_max_iter; ++it) {
       spmv(o, pv, Ap);
       const double pAp = ddot(pv, Ap);
-      if (!(pAp > 0.0)) break;
+      if (!(pAp > 0.0)) {  // non-positive curvature: stop before this iteration's update
+        --it;
+        break;
+      }
       const double alpha = rz / pAp;
       for (int i = 0; i < N; ++i) {
         x[i] += alpha * pv[i];
@@ -945,7 +1210,10 @@ int solve(Oracle& o) {
   double rho_old = 1.0, alpha = 1.0, omega = 1.0;
   for (it = 1; it <= o.prm.cg_max_iter; ++it) {
     const double rho = ddot(rh, r);
-    if (rho == 0.0 || !std::isfinite(rho)) break;
+    if (rho == 0.0 || !std::isfinite(rho)) {  // breakdown: stop before this iteration
+      --it;
+      break;
+    }
     if (it == 1) {
       pv = r;
     } else {
@@ -1181,35 +1449,37 @@ void update_q(Oracle& o, double alpha) {
   }
 }
 
+// barrier energies of the candidates and the vertex-ground pairs plus inertia, summed
+// exactly (compute_energy, abd.py:133-141)
 double energy_at(Oracle& o, const double* y, const double* Akp, const double* pkp) {
   Boxes bx;
   Lists L;
   static_boxes(o, y, bx);
   cull(o, bx, L);
-  double ec = 0.0;
+  XSum total;
   for (int type = 0; type < 2; ++type) {
     const std::vector<Cand>& C = type == 0 ? L.pt : L.ee;
     const int nc = (int)C.size();
-    std::vector<double> e(nc);
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < nc; ++i) {
-      V3 xs[4], rs[4];
-      fetch(o, y, C[i], type, xs, rs);
-      e[i] = contact_energy(type, xs, o.prm);
+#pragma omp parallel
+    {
+      XSum part;
+#pragma omp for schedule(static) nowait
+      for (int i = 0; i < nc; ++i) {
+        V3 xs[4], rs[4];
+        fetch(o, y, C[i], type, xs, rs);
+        part.add(contact_energy(type, xs, o.prm));
+      }
+#pragma omp critical
+      total.merge(part);
     }
-    if (g_reverse_sums)
-      for (int i = nc - 1; i >= 0; --i) ec += e[i];
-    else
-      for (int i = 0; i < nc; ++i) ec += e[i];
   }
   for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
     const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
-    ec += barrier(d * d, o.prm);
+    total.add(barrier(d * d, o.prm));
   }
-  double ei = 0.0;
   for (int b = 0; b < o.n; ++b)
-    if (!o.fixed[b]) ei += inertia_energy(o, b, Akp, pkp);
-  return ec + ei;
+    if (!o.fixed[b]) total.add(inertia_energy(o, b, Akp, pkp));
+  return total.round();
 }
 
 double compute_energy(Oracle& o, double alpha) {
@@ -1358,7 +1628,6 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
 void orc_destroy(void* h) { delete (Oracle*)h; }
 void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
 void orc_set_threads(int t) { omp_set_num_threads(t); }
-void orc_set_reverse_sums(int r) { g_reverse_sums = r; }
 int orc_max_threads() { return omp_get_max_threads(); }
 
 void orc_set_state(void* h, const double* A0, const double* p0, const double* Adot, const double* pdot,
@@ -1483,6 +1752,25 @@ int orc_contact_gh(int type, const double* xs12, const double* rs12, const Param
     rs[k] = {rs12[3 * k], rs12[3 * k + 1], rs12[3 * k + 2]};
   }
   return contact_gh(type, xs, rs, *prm, *d2, g24, Hi, Hj, Hij) ? 1 : 0;
+}
+
+// rank-one form of the same pair's terms (swap = 0): out[456] = H_IJ, H_II, H_JJ, g
+int orc_contact_terms(int type, const double* xs12, const double* rs12, const Params* prm, double* out) {
+  V3 xs[4], rs[4];
+  for (int k = 0; k < 4; ++k) {
+    xs[k] = {xs12[3 * k], xs12[3 * k + 1], xs12[3 * k + 2]};
+    rs[k] = {rs12[3 * k], rs12[3 * k + 1], rs12[3 * k + 2]};
+  }
+  return contact_terms(type, xs, rs, 0, *prm, out) ? 1 : 0;
+}
+
+double orc_log(double x) { return abd_log(x); }
+
+// exact sum of n values, rounded once
+double orc_exact_sum(const double* v, long n) {
+  XSum s;
+  for (long i = 0; i < n; ++i) s.add(v[i]);
+  return s.round();
 }
 
 double orc_contact_energy(int type, const double* xs12, const Params* prm) {

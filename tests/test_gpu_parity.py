@@ -1,10 +1,13 @@
 """GPU parity: libabd_b200.so (through the C ABI, via the Python mirror) against the CPU
 oracle on the same seeded scenes and states.
 
-Bars: bit-exact for vertex transforms and culled pair sets (compared as sorted sets),
-relative 1e-10 for assembled gradients / Hessian blocks, 1e-12 for energies and times of
-impact, and 1e-9 relative on positions after whole time steps with equal Newton iteration
-counts (plain FP64)."""
+Bar: bit for bit.  Vertex transforms, culled pair sets (compared as sorted sets), the
+assembled gradient and Hessian blocks, energies, times of impact, linear solves and whole
+time steps (positions, velocities and the iteration counts of Newton, the Krylov solver and
+the line search) are identical.  Both sides compute every term with the same operation
+order (no FMA contraction), sum every reduction exactly with a single rounding, and use
+the same IEEE-exact logarithm, so the order in which the GPU's threads deliver the terms
+does not reach the result."""
 import numpy as np
 import pytest
 
@@ -122,14 +125,12 @@ def test_gradient_hessian(scene_state):
     ref = o.gh(A, p)
     got = sim.gradient_hessian(torch.as_tensor(A, device="cuda"), torch.as_tensor(p, device="cuda"))
     assert got["n_active"] == ref["n_active"]
-    g, gr = got["g"].cpu().numpy(), ref["g"]
-    assert np.abs(g - gr).max() <= 1e-10 * np.abs(gr).max()
-    D, Dr = got["diag"].cpu().numpy(), ref["diag"]
-    assert np.abs(D - Dr).max() <= 1e-10 * np.abs(Dr).max()
+    np.testing.assert_array_equal(got["g"].cpu().numpy(), ref["g"])
+    np.testing.assert_array_equal(got["diag"].cpu().numpy(), ref["diag"])
     np.testing.assert_array_equal(got["ij"].cpu().numpy(), ref["ij"])
-    if len(ref["off"]):
-        O, Or = got["off"].cpu().numpy(), ref["off"]
-        assert np.abs(O - Or).max() <= 1e-10 * max(np.abs(Or).max(), np.abs(Dr).max())
+    np.testing.assert_array_equal(got["off"].cpu().numpy(), ref["off"])
+    if name == "pile_ground":
+        assert ref["n_active"] > 0  # the bodies rest on the ground and on each other
 
 
 def test_energy(scene_state):
@@ -140,7 +141,7 @@ def test_energy(scene_state):
         pk = st["p0"] + a * prm.dt * st["pdot"]
         e_ref = o.energy(Ak, pk)
         e = sim.compute_energy(torch.as_tensor(Ak, device="cuda"), torch.as_tensor(pk, device="cuda"))
-        assert e == pytest.approx(e_ref, rel=1e-12, abs=1e-300)
+        assert e == e_ref, (a, e, e_ref)
 
 
 def test_ccd(scene_state):
@@ -152,14 +153,13 @@ def test_ccd(scene_state):
         a_ref, raw_ref = o.ccd(st["A0"], st["p0"], A1, p1)
         cu = lambda v: torch.as_tensor(v, device="cuda")
         a, raw = sim.ccd(cu(st["A0"]), cu(st["p0"]), cu(A1), cu(p1))
-        assert raw == pytest.approx(raw_ref, rel=1e-12, abs=1e-15)
-        assert a == pytest.approx(a_ref, rel=1e-12, abs=1e-15)
+        assert raw == raw_ref and a == a_ref, (scale, raw, raw_ref)
 
 
 @pytest.mark.parametrize("solver", [0, 1])
 def test_solve(scene_state, solver):
-    """Same system, same contact clusters: the solutions agree to the FP64 conditioning floor
-    of the stiff contact system (cond ~ 1e10, so ~1e-5 relative), iteration counts closely."""
+    """Same system, same contact clusters, exact dot products and the same SpMV and
+    preconditioner order: identical iterates, so the same solution and iteration count."""
     name, bodies, prm0, o, st, sim = scene_state
     import dataclasses
     import torch
@@ -174,48 +174,40 @@ def test_solve(scene_state, solver):
         dq0 = np.zeros((len(bodies), 12))
         dq_ref, it_ref = o.solve(dq0)
         dq, it = sim.solve(torch.as_tensor(dq0, device="cuda"))
-        dq = dq.cpu().numpy()
-        rel = np.abs(dq - dq_ref).max() / max(np.abs(dq_ref).max(), 1e-300)
-        print(f"{name} solver={solver} rel dq diff {rel:.2e} iters {it} / {it_ref}")
-        assert rel <= 1e-4
-        assert abs(it - it_ref) <= 2
+        assert it == it_ref
+        np.testing.assert_array_equal(dq.cpu().numpy(), dq_ref)
     finally:
         sim.set_params(prm0)
         o.set_params(prm0)
 
 
-@pytest.mark.parametrize("case", ["c0", "pile"])
-def test_step_parity(case):
-    """Whole steps against the oracle: equal Newton counts and positions within 1e-6 relative
-    over 40 steps.  Free-flight steps agree to rounding; contact steps are bounded by the
-    conditioning of the stiff contact solve (truncated Newton carries the last step's
-    ~cond*eps relative difference), so the bar is 1e-6, not 1e-9."""
+@pytest.mark.parametrize("case,nsteps", [("c0", 200), ("pile", 60)])
+def test_step_parity(case, nsteps):
+    """Whole time steps against the oracle, bit for bit: positions, velocities, the dq warm
+    start and every iteration count, at every step (c0: the two-cube configuration for its
+    200 steps; pile: 8 bodies on the ground box, 60 steps through landing and contact)."""
     if case == "c0":
         bodies, prm, _ = scenes.make_config(0)
     else:
         bodies, prm = scenes.small_pile(2, 2, seed=7)
-    nsteps = 40
     o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
     sim = _sim(bodies, prm)
-    worst = 0.0
+    active = 0
     try:
         for s in range(nsteps):
             ri = o.step()
             gi = sim.step()
-            assert gi["status"] & ~16 == 0, gi
-            assert gi["newton_iters"] == ri["newton_iters"], (s, gi, ri)
+            assert gi["status"] == 0, (s, gi)
+            for k in ("newton_iters", "linear_iters", "ls_trials", "n_active"):
+                assert gi[k] == ri[k], (s, k, gi, ri)
+            assert gi["energy"] == ri["energy"], (s, gi["energy"], ri["energy"])
             st = o.get_state()
-            p = sim.states.p0.cpu().numpy()
-            A = sim.states.A0.cpu().numpy()
-            scale = max(1.0, np.abs(st["p0"]).max())
-            err = max(np.abs(p - st["p0"]).max() / scale, np.abs(A - st["A0"]).max())
-            worst = max(worst, err)
-            if s < 2:
-                assert err <= 1e-12, (s, err)  # free flight: rounding level
-            assert err <= 1e-6, (s, err)
-        xv = sim.x_view.cpu().numpy()
-        assert np.abs(xv - st["x_view"]).max() <= 1e-6 * max(1.0, np.abs(st["x_view"]).max())
-        print(f"{case}: worst relative position difference over {nsteps} steps {worst:.2e}")
+            for k in ("A0", "p0", "Adot", "pdot"):
+                np.testing.assert_array_equal(getattr(sim.states, k).cpu().numpy(), st[k], err_msg=f"step {s} {k}")
+            np.testing.assert_array_equal(sim.dq.cpu().numpy(), st["dq"], err_msg=f"step {s} dq")
+            active += ri["n_active"]
+        np.testing.assert_array_equal(sim.x_view.cpu().numpy(), st["x_view"])
+        assert active > 0  # the trajectory went through contact
     finally:
         sim.close()
 
