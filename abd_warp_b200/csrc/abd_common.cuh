@@ -25,6 +25,7 @@ enum : int {
   ST_NAN = 32,             // non-finite value in the Newton system
   ST_VG_OVERFLOW = 64,     // VG list capacity exceeded
   ST_ACT_OVERFLOW = 128,   // active-pair list capacity exceeded (host grows and reruns)
+  ST_CONTACT_OVERFLOW = 256,  // active-contact list capacity exceeded (host grows and reruns)
 };
 
 constexpr int kTraversalStack = 64;
@@ -186,7 +187,9 @@ struct Sim {
 
   // positions
   double *x = nullptr, *xk = nullptr;
-  Box* body_box = nullptr;  // [n]
+  Box* body_box = nullptr;  // [n] FP32 body boxes of the last pass (written by the pair mask)
+  unsigned long long* body_bnd = nullptr;  // [n][12] exact bounds as max-keys (broad phase)
+  int swept = 0;            // the last broad phase was swept
 
   // body pairs
   int W = 0;                       // mask words per row
@@ -207,8 +210,7 @@ struct Sim {
   // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
-  double* chunk_val = nullptr;     // [nch] minimum time of impact
-  XSum* chunk_acc = nullptr;  // [nch] exact barrier-energy sums
+  XSum* energy_acc = nullptr;      // exact energy of the last energy pass
 
   // candidate lists
   int cap_pt = 0, cap_ee = 0, cap_vg = 0;
@@ -220,9 +222,13 @@ struct Sim {
   double *pdiag = nullptr;         // [cap_pairs][2][144]: contributions to diag I, diag J
   double *pgrad = nullptr;         // [cap_pairs][2][12]
   int* pair_active = nullptr;      // [cap_pairs] active contacts of the pair
+  // active contacts of the GH pass: int4 (pair, type | swap << 1, primitive a, primitive b),
+  // appended in any order, then grouped by pair (pair_cand[4p]: offset, count, fill)
+  int cap_contacts = 0;
+  int4 *contacts = nullptr, *contacts_by_pair = nullptr;
+  int list_counts[4] = {0, 0, 0, 0};  // pairs, PT, EE, VG of the last list culling
   double* pair_val = nullptr;      // [cap_pairs] energy or toi per pair
-  double* body_val = nullptr;      // [n] minimum time of impact (vertex-ground)
-  XSum* body_acc = nullptr; // [n] exact inertia + vertex-ground energy sums
+
 
   // Newton system
   double *g = nullptr, *dq = nullptr, *diag = nullptr, *Minv = nullptr;  // [n][12], [n][144]
@@ -245,7 +251,7 @@ struct Sim {
   void* hstage = nullptr;          // pinned staging of the preconditioner's cluster tables
   size_t cap_hstage = 0;
   double* hval = nullptr;          // pinned host scalars
-  unsigned long long* dmin = nullptr;  // device min accumulators
+  unsigned long long* dmin = nullptr;  // [0]: complemented bits of the last CCD pass's minimum
 };
 
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
@@ -264,6 +270,7 @@ enum : int {
   DS_NPAIRS = 7,     // body pairs of the last culling pass
   DS_NADJ = 8,       // adjacency entries (2 x pairs)
   DS_NACTP = 9,      // active pairs appended by pair_weights
+  DS_NCONTACT = 12,  // active contacts appended by the GH pass
   DS_NSLOTS = 16
 };
 
@@ -292,16 +299,15 @@ cudaError_t rest_boxes(Sim& s);
 enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS = 3 };
 // A != null: internal node boxes are the affine images of the rest boxes under (A, p) (united
 // with (A1, p1) when swept); A == null: the refit boxes.  y0 / y1 are the positions.
+// ENERGY (at DOFs A, p; st for the inertia terms) adds the pass's whole energy -- contacts,
+// vertex-ground and inertia -- to energy_acc; CCD (at DOFs) maximises dmin[0] with the
+// complemented bits of every time of impact below 1 (contacts and vertex-ground).
 cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
-                   const double* y0, const double* y1);
+                   const double* y0, const double* y1, const abd_states* st = nullptr);
 cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y);
-cudaError_t body_energy(Sim& s, const abd_states& st, const double* Ak, const double* pk, const double* y);
-cudaError_t body_vg_toi(Sim& s, const double* y0, const double* y1);
 cudaError_t vg_list(Sim& s, const double* y0);
-cudaError_t sum_energy(Sim& s, double* out_dev);
 // active pairs with their coupling weights (device list + count in dstat DS_NACTP)
 cudaError_t pair_weights(Sim& s);
-cudaError_t min_toi(Sim& s, double* out_dev);
 cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
                         double* pout);

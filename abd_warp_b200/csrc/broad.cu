@@ -32,65 +32,147 @@ __global__ void k_transform(int V, const int* __restrict__ vbody, const double* 
 }
 
 // ---------------------------------------------------------------------------------------
+// body bounds as order-preserving 64-bit keys, maximised atomically (exact, any order):
+// bnd[12 b + k] = key(-lo0_k), key(hi0_k), key(-lo1_k), key(hi1_k) for k = 0..2 (y0, then
+// y1 when swept); 0 = no vertex
+// ---------------------------------------------------------------------------------------
+__device__ inline unsigned long long max_key(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
+}
+__device__ inline double key_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffULL) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// The FP32 body box of the reference (culling2.py:278-334): FP64 min / max of the vertices,
+// dilated by dhat / 2 in FP64 and rounded to FP32; swept boxes add the undilated FP32 box
+// of the end positions.
+__device__ inline Box body_box_of(const unsigned long long* k, bool swept, double dhh) {
+  Box B;
+  B.pad0 = B.pad1 = 0.f;
+  if (k[3] == 0) {  // no vertex
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      B.lo[j] = INFINITY;
+      B.hi[j] = -INFINITY;
+    }
+    return B;
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    B.lo[j] = (float)(-key_value(k[j]) - dhh);
+    B.hi[j] = (float)(key_value(k[3 + j]) + dhh);
+    if (swept) {
+      B.lo[j] = fminf(B.lo[j], (float)(-key_value(k[6 + j])));
+      B.hi[j] = fmaxf(B.hi[j], (float)key_value(k[9 + j]));
+    }
+  }
+  return B;
+}
+
+// One thread per vertex: y0 = x(A, p) (and y1 = x(A1, p1)) with the arithmetic of k_transform,
+// and the body bounds: lanes of a warp that share a body reduce their keys, one lane per
+// (warp, body) updates the body's keys atomically.
+__global__ void __launch_bounds__(256) k_vertex_broad(int V, const int* __restrict__ vbody,
+                                                      const double* __restrict__ x0, const double* __restrict__ A,
+                                                      const double* __restrict__ p, const double* __restrict__ A1,
+                                                      const double* __restrict__ p1, double* y0, double* y1,
+                                                      unsigned long long* bnd) {
+  const int v = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
+  const bool live = v < V;
+  const int b = live ? vbody[v] : -1;
+  unsigned long long key[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) key[k] = 0;
+  if (live) {
+    const double r0 = x0[3 * v], r1 = x0[3 * v + 1], r2 = x0[3 * v + 2];
+    const double* m = A + 9 * b;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double y = ((m[j] * r0 + m[3 + j] * r1) + m[6 + j] * r2) + p[3 * b + j];
+      y0[3 * v + j] = y;
+      key[j] = max_key(-y);
+      key[3 + j] = max_key(y);
+    }
+    if (A1) {
+      const double* m1 = A1 + 9 * b;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double z = ((m1[j] * r0 + m1[3 + j] * r1) + m1[6 + j] * r2) + p1[3 * b + j];
+        y1[3 * v + j] = z;
+        key[6 + j] = max_key(-z);
+        key[9 + j] = max_key(z);
+      }
+    }
+  }
+  // segmented reduction: one round per distinct body in the warp (bodies are contiguous)
+  unsigned pending = __ballot_sync(0xffffffffu, live);
+  const int nk = A1 ? 12 : 6;
+  while (pending) {
+    const int lead = __ffs(pending) - 1;
+    const int bl = __shfl_sync(0xffffffffu, b, lead);
+    const bool mine = live && b == bl;
+    pending &= ~__ballot_sync(0xffffffffu, mine);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      if (k >= nk) break;
+      unsigned long long x = mine ? key[k] : 0ULL;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+        x = y > x ? y : x;
+      }
+      if (lane == lead) atomicMax(&bnd[12 * (size_t)bl + k], x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // body pairs: overlap bit matrix, per-row prefix counts, then O(1) placement of every pair
 // ---------------------------------------------------------------------------------------
-constexpr int PR_ROWS = 4;      // rows per CTA of k_pair_mask (one warp each for the row scan)
-constexpr int PR_THREADS = 32 * PR_ROWS;
-constexpr int PR_TILE = 1024;   // body boxes staged in shared memory per tile
+constexpr int PR_THREADS = 256;  // one warp per row of the overlap matrix
+constexpr int PR_TILE = 1024;    // body boxes staged in shared memory per tile (32 KB)
 
-// Bit (I, J) of the overlap matrix (word w covers J in [32w, 32w + 32)), the per-row
-// exclusive prefix of the word popcounts (wpre), and the row counts: all neighbours (rcnt)
-// and neighbours J > I (ucnt), ready for the scan.
-__global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const Box* __restrict__ body_box,
-                                                          uint32_t* mask, int* wpre, int* rcnt, int* ucnt) {
+// Row I of the overlap matrix, one warp: lane l tests J = 32 w + l and the ballot is word w
+// (word w covers J in [32w, 32w + 32)).  The warp also keeps the per-row exclusive prefix
+// of the word popcounts (wpre) and the row counts: all neighbours (rcnt) and neighbours
+// J > I (ucnt), ready for the scan.  Every CTA builds the FP32 boxes of all bodies from the
+// bounds in shared memory (tile by tile) and stores those of its own rows in body_box.
+__global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const unsigned long long* __restrict__ bnd,
+                                                          int swept, double dhh, Box* body_box, uint32_t* mask,
+                                                          int* wpre, int* rcnt, int* ucnt) {
   __shared__ Box tile[PR_TILE];
-  __shared__ Box rows[PR_ROWS];
-  const int I0 = blockIdx.x * PR_ROWS;
-  if (threadIdx.x < PR_ROWS && I0 + (int)threadIdx.x < n) rows[threadIdx.x] = load_box(&body_box[I0 + threadIdx.x]);
+  const int I = (int)((blockIdx.x * (unsigned)PR_THREADS + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  const bool row = I < n;
+  Box a;
+  if (row) {
+    a = body_box_of(bnd + 12 * (size_t)I, swept, dhh);
+    if (lane == 0) store_box(&body_box[I], a);
+  }
+  int pre = 0, low = 0;
   for (int j0 = 0; j0 < n; j0 += PR_TILE) {
     const int jn = min(PR_TILE, n - j0);
     __syncthreads();
-    for (int k = threadIdx.x; k < jn; k += PR_THREADS) tile[k] = load_box(&body_box[j0 + k]);
+    for (int k = threadIdx.x; k < jn; k += PR_THREADS) tile[k] = body_box_of(bnd + 12 * (size_t)(j0 + k), swept, dhh);
     __syncthreads();
-    const int words = (jn + 31) / 32;
-    for (int it = threadIdx.x; it < PR_ROWS * words; it += PR_THREADS) {
-      const int r = it / words, wl = it % words, I = I0 + r;
-      if (I >= n) continue;
-      const Box a = rows[r];
-      uint32_t bits = 0;
-      const int jl0 = 32 * wl, jl1 = min(jn, jl0 + 32);
-      for (int jl = jl0; jl < jl1; ++jl) {
-        if (j0 + jl == I) continue;
-        if (overlap(a, tile[jl])) bits |= 1u << (jl - jl0);
+    if (!row) continue;
+    for (int wl = 0; wl < (jn + 31) / 32; ++wl) {
+      const int jl = 32 * wl + lane, J = j0 + jl;
+      const bool hit = jl < jn && J != I && overlap(a, tile[jl]);
+      const uint32_t bits = __ballot_sync(0xffffffffu, hit);
+      const int w = (j0 >> 5) + wl;
+      if (lane == 0) {
+        mask[(size_t)I * W + w] = bits;
+        wpre[(size_t)I * W + w] = pre;
       }
-      const size_t w = (size_t)I * W + (j0 >> 5) + wl;
-      mask[w] = bits;
-      wpre[w] = __popc(bits);
+      if (w == (I >> 5)) low = pre + __popc(bits & ((1u << (I & 31)) - 1u));
+      pre += __popc(bits);
     }
   }
-  __syncthreads();  // this CTA's mask rows are complete
-  const int lane = threadIdx.x & 31, I = I0 + (int)(threadIdx.x >> 5);
-  if (I >= n) return;
-  int* row = wpre + (size_t)I * W;
-  int carry = 0;
-  for (int w0 = 0; w0 < W; w0 += 32) {
-    const int w = w0 + lane;
-    const int c = w < W ? row[w] : 0;
-    int x = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (w < W) row[w] = carry + x - c;
-    carry += __shfl_sync(0xffffffffu, x, 31);
-  }
-  __syncwarp();
-  if (lane == 0) {
-    const int wI = I >> 5, b = I & 31;
-    const int low = row[wI] + (b ? __popc(mask[(size_t)I * W + wI] & ((1u << b) - 1u)) : 0);
-    rcnt[I] = carry;
-    ucnt[I] = carry - low;  // bit I itself is never set
+  if (row && lane == 0) {
+    rcnt[I] = pre;
+    ucnt[I] = pre - low;  // bit I itself is never set
   }
 }
 
@@ -197,7 +279,7 @@ struct BroadArgs {
   const double *A, *p, *A1, *p1;
   double *y0, *y1;
   double dhh;
-  Box* body_box;
+  unsigned long long* bnd;
   const int *tri_leaf, *edge_leaf;
   Box *tri_box, *edge_box;
   const int *tri_child, *edge_child, *tri_order, *edge_order, *tri_lvl, *edge_lvl, *tri_blvl, *edge_blvl;
@@ -283,8 +365,7 @@ __global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
       red[9 + j][warp] = hi1[j];
     }
   __syncthreads();  // also makes this CTA's y0 / y1 writes visible to all its threads
-  if (threadIdx.x == 0) {
-    Box B;
+  if (threadIdx.x == 0 && v1 > v0) {
     for (int j = 0; j < 3; ++j) {
       double l = red[j][0], h = red[3 + j][0], l1 = red[6 + j][0], h1 = red[9 + j][0];
       for (int w = 1; w < BB / 32; ++w) {
@@ -293,14 +374,13 @@ __global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
         l1 = fmin(l1, red[6 + j][w]);
         h1 = fmax(h1, red[9 + j][w]);
       }
-      B.lo[j] = (float)(l - a.dhh);
-      B.hi[j] = (float)(h + a.dhh);
+      a.bnd[12 * b + j] = max_key(-l);
+      a.bnd[12 * b + 3 + j] = max_key(h);
       if (swept) {
-        B.lo[j] = fminf(B.lo[j], (float)l1);
-        B.hi[j] = fmaxf(B.hi[j], (float)h1);
+        a.bnd[12 * b + 6 + j] = max_key(-l1);
+        a.bnd[12 * b + 9 + j] = max_key(h1);
       }
     }
-    store_box(&a.body_box[b], B);
   }
   // given positions only: leaf boxes (the narrow phase computes them on the fly otherwise)
   if (!a.refit) return;
@@ -343,7 +423,7 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
   a.y0 = y0;
   a.y1 = y1;
   a.dhh = s.prm.dhat * 0.5;
-  a.body_box = s.body_box;
+  a.bnd = s.body_bnd;
   a.tri_leaf = s.tri_tree.prim_leaf;
   a.edge_leaf = s.edge_tree.prim_leaf;
   a.tri_box = s.tri_tree.box;
@@ -357,7 +437,15 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
   a.tri_blvl = s.tri_tree.body_lvl;
   a.edge_blvl = s.edge_tree.body_lvl;
   a.refit = !(A && (!y1 || A1));
-  k_body_broad<<<s.n, BB, 0, s.stream>>>(a);
+  s.swept = y1 != nullptr;
+  cudaError_t e = cudaMemsetAsync(s.body_bnd, 0, sizeof(unsigned long long) * 12 * (size_t)s.n, s.stream);
+  if (e != cudaSuccess) return e;
+  if (a.refit) {
+    k_body_broad<<<s.n, BB, 0, s.stream>>>(a);
+  } else {
+    if (s.V == 0) return cudaSuccess;
+    k_vertex_broad<<<blocks(s.V, 256), 256, 0, s.stream>>>(s.V, s.vbody, s.x0, A, p, A1, p1, y0, y1, s.body_bnd);
+  }
   ++s.launches;
   return cudaGetLastError();
 }
@@ -384,8 +472,8 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
 // leaves the lists incomplete, for the host to grow and rerun at its next read of dstat.
 cudaError_t body_pairs(Sim& s) {
   const int n = s.n, W = s.W;
-  k_pair_mask<<<blocks(n, PR_ROWS), PR_THREADS, 0, s.stream>>>(n, W, s.body_box, s.pair_mask, s.pair_wpre,
-                                                               s.row_ptr, s.upper_ptr);
+  k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(
+      n, W, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box, s.pair_mask, s.pair_wpre, s.row_ptr, s.upper_ptr);
   k_pair_scan<<<1, 1024, 0, s.stream>>>(n, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj, s.dstat);
   k_pair_fill<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.pair_wpre, s.row_ptr,
                                                                    s.upper_ptr, s.cap_pairs, s.cap_adj, s.ij,

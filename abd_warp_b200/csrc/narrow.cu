@@ -40,8 +40,14 @@ struct NarrowArgs {
   const int *row_ptr, *adj_col;
   const Box* body_box;
   const int2* chunk;
-  double* chunk_val;
-  XSum* chunk_acc;
+  const int* adj_pair;
+  int cap_contacts;
+  int4 *contacts, *contacts_by_pair;
+  XSum* energy;                       // exact energy of the pass
+  unsigned long long* toi_key;        // complemented bits of the minimum time of impact
+  abd_states st;
+  const double *mass, *I0;
+  const int* fixed;
   const int *voff, *toff, *eoff, *tris, *edges;
   const double *y0, *y1, *x0;
   const double *A, *p, *A1, *p1;  // DOFs of y0 / y1 (affine node boxes), or null
@@ -247,17 +253,15 @@ __device__ inline int block_scan(int v, int* sh, int& excl) {
   return total;
 }
 
-// One CTA per body pair (grid = pair capacity): candidate lists, and for GH the pair's
-// contact assembly.  MODE is a template parameter so that the list pass is not held to the
-// register budget of the assembly.
-template <int MODE>
-__global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
+// Candidate lists (the reference's vec5i PT / EE lists, culling.py:85-99): one CTA per body
+// pair (grid = pair capacity), each pair a contiguous segment in traversal order.
+__global__ void __launch_bounds__(NT) k_pair_lists(NarrowArgs a) {
   const int p = blockIdx.x;
   // pair count of this pass (device); an overflowed pass is rerun by the host
   if (p >= a.dstat[DS_NPAIRS] || (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW)) return;
   PairInfo P = pair_info(a, p);
   const int items = P.nPT1 + P.nPT2 + P.nEE;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   __shared__ int sh[NW + 1];
   __shared__ float sdof[2][2][12];  // [I, J][y0, y1][A row-major, p]
   if (a.affine) {
@@ -302,7 +306,6 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
   }
   __syncthreads();
   if (!ok) {
-    if (tid == 0 && MODE == NARROW_GH) a.pair_active[p] = 0;
     return;
   }
   {
@@ -319,96 +322,126 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
         row[4] = type == 0 ? pb - a.toff[bJ] : pb - a.eoff[bJ];
       });
   }
-  if constexpr (MODE != NARROW_GH) return;
-  __syncthreads();  // the pair's list segment, written by this CTA, is now visible to it
+}
 
-  // ---- GH: contacts of the segment; every contact's 456 values are added exactly ----
-  __shared__ int act[NT];
+// ---------------------------------------------------------------------------------------
+// GH assembly: the active contacts found by the chunk pass, grouped by body pair
+// ---------------------------------------------------------------------------------------
+// single CTA: per-pair offsets of the contact lists (pair_cand[4p] = offset, [4p+1] = count,
+// [4p+2] = fill cursor); skipped when the pass overflowed (the host reruns it)
+__global__ void __launch_bounds__(1024) k_contact_scan(int cap_pairs, int* pair_cand, int* dstat) {
+  if (dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
+  const int np = min(dstat[DS_NPAIRS], cap_pairs);
+  __shared__ int sh[33];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < np; c0 += 1024) {
+    const int p = c0 + threadIdx.x;
+    const int v = p < np ? pair_cand[4 * p + 1] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = carry;
+      for (int w = 0; w < 32; ++w) {
+        const int t = sh[w];
+        sh[w] = acc;
+        acc += t;
+      }
+      sh[32] = acc;
+    }
+    __syncthreads();
+    if (p < np) {
+      pair_cand[4 * p] = sh[warp] + x - v;
+      pair_cand[4 * p + 2] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) carry = sh[32];
+    __syncthreads();
+  }
+}
+
+// contacts into their pair's segment (the order inside a segment does not matter: the
+// assembly sums exactly)
+__global__ void k_contact_scatter(int cap_contacts, const int4* __restrict__ in, int* pair_cand, int4* out,
+                                  const int* dstat) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
+  if (k >= min(dstat[DS_NCONTACT], cap_contacts)) return;
+  const int4 c = in[k];
+  out[pair_cand[4 * c.x] + atomicAdd(&pair_cand[4 * c.x + 2], 1)] = c;
+}
+
+// One CTA per body pair: every active contact of the pair (pt_ipc.py:111-190,
+// ee_ipc.py:381-430) as 5 rank-one terms, one warp per contact; its 456 values (H_IJ, the
+// contributions to H_II and H_JJ, and to g_I, g_J; put.py:25-66) are added exactly.
+__global__ void __launch_bounds__(NT) k_pair_assemble(NarrowArgs a) {
+  const int p = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (p >= a.dstat[DS_NPAIRS] || (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW))) return;
+  const int cnt = a.pair_cand[4 * p + 1], off = a.pair_cand[4 * p];
+  if (tid == 0) {
+    a.pair_active[p] = cnt;
+    if (cnt) atomicAdd(&a.dstat[DS_ACTIVE], cnt);
+  }
+  if (cnt == 0) return;
   __shared__ double ush[NW][5][24];
   extern __shared__ XSum xred[];  // [NOUT]
   for (int e = tid; e < NOUT * (kXD + 1); e += NT) reinterpret_cast<long long*>(xred)[e] = 0;
-  const int total = tpt + tee;
-  int nact_total = 0;
-  for (int c0 = 0; c0 < total; c0 += NT) {
-    const int c = c0 + tid;
-    int is_act = 0;
-    if (c < total) {
-      const int type = c < tpt ? 0 : 1;
-      const int* row = type == 0 ? &a.pt_list[5 * (size_t)(base_pt + c)] : &a.ee_list[5 * (size_t)(base_ee + c - tpt)];
-      const int pa = (type == 0 ? a.voff[row[0]] : a.eoff[row[0]]) + row[3];
-      const int pb = (type == 0 ? a.toff[row[1]] : a.eoff[row[1]]) + row[4];
-      int ids[4];
-      cand_vertices(a, type, pa, pb, ids);
-      d3 xs[4];
-      fetch(a.y0, ids, xs);
-      Geo G;
-      double d2;
-      is_act = contact_active(type, xs, a.prm, &G, &d2) ? 1 : 0;
-    }
-    int pos;
-    const int nact = block_scan(is_act, sh, pos);  // also orders the zeroing of xred before use
-    if (is_act) act[pos] = c;
-    __syncthreads();
-    nact_total += nact;
-    for (int ai = warp; ai < nact; ai += NW) {
-      const int cc = act[ai];
-      const int type = cc < tpt ? 0 : 1;
-      const int* row =
-          type == 0 ? &a.pt_list[5 * (size_t)(base_pt + cc)] : &a.ee_list[5 * (size_t)(base_ee + cc - tpt)];
-      const int swap = row[0] != P.I;  // point / first vertex group belongs to body J
-      const int pa = (type == 0 ? a.voff[row[0]] : a.eoff[row[0]]) + row[3];
-      const int pb = (type == 0 ? a.toff[row[1]] : a.eoff[row[1]]) + row[4];
-      int ids[4];
-      cand_vertices(a, type, pa, pb, ids);
-      d3 xs[4];
-      fetch(a.y0, ids, xs);
-      Geo G;
-      double d2;
-      contact_active(type, xs, a.prm, &G, &d2);
-      ContactScalars C;
-      contact_scalars(type, G, d2, a.prm, C);
-      if (lane < 24) {
-        const int side = lane / 12, m = (lane % 12) / 3, comp = lane % 3;
-        const int group = side ^ swap;  // vertex group whose body is this side
-        const int v0 = type == 0 ? (group ? 1 : 0) : (group ? 2 : 0);
-        const int v1 = type == 0 ? (group ? 4 : 1) : (group ? 4 : 2);
-        double dw[3];
+  __syncthreads();
+  for (int ci = warp; ci < cnt; ci += NW) {
+    const int4 rec = a.contacts_by_pair[off + ci];
+    const int type = rec.y & 1, swap = rec.y >> 1;
+    int ids[4];
+    cand_vertices(a, type, rec.z, rec.w, ids);
+    d3 xs[4];
+    fetch(a.y0, ids, xs);
+    Geo G;
+    double d2;
+    contact_active(type, xs, a.prm, &G, &d2);
+    ContactScalars C;
+    contact_scalars(type, G, d2, a.prm, C);
+    if (lane < 24) {
+      const int side = lane / 12, m = (lane % 12) / 3, comp = lane % 3;
+      const int group = side ^ swap;  // vertex group whose body is this side
+      const int v0 = type == 0 ? (group ? 1 : 0) : (group ? 2 : 0);
+      const int v1 = type == 0 ? (group ? 4 : 1) : (group ? 4 : 2);
+      double dw[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          double sacc = 0.0;
-          for (int v = v0; v < v1; ++v) {
-            const double w = m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]);
-            sacc += C.D[i][v] * w;
-          }
-          dw[i] = sacc;
+      for (int i = 0; i < 3; ++i) {
+        double sacc = 0.0;
+        for (int v = v0; v < v1; ++v) {
+          const double w = m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]);
+          sacc += C.D[i][v] * w;
         }
-#pragma unroll
-        for (int k = 0; k < 5; ++k)
-          ush[warp][k][lane] = dw[0] * C.q[k][comp] + dw[1] * C.q[k][3 + comp] + dw[2] * C.q[k][6 + comp];
+        dw[i] = sacc;
       }
-      __syncwarp();
-      for (int e = lane; e < NOUT; e += 32) {
-        double v = 0.0;
-        if (e < 432) {
-          const int blk = e / 144, r = (e % 144) / 12, cidx = e % 12;
-          const int ra = blk == 2 ? 12 + r : r;
-          const int cb = blk == 1 ? cidx : 12 + cidx;
 #pragma unroll
-          for (int k = 0; k < 5; ++k) v += C.coef[k] * (ush[warp][k][ra] * ush[warp][k][cb]);
-        } else {
-          v = C.gscale * ush[warp][4][e - 432];
-        }
-        xs_add_atomic(&xred[e], v);
-      }
-      __syncwarp();
+      for (int k = 0; k < 5; ++k)
+        ush[warp][k][lane] = dw[0] * C.q[k][comp] + dw[1] * C.q[k][3 + comp] + dw[2] * C.q[k][6 + comp];
     }
-    __syncthreads();
+    __syncwarp();
+    for (int e = lane; e < NOUT; e += 32) {
+      double v = 0.0;
+      if (e < 432) {
+        const int blk = e / 144, r = (e % 144) / 12, cidx = e % 12;
+        const int ra = blk == 2 ? 12 + r : r;
+        const int cb = blk == 1 ? cidx : 12 + cidx;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) v += C.coef[k] * (ush[warp][k][ra] * ush[warp][k][cb]);
+      } else {
+        v = C.gscale * ush[warp][4][e - 432];
+      }
+      xs_add_atomic(&xred[e], v);
+    }
+    __syncwarp();
   }
-  if (tid == 0) {
-    a.pair_active[p] = nact_total;
-    if (nact_total) atomicAdd(&a.dstat[DS_ACTIVE], nact_total);
-  }
-  if (nact_total == 0) return;
+  __syncthreads();
   for (int e = tid; e < NOUT; e += NT) {
     const double v = xs_round(xred[e]);
     if (e < 144) {
@@ -420,6 +453,72 @@ __global__ void __launch_bounds__(NT) k_narrow(NarrowArgs a) {
       a.pgrad[(size_t)p * 24 + (e - 432)] = v;
     }
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// per-body terms shared by the body kernels and the energy / CCD chunks
+// ---------------------------------------------------------------------------------------
+// predicted DOFs q~ = q0 + dt qdot (+ dt^2 g for p) (orthogonal_energy.py:24-32)
+__device__ inline void tilde_of(const abd_params& P, const abd_states& st, int b, double At[9], double pt[3]) {
+  const double dt = P.dt;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) At[k] = st.A0[9 * b + k] + dt * st.Adot[9 * b + k];
+  const double gv[3] = {0.0, P.gravity, 0.0};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) pt[k] = (st.p0[3 * b + k] + dt * st.pdot[3 * b + k]) + (dt * dt) * gv[k];
+}
+
+// does vertex v take part in the vertex-ground terms (culling.py:64-82)?  bb: its body box
+__device__ inline bool vg_candidate_of(const abd_params& P, const Box& bb, const double* y0, const double* y1, int v) {
+  if (!((double)bb.lo[1] < 0.5 * P.dhat + P.ground)) return false;
+  const Box q = point_box(y0, y1, v, (float)P.dhat);
+  Box g;
+  g.lo[0] = g.lo[1] = g.lo[2] = -1e3f;
+  g.hi[0] = 1e3f;
+  g.hi[1] = (float)P.ground;
+  g.hi[2] = 1e3f;
+  return overlap(q, g);
+}
+
+// inertia + orthogonality energy of a free body at trial DOFs K, pk (orthogonal_energy.py:24-32)
+__device__ inline double inertia_energy(const abd_params& P, const abd_states& st, const double* mass,
+                                        const double* I0, int b, const double* K, const double* pk) {
+  double At[9], pt[3];
+  tilde_of(P, st, b, At, pt);
+  double eo = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double tt =
+          (K[3 * i] * K[3 * j] + K[3 * i + 1] * K[3 * j + 1] + K[3 * i + 2] * K[3 * j + 2]) - (i == j ? 1.0 : 0.0);
+      eo += tt * tt;
+    }
+  eo = eo * P.stiffness;
+  double d0[3], d1[3], d2[3], d3v[3];
+  for (int k = 0; k < 3; ++k) {
+    d0[k] = pk[k] - pt[k];
+    d1[k] = K[k] - At[k];
+    d2[k] = K[3 + k] - At[3 + k];
+    d3v[k] = K[6 + k] - At[6 + k];
+  }
+  auto dd = [](const double* u) { return u[0] * u[0] + u[1] * u[1] + u[2] * u[2]; };
+  const double nm = dd(d0) * mass[b] + (dd(d1) + dd(d2) + dd(d3v)) * I0[b];
+  return eo * P.dt * P.dt + 0.5 * nm;
+}
+
+// time of impact of a vertex with the ground plane (ccd.py:9-18); 1 when none
+__device__ inline double vg_toi(const abd_params& P, const double* y0, const double* y1, int v) {
+  const double d1 = y1[3 * v + 1] - P.ground;
+  double tt = 1.0;
+  if (d1 < 0) {
+    const double d0 = y0[3 * v + 1] - P.ground;
+    tt = d0 / (d0 - d1);
+  }
+  return tt;
+}
+
+// minimum of non-negative doubles by atomicMax on the complemented bit patterns (0 = none)
+__device__ inline void toi_min(unsigned long long* key, double t) {
+  atomicMax(key, ~(unsigned long long)__double_as_longlong(t));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -438,13 +537,17 @@ __device__ inline bool ee_owner(int I, int nEI, int J, int nEJ) { return nEI > n
 // pairs (J, I) come from J's chunks), and its edges against the edge trees of the neighbours
 // it owns the EE candidates with -- the same candidates as the per-pair kernel, each query
 // box built once.  A query is only traversed into J's tree when it overlaps J's body box,
-// which contains every leaf box of J.  The (query, neighbour) combinations of a batch are
-// spread over the CTA's threads, so a chunk with few queries and many neighbours stays
-// parallel.  ENERGY sums the barrier energies (ipcsk/energy.py:9-48), CCD takes the minimum
-// time of impact (ccd.py:20-40, 133-186); both in a fixed order per chunk.
+// which contains every leaf box of J.  The overlapping (query, neighbour) combinations of a
+// batch are compacted and their traversals spread over the CTA's threads.  The first chunk
+// of every body also adds the body's own terms: inertia + orthogonality and the
+// vertex-ground barriers (ENERGY) or the vertex-ground times of impact (CCD).
+// ENERGY adds every nonzero term to one exact accumulator of the whole pass (any order gives
+// the same sum); CCD takes the minimum time of impact by an atomic maximum on complemented
+// bits.  (ipcsk/energy.py:9-48, orthogonal_energy.py:24-32, ccd.py:9-40, 133-186)
+constexpr int CW = 4 * CT;  // (query, neighbour) combinations tested per round
 template <int MODE>
 __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
-  constexpr bool ccd = MODE == NARROW_CCD;
+  constexpr bool ccd = MODE == NARROW_CCD, gh = MODE == NARROW_GH;
   const int c = blockIdx.x, tid = threadIdx.x;
   const int2 ch = a.chunk[c];
   const int I = ch.x;
@@ -456,7 +559,11 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   __shared__ int qprim[CT];  // point id, or ~edge id
   __shared__ Box nbox[NBB];
   __shared__ float ndof[NBB][24];
-  __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB];
+  __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB];
+  __shared__ unsigned short work[CW];
+  __shared__ int nwork;
+  __shared__ XSum xe;
+  __shared__ unsigned long long tkey;
   if (tid < Q) {
     const int k = ch.y + tid;
     if (k < nV) {
@@ -469,9 +576,31 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
     }
   }
-  double acc = 1.0;  // CCD: minimum time of impact
-  XSum xacc;         // ENERGY: exact sum of the barrier energies
-  xs_zero(xacc);
+  if (ccd) {
+    if (tid == 0) tkey = 0;
+  } else {
+    for (int e = tid; e < kXD + 1; e += CT) reinterpret_cast<long long*>(&xe)[e] = 0;
+  }
+  __syncthreads();
+  int cpt = 0, cee = 0;  // GH: candidates found by this thread
+  // the body's own terms, in its first chunk (GH: the body kernel adds them)
+  if (!gh && ch.y == 0) {
+    const Box bb = load_box(&a.body_box[I]);
+    const bool vg = a.prm.ground_enabled && a.prm.enable_vg;
+    for (int v = a.voff[I] + tid; vg && v < a.voff[I + 1]; v += CT) {
+      if (!vg_candidate_of(a.prm, bb, a.y0, a.y1, v)) continue;
+      if constexpr (ccd) {
+        const double t = vg_toi(a.prm, a.y0, a.y1, v);
+        if (t < 1.0) toi_min(&tkey, t);
+      } else {
+        const double d = a.y0[3 * v + 1] - a.prm.ground;
+        const double e = barrier(d * d, a.prm);
+        if (e != 0.0) xs_add_atomic(&xe, e);
+      }
+    }
+    if (!ccd && tid == 0 && !a.fixed[I])
+      xs_add_atomic(&xe, inertia_energy(a.prm, a.st, a.mass, a.I0, I, a.A + 9 * I, a.p + 3 * I));
+  }
   const bool ok = !(a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW);  // an overflowed pass is rerun
   const int r0 = a.row_ptr[I], r1 = min(a.row_ptr[I + 1], a.cap_adj);
   for (int b0 = (ok && Q > 0) ? r0 : r1; b0 < r1; b0 += NBB) {
@@ -484,6 +613,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       ntri[tid] = a.tri.body_root[J];
       nedge[tid] = a.edge.body_root[J];
       nown[tid] = ee_owner(I, nEI, J, a.eoff[J + 1] - a.eoff[J]);
+      if (gh) npair[tid] = a.adj_pair[b0 + tid];
     }
     for (int e = tid; e < 24 * nb; e += CT) {
       const int j = e / 24, t = (e / 12) & 1, cc = e % 12;
@@ -492,51 +622,84 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       const double* pp = t ? a.p1 : a.p;
       if (!t || a.y1) ndof[j][cc + 12 * t] = (float)(cc < 9 ? A[9 * J + cc] : pp[3 * J + cc - 9]);
     }
-    __syncthreads();
-    for (int it = tid; it < Q * nb; it += CT) {
-      const int q = it % Q, j = it / Q;
-      const int qp = qprim[q];
-      const bool pt = qp >= 0;
-      if (!pt && !nown[j]) continue;
-      const Box qb = qbox[q];
-      if (!overlap(qb, nbox[j])) continue;
-      auto visit = [&](int type, int pa, int pb) {
-        int ids[4];
-        cand_vertices(a, type, pa, pb, ids);
-        d3 xs[4];
-        fetch(a.y0, ids, xs);
-        if constexpr (ccd) {
-          d3 x1[4];
-          fetch(a.y1, ids, x1);
-          const double t = collision_time(type, xs, x1);
-          if (t < 1.0) acc = fmin(acc, t);
-        } else {
-          xs_add(xacc, contact_energy(type, xs, a.prm));
-        }
-      };
-      if (pt) {
-        traverse(node_boxes(a, &a.tri, true, ndof[j]), ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); });
-      } else {
-        // EE candidates are evaluated with the edge of the lower body first, as the per-pair lists
-        const bool lower = I < nJ[j];
-        traverse(node_boxes(a, &a.edge, false, ndof[j]), nedge[j], qb, a.dstat,
-                 [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); });
+    for (int w0 = 0; w0 < Q * nb; w0 += CW) {
+      if (tid == 0) nwork = 0;
+      __syncthreads();
+      // overlapping (query, neighbour) combinations of this round
+      for (int it = w0 + tid; it < min(Q * nb, w0 + CW); it += CT) {
+        const int q = it % Q, j = it / Q;
+        if (qprim[q] < 0 && !nown[j]) continue;
+        if (!overlap(qbox[q], nbox[j])) continue;
+        work[atomicAdd(&nwork, 1)] = (unsigned short)(q | (j << 8));
       }
-    }
-  }
-  if constexpr (ccd) {
-    __shared__ double red[CT];
-    red[tid] = acc;
-    __syncthreads();
-    for (int st = CT / 2; st > 0; st >>= 1) {
-      if (tid < st) red[tid] = fmin(red[tid], red[tid + st]);
+      __syncthreads();
+      for (int k = tid; k < nwork; k += CT) {
+        const int q = work[k] & 0xff, j = work[k] >> 8;
+        const int qp = qprim[q];
+        const Box qb = qbox[q];
+        auto visit = [&](int type, int pa, int pb) {
+          int ids[4];
+          cand_vertices(a, type, pa, pb, ids);
+          d3 xs[4];
+          fetch(a.y0, ids, xs);
+          if constexpr (gh) {
+            if (type == 0) ++cpt;
+            else ++cee;
+            Geo G;
+            double d2;
+            if (contact_active(type, xs, a.prm, &G, &d2)) {
+              // PT: the point is I's, the pair's first body is min(I, J); EE: lower body first
+              const int pr = npair[j], swap = (type == 0 && I > nJ[j]) ? 1 : 0;
+              const int pos = atomicAdd(&a.dstat[DS_NCONTACT], 1);
+              if (pos < a.cap_contacts) a.contacts[pos] = make_int4(pr, type | (swap << 1), pa, pb);
+              else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
+              atomicAdd(&a.pair_cand[4 * pr + 1], 1);
+            }
+          } else if constexpr (ccd) {
+            d3 x1[4];
+            fetch(a.y1, ids, x1);
+            const double t = collision_time(type, xs, x1);
+            if (t < 1.0) toi_min(&tkey, t);
+          } else {
+            const double e = contact_energy(type, xs, a.prm);
+            if (e != 0.0) xs_add_atomic(&xe, e);
+          }
+        };
+        if (qp >= 0) {
+          traverse(node_boxes(a, &a.tri, true, ndof[j]), ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); });
+        } else {
+          // EE candidates are evaluated with the edge of the lower body first, as the per-pair lists
+          const bool lower = I < nJ[j];
+          traverse(node_boxes(a, &a.edge, false, ndof[j]), nedge[j], qb, a.dstat,
+                   [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); });
+        }
+      }
       __syncthreads();
     }
-    if (tid == 0) a.chunk_val[c] = red[0];
-  } else {
-    __shared__ XSum xsh[CT / 32];
-    xs_block_sum(xacc, xsh);
-    if (tid == 0) a.chunk_acc[c] = xacc;
+  }
+  if constexpr (gh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      cpt += __shfl_xor_sync(0xffffffffu, cpt, o);
+      cee += __shfl_xor_sync(0xffffffffu, cee, o);
+    }
+    if ((tid & 31) == 0) {
+      if (cpt) atomicAdd(&a.dstat[DS_PT_COUNT], cpt);
+      if (cee) atomicAdd(&a.dstat[DS_EE_COUNT], cee);
+    }
+    return;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if constexpr (ccd) {
+      if (tkey) atomicMax(a.toi_key, tkey);
+    } else {
+      const long long* src = reinterpret_cast<const long long*>(&xe);
+      long long* dst = reinterpret_cast<long long*>(a.energy);
+      for (int e = 0; e < kXD; ++e)
+        if (src[e]) atomicAdd((unsigned long long*)&dst[e], (unsigned long long)src[e]);
+      if (src[kXD]) atomicOr((unsigned long long*)&dst[kXD], (unsigned long long)src[kXD]);
+    }
   }
 }
 
@@ -555,32 +718,17 @@ struct BodyArgs {
   const int *row_ptr, *adj_pair, *pair_active;
   const int2* ij;
   const double *pdiag, *pgrad;
-  double *diag, *g, *body_val;
-  XSum* body_acc;
+  double *diag, *g;
   int* dstat;
   int* vg_list;
   int cap_vg;
 };
 
 __device__ inline void tilde(const BodyArgs& a, int b, double At[9], double pt[3]) {
-  const double dt = a.prm.dt;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) At[k] = a.st.A0[9 * b + k] + dt * a.st.Adot[9 * b + k];
-  const double gv[3] = {0.0, a.prm.gravity, 0.0};
-#pragma unroll
-  for (int k = 0; k < 3; ++k) pt[k] = (a.st.p0[3 * b + k] + dt * a.st.pdot[3 * b + k]) + (dt * dt) * gv[k];
+  tilde_of(a.prm, a.st, b, At, pt);
 }
-
-// does vertex v of body b take part in the vertex-ground terms (culling.py:64-82)?
 __device__ inline bool vg_candidate(const BodyArgs& a, const Box& bb, const double* y0, const double* y1, int v) {
-  if (!((double)bb.lo[1] < 0.5 * a.prm.dhat + a.prm.ground)) return false;
-  const Box q = point_box(y0, y1, v, (float)a.prm.dhat);
-  Box g;
-  g.lo[0] = g.lo[1] = g.lo[2] = -1e3f;
-  g.hi[0] = 1e3f;
-  g.hi[1] = (float)a.prm.ground;
-  g.hi[2] = 1e3f;
-  return overlap(q, g);
+  return vg_candidate_of(a.prm, bb, y0, y1, v);
 }
 
 constexpr int BT = 160;
@@ -681,75 +829,6 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   else a.g[(size_t)b * 12 + (t - 144)] = val;
 }
 
-// body b's exact energy terms: vertex-ground barriers and inertia + orthogonality
-// (orthogonal_energy.py:24-32, vg_ipc.py / energy.py:24-33)
-__global__ void __launch_bounds__(128) k_body_energy(BodyArgs a) {
-  const int b = blockIdx.x, t = threadIdx.x;
-  __shared__ XSum xsh[4];
-  XSum acc;
-  xs_zero(acc);
-  if (a.prm.ground_enabled && a.prm.enable_vg) {
-    const Box bb = load_box(&a.body_box[b]);
-    for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
-      if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
-      const double d = a.y[3 * v + 1] - a.prm.ground;
-      xs_add(acc, barrier(d * d, a.prm));
-    }
-  }
-  if (t == 0 && !a.fixed[b]) {
-    double At[9], pt[3];
-    tilde(a, b, At, pt);
-    const double* K = a.A + 9 * b;  // trial DOFs Ak
-    double eo = 0.0;
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) {
-        const double tt = (K[3 * i] * K[3 * j] + K[3 * i + 1] * K[3 * j + 1] + K[3 * i + 2] * K[3 * j + 2]) -
-                          (i == j ? 1.0 : 0.0);
-        eo += tt * tt;
-      }
-    eo = eo * a.prm.stiffness;
-    const double* pk = a.p + 3 * b;
-    double d0[3], d1[3], d2[3], d3v[3];
-    for (int k = 0; k < 3; ++k) {
-      d0[k] = pk[k] - pt[k];
-      d1[k] = K[k] - At[k];
-      d2[k] = K[3 + k] - At[3 + k];
-      d3v[k] = K[6 + k] - At[6 + k];
-    }
-    auto dd = [](const double* u) { return u[0] * u[0] + u[1] * u[1] + u[2] * u[2]; };
-    const double nm = dd(d0) * a.mass[b] + (dd(d1) + dd(d2) + dd(d3v)) * a.I0[b];
-    xs_add(acc, eo * a.prm.dt * a.prm.dt + 0.5 * nm);
-  }
-  xs_block_sum(acc, xsh);
-  if (t == 0) a.body_acc[b] = acc;
-}
-
-__global__ void __launch_bounds__(128) k_body_vg_toi(BodyArgs a) {
-  const int b = blockIdx.x, t = threadIdx.x;
-  __shared__ double red[128];
-  double acc = 1.0;
-  if (a.prm.ground_enabled && a.prm.enable_vg) {
-    const Box bb = load_box(&a.body_box[b]);
-    for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
-      if (!vg_candidate(a, bb, a.y, a.y1, v)) continue;
-      const double d1 = a.y1[3 * v + 1] - a.prm.ground;
-      double tt = 1.0;
-      if (d1 < 0) {
-        const double d0 = a.y[3 * v + 1] - a.prm.ground;
-        tt = d0 / (d0 - d1);
-      }
-      if (tt < 1.0) acc = fmin(acc, tt);
-    }
-  }
-  red[t] = acc;
-  __syncthreads();
-  for (int s = 64; s > 0; s >>= 1) {
-    if (t < s) red[t] = fmin(red[t], red[t + s]);
-    __syncthreads();
-  }
-  if (t == 0) a.body_val[b] = red[0];
-}
-
 __global__ void k_vg_list(BodyArgs a) {
   const int b = blockIdx.x;
   const Box bb = load_box(&a.body_box[b]);
@@ -763,34 +842,6 @@ __global__ void k_vg_list(BodyArgs a) {
       atomicOr(&a.dstat[DS_STATUS], ST_VG_OVERFLOW);
     }
   }
-}
-
-// single-CTA exact sum of two accumulator arrays, rounded once
-__global__ void __launch_bounds__(1024) k_reduce_exact(const XSum* xa, int na, const XSum* xb, int nb, double* out) {
-  __shared__ XSum xsh[32];
-  XSum acc;
-  xs_zero(acc);
-  for (int i = threadIdx.x; i < na; i += 1024) xs_merge(acc, xa[i]);
-  for (int i = threadIdx.x; i < nb; i += 1024) xs_merge(acc, xb[i]);
-  xs_block_sum(acc, xsh);
-  if (threadIdx.x == 0) *out = xs_round(acc);
-}
-
-// deterministic single-CTA reduction of chunk and body values (sum or min)
-__global__ void __launch_bounds__(1024) k_reduce_vals(const double* pv, int np, const double* bv, int nb, int is_min,
-                                                      double* out) {
-  __shared__ double red[1024];
-  const int t = threadIdx.x;
-  double acc = is_min ? 1.0 : 0.0;
-  for (int i = t; i < np; i += 1024) acc = is_min ? fmin(acc, pv[i]) : acc + pv[i];
-  for (int i = t; i < nb; i += 1024) acc = is_min ? fmin(acc, bv[i]) : acc + bv[i];
-  red[t] = acc;
-  __syncthreads();
-  for (int s = 512; s > 0; s >>= 1) {
-    if (t < s) red[t] = is_min ? fmin(red[t], red[t + s]) : red[t] + red[t + s];
-    __syncthreads();
-  }
-  if (t == 0) *out = red[0];
 }
 
 // exported blocks follow the solver's view: pairs without active contacts or touching a fixed
@@ -866,7 +917,7 @@ __global__ void __launch_bounds__(256) k_dot(int N, const double* a, const doubl
 }
 
 NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
-                       const double* y0, const double* y1) {
+                       const double* y0, const double* y1, const abd_states* st) {
   NarrowArgs a;
   a.A = A;
   a.p = p;
@@ -882,8 +933,16 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.adj_col = s.adj_col;
   a.body_box = s.body_box;
   a.chunk = s.chunk;
-  a.chunk_val = s.chunk_val;
-  a.chunk_acc = s.chunk_acc;
+  a.energy = s.energy_acc;
+  a.adj_pair = s.adj_pair;
+  a.cap_contacts = s.cap_contacts;
+  a.contacts = s.contacts;
+  a.contacts_by_pair = s.contacts_by_pair;
+  a.toi_key = s.dmin;
+  a.st = st ? *st : abd_states{};
+  a.mass = s.mass;
+  a.I0 = s.I0;
+  a.fixed = s.fixed;
   a.voff = s.voff;
   a.toff = s.toff;
   a.eoff = s.eoff;
@@ -932,8 +991,6 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
   a.pgrad = s.pgrad;
   a.diag = s.diag;
   a.g = s.g;
-  a.body_val = s.body_val;
-  a.body_acc = s.body_acc;
   a.dstat = s.dstat;
   a.vg_list = s.vg_list;
   a.cap_vg = s.cap_vg;
@@ -943,22 +1000,34 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
 }  // namespace
 
 cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
-                   const double* y0, const double* y1) {
-  const NarrowArgs a = narrow_args(s, mode, A, p, A1, p1, y0, y1);
-  if (mode == NARROW_ENERGY || mode == NARROW_CCD) {
-    if (!a.affine) return cudaErrorInvalidValue;  // energy and CCD always run at DOFs
+                   const double* y0, const double* y1, const abd_states* st) {
+  const NarrowArgs a = narrow_args(s, mode, A, p, A1, p1, y0, y1, st);
+  if (mode == NARROW_ENERGY || mode == NARROW_CCD || mode == NARROW_GH) {
+    // energy, CCD and GH always run at DOFs; the energy needs the states (inertia terms)
+    if (!a.affine || (mode == NARROW_ENERGY && !(st && st->A0 && st->Adot && st->p0 && st->pdot)))
+      return cudaErrorInvalidValue;
     if (s.nch == 0) return cudaSuccess;
-    if (mode == NARROW_ENERGY) k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
-    else k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+    if (mode == NARROW_ENERGY) {
+      k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
+    } else if (mode == NARROW_CCD) {
+      k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+    } else {
+      cudaError_t e = cudaMemsetAsync(s.pair_cand, 0, sizeof(int) * 4 * (size_t)s.cap_pairs, s.stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCONTACT, 0, sizeof(int), s.stream);
+      if (e != cudaSuccess) return e;
+      k_chunk_narrow<NARROW_GH><<<s.nch, CT, 0, s.stream>>>(a);
+      k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
+      k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
+                                                                           s.contacts_by_pair, s.dstat);
+      const int smem = NOUT * (int)sizeof(XSum);
+      e = cudaFuncSetAttribute(k_pair_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      k_pair_assemble<<<s.cap_pairs, NT, smem, s.stream>>>(a);
+      s.launches += 3;
+    }
   } else {
     if (s.cap_pairs == 0) return cudaSuccess;
-    if (mode == NARROW_GH) {
-      const int smem = NOUT * (int)sizeof(XSum);
-      cudaError_t e = cudaFuncSetAttribute(k_narrow<NARROW_GH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e != cudaSuccess) return e;
-      k_narrow<NARROW_GH><<<s.cap_pairs, NT, smem, s.stream>>>(a);
-    }
-    else k_narrow<NARROW_LISTS><<<s.cap_pairs, NT, 0, s.stream>>>(a);
+    k_pair_lists<<<s.cap_pairs, NT, 0, s.stream>>>(a);
   }
   ++s.launches;
   return cudaGetLastError();
@@ -966,18 +1035,6 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
 
 cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y) {
   k_body_gh<<<s.n, BT, 0, s.stream>>>(body_args(s, &st, A, p, y, nullptr));
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t body_energy(Sim& s, const abd_states& st, const double* Ak, const double* pk, const double* y) {
-  k_body_energy<<<s.n, 128, 0, s.stream>>>(body_args(s, &st, Ak, pk, y, nullptr));
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t body_vg_toi(Sim& s, const double* y0, const double* y1) {
-  k_body_vg_toi<<<s.n, 128, 0, s.stream>>>(body_args(s, nullptr, nullptr, nullptr, y0, y1));
   ++s.launches;
   return cudaGetLastError();
 }
@@ -992,18 +1049,6 @@ cudaError_t vg_list(Sim& s, const double* y0) {
 cudaError_t vg_list_swept(Sim& s, const double* y0, const double* y1) {
   if (!(s.prm.ground_enabled && s.prm.enable_vg)) return cudaSuccess;
   k_vg_list<<<s.n, 128, 0, s.stream>>>(body_args(s, nullptr, nullptr, nullptr, y0, y1));
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t sum_energy(Sim& s, double* out) {
-  k_reduce_exact<<<1, 1024, 0, s.stream>>>(s.chunk_acc, s.nch, s.body_acc, s.n, out);
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t min_toi(Sim& s, double* out) {
-  k_reduce_vals<<<1, 1024, 0, s.stream>>>(s.chunk_val, s.nch, s.body_val, s.n, 1, out);
   ++s.launches;
   return cudaGetLastError();
 }

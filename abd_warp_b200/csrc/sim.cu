@@ -33,6 +33,46 @@ using abd::Sim;
     if ((x) != cudaSuccess) return ABD_ERR_CUDA; \
   } while (0)
 
+// The exact accumulator rounded to FP64 on the host (the same rounding as the device's).
+double xs_round_host(const abd::XSum& x) {
+  if (x.flags & (abd::XS_NAN | abd::XS_RANGE)) return std::nan("");
+  if (x.flags & abd::XS_PINF) return (x.flags & abd::XS_NINF) ? std::nan("") : INFINITY;
+  if (x.flags & abd::XS_NINF) return -INFINITY;
+  long long d[abd::kXD + 1];
+  for (int i = 0; i < abd::kXD; ++i) d[i] = x.d[i];
+  d[abd::kXD] = 0;
+  auto carry = [&]() {
+    for (int i = 0; i < abd::kXD; ++i) {
+      const long long c = d[i] >> 32;
+      d[i] -= c * 4294967296LL;
+      d[i + 1] += c;
+    }
+  };
+  carry();
+  const bool neg = d[abd::kXD] < 0;
+  if (neg) {
+    for (int i = 0; i <= abd::kXD; ++i) d[i] = -d[i];
+    carry();
+  }
+  int h = -1;
+  for (int i = 0; i <= abd::kXD; ++i)
+    if (d[i] != 0) h = i;
+  if (h < 0) return 0.0;
+  const unsigned long long t2 = (unsigned long long)d[h], t1 = h >= 1 ? (unsigned long long)d[h - 1] : 0ULL,
+                           t0 = h >= 2 ? (unsigned long long)d[h - 2] : 0ULL;
+  bool sticky = false;
+  for (int i = 0; i < h - 2; ++i) sticky = sticky || d[i] != 0;
+  const unsigned __int128 w = ((unsigned __int128)t2 << 64) | ((unsigned __int128)t1 << 32) | t0;
+  const int msb = 127 - __builtin_clzll(t2);
+  const int drop = msb - 52;
+  unsigned long long mant = (unsigned long long)(w >> drop);
+  const unsigned __int128 rem = w & ((((unsigned __int128)1) << drop) - 1);
+  const unsigned __int128 half = ((unsigned __int128)1) << (drop - 1);
+  if (rem > half || (rem == half && (sticky || (mant & 1ULL)))) ++mant;
+  const double r = std::ldexp((double)mant, drop + 32 * (h - 2) + abd::kXB0);
+  return neg ? -r : r;
+}
+
 template <class T>
 cudaError_t dalloc(T** p, size_t count) {
   return cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1));
@@ -73,6 +113,16 @@ int grow_pairs(Sim& s, int need) {
   return ABD_OK;
 }
 
+int grow_contacts(Sim& s, int need) {
+  if (need <= s.cap_contacts) return ABD_OK;
+  if (s.contacts) cudaFree(s.contacts);
+  if (s.contacts_by_pair) cudaFree(s.contacts_by_pair);
+  s.contacts = s.contacts_by_pair = nullptr;
+  s.cap_contacts = std::max(need + need / 2, 2 * s.cap_contacts);
+  if (dalloc(&s.contacts, s.cap_contacts) || dalloc(&s.contacts_by_pair, s.cap_contacts)) return ABD_ERR_OVERFLOW;
+  return ABD_OK;
+}
+
 int grow_act(Sim& s, int need) {
   if (need <= s.cap_act) return ABD_OK;
   if (s.act_pairs) cudaFree(s.act_pairs);
@@ -106,21 +156,23 @@ int grow_lists(Sim& s, int need_pt, int need_ee) {
 // A != null: y0 (and y1 when A1 != null) are computed from the DOFs inside the broad-phase
 // kernel; otherwise y0 / y1 are given positions.
 int culling(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* y0,
-            double* y1, int mode) {
+            double* y1, int mode, const abd_states* st = nullptr) {
   Sim& s = h->s;
   CK(abd::body_broad(s, A, p, A1, p1, y0, y1));
   CK(abd::body_pairs(s));
   if (mode == abd::NARROW_GH || mode == abd::NARROW_LISTS)  // PT, EE, VG and active counters
     CK(cudaMemsetAsync(s.dstat + abd::DS_PT_COUNT, 0, 4 * sizeof(int), s.stream));
-  CK(abd::narrow(s, mode, A, p, A1, p1, y0, y1));
+  if (mode == abd::NARROW_ENERGY) CK(cudaMemsetAsync(s.energy_acc, 0, sizeof(abd::XSum), s.stream));
+  if (mode == abd::NARROW_CCD) CK(cudaMemsetAsync(s.dmin, 0, sizeof(unsigned long long), s.stream));
+  CK(abd::narrow(s, mode, A, p, A1, p1, y0, y1, st));
   return ABD_OK;
 }
 
-// One synchronisation: the dstat mirror plus `nd` doubles from `dev` into hval (and, when
+// One synchronisation: the dstat mirror plus `nbytes` bytes from `dev` into hval (and, when
 // act is set, the active-pair list into hact).  Updates the host pair counts.
-int sync_read(Sim& s, const double* dev, int nd, bool act = false) {
+int sync_read(Sim& s, const void* dev, size_t nbytes, bool act = false) {
   CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-  if (nd > 0) CK(cudaMemcpyAsync(s.hval, dev, nd * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  if (nbytes > 0) CK(cudaMemcpyAsync(s.hval, dev, nbytes, cudaMemcpyDeviceToHost, s.stream));
   if (act && s.cap_act > 0)
     CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
   CK(cudaStreamSynchronize(s.stream));
@@ -136,7 +188,7 @@ constexpr int kRerun = -1;
 int overflow(Sim& s) {
   const int bits = s.hstat[abd::DS_STATUS];
   const int mask = abd::ST_PAIR_OVERFLOW | abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW | abd::ST_VG_OVERFLOW |
-                   abd::ST_ACT_OVERFLOW;
+                   abd::ST_ACT_OVERFLOW | abd::ST_CONTACT_OVERFLOW;
   if (!(bits & mask)) return 0;
   int r = ABD_OK;
   if (bits & abd::ST_PAIR_OVERFLOW) r = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
@@ -149,6 +201,7 @@ int overflow(Sim& s) {
     if (dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) r = ABD_ERR_OVERFLOW;
   }
   if (!r && (bits & abd::ST_ACT_OVERFLOW)) r = grow_act(s, s.hstat[abd::DS_NACTP]);
+  if (!r && (bits & abd::ST_CONTACT_OVERFLOW)) r = grow_contacts(s, s.hstat[abd::DS_NCONTACT]);
   if (r) return r;
   const int clear = bits & ~mask;
   s.hstat[abd::DS_STATUS] = clear;
@@ -160,40 +213,50 @@ int overflow(Sim& s) {
 
 constexpr int kMaxReruns = 6;
 
-// E(Ak, pk): barrier over the culling lists at xk + inertia (compute_energy, abd.py:133-141)
+// E(Ak, pk): barrier over the culling lists at xk + inertia (compute_energy, abd.py:133-141),
+// summed exactly on the device and rounded here
 int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* pk, double* E) {
   Sim& s = h->s;
   for (int tries = 0;; ++tries) {
-    int r = culling(h, Ak, pk, nullptr, nullptr, s.xk, nullptr, abd::NARROW_ENERGY);
+    int r = culling(h, Ak, pk, nullptr, nullptr, s.xk, nullptr, abd::NARROW_ENERGY, &st);
     if (r) return r;
-    CK(abd::body_energy(s, st, Ak, pk, s.xk));
-    CK(abd::sum_energy(s, s.scal + 8));
-    if ((r = sync_read(s, s.scal + 8, 1))) return r;
+    if ((r = sync_read(s, s.energy_acc, sizeof(abd::XSum)))) return r;
     if ((r = overflow(s)) > 0) return r;
     if (r == 0) break;
     if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
   }
-  *E = s.hval[0];
+  abd::XSum x;
+  std::memcpy(&x, s.hval, sizeof(x));
+  *E = xs_round_host(x);
   return ABD_OK;
 }
 
 // CCD bound between DOFs (A, p) and (A1, p1) (ccd, abd.py:278-303); positions land in x, xk.
-// The scalars scal[10], scal[11] (dq.g, g.g of the step) ride along in the same read into
-// hval[1], hval[2].
+// The dot products scal[10], scal[11] (dq.g, g.g of the step) ride along in the same read
+// (out: dots[2]).
 int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
-           double* raw) {
+           double* raw, double* dots = nullptr) {
   Sim& s = h->s;
   for (int tries = 0;; ++tries) {
     int r = culling(h, A, p, A1, p1, s.x, s.xk, abd::NARROW_CCD);
     if (r) return r;
-    CK(abd::body_vg_toi(s, s.x, s.xk));
-    CK(abd::min_toi(s, s.scal + 9));
-    if ((r = sync_read(s, s.scal + 9, 3))) return r;
+    if (dots) CK(cudaMemcpyAsync(s.hval + 1, s.scal + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    if ((r = sync_read(s, s.dmin, sizeof(unsigned long long)))) return r;
     if ((r = overflow(s)) > 0) return r;
     if (r == 0) break;
     if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
   }
-  const double toi = s.hval[0];
+  unsigned long long key;
+  std::memcpy(&key, s.hval, sizeof(key));
+  double toi = 1.0;
+  if (key) {
+    const unsigned long long bits = ~key;
+    std::memcpy(&toi, &bits, sizeof(toi));
+  }
+  if (dots) {
+    dots[0] = s.hval[1];
+    dots[1] = s.hval[2];
+  }
   if (raw) *raw = toi;
   double t = std::max(0.0, std::min(1.0, toi));
   if (t < 1.0) t *= 0.9;
@@ -328,6 +391,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.x, 3 * (size_t)V));
   ok(dalloc(&s.xk, 3 * (size_t)V));
   ok(dalloc(&s.body_box, n));
+  ok(dalloc(&s.body_bnd, 12 * (size_t)n));
   ok(dalloc(&s.pair_mask, (size_t)n * s.W));
   ok(dalloc(&s.pair_wpre, (size_t)n * s.W));
   {
@@ -335,17 +399,15 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     std::vector<int2> ch;
     for (int b = 0; b < n; ++b) {
       const int items = (d->vert_off[b + 1] - d->vert_off[b]) + (d->edge_off[b + 1] - d->edge_off[b]);
-      for (int i = 0; i < items; i += abd::kChunk) ch.push_back(make_int2(b, i));
+      // every body has at least one chunk: its first chunk also adds the body's own terms
+      for (int i = 0; i < std::max(items, 1); i += abd::kChunk) ch.push_back(make_int2(b, i));
     }
     s.nch = (int)ch.size();
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
-    ok(dalloc(&s.chunk_val, ch.size()));
-    ok(dalloc(&s.chunk_acc, ch.size()));
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // ch is a host temporary
   }
   ok(dalloc(&s.row_ptr, n + 1));
   ok(dalloc(&s.upper_ptr, n + 1));
-  ok(dalloc(&s.body_val, n));
   for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq, &s.zb})
     ok(dalloc(v, 12 * (size_t)n));
   ok(dalloc(&s.cl_ptr, n + 1));
@@ -356,11 +418,11 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
   ok(dalloc(&s.red_count, abd::kRedSlots));
   ok(dalloc(&s.scal, 32));
-  ok(dalloc(&s.body_acc, n));
+  ok(dalloc(&s.energy_acc, 1));
   ok(dalloc(&s.dstat, abd::DS_NSLOTS));
   ok(dalloc(&s.dmin, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 8 * sizeof(double), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 32 * sizeof(double), cudaHostAllocDefault);
   // preconditioner tables: cl_ptr, cl_body, body_cl (ints), cl_off (8-byte aligned long longs)
   s.cap_hstage = sizeof(int) * (3 * (size_t)n + 2) + sizeof(long long) * ((size_t)n + 2);
   if (e == cudaSuccess) e = cudaHostAlloc(&s.hstage, s.cap_hstage, cudaHostAllocDefault);
@@ -378,6 +440,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   s.cap_pairs = 0;
   int r = grow_pairs(s, std::max(256, 4 * n));
   if (!r) r = grow_act(s, std::max(1024, n));
+  if (!r) r = grow_contacts(s, std::max(4096, 4 * n));
   s.cap_pt = 0;
   s.cap_ee = 0;
   if (!r) r = grow_lists(s, std::max(1 << 14, V / 4), std::max(1 << 14, E / 4));
@@ -400,10 +463,10 @@ int abd_sim_destroy(abd_sim* h) {
   void* bufs[] = {s.voff, s.toff, s.eoff, s.vbody, s.tbody, s.ebody, s.tris, s.edges, s.x0, s.mass, s.I0,
                   s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
-                  s.pair_active, s.pair_val, s.body_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
+                  s.pair_active, s.pair_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
-                  s.chunk_val, s.chunk_acc, s.body_acc, s.red_count};
+                  s.energy_acc, s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact})
@@ -486,6 +549,7 @@ int cull_lists(abd_sim* h, const double* A, const double* p, const double* A1, c
   counts[1] = s.hstat[abd::DS_PT_COUNT];
   counts[2] = s.hstat[abd::DS_EE_COUNT];
   counts[3] = s.hstat[abd::DS_VG_COUNT];
+  for (int k = 0; k < 4; ++k) s.list_counts[k] = counts[k];
   return ABD_OK;
 }
 
@@ -508,8 +572,8 @@ int abd_collision_set_dofs(abd_sim* h, const double* A, const double* p, const d
 int abd_export_lists(abd_sim* h, int* ij, int* pt, int* ee, int* vg, int cap) {
   if (!h || cap < 0) return ABD_ERR_INVALID;
   Sim& s = h->s;
-  const int npt = s.hstat[abd::DS_PT_COUNT], nee = s.hstat[abd::DS_EE_COUNT], nvg = s.hstat[abd::DS_VG_COUNT];
-  if (ij) CK(cudaMemcpyAsync(ij, s.ij, sizeof(int2) * std::min(cap, s.n_pairs), cudaMemcpyDeviceToDevice, s.stream));
+  const int npairs = s.list_counts[0], npt = s.list_counts[1], nee = s.list_counts[2], nvg = s.list_counts[3];
+  if (ij) CK(cudaMemcpyAsync(ij, s.ij, sizeof(int2) * std::min(cap, npairs), cudaMemcpyDeviceToDevice, s.stream));
   if (pt) CK(cudaMemcpyAsync(pt, s.pt_list, sizeof(int) * 5 * std::min(cap, npt), cudaMemcpyDeviceToDevice, s.stream));
   if (ee) CK(cudaMemcpyAsync(ee, s.ee_list, sizeof(int) * 5 * std::min(cap, nee), cudaMemcpyDeviceToDevice, s.stream));
   if (vg) CK(cudaMemcpyAsync(vg, s.vg_list, sizeof(int) * 2 * std::min(cap, nvg), cudaMemcpyDeviceToDevice, s.stream));
@@ -586,9 +650,9 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     CK(abd::dot(s, s.g, s.g, 11, s.scal + 11));
     // CCD bound (abd.py:278-303)
     CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
-    double alpha;
-    if ((r = ccd_at(h, st.A, st.p, st.Ak, st.pk, &alpha, &inf.toi))) return r;
-    const double qTg = s.hval[1], gTg = s.hval[2];
+    double alpha, dots[2];
+    if ((r = ccd_at(h, st.A, st.p, st.Ak, st.pk, &alpha, &inf.toi, dots))) return r;
+    const double qTg = dots[0], gTg = dots[1];
     // backtracking line search (abd.py:146-160)
     double E1 = E0;
     for (;;) {

@@ -119,7 +119,9 @@ int abd_collision_set(abd_sim* sim, const double* y0_dev, const double* y1_dev, 
  * abd/abd.py:170-207, as step and ccd call them at abd.py:226-227, 278-280). */
 int abd_collision_set_dofs(abd_sim* sim, const double* A_dev, const double* p_dev, const double* A1_dev,
                            const double* p1_dev, int counts[4]);
-/* Copy the last culling lists into device buffers of capacity cap rows:
+/* Copy the lists of the last abd_collision_set / abd_collision_set_dofs call (valid until the
+ * next call that culls: abd_step, abd_ipc_gh, abd_compute_energy, abd_ccd or another
+ * collision set) into device buffers of capacity cap rows:
  * ij [cap][2] (I < J), pt [cap][5] and ee [cap][5] as (I, J, pair, local prim of I, local
  * prim of J) like the reference's vec5i lists (culling.py:85-99), vg [cap][2] (body,
  * global vertex).  Any pointer may be NULL. */
