@@ -169,6 +169,8 @@ struct Tree {
 // ---------------------------------------------------------------------------------------
 // the simulator
 // ---------------------------------------------------------------------------------------
+struct Mailbox;
+
 struct Sim {
   cudaStream_t stream = 0;
   abd_params prm{};
@@ -210,7 +212,15 @@ struct Sim {
   // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
-  XSum* energy_acc = nullptr;      // exact energy of the last energy pass
+  XSum* energy_acc = nullptr;      // = &box->energy
+  // everything the host reads after a pass, in one device block (one copy per sync)
+  Mailbox* box = nullptr;          // device
+  Mailbox* hbox = nullptr;         // pinned host mirror
+  int* row_cnt = nullptr;          // [n] neighbours of each body (pair mask)
+  int* upper_cnt = nullptr;        // [n] neighbours J > I
+  int* kcount = nullptr;           // [4] last-CTA counters of single-pass kernels
+  double* dpar = nullptr;          // device pass parameters: [0] trial step, [1] = 1
+  double* hpar = nullptr;          // pinned staging of dpar
 
   // candidate lists
   int cap_pt = 0, cap_ee = 0, cap_vg = 0;
@@ -246,12 +256,12 @@ struct Sim {
   XSum* partials = nullptr; // exact reduction partials [kRedSlots][kRedBlocks]
   int* red_count = nullptr;        // [kRedSlots] CTAs done per reduction (last CTA finishes)
   double* scal = nullptr;          // solver scalars
-  int* dstat = nullptr;            // device: [0] status, [1..] counters
+  int* dstat = nullptr;            // = box->dstat: [0] status, [1..] counters
   int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
   void* hstage = nullptr;          // pinned staging of the preconditioner's cluster tables
   size_t cap_hstage = 0;
   double* hval = nullptr;          // pinned host scalars
-  unsigned long long* dmin = nullptr;  // [0]: complemented bits of the last CCD pass's minimum
+  unsigned long long* dmin = nullptr;  // = &box->toi_key
 };
 
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
@@ -274,6 +284,16 @@ enum : int {
   DS_NSLOTS = 16
 };
 
+// The host's view of a pass: status word and counters, the exact energy, the minimum time of
+// impact and the Newton dot products, contiguous so that one copy brings them all.
+struct Mailbox {
+  int dstat[DS_NSLOTS];
+  XSum energy;
+  unsigned long long toi_key;  // complemented bits of the minimum time of impact (0: none)
+  double dots[2];              // dq.g, g.g
+};
+
+
 // ---------------------------------------------------------------------------------------
 // launchers (each returns cudaError_t of the launch)
 // ---------------------------------------------------------------------------------------
@@ -285,13 +305,27 @@ cudaError_t radix_sort_pairs(Sim& s, unsigned long long* keys, int* vals, unsign
 
 // broad.cu
 cudaError_t transform(Sim& s, const double* A, const double* p, double* x);
-cudaError_t body_pairs(Sim& s);
-// fused per-body broad phase: body boxes (static, or swept when y1 != null) and leaf boxes.
-// A != null: y0 = x(A, p) (and y1 = x(A1, p1) when A1 != null) are computed here and the
-// traversal bounds internal nodes by the affine images of their rest boxes; A == null: y0 /
-// y1 are given positions and the body subtrees are refit level by level.
+// DOFs of a pass: (A, p) as given, or, when dq is set, (A, p) - alpha dq with alpha read from
+// device memory, written to (Aout, pout) by the broad phase (update_qk, abd.py:154-157)
+struct Dofs {
+  const double *A = nullptr, *p = nullptr;
+  const double* dq = nullptr;
+  const double* alpha = nullptr;  // device scalar
+  double *Aout = nullptr, *pout = nullptr;
+  const double* Aeff() const { return dq ? Aout : A; }
+  const double* peff() const { return dq ? pout : p; }
+};
+
+// Broad phase.  With DOFs (d0, and d1 for swept boxes): y0 = x(d0) (and y1 = x(d1)), one
+// thread per vertex, and the exact body bounds; the traversal bounds internal nodes by the
+// affine images of their rest boxes.  Without (d0 == null): y0 / y1 are given positions, the
+// leaf boxes are stored and the body subtrees refit level by level.
+cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, double* y1);
 cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A1, const double* p1, double* y0,
                        double* y1);
+// body pairs: full (mask, scan, fill: the sorted pair list and the adjacency with pair
+// indices) or mask only (row counts and the bit matrix, all the energy and CCD passes need)
+cudaError_t body_pairs(Sim& s, bool full);
 // rest-frame internal node boxes of both trees (once, at creation)
 cudaError_t rest_boxes(Sim& s);
 

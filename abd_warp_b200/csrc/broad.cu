@@ -71,44 +71,81 @@ __device__ inline Box body_box_of(const unsigned long long* k, bool swept, doubl
   return B;
 }
 
-// One thread per vertex: y0 = x(A, p) (and y1 = x(A1, p1)) with the arithmetic of k_transform,
-// and the body bounds: lanes of a warp that share a body reduce their keys, one lane per
-// (warp, body) updates the body's keys atomically.
-__global__ void __launch_bounds__(256) k_vertex_broad(int V, const int* __restrict__ vbody,
-                                                      const double* __restrict__ x0, const double* __restrict__ A,
-                                                      const double* __restrict__ p, const double* __restrict__ A1,
-                                                      const double* __restrict__ p1, double* y0, double* y1,
-                                                      unsigned long long* bnd) {
-  const int v = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
-  const bool live = v < V;
-  const int b = live ? vbody[v] : -1;
+struct VertexArgs {
+  int V, n;
+  const int* vbody;
+  const double* x0;
+  Dofs d[2];   // d[1] used when swept
+  int swept;
+  double *y0, *y1;
+  unsigned long long* bnd;
+  Mailbox* box;  // accumulators of the pass, cleared here
+};
+
+// DOFs of body b in set k: as given, or (A, p) - alpha dq (same arithmetic as k_update_dofs)
+__device__ inline void body_dofs(const Dofs& d, int b, double M[12]) {
+  if (!d.dq) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) M[k] = d.A[9 * b + k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) M[9 + k] = d.p[3 * b + k];
+    return;
+  }
+  const double al = *d.alpha;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) M[9 + k] = d.p[3 * b + k] - d.dq[12 * b + k] * al;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) M[3 * r + k] = d.A[9 * b + 3 * r + k] - d.dq[12 * b + 3 * (r + 1) + k] * al;
+}
+
+// One thread per vertex (and, for t < n, per body): the body's DOFs of each set (written out
+// when updated), y0 = x(d[0]) (and y1 = x(d[1])) with the arithmetic of k_transform, and the
+// body bounds: lanes of a warp that share a body reduce their keys, one lane per (warp,
+// body) updates the body's keys atomically.  Block 0 clears the pass's accumulators.
+__global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
+  const int t = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
+  if (blockIdx.x == 0) {
+    if (threadIdx.x <= kXD) reinterpret_cast<long long*>(&a.box->energy)[threadIdx.x] = 0;
+    if (threadIdx.x == 32) a.box->toi_key = 0;
+  }
+  const int nset = a.swept ? 2 : 1;
+  if (t < a.n) {
+    for (int k = 0; k < nset; ++k) {
+      if (!a.d[k].dq) continue;
+      double M[12];
+      body_dofs(a.d[k], t, M);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) a.d[k].Aout[9 * t + i] = M[i];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) a.d[k].pout[3 * t + i] = M[9 + i];
+    }
+  }
+  const int v = t;
+  const bool live = v < a.V;
+  const int b = live ? a.vbody[v] : -1;
   unsigned long long key[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) key[k] = 0;
   if (live) {
-    const double r0 = x0[3 * v], r1 = x0[3 * v + 1], r2 = x0[3 * v + 2];
-    const double* m = A + 9 * b;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const double y = ((m[j] * r0 + m[3 + j] * r1) + m[6 + j] * r2) + p[3 * b + j];
-      y0[3 * v + j] = y;
-      key[j] = max_key(-y);
-      key[3 + j] = max_key(y);
-    }
-    if (A1) {
-      const double* m1 = A1 + 9 * b;
+    const double r0 = a.x0[3 * v], r1 = a.x0[3 * v + 1], r2 = a.x0[3 * v + 2];
+    for (int k = 0; k < nset; ++k) {
+      double M[12];
+      body_dofs(a.d[k], b, M);
+      double* y = k ? a.y1 : a.y0;
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const double z = ((m1[j] * r0 + m1[3 + j] * r1) + m1[6 + j] * r2) + p1[3 * b + j];
-        y1[3 * v + j] = z;
-        key[6 + j] = max_key(-z);
-        key[9 + j] = max_key(z);
+        const double c = ((M[j] * r0 + M[3 + j] * r1) + M[6 + j] * r2) + M[9 + j];
+        y[3 * v + j] = c;
+        key[6 * k + j] = max_key(-c);
+        key[6 * k + 3 + j] = max_key(c);
       }
     }
   }
   // segmented reduction: one round per distinct body in the warp (bodies are contiguous)
   unsigned pending = __ballot_sync(0xffffffffu, live);
-  const int nk = A1 ? 12 : 6;
+  const int nk = 6 * nset;
   while (pending) {
     const int lead = __ffs(pending) - 1;
     const int bl = __shfl_sync(0xffffffffu, b, lead);
@@ -123,7 +160,7 @@ __global__ void __launch_bounds__(256) k_vertex_broad(int V, const int* __restri
         const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
         x = y > x ? y : x;
       }
-      if (lane == lead) atomicMax(&bnd[12 * (size_t)bl + k], x);
+      if (lane == lead) atomicMax(&a.bnd[12 * (size_t)bl + k], x);
     }
   }
 }
@@ -139,10 +176,11 @@ constexpr int PR_TILE = 1024;    // body boxes staged in shared memory per tile 
 // of the word popcounts (wpre) and the row counts: all neighbours (rcnt) and neighbours
 // J > I (ucnt), ready for the scan.  Every CTA builds the FP32 boxes of all bodies from the
 // bounds in shared memory (tile by tile) and stores those of its own rows in body_box.
-__global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const unsigned long long* __restrict__ bnd,
-                                                          int swept, double dhh, Box* body_box, uint32_t* mask,
-                                                          int* wpre, int* rcnt, int* ucnt) {
+__global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, unsigned long long* bnd, int swept, double dhh,
+                                                          Box* body_box, uint32_t* mask, int* wpre, int* rcnt,
+                                                          int* ucnt, int* count) {
   __shared__ Box tile[PR_TILE];
+  __shared__ bool last;
   const int I = (int)((blockIdx.x * (unsigned)PR_THREADS + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   const bool row = I < n;
   Box a;
@@ -174,12 +212,24 @@ __global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const un
     rcnt[I] = pre;
     ucnt[I] = pre - low;  // bit I itself is never set
   }
+  // the last CTA to finish clears the bounds for the next broad phase (every CTA has read
+  // all of them by now)
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(count, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  for (int k = threadIdx.x; k < 12 * n; k += PR_THREADS) bnd[k] = 0ULL;
+  if (threadIdx.x == 0) *count = 0;
 }
 
-// Single CTA: exclusive scans of the row counts into row_ptr / upper_ptr (in place; index n
-// gets the totals).  Totals land in dstat; capacities that are short raise
-// ST_PAIR_OVERFLOW (the host grows and reruns).
-__global__ void __launch_bounds__(1024) k_pair_scan(int n, int* row_ptr, int* upper_ptr, int cap_pairs, int cap_adj,
+// Single CTA: exclusive scans of the row counts into row_ptr / upper_ptr (index n gets the
+// totals).  Totals land in dstat; capacities that are short raise ST_PAIR_OVERFLOW (the host
+// grows and reruns).  Also clears the counters of the list / GH passes that follow.
+__global__ void __launch_bounds__(1024) k_pair_scan(int n, const int* rcnt, const int* ucnt, int* row_ptr,
+                                                    int* upper_ptr, int cap_pairs, int cap_adj, int* pair_cand,
                                                     int* dstat) {
   __shared__ int sh[2][33];
   __shared__ int carry[2];
@@ -187,7 +237,7 @@ __global__ void __launch_bounds__(1024) k_pair_scan(int n, int* row_ptr, int* up
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int c0 = 0; c0 < n; c0 += 1024) {
     const int I = c0 + threadIdx.x;
-    const int full = I < n ? row_ptr[I] : 0, upper = I < n ? upper_ptr[I] : 0;
+    const int full = I < n ? rcnt[I] : 0, upper = I < n ? ucnt[I] : 0;
     int xf = full, xu = upper;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -220,12 +270,16 @@ __global__ void __launch_bounds__(1024) k_pair_scan(int n, int* row_ptr, int* up
     if (threadIdx.x < 2) carry[threadIdx.x] = sh[threadIdx.x][32];
     __syncthreads();
   }
+  const int npairs = carry[1];
+  for (int p = threadIdx.x; p < min(npairs, cap_pairs); p += 1024) pair_cand[4 * p + 1] = 0;
   if (threadIdx.x == 0) {
     row_ptr[n] = carry[0];
-    upper_ptr[n] = carry[1];
+    upper_ptr[n] = npairs;
     dstat[DS_NADJ] = carry[0];
-    dstat[DS_NPAIRS] = carry[1];
-    if (carry[1] > cap_pairs || carry[0] > cap_adj) atomicOr(&dstat[DS_STATUS], ST_PAIR_OVERFLOW);
+    dstat[DS_NPAIRS] = npairs;
+    dstat[DS_PT_COUNT] = dstat[DS_EE_COUNT] = dstat[DS_VG_COUNT] = dstat[DS_ACTIVE] = 0;
+    dstat[DS_NCONTACT] = 0;
+    if (npairs > cap_pairs || carry[0] > cap_adj) atomicOr(&dstat[DS_STATUS], ST_PAIR_OVERFLOW);
   }
 }
 
@@ -436,16 +490,37 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
   a.edge_lvl = s.edge_tree.lvl;
   a.tri_blvl = s.tri_tree.body_lvl;
   a.edge_blvl = s.edge_tree.body_lvl;
-  a.refit = !(A && (!y1 || A1));
+  a.refit = 1;
   s.swept = y1 != nullptr;
-  cudaError_t e = cudaMemsetAsync(s.body_bnd, 0, sizeof(unsigned long long) * 12 * (size_t)s.n, s.stream);
-  if (e != cudaSuccess) return e;
-  if (a.refit) {
-    k_body_broad<<<s.n, BB, 0, s.stream>>>(a);
-  } else {
-    if (s.V == 0) return cudaSuccess;
-    k_vertex_broad<<<blocks(s.V, 256), 256, 0, s.stream>>>(s.V, s.vbody, s.x0, A, p, A1, p1, y0, y1, s.body_bnd);
+  if (A && (!y1 || A1)) {  // DOFs given: the vertex-parallel path
+    Dofs d0, d1;
+    d0.A = A;
+    d0.p = p;
+    d1.A = A1;
+    d1.p = p1;
+    return body_broad(s, &d0, y1 ? &d1 : nullptr, y0, y1);
   }
+  k_body_broad<<<s.n, BB, 0, s.stream>>>(a);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, double* y1) {
+  VertexArgs a;
+  a.V = s.V;
+  a.n = s.n;
+  a.vbody = s.vbody;
+  a.x0 = s.x0;
+  a.d[0] = *d0;
+  if (d1) a.d[1] = *d1;
+  a.swept = d1 != nullptr;
+  a.y0 = y0;
+  a.y1 = y1;
+  a.bnd = s.body_bnd;
+  a.box = s.box;
+  s.swept = a.swept;
+  const int t = s.V > s.n ? s.V : s.n;
+  k_vertex_broad<<<blocks(t, 256), 256, 0, s.stream>>>(a);
   ++s.launches;
   return cudaGetLastError();
 }
@@ -456,6 +531,8 @@ cudaError_t rest_boxes(Sim& s) {
   for (Tree* t : {&s.tri_tree, &s.edge_tree})
     if (e == cudaSuccess && t->N > 1)
       e = cudaMemcpyAsync(t->rest, t->box, sizeof(Box) * (size_t)(t->N - 1), cudaMemcpyDeviceToDevice, s.stream);
+  // no pair pass follows: clear the bounds here (the pair mask clears them otherwise)
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.body_bnd, 0, sizeof(unsigned long long) * 12 * (size_t)s.n, s.stream);
   return e;
 }
 
@@ -466,19 +543,25 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
   return cudaGetLastError();
 }
 
-// Body pairs I < J with overlapping boxes (the ij list, sorted) and the symmetric CSR
-// adjacency (row I: neighbours in increasing J, with the pair index of {I, J}).  Counts stay
-// on the device (dstat DS_NPAIRS / DS_NADJ); a short capacity raises ST_PAIR_OVERFLOW and
-// leaves the lists incomplete, for the host to grow and rerun at its next read of dstat.
-cudaError_t body_pairs(Sim& s) {
+// Body pairs I < J with overlapping boxes: the bit matrix and row counts, and when `full` the
+// sorted ij list and the symmetric CSR adjacency (row I: neighbours in increasing J, with
+// the pair index of {I, J}).  Counts stay on the device (dstat DS_NPAIRS / DS_NADJ); a short
+// capacity raises ST_PAIR_OVERFLOW and leaves the lists incomplete, for the host to grow and
+// rerun at its next read of dstat.
+cudaError_t body_pairs(Sim& s, bool full) {
   const int n = s.n, W = s.W;
   k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(
-      n, W, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box, s.pair_mask, s.pair_wpre, s.row_ptr, s.upper_ptr);
-  k_pair_scan<<<1, 1024, 0, s.stream>>>(n, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj, s.dstat);
-  k_pair_fill<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.pair_wpre, s.row_ptr,
-                                                                   s.upper_ptr, s.cap_pairs, s.cap_adj, s.ij,
-                                                                   s.adj_col, s.adj_pair);
-  s.launches += 3;
+      n, W, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box, s.pair_mask, s.pair_wpre, s.row_cnt, s.upper_cnt,
+      s.kcount);
+  ++s.launches;
+  if (full) {
+    k_pair_scan<<<1, 1024, 0, s.stream>>>(n, s.row_cnt, s.upper_cnt, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj,
+                                          s.pair_cand, s.dstat);
+    k_pair_fill<<<blocks((long long)n * W, 256), 256, 0, s.stream>>>(n, W, s.pair_mask, s.pair_wpre, s.row_ptr,
+                                                                     s.upper_ptr, s.cap_pairs, s.cap_adj, s.ij,
+                                                                     s.adj_col, s.adj_pair);
+    s.launches += 2;
+  }
   return cudaGetLastError();
 }
 

@@ -37,7 +37,10 @@ struct NarrowArgs {
   abd_params prm;
   int n, cap_adj;
   const int2* ij;
-  const int *row_ptr, *adj_col;
+  const int *row_ptr, *adj_col, *row_cnt;
+  const uint32_t* pair_mask;
+  const int* pair_wpre;
+  int W;
   const Box* body_box;
   const int2* chunk;
   const int* adj_pair;
@@ -527,6 +530,21 @@ __device__ inline void toi_min(unsigned long long* key, double t) {
 constexpr int CT = kChunk;  // threads per chunk CTA
 constexpr int NBB = 64;     // neighbours staged per batch
 
+// The k-th neighbour (increasing order) of body I from the overlap bit matrix: the word by
+// binary search over the row's prefix counts, then the bit inside it.
+__device__ inline int kth_neighbour(const NarrowArgs& a, int I, int k) {
+  const int* pre = a.pair_wpre + (size_t)I * a.W;
+  int lo = 0, hi = a.W - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= k) lo = mid;
+    else hi = mid - 1;
+  }
+  uint32_t m = a.pair_mask[(size_t)I * a.W + lo];
+  for (int r = k - pre[lo]; r > 0; --r) m &= m - 1;
+  return 32 * lo + __ffs(m) - 1;
+}
+
 // Which body of a pair {I, J} queries the other's edge tree for the EE candidates: the one
 // with more edges (ties: the higher index), so that a body with few edges and many
 // neighbours (a ground box) does not serialise them.  The candidate set does not depend on
@@ -601,23 +619,32 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
     if (!ccd && tid == 0 && !a.fixed[I])
       xs_add_atomic(&xe, inertia_energy(a.prm, a.st, a.mass, a.I0, I, a.A + 9 * I, a.p + 3 * I));
   }
-  const bool ok = !(a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW);  // an overflowed pass is rerun
-  const int r0 = a.row_ptr[I], r1 = min(a.row_ptr[I + 1], a.cap_adj);
-  for (int b0 = (ok && Q > 0) ? r0 : r1; b0 < r1; b0 += NBB) {
-    const int nb = min(NBB, r1 - b0);
+  // neighbours of I in increasing order: GH from the adjacency (it needs the pair indices;
+  // an overflowed pass is rerun), ENERGY / CCD straight from the overlap bit matrix
+  int r0 = 0, deg;
+  if constexpr (gh) {
+    r0 = a.row_ptr[I];
+    deg = (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW) ? 0 : min(a.row_ptr[I + 1], a.cap_adj) - r0;
+  } else {
+    deg = a.row_cnt[I];
+  }
+  if (Q == 0) deg = 0;
+  for (int b0 = 0; b0 < deg; b0 += NBB) {
+    const int nb = min(NBB, deg - b0);
     __syncthreads();
     if (tid < nb) {
-      const int J = a.adj_col[b0 + tid];
+      const int J = gh ? a.adj_col[r0 + b0 + tid] : kth_neighbour(a, I, b0 + tid);
       nJ[tid] = J;
       nbox[tid] = load_box(&a.body_box[J]);
       ntri[tid] = a.tri.body_root[J];
       nedge[tid] = a.edge.body_root[J];
       nown[tid] = ee_owner(I, nEI, J, a.eoff[J + 1] - a.eoff[J]);
-      if (gh) npair[tid] = a.adj_pair[b0 + tid];
+      if (gh) npair[tid] = a.adj_pair[r0 + b0 + tid];
     }
+    __syncthreads();
     for (int e = tid; e < 24 * nb; e += CT) {
       const int j = e / 24, t = (e / 12) & 1, cc = e % 12;
-      const int J = a.adj_col[b0 + j];
+      const int J = nJ[j];
       const double* A = t ? a.A1 : a.A;
       const double* pp = t ? a.p1 : a.p;
       if (!t || a.y1) ndof[j][cc + 12 * t] = (float)(cc < 9 ? A[9 * J + cc] : pp[3 * J + cc - 9]);
@@ -931,6 +958,10 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.ij = s.ij;
   a.row_ptr = s.row_ptr;
   a.adj_col = s.adj_col;
+  a.row_cnt = s.row_cnt;
+  a.pair_mask = s.pair_mask;
+  a.pair_wpre = s.pair_wpre;
+  a.W = s.W;
   a.body_box = s.body_box;
   a.chunk = s.chunk;
   a.energy = s.energy_acc;

@@ -151,31 +151,49 @@ int grow_lists(Sim& s, int need_pt, int need_ee) {
 }
 
 // Boxes, body pairs and the narrow pass of `mode` on positions y0 (static) or y0 -> y1
-// (swept), all asynchronous: counts and overflow bits stay in dstat until the caller's next
-// read (sync_read), after which overflow() grows what was short and asks for a rerun.
-// A != null: y0 (and y1 when A1 != null) are computed from the DOFs inside the broad-phase
-// kernel; otherwise y0 / y1 are given positions.
-int culling(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* y0,
-            double* y1, int mode, const abd_states* st = nullptr) {
+// (swept), all asynchronous: counts and overflow bits stay in the mailbox until the caller's
+// next read (sync_read), after which overflow() grows what was short and asks for a rerun.
+// d0 != null: y0 (and y1 when d1 != null) are computed from the DOFs by the broad phase;
+// otherwise y0 / y1 are given positions.
+int culling(abd_sim* h, const abd::Dofs* d0, const abd::Dofs* d1, double* y0, double* y1, int mode,
+            const abd_states* st = nullptr) {
   Sim& s = h->s;
-  CK(abd::body_broad(s, A, p, A1, p1, y0, y1));
-  CK(abd::body_pairs(s));
-  if (mode == abd::NARROW_GH || mode == abd::NARROW_LISTS)  // PT, EE, VG and active counters
-    CK(cudaMemsetAsync(s.dstat + abd::DS_PT_COUNT, 0, 4 * sizeof(int), s.stream));
-  if (mode == abd::NARROW_ENERGY) CK(cudaMemsetAsync(s.energy_acc, 0, sizeof(abd::XSum), s.stream));
-  if (mode == abd::NARROW_CCD) CK(cudaMemsetAsync(s.dmin, 0, sizeof(unsigned long long), s.stream));
-  CK(abd::narrow(s, mode, A, p, A1, p1, y0, y1, st));
+  if (d0) CK(abd::body_broad(s, d0, d1, y0, y1));
+  else CK(abd::body_broad(s, nullptr, nullptr, nullptr, nullptr, y0, y1));
+  const bool full = mode == abd::NARROW_GH || mode == abd::NARROW_LISTS;
+  CK(abd::body_pairs(s, full));
+  CK(abd::narrow(s, mode, d0 ? d0->Aeff() : nullptr, d0 ? d0->peff() : nullptr, d1 ? d1->Aeff() : nullptr,
+                 d1 ? d1->peff() : nullptr, y0, y1, st));
   return ABD_OK;
 }
 
-// One synchronisation: the dstat mirror plus `nbytes` bytes from `dev` into hval (and, when
-// act is set, the active-pair list into hact).  Updates the host pair counts.
-int sync_read(Sim& s, const void* dev, size_t nbytes, bool act = false) {
-  CK(cudaMemcpyAsync(s.hstat, s.dstat, abd::DS_NSLOTS * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-  if (nbytes > 0) CK(cudaMemcpyAsync(s.hval, dev, nbytes, cudaMemcpyDeviceToHost, s.stream));
+abd::Dofs direct(const double* A, const double* p) {
+  abd::Dofs d;
+  d.A = A;
+  d.p = p;
+  return d;
+}
+
+// (A, p) - alpha dq into (Aout, pout), alpha = s.dpar[slot] on the device
+abd::Dofs updated(Sim& s, const double* A, const double* p, int slot, double* Aout, double* pout) {
+  abd::Dofs d;
+  d.A = A;
+  d.p = p;
+  d.dq = s.dq;
+  d.alpha = s.dpar + slot;
+  d.Aout = Aout;
+  d.pout = pout;
+  return d;
+}
+
+// One synchronisation: the mailbox (status, counters, energy, time of impact, dots) and,
+// when act is set, the active-pair list.  Updates the host mirror and pair counts.
+int sync_read(Sim& s, bool act = false) {
+  CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
   if (act && s.cap_act > 0)
     CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
   CK(cudaStreamSynchronize(s.stream));
+  std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
   s.n_pairs = s.hstat[abd::DS_NPAIRS];
   s.n_adj = s.hstat[abd::DS_NADJ];
   return ABD_OK;
@@ -213,49 +231,40 @@ int overflow(Sim& s) {
 
 constexpr int kMaxReruns = 6;
 
-// E(Ak, pk): barrier over the culling lists at xk + inertia (compute_energy, abd.py:133-141),
-// summed exactly on the device and rounded here
-int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* pk, double* E) {
+// E at the DOFs d: barrier over the culling lists + inertia (compute_energy, abd.py:133-141),
+// summed exactly on the device and rounded here.  The energy pass has no capacities.
+int energy_of(abd_sim* h, const abd_states& st, const abd::Dofs& d, double* E) {
   Sim& s = h->s;
-  for (int tries = 0;; ++tries) {
-    int r = culling(h, Ak, pk, nullptr, nullptr, s.xk, nullptr, abd::NARROW_ENERGY, &st);
-    if (r) return r;
-    if ((r = sync_read(s, s.energy_acc, sizeof(abd::XSum)))) return r;
-    if ((r = overflow(s)) > 0) return r;
-    if (r == 0) break;
-    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
-  }
-  abd::XSum x;
-  std::memcpy(&x, s.hval, sizeof(x));
-  *E = xs_round_host(x);
+  int r = culling(h, &d, nullptr, s.xk, nullptr, abd::NARROW_ENERGY, &st);
+  if (r) return r;
+  if ((r = sync_read(s))) return r;
+  *E = xs_round_host(s.hbox->energy);
   return ABD_OK;
 }
 
-// CCD bound between DOFs (A, p) and (A1, p1) (ccd, abd.py:278-303); positions land in x, xk.
-// The dot products scal[10], scal[11] (dq.g, g.g of the step) ride along in the same read
-// (out: dots[2]).
-int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
-           double* raw, double* dots = nullptr) {
+int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* pk, double* E) {
+  return energy_of(h, st, direct(Ak, pk), E);
+}
+
+// Energy at q - alpha dq (written to Ak, pk): one trial of the line search (abd.py:146-160)
+int energy_trial(abd_sim* h, const abd_states& st, double alpha, double* E) {
   Sim& s = h->s;
-  for (int tries = 0;; ++tries) {
-    int r = culling(h, A, p, A1, p1, s.x, s.xk, abd::NARROW_CCD);
-    if (r) return r;
-    if (dots) CK(cudaMemcpyAsync(s.hval + 1, s.scal + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    if ((r = sync_read(s, s.dmin, sizeof(unsigned long long)))) return r;
-    if ((r = overflow(s)) > 0) return r;
-    if (r == 0) break;
-    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
-  }
-  unsigned long long key;
-  std::memcpy(&key, s.hval, sizeof(key));
+  s.hpar[0] = alpha;
+  CK(cudaMemcpyAsync(s.dpar, s.hpar, sizeof(double), cudaMemcpyHostToDevice, s.stream));
+  return energy_of(h, st, updated(s, st.A, st.p, 0, st.Ak, st.pk), E);
+}
+
+// CCD bound between DOFs d0 and d1 (ccd, abd.py:278-303); positions land in x, xk.  The
+// mailbox's dots (dq.g, g.g of the step) ride along in the same read.
+int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, double* raw) {
+  Sim& s = h->s;
+  int r = culling(h, &d0, &d1, s.x, s.xk, abd::NARROW_CCD);
+  if (r) return r;
+  if ((r = sync_read(s))) return r;
   double toi = 1.0;
-  if (key) {
+  if (const unsigned long long key = s.hbox->toi_key) {
     const unsigned long long bits = ~key;
     std::memcpy(&toi, &bits, sizeof(toi));
-  }
-  if (dots) {
-    dots[0] = s.hval[1];
-    dots[1] = s.hval[2];
   }
   if (raw) *raw = toi;
   double t = std::max(0.0, std::min(1.0, toi));
@@ -264,15 +273,21 @@ int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const
   return ABD_OK;
 }
 
+int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
+           double* raw) {
+  return ccd_of(h, direct(A, p), direct(A1, p1), alpha, raw);
+}
+
 // Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner
 int gh_at(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active) {
   Sim& s = h->s;
+  const abd::Dofs d = direct(A, p);
   for (int tries = 0;; ++tries) {
-    int r = culling(h, A, p, nullptr, nullptr, s.x, nullptr, abd::NARROW_GH);
+    int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
     if (r) return r;
     CK(abd::body_gh(s, st, A, p, s.x));
     CK(abd::pair_weights(s));
-    if ((r = sync_read(s, nullptr, 0, true))) return r;
+    if ((r = sync_read(s, true))) return r;
     if ((r = overflow(s)) > 0) return r;
     if (r == 0) break;
     if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
@@ -418,17 +433,34 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
   ok(dalloc(&s.red_count, abd::kRedSlots));
   ok(dalloc(&s.scal, 32));
-  ok(dalloc(&s.energy_acc, 1));
-  ok(dalloc(&s.dstat, abd::DS_NSLOTS));
-  ok(dalloc(&s.dmin, 4));
+
+  ok(dalloc(&s.box, 1));
+  if (e == cudaSuccess) {
+    s.dstat = s.box->dstat;
+    s.energy_acc = &s.box->energy;
+    s.dmin = &s.box->toi_key;
+  }
+  ok(dalloc(&s.dpar, 4));
+  ok(dalloc(&s.row_cnt, n));
+  ok(dalloc(&s.upper_cnt, n));
+  ok(dalloc(&s.kcount, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hbox, sizeof(abd::Mailbox), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, 4 * sizeof(double), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 32 * sizeof(double), cudaHostAllocDefault);
   // preconditioner tables: cl_ptr, cl_body, body_cl (ints), cl_off (8-byte aligned long longs)
   s.cap_hstage = sizeof(int) * (3 * (size_t)n + 2) + sizeof(long long) * ((size_t)n + 2);
   if (e == cudaSuccess) e = cudaHostAlloc(&s.hstage, s.cap_hstage, cudaHostAllocDefault);
   if (e == cudaSuccess) e = abd::rest_boxes(s);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat, 0, sizeof(int) * abd::DS_NSLOTS, s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.kcount, 0, 4 * sizeof(int), s.stream);
+  if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, 0}
+    s.hpar[0] = 0.0;
+    s.hpar[1] = 1.0;
+    s.hpar[2] = s.hpar[3] = 0.0;
+    e = cudaMemcpyAsync(s.dpar, s.hpar, 4 * sizeof(double), cudaMemcpyHostToDevice, s.stream);
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(s.red_count, 0, sizeof(int) * abd::kRedSlots, s.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
   if (tcd) cudaFree(tcd);
@@ -464,12 +496,12 @@ int abd_sim_destroy(abd_sim* h) {
                   s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
                   s.pair_active, s.pair_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
-                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.dstat, s.dmin,
+                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.row_cnt, s.upper_cnt, s.kcount,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
-                  s.energy_acc, s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair};
+                  s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact})
+  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar})
     if (q) cudaFreeHost(q);
   delete h;
   return ABD_OK;
@@ -536,11 +568,12 @@ namespace {
 int cull_lists(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* y0,
                double* y1, int counts[4]) {
   Sim& s = h->s;
+  const abd::Dofs d0 = direct(A, p), d1 = direct(A1, p1);
   for (int tries = 0;; ++tries) {
-    int r = culling(h, A, p, A1, p1, y0, y1, abd::NARROW_LISTS);
+    int r = culling(h, A ? &d0 : nullptr, A && A1 ? &d1 : nullptr, y0, y1, abd::NARROW_LISTS);
     if (r) return r;
     CK(y1 ? abd::vg_list_swept(s, y0, y1) : abd::vg_list(s, y0));
-    if ((r = sync_read(s, nullptr, 0))) return r;
+    if ((r = sync_read(s))) return r;
     if ((r = overflow(s)) > 0) return r;
     if (r == 0) break;
     if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
@@ -629,8 +662,7 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
   abd_step_info inf{};
   int r;
   double E0;
-  CK(abd::update_dofs(s, st.A, st.p, s.dq, 0.0, st.Ak, st.pk));
-  if ((r = energy_at(h, st, st.Ak, st.pk, &E0))) return r;
+  if ((r = energy_trial(h, st, 0.0, &E0))) return r;  // Ak = A - 0 dq
   int it = 0;
   for (;;) {
     int nact = 0;
@@ -646,18 +678,16 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
     inf.linear_iters += lin;
     // dq.g and g.g (abd.py:148, 265), read back together with the CCD bound
-    CK(abd::dot(s, s.dq, s.g, 10, s.scal + 10));
-    CK(abd::dot(s, s.g, s.g, 11, s.scal + 11));
-    // CCD bound (abd.py:278-303)
-    CK(abd::update_dofs(s, st.A, st.p, s.dq, 1.0, st.Ak, st.pk));
-    double alpha, dots[2];
-    if ((r = ccd_at(h, st.A, st.p, st.Ak, st.pk, &alpha, &inf.toi, dots))) return r;
-    const double qTg = dots[0], gTg = dots[1];
+    CK(abd::dot(s, s.dq, s.g, 10, &s.box->dots[0]));
+    CK(abd::dot(s, s.g, s.g, 11, &s.box->dots[1]));
+    // CCD bound between q and q - dq (abd.py:278-303); Ak, pk = q - dq
+    double alpha;
+    if ((r = ccd_of(h, direct(st.A, st.p), updated(s, st.A, st.p, 1, st.Ak, st.pk), &alpha, &inf.toi))) return r;
+    const double qTg = s.hbox->dots[0], gTg = s.hbox->dots[1];
     // backtracking line search (abd.py:146-160)
     double E1 = E0;
     for (;;) {
-      CK(abd::update_dofs(s, st.A, st.p, s.dq, alpha, st.Ak, st.pk));
-      if ((r = energy_at(h, st, st.Ak, st.pk, &E1))) return r;
+      if ((r = energy_trial(h, st, alpha, &E1))) return r;
       ++inf.ls_trials;
       const bool wolfe = E1 < E0 + P.armijo_sign * P.c1 * alpha * qTg ||
                          std::fabs(E1 - E0) <= P.ls_noise_floor * std::fabs(E0);
