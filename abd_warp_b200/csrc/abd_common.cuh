@@ -171,6 +171,13 @@ struct Tree {
 // ---------------------------------------------------------------------------------------
 struct Mailbox;
 
+// one captured pass (see abd_graph.cuh)
+struct GraphSlot {
+  cudaGraphExec_t exec = nullptr;
+  uint64_t key = 0;
+  long long nlaunch = 0;  // kernels per replay
+};
+
 struct Sim {
   cudaStream_t stream = 0;
   abd_params prm{};
@@ -220,6 +227,12 @@ struct Sim {
   int* upper_cnt = nullptr;        // [n] neighbours J > I
   int* kcount = nullptr;           // [4] last-CTA counters of single-pass kernels
   double* dpar = nullptr;          // device pass parameters: [0] trial step, [1] = 1
+  int* dint = nullptr;             // device integers: [0] preconditioner clusters
+  int* hint = nullptr;             // pinned staging of dint
+  // captured passes: energy trial, CCD bound, GH, Krylov setup and one block of iterations
+  cudaStream_t cap_stream = nullptr;
+  GraphSlot g_energy, g_ccd, g_gh, g_kinit, g_kblock;
+  unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
   double* hpar = nullptr;          // pinned staging of dpar
 
   // candidate lists
@@ -281,6 +294,7 @@ enum : int {
   DS_NADJ = 8,       // adjacency entries (2 x pairs)
   DS_NACTP = 9,      // active pairs appended by pair_weights
   DS_NCONTACT = 12,  // active contacts appended by the GH pass
+  DS_IT = 13,        // Krylov iteration counter (device-side, for replayed blocks)
   DS_NSLOTS = 16
 };
 

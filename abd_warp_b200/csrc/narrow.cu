@@ -1050,9 +1050,8 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
       k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
                                                                            s.contacts_by_pair, s.dstat);
-      const int smem = NOUT * (int)sizeof(XSum);
-      e = cudaFuncSetAttribute(k_pair_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e != cudaSuccess) return e;
+      constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
+      static_assert(smem + 4096 <= 48 * 1024, "pair assembly shared memory");
       k_pair_assemble<<<s.cap_pairs, NT, smem, s.stream>>>(a);
       s.launches += 3;
     }

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "abd_common.cuh"
+#include "abd_graph.cuh"
 
 namespace abd {
 cudaError_t vg_list_swept(Sim& s, const double* y0, const double* y1);
@@ -231,13 +232,30 @@ int overflow(Sim& s) {
 
 constexpr int kMaxReruns = 6;
 
+uint64_t states_key(const Sim& s, const abd_states& st) {
+  abd::KeyHash k;
+  k.add(st.A).add(st.p).add(st.Ak).add(st.pk).add(st.A0).add(st.p0).add(st.Adot).add(st.pdot);
+  k.add(s.prm_version).add(s.dq).add(s.x).add(s.xk).add(s.box);
+  return k.h;
+}
+
 // E at the DOFs d: barrier over the culling lists + inertia (compute_energy, abd.py:133-141),
 // summed exactly on the device and rounded here.  The energy pass has no capacities.
-int energy_of(abd_sim* h, const abd_states& st, const abd::Dofs& d, double* E) {
+// g: replay slot for the step's trials (the DOFs then depend only on device data).
+int energy_of(abd_sim* h, const abd_states& st, const abd::Dofs& d, double* E, abd::GraphSlot* g = nullptr,
+              uint64_t key = 0) {
   Sim& s = h->s;
-  int r = culling(h, &d, nullptr, s.xk, nullptr, abd::NARROW_ENERGY, &st);
+  auto issue = [&]() -> int {
+    if (d.dq && cudaMemcpyAsync(s.dpar, s.hpar, sizeof(double), cudaMemcpyHostToDevice, s.stream)) return ABD_ERR_CUDA;
+    int r = culling(h, &d, nullptr, s.xk, nullptr, abd::NARROW_ENERGY, &st);
+    if (r) return r;
+    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
+    return ABD_OK;
+  };
+  int r = g ? abd::run_graph(s, *g, key, issue) : issue();
   if (r) return r;
-  if ((r = sync_read(s))) return r;
+  CK(cudaStreamSynchronize(s.stream));
+  std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
   *E = xs_round_host(s.hbox->energy);
   return ABD_OK;
 }
@@ -249,21 +267,31 @@ int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* 
 // Energy at q - alpha dq (written to Ak, pk): one trial of the line search (abd.py:146-160)
 int energy_trial(abd_sim* h, const abd_states& st, double alpha, double* E) {
   Sim& s = h->s;
-  s.hpar[0] = alpha;
-  CK(cudaMemcpyAsync(s.dpar, s.hpar, sizeof(double), cudaMemcpyHostToDevice, s.stream));
-  return energy_of(h, st, updated(s, st.A, st.p, 0, st.Ak, st.pk), E);
+  s.hpar[0] = alpha;  // copied to dpar[0] by the pass itself
+  return energy_of(h, st, updated(s, st.A, st.p, 0, st.Ak, st.pk), E, &s.g_energy, states_key(s, st));
 }
 
-// CCD bound between DOFs d0 and d1 (ccd, abd.py:278-303); positions land in x, xk.  The
-// mailbox's dots (dq.g, g.g of the step) ride along in the same read.
-int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, double* raw) {
+// CCD bound between DOFs d0 and d1 (ccd, abd.py:278-303); positions land in x, xk.  pre()
+// enqueues work that belongs to the same pass (the step's dot products, whose results ride
+// along in the mailbox).
+template <class Pre>
+int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, double* raw, Pre&& pre,
+           abd::GraphSlot* g = nullptr, uint64_t key = 0) {
   Sim& s = h->s;
-  int r = culling(h, &d0, &d1, s.x, s.xk, abd::NARROW_CCD);
+  auto issue = [&]() -> int {
+    int r = pre();
+    if (r) return r;
+    if ((r = culling(h, &d0, &d1, s.x, s.xk, abd::NARROW_CCD))) return r;
+    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
+    return ABD_OK;
+  };
+  int r = g ? abd::run_graph(s, *g, key, issue) : issue();
   if (r) return r;
-  if ((r = sync_read(s))) return r;
+  CK(cudaStreamSynchronize(s.stream));
+  std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
   double toi = 1.0;
-  if (const unsigned long long key = s.hbox->toi_key) {
-    const unsigned long long bits = ~key;
+  if (const unsigned long long key2 = s.hbox->toi_key) {
+    const unsigned long long bits = ~key2;
     std::memcpy(&toi, &bits, sizeof(toi));
   }
   if (raw) *raw = toi;
@@ -275,25 +303,51 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
 
 int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
            double* raw) {
-  return ccd_of(h, direct(A, p), direct(A1, p1), alpha, raw);
+  return ccd_of(h, direct(A, p), direct(A1, p1), alpha, raw, []() -> int { return ABD_OK; });
 }
 
-// Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner
-int gh_at(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active) {
+// Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner.
+// g: replay slot for the step (its key covers every capacity the captured grids depend on).
+int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active,
+          abd::GraphSlot* g = nullptr) {
   Sim& s = h->s;
   const abd::Dofs d = direct(A, p);
-  for (int tries = 0;; ++tries) {
+  auto issue = [&]() -> int {
     int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
     if (r) return r;
     CK(abd::body_gh(s, st, A, p, s.x));
     CK(abd::pair_weights(s));
-    if ((r = sync_read(s, true))) return r;
+    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
+    if (s.cap_act > 0)
+      CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
+    return ABD_OK;
+  };
+  for (int tries = 0;; ++tries) {
+    int r;
+    if (g) {
+      abd::KeyHash k;
+      k.add(states_key(s, st)).add(A).add(p).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
+      k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
+      k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.hact);
+      r = abd::run_graph(s, *g, k.h, issue);
+    } else {
+      r = issue();
+    }
+    if (r) return r;
+    CK(cudaStreamSynchronize(s.stream));
+    std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
+    s.n_pairs = s.hstat[abd::DS_NPAIRS];
+    s.n_adj = s.hstat[abd::DS_NADJ];
     if ((r = overflow(s)) > 0) return r;
     if (r == 0) break;
     if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
   }
   if (n_active) *n_active = s.hstat[abd::DS_ACTIVE];
   return ABD_OK;
+}
+
+int gh_at(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active) {
+  return gh_of(h, st, A, p, n_active);
 }
 
 int take_status(abd_sim* h) {
@@ -441,12 +495,15 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     s.dmin = &s.box->toi_key;
   }
   ok(dalloc(&s.dpar, 4));
+  ok(dalloc(&s.dint, 4));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   ok(dalloc(&s.row_cnt, n));
   ok(dalloc(&s.upper_cnt, n));
   ok(dalloc(&s.kcount, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hbox, sizeof(abd::Mailbox), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, 4 * sizeof(double), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hint, 4 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 32 * sizeof(double), cudaHostAllocDefault);
   // preconditioner tables: cl_ptr, cl_body, body_cl (ints), cl_off (8-byte aligned long longs)
   s.cap_hstage = sizeof(int) * (3 * (size_t)n + 2) + sizeof(long long) * ((size_t)n + 2);
@@ -496,12 +553,17 @@ int abd_sim_destroy(abd_sim* h) {
                   s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
                   s.pair_active, s.pair_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
-                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.row_cnt, s.upper_cnt, s.kcount,
+                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.dint,
+                  s.row_cnt, s.upper_cnt, s.kcount,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar})
+  for (abd::GraphSlot* g : {&s.g_energy, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_kblock})
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
+  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar,
+                  (void*)s.hint})
     if (q) cudaFreeHost(q);
   delete h;
   return ABD_OK;
@@ -510,6 +572,7 @@ int abd_sim_destroy(abd_sim* h) {
 int abd_sim_set_params(abd_sim* h, const abd_params* prm) {
   if (!h || !prm) return ABD_ERR_INVALID;
   h->s.prm = *prm;
+  ++h->s.prm_version;  // parameters are kernel arguments of the captured passes
   return ABD_OK;
 }
 
@@ -666,7 +729,7 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
   int it = 0;
   for (;;) {
     int nact = 0;
-    if ((r = gh_at(h, st, st.A, st.p, &nact))) return r;
+    if ((r = gh_of(h, st, st.A, st.p, &nact, &s.g_gh))) return r;
     if (it == 0) {
       inf.n_pt = s.hstat[abd::DS_PT_COUNT];
       inf.n_ee = s.hstat[abd::DS_EE_COUNT];
@@ -678,11 +741,17 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
     inf.linear_iters += lin;
     // dq.g and g.g (abd.py:148, 265), read back together with the CCD bound
-    CK(abd::dot(s, s.dq, s.g, 10, &s.box->dots[0]));
-    CK(abd::dot(s, s.g, s.g, 11, &s.box->dots[1]));
-    // CCD bound between q and q - dq (abd.py:278-303); Ak, pk = q - dq
+    // dq.g, g.g (abd.py:148, 265) and the CCD bound between q and q - dq (abd.py:278-303),
+    // one pass; Ak, pk = q - dq
     double alpha;
-    if ((r = ccd_of(h, direct(st.A, st.p), updated(s, st.A, st.p, 1, st.Ak, st.pk), &alpha, &inf.toi))) return r;
+    auto dots = [&]() -> int {
+      CK(abd::dot(s, s.dq, s.g, 10, &s.box->dots[0]));
+      CK(abd::dot(s, s.g, s.g, 11, &s.box->dots[1]));
+      return ABD_OK;
+    };
+    if ((r = ccd_of(h, direct(st.A, st.p), updated(s, st.A, st.p, 1, st.Ak, st.pk), &alpha, &inf.toi, dots,
+                    &s.g_ccd, states_key(s, st))))
+      return r;
     const double qTg = s.hbox->dots[0], gTg = s.hbox->dots[1];
     // backtracking line search (abd.py:146-160)
     double E1 = E0;

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "abd_common.cuh"
+#include "abd_graph.cuh"
 
 namespace abd {
 
@@ -48,7 +49,9 @@ struct SolverArgs {
   const double *diag, *offdiag;
   const int *row_ptr, *adj_col, *adj_pair, *pair_active, *fixed;
   const int2* ij;
-  int ncl;
+  int ncl;            // clusters (setup kernel)
+  const int* ncl_dev; // clusters (device copy: the replayed Krylov kernels read it)
+  int maxit;
   const int *cl_ptr, *cl_body;
   const long long* cl_off;
   double* cl_inv;
@@ -141,6 +144,12 @@ __device__ inline bool solver_done(const int* dstat) {
   return ((volatile const int*)dstat)[DS_R_DONE] != 0 || ((volatile const int*)dstat)[DS_S_DONE] != 0;
 }
 
+// the current Krylov iteration (device counter advanced by k_next_iteration); iterations
+// beyond the limit do nothing, so a replayed block may overrun it harmlessly
+__device__ inline int iteration(const SolverArgs& a) { return a.dstat[DS_IT]; }
+
+__global__ void k_next_iteration(int* dstat) { dstat[DS_IT] += 1; }
+
 // ---- preconditioner setup: assemble and invert each cluster's dense block system ----
 __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, int c1, const int* body_cl) {
   extern __shared__ double K[];
@@ -204,12 +213,13 @@ __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, in
 // into copy (if not null)
 __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out,
                                               double* copy, int slot) {
-  if (it_guard && solver_done(a.dstat)) return;
+  if (it_guard && (solver_done(a.dstat) || iteration(a) > a.maxit)) return;
   __shared__ double vs[12 * kMaxCluster];
   XSum d0, d1;
   xs_zero(d0);
   xs_zero(d1);
-  for (int c = blockIdx.x; c < a.ncl; c += gridDim.x) {
+  const int ncl = *a.ncl_dev;
+  for (int c = blockIdx.x; c < ncl; c += gridDim.x) {
     const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
     for (int i = threadIdx.x; i < D; i += AT) vs[i] = in[(size_t)a.cl_body[base + i / 12] * 12 + i % 12];
     __syncthreads();
@@ -252,8 +262,9 @@ __global__ void __launch_bounds__(256) k_residual(SolverArgs a, const double* bv
 
 // ---- PCG ----
 // K1: converged if r.z <= thr^2; else Ap = A p with partial p.Ap
-__global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, int it, const double* pv, double* Ap) {
-  if (solver_done(a.dstat)) return;
+__global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, const double* pv, double* Ap) {
+  const int it = iteration(a);
+  if (solver_done(a.dstat) || it > a.maxit) return;
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
   const int slots[1] = {rz};
   double sc[1];
@@ -281,9 +292,10 @@ __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, int it, const doubl
 }
 
 // K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature)
-__global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, int it, const double* pv, const double* Ap, double* x,
+__global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, const double* pv, const double* Ap, double* x,
                                                double* r) {
-  if (solver_done(a.dstat)) return;
+  const int it = iteration(a);
+  if (solver_done(a.dstat) || it > a.maxit) return;
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
   const int slots[2] = {rz, SL_PAP};
   double sc[2];
@@ -308,8 +320,9 @@ __global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, int it, const doubl
 }
 
 // K3 (after z = M r with partial r.z into the new slot): beta = rz_new / rz_old; p = z + beta p
-__global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, int it, const double* z, double* pv) {
-  if (solver_done(a.dstat)) return;
+__global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, const double* z, double* pv) {
+  const int it = iteration(a);
+  if (solver_done(a.dstat) || it > a.maxit) return;
   const int rz_old = (it & 1) ? SL_RZ0 : SL_RZ1, rz_new = (it & 1) ? SL_RZ1 : SL_RZ0;
   const int slots[2] = {rz_new, rz_old};
   double sc[2];
@@ -327,8 +340,9 @@ __global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, int it, const doubl
 
 // ---- BiCGSTAB (right preconditioned) ----
 // K1: converged if r.M^-1 r small; rho = rh.r; p = r + beta (p - omega v)
-__global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, int it, const double* r, double* pv, const double* v) {
-  if (solver_done(a.dstat)) return;
+__global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, const double* r, double* pv, const double* v) {
+  const int it = iteration(a);
+  if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[2] = {SL_RZ0, SL_RHR};
   double sc[2];
   cta_scalars(a, slots, 2, sc);
@@ -356,7 +370,7 @@ __global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, int it, const doub
 // out = A in; partials w0.out (slot0), w1.out (slot1)
 __global__ void __launch_bounds__(256) k_spmv(SolverArgs a, const double* in, double* out, const double* w0, int slot0,
                                               const double* w1, int slot1) {
-  if (solver_done(a.dstat)) return;
+  if (solver_done(a.dstat) || iteration(a) > a.maxit) return;
   const int lane = threadIdx.x & 31;
   XSum d0, d1;
   xs_zero(d0);
@@ -374,8 +388,9 @@ __global__ void __launch_bounds__(256) k_spmv(SolverArgs a, const double* in, do
 }
 
 // K3: alpha = rho / rh.v; s = r - alpha v
-__global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, int it, const double* r, const double* v, double* s) {
-  if (solver_done(a.dstat)) return;
+__global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, const double* r, const double* v, double* s) {
+  const int it = iteration(a);
+  if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[1] = {SL_RHV};
   double sc[1];
   cta_scalars(a, slots, 1, sc);
@@ -391,9 +406,10 @@ __global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, int it, const doub
 }
 
 // K4 (after z = M s with partial s.z): if small, x += alpha y and stop
-__global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, int it, const double* y, double* x) {
+__global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, const double* y, double* x) {
+  const int it = iteration(a);
   const volatile int* ds = a.dstat;
-  if (ds[DS_R_DONE] != 0 || (ds[DS_S_DONE] != 0 && ds[DS_S_DONE] != it)) return;
+  if (ds[DS_R_DONE] != 0 || (ds[DS_S_DONE] != 0 && ds[DS_S_DONE] != it) || it > a.maxit) return;
   const int slots[1] = {SL_SZ};
   double sc[1];
   cta_scalars(a, slots, 1, sc);
@@ -413,10 +429,11 @@ __global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, int it, const doub
 }
 
 // K6: omega = t.s / t.t; x += alpha y + omega z; r = s - omega t; partial rh.r
-__global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, int it, const double* y, const double* z,
+__global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, const double* z,
                                                 const double* s, const double* t, const double* rh, double* x,
                                                 double* r) {
-  if (solver_done(a.dstat)) return;
+  const int it = iteration(a);
+  if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[2] = {SL_TS, SL_TT};
   double sc[2];
   cta_scalars(a, slots, 2, sc);
@@ -484,6 +501,8 @@ SolverArgs solver_args(Sim& s) {
   a.fixed = s.fixed;
   a.ij = s.ij;
   a.ncl = s.ncl;
+  a.ncl_dev = s.dint;
+  a.maxit = s.prm.cg_max_iter;
   a.cl_ptr = s.cl_ptr;
   a.cl_body = s.cl_body;
   a.cl_off = s.cl_off;
@@ -587,7 +606,9 @@ int build_preconditioner(Sim& s) {
   }
   // body -> cluster map rides in the scratch vector zb (as ints) during the setup kernel
   int* body_cl_dev = reinterpret_cast<int*>(s.zb);
-  if (cudaMemcpyAsync(s.cl_ptr, cl_ptr, sizeof(int) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
+  s.hint[0] = ncl;
+  if (cudaMemcpyAsync(s.dint, s.hint, sizeof(int), cudaMemcpyHostToDevice, s.stream) ||
+      cudaMemcpyAsync(s.cl_ptr, cl_ptr, sizeof(int) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
       cudaMemcpyAsync(s.cl_body, cl_body, sizeof(int) * n, cudaMemcpyHostToDevice, s.stream) ||
       cudaMemcpyAsync(s.cl_off, cl_off, sizeof(long long) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
       cudaMemcpyAsync(body_cl_dev, body_cl, sizeof(int) * n, cudaMemcpyHostToDevice, s.stream))
@@ -603,59 +624,75 @@ int build_preconditioner(Sim& s) {
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
-// Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.
+// Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  The setup and each
+// block of kCheckEvery iterations are replayed graphs; the host reads the convergence flags
+// (in the mailbox) after every block.
 int krylov_solve(Sim& s, double* x, int* iters_out) {
-  SolverArgs a = solver_args(s);
+  const SolverArgs a = solver_args(s);
   const double* bvec = s.g;
-  cudaStream_t st = s.stream;
   const bool pcg = s.prm.solver == 1;
-  // b^T M^-1 b sets the threshold
-  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
-  k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
-                                         pcg ? nullptr : s.v);
-  s.launches += 2;
-  cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st);
-  cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st);
-  k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x);
-  ++s.launches;
-  // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
-  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
-  ++s.launches;
+  KeyHash kh;
+  kh.add(x).add(s.n).add(s.prm_version).add(s.prm.solver).add(s.prm.cg_max_iter).add(s.cl_inv).add(s.box);
+  const uint64_t key = kh.h;
+  int r = run_graph(s, s.g_kinit, key, [&]() -> int {
+    cudaStream_t st = s.stream;
+    // b^T M^-1 b sets the threshold
+    k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
+    k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
+                                           pcg ? nullptr : s.v);
+    if (cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st) ||
+        cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st) ||
+        cudaMemsetAsync(s.dstat + DS_IT, 0, sizeof(int), st))
+      return ABD_ERR_CUDA;
+    k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x);
+    // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
+    k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
+    s.launches += 4;
+    return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+  });
+  if (r) return r;
   const int maxit = s.prm.cg_max_iter;
-  int it = 1;
-  for (;;) {
-    for (int k = 0; k < kCheckEvery && it <= maxit; ++k, ++it) {
-      if (pcg) {
-        const int rz_new = (it & 1) ? SL_RZ1 : SL_RZ0;
-        k_pcg_1<<<kRedBlocks, 256, 0, st>>>(a, it, s.pv, s.v);
-        k_pcg_2<<<kRedBlocks, 256, 0, st>>>(a, it, s.pv, s.v, x, s.r);
-        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.z, nullptr, rz_new);
-        k_pcg_3<<<kRedBlocks, 256, 0, st>>>(a, it, s.z, s.pv);
-        s.launches += 4;
-      } else {
-        k_bicg_1<<<kRedBlocks, 256, 0, st>>>(a, it, s.r, s.pv, s.v);
-        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.pv, s.y, nullptr, -1);
-        k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
-        k_bicg_3<<<kRedBlocks, 256, 0, st>>>(a, it, s.r, s.v, s.s);
-        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
-        k_bicg_4<<<kRedBlocks, 256, 0, st>>>(a, it, s.y, x);
-        k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
-        k_bicg_6<<<kRedBlocks, 256, 0, st>>>(a, it, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-        k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
-        s.launches += 9;
+  for (int done = 0;;) {
+    r = run_graph(s, s.g_kblock, key, [&]() -> int {
+      cudaStream_t st = s.stream;
+      // iterations start at odd numbers (1, 1 + kCheckEvery, ...), so each position of the
+      // block has a fixed parity and the alternating r.z slots are the same in every block
+      for (int k = 0; k < kCheckEvery; ++k) {
+        k_next_iteration<<<1, 1, 0, st>>>(s.dstat);
+        if (pcg) {
+          const int rz_new = ((1 + k) & 1) ? SL_RZ1 : SL_RZ0;
+          k_pcg_1<<<kRedBlocks, 256, 0, st>>>(a, s.pv, s.v);
+          k_pcg_2<<<kRedBlocks, 256, 0, st>>>(a, s.pv, s.v, x, s.r);
+          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.z, nullptr, rz_new);
+          k_pcg_3<<<kRedBlocks, 256, 0, st>>>(a, s.z, s.pv);
+          s.launches += 5;
+        } else {
+          k_bicg_1<<<kRedBlocks, 256, 0, st>>>(a, s.r, s.pv, s.v);
+          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.pv, s.y, nullptr, -1);
+          k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
+          k_bicg_3<<<kRedBlocks, 256, 0, st>>>(a, s.r, s.v, s.s);
+          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
+          k_bicg_4<<<kRedBlocks, 256, 0, st>>>(a, s.y, x);
+          k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
+          k_bicg_6<<<kRedBlocks, 256, 0, st>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
+          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
+          s.launches += 10;
+        }
       }
-    }
-    if (cudaGetLastError() != cudaSuccess) return ABD_ERR_CUDA;
-    cudaMemcpyAsync(s.hstat + 18, s.dstat + DS_R_DONE, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(s.hstat + 20, s.dstat + DS_SOLVER_ITERS, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return ABD_ERR_CUDA;
-    if (s.hstat[18] || s.hstat[19]) break;
-    if (it > maxit) {
+      if (cudaMemcpyAsync(s.hbox, s.box, sizeof(Mailbox), cudaMemcpyDeviceToHost, st)) return ABD_ERR_CUDA;
+      return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+    });
+    if (r) return r;
+    if (cudaStreamSynchronize(s.stream) != cudaSuccess) return ABD_ERR_CUDA;
+    done += kCheckEvery;
+    const int* ds = s.hbox->dstat;
+    if (ds[DS_R_DONE] || ds[DS_S_DONE]) break;
+    if (done >= maxit) {
       s.host_status |= ST_SOLVER_NOCONV;  // not converged: reported through the status bits
       break;
     }
   }
-  if (iters_out) *iters_out = s.hstat[20];
+  if (iters_out) *iters_out = s.hbox->dstat[DS_SOLVER_ITERS];
   return ABD_OK;
 }
 
