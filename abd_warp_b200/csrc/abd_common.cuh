@@ -26,6 +26,7 @@ enum : int {
   ST_VG_OVERFLOW = 64,     // VG list capacity exceeded
   ST_ACT_OVERFLOW = 128,   // active-pair list capacity exceeded (host grows and reruns)
   ST_CONTACT_OVERFLOW = 256,  // active-contact list capacity exceeded (host grows and reruns)
+  ST_CCD_OVERFLOW = 512,   // CCD candidate list capacity exceeded (host grows and reruns)
 };
 
 constexpr int kTraversalStack = 64;
@@ -219,11 +220,15 @@ struct Sim {
   // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
+  Box* chunk_box = nullptr;        // [nch] rest-frame box of each chunk's items
+  int* vperm = nullptr;            // [V] vertices of each body in Morton order (chunk items)
   XSum* energy_acc = nullptr;      // = &box->energy
   // everything the host reads after a pass, in one device block (one copy per sync)
   Mailbox* box = nullptr;          // device
   Mailbox* hbox = nullptr;         // pinned host mirror
   int* row_cnt = nullptr;          // [n] neighbours of each body (pair mask)
+  int* nbr = nullptr;              // [n][kNbList] first neighbours of each body (pair mask)
+  float* fdof = nullptr;           // [n][2][12] FP32 DOFs of the last broad phase
   int* upper_cnt = nullptr;        // [n] neighbours J > I
   int* kcount = nullptr;           // [4] last-CTA counters of single-pass kernels
   double* dpar = nullptr;          // device pass parameters: [0] trial step, [1] = 1
@@ -231,8 +236,16 @@ struct Sim {
   int* hint = nullptr;             // pinned staging of dint
   // captured passes: energy trial, CCD bound, GH, Krylov setup and one block of iterations
   cudaStream_t cap_stream = nullptr;
-  GraphSlot g_energy, g_ccd, g_gh, g_kinit, g_kblock;
+  GraphSlot g_energy, g_energy_ev, g_ccd, g_gh, g_kinit, g_kblock;
   unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
+  // kernel profiling of the energy pass's narrow kernel: CUDA events around it (recorded as
+  // graph nodes), its duration and algorithmic bytes accumulated after every pass
+  int prof_on = 0;                 // 0 off, 1 time every kProfEvery-th pass, 2 time and count all
+  int prof_events = 0;             // this pass records the events
+  long long prof_tick = 0;
+  cudaEvent_t prof_ev[2] = {nullptr, nullptr};
+  double prof_ms = 0.0, prof_bytes = 0.0;
+  long long prof_launches = 0;
   double* hpar = nullptr;          // pinned staging of dpar
 
   // candidate lists
@@ -249,6 +262,8 @@ struct Sim {
   // appended in any order, then grouped by pair (pair_cand[4p]: offset, count, fill)
   int cap_contacts = 0;
   int4 *contacts = nullptr, *contacts_by_pair = nullptr;
+  int cap_ccd = 0;
+  int4* ccd_cand = nullptr;        // CCD candidates (type, primitive a, primitive b)
   int list_counts[4] = {0, 0, 0, 0};  // pairs, PT, EE, VG of the last list culling
   double* pair_val = nullptr;      // [cap_pairs] energy or toi per pair
 
@@ -279,6 +294,7 @@ struct Sim {
 
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
 constexpr int kChunk = 128;       // items per chunk of the energy / CCD narrow passes
+constexpr int kNbList = 32;       // neighbours per body listed by the pair mask
 constexpr int kRedSlots = 12;
 
 // dstat layout
@@ -295,6 +311,7 @@ enum : int {
   DS_NACTP = 9,      // active pairs appended by pair_weights
   DS_NCONTACT = 12,  // active contacts appended by the GH pass
   DS_IT = 13,        // Krylov iteration counter (device-side, for replayed blocks)
+  DS_NCCD = 14,      // CCD candidates appended by the CCD pass
   DS_NSLOTS = 16
 };
 
@@ -305,7 +322,22 @@ struct Mailbox {
   XSum energy;
   unsigned long long toi_key;  // complemented bits of the minimum time of impact (0: none)
   double dots[2];              // dq.g, g.g
+  // work counters of the energy pass's narrow kernel (kernel profiling only), spread over
+  // 32 rows against atomic contention: [row][PF_*]
+  unsigned long long prof[32][8];
 };
+
+// counters of the energy pass's narrow kernel: the data it reads, per kind of access
+enum : int {
+  PF_POINT = 0,      // point queries: FP64 position (24 B)
+  PF_EDGE = 1,       // edge queries: two vertex ids + two positions (56 B)
+  PF_NEIGHBOUR = 2,  // (chunk, neighbour) records: body box, FP32 DOFs, roots (140 B)
+  PF_NODE = 3,       // internal tree nodes tested: rest box + child ids (40 B)
+  PF_TRI = 4,        // triangle leaves tested: three ids + three positions (84 B)
+  PF_EDGELEAF = 5,   // edge leaves tested: two ids + two positions (56 B)
+  PF_N = 6
+};
+constexpr double kProfBytes[PF_N] = {24.0, 56.0, 140.0, 40.0, 84.0, 56.0};
 
 
 // ---------------------------------------------------------------------------------------
@@ -360,8 +392,9 @@ cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
                         double* pout);
 cudaError_t finish_step(Sim& s, const abd_states& st, double* xview);
-// exact dot product of two [n][12] vectors into *out_dev (reduction slot `slot`)
-cudaError_t dot(Sim& s, const double* a, const double* b, int slot, double* out_dev);
+// exact dot products a.b (and c.d when c != null) of [n][12] vectors into out_dev[0], [1]
+// (reduction slots 10 and 11)
+cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev);
 
 // solver.cu
 int build_preconditioner(Sim& s);                 // returns ABD status

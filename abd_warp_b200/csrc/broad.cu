@@ -79,6 +79,7 @@ struct VertexArgs {
   int swept;
   double *y0, *y1;
   unsigned long long* bnd;
+  float* fdof;   // [n][2][12] FP32 DOFs (A row-major, p) of each set
   Mailbox* box;  // accumulators of the pass, cleared here
 };
 
@@ -101,33 +102,39 @@ __device__ inline void body_dofs(const Dofs& d, int b, double M[12]) {
 }
 
 // One thread per vertex (and, for t < n, per body): the body's DOFs of each set (written out
-// when updated), y0 = x(d[0]) (and y1 = x(d[1])) with the arithmetic of k_transform, and the
-// body bounds: lanes of a warp that share a body reduce their keys, one lane per (warp,
-// body) updates the body's keys atomically.  Block 0 clears the pass's accumulators.
+// when updated, and as FP32 copies for the traversal's node boxes), y0 = x(d[0]) (and
+// y1 = x(d[1])) with the arithmetic of k_transform, and the body bounds: lanes of a warp that
+// share a body reduce their coordinates (min / max are exact), one lane per (warp, body)
+// updates the body's keys atomically.  Block 0 clears the pass's accumulators.
 __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
   const int t = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
   if (blockIdx.x == 0) {
     if (threadIdx.x <= kXD) reinterpret_cast<long long*>(&a.box->energy)[threadIdx.x] = 0;
     if (threadIdx.x == 32) a.box->toi_key = 0;
+    static_assert(sizeof(a.box->prof) / sizeof(unsigned long long) == 256, "one counter per thread");
+    (&a.box->prof[0][0])[threadIdx.x] = 0;
   }
   const int nset = a.swept ? 2 : 1;
   if (t < a.n) {
     for (int k = 0; k < nset; ++k) {
-      if (!a.d[k].dq) continue;
       double M[12];
       body_dofs(a.d[k], t, M);
+      if (a.d[k].dq) {
 #pragma unroll
-      for (int i = 0; i < 9; ++i) a.d[k].Aout[9 * t + i] = M[i];
+        for (int i = 0; i < 9; ++i) a.d[k].Aout[9 * t + i] = M[i];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) a.d[k].pout[3 * t + i] = M[9 + i];
+        for (int i = 0; i < 3; ++i) a.d[k].pout[3 * t + i] = M[9 + i];
+      }
+      float4* f = reinterpret_cast<float4*>(a.fdof + 24 * (size_t)t + 12 * k);
+      f[0] = make_float4((float)M[0], (float)M[1], (float)M[2], (float)M[3]);
+      f[1] = make_float4((float)M[4], (float)M[5], (float)M[6], (float)M[7]);
+      f[2] = make_float4((float)M[8], (float)M[9], (float)M[10], (float)M[11]);
     }
   }
   const int v = t;
   const bool live = v < a.V;
   const int b = live ? a.vbody[v] : -1;
-  unsigned long long key[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) key[k] = 0;
+  double c[6];
   if (live) {
     const double r0 = a.x0[3 * v], r1 = a.x0[3 * v + 1], r2 = a.x0[3 * v + 2];
     for (int k = 0; k < nset; ++k) {
@@ -136,73 +143,90 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
       double* y = k ? a.y1 : a.y0;
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const double c = ((M[j] * r0 + M[3 + j] * r1) + M[6 + j] * r2) + M[9 + j];
-        y[3 * v + j] = c;
-        key[6 * k + j] = max_key(-c);
-        key[6 * k + 3 + j] = max_key(c);
+        const double cj = ((M[j] * r0 + M[3 + j] * r1) + M[6 + j] * r2) + M[9 + j];
+        y[3 * v + j] = cj;
+        c[3 * k + j] = cj;
       }
     }
   }
   // segmented reduction: one round per distinct body in the warp (bodies are contiguous)
   unsigned pending = __ballot_sync(0xffffffffu, live);
-  const int nk = 6 * nset;
   while (pending) {
     const int lead = __ffs(pending) - 1;
     const int bl = __shfl_sync(0xffffffffu, b, lead);
     const bool mine = live && b == bl;
     pending &= ~__ballot_sync(0xffffffffu, mine);
-#pragma unroll
-    for (int k = 0; k < 12; ++k) {
-      if (k >= nk) break;
-      unsigned long long x = mine ? key[k] : 0ULL;
+    for (int k = 0; k < 3 * nset; ++k) {
+      double lo = mine ? c[k] : INFINITY, hi = mine ? c[k] : -INFINITY;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
-        x = y > x ? y : x;
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
       }
-      if (lane == lead) atomicMax(&a.bnd[12 * (size_t)bl + k], x);
+      if (lane == lead) {
+        const int set = k / 3, j = k % 3;
+        atomicMax(&a.bnd[12 * (size_t)bl + 6 * set + j], max_key(-lo));
+        atomicMax(&a.bnd[12 * (size_t)bl + 6 * set + 3 + j], max_key(hi));
+      }
     }
   }
+}
+
+// FP32 body boxes from the bounds (one thread per body), which are cleared for the next pass
+__global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double dhh, Box* body_box) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  unsigned long long k[12];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    k[i] = bnd[12 * (size_t)b + i];
+    bnd[12 * (size_t)b + i] = 0ULL;
+  }
+  store_box(&body_box[b], body_box_of(k, swept, dhh));
 }
 
 // ---------------------------------------------------------------------------------------
 // body pairs: overlap bit matrix, per-row prefix counts, then O(1) placement of every pair
 // ---------------------------------------------------------------------------------------
-constexpr int PR_THREADS = 256;  // one warp per row of the overlap matrix
+constexpr int PR_THREADS = 128;  // one warp per row of the overlap matrix
 constexpr int PR_TILE = 1024;    // body boxes staged in shared memory per tile (32 KB)
 
 // Row I of the overlap matrix, one warp: lane l tests J = 32 w + l and the ballot is word w
 // (word w covers J in [32w, 32w + 32)).  The warp also keeps the per-row exclusive prefix
-// of the word popcounts (wpre) and the row counts: all neighbours (rcnt) and neighbours
-// J > I (ucnt), ready for the scan.  Every CTA builds the FP32 boxes of all bodies from the
-// bounds in shared memory (tile by tile) and stores those of its own rows in body_box.
-__global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, unsigned long long* bnd, int swept, double dhh,
-                                                          Box* body_box, uint32_t* mask, int* wpre, int* rcnt,
-                                                          int* ucnt, int* count) {
-  __shared__ Box tile[PR_TILE];
-  __shared__ bool last;
+// of the word popcounts (wpre), the row counts -- all neighbours (rcnt) and neighbours J > I
+// (ucnt) -- and the first kNbList neighbours in increasing order (nbr).
+__global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const Box* __restrict__ body_box,
+                                                          uint32_t* mask, int* wpre, int* rcnt, int* ucnt,
+                                                          int* nbr) {
+  __shared__ float4 tile[2 * PR_TILE];
   const int I = (int)((blockIdx.x * (unsigned)PR_THREADS + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   const bool row = I < n;
-  Box a;
-  if (row) {
-    a = body_box_of(bnd + 12 * (size_t)I, swept, dhh);
-    if (lane == 0) store_box(&body_box[I], a);
-  }
+  const Box a = row ? load_box(&body_box[I]) : Box{};
+  const float4* src = reinterpret_cast<const float4*>(body_box);
   int pre = 0, low = 0;
   for (int j0 = 0; j0 < n; j0 += PR_TILE) {
     const int jn = min(PR_TILE, n - j0);
     __syncthreads();
-    for (int k = threadIdx.x; k < jn; k += PR_THREADS) tile[k] = body_box_of(bnd + 12 * (size_t)(j0 + k), swept, dhh);
+    for (int k = threadIdx.x; k < 2 * jn; k += PR_THREADS) tile[k] = __ldg(&src[2 * (size_t)j0 + k]);
     __syncthreads();
     if (!row) continue;
     for (int wl = 0; wl < (jn + 31) / 32; ++wl) {
       const int jl = 32 * wl + lane, J = j0 + jl;
-      const bool hit = jl < jn && J != I && overlap(a, tile[jl]);
+      bool hit = false;
+      if (jl < jn && J != I) {
+        const float4 lo = tile[2 * jl], hi = tile[2 * jl + 1];
+        hit = !(a.lo[0] > hi.x || lo.x > a.hi[0] || a.lo[1] > hi.y || lo.y > a.hi[1] || a.lo[2] > hi.z ||
+                lo.z > a.hi[2]);
+      }
       const uint32_t bits = __ballot_sync(0xffffffffu, hit);
       const int w = (j0 >> 5) + wl;
       if (lane == 0) {
         mask[(size_t)I * W + w] = bits;
         wpre[(size_t)I * W + w] = pre;
+      }
+      if (hit) {
+        const int pos = pre + __popc(bits & ((1u << lane) - 1u));
+        if (pos < kNbList) nbr[(size_t)I * kNbList + pos] = J;
       }
       if (w == (I >> 5)) low = pre + __popc(bits & ((1u << (I & 31)) - 1u));
       pre += __popc(bits);
@@ -212,17 +236,6 @@ __global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, unsigned
     rcnt[I] = pre;
     ucnt[I] = pre - low;  // bit I itself is never set
   }
-  // the last CTA to finish clears the bounds for the next broad phase (every CTA has read
-  // all of them by now)
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(count, 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  for (int k = threadIdx.x; k < 12 * n; k += PR_THREADS) bnd[k] = 0ULL;
-  if (threadIdx.x == 0) *count = 0;
 }
 
 // Single CTA: exclusive scans of the row counts into row_ptr / upper_ptr (index n gets the
@@ -517,6 +530,7 @@ cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, doubl
   a.y0 = y0;
   a.y1 = y1;
   a.bnd = s.body_bnd;
+  a.fdof = s.fdof;
   a.box = s.box;
   s.swept = a.swept;
   const int t = s.V > s.n ? s.V : s.n;
@@ -550,10 +564,10 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
 // rerun at its next read of dstat.
 cudaError_t body_pairs(Sim& s, bool full) {
   const int n = s.n, W = s.W;
-  k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(
-      n, W, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box, s.pair_mask, s.pair_wpre, s.row_cnt, s.upper_cnt,
-      s.kcount);
-  ++s.launches;
+  k_body_boxes<<<blocks(n, 128), 128, 0, s.stream>>>(n, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box);
+  k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(n, W, s.body_box, s.pair_mask, s.pair_wpre,
+                                                                         s.row_cnt, s.upper_cnt, s.nbr);
+  s.launches += 2;
   if (full) {
     k_pair_scan<<<1, 1024, 0, s.stream>>>(n, s.row_cnt, s.upper_cnt, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj,
                                           s.pair_cand, s.dstat);

@@ -19,6 +19,8 @@
 // vertex-ground terms (vg_ipc.py:4-34, culling.py:54-82, ccd.py:9-18, energy.py:24-33).
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include "abd_common.cuh"
 #include "abd_geometry.cuh"
 
@@ -40,13 +42,21 @@ struct NarrowArgs {
   const int *row_ptr, *adj_col, *row_cnt;
   const uint32_t* pair_mask;
   const int* pair_wpre;
+  const int* nbr;
+  const float* fdof;
+  const Box* chunk_box;
+  const int* vperm;
   int W;
   const Box* body_box;
   const int2* chunk;
   const int* adj_pair;
+  int cap_ccd;
+  int4* ccd_cand;
   int cap_contacts;
   int4 *contacts, *contacts_by_pair;
-  XSum* energy;                       // exact energy of the pass
+  XSum* energy;
+  int prof;                     // kernel profiling: count the data read into prof rows
+  unsigned long long* prof_rows;                       // exact energy of the pass
   unsigned long long* toi_key;        // complemented bits of the minimum time of impact
   abd_states st;
   const double *mass, *I0;
@@ -126,16 +136,29 @@ struct NodeBoxes {
 
 // Stack traversal of the subtree rooted at `root`; calls f(prim) for every leaf whose box
 // overlaps q, in a fixed depth-first order.
+// visits: tested internal nodes and leaves (kernel profiling)
+struct Visits {
+  unsigned internal = 0, leaf = 0;
+};
+
 template <class F>
 __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int* dstat, F&& f) {
+  Visits v;
+  traverse(nb, root, q, dstat, f, v);
+}
+
+template <class F>
+__device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int* dstat, F&& f, Visits& cnt) {
   if (root < 0) return;
   const Tree& tr = *nb.tr;
   const int L0 = tr.N - 1;
   if (root >= L0) {
     const int prim = __ldg(&tr.leaf_prim[root - L0]);
+    ++cnt.leaf;
     if (overlap(nb.leaf(root, prim), q)) f(prim);
     return;
   }
+  ++cnt.internal;
   if (!overlap(nb.internal(root), q)) return;
   int stack[kTraversalStack];
   int sp = 0;
@@ -148,8 +171,9 @@ __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int
       const int c = h ? c1 : c0;
       if (c >= L0) {
         const int prim = __ldg(&tr.leaf_prim[c - L0]);
+        ++cnt.leaf;
         if (overlap(nb.leaf(c, prim), q)) f(prim);
-      } else if (overlap(nb.internal(c), q)) {
+      } else if (++cnt.internal, overlap(nb.internal(c), q)) {
         if (sp < kTraversalStack) stack[sp++] = c;
         else atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
       }
@@ -528,6 +552,7 @@ __device__ inline void toi_min(unsigned long long* key, double t) {
 // energy / CCD passes: one CTA per chunk of one body's points and edges
 // ---------------------------------------------------------------------------------------
 constexpr int CT = kChunk;  // threads per chunk CTA
+constexpr int kNoQuery = INT_MIN;  // a chunk item whose primitive kind is disabled
 constexpr int NBB = 64;     // neighbours staged per batch
 
 // The k-th neighbour (increasing order) of body I from the overlap bit matrix: the word by
@@ -570,28 +595,29 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   const int2 ch = a.chunk[c];
   const int I = ch.x;
   const int nEI = a.eoff[I + 1] - a.eoff[I];
-  const int nV = a.prm.enable_pt ? a.voff[I + 1] - a.voff[I] : 0;
-  const int nE = a.prm.enable_ee ? nEI : 0;
-  const int Q = max(0, min(CT, nV + nE - ch.y));
+  const int nV = a.voff[I + 1] - a.voff[I];  // items: the body's points, then its edges
+  const int Q = max(0, min(CT, nV + nEI - ch.y));
   __shared__ Box qbox[CT];
-  __shared__ int qprim[CT];  // point id, or ~edge id
+  __shared__ int qprim[CT];  // point id, ~edge id, or kNoQuery (primitive kind disabled)
   __shared__ Box nbox[NBB];
-  __shared__ float ndof[NBB][24];
-  __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB];
+  __shared__ __align__(16) float ndof[NBB][24];
+  __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB], nrel[NBB];
   __shared__ unsigned short work[CW];
   __shared__ int nwork;
   __shared__ XSum xe;
   __shared__ unsigned long long tkey;
-  if (tid < Q) {
-    const int k = ch.y + tid;
-    if (k < nV) {
-      const int v = a.voff[I] + k;
-      qprim[tid] = v;
-      qbox[tid] = point_box(a.y0, a.y1, v, (float)a.prm.dhat);
-    } else {
-      const int e = a.eoff[I] + (k - nV);
-      qprim[tid] = ~e;
-      qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
+  __shared__ Box cbx;  // the chunk's world box: every query box of the chunk lies inside
+  if (tid == 0 && Q > 0) {
+    const Box R = load_box(&a.chunk_box[c]);
+    const float pad = __double2float_ru(a.prm.dhat);
+    cbx = affine_box(R, a.fdof + 24 * (size_t)I, pad);
+    if (a.y1) {
+      const Box B1 = affine_box(R, a.fdof + 24 * (size_t)I + 12, pad);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        cbx.lo[k] = fminf(cbx.lo[k], B1.lo[k]);
+        cbx.hi[k] = fmaxf(cbx.hi[k], B1.hi[k]);
+      }
     }
   }
   if (ccd) {
@@ -601,6 +627,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   }
   __syncthreads();
   int cpt = 0, cee = 0;  // GH: candidates found by this thread
+  unsigned pf_node = 0, pf_tri = 0, pf_edge = 0;  // profiling: tree nodes and leaves tested
   // the body's own terms, in its first chunk (GH: the body kernel adds them)
   if (!gh && ch.y == 0) {
     const Box bb = load_box(&a.body_box[I]);
@@ -629,25 +656,51 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
     deg = a.row_cnt[I];
   }
   if (Q == 0) deg = 0;
+  bool loaded = false;  // queries are loaded when the first neighbour overlaps the chunk
   for (int b0 = 0; b0 < deg; b0 += NBB) {
     const int nb = min(NBB, deg - b0);
     __syncthreads();
+    int rel = 0;
     if (tid < nb) {
-      const int J = gh ? a.adj_col[r0 + b0 + tid] : kth_neighbour(a, I, b0 + tid);
+      const int k = b0 + tid;
+      const int J = gh ? a.adj_col[r0 + k] : (k < kNbList ? a.nbr[(size_t)I * kNbList + k] : kth_neighbour(a, I, k));
       nJ[tid] = J;
       nbox[tid] = load_box(&a.body_box[J]);
+      rel = overlap(cbx, nbox[tid]) ? 1 : 0;
+      nrel[tid] = rel;
       ntri[tid] = a.tri.body_root[J];
       nedge[tid] = a.edge.body_root[J];
       nown[tid] = ee_owner(I, nEI, J, a.eoff[J + 1] - a.eoff[J]);
       if (gh) npair[tid] = a.adj_pair[r0 + b0 + tid];
     }
-    __syncthreads();
-    for (int e = tid; e < 24 * nb; e += CT) {
-      const int j = e / 24, t = (e / 12) & 1, cc = e % 12;
-      const int J = nJ[j];
-      const double* A = t ? a.A1 : a.A;
-      const double* pp = t ? a.p1 : a.p;
-      if (!t || a.y1) ndof[j][cc + 12 * t] = (float)(cc < 9 ? A[9 * J + cc] : pp[3 * J + cc - 9]);
+    if (!__syncthreads_or(rel)) continue;  // the chunk touches none of these neighbours
+    if (!loaded) {
+      loaded = true;
+      if (tid < Q) {
+        const int k = ch.y + tid;
+        if (k < nV) {
+          const int v = __ldg(&a.vperm[a.voff[I] + k]);
+          qprim[tid] = a.prm.enable_pt ? v : kNoQuery;
+          qbox[tid] = point_box(a.y0, a.y1, v, (float)a.prm.dhat);
+        } else {
+          const int e = __ldg(&a.edge.leaf_prim[a.eoff[I] + (k - nV)]);
+          qprim[tid] = a.prm.enable_ee ? ~e : kNoQuery;
+          qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
+        }
+      }
+      if constexpr (MODE == NARROW_ENERGY) {
+        if (a.prof && tid == 0) {
+          const int qp = max(0, min(Q, nV - ch.y));
+          atomicAdd(&a.prof_rows[8 * (blockIdx.x & 31) + PF_POINT], (unsigned long long)qp);
+          atomicAdd(&a.prof_rows[8 * (blockIdx.x & 31) + PF_EDGE], (unsigned long long)(Q - qp));
+        }
+      }
+    }
+    // FP32 DOFs of the neighbours, as the broad phase wrote them (6 x 16 B per neighbour)
+    for (int e = tid; e < 6 * nb; e += CT) {
+      const int j = e / 6, q = e % 6;
+      if (q < 3 || a.y1)
+        reinterpret_cast<float4*>(ndof[j])[q] = __ldg(reinterpret_cast<const float4*>(a.fdof + 24 * (size_t)nJ[j]) + q);
     }
     for (int w0 = 0; w0 < Q * nb; w0 += CW) {
       if (tid == 0) nwork = 0;
@@ -655,7 +708,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       // overlapping (query, neighbour) combinations of this round
       for (int it = w0 + tid; it < min(Q * nb, w0 + CW); it += CT) {
         const int q = it % Q, j = it / Q;
-        if (qprim[q] < 0 && !nown[j]) continue;
+        if (!nrel[j] || qprim[q] == kNoQuery || (qprim[q] < 0 && !nown[j])) continue;
         if (!overlap(qbox[q], nbox[j])) continue;
         work[atomicAdd(&nwork, 1)] = (unsigned short)(q | (j << 8));
       }
@@ -666,9 +719,11 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
         const Box qb = qbox[q];
         auto visit = [&](int type, int pa, int pb) {
           int ids[4];
-          cand_vertices(a, type, pa, pb, ids);
           d3 xs[4];
-          fetch(a.y0, ids, xs);
+          if constexpr (!ccd) {
+            cand_vertices(a, type, pa, pb, ids);
+            fetch(a.y0, ids, xs);
+          }
           if constexpr (gh) {
             if (type == 0) ++cpt;
             else ++cee;
@@ -683,22 +738,28 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
               atomicAdd(&a.pair_cand[4 * pr + 1], 1);
             }
           } else if constexpr (ccd) {
-            d3 x1[4];
-            fetch(a.y1, ids, x1);
-            const double t = collision_time(type, xs, x1);
-            if (t < 1.0) toi_min(&tkey, t);
+            // evaluated by k_ccd_eval, one thread per candidate
+            const int pos = atomicAdd(&a.dstat[DS_NCCD], 1);
+            if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
+            else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
           } else {
             const double e = contact_energy(type, xs, a.prm);
             if (e != 0.0) xs_add_atomic(&xe, e);
           }
         };
         if (qp >= 0) {
-          traverse(node_boxes(a, &a.tri, true, ndof[j]), ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); });
+          Visits vc;
+          traverse(node_boxes(a, &a.tri, true, ndof[j]), ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); }, vc);
+          pf_node += vc.internal;
+          pf_tri += vc.leaf;
         } else {
           // EE candidates are evaluated with the edge of the lower body first, as the per-pair lists
           const bool lower = I < nJ[j];
+          Visits vc;
           traverse(node_boxes(a, &a.edge, false, ndof[j]), nedge[j], qb, a.dstat,
-                   [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); });
+                   [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); }, vc);
+          pf_node += vc.internal;
+          pf_edge += vc.leaf;
         }
       }
       __syncthreads();
@@ -716,6 +777,21 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
     }
     return;
   }
+  if (MODE == NARROW_ENERGY && a.prof) {  // kernel profiling: the data this chunk read
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      pf_node += __shfl_xor_sync(0xffffffffu, pf_node, o);
+      pf_tri += __shfl_xor_sync(0xffffffffu, pf_tri, o);
+      pf_edge += __shfl_xor_sync(0xffffffffu, pf_edge, o);
+    }
+    unsigned long long* row = a.prof_rows + 8 * (blockIdx.x & 31);
+    if ((tid & 31) == 0) {
+      atomicAdd(&row[PF_NODE], (unsigned long long)pf_node);
+      atomicAdd(&row[PF_TRI], (unsigned long long)pf_tri);
+      atomicAdd(&row[PF_EDGELEAF], (unsigned long long)pf_edge);
+    }
+    if (tid == 0 && deg > 0) atomicAdd(&row[PF_NEIGHBOUR], (unsigned long long)deg);
+  }
   __syncthreads();
   if (tid == 0) {
     if constexpr (ccd) {
@@ -728,6 +804,21 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       if (src[kXD]) atomicOr((unsigned long long*)&dst[kXD], (unsigned long long)src[kXD]);
     }
   }
+}
+
+// Times of impact of the CCD candidates, one thread per candidate (ccd.py:20-40, 133-186);
+// the minimum below 1 goes to the mailbox key
+__global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= min(a.dstat[DS_NCCD], a.cap_ccd) || (a.dstat[DS_STATUS] & ST_CCD_OVERFLOW)) return;
+  const int4 c = a.ccd_cand[k];
+  int ids[4];
+  cand_vertices(a, c.x, c.y, c.z, ids);
+  d3 x0[4], x1[4];
+  fetch(a.y0, ids, x0);
+  fetch(a.y1, ids, x1);
+  const double t = collision_time(c.x, x0, x1);
+  if (t < 1.0) toi_min(a.toi_key, t);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -910,37 +1001,44 @@ __global__ void k_finish(int n, double dt, abd_states st) {
   }
 }
 
-// Exact dot product on a fixed grid of kRedBlocks CTAs; the last CTA to finish sums the
-// partials and writes the rounded result to *out.
-__global__ void __launch_bounds__(256) k_dot(int N, const double* a, const double* b, XSum* part, int* count,
-                                             double* out) {
+// Exact dot products a.b and c.d (c may be null) on a fixed grid of kRedDot CTAs; the last CTA
+// to finish sums the partials and writes the rounded results to out[0], out[1].
+constexpr int kRedDot = 64;
+__global__ void __launch_bounds__(256) k_dots(int N, const double* a, const double* b, const double* c,
+                                              const double* d, XSum* part, int* count, double* out) {
   __shared__ XSum sh[8];
   __shared__ bool last;
-  XSum acc;
-  xs_zero(acc);
-  for (int i = blockIdx.x * 256 + threadIdx.x; i < N; i += kRedBlocks * 256) xs_add(acc, a[i] * b[i]);
-  xs_block_sum(acc, sh);
+  XSum x0, x1;
+  xs_zero(x0);
+  xs_zero(x1);
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < N; i += kRedDot * 256) {
+    xs_add(x0, a[i] * b[i]);
+    if (c) xs_add(x1, c[i] * d[i]);
+  }
+  xs_block_sum(x0, sh);
+  xs_block_sum(x1, sh);
   if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc;
+    part[blockIdx.x] = x0;
+    part[kRedDot + blockIdx.x] = x1;
     __threadfence();
-    last = atomicAdd(count, 1) == kRedBlocks - 1;
+    last = atomicAdd(count, 1) == kRedDot - 1;
   }
   __syncthreads();
-  if (!last || threadIdx.x >= 32) return;
+  if (!last) return;
   __threadfence();
-  XSum t;
-  xs_zero(t);
-  for (int i = threadIdx.x; i < kRedBlocks; i += 32) {
-    const long long* q = reinterpret_cast<const long long*>(part + i);
+  for (int k = 0; k < (c ? 2 : 1); ++k) {
+    XSum t;
+    xs_zero(t);
+    for (int i = threadIdx.x; i < kRedDot; i += 256) {
+      const long long* q = reinterpret_cast<const long long*>(part + k * kRedDot + i);
 #pragma unroll
-    for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
-    t.flags |= __ldcg(q + kXD);
+      for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
+      t.flags |= __ldcg(q + kXD);
+    }
+    xs_block_sum(t, sh);
+    if (threadIdx.x == 0) out[k] = xs_round(t);
   }
-  xs_warp_sum(t);
-  if (threadIdx.x == 0) {
-    *out = xs_round(t);
-    *count = 0;
-  }
+  if (threadIdx.x == 0) *count = 0;
 }
 
 NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
@@ -961,11 +1059,19 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.row_cnt = s.row_cnt;
   a.pair_mask = s.pair_mask;
   a.pair_wpre = s.pair_wpre;
+  a.nbr = s.nbr;
+  a.fdof = s.fdof;
+  a.chunk_box = s.chunk_box;
+  a.vperm = s.vperm;
   a.W = s.W;
   a.body_box = s.body_box;
   a.chunk = s.chunk;
   a.energy = s.energy_acc;
+  a.prof = s.prof_on == 2;
+  a.prof_rows = &s.box->prof[0][0];
   a.adj_pair = s.adj_pair;
+  a.cap_ccd = s.cap_ccd;
+  a.ccd_cand = s.ccd_cand;
   a.cap_contacts = s.cap_contacts;
   a.contacts = s.contacts;
   a.contacts_by_pair = s.contacts_by_pair;
@@ -1039,9 +1145,17 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       return cudaErrorInvalidValue;
     if (s.nch == 0) return cudaSuccess;
     if (mode == NARROW_ENERGY) {
+      if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[0], s.stream, cudaEventRecordExternal))
+        return cudaErrorUnknown;
       k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
+      if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[1], s.stream, cudaEventRecordExternal))
+        return cudaErrorUnknown;
     } else if (mode == NARROW_CCD) {
+      cudaError_t e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, sizeof(int), s.stream);
+      if (e != cudaSuccess) return e;
       k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+      k_ccd_eval<<<blocks(s.cap_ccd, 128), 128, 0, s.stream>>>(a);
+      ++s.launches;
     } else {
       cudaError_t e = cudaMemsetAsync(s.pair_cand, 0, sizeof(int) * 4 * (size_t)s.cap_pairs, s.stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCONTACT, 0, sizeof(int), s.stream);
@@ -1106,9 +1220,10 @@ cudaError_t finish_step(Sim& s, const abd_states& st, double* xview) {
   return transform(s, st.A0, st.p0, xview);
 }
 
-cudaError_t dot(Sim& s, const double* a, const double* b, int slot, double* out_dev) {
-  k_dot<<<kRedBlocks, 256, 0, s.stream>>>(12 * s.n, a, b, s.partials + (size_t)slot * kRedBlocks, s.red_count + slot,
-                                          out_dev);
+cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev) {
+  static_assert(2 * kRedDot <= 2 * kRedBlocks, "dot partials fit two reduction slots");
+  k_dots<<<kRedDot, 256, 0, s.stream>>>(12 * s.n, a, b, c, d, s.partials + 10 * (size_t)kRedBlocks,
+                                        s.red_count + 10, out_dev);
   ++s.launches;
   return cudaGetLastError();
 }

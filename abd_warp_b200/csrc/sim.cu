@@ -124,6 +124,15 @@ int grow_contacts(Sim& s, int need) {
   return ABD_OK;
 }
 
+int grow_ccd(Sim& s, int need) {
+  if (need <= s.cap_ccd) return ABD_OK;
+  if (s.ccd_cand) cudaFree(s.ccd_cand);
+  s.ccd_cand = nullptr;
+  s.cap_ccd = std::max(need + need / 2, 2 * s.cap_ccd);
+  if (dalloc(&s.ccd_cand, s.cap_ccd)) return ABD_ERR_OVERFLOW;
+  return ABD_OK;
+}
+
 int grow_act(Sim& s, int need) {
   if (need <= s.cap_act) return ABD_OK;
   if (s.act_pairs) cudaFree(s.act_pairs);
@@ -207,7 +216,7 @@ constexpr int kRerun = -1;
 int overflow(Sim& s) {
   const int bits = s.hstat[abd::DS_STATUS];
   const int mask = abd::ST_PAIR_OVERFLOW | abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW | abd::ST_VG_OVERFLOW |
-                   abd::ST_ACT_OVERFLOW | abd::ST_CONTACT_OVERFLOW;
+                   abd::ST_ACT_OVERFLOW | abd::ST_CONTACT_OVERFLOW | abd::ST_CCD_OVERFLOW;
   if (!(bits & mask)) return 0;
   int r = ABD_OK;
   if (bits & abd::ST_PAIR_OVERFLOW) r = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
@@ -221,6 +230,7 @@ int overflow(Sim& s) {
   }
   if (!r && (bits & abd::ST_ACT_OVERFLOW)) r = grow_act(s, s.hstat[abd::DS_NACTP]);
   if (!r && (bits & abd::ST_CONTACT_OVERFLOW)) r = grow_contacts(s, s.hstat[abd::DS_NCONTACT]);
+  if (!r && (bits & abd::ST_CCD_OVERFLOW)) r = grow_ccd(s, s.hstat[abd::DS_NCCD]);
   if (r) return r;
   const int clear = bits & ~mask;
   s.hstat[abd::DS_STATUS] = clear;
@@ -252,11 +262,27 @@ int energy_of(abd_sim* h, const abd_states& st, const abd::Dofs& d, double* E, a
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
-  int r = g ? abd::run_graph(s, *g, key, issue) : issue();
+  // kernel profiling: events around the narrow kernel on every kProfEvery-th trial (mode 1,
+  // their nodes cost a few microseconds) or every pass (mode 2, which also counts bytes)
+  constexpr int kProfEvery = 8;
+  s.prof_events = s.prof_on == 2 || (s.prof_on == 1 && (!g || s.prof_tick++ % kProfEvery == 0));
+  if (g && s.prof_events) g = &s.g_energy_ev;
+  abd::KeyHash k;
+  k.add(key).add(s.prof_on).add(s.prof_events);
+  int r = g ? abd::run_graph(s, *g, k.h, issue) : issue();
   if (r) return r;
   CK(cudaStreamSynchronize(s.stream));
   std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
   *E = xs_round_host(s.hbox->energy);
+  if (s.prof_events) {  // the narrow kernel's duration and the data it read
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s.prof_ev[0], s.prof_ev[1]));
+    s.prof_ms += ms;
+    ++s.prof_launches;
+    if (s.prof_on == 2)
+      for (int row = 0; row < 32; ++row)
+        for (int c = 0; c < abd::PF_N; ++c) s.prof_bytes += abd::kProfBytes[c] * (double)s.hbox->prof[row][c];
+  }
   return ABD_OK;
 }
 
@@ -285,10 +311,17 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
-  int r = g ? abd::run_graph(s, *g, key, issue) : issue();
-  if (r) return r;
-  CK(cudaStreamSynchronize(s.stream));
-  std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
+  for (int tries = 0;; ++tries) {  // the candidate list has a capacity: grow and rerun
+    abd::KeyHash k;
+    k.add(key).add(s.cap_ccd).add(s.ccd_cand);
+    int r = g ? abd::run_graph(s, *g, k.h, issue) : issue();
+    if (r) return r;
+    CK(cudaStreamSynchronize(s.stream));
+    std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
+    if ((r = overflow(s)) > 0) return r;
+    if (r == 0) break;
+    if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
+  }
   double toi = 1.0;
   if (const unsigned long long key2 = s.hbox->toi_key) {
     const unsigned long long bits = ~key2;
@@ -464,16 +497,77 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.pair_mask, (size_t)n * s.W));
   ok(dalloc(&s.pair_wpre, (size_t)n * s.W));
   {
-    // energy / CCD work chunks: kChunk items (points, then edges) of one body each
-    std::vector<int2> ch;
+    // Work chunks of the narrow passes: kChunk items of one body each, the body's points in
+    // Morton order of their rest positions, then its edges in the edge tree's leaf order
+    // (also Morton order), so that a chunk covers a compact patch of the surface.  Each
+    // chunk's rest-frame box bounds its items; a chunk whose box, moved by the body's DOFs,
+    // overlaps no neighbouring body skips its queries.
+    std::vector<int> eleaf(E > 0 ? E : 1);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // the trees are built
+    if (e == cudaSuccess && E > 0)
+      e = cudaMemcpy(eleaf.data(), s.edge_tree.leaf_prim, sizeof(int) * E, cudaMemcpyDeviceToHost);
+    std::vector<int> vperm(V);
     for (int b = 0; b < n; ++b) {
-      const int items = (d->vert_off[b + 1] - d->vert_off[b]) + (d->edge_off[b + 1] - d->edge_off[b]);
+      const int v0 = d->vert_off[b], v1 = d->vert_off[b + 1];
+      double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (int v = v0; v < v1; ++v)
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = std::min(lo[k], d->x0[3 * v + k]);
+          hi[k] = std::max(hi[k], d->x0[3 * v + k]);
+        }
+      std::vector<std::pair<unsigned, int>> key;
+      for (int v = v0; v < v1; ++v) {
+        unsigned c[3];
+        for (int k = 0; k < 3; ++k) {
+          const double ext = hi[k] - lo[k];
+          const double u = ext > 0 ? (d->x0[3 * v + k] - lo[k]) / ext : 0.0;
+          c[k] = (unsigned)std::min(1023.0, std::max(0.0, u * 1024.0));
+        }
+        unsigned m = 0;
+        for (int bit = 9; bit >= 0; --bit)
+          for (int k = 0; k < 3; ++k) m = (m << 1) | ((c[k] >> bit) & 1u);
+        key.push_back({m, v});
+      }
+      std::sort(key.begin(), key.end());
+      for (int i = 0; i < v1 - v0; ++i) vperm[v0 + i] = key[i].second;
+    }
+    std::vector<int2> ch;
+    std::vector<abd::Box> cbox;
+    for (int b = 0; b < n; ++b) {
+      const int nv = d->vert_off[b + 1] - d->vert_off[b], ne = d->edge_off[b + 1] - d->edge_off[b];
+      const int items = nv + ne;
       // every body has at least one chunk: its first chunk also adds the body's own terms
-      for (int i = 0; i < std::max(items, 1); i += abd::kChunk) ch.push_back(make_int2(b, i));
+      for (int i0 = 0; i0 < std::max(items, 1); i0 += abd::kChunk) {
+        ch.push_back(make_int2(b, i0));
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        auto add = [&](int v) {
+          for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], d->x0[3 * v + k]);
+            hi[k] = std::max(hi[k], d->x0[3 * v + k]);
+          }
+        };
+        for (int i = i0; i < std::min(items, i0 + abd::kChunk); ++i) {
+          if (i < nv) {
+            add(vperm[d->vert_off[b] + i]);
+          } else {
+            const int eg = eleaf[d->edge_off[b] + (i - nv)];
+            add(d->edges[2 * eg]);
+            add(d->edges[2 * eg + 1]);
+          }
+        }
+        abd::Box B{};
+        for (int k = 0; k < 3; ++k) {  // rounded outward to FP32
+          B.lo[k] = items ? std::nextafter((float)lo[k], -INFINITY) : 0.f;
+          B.hi[k] = items ? std::nextafter((float)hi[k], INFINITY) : 0.f;
+        }
+        cbox.push_back(B);
+      }
     }
     s.nch = (int)ch.size();
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // ch is a host temporary
+    ok(upload(&s.chunk_box, cbox.data(), cbox.size(), s.stream));
+    ok(upload(&s.vperm, vperm.data(), vperm.size(), s.stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // host temporaries
   }
   ok(dalloc(&s.row_ptr, n + 1));
   ok(dalloc(&s.upper_ptr, n + 1));
@@ -498,6 +592,8 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.dint, 4));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   ok(dalloc(&s.row_cnt, n));
+  ok(dalloc(&s.nbr, (size_t)n * abd::kNbList));
+  ok(dalloc(&s.fdof, 24 * (size_t)n));
   ok(dalloc(&s.upper_cnt, n));
   ok(dalloc(&s.kcount, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
@@ -527,9 +623,10 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     return ABD_ERR_CUDA;
   }
   s.cap_pairs = 0;
-  int r = grow_pairs(s, std::max(256, 4 * n));
+  int r = grow_pairs(s, std::max(256, 8 * n));
   if (!r) r = grow_act(s, std::max(1024, n));
-  if (!r) r = grow_contacts(s, std::max(4096, 4 * n));
+  if (!r) r = grow_contacts(s, std::max(4096, 8 * n));
+  if (!r) r = grow_ccd(s, std::max(1 << 15, 32 * n));
   s.cap_pt = 0;
   s.cap_ee = 0;
   if (!r) r = grow_lists(s, std::max(1 << 14, V / 4), std::max(1 << 14, E / 4));
@@ -554,14 +651,16 @@ int abd_sim_destroy(abd_sim* h) {
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
                   s.pair_active, s.pair_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.dint,
-                  s.row_cnt, s.upper_cnt, s.kcount,
+                  s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
-                  s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair};
+                  s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (abd::GraphSlot* g : {&s.g_energy, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_kblock})
+  for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_kblock})
     if (g->exec) cudaGraphExecDestroy(g->exec);
   if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
+  for (cudaEvent_t ev : s.prof_ev)
+    if (ev) cudaEventDestroy(ev);
   for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar,
                   (void*)s.hint})
     if (q) cudaFreeHost(q);
@@ -610,6 +709,28 @@ int abd_sim_sizes(const abd_sim* h, int* n, int* V, int* T, int* E) {
 }
 
 long long abd_launch_count(const abd_sim* h) { return h ? h->s.launches : 0; }
+
+int abd_profile(abd_sim* h, int enable) {
+  if (!h) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  if (enable && !s.prof_ev[0]) {
+    CK(cudaEventCreate(&s.prof_ev[0]));
+    CK(cudaEventCreate(&s.prof_ev[1]));
+  }
+  s.prof_on = enable == 2 ? 2 : (enable ? 1 : 0);
+  s.prof_tick = 0;
+  s.prof_ms = s.prof_bytes = 0.0;
+  s.prof_launches = 0;
+  return ABD_OK;
+}
+
+int abd_profile_read(const abd_sim* h, double* ms, long long* launches, double* bytes) {
+  if (!h) return ABD_ERR_INVALID;
+  if (ms) *ms = h->s.prof_ms;
+  if (launches) *launches = h->s.prof_launches;
+  if (bytes) *bytes = h->s.prof_bytes;
+  return ABD_OK;
+}
 
 int abd_take_status(abd_sim* h, int* status) {
   if (!h || !status) return ABD_ERR_INVALID;
@@ -745,8 +866,7 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     // one pass; Ak, pk = q - dq
     double alpha;
     auto dots = [&]() -> int {
-      CK(abd::dot(s, s.dq, s.g, 10, &s.box->dots[0]));
-      CK(abd::dot(s, s.g, s.g, 11, &s.box->dots[1]));
+      CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots));
       return ABD_OK;
     };
     if ((r = ccd_of(h, direct(st.A, st.p), updated(s, st.A, st.p, 1, st.Ak, st.pk), &alpha, &inf.toi, dots,

@@ -95,17 +95,15 @@ __device__ inline void cta_partials(const SolverArgs& a, XSum& x0, XSum& x1, int
     if (slot < 0) continue;
     XSum t;
     xs_zero(t);
-    if (threadIdx.x < 32) {
-      const XSum* P = a.part + slot * kRedBlocks;
-      for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
-        const long long* q = reinterpret_cast<const long long*>(P + i);
+    const XSum* P = a.part + slot * kRedBlocks;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      const long long* q = reinterpret_cast<const long long*>(P + i);
 #pragma unroll
-        for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
-        t.flags |= __ldcg(q + kXD);
-      }
-      xs_warp_sum(t);
-      if (threadIdx.x == 0) a.scal[SC_RED + slot] = xs_round(t);
+      for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
+      t.flags |= __ldcg(q + kXD);
     }
+    xs_block_sum(t, sh);
+    if (threadIdx.x == 0) a.scal[SC_RED + slot] = xs_round(t);
   }
   if (threadIdx.x == 0) a.red_count[cslot] = 0;
 }
@@ -209,31 +207,34 @@ __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, in
   }
 }
 
-// out = M^-1 in (cluster by cluster); partial in.out into slot (if >= 0); also copies out
-// into copy (if not null)
+// out = M^-1 in, one warp per cluster: lane i computes rows i, i + 32, ... of the cluster's
+// dense inverse times the gathered input, summing over the columns in order; partial in.out
+// into slot (if >= 0); also copies out into copy (if not null)
 __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out,
                                               double* copy, int slot) {
   if (it_guard && (solver_done(a.dstat) || iteration(a) > a.maxit)) return;
-  __shared__ double vs[12 * kMaxCluster];
+  constexpr int NWA = AT / 32;
+  __shared__ double vs[NWA][12 * kMaxCluster];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   XSum d0, d1;
   xs_zero(d0);
   xs_zero(d1);
   const int ncl = *a.ncl_dev;
-  for (int c = blockIdx.x; c < ncl; c += gridDim.x) {
-    const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
-    for (int i = threadIdx.x; i < D; i += AT) vs[i] = in[(size_t)a.cl_body[base + i / 12] * 12 + i % 12];
-    __syncthreads();
+  for (int c = blockIdx.x * NWA + warp; c < ncl; c += gridDim.x * NWA) {
+    const int base = a.cl_ptr[c], sz = a.cl_ptr[c + 1] - base, D = 12 * sz;
+    for (int i = lane; i < D; i += 32) vs[warp][i] = in[(size_t)a.cl_body[base + i / 12] * 12 + i % 12];
+    __syncwarp();
     const double* Kc = a.cl_inv + a.cl_off[c];
-    for (int i = threadIdx.x; i < D; i += AT) {
+    for (int i = lane; i < D; i += 32) {
       double acc = 0.0;
       const double* row = Kc + (size_t)i * D;
-      for (int j = 0; j < D; ++j) acc += row[j] * vs[j];
+      for (int j = 0; j < D; ++j) acc += row[j] * vs[warp][j];
       const size_t gi = (size_t)a.cl_body[base + i / 12] * 12 + i % 12;
       out[gi] = acc;
       if (copy) copy[gi] = acc;
-      if (slot >= 0) xs_add(d0, vs[i] * acc);
+      if (slot >= 0) xs_add(d0, vs[warp][i] * acc);
     }
-    __syncthreads();
+    __syncwarp();
   }
   if (slot >= 0) cta_partials(a, d0, d1, slot, -1);
 }

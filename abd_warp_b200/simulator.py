@@ -280,5 +280,17 @@ class AffineBodySimulator:
         _lib.check(self._L.abd_sim_get_g(self._h, _ptr(out)), "abd_sim_get_g")
         return out
 
+    def profile(self, mode: int = 1):
+        """Start (reset) or stop (0) the timing of the energy pass's narrow-phase kernel; mode 2
+        also counts the data it reads (algorithmic bytes), which slows the kernel down."""
+        _lib.check(self._L.abd_profile(self._h, int(mode)), "abd_profile")
+
+    def profile_read(self):
+        """(kernel ms, launches, algorithmic bytes) accumulated since profile()."""
+        ms, n, b = ctypes.c_double(0), ctypes.c_longlong(0), ctypes.c_double(0)
+        _lib.check(self._L.abd_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)),
+                   "abd_profile_read")
+        return ms.value, n.value, b.value
+
     def launch_count(self) -> int:
         return int(self._L.abd_launch_count(self._h))

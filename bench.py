@@ -1,39 +1,62 @@
 """Benchmark of the ABD implicit contact time step on B200.
 
-Workload: the 1024-body pile (512 cubes + 512 level-3 icospheres on a fixed ground box,
-V = 332,808, T = 661,516, E = 992,274), seeded synthetic scene.  A step is one implicit time
-step (Newton with CCD-bounded line search).  W warm-up steps run first (they also advance
-the pile into contact), then K steps are timed with CUDA events; L2 is flushed between
-timed steps by writing a 256 MiB buffer.
+Workload: the 1024-body pile (512 cubes + 512 level-3 icospheres dropped on a fixed ground
+box; V = 332,808, T = 661,516, E = 992,274), a seeded synthetic scene.  A step is one
+implicit time step (Newton with CCD-bounded backtracking line search).  W untimed warm-up
+steps run first; the scene is then reset to its initial state and K steps of its trajectory
+are timed (K = 300, the whole trajectory, by default: the cost of a step grows as the pile
+settles into contact).  Each step is timed with CUDA events on the simulator's stream, and
+L2 is flushed before every step by writing a 256 MiB buffer.
+
+value: steps/s on device-resident states.  e2e: the same trajectory again through the public
+API with host buffers -- every step copies its inputs (A0, p0, Adot, pdot) from pinned host
+memory and reads the new vertex positions back.
+
+roofline: the energy pass's narrow-phase kernel, the largest share of the step, timed with
+CUDA events around every 8th of its launches inside the timed region; the data it reads
+(algorithmic bytes) is counted by the kernel in a replay of the same (deterministic)
+trajectory, which makes the same launches.
 
 Multi-GPU: the step does not shard (one coupled Newton solve per scene), so N ranks run N
 independent replicas; value = N * K / max-over-ranks time.
 
 --impl reference times the CPU FP64 oracle (the restatement of the reference's step; the
-reference itself needs Warp and abdtk, absent here) on the host cores for the same scene.
+reference itself needs Warp and abdtk, absent here) on all host cores: steps from oracle
+states at steps 0, 75, 150 and 225 of the same trajectory (tests/golden/c2_states.npz),
+weighted equally.  The GPU arm's cpu_baseline is the same measurement on a smaller budget.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import subprocess
 import sys
-import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "ABD steps/s vs plain FP64 on same B200 at ≤1e-6 rel pos err; adjoint grads/s"
-WORKLOAD = "pile_1024_bodies_512cubes_512icosphereL3_ground (config 2)"
+METRIC = "ABD steps/s vs plain FP64 on same B200 at \u22641e-6 rel pos err; adjoint grads/s"
+WORKLOAD = "pile of 1024 bodies (512 cubes + 512 level-3 icospheres) on a ground box, 300-step trajectory"
+STATES = os.path.join(ROOT, "tests", "golden", "c2_states.npz")
+# DRAM bytes per launch of the energy narrow kernel (dram__bytes_read.sum + write.sum) from
+# the ncu capture summarised in profiles/k_chunk_narrow_energy_pile1024.md
+NCU_TRAFFIC_PER_LAUNCH = None
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
@@ -55,101 +78,113 @@ def make_scene():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed region."""
+    """SM clocks, power and throttle reasons of the GPU sampled every 100 ms during the timed
+    region, in-process through NVML (the data nvidia-smi reports; a polling nvidia-smi
+    process would compete with the step's host synchronisations)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = {"hw_slowdown": "nvmlClocksThrottleReasonHwSlowdown",
+             "hw_thermal_slowdown": "nvmlClocksThrottleReasonHwThermalSlowdown",
+             "sw_thermal_slowdown": "nvmlClocksThrottleReasonSwThermalSlowdown",
+             "sw_power_cap": "nvmlClocksThrottleReasonSwPowerCap"}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.thread = None
+        self.stop_flag = False
+        self.err = None
+
+    def _handle(self, nv):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device.index or 0)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+        except Exception as exc:  # no NVML: reported in the line
+            self.err = f"nvml unavailable: {exc}"
+            return
+        masks = {k: getattr(nv, v, 0) for k, v in self.NAMES.items()}
+
+        def run():
+            while not self.stop_flag:
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                    self.rows.append((sm, mx, pw, [k for k, m in masks.items() if rs & m]))
+                except Exception as exc:
+                    self.err = str(exc)
+                time.sleep(0.1)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "not sampled"]}
+        self.stop_flag = True
+        self.thread.join()
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
-        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+        sm = sorted(r[0] for r in self.rows)
+        return {"sm_mhz": float(sm[len(sm) // 2]), "sm_max_mhz": float(max(r[1] for r in self.rows)),
+                "reasons": sorted({x for r in self.rows for x in r[3]}), "samples": len(self.rows),
+                "power_w_max": max(r[2] for r in self.rows), "source": "NVML, every 100 ms"}
 
 
-def cpu_baseline_sample(bodies, prm, state, budget):
-    """Time the CPU FP64 oracle on the same scene from the given state, for about `budget`
-    seconds of work (at least one step).  Returns (steps_per_s, steps, threads)."""
+def oracle_sample(budget, max_steps=None):
+    """Oracle steps/s over the trajectory: from each stored state, steps for budget / 4
+    seconds (at least one), the mean time per step weighted equally over the states.
+    Returns (steps_per_s, steps, threads, description)."""
+    import numpy as np
+
     import oracle
     from abd_warp_b200 import scenes
+    bodies, prm = make_scene()
     o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
-    o.set_state(state["A0"], state["p0"], state["Adot"], state["pdot"], state["dq"])
     threads = oracle.max_threads()
-    t0 = time.perf_counter()
-    n = 0
-    while True:
-        o.step()
-        n += 1
-        if time.perf_counter() - t0 >= budget:
-            break
-    dt = time.perf_counter() - t0
-    return n / dt, n, threads
+    z = np.load(STATES)
+    per_state, total = [], 0
+    for s in z["steps"]:
+        o.set_state(*(z[f"s{s}_{k}"] for k in ("A0", "p0", "Adot", "pdot", "dq")))
+        t0 = time.perf_counter()
+        n = 0
+        while True:
+            o.step()
+            n += 1
+            if time.perf_counter() - t0 >= budget / len(z["steps"]) or (max_steps and n >= max_steps):
+                break
+        per_state.append((time.perf_counter() - t0) / n)
+        total += n
+    mean = sum(per_state) / len(per_state)
+    desc = (f"{total} oracle steps from the states at steps {', '.join(str(int(s)) for s in z['steps'])} of the "
+            f"trajectory, mean time per step weighted equally over the states")
+    return 1.0 / mean, total, threads, desc
 
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import oracle
-    from abd_warp_b200 import scenes
-    bodies, prm = make_scene()
-    o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
-    threads = oracle.max_threads()
-    budget = 150.0
-    t_start = time.perf_counter()
-    for _ in range(args.warmup):
-        o.step()
-        if time.perf_counter() - t_start > budget / 2:
-            break
-    t0 = time.perf_counter()
-    n = 0
-    for _ in range(args.steps):
-        o.step()
-        n += 1
-        if time.perf_counter() - t0 > budget / 2:
-            break
-    el = time.perf_counter() - t0
-    v = n / el
+    bodies, _ = make_scene()
+    # a bounded sample: about 2 minutes of host work
+    v, n, threads, desc = oracle_sample(budget=120.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
-        "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {"workload": WORKLOAD, "bodies": len(bodies), "precision": "fp64"},
-        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} oracle steps after {args.warmup} warm-up steps (time-capped)"},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -177,21 +212,25 @@ def main():
     if args.precision == "mixed":
         prm.precision = PRECISION_MIXED
     sim = AffineBodySimulator(bodies=bodies, params=prm, device=f"cuda:{local}")
+    s = sim.states
     stream = torch.cuda.current_stream(dev)
+    names = ("A0", "p0", "Adot", "pdot")
+
+    def reset():  # back to the scene's initial state (dq warm start 0)
+        sim.reset()
+        torch.cuda.synchronize(dev)
+
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     for _ in range(max(args.warmup, 3)):
         sim.step()
-    torch.cuda.synchronize(dev)
-    # state at the start of the timed region (for the CPU baseline sample)
-    s = sim.states
-    start_state = {"A0": s.A0.cpu().numpy(), "p0": s.p0.cpu().numpy(), "Adot": s.Adot.cpu().numpy(),
-                   "pdot": s.pdot.cpu().numpy(), "dq": sim.dq.cpu().numpy()}
-    # ---- device-resident timing ----
-    clocks = ClockSampler(local)
+    reset()
+    # ---- device-resident timing of K steps of the trajectory ----
+    clocks = ClockSampler(dev)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
+    sim.profile(1)  # CUDA events around every 8th launch of the energy narrow kernel
     launches0 = sim.launch_count()
     total_ms = 0.0
     infos = []
@@ -207,6 +246,8 @@ def main():
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
     launches = sim.launch_count() - launches0
+    k_ms, k_launches, _ = sim.profile_read()
+    sim.profile(0)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.barrier()
@@ -214,7 +255,8 @@ def main():
     max_ms = float(t.item())
     value = world * args.steps / (max_ms / 1e3)
     # ---- end to end through the public API with host buffers ----
-    pin = {k: getattr(s, k).cpu().pin_memory() for k in ("A0", "p0", "Adot", "pdot")}
+    reset()
+    pin = {k: getattr(s, k).cpu().pin_memory() for k in names}
     xv_host = torch.empty(sim.x_view.shape, dtype=torch.float64).pin_memory()
     h2d = sum(v.numel() * 8 for v in pin.values())
     d2h = xv_host.numel() * 8
@@ -229,38 +271,54 @@ def main():
         e0.record(stream)
         for k, v in pin.items():
             getattr(s, k).copy_(v, non_blocking=True)
-        info = sim.step()
+        sim.step()
         xv_host.copy_(sim.x_view, non_blocking=True)
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-        for k in pin:
+        for k in pin:  # the caller keeps the new state on the host for its next step
             pin[k].copy_(getattr(s, k))
     te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps / (float(te.item()) / 1e3)
-    newton = [i["newton_iters"] for i in infos]
-    lin = [i["linear_iters"] for i in infos]
+    # the algorithmic bytes of the same launches: the trajectory is deterministic, so a replay
+    # with the kernel counting what it reads has the same launches (not timed: counting slows it)
+    reset()
+    sim.profile(2)
+    for _ in range(args.steps):
+        sim.step()
+    _, c_launches, c_bytes = sim.profile_read()
+    sim.profile(0)
+    peak, peak_kind = measured_hbm_peak()
+    bytes_per_launch = c_bytes / max(c_launches, 1)
+    us_per_launch = 1e3 * k_ms / max(k_launches, 1)
+    achieved = bytes_per_launch / (us_per_launch * 1e-6) / 1e9 if k_ms > 0 else None
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {"workload": WORKLOAD, "bodies": len(bodies), "verts": int(sim.n_verts),
+                   "timed_steps": f"steps 1..{args.steps} of the trajectory from the initial state",
                    "precision": args.precision, "parallelism": f"replicas{world}",
-                   "l2": "flushed between timed steps (256 MiB write)",
-                   "newton_iters_per_step": float(np.mean(newton)),
-                   "linear_iters_per_step": float(np.mean(lin)),
+                   "l2": "flushed before every timed step (256 MiB write)",
+                   "newton_iters_per_step": float(np.mean([i["newton_iters"] for i in infos])),
+                   "linear_iters_per_step": float(np.mean([i["linear_iters"] for i in infos])),
                    "ls_trials_per_step": float(np.mean([i["ls_trials"] for i in infos])),
-                   "active_contacts_last": infos[-1]["n_active"]},
+                   "active_contacts_max": int(max(i["n_active"] for i in infos))},
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "roofline": {"kernel": "k_chunk_narrow<ENERGY> (energy pass narrow phase)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                     "peak_kind": peak_kind, "timed_launches": k_launches, "counted_launches": c_launches,
+                     "avg_launch_us": us_per_launch, "bytes_per_launch": bytes_per_launch},
     }
     if rank == 0 and not args.no_cpu_baseline:
-        v, n, threads = cpu_baseline_sample(bodies, prm, start_state, args.cpu_budget)
-        line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
-                                "sample": f"{n} CPU-oracle steps from the state at the start of the timed region"}
+        v, n, threads, desc = oracle_sample(args.cpu_budget)
+        line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()
