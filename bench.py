@@ -40,8 +40,9 @@ METRIC = "ABD steps/s vs plain FP64 on same B200 at \u22641e-6 rel pos err; adjo
 WORKLOAD = "pile of 1024 bodies (512 cubes + 512 level-3 icospheres) on a ground box, 300-step trajectory"
 STATES = os.path.join(ROOT, "tests", "golden", "c2_states.npz")
 # DRAM bytes per launch of the energy narrow kernel (dram__bytes_read.sum + write.sum) from
-# the ncu capture summarised in profiles/k_chunk_narrow_energy_pile1024.md
-NCU_TRAFFIC_PER_LAUNCH = None
+# the ncu capture at trajectory step 225 summarised in
+# profiles/k_chunk_narrow_energy_pile1024_state225.md (the contact-rich end of the trajectory)
+NCU_TRAFFIC_PER_LAUNCH = 5.73e6
 
 
 def measured_hbm_peak():
@@ -61,6 +62,9 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--start-state", type=int, default=None,
+                    help="start from the stored oracle state at this step of the trajectory (0, 75, 150 or 225; "
+                         "for profiling a contact-rich stretch) instead of the initial state")
     return ap.parse_args()
 
 
@@ -216,11 +220,23 @@ def main():
     stream = torch.cuda.current_stream(dev)
     names = ("A0", "p0", "Adot", "pdot")
 
-    def reset():  # back to the scene's initial state (dq warm start 0)
+    start = None
+    if args.start_state is not None:
+        z = np.load(STATES)
+        start = {k: torch.as_tensor(z[f"s{args.start_state}_{k}"], device=dev) for k in (*names, "dq")}
+
+    def reset():  # back to the start state (the scene's initial state, dq warm start 0)
         sim.reset()
+        if start is not None:
+            for k in names:
+                getattr(s, k).copy_(start[k])
+            s.A.copy_(s.A0)
+            s.p.copy_(s.p0)
+            sim.dq = start["dq"]
         torch.cuda.synchronize(dev)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    reset()
     for _ in range(max(args.warmup, 3)):
         sim.step()
     reset()
@@ -299,7 +315,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {"workload": WORKLOAD, "bodies": len(bodies), "verts": int(sim.n_verts),
-                   "timed_steps": f"steps 1..{args.steps} of the trajectory from the initial state",
+                   "timed_steps": (f"steps 1..{args.steps} of the trajectory from the initial state"
+                                   if start is None else
+                                   f"{args.steps} steps from the state at step {args.start_state} of the trajectory"),
                    "precision": args.precision, "parallelism": f"replicas{world}",
                    "l2": "flushed before every timed step (256 MiB write)",
                    "newton_iters_per_step": float(np.mean([i["newton_iters"] for i in infos])),
