@@ -75,6 +75,7 @@ def load():
         "abd_solve": ([P, P, P], c_int),
         "abd_compute_energy": ([P, P, P, P, P], c_int),
         "abd_ccd": ([P, P, P, P, P, P, P], c_int),
+        "abd_energies_along": ([P, P, P, P, P, c_int, P], c_int),
         "abd_take_status": ([P, P], c_int),
         "abd_status_string": ([c_int], ctypes.c_char_p),
         "abd_launch_count": ([P], c_longlong),
@@ -95,7 +96,7 @@ def exported_symbols():
     return ["abd_sim_create", "abd_sim_destroy", "abd_sim_set_params", "abd_sim_set_stream", "abd_sim_reset",
             "abd_sim_get_dq", "abd_sim_set_dq", "abd_sim_get_g", "abd_sim_sizes", "abd_step", "abd_update_mesh_vertex",
             "abd_collision_set", "abd_collision_set_dofs", "abd_export_lists", "abd_ipc_gh", "abd_export_system", "abd_solve",
-            "abd_compute_energy", "abd_ccd", "abd_take_status", "abd_status_string", "abd_launch_count",
+            "abd_compute_energy", "abd_ccd", "abd_energies_along", "abd_take_status", "abd_status_string", "abd_launch_count",
             "abd_profile", "abd_profile_read"]
 
 

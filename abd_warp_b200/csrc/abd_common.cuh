@@ -27,6 +27,7 @@ enum : int {
   ST_ACT_OVERFLOW = 128,   // active-pair list capacity exceeded (host grows and reruns)
   ST_CONTACT_OVERFLOW = 256,  // active-contact list capacity exceeded (host grows and reruns)
   ST_CCD_OVERFLOW = 512,   // CCD candidate list capacity exceeded (host grows and reruns)
+  ST_ECAND_OVERFLOW = 1024,  // line-search candidate list capacity exceeded (grow and rerun)
 };
 
 constexpr int kTraversalStack = 64;
@@ -156,9 +157,10 @@ struct Tree {
   int* prim_leaf = nullptr;   // [N] primitive index -> sorted position
   int* body_root = nullptr;   // [n] node id of the body's subtree, -1 if the body has none
   Box* box = nullptr;         // [2N-1] world boxes: internal nodes (refit), then leaves
-  // [N-1] internal node boxes in the body's rest frame (the refit of the rest positions);
-  // when the positions are x = A^T r + p, a node's world box is bounded by the affine image
-  // of its rest box, which the traversal computes from the body's DOFs instead of a refit
+  // [2N-1] node boxes in the body's rest frame (the refit of the rest positions: internal
+  // nodes, then leaves); when the positions are x = A^T r + p, a node's world box is bounded
+  // by the affine image of its rest box, which the traversal computes from the body's DOFs
+  // instead of a refit
   Box* rest = nullptr;
   // per-body bottom-up refit schedule: the internal nodes of body b's subtree grouped by
   // height, order[lvl[body_lvl[b] + h - 1] .. lvl[body_lvl[b] + h]) for h = 1..heights
@@ -198,6 +200,10 @@ struct Sim {
   // positions
   double *x = nullptr, *xk = nullptr;
   Box* body_box = nullptr;  // [n] FP32 body boxes of the last pass (written by the pair mask)
+  Box* body_rest = nullptr; // [n] rest-frame box of each body's vertices
+  // [n] boxes holding the body's box at every DOF set between the two of a swept pass (the
+  // line-search candidate pass culls its body pairs with them)
+  Box* body_sup = nullptr;
   unsigned long long* body_bnd = nullptr;  // [n][12] exact bounds as max-keys (broad phase)
   int swept = 0;            // the last broad phase was swept
 
@@ -231,12 +237,14 @@ struct Sim {
   float* fdof = nullptr;           // [n][2][12] FP32 DOFs of the last broad phase
   int* upper_cnt = nullptr;        // [n] neighbours J > I
   int* kcount = nullptr;           // [4] last-CTA counters of single-pass kernels
-  double* dpar = nullptr;          // device pass parameters: [0] trial step, [1] = 1
+  // device pass parameters: [0] trial step, [1] = 1, [kParK] trials of a line-search batch,
+  // [kParAlpha + k] their step lengths
+  double* dpar = nullptr;
   int* dint = nullptr;             // device integers: [0] preconditioner clusters
   int* hint = nullptr;             // pinned staging of dint
   // captured passes: energy trial, CCD bound, GH, Krylov setup and one block of iterations
   cudaStream_t cap_stream = nullptr;
-  GraphSlot g_energy, g_energy_ev, g_ccd, g_gh, g_kinit, g_kblock;
+  GraphSlot g_energy, g_energy_ev, g_ccd, g_gh, g_kinit, g_kblock, g_ls;
   unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
   // kernel profiling of the energy pass's narrow kernel: CUDA events around it (recorded as
   // graph nodes), its duration and algorithmic bytes accumulated after every pass
@@ -264,6 +272,12 @@ struct Sim {
   int4 *contacts = nullptr, *contacts_by_pair = nullptr;
   int cap_ccd = 0;
   int4* ccd_cand = nullptr;        // CCD candidates (type, primitive a, primitive b)
+  // line-search candidates of the last CCD pass: every PT / EE pair that can be in the
+  // culled set at some DOFs between its two sets (type, primitive a, primitive b)
+  int cap_ecand = 0;
+  int4* ecand = nullptr;
+  unsigned long long* ls_bnd = nullptr;  // [kLsMax][n][6] body bounds of the trials (max-keys)
+  Box* ls_box = nullptr;                 // [kLsMax][n] body boxes of the trials
   int list_counts[4] = {0, 0, 0, 0};  // pairs, PT, EE, VG of the last list culling
   double* pair_val = nullptr;      // [cap_pairs] energy or toi per pair
 
@@ -296,6 +310,10 @@ constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction 
 constexpr int kChunk = 128;       // items per chunk of the energy / CCD narrow passes
 constexpr int kNbList = 32;       // neighbours per body listed by the pair mask
 constexpr int kRedSlots = 12;
+constexpr int kLsMax = 16;        // line-search trials evaluated per batch
+constexpr int kParK = 4;          // dpar slot of a batch's trial count
+constexpr int kParAlpha = 5;      // dpar slots of its step lengths
+constexpr int kNPar = kParAlpha + kLsMax;
 
 // dstat layout
 enum : int {
@@ -312,6 +330,7 @@ enum : int {
   DS_NCONTACT = 12,  // active contacts appended by the GH pass
   DS_IT = 13,        // Krylov iteration counter (device-side, for replayed blocks)
   DS_NCCD = 14,      // CCD candidates appended by the CCD pass
+  DS_NECAND = 15,    // line-search candidates appended by the CCD pass
   DS_NSLOTS = 16
 };
 
@@ -322,6 +341,7 @@ struct Mailbox {
   XSum energy;
   unsigned long long toi_key;  // complemented bits of the minimum time of impact (0: none)
   double dots[2];              // dq.g, g.g
+  XSum ls_energy[kLsMax];      // exact energies of a line-search batch's trials
   // work counters of the energy pass's narrow kernel (kernel profiling only), spread over
   // 32 rows against atomic contention: [row][PF_*]
   unsigned long long prof[32][8];
@@ -371,12 +391,14 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
                        double* y1);
 // body pairs: full (mask, scan, fill: the sorted pair list and the adjacency with pair
 // indices) or mask only (row counts and the bit matrix, all the energy and CCD passes need)
-cudaError_t body_pairs(Sim& s, bool full);
+// sup: cull with the boxes over every DOF set between the two of a swept pass (body_sup)
+cudaError_t body_pairs(Sim& s, bool full, bool sup = false);
 // rest-frame internal node boxes of both trees (once, at creation)
 cudaError_t rest_boxes(Sim& s);
 
 // narrow.cu
-enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS = 3 };
+// CCD_LS: the CCD pass that also collects the line-search candidates (ecand)
+enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS = 3, NARROW_CCD_LS = 4 };
 // A != null: internal node boxes are the affine images of the rest boxes under (A, p) (united
 // with (A1, p1) when swept); A == null: the refit boxes.  y0 / y1 are the positions.
 // ENERGY (at DOFs A, p; st for the inertia terms) adds the pass's whole energy -- contacts,
@@ -395,6 +417,12 @@ cudaError_t finish_step(Sim& s, const abd_states& st, double* xview);
 // exact dot products a.b (and c.d when c != null) of [n][12] vectors into out_dev[0], [1]
 // (reduction slots 10 and 11)
 cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev);
+
+// linesearch.cu
+// Energies at (A, p) - alpha_k dq for the dpar[kParK] step lengths dpar[kParAlpha + k] in
+// [0, 1], from the candidates of the last CCD_LS pass between (A, p) and (A, p) - dq, into
+// the mailbox's ls_energy[k]
+cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p);
 
 // solver.cu
 int build_preconditioner(Sim& s);                 // returns ABD status

@@ -12,7 +12,7 @@
 // y0 with the undilated float32 boxes at y1.
 #include <cuda_runtime.h>
 
-#include "abd_common.cuh"
+#include "abd_body.cuh"
 
 namespace abd {
 
@@ -29,46 +29,6 @@ __global__ void k_transform(int V, const int* __restrict__ vbody, const double* 
   const double* a = A + 9 * b;
 #pragma unroll
   for (int j = 0; j < 3; ++j) x[3 * v + j] = ((a[j] * r0 + a[3 + j] * r1) + a[6 + j] * r2) + p[3 * b + j];
-}
-
-// ---------------------------------------------------------------------------------------
-// body bounds as order-preserving 64-bit keys, maximised atomically (exact, any order):
-// bnd[12 b + k] = key(-lo0_k), key(hi0_k), key(-lo1_k), key(hi1_k) for k = 0..2 (y0, then
-// y1 when swept); 0 = no vertex
-// ---------------------------------------------------------------------------------------
-__device__ inline unsigned long long max_key(double x) {
-  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
-  return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
-}
-__device__ inline double key_value(unsigned long long k) {
-  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffULL) : ~k;
-  return __longlong_as_double((long long)b);
-}
-
-// The FP32 body box of the reference (culling2.py:278-334): FP64 min / max of the vertices,
-// dilated by dhat / 2 in FP64 and rounded to FP32; swept boxes add the undilated FP32 box
-// of the end positions.
-__device__ inline Box body_box_of(const unsigned long long* k, bool swept, double dhh) {
-  Box B;
-  B.pad0 = B.pad1 = 0.f;
-  if (k[3] == 0) {  // no vertex
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      B.lo[j] = INFINITY;
-      B.hi[j] = -INFINITY;
-    }
-    return B;
-  }
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    B.lo[j] = (float)(-key_value(k[j]) - dhh);
-    B.hi[j] = (float)(key_value(k[3 + j]) + dhh);
-    if (swept) {
-      B.lo[j] = fminf(B.lo[j], (float)(-key_value(k[6 + j])));
-      B.hi[j] = fmaxf(B.hi[j], (float)key_value(k[9 + j]));
-    }
-  }
-  return B;
 }
 
 struct VertexArgs {
@@ -92,13 +52,7 @@ __device__ inline void body_dofs(const Dofs& d, int b, double M[12]) {
     for (int k = 0; k < 3; ++k) M[9 + k] = d.p[3 * b + k];
     return;
   }
-  const double al = *d.alpha;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) M[9 + k] = d.p[3 * b + k] - d.dq[12 * b + k] * al;
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) M[3 * r + k] = d.A[9 * b + 3 * r + k] - d.dq[12 * b + 3 * (r + 1) + k] * al;
+  dofs_at(d.A, d.p, d.dq, b, *d.alpha, M);
 }
 
 // One thread per vertex (and, for t < n, per body): the body's DOFs of each set (written out
@@ -143,7 +97,7 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
       double* y = k ? a.y1 : a.y0;
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const double cj = ((M[j] * r0 + M[3 + j] * r1) + M[6 + j] * r2) + M[9 + j];
+        const double cj = xform(M, r0, r1, r2, j);
         y[3 * v + j] = cj;
         c[3 * k + j] = cj;
       }
@@ -172,8 +126,11 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
   }
 }
 
-// FP32 body boxes from the bounds (one thread per body), which are cleared for the next pass
-__global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double dhh, Box* body_box) {
+// FP32 body boxes from the bounds (one thread per body), which are cleared for the next pass.
+// With body_sup: also the affine images of the body's rest box under both DOF sets, dilated
+// by dhat / 2, which hold the body's box at every DOF set between the two.
+__global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double dhh, Box* body_box,
+                             const Box* body_rest, const float* fdof, Box* body_sup) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   unsigned long long k[12];
@@ -183,6 +140,10 @@ __global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double d
     bnd[12 * (size_t)b + i] = 0ULL;
   }
   store_box(&body_box[b], body_box_of(k, swept, dhh));
+  if (body_sup) {
+    const float* m = fdof + 24 * (size_t)b;
+    store_box(&body_sup[b], affine_box2(load_box(&body_rest[b]), m, swept ? m + 12 : nullptr, __double2float_ru(dhh)));
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -539,12 +500,13 @@ cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, doubl
   return cudaGetLastError();
 }
 
-// Rest-frame boxes of the internal nodes: the refit of the rest positions, copied aside.
+// Rest-frame boxes of all nodes: the leaf boxes and refit of the rest positions, copied aside.
 cudaError_t rest_boxes(Sim& s) {
   cudaError_t e = body_broad(s, nullptr, nullptr, nullptr, nullptr, s.x0, nullptr);
   for (Tree* t : {&s.tri_tree, &s.edge_tree})
-    if (e == cudaSuccess && t->N > 1)
-      e = cudaMemcpyAsync(t->rest, t->box, sizeof(Box) * (size_t)(t->N - 1), cudaMemcpyDeviceToDevice, s.stream);
+    if (e == cudaSuccess && t->N > 0)
+      e = cudaMemcpyAsync(t->rest, t->box, sizeof(Box) * (size_t)(2 * t->N - 1), cudaMemcpyDeviceToDevice,
+                          s.stream);
   // no pair pass follows: clear the bounds here (the pair mask clears them otherwise)
   if (e == cudaSuccess) e = cudaMemsetAsync(s.body_bnd, 0, sizeof(unsigned long long) * 12 * (size_t)s.n, s.stream);
   return e;
@@ -562,11 +524,13 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
 // the pair index of {I, J}).  Counts stay on the device (dstat DS_NPAIRS / DS_NADJ); a short
 // capacity raises ST_PAIR_OVERFLOW and leaves the lists incomplete, for the host to grow and
 // rerun at its next read of dstat.
-cudaError_t body_pairs(Sim& s, bool full) {
+cudaError_t body_pairs(Sim& s, bool full, bool sup) {
   const int n = s.n, W = s.W;
-  k_body_boxes<<<blocks(n, 128), 128, 0, s.stream>>>(n, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box);
-  k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(n, W, s.body_box, s.pair_mask, s.pair_wpre,
-                                                                         s.row_cnt, s.upper_cnt, s.nbr);
+  k_body_boxes<<<blocks(n, 128), 128, 0, s.stream>>>(n, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box,
+                                                     s.body_rest, s.fdof, sup ? s.body_sup : nullptr);
+  k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(n, W, sup ? s.body_sup : s.body_box,
+                                                                         s.pair_mask, s.pair_wpre, s.row_cnt,
+                                                                         s.upper_cnt, s.nbr);
   s.launches += 2;
   if (full) {
     k_pair_scan<<<1, 1024, 0, s.stream>>>(n, s.row_cnt, s.upper_cnt, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj,

@@ -245,7 +245,7 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body, const doub
   TRY(cudaMalloc(&tr.leaf_prim, sizeof(int) * (size_t)(N > 0 ? N : 1)));
   TRY(cudaMalloc(&tr.prim_leaf, sizeof(int) * (size_t)(N > 0 ? N : 1)));
   TRY(cudaMalloc(&tr.body_root, sizeof(int) * (size_t)n));
-  TRY(cudaMalloc(&tr.rest, sizeof(Box) * (size_t)(N > 1 ? N - 1 : 1)));
+  TRY(cudaMalloc(&tr.rest, sizeof(Box) * (size_t)(N > 0 ? 2 * N - 1 : 1)));
   TRY(cudaMalloc(&tr.box, sizeof(Box) * nodes));
   TRY(cudaMemsetAsync(tr.body_root, 0xff, sizeof(int) * n, s.stream));
   TRY(cudaMemsetAsync(tr.parent, 0xff, sizeof(int) * nodes, s.stream));

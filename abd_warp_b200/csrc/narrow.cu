@@ -21,7 +21,7 @@
 
 #include <climits>
 
-#include "abd_common.cuh"
+#include "abd_body.cuh"
 #include "abd_geometry.cuh"
 
 namespace abd {
@@ -52,6 +52,9 @@ struct NarrowArgs {
   const int* adj_pair;
   int cap_ccd;
   int4* ccd_cand;
+  const Box* body_sup;          // CCD_LS: body boxes over every DOF set between the two
+  int cap_ecand;
+  int4* ecand;                  // CCD_LS: line-search candidates
   int cap_contacts;
   int4 *contacts, *contacts_by_pair;
   XSum* energy;
@@ -74,62 +77,27 @@ struct NarrowArgs {
   int* pair_active;
 };
 
-// Conservative world box of an internal node of a body moving by x = A^T r + p, from its
-// rest-frame box R: centre and half extents map to p + A^T c and |A|^T h.  Computed in
-// FP32 from FP32 copies m = (A row-major, p) of the DOFs; every rounding error of that
-// (operand conversion, the products and sums, the rest box's own rounding) stays below
-// 2^-21 (|p_j| + sum_k |A_kj| max(|R.lo_k|, |R.hi_k|)), so a margin of 2^-16 of that plus the
-// leaf dilation `pad` (rounded up) keeps every leaf box of the subtree inside the result.
-__device__ inline Box affine_box(const Box& R, const float* m, float pad) {
-  float c[3], h[3], e[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    c[k] = 0.5f * (R.lo[k] + R.hi[k]);
-    h[k] = 0.5f * (R.hi[k] - R.lo[k]);
-    e[k] = fmaxf(fabsf(R.lo[k]), fabsf(R.hi[k]));
-  }
-  Box B;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const float a0 = m[j], a1 = m[3 + j], a2 = m[6 + j];
-    const float cw = __fmaf_rn(a2, c[2], __fmaf_rn(a1, c[1], __fmaf_rn(a0, c[0], m[9 + j])));
-    const float hw = __fmaf_rn(fabsf(a2), h[2], __fmaf_rn(fabsf(a1), h[1], fabsf(a0) * h[0]));
-    const float sc = __fmaf_rn(fabsf(a2), e[2], __fmaf_rn(fabsf(a1), e[1], __fmaf_rn(fabsf(a0), e[0], fabsf(m[9 + j]))));
-    const float w = hw + __fmaf_rn(sc, 0x1p-16f, pad);
-    B.lo[j] = cw - w;
-    B.hi[j] = cw + w;
-  }
-  B.pad0 = B.pad1 = 0.f;
-  return B;
-}
-
 // Per-CTA view of one body's subtree boxes.  Refit mode (m0 == null): the stored boxes.
 // Affine mode: internal nodes are the affine images of their rest boxes under the body's
-// DOFs at y0 (m0) and, when swept, y1 (m1); leaves are computed from the positions.
+// DOFs at y0 (m0) and, when swept, y1 (m1); leaves are computed from the positions, or, with
+// sup, are the affine images of their rest boxes too (boxes that hold the leaf's box at every
+// DOF set between m0 and m1).
 struct NodeBoxes {
   const Tree* tr;
   const float *m0, *m1;
   float pad;
   const int* prims;   // tris or edges
   int tri;            // 1: triangle tree, 0: edge tree
+  int sup;
   const double *y0, *y1;
   double dhh;
   __device__ inline Box internal(int node) const {
     if (!m0) return load_box(&tr->box[node]);
-    const Box R = load_box(&tr->rest[node]);
-    Box B = affine_box(R, m0, pad);
-    if (m1) {
-      const Box B1 = affine_box(R, m1, pad);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        B.lo[k] = fminf(B.lo[k], B1.lo[k]);
-        B.hi[k] = fmaxf(B.hi[k], B1.hi[k]);
-      }
-    }
-    return B;
+    return affine_box2(load_box(&tr->rest[node]), m0, m1, pad);
   }
   __device__ inline Box leaf(int node, int prim) const {
     if (!m0) return load_box(&tr->box[node]);
+    if (sup) return affine_box2(load_box(&tr->rest[node]), m0, m1, pad);
     return tri ? tri_leaf_box(prims, y0, y1, prim) : edge_leaf_box(prims, y0, y1, prim, dhh);
   }
 };
@@ -207,6 +175,7 @@ __device__ inline NodeBoxes node_boxes(const NarrowArgs& a, const Tree* tr, bool
   nb.pad = __double2float_ru(0.5 * a.prm.dhat);
   nb.prims = tri ? a.tris : a.edges;
   nb.tri = tri;
+  nb.sup = 0;
   nb.y0 = a.y0;
   nb.y1 = a.y1;
   nb.dhh = 0.5 * a.prm.dhat;
@@ -485,51 +454,9 @@ __global__ void __launch_bounds__(NT) k_pair_assemble(NarrowArgs a) {
 // ---------------------------------------------------------------------------------------
 // per-body terms shared by the body kernels and the energy / CCD chunks
 // ---------------------------------------------------------------------------------------
-// predicted DOFs q~ = q0 + dt qdot (+ dt^2 g for p) (orthogonal_energy.py:24-32)
-__device__ inline void tilde_of(const abd_params& P, const abd_states& st, int b, double At[9], double pt[3]) {
-  const double dt = P.dt;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) At[k] = st.A0[9 * b + k] + dt * st.Adot[9 * b + k];
-  const double gv[3] = {0.0, P.gravity, 0.0};
-#pragma unroll
-  for (int k = 0; k < 3; ++k) pt[k] = (st.p0[3 * b + k] + dt * st.pdot[3 * b + k]) + (dt * dt) * gv[k];
-}
-
 // does vertex v take part in the vertex-ground terms (culling.py:64-82)?  bb: its body box
 __device__ inline bool vg_candidate_of(const abd_params& P, const Box& bb, const double* y0, const double* y1, int v) {
-  if (!((double)bb.lo[1] < 0.5 * P.dhat + P.ground)) return false;
-  const Box q = point_box(y0, y1, v, (float)P.dhat);
-  Box g;
-  g.lo[0] = g.lo[1] = g.lo[2] = -1e3f;
-  g.hi[0] = 1e3f;
-  g.hi[1] = (float)P.ground;
-  g.hi[2] = 1e3f;
-  return overlap(q, g);
-}
-
-// inertia + orthogonality energy of a free body at trial DOFs K, pk (orthogonal_energy.py:24-32)
-__device__ inline double inertia_energy(const abd_params& P, const abd_states& st, const double* mass,
-                                        const double* I0, int b, const double* K, const double* pk) {
-  double At[9], pt[3];
-  tilde_of(P, st, b, At, pt);
-  double eo = 0.0;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      const double tt =
-          (K[3 * i] * K[3 * j] + K[3 * i + 1] * K[3 * j + 1] + K[3 * i + 2] * K[3 * j + 2]) - (i == j ? 1.0 : 0.0);
-      eo += tt * tt;
-    }
-  eo = eo * P.stiffness;
-  double d0[3], d1[3], d2[3], d3v[3];
-  for (int k = 0; k < 3; ++k) {
-    d0[k] = pk[k] - pt[k];
-    d1[k] = K[k] - At[k];
-    d2[k] = K[3 + k] - At[3 + k];
-    d3v[k] = K[6 + k] - At[6 + k];
-  }
-  auto dd = [](const double* u) { return u[0] * u[0] + u[1] * u[1] + u[2] * u[2]; };
-  const double nm = dd(d0) * mass[b] + (dd(d1) + dd(d2) + dd(d3v)) * I0[b];
-  return eo * P.dt * P.dt + 0.5 * nm;
+  return vg_box_test(P, bb, point_box(y0, y1, v, (float)P.dhat));
 }
 
 // time of impact of a vertex with the ground plane (ccd.py:9-18); 1 when none
@@ -587,10 +514,16 @@ __device__ inline bool ee_owner(int I, int nEI, int J, int nEJ) { return nEI > n
 // ENERGY adds every nonzero term to one exact accumulator of the whole pass (any order gives
 // the same sum); CCD takes the minimum time of impact by an atomic maximum on complemented
 // bits.  (ipcsk/energy.py:9-48, orthogonal_energy.py:24-32, ccd.py:9-40, 133-186)
+// CCD_LS is the CCD pass of the step: it culls with boxes that hold every box of the
+// primitives at all DOF sets between the pass's two (body_sup, the affine images of the
+// queries' and leaves' rest boxes) and appends every pair found to the line-search
+// candidates; the pairs that also pass the CCD pass's own boxes (body pair, query and leaf)
+// become CCD candidates, the same set as the CCD pass finds.
 constexpr int CW = 4 * CT;  // (query, neighbour) combinations tested per round
 template <int MODE>
 __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
-  constexpr bool ccd = MODE == NARROW_CCD, gh = MODE == NARROW_GH;
+  constexpr bool ls = MODE == NARROW_CCD_LS;
+  constexpr bool ccd = MODE == NARROW_CCD || ls, gh = MODE == NARROW_GH;
   const int c = blockIdx.x, tid = threadIdx.x;
   const int2 ch = a.chunk[c];
   const int I = ch.x;
@@ -598,7 +531,9 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   const int nV = a.voff[I + 1] - a.voff[I];  // items: the body's points, then its edges
   const int Q = max(0, min(CT, nV + nEI - ch.y));
   __shared__ Box qbox[CT];
+  __shared__ Box qsup[ls ? CT : 1];  // CCD_LS: query boxes over the DOF range
   __shared__ int qprim[CT];  // point id, ~edge id, or kNoQuery (primitive kind disabled)
+  __shared__ int nccd[ls ? NBB : 1];  // CCD_LS: the body pair passes the CCD pass's body boxes
   __shared__ Box nbox[NBB];
   __shared__ __align__(16) float ndof[NBB][24];
   __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB], nrel[NBB];
@@ -665,7 +600,8 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       const int k = b0 + tid;
       const int J = gh ? a.adj_col[r0 + k] : (k < kNbList ? a.nbr[(size_t)I * kNbList + k] : kth_neighbour(a, I, k));
       nJ[tid] = J;
-      nbox[tid] = load_box(&a.body_box[J]);
+      nbox[tid] = load_box(&(ls ? a.body_sup : a.body_box)[J]);
+      if constexpr (ls) nccd[tid] = overlap(load_box(&a.body_box[I]), load_box(&a.body_box[J])) ? 1 : 0;
       rel = overlap(cbx, nbox[tid]) ? 1 : 0;
       nrel[tid] = rel;
       ntri[tid] = a.tri.body_root[J];
@@ -678,14 +614,24 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       loaded = true;
       if (tid < Q) {
         const int k = ch.y + tid;
+        const float* m = a.fdof + 24 * (size_t)I;
         if (k < nV) {
           const int v = __ldg(&a.vperm[a.voff[I] + k]);
           qprim[tid] = a.prm.enable_pt ? v : kNoQuery;
           qbox[tid] = point_box(a.y0, a.y1, v, (float)a.prm.dhat);
+          if constexpr (ls) {
+            Box R;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) R.lo[d] = R.hi[d] = (float)__ldg(&a.x0[3 * v + d]);
+            qsup[tid] = affine_box2(R, m, m + 12, __double2float_ru(a.prm.dhat));
+          }
         } else {
           const int e = __ldg(&a.edge.leaf_prim[a.eoff[I] + (k - nV)]);
           qprim[tid] = a.prm.enable_ee ? ~e : kNoQuery;
           qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
+          if constexpr (ls)
+            qsup[tid] = affine_box2(load_box(&a.edge.rest[(a.edge.N - 1) + a.eoff[I] + (k - nV)]), m, m + 12,
+                                    __double2float_ru(0.5 * a.prm.dhat));
         }
       }
       if constexpr (MODE == NARROW_ENERGY) {
@@ -709,15 +655,16 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       for (int it = w0 + tid; it < min(Q * nb, w0 + CW); it += CT) {
         const int q = it % Q, j = it / Q;
         if (!nrel[j] || qprim[q] == kNoQuery || (qprim[q] < 0 && !nown[j])) continue;
-        if (!overlap(qbox[q], nbox[j])) continue;
+        if (!overlap(ls ? qsup[q] : qbox[q], nbox[j])) continue;
         work[atomicAdd(&nwork, 1)] = (unsigned short)(q | (j << 8));
       }
       __syncthreads();
       for (int k = tid; k < nwork; k += CT) {
         const int q = work[k] & 0xff, j = work[k] >> 8;
         const int qp = qprim[q];
-        const Box qb = qbox[q];
-        auto visit = [&](int type, int pa, int pb) {
+        const Box qb = ls ? qsup[q] : qbox[q];
+        // ex: the pair passes the CCD pass's own boxes (CCD_LS)
+        auto visit = [&](int type, int pa, int pb, bool ex) {
           int ids[4];
           d3 xs[4];
           if constexpr (!ccd) {
@@ -738,10 +685,16 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
               atomicAdd(&a.pair_cand[4 * pr + 1], 1);
             }
           } else if constexpr (ccd) {
-            // evaluated by k_ccd_eval, one thread per candidate
-            const int pos = atomicAdd(&a.dstat[DS_NCCD], 1);
-            if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
-            else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+            if constexpr (ls) {
+              const int pos = atomicAdd(&a.dstat[DS_NECAND], 1);
+              if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
+              else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
+            }
+            if (ex) {  // evaluated by k_ccd_eval, one thread per candidate
+              const int pos = atomicAdd(&a.dstat[DS_NCCD], 1);
+              if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
+              else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+            }
           } else {
             const double e = contact_energy(type, xs, a.prm);
             if (e != 0.0) xs_add_atomic(&xe, e);
@@ -749,15 +702,26 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
         };
         if (qp >= 0) {
           Visits vc;
-          traverse(node_boxes(a, &a.tri, true, ndof[j]), ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); }, vc);
+          NodeBoxes nbt = node_boxes(a, &a.tri, true, ndof[j]);
+          nbt.sup = ls;
+          traverse(nbt, ntri[j], qb, a.dstat, [&](int t) {
+            bool ex = true;
+            if constexpr (ls) ex = nccd[j] && overlap(tri_leaf_box(a.tris, a.y0, a.y1, t), qbox[q]);
+            visit(0, qp, t, ex);
+          }, vc);
           pf_node += vc.internal;
           pf_tri += vc.leaf;
         } else {
           // EE candidates are evaluated with the edge of the lower body first, as the per-pair lists
           const bool lower = I < nJ[j];
           Visits vc;
-          traverse(node_boxes(a, &a.edge, false, ndof[j]), nedge[j], qb, a.dstat,
-                   [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); }, vc);
+          NodeBoxes nbe = node_boxes(a, &a.edge, false, ndof[j]);
+          nbe.sup = ls;
+          traverse(nbe, nedge[j], qb, a.dstat, [&](int e) {
+            bool ex = true;
+            if constexpr (ls) ex = nccd[j] && overlap(edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat), qbox[q]);
+            lower ? visit(1, ~qp, e, ex) : visit(1, e, ~qp, ex);
+          }, vc);
           pf_node += vc.internal;
           pf_edge += vc.leaf;
         }
@@ -1072,6 +1036,9 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.adj_pair = s.adj_pair;
   a.cap_ccd = s.cap_ccd;
   a.ccd_cand = s.ccd_cand;
+  a.body_sup = s.body_sup;
+  a.cap_ecand = s.cap_ecand;
+  a.ecand = s.ecand;
   a.cap_contacts = s.cap_contacts;
   a.contacts = s.contacts;
   a.contacts_by_pair = s.contacts_by_pair;
@@ -1139,7 +1106,7 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
 cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
                    const double* y0, const double* y1, const abd_states* st) {
   const NarrowArgs a = narrow_args(s, mode, A, p, A1, p1, y0, y1, st);
-  if (mode == NARROW_ENERGY || mode == NARROW_CCD || mode == NARROW_GH) {
+  if (mode == NARROW_ENERGY || mode == NARROW_CCD || mode == NARROW_CCD_LS || mode == NARROW_GH) {
     // energy, CCD and GH always run at DOFs; the energy needs the states (inertia terms)
     if (!a.affine || (mode == NARROW_ENERGY && !(st && st->A0 && st->Adot && st->p0 && st->pdot)))
       return cudaErrorInvalidValue;
@@ -1150,10 +1117,17 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
       if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[1], s.stream, cudaEventRecordExternal))
         return cudaErrorUnknown;
-    } else if (mode == NARROW_CCD) {
-      cudaError_t e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, sizeof(int), s.stream);
+    } else if (mode == NARROW_CCD || mode == NARROW_CCD_LS) {
+      // DS_NCCD and DS_NECAND are adjacent
+      static_assert(DS_NECAND == DS_NCCD + 1, "candidate counters");
+      cudaError_t e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, 2 * sizeof(int), s.stream);
       if (e != cudaSuccess) return e;
-      k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+      if (mode == NARROW_CCD_LS) {
+        if (!a.y1) return cudaErrorInvalidValue;
+        k_chunk_narrow<NARROW_CCD_LS><<<s.nch, CT, 0, s.stream>>>(a);
+      } else {
+        k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+      }
       k_ccd_eval<<<blocks(s.cap_ccd, 128), 128, 0, s.stream>>>(a);
       ++s.launches;
     } else {

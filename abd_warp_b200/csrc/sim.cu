@@ -133,6 +133,15 @@ int grow_ccd(Sim& s, int need) {
   return ABD_OK;
 }
 
+int grow_ecand(Sim& s, int need) {
+  if (need <= s.cap_ecand) return ABD_OK;
+  if (s.ecand) cudaFree(s.ecand);
+  s.ecand = nullptr;
+  s.cap_ecand = std::max(need + need / 2, 2 * s.cap_ecand);
+  if (dalloc(&s.ecand, s.cap_ecand)) return ABD_ERR_OVERFLOW;
+  return ABD_OK;
+}
+
 int grow_act(Sim& s, int need) {
   if (need <= s.cap_act) return ABD_OK;
   if (s.act_pairs) cudaFree(s.act_pairs);
@@ -171,7 +180,7 @@ int culling(abd_sim* h, const abd::Dofs* d0, const abd::Dofs* d1, double* y0, do
   if (d0) CK(abd::body_broad(s, d0, d1, y0, y1));
   else CK(abd::body_broad(s, nullptr, nullptr, nullptr, nullptr, y0, y1));
   const bool full = mode == abd::NARROW_GH || mode == abd::NARROW_LISTS;
-  CK(abd::body_pairs(s, full));
+  CK(abd::body_pairs(s, full, mode == abd::NARROW_CCD_LS));
   CK(abd::narrow(s, mode, d0 ? d0->Aeff() : nullptr, d0 ? d0->peff() : nullptr, d1 ? d1->Aeff() : nullptr,
                  d1 ? d1->peff() : nullptr, y0, y1, st));
   return ABD_OK;
@@ -216,7 +225,8 @@ constexpr int kRerun = -1;
 int overflow(Sim& s) {
   const int bits = s.hstat[abd::DS_STATUS];
   const int mask = abd::ST_PAIR_OVERFLOW | abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW | abd::ST_VG_OVERFLOW |
-                   abd::ST_ACT_OVERFLOW | abd::ST_CONTACT_OVERFLOW | abd::ST_CCD_OVERFLOW;
+                   abd::ST_ACT_OVERFLOW | abd::ST_CONTACT_OVERFLOW | abd::ST_CCD_OVERFLOW |
+                   abd::ST_ECAND_OVERFLOW;
   if (!(bits & mask)) return 0;
   int r = ABD_OK;
   if (bits & abd::ST_PAIR_OVERFLOW) r = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
@@ -231,6 +241,7 @@ int overflow(Sim& s) {
   if (!r && (bits & abd::ST_ACT_OVERFLOW)) r = grow_act(s, s.hstat[abd::DS_NACTP]);
   if (!r && (bits & abd::ST_CONTACT_OVERFLOW)) r = grow_contacts(s, s.hstat[abd::DS_NCONTACT]);
   if (!r && (bits & abd::ST_CCD_OVERFLOW)) r = grow_ccd(s, s.hstat[abd::DS_NCCD]);
+  if (!r && (bits & abd::ST_ECAND_OVERFLOW)) r = grow_ecand(s, s.hstat[abd::DS_NECAND]);
   if (r) return r;
   const int clear = bits & ~mask;
   s.hstat[abd::DS_STATUS] = clear;
@@ -299,21 +310,22 @@ int energy_trial(abd_sim* h, const abd_states& st, double alpha, double* E) {
 
 // CCD bound between DOFs d0 and d1 (ccd, abd.py:278-303); positions land in x, xk.  pre()
 // enqueues work that belongs to the same pass (the step's dot products, whose results ride
-// along in the mailbox).
+// along in the mailbox).  mode NARROW_CCD_LS also collects the line-search candidates
+// between d0 and d1 for ls_batch.
 template <class Pre>
 int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, double* raw, Pre&& pre,
-           abd::GraphSlot* g = nullptr, uint64_t key = 0) {
+           abd::GraphSlot* g = nullptr, uint64_t key = 0, int mode = abd::NARROW_CCD) {
   Sim& s = h->s;
   auto issue = [&]() -> int {
     int r = pre();
     if (r) return r;
-    if ((r = culling(h, &d0, &d1, s.x, s.xk, abd::NARROW_CCD))) return r;
+    if ((r = culling(h, &d0, &d1, s.x, s.xk, mode))) return r;
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
-  for (int tries = 0;; ++tries) {  // the candidate list has a capacity: grow and rerun
+  for (int tries = 0;; ++tries) {  // the candidate lists have capacities: grow and rerun
     abd::KeyHash k;
-    k.add(key).add(s.cap_ccd).add(s.ccd_cand);
+    k.add(key).add(s.cap_ccd).add(s.ccd_cand).add(mode).add(s.cap_ecand).add(s.ecand);
     int r = g ? abd::run_graph(s, *g, k.h, issue) : issue();
     if (r) return r;
     CK(cudaStreamSynchronize(s.stream));
@@ -337,6 +349,32 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
 int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
            double* raw) {
   return ccd_of(h, direct(A, p), direct(A1, p1), alpha, raw, []() -> int { return ABD_OK; });
+}
+
+// Energies at (A, p) - al[k] dq, k < K <= kLsMax, 0 <= al[k] <= 1, from the candidates of the
+// last CCD_LS pass between (A, p) and (A, p) - dq: one replayed pass and one read.  Each is
+// bitwise the energy pass's at the same DOFs.
+int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p, const double* al, int K,
+             double* E, uint64_t key) {
+  Sim& s = h->s;
+  if (K < 1 || K > abd::kLsMax) return ABD_ERR_INVALID;
+  s.hpar[abd::kParK] = K;
+  for (int k = 0; k < abd::kLsMax; ++k) s.hpar[abd::kParAlpha + k] = k < K ? al[k] : 0.0;
+  auto issue = [&]() -> int {
+    CK(cudaMemcpyAsync(s.dpar + abd::kParK, s.hpar + abd::kParK, sizeof(double) * (1 + abd::kLsMax),
+                       cudaMemcpyHostToDevice, s.stream));
+    CK(abd::ls_energies(s, st, A, p));
+    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
+    return ABD_OK;
+  };
+  abd::KeyHash kh;
+  kh.add(key).add(A).add(p).add(s.cap_ecand).add(s.ecand);
+  int r = abd::run_graph(s, s.g_ls, kh.h, issue);
+  if (r) return r;
+  CK(cudaStreamSynchronize(s.stream));
+  std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
+  for (int k = 0; k < K; ++k) E[k] = xs_round_host(s.hbox->ls_energy[k]);
+  return ABD_OK;
 }
 
 // Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner.
@@ -564,6 +602,21 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
       }
     }
     s.nch = (int)ch.size();
+    // each body's rest box: the union of its chunks' boxes
+    std::vector<abd::Box> brest(n);
+    for (int b = 0; b < n; ++b)
+      for (int k = 0; k < 3; ++k) {
+        brest[b].lo[k] = INFINITY;
+        brest[b].hi[k] = -INFINITY;
+      }
+    for (size_t c = 0; c < ch.size(); ++c) {
+      abd::Box& B = brest[ch[c].x];
+      for (int k = 0; k < 3; ++k) {
+        B.lo[k] = std::min(B.lo[k], cbox[c].lo[k]);
+        B.hi[k] = std::max(B.hi[k], cbox[c].hi[k]);
+      }
+    }
+    ok(upload(&s.body_rest, brest.data(), brest.size(), s.stream));
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
     ok(upload(&s.chunk_box, cbox.data(), cbox.size(), s.stream));
     ok(upload(&s.vperm, vperm.data(), vperm.size(), s.stream));
@@ -588,7 +641,10 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     s.energy_acc = &s.box->energy;
     s.dmin = &s.box->toi_key;
   }
-  ok(dalloc(&s.dpar, 4));
+  ok(dalloc(&s.dpar, abd::kNPar));
+  ok(dalloc(&s.body_sup, n));
+  ok(dalloc(&s.ls_bnd, 6 * (size_t)abd::kLsMax * n));
+  ok(dalloc(&s.ls_box, (size_t)abd::kLsMax * n));
   ok(dalloc(&s.dint, 4));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   ok(dalloc(&s.row_cnt, n));
@@ -598,7 +654,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.kcount, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hbox, sizeof(abd::Mailbox), cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, 4 * sizeof(double), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, abd::kNPar * sizeof(double), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hint, 4 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 32 * sizeof(double), cudaHostAllocDefault);
   // preconditioner tables: cl_ptr, cl_body, body_cl (ints), cl_off (8-byte aligned long longs)
@@ -608,11 +664,11 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.kcount, 0, 4 * sizeof(int), s.stream);
-  if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, 0}
-    s.hpar[0] = 0.0;
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.ls_bnd, 0, sizeof(unsigned long long) * 6 * abd::kLsMax * n, s.stream);
+  if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, ...}
+    for (int k = 0; k < abd::kNPar; ++k) s.hpar[k] = 0.0;
     s.hpar[1] = 1.0;
-    s.hpar[2] = s.hpar[3] = 0.0;
-    e = cudaMemcpyAsync(s.dpar, s.hpar, 4 * sizeof(double), cudaMemcpyHostToDevice, s.stream);
+    e = cudaMemcpyAsync(s.dpar, s.hpar, abd::kNPar * sizeof(double), cudaMemcpyHostToDevice, s.stream);
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(s.red_count, 0, sizeof(int) * abd::kRedSlots, s.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
@@ -627,6 +683,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (!r) r = grow_act(s, std::max(1024, n));
   if (!r) r = grow_contacts(s, std::max(4096, 8 * n));
   if (!r) r = grow_ccd(s, std::max(1 << 15, 32 * n));
+  if (!r) r = grow_ecand(s, std::max(1 << 15, 32 * n));
   s.cap_pt = 0;
   s.cap_ee = 0;
   if (!r) r = grow_lists(s, std::max(1 << 14, V / 4), std::max(1 << 14, E / 4));
@@ -653,10 +710,11 @@ int abd_sim_destroy(abd_sim* h) {
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.dint,
                   s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
-                  s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand};
+                  s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
+                  s.body_sup, s.ls_bnd, s.ls_box};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_kblock})
+  for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_kblock, &s.g_ls})
     if (g->exec) cudaGraphExecDestroy(g->exec);
   if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
   for (cudaEvent_t ev : s.prof_ev)
@@ -832,6 +890,21 @@ int abd_ccd(abd_sim* h, const double* A, const double* p, const double* A1, cons
   return ccd_at(h, A, p, A1, p1, alpha, raw);
 }
 
+int abd_energies_along(abd_sim* h, const abd_states* st, const double* A, const double* p, const double* alphas,
+                       int K, double* E) {
+  if (!h || !st || !A || !p || !alphas || !E || K < 0 || !st->Ak || !st->pk) return ABD_ERR_INVALID;
+  for (int k = 0; k < K; ++k)
+    if (!(alphas[k] >= 0.0 && alphas[k] <= 1.0)) return ABD_ERR_INVALID;
+  if (K == 0) return ABD_OK;
+  Sim& s = h->s;
+  double a1 = 0.0, raw = 0.0;
+  int r = ccd_of(h, direct(A, p), updated(s, A, p, 1, st->Ak, st->pk), &a1, &raw, []() -> int { return ABD_OK; },
+                 nullptr, 0, abd::NARROW_CCD_LS);
+  for (int k0 = 0; !r && k0 < K; k0 += abd::kLsMax)
+    r = ls_batch(h, *st, A, p, alphas + k0, std::min(abd::kLsMax, K - k0), E + k0, states_key(s, *st));
+  return r;
+}
+
 int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
   if (!h || !stp) return ABD_ERR_INVALID;
   Sim& s = h->s;
@@ -870,21 +943,37 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
       return ABD_OK;
     };
     if ((r = ccd_of(h, direct(st.A, st.p), updated(s, st.A, st.p, 1, st.Ak, st.pk), &alpha, &inf.toi, dots,
-                    &s.g_ccd, states_key(s, st))))
+                    &s.g_ccd, states_key(s, st), abd::NARROW_CCD_LS)))
       return r;
     const double qTg = s.hbox->dots[0], gTg = s.hbox->dots[1];
-    // backtracking line search (abd.py:146-160)
+    // backtracking line search (abd.py:146-160): the trials alpha, alpha / 2, ... up to the
+    // first below alpha_min, kLsMax per batch; the first trial that passes is taken, as in
+    // the sequential search
     double E1 = E0;
-    for (;;) {
-      if ((r = energy_trial(h, st, alpha, &E1))) return r;
-      ++inf.ls_trials;
-      const bool wolfe = E1 < E0 + P.armijo_sign * P.c1 * alpha * qTg ||
-                         std::fabs(E1 - E0) <= P.ls_noise_floor * std::fabs(E0);
-      if (wolfe || alpha < P.alpha_min) break;
-      alpha *= 0.5;
+    for (bool done = false; !done;) {
+      double al[abd::kLsMax], Eb[abd::kLsMax];
+      int K = 0;
+      for (double a_ = alpha; K < abd::kLsMax;) {
+        al[K++] = a_;
+        if (a_ < P.alpha_min) break;
+        a_ *= 0.5;
+      }
+      if ((r = ls_batch(h, st, st.A, st.p, al, K, Eb, states_key(s, st)))) return r;
+      for (int k = 0; k < K && !done; ++k) {
+        alpha = al[k];
+        E1 = Eb[k];
+        ++inf.ls_trials;
+        const bool wolfe = E1 < E0 + P.armijo_sign * P.c1 * alpha * qTg ||
+                           std::fabs(E1 - E0) <= P.ls_noise_floor * std::fabs(E0);
+        done = wolfe || alpha < P.alpha_min;
+      }
+      if (!done) alpha *= 0.5;
     }
     E0 = E1;
     CK(abd::update_dofs(s, st.A, st.p, s.dq, alpha, st.A, st.p));
+    // Ak, pk: the DOFs of the accepted trial, as the sequential search leaves them
+    CK(cudaMemcpyAsync(st.Ak, st.A, nA, cudaMemcpyDeviceToDevice, s.stream));
+    CK(cudaMemcpyAsync(st.pk, st.p, np, cudaMemcpyDeviceToDevice, s.stream));
     ++it;
     inf.alpha = alpha;
     if (gTg < P.tol || it >= P.max_iter) break;

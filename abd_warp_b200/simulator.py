@@ -257,6 +257,21 @@ class AffineBodySimulator:
                                    _ptr(p1.contiguous()), ctypes.byref(a), ctypes.byref(raw)), "abd_ccd")
         return a.value, raw.value
 
+    def energies_along(self, alphas, A=None, p=None):
+        """Energies at (A, p) - alpha dq for step lengths 0 <= alpha <= 1 along the current dq
+        (default A, p: the states' iterate), as the step's line search evaluates its trials:
+        one culling pass over the whole segment, then the trials in batches.  Each value is
+        bitwise compute_energy at the same DOFs.  Ak, pk receive (A, p) - dq."""
+        s = self.states
+        A = s.A if A is None else A.contiguous()
+        p = s.p if p is None else p.contiguous()
+        al = (ctypes.c_double * max(1, len(alphas)))(*[float(a) for a in alphas])
+        E = (ctypes.c_double * max(1, len(alphas)))()
+        cst = self._cstates()
+        _lib.check(self._L.abd_energies_along(self._h, ctypes.byref(cst), _ptr(A), _ptr(p), al, len(alphas), E),
+                   "abd_energies_along")
+        return [E[k] for k in range(len(alphas))]
+
     # ------------------------------------------------------------------ dq / g
     @property
     def dq(self):

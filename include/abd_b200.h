@@ -120,8 +120,8 @@ int abd_collision_set(abd_sim* sim, const double* y0_dev, const double* y1_dev, 
 int abd_collision_set_dofs(abd_sim* sim, const double* A_dev, const double* p_dev, const double* A1_dev,
                            const double* p1_dev, int counts[4]);
 /* Copy the lists of the last abd_collision_set / abd_collision_set_dofs call (valid until the
- * next call that culls: abd_step, abd_ipc_gh, abd_compute_energy, abd_ccd or another
- * collision set) into device buffers of capacity cap rows:
+ * next call that culls: abd_step, abd_ipc_gh, abd_compute_energy, abd_ccd,
+ * abd_energies_along or another collision set) into device buffers of capacity cap rows:
  * ij [cap][2] (I < J), pt [cap][5] and ee [cap][5] as (I, J, pair, local prim of I, local
  * prim of J) like the reference's vec5i lists (culling.py:85-99), vg [cap][2] (body,
  * global vertex).  Any pointer may be NULL. */
@@ -151,6 +151,17 @@ int abd_compute_energy(abd_sim* sim, const abd_states* st, const double* Ak_dev,
  * clamp(toi, 0, 1) * (0.9 if < 1), raw_toi (host, may be NULL) the unclamped minimum. */
 int abd_ccd(abd_sim* sim, const double* A_dev, const double* p_dev, const double* A1_dev, const double* p1_dev,
             double* alpha, double* raw_toi);
+
+/* Energies along the search direction: E[k] = the energy at (A, p) - alphas[k] dq (dq: the
+ * simulator's, set by abd_sim_set_dq or left by abd_step) for K step lengths 0 <= alphas[k] <= 1
+ * (host array), each bitwise equal to abd_compute_energy at those DOFs.  This is how abd_step
+ * evaluates its line-search trials (abd.py:146-160 evaluates compute_energy once per trial):
+ * one culling pass between (A, p) and (A, p) - dq collects every contact candidate that any
+ * step length in [0, 1] can produce, then each batch of up to 16 trials re-evaluates only
+ * those, with the reference's culling predicate applied at each trial's DOFs.  st->Ak, st->pk
+ * receive (A, p) - dq. */
+int abd_energies_along(abd_sim* sim, const abd_states* st, const double* A_dev, const double* p_dev,
+                       const double* alphas, int K, double* E);
 
 /* Inertia + orthogonality energy of n_bodies bodies at trial DOFs (Ak, pk), with the
  * prediction from st->A0 / p0 / Adot / pdot, written to E_dev (one double).  No counterpart in

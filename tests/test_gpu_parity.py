@@ -144,6 +144,34 @@ def test_energy(scene_state):
         assert e == e_ref, (a, e, e_ref)
 
 
+def test_energies_along(scene_state):
+    """The step's batched line-search energies: one culling pass over the segment from (A, p)
+    to (A, p) - dq, then every trial re-evaluated from those candidates with the culling
+    predicate applied at the trial's DOFs.  Each energy equals the oracle's energy pass at the
+    same DOFs bit for bit, and the library's own energy pass too; 20 step lengths take two
+    batches."""
+    name, bodies, prm, o, st, sim = scene_state
+    import torch
+    n = len(bodies)
+    fixed = np.array([bool(b.fixed) for b in bodies])
+    dq = np.zeros((n, 12))
+    dq[:, :3] = -3 * prm.dt * st["pdot"] + np.array([0.0, 0.02, 0.0])
+    dq[:, 3:] = -3 * prm.dt * st["Adot"].reshape(n, 9)
+    dq[fixed] = 0.0
+    alphas = [2.0 ** -k for k in range(18)] + [0.0, 0.7]
+    A, p = st["A0"], st["p0"]
+    sim.dq = torch.as_tensor(dq)
+    try:
+        got = sim.energies_along(alphas, torch.as_tensor(A, device="cuda"), torch.as_tensor(p, device="cuda"))
+        for al, e in zip(alphas, got):
+            Ak = A - dq[:, 3:].reshape(n, 3, 3) * al
+            pk = p - dq[:, :3] * al
+            assert e == o.energy(Ak, pk), (name, al, e, o.energy(Ak, pk))
+            assert e == sim.compute_energy(torch.as_tensor(Ak, device="cuda"), torch.as_tensor(pk, device="cuda"))
+    finally:
+        sim.dq = torch.as_tensor(st["dq"])
+
+
 def test_ccd(scene_state):
     name, bodies, prm, o, st, sim = scene_state
     import torch
