@@ -60,58 +60,94 @@ __device__ inline void flush(XSum* dst, const XSum* acc, int K) {
   }
 }
 
+// Warp-wide maximum of the 64-bit keys of the lanes in seg (every lane of seg calls it): the
+// maximum high word first, then the maximum low word among the lanes that hold it.
+__device__ inline unsigned long long seg_max_key(unsigned seg, unsigned long long key) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned hm = __reduce_max_sync(seg, hi);
+  const unsigned lm = __reduce_max_sync(seg, hi == hm ? lo : 0u);
+  return ((unsigned long long)hm << 32) | lm;
+}
+
 // One thread per vertex (and, for t < n, per body): the inertia + orthogonality energy of
-// each free body and the exact bounds of each body at every trial.  Lanes of a warp that
-// share a body reduce their coordinates (min / max are exact); one lane per (warp, body)
-// updates the body's keys atomically.
+// each free body and the exact bounds of each body at every trial.  The body terms of a
+// warp are summed exactly across the warp before one lane adds them to the block's
+// accumulator.  Lanes of a warp that share a body reduce their bounds keys (order-preserving,
+// so the maximum key is the exact min / max); one lane per (warp, body) updates the body's
+// keys atomically.
 __global__ void __launch_bounds__(256) k_ls_bounds(LsArgs a) {
   const int K = ls_trials(a);
   const int t = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
   __shared__ XSum acc[kLsMax];
   for (int e = threadIdx.x; e < kLsMax * (kXD + 1); e += 256) reinterpret_cast<long long*>(acc)[e] = 0;
   __syncthreads();
-  if (t < a.n && !a.fixed[t]) {
+  if (blockIdx.x * 256 < a.n) {  // block-uniform: the warps that hold bodies
+    const bool body = t < a.n && !a.fixed[t];
     for (int k = 0; k < K; ++k) {
-      double M[12];
-      dofs_at(a.A, a.p, a.dq, t, a.dpar[kParAlpha + k], M);
-      xs_add_atomic(&acc[k], inertia_energy(a.prm, a.st, a.mass, a.I0, t, M, M + 9));
+      XSum r;
+      xs_zero(r);
+      if (body) {
+        double M[12];
+        dofs_at(a.A, a.p, a.dq, t, a.dpar[kParAlpha + k], M);
+        xs_add(r, inertia_energy(a.prm, a.st, a.mass, a.I0, t, M, M + 9));
+      }
+      xs_warp_sum(r);
+      if (lane == 0) {
+        long long* d = reinterpret_cast<long long*>(&acc[k]);
+#pragma unroll
+        for (int i = 0; i < kXD; ++i)
+          if (r.d[i]) atomicAdd((unsigned long long*)&d[i], (unsigned long long)r.d[i]);
+        if (r.flags) atomicOr((unsigned long long*)&d[kXD], (unsigned long long)r.flags);
+      }
     }
   }
   const bool live = t < a.V;
   const int b = live ? a.vbody[t] : -1;
-  double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+  double r0 = 0.0, r1 = 0.0, r2 = 0.0, q[12], dq[12];
   if (live) {
     r0 = a.x0[3 * t];
     r1 = a.x0[3 * t + 1];
     r2 = a.x0[3 * t + 2];
-  }
-  for (int k = 0; k < K; ++k) {
-    double c[3] = {0.0, 0.0, 0.0};
-    if (live) {
-      double M[12];
-      dofs_at(a.A, a.p, a.dq, b, a.dpar[kParAlpha + k], M);
 #pragma unroll
-      for (int j = 0; j < 3; ++j) c[j] = xform(M, r0, r1, r2, j);
+    for (int i = 0; i < 9; ++i) q[i] = a.A[9 * b + i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) q[9 + i] = a.p[3 * b + i];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) dq[i] = a.dq[12 * b + i];
+  }
+  const unsigned livemask = __ballot_sync(0xffffffffu, live);
+  for (int k = 0; k < K; ++k) {
+    const double al = a.dpar[kParAlpha + k];
+    unsigned long long key[6];
+    if (live) {
+      // dofs_at and xform with the DOFs held in registers
+      double M[12];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) M[9 + i] = q[9 + i] - dq[i] * al;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) M[3 * r + i] = q[3 * r + i] - dq[3 * (r + 1) + i] * al;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double c = xform(M, r0, r1, r2, j);
+        key[j] = max_key(-c);
+        key[3 + j] = max_key(c);
+      }
     }
-    // segmented reduction: one round per distinct body in the warp (bodies are contiguous)
-    unsigned pending = __ballot_sync(0xffffffffu, live);
+    // one round per distinct body in the warp (bodies are contiguous)
+    unsigned pending = livemask;
     while (pending) {
       const int lead = __ffs(pending) - 1;
       const int bl = __shfl_sync(0xffffffffu, b, lead);
-      const bool mine = live && b == bl;
-      pending &= ~__ballot_sync(0xffffffffu, mine);
+      const unsigned seg = __ballot_sync(0xffffffffu, live && b == bl);
+      pending &= ~seg;
+      if (live && b == bl) {
+        unsigned long long* kb = a.bnd + 6 * ((size_t)k * a.n + bl);
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        double lo = mine ? c[j] : INFINITY, hi = mine ? c[j] : -INFINITY;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-          hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        }
-        if (lane == lead) {
-          unsigned long long* kb = a.bnd + 6 * ((size_t)k * a.n + bl);
-          atomicMax(&kb[j], max_key(-lo));
-          atomicMax(&kb[3 + j], max_key(hi));
+        for (int i = 0; i < 6; ++i) {
+          const unsigned long long m = seg_max_key(seg, key[i]);
+          if (lane == lead) atomicMax(&kb[i], m);
         }
       }
     }
