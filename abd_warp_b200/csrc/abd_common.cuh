@@ -244,7 +244,8 @@ struct Sim {
   int* hint = nullptr;             // pinned staging of dint
   // captured passes: energy trial, CCD bound, GH, Krylov setup and one block of iterations
   cudaStream_t cap_stream = nullptr;
-  GraphSlot g_energy, g_energy_ev, g_ccd, g_gh, g_kinit, g_kblock, g_ls;
+  cudaStream_t cap_stream2 = nullptr;  // captures the bodies of conditional (loop) nodes
+  GraphSlot g_energy, g_energy_ev, g_ccd, g_gh, g_kinit, g_ls;
   unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
   // kernel profiling of the energy pass's narrow kernel: CUDA events around it (recorded as
   // graph nodes), its duration and algorithmic bytes accumulated after every pass

@@ -647,6 +647,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.ls_box, (size_t)abd::kLsMax * n));
   ok(dalloc(&s.dint, 4));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream2, cudaStreamNonBlocking);
   ok(dalloc(&s.row_cnt, n));
   ok(dalloc(&s.nbr, (size_t)n * abd::kNbList));
   ok(dalloc(&s.fdof, 24 * (size_t)n));
@@ -714,9 +715,10 @@ int abd_sim_destroy(abd_sim* h) {
                   s.body_sup, s.ls_bnd, s.ls_box};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_kblock, &s.g_ls})
+  for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_ls})
     if (g->exec) cudaGraphExecDestroy(g->exec);
   if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
+  if (s.cap_stream2) cudaStreamDestroy(s.cap_stream2);
   for (cudaEvent_t ev : s.prof_ev)
     if (ev) cudaEventDestroy(ev);
   for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar,

@@ -14,9 +14,11 @@
 // reference's choice).  Convergence is measured in the preconditioned norm,
 // r^T M^-1 r <= tol^2 b^T M^-1 b, which stays resolvable in FP64 although the plain residual
 // of such stiff systems has a rounding floor near eps * cond.  The SpMV is warp per block row
-// (24 lanes = 12 rows x 2 half-rows).  Dot products are per-CTA partials on a fixed grid of
-// kRedBlocks CTAs summed in a fixed order, so the solve is bitwise reproducible.  The host
-// checks the device-side convergence flags every kCheckEvery iterations.
+// (24 lanes = 12 rows x 2 half-rows).  Dot products are exact (per-CTA partials summed in
+// fixed point), so the solve is bitwise reproducible.  The iterations run as the body of a
+// CUDA graph WHILE node: the last kernel of an iteration advances the device iteration
+// counter, makes the convergence test that the next iteration would make, and sets the
+// loop's condition, so a solve runs exactly its iterations with no host round trip.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,7 +35,6 @@ namespace abd {
 namespace {
 
 constexpr int WPB = 8;          // warps (body rows) per CTA of the row kernels
-constexpr int kCheckEvery = 8;  // iterations launched between host checks
 constexpr int AT = 128;         // threads of the cluster kernels
 constexpr int kMaxCluster = 12; // bodies per cluster: 144 x 144 doubles fit in shared memory
 
@@ -142,11 +143,35 @@ __device__ inline bool solver_done(const int* dstat) {
   return ((volatile const int*)dstat)[DS_R_DONE] != 0 || ((volatile const int*)dstat)[DS_S_DONE] != 0;
 }
 
-// the current Krylov iteration (device counter advanced by k_next_iteration); iterations
-// beyond the limit do nothing, so a replayed block may overrun it harmlessly
+// the current Krylov iteration (device counter, 1 at the first iteration, advanced by
+// k_loop_end); iterations beyond the limit do nothing
 __device__ inline int iteration(const SolverArgs& a) { return a.dstat[DS_IT]; }
 
-__global__ void k_next_iteration(int* dstat) { dstat[DS_IT] += 1; }
+constexpr int kSlotRzNew = -2;  // k_apply: the r.z slot of the current iteration's new value
+
+// Last kernel of a loop iteration (one thread): advances the iteration counter, makes the
+// convergence test of the next iteration's first kernel (PCG: r.z against the threshold;
+// BiCGSTAB: r.M^-1 r and rho = rh.r), records a stop as that kernel would, and sets the
+// WHILE node's condition.  The loop ends at convergence or after maxit iterations.
+__global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) {
+  const int it = a.dstat[DS_IT];
+  bool stop = solver_done(a.dstat) || it + 1 > a.maxit;
+  if (!stop) {
+    const double thr2 = a.scal[SC_THR2];
+    if (pcg) {
+      stop = !(a.scal[SC_RED + ((it & 1) ? SL_RZ1 : SL_RZ0)] > thr2);
+    } else {
+      const double rho = a.scal[SC_RED + SL_RHR];
+      stop = !(a.scal[SC_RED + SL_RZ0] > thr2) || rho == 0.0 || !isfinite(rho);
+    }
+    if (stop) {
+      a.dstat[DS_R_DONE] = it + 1;
+      a.dstat[DS_SOLVER_ITERS] = it;
+    }
+  }
+  a.dstat[DS_IT] = it + 1;
+  cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
 
 // ---- preconditioner setup: assemble and invert each cluster's dense block system ----
 __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, int c1, const int* body_cl) {
@@ -213,6 +238,7 @@ __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, in
 __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out,
                                               double* copy, int slot) {
   if (it_guard && (solver_done(a.dstat) || iteration(a) > a.maxit)) return;
+  if (slot == kSlotRzNew) slot = (iteration(a) & 1) ? SL_RZ1 : SL_RZ0;
   constexpr int NWA = AT / 32;
   __shared__ double vs[NWA][12 * kMaxCluster];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -486,6 +512,7 @@ __global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, 
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
     a.scal[SC_THR2] = tol2 * b;
+    a.dstat[DS_IT] = 1;
     if (!(b > 0.0)) a.dstat[DS_R_DONE] = 1;
   }
 }
@@ -625,75 +652,83 @@ int build_preconditioner(Sim& s) {
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
-// Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  The setup and each
-// block of kCheckEvery iterations are replayed graphs; the host reads the convergence flags
-// (in the mailbox) after every block.
+// Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  One replayed graph:
+// the setup kernels, then a WHILE node whose body is one iteration (its last kernel sets the
+// loop condition), then the mailbox copy; the host reads the outcome once.
 int krylov_solve(Sim& s, double* x, int* iters_out) {
   const SolverArgs a = solver_args(s);
   const double* bvec = s.g;
   const bool pcg = s.prm.solver == 1;
+  const int per_iter = pcg ? 5 : 10;  // kernels of one iteration
   KeyHash kh;
   kh.add(x).add(s.n).add(s.prm_version).add(s.prm.solver).add(s.prm.cg_max_iter).add(s.cl_inv).add(s.box);
-  const uint64_t key = kh.h;
-  int r = run_graph(s, s.g_kinit, key, [&]() -> int {
+  int r = run_graph(s, s.g_kinit, kh.h, [&]() -> int {
     cudaStream_t st = s.stream;
     // b^T M^-1 b sets the threshold
     k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
     k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
                                            pcg ? nullptr : s.v);
     if (cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st) ||
-        cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st) ||
-        cudaMemsetAsync(s.dstat + DS_IT, 0, sizeof(int), st))
+        cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st))
       return ABD_ERR_CUDA;
     k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x);
     // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
     k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
     s.launches += 4;
+    // the iteration loop: a WHILE node on the capture, its body captured on a second stream
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusActive)
+      return ABD_ERR_CUDA;
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) return ABD_ERR_CUDA;
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t loop;
+    if (cudaGraphAddNode(&loop, graph, deps, ndeps, &np) != cudaSuccess) return ABD_ERR_CUDA;
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+      return ABD_ERR_CUDA;
+    cudaStream_t bs = s.cap_stream2;
+    if (cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return ABD_ERR_CUDA;
+    if (pcg) {
+      k_pcg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v);
+      k_pcg_2<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v, x, s.r);
+      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.z, nullptr, kSlotRzNew);
+      k_pcg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.pv);
+    } else {
+      k_bicg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.pv, s.v);
+      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.pv, s.y, nullptr, -1);
+      k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
+      k_bicg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.v, s.s);
+      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
+      k_bicg_4<<<kRedBlocks, 256, 0, bs>>>(a, s.y, x);
+      k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
+      k_bicg_6<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
+      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
+    }
+    k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
+    s.launches += per_iter;
+    cudaGraph_t body_out = nullptr;
+    const cudaError_t eb = cudaGetLastError();
+    if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
+    if (cudaMemcpyAsync(s.hbox, s.box, sizeof(Mailbox), cudaMemcpyDeviceToHost, st)) return ABD_ERR_CUDA;
     return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
   });
   if (r) return r;
-  const int maxit = s.prm.cg_max_iter;
-  for (int done = 0;;) {
-    r = run_graph(s, s.g_kblock, key, [&]() -> int {
-      cudaStream_t st = s.stream;
-      // iterations start at odd numbers (1, 1 + kCheckEvery, ...), so each position of the
-      // block has a fixed parity and the alternating r.z slots are the same in every block
-      for (int k = 0; k < kCheckEvery; ++k) {
-        k_next_iteration<<<1, 1, 0, st>>>(s.dstat);
-        if (pcg) {
-          const int rz_new = ((1 + k) & 1) ? SL_RZ1 : SL_RZ0;
-          k_pcg_1<<<kRedBlocks, 256, 0, st>>>(a, s.pv, s.v);
-          k_pcg_2<<<kRedBlocks, 256, 0, st>>>(a, s.pv, s.v, x, s.r);
-          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.z, nullptr, rz_new);
-          k_pcg_3<<<kRedBlocks, 256, 0, st>>>(a, s.z, s.pv);
-          s.launches += 5;
-        } else {
-          k_bicg_1<<<kRedBlocks, 256, 0, st>>>(a, s.r, s.pv, s.v);
-          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.pv, s.y, nullptr, -1);
-          k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
-          k_bicg_3<<<kRedBlocks, 256, 0, st>>>(a, s.r, s.v, s.s);
-          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
-          k_bicg_4<<<kRedBlocks, 256, 0, st>>>(a, s.y, x);
-          k_spmv<<<kRedBlocks, 256, 0, st>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
-          k_bicg_6<<<kRedBlocks, 256, 0, st>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-          k_apply<<<kRedBlocks, AT, 0, st>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
-          s.launches += 10;
-        }
-      }
-      if (cudaMemcpyAsync(s.hbox, s.box, sizeof(Mailbox), cudaMemcpyDeviceToHost, st)) return ABD_ERR_CUDA;
-      return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
-    });
-    if (r) return r;
-    if (cudaStreamSynchronize(s.stream) != cudaSuccess) return ABD_ERR_CUDA;
-    done += kCheckEvery;
-    const int* ds = s.hbox->dstat;
-    if (ds[DS_R_DONE] || ds[DS_S_DONE]) break;
-    if (done >= maxit) {
-      s.host_status |= ST_SOLVER_NOCONV;  // not converged: reported through the status bits
-      break;
-    }
-  }
-  if (iters_out) *iters_out = s.hbox->dstat[DS_SOLVER_ITERS];
+  if (cudaStreamSynchronize(s.stream) != cudaSuccess) return ABD_ERR_CUDA;
+  const int* ds = s.hbox->dstat;
+  // the graph's launch count covers one iteration; the loop ran ds[DS_IT] - 1
+  s.launches += (long long)per_iter * std::max(0, ds[DS_IT] - 2);
+  if (!(ds[DS_R_DONE] || ds[DS_S_DONE])) s.host_status |= ST_SOLVER_NOCONV;  // reported through the status bits
+  if (iters_out) *iters_out = ds[DS_SOLVER_ITERS];
   return ABD_OK;
 }
 
