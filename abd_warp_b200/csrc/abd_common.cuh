@@ -162,6 +162,11 @@ struct Tree {
   // by the affine image of its rest box, which the traversal computes from the body's DOFs
   // instead of a refit
   Box* rest = nullptr;
+  // per internal node, its two children as the traversal needs them, so that one visit is one
+  // round of independent loads: the children's rest boxes [N-1][2] and their codes [N-1]
+  // (the child's node id if internal, ~primitive if a leaf)
+  Box* crest = nullptr;
+  int2* ccode = nullptr;
   // per-body bottom-up refit schedule: the internal nodes of body b's subtree grouped by
   // height, order[lvl[body_lvl[b] + h - 1] .. lvl[body_lvl[b] + h]) for h = 1..heights
   int* order = nullptr;       // [N-1]
@@ -353,12 +358,12 @@ enum : int {
   PF_POINT = 0,      // point queries: FP64 position (24 B)
   PF_EDGE = 1,       // edge queries: two vertex ids + two positions (56 B)
   PF_NEIGHBOUR = 2,  // (chunk, neighbour) records: body box, FP32 DOFs, roots (140 B)
-  PF_NODE = 3,       // internal tree nodes tested: rest box + child ids (40 B)
+  PF_NODE = 3,       // internal tree nodes tested: rest box + child code (36 B)
   PF_TRI = 4,        // triangle leaves tested: three ids + three positions (84 B)
   PF_EDGELEAF = 5,   // edge leaves tested: two ids + two positions (56 B)
   PF_N = 6
 };
-constexpr double kProfBytes[PF_N] = {24.0, 56.0, 140.0, 40.0, 84.0, 56.0};
+constexpr double kProfBytes[PF_N] = {24.0, 56.0, 140.0, 36.0, 84.0, 56.0};
 
 
 // ---------------------------------------------------------------------------------------

@@ -500,13 +500,39 @@ cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, doubl
   return cudaGetLastError();
 }
 
-// Rest-frame boxes of all nodes: the leaf boxes and refit of the rest positions, copied aside.
+// child tables of the traversal (one thread per internal node)
+__global__ void k_child_tables(int N, const int* child, const int* leaf_prim, const Box* rest, Box* crest,
+                               int2* ccode) {
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= N - 1) return;
+  int code[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int c = child[2 * node + h];
+    store_box(&crest[2 * node + h], load_box(&rest[c]));
+    code[h] = c >= N - 1 ? ~leaf_prim[c - (N - 1)] : c;
+  }
+  ccode[node] = make_int2(code[0], code[1]);
+}
+
+// Rest-frame boxes of all nodes: the leaf boxes and refit of the rest positions, copied aside,
+// and the traversal's child tables.
 cudaError_t rest_boxes(Sim& s) {
   cudaError_t e = body_broad(s, nullptr, nullptr, nullptr, nullptr, s.x0, nullptr);
   for (Tree* t : {&s.tri_tree, &s.edge_tree})
     if (e == cudaSuccess && t->N > 0)
       e = cudaMemcpyAsync(t->rest, t->box, sizeof(Box) * (size_t)(2 * t->N - 1), cudaMemcpyDeviceToDevice,
                           s.stream);
+  for (Tree* t : {&s.tri_tree, &s.edge_tree})
+    if (e == cudaSuccess && t->N > 1) {
+      if ((e = cudaMalloc(&t->crest, sizeof(Box) * 2 * (size_t)(t->N - 1))) != cudaSuccess ||
+          (e = cudaMalloc(&t->ccode, sizeof(int2) * (size_t)(t->N - 1))) != cudaSuccess)
+        break;
+      k_child_tables<<<blocks(t->N - 1, 256), 256, 0, s.stream>>>(t->N, t->child, t->leaf_prim, t->rest, t->crest,
+                                                                   t->ccode);
+      ++s.launches;
+      e = cudaGetLastError();
+    }
   // no pair pass follows: clear the bounds here (the pair mask clears them otherwise)
   if (e == cudaSuccess) e = cudaMemsetAsync(s.body_bnd, 0, sizeof(unsigned long long) * 12 * (size_t)s.n, s.stream);
   return e;

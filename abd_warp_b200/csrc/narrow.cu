@@ -103,7 +103,9 @@ struct NodeBoxes {
 };
 
 // Stack traversal of the subtree rooted at `root`; calls f(prim) for every leaf whose box
-// overlaps q, in a fixed depth-first order.
+// overlaps q, in a fixed depth-first order.  Affine mode reads a popped node's child tables
+// (codes and rest boxes, indexed by the node itself), so a visit costs one round of
+// independent loads; refit mode reads the stored world boxes of the children.
 // visits: tested internal nodes and leaves (kernel profiling)
 struct Visits {
   unsigned internal = 0, leaf = 0;
@@ -133,17 +135,30 @@ __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int
   stack[sp++] = root;
   while (sp > 0) {
     const int node = stack[--sp];
-    const int c0 = __ldg(&tr.child[2 * node]), c1 = __ldg(&tr.child[2 * node + 1]);
+    const int2 cc = __ldg(&tr.ccode[node]);
+    Box R[2];
+    if (nb.m0) {
+      R[0] = load_box(&tr.crest[2 * node]);
+      R[1] = load_box(&tr.crest[2 * node + 1]);
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int c = h ? c1 : c0;
-      if (c >= L0) {
-        const int prim = __ldg(&tr.leaf_prim[c - L0]);
+      const int code = h ? cc.y : cc.x;
+      if (code < 0) {
+        const int prim = ~code;
         ++cnt.leaf;
-        if (overlap(nb.leaf(c, prim), q)) f(prim);
-      } else if (++cnt.internal, overlap(nb.internal(c), q)) {
-        if (sp < kTraversalStack) stack[sp++] = c;
-        else atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
+        Box B;
+        if (!nb.m0) B = load_box(&tr.box[L0 + __ldg(&tr.prim_leaf[prim])]);
+        else if (nb.sup) B = affine_box2(R[h], nb.m0, nb.m1, nb.pad);
+        else B = nb.tri ? tri_leaf_box(nb.prims, nb.y0, nb.y1, prim) : edge_leaf_box(nb.prims, nb.y0, nb.y1, prim, nb.dhh);
+        if (overlap(B, q)) f(prim);
+      } else {
+        ++cnt.internal;
+        const Box B = nb.m0 ? affine_box2(R[h], nb.m0, nb.m1, nb.pad) : load_box(&tr.box[code]);
+        if (overlap(B, q)) {
+          if (sp < kTraversalStack) stack[sp++] = code;
+          else atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
+        }
       }
     }
   }

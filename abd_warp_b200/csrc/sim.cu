@@ -88,7 +88,8 @@ cudaError_t upload(T** p, const T* host, size_t count, cudaStream_t st) {
 
 void free_tree(abd::Tree& t) {
   for (void* q : {(void*)t.child, (void*)t.parent, (void*)t.leaf_prim, (void*)t.prim_leaf, (void*)t.body_root,
-                  (void*)t.rest, (void*)t.box, (void*)t.order, (void*)t.lvl, (void*)t.body_lvl})
+                  (void*)t.rest, (void*)t.box, (void*)t.order, (void*)t.lvl, (void*)t.body_lvl, (void*)t.crest,
+                  (void*)t.ccode})
     if (q) cudaFree(q);
   t = abd::Tree{};
 }

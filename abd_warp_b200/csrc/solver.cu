@@ -35,7 +35,8 @@ namespace abd {
 namespace {
 
 constexpr int WPB = 8;          // warps (body rows) per CTA of the row kernels
-constexpr int AT = 128;         // threads of the cluster kernels
+constexpr int AT = 128;         // threads of the cluster apply kernel
+constexpr int IT = 512;         // threads of the cluster inverse kernel (one CTA per cluster)
 constexpr int kMaxCluster = 12; // bodies per cluster: 144 x 144 doubles fit in shared memory
 
 // slots of Sim::partials
@@ -174,15 +175,15 @@ __global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) 
 }
 
 // ---- preconditioner setup: assemble and invert each cluster's dense block system ----
-__global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, int c1, const int* body_cl) {
+__global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, int c0, int c1, const int* body_cl) {
   extern __shared__ double K[];
   for (int c = c0 + blockIdx.x; c < c1; c += gridDim.x) {
     const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
-    for (int e = threadIdx.x; e < D * D; e += AT) K[e] = 0.0;
+    for (int e = threadIdx.x; e < D * D; e += IT) K[e] = 0.0;
     __syncthreads();
     // block row of every member: its diagonal block and the blocks of active pairs whose
     // other body is in the same cluster
-    for (int e = threadIdx.x; e < s * 144; e += AT) {
+    for (int e = threadIdx.x; e < s * 144; e += IT) {
       const int li = e / 144, rc = e % 144;
       const int b = a.cl_body[base + li];
       K[(size_t)(12 * li + rc / 12) * D + 12 * li + rc % 12] = a.diag[(size_t)b * 144 + rc];
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, in
           while (a.cl_body[base + lj] != J) ++lj;  // members are few (<= kMaxCluster)
           const int side = a.ij[pr].x == b ? 0 : 1;
           const double* O = a.offdiag + (size_t)pr * 288 + side * 144;
-          for (int rc = threadIdx.x; rc < 144; rc += AT)
+          for (int rc = threadIdx.x; rc < 144; rc += IT)
             K[(size_t)(12 * li + rc / 12) * D + 12 * lj + rc % 12] = O[rc];
         }
       }
@@ -213,13 +214,13 @@ __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, in
       const double ip = 1.0 / p;
       if (threadIdx.x == 0) K[(size_t)k * D + k] = 1.0;
       __syncthreads();
-      for (int j = threadIdx.x; j < D; j += AT) K[(size_t)k * D + j] *= ip;
-      for (int i = threadIdx.x; i < D; i += AT) f[i] = (i == k) ? 0.0 : K[(size_t)i * D + k];
+      for (int j = threadIdx.x; j < D; j += IT) K[(size_t)k * D + j] *= ip;
+      for (int i = threadIdx.x; i < D; i += IT) f[i] = (i == k) ? 0.0 : K[(size_t)i * D + k];
       __syncthreads();
-      for (int i = threadIdx.x; i < D; i += AT)
+      for (int i = threadIdx.x; i < D; i += IT)
         if (i != k) K[(size_t)i * D + k] = 0.0;
       __syncthreads();
-      for (int e = threadIdx.x; e < D * D; e += AT) {
+      for (int e = threadIdx.x; e < D * D; e += IT) {
         const int i = e / D, j = e % D;
         const double fi = f[i];
         if (i != k && fi != 0.0) K[e] -= fi * K[(size_t)k * D + j];
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(AT) k_cluster_inverse(SolverArgs a, int c0, in
       __syncthreads();
     }
     double* out = a.cl_inv + a.cl_off[c];
-    for (int e = threadIdx.x; e < D * D; e += AT) out[e] = K[e];
+    for (int e = threadIdx.x; e < D * D; e += IT) out[e] = K[e];
     __syncthreads();
   }
 }
@@ -647,7 +648,7 @@ int build_preconditioner(Sim& s) {
       cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return ABD_ERR_CUDA;
   const int grid = std::min(s.ncl, 4 * 148);
-  k_cluster_inverse<<<grid, AT, smem, s.stream>>>(a, 0, s.ncl, body_cl_dev);
+  k_cluster_inverse<<<grid, IT, smem, s.stream>>>(a, 0, s.ncl, body_cl_dev);
   ++s.launches;
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }

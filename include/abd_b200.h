@@ -190,7 +190,7 @@ long long abd_launch_count(const abd_sim* sim);
  * the data the kernel reads (and slows it down).
  * abd_profile_read returns the accumulated kernel time (ms), the number of launches and, for
  * mode 2, the algorithmic bytes (point queries 24 B, edge queries 56 B, (chunk, neighbour)
- * records 140 B, internal nodes 40 B, triangle leaves 84 B, edge leaves 56 B).
+ * records 140 B, internal nodes 36 B, triangle leaves 84 B, edge leaves 56 B).
  * abd_profile(sim, 0) stops. */
 int abd_profile(abd_sim* sim, int enable);
 int abd_profile_read(const abd_sim* sim, double* ms, long long* launches, double* bytes);
