@@ -233,6 +233,9 @@ struct Sim {
   int2* chunk = nullptr;           // [nch]
   Box* chunk_box = nullptr;        // [nch] rest-frame box of each chunk's items
   int* vperm = nullptr;            // [V] vertices of each body in Morton order (chunk items)
+  // vertex slices of the line-search bounds: (body, first vertex, count), count <= kSlice
+  int nslice = 0;
+  int4* slice = nullptr;
   XSum* energy_acc = nullptr;      // = &box->energy
   // everything the host reads after a pass, in one device block (one copy per sync)
   Mailbox* box = nullptr;          // device
@@ -317,6 +320,7 @@ constexpr int kChunk = 128;       // items per chunk of the energy / CCD narrow 
 constexpr int kNbList = 32;       // neighbours per body listed by the pair mask
 constexpr int kRedSlots = 12;
 constexpr int kLsMax = 16;        // line-search trials evaluated per batch
+constexpr int kSlice = 64;        // vertices per slice of the line-search bounds (two per lane)
 constexpr int kParK = 4;          // dpar slot of a batch's trial count
 constexpr int kParAlpha = 5;      // dpar slots of its step lengths
 constexpr int kNPar = kParAlpha + kLsMax;

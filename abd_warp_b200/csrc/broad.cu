@@ -41,6 +41,8 @@ struct VertexArgs {
   unsigned long long* bnd;
   float* fdof;   // [n][2][12] FP32 DOFs (A row-major, p) of each set
   Mailbox* box;  // accumulators of the pass, cleared here
+  int nslice;
+  const int4* slice;  // vertex slices: (body, first vertex, count <= kSlice)
 };
 
 // DOFs of body b in set k: as given, or (A, p) - alpha dq (same arithmetic as k_update_dofs)
@@ -55,13 +57,24 @@ __device__ inline void body_dofs(const Dofs& d, int b, double M[12]) {
   dofs_at(d.A, d.p, d.dq, b, *d.alpha, M);
 }
 
-// One thread per vertex (and, for t < n, per body): the body's DOFs of each set (written out
-// when updated, and as FP32 copies for the traversal's node boxes), y0 = x(d[0]) (and
-// y1 = x(d[1])) with the arithmetic of k_transform, and the body bounds: lanes of a warp that
-// share a body reduce their coordinates (min / max are exact), one lane per (warp, body)
-// updates the body's keys atomically.  Block 0 clears the pass's accumulators.
+// Warp-wide maximum of the 64-bit keys of all lanes: the maximum high word first, then the
+// maximum low word among the lanes that hold it.
+__device__ inline unsigned long long warp_max_key(unsigned long long key) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned hm = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned lm = __reduce_max_sync(0xffffffffu, hi == hm ? lo : 0u);
+  return ((unsigned long long)hm << 32) | lm;
+}
+
+// One warp per vertex slice (at most kSlice = 64 vertices of one body, two per lane):
+// y0 = x(d[0]) (and y1 = x(d[1])) with the arithmetic of k_transform, and the body bounds:
+// each lane takes the min / max of its vertices' coordinates, the warp reduces their
+// order-preserving keys (the maximum key is the exact min / max) and lane 0 updates the
+// body's keys atomically.  Then one thread per body: the body's DOFs of each set (written
+// out when updated, and as FP32 copies for the traversal's node boxes).  Block 0 clears the
+// pass's accumulators.
 __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
-  const int t = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * 256 + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (blockIdx.x == 0) {
     if (threadIdx.x <= kXD) reinterpret_cast<long long*>(&a.box->energy)[threadIdx.x] = 0;
     if (threadIdx.x == 32) a.box->toi_key = 0;
@@ -69,6 +82,41 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
     (&a.box->prof[0][0])[threadIdx.x] = 0;
   }
   const int nset = a.swept ? 2 : 1;
+  if (w < a.nslice) {
+    const int4 sl = a.slice[w];  // body, first vertex, vertices
+    const int b = sl.x;
+    const bool has[2] = {lane < sl.z, lane + 32 < sl.z};
+    double r[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) r[h][j] = has[h] ? a.x0[3 * (sl.y + lane + 32 * h) + j] : 0.0;
+    for (int k = 0; k < nset; ++k) {
+      double M[12];
+      body_dofs(a.d[k], b, M);
+      double* y = k ? a.y1 : a.y0;
+      unsigned long long* kb = a.bnd + 12 * (size_t)b + 6 * k;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double lo = INFINITY, hi = -INFINITY;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (has[h]) {
+            const double c = xform(M, r[h][0], r[h][1], r[h][2], j);
+            y[3 * (sl.y + lane + 32 * h) + j] = c;
+            lo = fmin(lo, c);
+            hi = fmax(hi, c);
+          }
+        const unsigned long long mlo = warp_max_key(max_key(-lo)), mhi = warp_max_key(max_key(hi));
+        if (lane == 0) {
+          atomicMax(&kb[j], mlo);
+          atomicMax(&kb[3 + j], mhi);
+        }
+      }
+    }
+    return;
+  }
+  const int t = 32 * (w - a.nslice) + lane;
   if (t < a.n) {
     for (int k = 0; k < nset; ++k) {
       double M[12];
@@ -83,45 +131,6 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
       f[0] = make_float4((float)M[0], (float)M[1], (float)M[2], (float)M[3]);
       f[1] = make_float4((float)M[4], (float)M[5], (float)M[6], (float)M[7]);
       f[2] = make_float4((float)M[8], (float)M[9], (float)M[10], (float)M[11]);
-    }
-  }
-  const int v = t;
-  const bool live = v < a.V;
-  const int b = live ? a.vbody[v] : -1;
-  double c[6];
-  if (live) {
-    const double r0 = a.x0[3 * v], r1 = a.x0[3 * v + 1], r2 = a.x0[3 * v + 2];
-    for (int k = 0; k < nset; ++k) {
-      double M[12];
-      body_dofs(a.d[k], b, M);
-      double* y = k ? a.y1 : a.y0;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const double cj = xform(M, r0, r1, r2, j);
-        y[3 * v + j] = cj;
-        c[3 * k + j] = cj;
-      }
-    }
-  }
-  // segmented reduction: one round per distinct body in the warp (bodies are contiguous)
-  unsigned pending = __ballot_sync(0xffffffffu, live);
-  while (pending) {
-    const int lead = __ffs(pending) - 1;
-    const int bl = __shfl_sync(0xffffffffu, b, lead);
-    const bool mine = live && b == bl;
-    pending &= ~__ballot_sync(0xffffffffu, mine);
-    for (int k = 0; k < 3 * nset; ++k) {
-      double lo = mine ? c[k] : INFINITY, hi = mine ? c[k] : -INFINITY;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-      }
-      if (lane == lead) {
-        const int set = k / 3, j = k % 3;
-        atomicMax(&a.bnd[12 * (size_t)bl + 6 * set + j], max_key(-lo));
-        atomicMax(&a.bnd[12 * (size_t)bl + 6 * set + 3 + j], max_key(hi));
-      }
     }
   }
 }
@@ -149,7 +158,7 @@ __global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double d
 // ---------------------------------------------------------------------------------------
 // body pairs: overlap bit matrix, per-row prefix counts, then O(1) placement of every pair
 // ---------------------------------------------------------------------------------------
-constexpr int PR_THREADS = 128;  // one warp per row of the overlap matrix
+constexpr int PR_THREADS = 512;  // one warp per row of the overlap matrix
 constexpr int PR_TILE = 1024;    // body boxes staged in shared memory per tile (32 KB)
 
 // Row I of the overlap matrix, one warp: lane l tests J = 32 w + l and the ballot is word w
@@ -493,9 +502,11 @@ cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, doubl
   a.bnd = s.body_bnd;
   a.fdof = s.fdof;
   a.box = s.box;
+  a.nslice = s.nslice;
+  a.slice = s.slice;
   s.swept = a.swept;
-  const int t = s.V > s.n ? s.V : s.n;
-  k_vertex_broad<<<blocks(t, 256), 256, 0, s.stream>>>(a);
+  const long long warps = (long long)s.nslice + (s.n + 31) / 32;
+  k_vertex_broad<<<blocks(32 * warps, 256), 256, 0, s.stream>>>(a);
   ++s.launches;
   return cudaGetLastError();
 }

@@ -44,6 +44,8 @@ struct LsArgs {
   int cap_ecand;
   const int* dstat;
   XSum* energy;                 // [kLsMax] exact energies of the trials
+  int nslice;
+  const int4* slice;            // vertex slices: (body, first vertex, count <= 64)
 };
 
 __device__ inline int ls_trials(const LsArgs& a) { return (int)a.dpar[kParK]; }
@@ -69,19 +71,69 @@ __device__ inline unsigned long long seg_max_key(unsigned seg, unsigned long lon
   return ((unsigned long long)hm << 32) | lm;
 }
 
-// One thread per vertex (and, for t < n, per body): the inertia + orthogonality energy of
-// each free body and the exact bounds of each body at every trial.  The body terms of a
-// warp are summed exactly across the warp before one lane adds them to the block's
-// accumulator.  Lanes of a warp that share a body reduce their bounds keys (order-preserving,
-// so the maximum key is the exact min / max); one lane per (warp, body) updates the body's
-// keys atomically.
+// One warp per vertex slice (at most 64 vertices of one body: two per lane) for the exact
+// bounds of each body at every trial, then one warp per 32 bodies for the inertia +
+// orthogonality energy of each free body, summed exactly across the warp before one lane
+// adds it to the block's accumulator.  A slice's lanes take the min / max of their vertices'
+// coordinates and the warp reduces the order-preserving keys of those (the maximum key is
+// the exact min / max); lane 0 updates the body's keys atomically.
 __global__ void __launch_bounds__(256) k_ls_bounds(LsArgs a) {
   const int K = ls_trials(a);
-  const int t = blockIdx.x * 256 + threadIdx.x, lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * 256 + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   __shared__ XSum acc[kLsMax];
   for (int e = threadIdx.x; e < kLsMax * (kXD + 1); e += 256) reinterpret_cast<long long*>(acc)[e] = 0;
   __syncthreads();
-  if (blockIdx.x * 256 < a.n) {  // block-uniform: the warps that hold bodies
+  if (w < a.nslice) {
+    const int4 sl = a.slice[w];  // body, first vertex, vertices
+    const int b = sl.x;
+    double r[2][3], q[12], dq[12];
+    const bool has0 = lane < sl.z, has1 = lane + 32 < sl.z;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int v = sl.y + lane + 32 * h;
+      const bool has = h ? has1 : has0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) r[h][j] = has ? a.x0[3 * v + j] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) q[i] = a.A[9 * b + i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) q[9 + i] = a.p[3 * b + i];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) dq[i] = a.dq[12 * b + i];
+    for (int k = 0; k < K; ++k) {
+      const double al = a.dpar[kParAlpha + k];
+      double M[12];  // dofs_at with the DOFs held in registers
+#pragma unroll
+      for (int i = 0; i < 3; ++i) M[9 + i] = q[9 + i] - dq[i] * al;
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) M[3 * rr + i] = q[3 * rr + i] - dq[3 * (rr + 1) + i] * al;
+      unsigned long long* kb = a.bnd + 6 * ((size_t)k * a.n + b);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double lo = INFINITY, hi = -INFINITY;
+        if (has0) {
+          const double c = xform(M, r[0][0], r[0][1], r[0][2], j);
+          lo = c;
+          hi = c;
+        }
+        if (has1) {
+          const double c = xform(M, r[1][0], r[1][1], r[1][2], j);
+          lo = fmin(lo, c);
+          hi = fmax(hi, c);
+        }
+        const unsigned long long mlo = seg_max_key(0xffffffffu, max_key(-lo));
+        const unsigned long long mhi = seg_max_key(0xffffffffu, max_key(hi));
+        if (lane == 0) {
+          atomicMax(&kb[j], mlo);
+          atomicMax(&kb[3 + j], mhi);
+        }
+      }
+    }
+  } else if (w - a.nslice < (a.n + 31) / 32) {
+    const int t = 32 * (w - a.nslice) + lane;
     const bool body = t < a.n && !a.fixed[t];
     for (int k = 0; k < K; ++k) {
       XSum r;
@@ -98,57 +150,6 @@ __global__ void __launch_bounds__(256) k_ls_bounds(LsArgs a) {
         for (int i = 0; i < kXD; ++i)
           if (r.d[i]) atomicAdd((unsigned long long*)&d[i], (unsigned long long)r.d[i]);
         if (r.flags) atomicOr((unsigned long long*)&d[kXD], (unsigned long long)r.flags);
-      }
-    }
-  }
-  const bool live = t < a.V;
-  const int b = live ? a.vbody[t] : -1;
-  double r0 = 0.0, r1 = 0.0, r2 = 0.0, q[12], dq[12];
-  if (live) {
-    r0 = a.x0[3 * t];
-    r1 = a.x0[3 * t + 1];
-    r2 = a.x0[3 * t + 2];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) q[i] = a.A[9 * b + i];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) q[9 + i] = a.p[3 * b + i];
-#pragma unroll
-    for (int i = 0; i < 12; ++i) dq[i] = a.dq[12 * b + i];
-  }
-  const unsigned livemask = __ballot_sync(0xffffffffu, live);
-  for (int k = 0; k < K; ++k) {
-    const double al = a.dpar[kParAlpha + k];
-    unsigned long long key[6];
-    if (live) {
-      // dofs_at and xform with the DOFs held in registers
-      double M[12];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) M[9 + i] = q[9 + i] - dq[i] * al;
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) M[3 * r + i] = q[3 * r + i] - dq[3 * (r + 1) + i] * al;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const double c = xform(M, r0, r1, r2, j);
-        key[j] = max_key(-c);
-        key[3 + j] = max_key(c);
-      }
-    }
-    // one round per distinct body in the warp (bodies are contiguous)
-    unsigned pending = livemask;
-    while (pending) {
-      const int lead = __ffs(pending) - 1;
-      const int bl = __shfl_sync(0xffffffffu, b, lead);
-      const unsigned seg = __ballot_sync(0xffffffffu, live && b == bl);
-      pending &= ~seg;
-      if (live && b == bl) {
-        unsigned long long* kb = a.bnd + 6 * ((size_t)k * a.n + bl);
-#pragma unroll
-        for (int i = 0; i < 6; ++i) {
-          const unsigned long long m = seg_max_key(seg, key[i]);
-          if (lane == lead) atomicMax(&kb[i], m);
-        }
       }
     }
   }
@@ -271,10 +272,12 @@ cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const dou
   a.cap_ecand = s.cap_ecand;
   a.dstat = s.dstat;
   a.energy = s.box->ls_energy;
+  a.nslice = s.nslice;
+  a.slice = s.slice;
   cudaError_t e = cudaMemsetAsync(a.energy, 0, sizeof(XSum) * kLsMax, s.stream);
   if (e != cudaSuccess) return e;
-  const int t = s.V > s.n ? s.V : s.n;
-  k_ls_bounds<<<blocks(t, 256), 256, 0, s.stream>>>(a);
+  const long long warps = (long long)s.nslice + (s.n + 31) / 32;
+  k_ls_bounds<<<blocks(32 * warps, 256), 256, 0, s.stream>>>(a);
   k_ls_boxes<<<blocks((long long)kLsMax * s.n, 256), 256, 0, s.stream>>>(a);
   const int G = kRedBlocks;
   const int Gv = (s.prm.ground_enabled && s.prm.enable_vg) ? kRedBlocks : 0;

@@ -389,79 +389,83 @@ __global__ void k_contact_scatter(int cap_contacts, const int4* __restrict__ in,
   out[pair_cand[4 * c.x] + atomicAdd(&pair_cand[4 * c.x + 2], 1)] = c;
 }
 
-// One CTA per body pair: every active contact of the pair (pt_ipc.py:111-190,
+// CTAs loop over the body pairs: every active contact of a pair (pt_ipc.py:111-190,
 // ee_ipc.py:381-430) as 5 rank-one terms, one warp per contact; its 456 values (H_IJ, the
 // contributions to H_II and H_JJ, and to g_I, g_J; put.py:25-66) are added exactly.
 __global__ void __launch_bounds__(NT) k_pair_assemble(NarrowArgs a) {
-  const int p = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (p >= a.dstat[DS_NPAIRS] || (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW))) return;
-  const int cnt = a.pair_cand[4 * p + 1], off = a.pair_cand[4 * p];
-  if (tid == 0) {
-    a.pair_active[p] = cnt;
-    if (cnt) atomicAdd(&a.dstat[DS_ACTIVE], cnt);
-  }
-  if (cnt == 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
+  const int npairs = a.dstat[DS_NPAIRS];
   __shared__ double ush[NW][5][24];
   extern __shared__ XSum xred[];  // [NOUT]
-  for (int e = tid; e < NOUT * (kXD + 1); e += NT) reinterpret_cast<long long*>(xred)[e] = 0;
-  __syncthreads();
-  for (int ci = warp; ci < cnt; ci += NW) {
-    const int4 rec = a.contacts_by_pair[off + ci];
-    const int type = rec.y & 1, swap = rec.y >> 1;
-    int ids[4];
-    cand_vertices(a, type, rec.z, rec.w, ids);
-    d3 xs[4];
-    fetch(a.y0, ids, xs);
-    Geo G;
-    double d2;
-    contact_active(type, xs, a.prm, &G, &d2);
-    ContactScalars C;
-    contact_scalars(type, G, d2, a.prm, C);
-    if (lane < 24) {
-      const int side = lane / 12, m = (lane % 12) / 3, comp = lane % 3;
-      const int group = side ^ swap;  // vertex group whose body is this side
-      const int v0 = type == 0 ? (group ? 1 : 0) : (group ? 2 : 0);
-      const int v1 = type == 0 ? (group ? 4 : 1) : (group ? 4 : 2);
-      double dw[3];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        double sacc = 0.0;
-        for (int v = v0; v < v1; ++v) {
-          const double w = m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]);
-          sacc += C.D[i][v] * w;
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {  // pairs, grid-stride
+    const int cnt = a.pair_cand[4 * p + 1], off = a.pair_cand[4 * p];
+    if (tid == 0) {
+      a.pair_active[p] = cnt;
+      if (cnt) atomicAdd(&a.dstat[DS_ACTIVE], cnt);
+    }
+    if (cnt == 0) continue;
+    __syncthreads();  // the previous pair's results are read out of xred
+    for (int e = tid; e < NOUT * (kXD + 1); e += NT) reinterpret_cast<long long*>(xred)[e] = 0;
+    __syncthreads();
+    for (int ci = warp; ci < cnt; ci += NW) {
+      const int4 rec = a.contacts_by_pair[off + ci];
+      const int type = rec.y & 1, swap = rec.y >> 1;
+      int ids[4];
+      cand_vertices(a, type, rec.z, rec.w, ids);
+      d3 xs[4];
+      fetch(a.y0, ids, xs);
+      Geo G;
+      double d2;
+      contact_active(type, xs, a.prm, &G, &d2);
+      ContactScalars C;
+      contact_scalars(type, G, d2, a.prm, C);
+      if (lane < 24) {
+        const int side = lane / 12, m = (lane % 12) / 3, comp = lane % 3;
+        const int group = side ^ swap;  // vertex group whose body is this side
+        const int v0 = type == 0 ? (group ? 1 : 0) : (group ? 2 : 0);
+        const int v1 = type == 0 ? (group ? 4 : 1) : (group ? 4 : 2);
+        double dw[3];
+  #pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          double sacc = 0.0;
+          for (int v = v0; v < v1; ++v) {
+            const double w = m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]);
+            sacc += C.D[i][v] * w;
+          }
+          dw[i] = sacc;
         }
-        dw[i] = sacc;
+  #pragma unroll
+        for (int k = 0; k < 5; ++k)
+          ush[warp][k][lane] = dw[0] * C.q[k][comp] + dw[1] * C.q[k][3 + comp] + dw[2] * C.q[k][6 + comp];
       }
-#pragma unroll
-      for (int k = 0; k < 5; ++k)
-        ush[warp][k][lane] = dw[0] * C.q[k][comp] + dw[1] * C.q[k][3 + comp] + dw[2] * C.q[k][6 + comp];
+      __syncwarp();
+      for (int e = lane; e < NOUT; e += 32) {
+        double v = 0.0;
+        if (e < 432) {
+          const int blk = e / 144, r = (e % 144) / 12, cidx = e % 12;
+          const int ra = blk == 2 ? 12 + r : r;
+          const int cb = blk == 1 ? cidx : 12 + cidx;
+  #pragma unroll
+          for (int k = 0; k < 5; ++k) v += C.coef[k] * (ush[warp][k][ra] * ush[warp][k][cb]);
+        } else {
+          v = C.gscale * ush[warp][4][e - 432];
+        }
+        xs_add_atomic(&xred[e], v);
+      }
+      __syncwarp();
     }
-    __syncwarp();
-    for (int e = lane; e < NOUT; e += 32) {
-      double v = 0.0;
-      if (e < 432) {
-        const int blk = e / 144, r = (e % 144) / 12, cidx = e % 12;
-        const int ra = blk == 2 ? 12 + r : r;
-        const int cb = blk == 1 ? cidx : 12 + cidx;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) v += C.coef[k] * (ush[warp][k][ra] * ush[warp][k][cb]);
+    __syncthreads();
+    for (int e = tid; e < NOUT; e += NT) {
+      const double v = xs_round(xred[e]);
+      if (e < 144) {
+        a.offdiag[(size_t)p * 288 + e] = v;
+        a.offdiag[(size_t)p * 288 + 144 + (e % 12) * 12 + e / 12] = v;
+      } else if (e < 432) {
+        a.pdiag[(size_t)p * 288 + (e - 144)] = v;
       } else {
-        v = C.gscale * ush[warp][4][e - 432];
+        a.pgrad[(size_t)p * 24 + (e - 432)] = v;
       }
-      xs_add_atomic(&xred[e], v);
-    }
-    __syncwarp();
-  }
-  __syncthreads();
-  for (int e = tid; e < NOUT; e += NT) {
-    const double v = xs_round(xred[e]);
-    if (e < 144) {
-      a.offdiag[(size_t)p * 288 + e] = v;
-      a.offdiag[(size_t)p * 288 + 144 + (e % 12) * 12 + e / 12] = v;
-    } else if (e < 432) {
-      a.pdiag[(size_t)p * 288 + (e - 144)] = v;
-    } else {
-      a.pgrad[(size_t)p * 24 + (e - 432)] = v;
     }
   }
 }
@@ -1155,7 +1159,7 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
                                                                            s.contacts_by_pair, s.dstat);
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
       static_assert(smem + 4096 <= 48 * 1024, "pair assembly shared memory");
-      k_pair_assemble<<<s.cap_pairs, NT, smem, s.stream>>>(a);
+      k_pair_assemble<<<s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148, NT, smem, s.stream>>>(a);
       s.launches += 3;
     }
   } else {

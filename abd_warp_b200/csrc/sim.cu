@@ -618,6 +618,12 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
       }
     }
     ok(upload(&s.body_rest, brest.data(), brest.size(), s.stream));
+    std::vector<int4> slices;
+    for (int b = 0; b < n; ++b)
+      for (int v = d->vert_off[b]; v < d->vert_off[b + 1]; v += abd::kSlice)
+        slices.push_back(make_int4(b, v, std::min(abd::kSlice, d->vert_off[b + 1] - v), 0));
+    s.nslice = (int)slices.size();
+    ok(upload(&s.slice, slices.data(), slices.size(), s.stream));
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
     ok(upload(&s.chunk_box, cbox.data(), cbox.size(), s.stream));
     ok(upload(&s.vperm, vperm.data(), vperm.size(), s.stream));
@@ -713,7 +719,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
-                  s.body_sup, s.ls_bnd, s.ls_box};
+                  s.body_sup, s.ls_bnd, s.ls_box, s.slice};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_ls})
