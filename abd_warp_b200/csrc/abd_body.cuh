@@ -103,17 +103,22 @@ __device__ inline Box edge_box_at(const d3& a, const d3& b, double dhh) {
   return B;
 }
 
-// Vertex-ground culling (culling.py:64-82): the vertex's body box bb reaches below
-// ground + dhat / 2 and the vertex's box q overlaps the half space under the plane.
-__device__ inline bool vg_box_test(const abd_params& P, const Box& bb, const Box& q) {
-  if (!((double)bb.lo[1] < 0.5 * P.dhat + P.ground)) return false;
+// the box of the vertex-ground culling's half space under the plane (culling.py:64-82)
+__device__ inline Box ground_box(const abd_params& P) {
   Box g;
   g.lo[0] = g.lo[1] = g.lo[2] = -1e3f;
   g.hi[0] = 1e3f;
   g.hi[1] = (float)P.ground;
   g.hi[2] = 1e3f;
   g.pad0 = g.pad1 = 0.f;
-  return overlap(q, g);
+  return g;
+}
+
+// Vertex-ground culling (culling.py:64-82): the vertex's body box bb reaches below
+// ground + dhat / 2 and the vertex's box q overlaps the half space under the plane.
+__device__ inline bool vg_box_test(const abd_params& P, const Box& bb, const Box& q) {
+  if (!((double)bb.lo[1] < 0.5 * P.dhat + P.ground)) return false;
+  return overlap(q, ground_box(P));
 }
 
 // Conservative world box of a rest-frame box R of a body moving by x = A^T r + p.  Centre

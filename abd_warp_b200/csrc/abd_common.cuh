@@ -285,8 +285,6 @@ struct Sim {
   // culled set at some DOFs between its two sets (type, primitive a, primitive b)
   int cap_ecand = 0;
   int4* ecand = nullptr;
-  unsigned long long* ls_bnd = nullptr;  // [kLsMax][n][6] body bounds of the trials (max-keys)
-  Box* ls_box = nullptr;                 // [kLsMax][n] body boxes of the trials
   int list_counts[4] = {0, 0, 0, 0};  // pairs, PT, EE, VG of the last list culling
   double* pair_val = nullptr;      // [cap_pairs] energy or toi per pair
 

@@ -650,8 +650,6 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   }
   ok(dalloc(&s.dpar, abd::kNPar));
   ok(dalloc(&s.body_sup, n));
-  ok(dalloc(&s.ls_bnd, 6 * (size_t)abd::kLsMax * n));
-  ok(dalloc(&s.ls_box, (size_t)abd::kLsMax * n));
   ok(dalloc(&s.dint, 4));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream2, cudaStreamNonBlocking);
@@ -672,7 +670,6 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.kcount, 0, 4 * sizeof(int), s.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s.ls_bnd, 0, sizeof(unsigned long long) * 6 * abd::kLsMax * n, s.stream);
   if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, ...}
     for (int k = 0; k < abd::kNPar; ++k) s.hpar[k] = 0.0;
     s.hpar[1] = 1.0;
@@ -719,7 +716,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
-                  s.body_sup, s.ls_bnd, s.ls_box, s.slice};
+                  s.body_sup, s.slice};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_ls})

@@ -139,12 +139,15 @@ def make_config(index: int, seed: int | None = None):
 
 
 def small_pile(n_side: int = 2, layers: int = 2, seed: int = 7, level: int = 1,
-               radius: float = 0.2):
+               radius: float = 0.2, plane: bool = False):
     """A small mixed pile for fast parity tests: cubes and icospheres on a grid above
-    the ground box."""
+    the ground box, or, with plane, above the vertex-ground plane y = 0 (no ground body)."""
     prm = SimParams()
     rng = np.random.default_rng(seed)
-    bodies = [ground_box()]
+    bodies = [] if plane else [ground_box()]
+    if plane:
+        prm.ground_enabled = True
+        prm.ground = 0.0
     sp = 2.2 * radius + 0.05
     y0 = radius * 1.8 + 2 * prm.dhat
     t = 0

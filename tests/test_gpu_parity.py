@@ -53,6 +53,7 @@ SCENES = {
     "c0_contact": lambda: (scenes.make_config(0)[0], SimParams(), 3),
     "pile_ground": lambda: (scenes.small_pile(2, 2, seed=7)[0], SimParams(), 30),
     "c1_start": lambda: (scenes.make_config(1)[0], SimParams(), 0),
+    "pile_plane": lambda: (*scenes.small_pile(2, 2, seed=7, plane=True), 30),
 }
 
 
@@ -94,7 +95,7 @@ def test_culling_sets_bitexact(scene_state, swept):
     for k in ("pt", "ee", "vg"):
         np.testing.assert_array_equal(_sorted_rows(got[k]), _sorted_rows(ref[k]), err_msg=f"{name} {k}")
     if name != "c1_start":
-        assert len(ref["pt"]) + len(ref["ee"]) > 0
+        assert len(ref["pt"]) + len(ref["ee"]) + len(ref["vg"]) > 0
 
 
 @pytest.mark.parametrize("swept", [False, True])
@@ -209,15 +210,16 @@ def test_solve(scene_state, solver):
         o.set_params(prm0)
 
 
-@pytest.mark.parametrize("case,nsteps", [("c0", 200), ("pile", 60)])
+@pytest.mark.parametrize("case,nsteps", [("c0", 200), ("pile", 60), ("plane", 60)])
 def test_step_parity(case, nsteps):
     """Whole time steps against the oracle, bit for bit: positions, velocities, the dq warm
     start and every iteration count, at every step (c0: the two-cube configuration for its
-    200 steps; pile: 8 bodies on the ground box, 60 steps through landing and contact)."""
+    200 steps; pile: 8 bodies on the ground box, 60 steps through landing and contact;
+    plane: the same bodies landing on the vertex-ground plane)."""
     if case == "c0":
         bodies, prm, _ = scenes.make_config(0)
     else:
-        bodies, prm = scenes.small_pile(2, 2, seed=7)
+        bodies, prm = scenes.small_pile(2, 2, seed=7, plane=case == "plane")
     o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
     sim = _sim(bodies, prm)
     active = 0
