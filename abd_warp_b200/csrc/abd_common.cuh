@@ -31,6 +31,7 @@ enum : int {
 };
 
 constexpr int kTraversalStack = 64;
+constexpr int kNoChild = (int)0x80000000;  // unused slot of a node's child table
 
 // ---------------------------------------------------------------------------------------
 // small vector helpers (FP64)
@@ -162,11 +163,13 @@ struct Tree {
   // by the affine image of its rest box, which the traversal computes from the body's DOFs
   // instead of a refit
   Box* rest = nullptr;
-  // per internal node, its two children as the traversal needs them, so that one visit is one
-  // round of independent loads: the children's rest boxes [N-1][2] and their codes [N-1]
-  // (the child's node id if internal, ~primitive if a leaf)
+  // per internal node, its up to four descendants one or two levels down (its children that
+  // are leaves and the children of its internal children) as the traversal needs them, so
+  // that one visit is one round of independent loads and the walk is half as deep: their
+  // rest boxes [N-1][4] and codes [N-1] (node id if internal, ~primitive if a leaf,
+  // kNoChild for an unused slot)
   Box* crest = nullptr;
-  int2* ccode = nullptr;
+  int4* ccode = nullptr;
   // per-body bottom-up refit schedule: the internal nodes of body b's subtree grouped by
   // height, order[lvl[body_lvl[b] + h - 1] .. lvl[body_lvl[b] + h]) for h = 1..heights
   int* order = nullptr;       // [N-1]
@@ -395,8 +398,9 @@ struct Dofs {
 // affine images of their rest boxes.  Without (d0 == null): y0 / y1 are given positions, the
 // leaf boxes are stored and the body subtrees refit level by level.
 cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, double* y1);
+// (dhh: the edge dilation, default dhat / 2)
 cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A1, const double* p1, double* y0,
-                       double* y1);
+                       double* y1, double dhh = -1.0);
 // body pairs: full (mask, scan, fill: the sorted pair list and the adjacency with pair
 // indices) or mask only (row counts and the bit matrix, all the energy and CCD passes need)
 // sup: cull with the boxes over every DOF set between the two of a swept pass (body_sup)

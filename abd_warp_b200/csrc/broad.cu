@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(BB) k_body_broad(BroadArgs a) {
 }  // namespace
 
 cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A1, const double* p1, double* y0,
-                       double* y1) {
+                       double* y1, double dhh) {
   BroadArgs a;
   a.n = s.n;
   a.V = s.V;
@@ -459,7 +459,7 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
   a.p1 = p1;
   a.y0 = y0;
   a.y1 = y1;
-  a.dhh = s.prm.dhat * 0.5;
+  a.dhh = dhh >= 0.0 ? dhh : s.prm.dhat * 0.5;
   a.bnd = s.body_bnd;
   a.tri_leaf = s.tri_tree.prim_leaf;
   a.edge_leaf = s.edge_tree.prim_leaf;
@@ -511,33 +511,45 @@ cudaError_t body_broad(Sim& s, const Dofs* d0, const Dofs* d1, double* y0, doubl
   return cudaGetLastError();
 }
 
-// child tables of the traversal (one thread per internal node)
+// child tables of the traversal (one thread per internal node): the node's children that
+// are leaves and the children of its internal children, up to four
 __global__ void k_child_tables(int N, const int* child, const int* leaf_prim, const Box* rest, Box* crest,
-                               int2* ccode) {
+                               int4* ccode) {
   const int node = blockIdx.x * blockDim.x + threadIdx.x;
   if (node >= N - 1) return;
-  int code[2];
-#pragma unroll
+  const int L0 = N - 1;
+  int code[4] = {kNoChild, kNoChild, kNoChild, kNoChild}, m = 0;
+  Box zero{};
   for (int h = 0; h < 2; ++h) {
     const int c = child[2 * node + h];
-    store_box(&crest[2 * node + h], load_box(&rest[c]));
-    code[h] = c >= N - 1 ? ~leaf_prim[c - (N - 1)] : c;
+    if (c >= L0) {
+      store_box(&crest[4 * node + m], load_box(&rest[c]));
+      code[m++] = ~leaf_prim[c - L0];
+    } else {
+      for (int g = 0; g < 2; ++g) {
+        const int cc = child[2 * c + g];
+        store_box(&crest[4 * node + m], load_box(&rest[cc]));
+        code[m++] = cc >= L0 ? ~leaf_prim[cc - L0] : cc;
+      }
+    }
   }
-  ccode[node] = make_int2(code[0], code[1]);
+  for (int i = m; i < 4; ++i) store_box(&crest[4 * node + i], zero);
+  ccode[node] = make_int4(code[0], code[1], code[2], code[3]);
 }
 
-// Rest-frame boxes of all nodes: the leaf boxes and refit of the rest positions, copied aside,
-// and the traversal's child tables.
+// Rest-frame boxes of all nodes: the undilated leaf boxes and refit of the rest positions,
+// copied aside, and the traversal's child tables.  (The traversal dilates the boxes' world
+// images by what each kind of primitive box needs.)
 cudaError_t rest_boxes(Sim& s) {
-  cudaError_t e = body_broad(s, nullptr, nullptr, nullptr, nullptr, s.x0, nullptr);
+  cudaError_t e = body_broad(s, nullptr, nullptr, nullptr, nullptr, s.x0, nullptr, 0.0);
   for (Tree* t : {&s.tri_tree, &s.edge_tree})
     if (e == cudaSuccess && t->N > 0)
       e = cudaMemcpyAsync(t->rest, t->box, sizeof(Box) * (size_t)(2 * t->N - 1), cudaMemcpyDeviceToDevice,
                           s.stream);
   for (Tree* t : {&s.tri_tree, &s.edge_tree})
     if (e == cudaSuccess && t->N > 1) {
-      if ((e = cudaMalloc(&t->crest, sizeof(Box) * 2 * (size_t)(t->N - 1))) != cudaSuccess ||
-          (e = cudaMalloc(&t->ccode, sizeof(int2) * (size_t)(t->N - 1))) != cudaSuccess)
+      if ((e = cudaMalloc(&t->crest, sizeof(Box) * 4 * (size_t)(t->N - 1))) != cudaSuccess ||
+          (e = cudaMalloc(&t->ccode, sizeof(int4) * (size_t)(t->N - 1))) != cudaSuccess)
         break;
       k_child_tables<<<blocks(t->N - 1, 256), 256, 0, s.stream>>>(t->N, t->child, t->leaf_prim, t->rest, t->crest,
                                                                    t->ccode);

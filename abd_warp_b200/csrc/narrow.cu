@@ -103,9 +103,10 @@ struct NodeBoxes {
 };
 
 // Stack traversal of the subtree rooted at `root`; calls f(prim) for every leaf whose box
-// overlaps q, in a fixed depth-first order.  Affine mode reads a popped node's child tables
-// (codes and rest boxes, indexed by the node itself), so a visit costs one round of
-// independent loads; refit mode reads the stored world boxes of the children.
+// overlaps q, in a fixed depth-first order.  A popped node's child table lists its up to four
+// descendants one or two levels down, tested together: the walk is half as deep as the
+// binary tree's, and in affine mode a visit costs one round of independent loads (codes and
+// rest boxes, indexed by the node itself); refit mode reads the stored world boxes.
 // visits: tested internal nodes and leaves (kernel profiling)
 struct Visits {
   unsigned internal = 0, leaf = 0;
@@ -135,15 +136,16 @@ __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int
   stack[sp++] = root;
   while (sp > 0) {
     const int node = stack[--sp];
-    const int2 cc = __ldg(&tr.ccode[node]);
-    Box R[2];
+    const int4 cc = __ldg(&tr.ccode[node]);
+    Box R[4];
     if (nb.m0) {
-      R[0] = load_box(&tr.crest[2 * node]);
-      R[1] = load_box(&tr.crest[2 * node + 1]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h) R[h] = load_box(&tr.crest[4 * node + h]);
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int code = h ? cc.y : cc.x;
+    for (int h = 0; h < 4; ++h) {
+      const int code = h == 0 ? cc.x : h == 1 ? cc.y : h == 2 ? cc.z : cc.w;
+      if (code == kNoChild) continue;
       if (code < 0) {
         const int prim = ~code;
         ++cnt.leaf;
@@ -187,7 +189,7 @@ __device__ inline NodeBoxes node_boxes(const NarrowArgs& a, const Tree* tr, bool
   nb.tr = tr;
   nb.m0 = m;
   nb.m1 = m && a.y1 ? m + 12 : nullptr;
-  nb.pad = __double2float_ru(0.5 * a.prm.dhat);
+  nb.pad = tri ? 0.f : __double2float_ru(0.5 * a.prm.dhat);  // triangle boxes are undilated
   nb.prims = tri ? a.tris : a.edges;
   nb.tri = tri;
   nb.sup = 0;
@@ -842,13 +844,16 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   double val = 0.0;
   // vertex-ground sums, exact: g (4 y-components) and H (4x4 yy-components)
   __shared__ XSum vx[20];
-  const bool vg_on = a.prm.ground_enabled && a.prm.enable_vg && !fixed;
+  const bool vg_any = a.prm.ground_enabled && a.prm.enable_vg, vg_on = vg_any && !fixed;
   for (int e = t; e < 20 * (kXD + 1); e += BT) reinterpret_cast<long long*>(vx)[e] = 0;
   __syncthreads();
-  if (vg_on && t < 128) {
+  if (vg_any && t < 128) {
     const Box bb = load_box(&a.body_box[b]);
+    int cnt = 0;  // the culling's vertex-ground pairs, fixed bodies included (culling.py:54-82)
     for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
       if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
+      ++cnt;
+      if (!vg_on) continue;
       const double d = a.y[3 * v + 1] - a.prm.ground;
       const double d2b = barrier_d2(d * d, a.prm), db = barrier_d1(d * d, a.prm);
       const double th[4] = {1.0, a.x0[3 * v], a.x0[3 * v + 1], a.x0[3 * v + 2]};
@@ -859,6 +864,7 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
         for (int jj = 0; jj < 4; ++jj) xs_add_atomic(&vx[4 + 4 * ii + jj], (((th[ii] * th[jj]) * d2b) * 4.0) * d * d);
       }
     }
+    if (cnt) atomicAdd(&a.dstat[DS_VG_COUNT], cnt);
   }
   __syncthreads();
   if (t >= 156) return;

@@ -933,6 +933,7 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     if (it == 0) {
       inf.n_pt = s.hstat[abd::DS_PT_COUNT];
       inf.n_ee = s.hstat[abd::DS_EE_COUNT];
+      inf.n_vg = s.hstat[abd::DS_VG_COUNT];
       inf.n_ij = s.n_pairs;
     }
     inf.n_active = nact;
@@ -988,7 +989,6 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
   inf.newton_iters = it;
   inf.energy = E0;
   inf.status = take_status(h);
-  inf.n_vg = 0;
   if (info) *info = inf;
   return (inf.status & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
 }

@@ -220,10 +220,10 @@ __global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, int c0, in
       for (int i = threadIdx.x; i < D; i += IT)
         if (i != k) K[(size_t)i * D + k] = 0.0;
       __syncthreads();
-      for (int e = threadIdx.x; e < D * D; e += IT) {
-        const int i = e / D, j = e % D;
+      for (int i = (int)(threadIdx.x >> 5); i < D; i += IT / 32) {  // a warp per row
         const double fi = f[i];
-        if (i != k && fi != 0.0) K[e] -= fi * K[(size_t)k * D + j];
+        if (i == k || fi == 0.0) continue;
+        for (int j = (int)(threadIdx.x & 31); j < D; j += 32) K[(size_t)i * D + j] -= fi * K[(size_t)k * D + j];
       }
       __syncthreads();
     }

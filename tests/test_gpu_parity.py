@@ -228,7 +228,7 @@ def test_step_parity(case, nsteps):
             ri = o.step()
             gi = sim.step()
             assert gi["status"] == 0, (s, gi)
-            for k in ("newton_iters", "linear_iters", "ls_trials", "n_active"):
+            for k in ("newton_iters", "linear_iters", "ls_trials", "n_active", "n_pt", "n_ee", "n_vg", "n_ij"):
                 assert gi[k] == ri[k], (s, k, gi, ri)
             assert gi["energy"] == ri["energy"], (s, gi["energy"], ri["energy"])
             st = o.get_state()
