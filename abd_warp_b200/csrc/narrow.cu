@@ -21,6 +21,8 @@
 
 #include <climits>
 
+#include <cooperative_groups.h>
+
 #include "abd_body.cuh"
 #include "abd_geometry.cuh"
 
@@ -53,6 +55,7 @@ struct NarrowArgs {
   int cap_ccd;
   int4* ccd_cand;
   const Box* body_sup;          // CCD_LS: body boxes over every DOF set between the two
+  const int* vbody;
   int cap_ecand;
   int4* ecand;                  // CCD_LS: line-search candidates
   int cap_contacts;
@@ -217,6 +220,15 @@ __device__ inline void visit_item(const NarrowArgs& a, const PairInfo& P, int k,
     traverse(node_boxes(a, &a.edge, false, P.dof ? P.dof + 24 : nullptr), __ldg(&a.edge.body_root[P.J]), q,
              a.dstat, [&](int eb) { f(1, 0, e, eb); });
   }
+}
+
+// A slot of an append-only list: one atomic per group of lanes that append together.
+__device__ inline int append_slot(int* counter) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+  return g.shfl(base, 0) + (int)g.thread_rank();
 }
 
 // global vertex ids of a candidate: PT (point v, triangle t), EE (edge a, edge b)
@@ -394,11 +406,13 @@ __global__ void k_contact_scatter(int cap_contacts, const int4* __restrict__ in,
 // CTAs loop over the body pairs: every active contact of a pair (pt_ipc.py:111-190,
 // ee_ipc.py:381-430) as 5 rank-one terms, one warp per contact; its 456 values (H_IJ, the
 // contributions to H_II and H_JJ, and to g_I, g_J; put.py:25-66) are added exactly.
-__global__ void __launch_bounds__(NT) k_pair_assemble(NarrowArgs a) {
+constexpr int PT_THREADS = 256;  // threads of the pair assembly (a warp per contact)
+constexpr int PT_WARPS = PT_THREADS / 32;
+__global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
   const int npairs = a.dstat[DS_NPAIRS];
-  __shared__ double ush[NW][5][24];
+  __shared__ double ush[PT_WARPS][5][24];
   extern __shared__ XSum xred[];  // [NOUT]
   for (int p = blockIdx.x; p < npairs; p += gridDim.x) {  // pairs, grid-stride
     const int cnt = a.pair_cand[4 * p + 1], off = a.pair_cand[4 * p];
@@ -408,9 +422,9 @@ __global__ void __launch_bounds__(NT) k_pair_assemble(NarrowArgs a) {
     }
     if (cnt == 0) continue;
     __syncthreads();  // the previous pair's results are read out of xred
-    for (int e = tid; e < NOUT * (kXD + 1); e += NT) reinterpret_cast<long long*>(xred)[e] = 0;
+    for (int e = tid; e < NOUT * (kXD + 1); e += PT_THREADS) reinterpret_cast<long long*>(xred)[e] = 0;
     __syncthreads();
-    for (int ci = warp; ci < cnt; ci += NW) {
+    for (int ci = warp; ci < cnt; ci += PT_WARPS) {
       const int4 rec = a.contacts_by_pair[off + ci];
       const int type = rec.y & 1, swap = rec.y >> 1;
       int ids[4];
@@ -458,7 +472,7 @@ __global__ void __launch_bounds__(NT) k_pair_assemble(NarrowArgs a) {
       __syncwarp();
     }
     __syncthreads();
-    for (int e = tid; e < NOUT; e += NT) {
+    for (int e = tid; e < NOUT; e += PT_THREADS) {
       const double v = xs_round(xred[e]);
       if (e < 144) {
         a.offdiag[(size_t)p * 288 + e] = v;
@@ -554,7 +568,6 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   __shared__ Box qbox[CT];
   __shared__ Box qsup[ls ? CT : 1];  // CCD_LS: query boxes over the DOF range
   __shared__ int qprim[CT];  // point id, ~edge id, or kNoQuery (primitive kind disabled)
-  __shared__ int nccd[ls ? NBB : 1];  // CCD_LS: the body pair passes the CCD pass's body boxes
   __shared__ Box nbox[NBB];
   __shared__ __align__(16) float ndof[NBB][24];
   __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB], nrel[NBB];
@@ -582,7 +595,6 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
     for (int e = tid; e < kXD + 1; e += CT) reinterpret_cast<long long*>(&xe)[e] = 0;
   }
   __syncthreads();
-  int cpt = 0, cee = 0;  // GH: candidates found by this thread
   unsigned pf_node = 0, pf_tri = 0, pf_edge = 0;  // profiling: tree nodes and leaves tested
   // the body's own terms, in its first chunk (GH: the body kernel adds them)
   if (!gh && ch.y == 0) {
@@ -622,7 +634,6 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       const int J = gh ? a.adj_col[r0 + k] : (k < kNbList ? a.nbr[(size_t)I * kNbList + k] : kth_neighbour(a, I, k));
       nJ[tid] = J;
       nbox[tid] = load_box(&(ls ? a.body_sup : a.body_box)[J]);
-      if constexpr (ls) nccd[tid] = overlap(load_box(&a.body_box[I]), load_box(&a.body_box[J])) ? 1 : 0;
       rel = overlap(cbx, nbox[tid]) ? 1 : 0;
       nrel[tid] = rel;
       ntri[tid] = a.tri.body_root[J];
@@ -684,39 +695,28 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
         const int q = work[k] & 0xff, j = work[k] >> 8;
         const int qp = qprim[q];
         const Box qb = ls ? qsup[q] : qbox[q];
-        // ex: the pair passes the CCD pass's own boxes (CCD_LS)
-        auto visit = [&](int type, int pa, int pb, bool ex) {
-          int ids[4];
-          d3 xs[4];
-          if constexpr (!ccd) {
+        auto visit = [&](int type, int pa, int pb) {
+          if constexpr (gh) {
+            // evaluated by k_gh_eval, one thread per candidate.  PT: the point is I's, the
+            // pair's first body is min(I, J); EE: the lower body's edge comes first
+            const int swap = (type == 0 && I > nJ[j]) ? 1 : 0;
+            const int pos = append_slot(&a.dstat[DS_NCCD]);
+            if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(npair[j], type | (swap << 1), pa, pb);
+            else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+          } else if constexpr (ls) {
+            // line-search candidates; k_ccd_eval takes those that pass the CCD pass's boxes
+            const int pos = append_slot(&a.dstat[DS_NECAND]);
+            if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
+            else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
+          } else if constexpr (ccd) {  // evaluated by k_ccd_eval, one thread per candidate
+            const int pos = append_slot(&a.dstat[DS_NCCD]);
+            if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
+            else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+          } else {
+            int ids[4];
+            d3 xs[4];
             cand_vertices(a, type, pa, pb, ids);
             fetch(a.y0, ids, xs);
-          }
-          if constexpr (gh) {
-            if (type == 0) ++cpt;
-            else ++cee;
-            Geo G;
-            double d2;
-            if (contact_active(type, xs, a.prm, &G, &d2)) {
-              // PT: the point is I's, the pair's first body is min(I, J); EE: lower body first
-              const int pr = npair[j], swap = (type == 0 && I > nJ[j]) ? 1 : 0;
-              const int pos = atomicAdd(&a.dstat[DS_NCONTACT], 1);
-              if (pos < a.cap_contacts) a.contacts[pos] = make_int4(pr, type | (swap << 1), pa, pb);
-              else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
-              atomicAdd(&a.pair_cand[4 * pr + 1], 1);
-            }
-          } else if constexpr (ccd) {
-            if constexpr (ls) {
-              const int pos = atomicAdd(&a.dstat[DS_NECAND], 1);
-              if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
-              else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
-            }
-            if (ex) {  // evaluated by k_ccd_eval, one thread per candidate
-              const int pos = atomicAdd(&a.dstat[DS_NCCD], 1);
-              if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
-              else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
-            }
-          } else {
             const double e = contact_energy(type, xs, a.prm);
             if (e != 0.0) xs_add_atomic(&xe, e);
           }
@@ -725,11 +725,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
           Visits vc;
           NodeBoxes nbt = node_boxes(a, &a.tri, true, ndof[j]);
           nbt.sup = ls;
-          traverse(nbt, ntri[j], qb, a.dstat, [&](int t) {
-            bool ex = true;
-            if constexpr (ls) ex = nccd[j] && overlap(tri_leaf_box(a.tris, a.y0, a.y1, t), qbox[q]);
-            visit(0, qp, t, ex);
-          }, vc);
+          traverse(nbt, ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); }, vc);
           pf_node += vc.internal;
           pf_tri += vc.leaf;
         } else {
@@ -738,11 +734,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
           Visits vc;
           NodeBoxes nbe = node_boxes(a, &a.edge, false, ndof[j]);
           nbe.sup = ls;
-          traverse(nbe, nedge[j], qb, a.dstat, [&](int e) {
-            bool ex = true;
-            if constexpr (ls) ex = nccd[j] && overlap(edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat), qbox[q]);
-            lower ? visit(1, ~qp, e, ex) : visit(1, e, ~qp, ex);
-          }, vc);
+          traverse(nbe, nedge[j], qb, a.dstat, [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); }, vc);
           pf_node += vc.internal;
           pf_edge += vc.leaf;
         }
@@ -750,18 +742,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       __syncthreads();
     }
   }
-  if constexpr (gh) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      cpt += __shfl_xor_sync(0xffffffffu, cpt, o);
-      cee += __shfl_xor_sync(0xffffffffu, cee, o);
-    }
-    if ((tid & 31) == 0) {
-      if (cpt) atomicAdd(&a.dstat[DS_PT_COUNT], cpt);
-      if (cee) atomicAdd(&a.dstat[DS_EE_COUNT], cee);
-    }
-    return;
-  }
+  if constexpr (gh) return;
   if (MODE == NARROW_ENERGY && a.prof) {  // kernel profiling: the data this chunk read
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -792,18 +773,69 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
 }
 
 // Times of impact of the CCD candidates, one thread per candidate (ccd.py:20-40, 133-186);
-// the minimum below 1 goes to the mailbox key
+// the minimum below 1 goes to the mailbox key.  LS: the candidates are the line-search
+// candidates of a CCD_LS pass, and each is first put to the CCD pass's own culling
+// predicate: the exact swept body boxes overlap and the two swept primitive boxes overlap.
+template <bool LS>
 __global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= min(a.dstat[DS_NCCD], a.cap_ccd) || (a.dstat[DS_STATUS] & ST_CCD_OVERFLOW)) return;
-  const int4 c = a.ccd_cand[k];
-  int ids[4];
-  cand_vertices(a, c.x, c.y, c.z, ids);
-  d3 x0[4], x1[4];
-  fetch(a.y0, ids, x0);
-  fetch(a.y1, ids, x1);
-  const double t = collision_time(c.x, x0, x1);
-  if (t < 1.0) toi_min(a.toi_key, t);
+  const int n = LS ? min(a.dstat[DS_NECAND], a.cap_ecand) : min(a.dstat[DS_NCCD], a.cap_ccd);
+  if (a.dstat[DS_STATUS] & (LS ? ST_ECAND_OVERFLOW : ST_CCD_OVERFLOW)) return;
+  const int4* cand = LS ? a.ecand : a.ccd_cand;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int4 c = cand[k];
+    int ids[4];
+    cand_vertices(a, c.x, c.y, c.z, ids);
+    if (LS) {
+      const int bA = __ldg(&a.vbody[ids[0]]), bB = __ldg(&a.vbody[ids[c.x == 0 ? 1 : 2]]);
+      if (!overlap(load_box(&a.body_box[bA]), load_box(&a.body_box[bB]))) continue;
+      const double dhh = 0.5 * a.prm.dhat;
+      const bool hit = c.x == 0 ? overlap(point_box(a.y0, a.y1, c.y, (float)a.prm.dhat), tri_leaf_box(a.tris, a.y0, a.y1, c.z))
+                                : overlap(edge_leaf_box(a.edges, a.y0, a.y1, c.y, dhh),
+                                          edge_leaf_box(a.edges, a.y0, a.y1, c.z, dhh));
+      if (!hit) continue;
+    }
+    d3 x0[4], x1[4];
+    fetch(a.y0, ids, x0);
+    fetch(a.y1, ids, x1);
+    const double t = collision_time(c.x, x0, x1);
+    if (t < 1.0) toi_min(a.toi_key, t);
+  }
+}
+
+// Contacts of the GH pass's candidates, one thread per candidate: the active ones
+// (pt_ipc.py:13-22, 114; ee_ipc.py:13-23, 382) are appended for the per-pair assembly and
+// counted per pair; the candidates are counted per kind.
+__global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
+  if (a.dstat[DS_STATUS] & (ST_CCD_OVERFLOW | ST_PAIR_OVERFLOW)) return;
+  const int n = min(a.dstat[DS_NCCD], a.cap_ccd);
+  int cpt = 0, cee = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int4 c = a.ccd_cand[k];  // pair, type | swap << 1, primitive a, primitive b
+    const int type = c.y & 1;
+    if (type == 0) ++cpt;
+    else ++cee;
+    int ids[4];
+    d3 xs[4];
+    cand_vertices(a, type, c.z, c.w, ids);
+    fetch(a.y0, ids, xs);
+    Geo G;
+    double d2;
+    if (contact_active(type, xs, a.prm, &G, &d2)) {
+      const int pos = append_slot(&a.dstat[DS_NCONTACT]);
+      if (pos < a.cap_contacts) a.contacts[pos] = c;
+      else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
+      atomicAdd(&a.pair_cand[4 * c.x + 1], 1);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cpt += __shfl_xor_sync(0xffffffffu, cpt, o);
+    cee += __shfl_xor_sync(0xffffffffu, cee, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (cpt) atomicAdd(&a.dstat[DS_PT_COUNT], cpt);
+    if (cee) atomicAdd(&a.dstat[DS_EE_COUNT], cee);
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1062,6 +1094,7 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.cap_ccd = s.cap_ccd;
   a.ccd_cand = s.ccd_cand;
   a.body_sup = s.body_sup;
+  a.vbody = s.vbody;
   a.cap_ecand = s.cap_ecand;
   a.ecand = s.ecand;
   a.cap_contacts = s.cap_contacts;
@@ -1150,22 +1183,26 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if (mode == NARROW_CCD_LS) {
         if (!a.y1) return cudaErrorInvalidValue;
         k_chunk_narrow<NARROW_CCD_LS><<<s.nch, CT, 0, s.stream>>>(a);
+        k_ccd_eval<true><<<kRedBlocks, 128, 0, s.stream>>>(a);
       } else {
         k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+        k_ccd_eval<false><<<kRedBlocks, 128, 0, s.stream>>>(a);
       }
-      k_ccd_eval<<<blocks(s.cap_ccd, 128), 128, 0, s.stream>>>(a);
       ++s.launches;
     } else {
       cudaError_t e = cudaMemsetAsync(s.pair_cand, 0, sizeof(int) * 4 * (size_t)s.cap_pairs, s.stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCONTACT, 0, sizeof(int), s.stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, sizeof(int), s.stream);
       if (e != cudaSuccess) return e;
       k_chunk_narrow<NARROW_GH><<<s.nch, CT, 0, s.stream>>>(a);
+      k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
+      ++s.launches;
       k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
       k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
                                                                            s.contacts_by_pair, s.dstat);
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
-      static_assert(smem + 4096 <= 48 * 1024, "pair assembly shared memory");
-      k_pair_assemble<<<s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148, NT, smem, s.stream>>>(a);
+      static_assert(smem + sizeof(double) * PT_WARPS * 5 * 24 + 256 <= 48 * 1024, "pair assembly shared memory");
+      k_pair_assemble<<<s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148, PT_THREADS, smem, s.stream>>>(a);
       s.launches += 3;
     }
   } else {

@@ -401,6 +401,7 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
       k.add(states_key(s, st)).add(A).add(p).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
       k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
       k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.hact);
+      k.add(s.cap_ccd).add(s.ccd_cand);
       r = abd::run_graph(s, *g, k.h, issue);
     } else {
       r = issue();
