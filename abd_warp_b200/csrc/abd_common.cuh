@@ -256,10 +256,10 @@ struct Sim {
   // captured passes: energy trial, CCD bound, GH, Krylov setup and one block of iterations
   cudaStream_t cap_stream = nullptr;
   cudaStream_t cap_stream2 = nullptr;  // captures the bodies of conditional (loop) nodes
-  GraphSlot g_energy, g_energy_ev, g_ccd, g_gh, g_kinit, g_ls;
+  GraphSlot g_energy, g_ccd, g_ccd_ev, g_gh, g_kinit, g_ls;
   unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
-  // kernel profiling of the energy pass's narrow kernel: CUDA events around it (recorded as
-  // graph nodes), its duration and algorithmic bytes accumulated after every pass
+  // kernel profiling of the line-search candidate pass's narrow kernel: CUDA events around
+  // it (recorded as graph nodes), its duration and algorithmic bytes accumulated per pass
   int prof_on = 0;                 // 0 off, 1 time every kProfEvery-th pass, 2 time and count all
   int prof_events = 0;             // this pass records the events
   long long prof_tick = 0;
@@ -353,22 +353,24 @@ struct Mailbox {
   unsigned long long toi_key;  // complemented bits of the minimum time of impact (0: none)
   double dots[2];              // dq.g, g.g
   XSum ls_energy[kLsMax];      // exact energies of a line-search batch's trials
-  // work counters of the energy pass's narrow kernel (kernel profiling only), spread over
-  // 32 rows against atomic contention: [row][PF_*]
+  // work counters of the line-search candidate pass's narrow kernel (kernel profiling only),
+  // spread over 32 rows against atomic contention: [row][PF_*]
   unsigned long long prof[32][8];
 };
 
-// counters of the energy pass's narrow kernel: the data it reads, per kind of access
+// counters of the line-search candidate pass's narrow kernel (kernel profiling): the data it
+// reads and writes, per kind of access
 enum : int {
-  PF_POINT = 0,      // point queries: FP64 position (24 B)
-  PF_EDGE = 1,       // edge queries: two vertex ids + two positions (56 B)
-  PF_NEIGHBOUR = 2,  // (chunk, neighbour) records: body box, FP32 DOFs, roots (140 B)
-  PF_NODE = 3,       // internal tree nodes tested: rest box + child code (36 B)
-  PF_TRI = 4,        // triangle leaves tested: three ids + three positions (84 B)
-  PF_EDGELEAF = 5,   // edge leaves tested: two ids + two positions (56 B)
-  PF_N = 6
+  PF_POINT = 0,      // point queries: FP64 rest position (24 B)
+  PF_EDGE = 1,       // edge queries: leaf position + rest box (36 B)
+  PF_NEIGHBOUR = 2,  // (chunk, neighbour) records: body box, FP32 DOFs of both sets, roots (140 B)
+  PF_NODE = 3,       // internal tree entries tested: rest box + child code (36 B)
+  PF_TRI = 4,        // triangle leaf entries tested: rest box + code (36 B)
+  PF_EDGELEAF = 5,   // edge leaf entries tested: rest box + code (36 B)
+  PF_CAND = 6,       // candidates appended (16 B written)
+  PF_N = 7
 };
-constexpr double kProfBytes[PF_N] = {24.0, 56.0, 140.0, 36.0, 84.0, 56.0};
+constexpr double kProfBytes[PF_N] = {24.0, 36.0, 140.0, 36.0, 36.0, 36.0, 16.0};
 
 
 // ---------------------------------------------------------------------------------------

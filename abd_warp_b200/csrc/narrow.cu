@@ -80,6 +80,9 @@ struct NarrowArgs {
   int* pair_active;
 };
 
+// start bringing the line at p into L2
+__device__ inline void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Per-CTA view of one body's subtree boxes.  Refit mode (m0 == null): the stored boxes.
 // Affine mode: internal nodes are the affine images of their rest boxes under the body's
 // DOFs at y0 (m0) and, when swept, y1 (m1); leaves are computed from the positions, or, with
@@ -161,8 +164,16 @@ __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int
         ++cnt.internal;
         const Box B = nb.m0 ? affine_box2(R[h], nb.m0, nb.m1, nb.pad) : load_box(&tr.box[code]);
         if (overlap(B, q)) {
-          if (sp < kTraversalStack) stack[sp++] = code;
-          else atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
+          if (sp < kTraversalStack) {
+            stack[sp++] = code;
+            // every pushed node is popped later: start bringing its child table to L2 now
+            if (nb.m0) {
+              prefetch_l2(&tr.ccode[code]);
+              prefetch_l2(&tr.crest[4 * code]);
+            }
+          } else {
+            atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
+          }
         }
       }
     }
@@ -565,8 +576,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   const int nEI = a.eoff[I + 1] - a.eoff[I];
   const int nV = a.voff[I + 1] - a.voff[I];  // items: the body's points, then its edges
   const int Q = max(0, min(CT, nV + nEI - ch.y));
-  __shared__ Box qbox[CT];
-  __shared__ Box qsup[ls ? CT : 1];  // CCD_LS: query boxes over the DOF range
+  __shared__ Box qbox[CT];  // query boxes (CCD_LS: over the DOF range)
   __shared__ int qprim[CT];  // point id, ~edge id, or kNoQuery (primitive kind disabled)
   __shared__ Box nbox[NBB];
   __shared__ __align__(16) float ndof[NBB][24];
@@ -595,7 +605,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
     for (int e = tid; e < kXD + 1; e += CT) reinterpret_cast<long long*>(&xe)[e] = 0;
   }
   __syncthreads();
-  unsigned pf_node = 0, pf_tri = 0, pf_edge = 0;  // profiling: tree nodes and leaves tested
+  unsigned pf_node = 0, pf_tri = 0, pf_edge = 0, pf_cand = 0;  // profiling: entries tested, candidates
   // the body's own terms, in its first chunk (GH: the body kernel adds them)
   if (!gh && ch.y == 0) {
     const Box bb = load_box(&a.body_box[I]);
@@ -650,23 +660,25 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
         if (k < nV) {
           const int v = __ldg(&a.vperm[a.voff[I] + k]);
           qprim[tid] = a.prm.enable_pt ? v : kNoQuery;
-          qbox[tid] = point_box(a.y0, a.y1, v, (float)a.prm.dhat);
-          if constexpr (ls) {
+          if constexpr (ls) {  // the point's box over the DOF range, from its rest position
             Box R;
 #pragma unroll
             for (int d = 0; d < 3; ++d) R.lo[d] = R.hi[d] = (float)__ldg(&a.x0[3 * v + d]);
-            qsup[tid] = affine_box2(R, m, m + 12, __double2float_ru(a.prm.dhat));
+            qbox[tid] = affine_box2(R, m, m + 12, __double2float_ru(a.prm.dhat));
+          } else {
+            qbox[tid] = point_box(a.y0, a.y1, v, (float)a.prm.dhat);
           }
         } else {
           const int e = __ldg(&a.edge.leaf_prim[a.eoff[I] + (k - nV)]);
           qprim[tid] = a.prm.enable_ee ? ~e : kNoQuery;
-          qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
-          if constexpr (ls)
-            qsup[tid] = affine_box2(load_box(&a.edge.rest[(a.edge.N - 1) + a.eoff[I] + (k - nV)]), m, m + 12,
+          if constexpr (ls)  // the edge's box over the DOF range, from its rest box
+            qbox[tid] = affine_box2(load_box(&a.edge.rest[(a.edge.N - 1) + a.eoff[I] + (k - nV)]), m, m + 12,
                                     __double2float_ru(0.5 * a.prm.dhat));
+          else
+            qbox[tid] = edge_leaf_box(a.edges, a.y0, a.y1, e, 0.5 * a.prm.dhat);
         }
       }
-      if constexpr (MODE == NARROW_ENERGY) {
+      if constexpr (ls) {
         if (a.prof && tid == 0) {
           const int qp = max(0, min(Q, nV - ch.y));
           atomicAdd(&a.prof_rows[8 * (blockIdx.x & 31) + PF_POINT], (unsigned long long)qp);
@@ -687,14 +699,14 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       for (int it = w0 + tid; it < min(Q * nb, w0 + CW); it += CT) {
         const int q = it % Q, j = it / Q;
         if (!nrel[j] || qprim[q] == kNoQuery || (qprim[q] < 0 && !nown[j])) continue;
-        if (!overlap(ls ? qsup[q] : qbox[q], nbox[j])) continue;
+        if (!overlap(qbox[q], nbox[j])) continue;
         work[atomicAdd(&nwork, 1)] = (unsigned short)(q | (j << 8));
       }
       __syncthreads();
       for (int k = tid; k < nwork; k += CT) {
         const int q = work[k] & 0xff, j = work[k] >> 8;
         const int qp = qprim[q];
-        const Box qb = ls ? qsup[q] : qbox[q];
+        const Box qb = qbox[q];
         auto visit = [&](int type, int pa, int pb) {
           if constexpr (gh) {
             // evaluated by k_gh_eval, one thread per candidate.  PT: the point is I's, the
@@ -706,6 +718,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
           } else if constexpr (ls) {
             // line-search candidates; k_ccd_eval takes those that pass the CCD pass's boxes
             const int pos = append_slot(&a.dstat[DS_NECAND]);
+            ++pf_cand;
             if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
             else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
           } else if constexpr (ccd) {  // evaluated by k_ccd_eval, one thread per candidate
@@ -743,18 +756,20 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
     }
   }
   if constexpr (gh) return;
-  if (MODE == NARROW_ENERGY && a.prof) {  // kernel profiling: the data this chunk read
+  if (ls && a.prof) {  // kernel profiling: the data this chunk read and wrote
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       pf_node += __shfl_xor_sync(0xffffffffu, pf_node, o);
       pf_tri += __shfl_xor_sync(0xffffffffu, pf_tri, o);
       pf_edge += __shfl_xor_sync(0xffffffffu, pf_edge, o);
+      pf_cand += __shfl_xor_sync(0xffffffffu, pf_cand, o);
     }
     unsigned long long* row = a.prof_rows + 8 * (blockIdx.x & 31);
     if ((tid & 31) == 0) {
       atomicAdd(&row[PF_NODE], (unsigned long long)pf_node);
       atomicAdd(&row[PF_TRI], (unsigned long long)pf_tri);
       atomicAdd(&row[PF_EDGELEAF], (unsigned long long)pf_edge);
+      atomicAdd(&row[PF_CAND], (unsigned long long)pf_cand);
     }
     if (tid == 0 && deg > 0) atomicAdd(&row[PF_NEIGHBOUR], (unsigned long long)deg);
   }
@@ -1170,11 +1185,7 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       return cudaErrorInvalidValue;
     if (s.nch == 0) return cudaSuccess;
     if (mode == NARROW_ENERGY) {
-      if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[0], s.stream, cudaEventRecordExternal))
-        return cudaErrorUnknown;
       k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
-      if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[1], s.stream, cudaEventRecordExternal))
-        return cudaErrorUnknown;
     } else if (mode == NARROW_CCD || mode == NARROW_CCD_LS) {
       // DS_NCCD and DS_NECAND are adjacent
       static_assert(DS_NECAND == DS_NCCD + 1, "candidate counters");
@@ -1182,7 +1193,11 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if (e != cudaSuccess) return e;
       if (mode == NARROW_CCD_LS) {
         if (!a.y1) return cudaErrorInvalidValue;
+        if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[0], s.stream, cudaEventRecordExternal))
+          return cudaErrorUnknown;
         k_chunk_narrow<NARROW_CCD_LS><<<s.nch, CT, 0, s.stream>>>(a);
+        if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[1], s.stream, cudaEventRecordExternal))
+          return cudaErrorUnknown;
         k_ccd_eval<true><<<kRedBlocks, 128, 0, s.stream>>>(a);
       } else {
         k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);

@@ -274,27 +274,14 @@ int energy_of(abd_sim* h, const abd_states& st, const abd::Dofs& d, double* E, a
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
-  // kernel profiling: events around the narrow kernel on every kProfEvery-th trial (mode 1,
-  // their nodes cost a few microseconds) or every pass (mode 2, which also counts bytes)
-  constexpr int kProfEvery = 8;
-  s.prof_events = s.prof_on == 2 || (s.prof_on == 1 && (!g || s.prof_tick++ % kProfEvery == 0));
-  if (g && s.prof_events) g = &s.g_energy_ev;
+  s.prof_events = 0;
   abd::KeyHash k;
-  k.add(key).add(s.prof_on).add(s.prof_events);
+  k.add(key);
   int r = g ? abd::run_graph(s, *g, k.h, issue) : issue();
   if (r) return r;
   CK(cudaStreamSynchronize(s.stream));
   std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
   *E = xs_round_host(s.hbox->energy);
-  if (s.prof_events) {  // the narrow kernel's duration and the data it read
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, s.prof_ev[0], s.prof_ev[1]));
-    s.prof_ms += ms;
-    ++s.prof_launches;
-    if (s.prof_on == 2)
-      for (int row = 0; row < 32; ++row)
-        for (int c = 0; c < abd::PF_N; ++c) s.prof_bytes += abd::kProfBytes[c] * (double)s.hbox->prof[row][c];
-  }
   return ABD_OK;
 }
 
@@ -324,9 +311,16 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
+  // kernel profiling of the line-search candidate pass's narrow kernel: events around it on
+  // every kProfEvery-th pass of the step (mode 1; their graph nodes cost a few microseconds)
+  // or on every pass (mode 2, which also counts its bytes)
+  constexpr int kProfEvery = 4;
+  const bool ls = mode == abd::NARROW_CCD_LS;
+  s.prof_events = ls && (s.prof_on == 2 || (s.prof_on == 1 && (!g || s.prof_tick++ % kProfEvery == 0)));
+  if (g && s.prof_events) g = &s.g_ccd_ev;
   for (int tries = 0;; ++tries) {  // the candidate lists have capacities: grow and rerun
     abd::KeyHash k;
-    k.add(key).add(s.cap_ccd).add(s.ccd_cand).add(mode).add(s.cap_ecand).add(s.ecand);
+    k.add(key).add(s.cap_ccd).add(s.ccd_cand).add(mode).add(s.cap_ecand).add(s.ecand).add(s.prof_on).add(s.prof_events);
     int r = g ? abd::run_graph(s, *g, k.h, issue) : issue();
     if (r) return r;
     CK(cudaStreamSynchronize(s.stream));
@@ -334,6 +328,16 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
     if ((r = overflow(s)) > 0) return r;
     if (r == 0) break;
     if (tries >= kMaxReruns) return ABD_ERR_OVERFLOW;
+  }
+  if (s.prof_events) {  // the narrow kernel's duration and the data it moved
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s.prof_ev[0], s.prof_ev[1]));
+    s.prof_ms += ms;
+    ++s.prof_launches;
+    if (s.prof_on == 2)
+      for (int row = 0; row < 32; ++row)
+        for (int c = 0; c < abd::PF_N; ++c) s.prof_bytes += abd::kProfBytes[c] * (double)s.hbox->prof[row][c];
+    s.prof_events = 0;
   }
   double toi = 1.0;
   if (const unsigned long long key2 = s.hbox->toi_key) {
@@ -720,7 +724,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.body_sup, s.slice};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (abd::GraphSlot* g : {&s.g_energy, &s.g_energy_ev, &s.g_ccd, &s.g_gh, &s.g_kinit, &s.g_ls})
+  for (abd::GraphSlot* g : {&s.g_energy, &s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_kinit, &s.g_ls})
     if (g->exec) cudaGraphExecDestroy(g->exec);
   if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
   if (s.cap_stream2) cudaStreamDestroy(s.cap_stream2);

@@ -296,8 +296,9 @@ class AffineBodySimulator:
         return out
 
     def profile(self, mode: int = 1):
-        """Start (reset) or stop (0) the timing of the energy pass's narrow-phase kernel; mode 2
-        also counts the data it reads (algorithmic bytes), which slows the kernel down."""
+        """Start (reset) or stop (0) the timing of the step's CCD-pass narrow kernel (which also
+        collects the line-search candidates); mode 2 also counts the data it moves (algorithmic
+        bytes), which slows the kernel down."""
         _lib.check(self._L.abd_profile(self._h, int(mode)), "abd_profile")
 
     def profile_read(self):

@@ -12,10 +12,10 @@ value: steps/s on device-resident states.  e2e: the same trajectory again throug
 API with host buffers -- every step copies its inputs (A0, p0, Adot, pdot) from pinned host
 memory and reads the new vertex positions back.
 
-roofline: the energy pass's narrow-phase kernel, the largest share of the step, timed with
-CUDA events around every 8th of its launches inside the timed region; the data it reads
-(algorithmic bytes) is counted by the kernel in a replay of the same (deterministic)
-trajectory, which makes the same launches.
+roofline: the narrow-phase kernel of the CCD pass, which also collects the line-search
+candidates (the largest share of the step), timed with CUDA events around every 4th of its
+launches inside the timed region; the data it moves (algorithmic bytes) is counted by the
+kernel in a replay of the same (deterministic) trajectory, which makes the same launches.
 
 Multi-GPU: the step does not shard (one coupled Newton solve per scene), so N ranks run N
 independent replicas; value = N * K / max-over-ranks time.
@@ -39,10 +39,10 @@ sys.path.insert(0, ROOT)
 METRIC = "ABD steps/s vs plain FP64 on same B200 at \u22641e-6 rel pos err; adjoint grads/s"
 WORKLOAD = "pile of 1024 bodies (512 cubes + 512 level-3 icospheres) on a ground box, 300-step trajectory"
 STATES = os.path.join(ROOT, "tests", "golden", "c2_states.npz")
-# DRAM bytes per launch of the energy narrow kernel (dram__bytes_read.sum + write.sum) from
-# the ncu capture at trajectory step 225 summarised in
-# profiles/k_chunk_narrow_energy_pile1024_state225.md (the contact-rich end of the trajectory)
-NCU_TRAFFIC_PER_LAUNCH = 5.73e6
+# DRAM bytes per launch of the CCD pass's narrow kernel (dram__bytes_read.sum + write.sum)
+# from the ncu capture at trajectory step 225 summarised in
+# profiles/k_chunk_narrow_ccdls_pile1024_state225.md (the contact-rich end of the trajectory)
+NCU_TRAFFIC_PER_LAUNCH = 13.23e6
 
 
 def measured_hbm_peak():
@@ -246,7 +246,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
-    sim.profile(1)  # CUDA events around every 8th launch of the energy narrow kernel
+    sim.profile(1)  # CUDA events around every 4th launch of the CCD pass's narrow kernel
     launches0 = sim.launch_count()
     total_ms = 0.0
     infos = []
@@ -327,7 +327,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clk,
-        "roofline": {"kernel": "k_chunk_narrow<ENERGY> (energy pass narrow phase)", "bound": "hbm",
+        "roofline": {"kernel": "k_chunk_narrow<CCD_LS> (narrow phase of the CCD pass, which also collects "
+                               "the line-search candidates)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": NCU_TRAFFIC_PER_LAUNCH,

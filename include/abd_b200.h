@@ -184,13 +184,13 @@ const char* abd_status_string(int code);
 long long abd_launch_count(const abd_sim* sim);
 
 /* Kernel profiling (no counterpart in the reference; used by the benchmark's roofline).
- * abd_profile(sim, mode) resets the counters; from then on energy passes (line search and
- * compute_energy) record CUDA events around their narrow-phase kernel on the simulator's
- * stream -- every 8th line-search trial in mode 1, every pass in mode 2, which also counts
- * the data the kernel reads (and slows it down).
+ * abd_profile(sim, mode) resets the counters; from then on the step's CCD passes (which also
+ * collect the line-search candidates) record CUDA events around their narrow-phase kernel on
+ * the simulator's stream -- every 4th pass in mode 1, every pass in mode 2, which also counts
+ * the data the kernel moves (and slows it down).
  * abd_profile_read returns the accumulated kernel time (ms), the number of launches and, for
- * mode 2, the algorithmic bytes (point queries 24 B, edge queries 56 B, (chunk, neighbour)
- * records 140 B, internal nodes 36 B, triangle leaves 84 B, edge leaves 56 B).
+ * mode 2, the algorithmic bytes (point queries 24 B, edge queries 36 B, (chunk, neighbour)
+ * records 140 B, tree entries tested 36 B, candidates written 16 B).
  * abd_profile(sim, 0) stops. */
 int abd_profile(abd_sim* sim, int enable);
 int abd_profile_read(const abd_sim* sim, double* ms, long long* launches, double* bytes);
