@@ -39,20 +39,25 @@ def _read_obj(path: str):
     return np.asarray(V, dtype=np.float64), np.asarray(F, dtype=np.int32)
 
 
-def mesh_from_spec(spec: str, folder: str = ""):
+def mesh_from_spec(spec: str, folder: str = "", mesh_map: dict | None = None):
     """Procedural mesh names stand in for the reference's asset files
     (simulator/mesh.py:37-55): ``cube[:edge]``, ``box:sx,sy,sz``,
-    ``icosphere:level[:radius]``, or a path to an ``.obj`` file."""
-    if spec.startswith("cube"):
+    ``icosphere:level[:radius]``, or a path to an ``.obj`` file.  ``mesh_map`` renames asset
+    files that have no reader here (the reference's ``.bgeo`` / ``.usd`` assets) to one of
+    those, e.g. ``{"box.bgeo": "cube:1.0"}``."""
+    if mesh_map and spec in mesh_map:
+        return mesh_from_spec(mesh_map[spec], folder)
+    kind = spec.split(":")[0]
+    if kind == "cube":
         parts = spec.split(":")
         return cube_mesh(float(parts[1]) if len(parts) > 1 else 1.0)
-    if spec.startswith("box"):
+    if kind == "box":
         parts = spec.split(":")
         if len(parts) == 1:
             return cube_mesh(1.0)
         sx, sy, sz = (float(t) for t in parts[1].split(","))
         return box_mesh(sx, sy, sz)
-    if spec.startswith("icosphere"):
+    if kind == "icosphere":
         parts = spec.split(":")
         level = int(parts[1]) if len(parts) > 1 else 2
         radius = float(parts[2]) if len(parts) > 2 else 1.0
@@ -60,7 +65,7 @@ def mesh_from_spec(spec: str, folder: str = ""):
     if spec.endswith(".obj"):
         return _read_obj(os.path.join(folder, spec))
     raise ValueError(f"unsupported mesh '{spec}': bgeo/usd readers are not available; "
-                     "use cube / box / icosphere or an .obj file")
+                     "use cube / box / icosphere or an .obj file, or map the name with mesh_map")
 
 
 class AffineMesh:
@@ -80,9 +85,9 @@ class AffineMesh:
             "pdot": np.zeros(3),
         }
 
-    def __init__(self, obj_json: dict, density: float = DEFAULT_DENSITY):
+    def __init__(self, obj_json: dict, density: float = DEFAULT_DENSITY, mesh_map: dict | None = None):
         spec = obj_json.get("file", "cube")
-        V, F = mesh_from_spec(spec, obj_json.get("folder", ""))
+        V, F = mesh_from_spec(spec, obj_json.get("folder", ""), mesh_map)
         mass, com, I0 = mass_properties(V, F, density)
         self.V = np.ascontiguousarray(V - com, dtype=np.float64)
         self.F = np.ascontiguousarray(F, dtype=np.int32)
@@ -155,11 +160,11 @@ class Scene:
     """JSON scene -> list of :class:`AffineMesh` (simulator/scene.py:52-60)."""
 
     def __init__(self, member_type=AffineMesh, scene_config_file: str | None = None,
-                 objects: list | None = None, density: float = DEFAULT_DENSITY):
+                 objects: list | None = None, density: float = DEFAULT_DENSITY, mesh_map: dict | None = None):
         self.kinetic_objects = []
         if objects is None:
             with open(scene_config_file) as f:
                 objects = json.load(f)["objects"]
         for obj in objects:
             self.kinetic_objects.append(obj if isinstance(obj, AffineMesh)
-                                        else member_type(obj, density=density))
+                                        else member_type(obj, density=density, mesh_map=mesh_map))

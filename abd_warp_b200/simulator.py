@@ -3,10 +3,16 @@ library.
 
 Construction mirrors ``AffineBodySimulator(config_file)`` / ``BaseSimulator.__init__``
 (abd/abd.py:21-95, simulator/base.py:31-45): the config JSON names a scene JSON whose
-``objects`` become :class:`AffineMesh` bodies.  Unlike the reference, the physics keys of the
-config (``dt, dhat, kappa, stiffness, tol, max_iter`` and any other :class:`SimParams` field)
-are honoured (the reference ignores them, abd/abd.py:107-121).  Scenes can also be passed
-directly as a list of bodies.
+``objects`` become :class:`AffineMesh` bodies, and its ``simulator_args`` keys (frame range,
+``save_sequence``, output folder, verbosity; simulator/base.py:17-28) become attributes.
+Unlike the reference, the physics keys of the config (``dt, dhat, kappa, stiffness, tol,
+max_iter`` and any other :class:`SimParams` field) are honoured (the reference ignores them,
+abd/abd.py:107-121).  Scenes can also be passed directly as a list of bodies.
+
+Headless trajectory export replaces the reference's viewer loop (abd/abd.py:364-416) and its
+``export_frame`` stub (simulator/base.py:70-75): ``run()`` steps the frames
+``[frame_in, frame_out)`` and, with ``save_sequence``, writes each frame's vertex positions to
+``output_seq_folder/frame_NNNN.npz`` (read back by :func:`load_trajectory`).
 
 All arrays live on one CUDA device as float64 torch tensors.  ``step()`` runs the whole
 Newton time step inside libabd_b200.so; the stage methods (``collision_set``,
@@ -38,21 +44,43 @@ class AffineBodySimulator:
     (numpy bool per body), plus ``g`` / ``dq`` properties, ``params`` and ``last_info``.
     """
 
+    @classmethod
+    def simulator_args(cls):
+        """Frame-loop arguments and their defaults, overridden by the config file's keys
+        (simulator/base.py:17-28)."""
+        return {
+            "frame_in": 0,
+            "frame_out": 100,
+            "save_sequence": False,
+            "input_seq_folder": "bgeo/",
+            "output_seq_folder": "bgeo/",
+            "verbose": 0,
+        }
+
     def __init__(self, config_file: str | None = None, bodies=None, params: SimParams | None = None,
-                 device: str = "cuda"):
+                 device: str = "cuda", mesh_map: dict | None = None):
         import torch
         self.torch = torch
         self.params = params if params is not None else SimParams()
+        config = {}
         if config_file is not None:
             with open(config_file) as f:
                 config = json.load(f)
             for k, v in config.items():
                 if hasattr(self.params, k) and not k.startswith("_"):
                     setattr(self.params, k, v)
+        for k, v in self.simulator_args().items():
+            setattr(self, k, config.get(k, v))
+        if config_file is not None:
+            here = os.path.dirname(os.path.abspath(config_file))
+            for k in ("input_seq_folder", "output_seq_folder"):
+                if k in config and not os.path.isabs(getattr(self, k)):
+                    setattr(self, k, os.path.join(here, getattr(self, k)))
             scene_file = config["scene"]
             if not os.path.isabs(scene_file):
-                scene_file = os.path.join(os.path.dirname(os.path.abspath(config_file)), scene_file)
-            self.scene = Scene(AffineMesh, scene_config_file=scene_file)
+                scene_file = os.path.join(here, scene_file)
+            mesh_map = {**config.get("mesh_map", {}), **(mesh_map or {})}
+            self.scene = Scene(AffineMesh, scene_config_file=scene_file, mesh_map=mesh_map)
         else:
             if bodies is None:
                 raise ValueError("pass config_file or bodies")
@@ -154,6 +182,36 @@ class AffineBodySimulator:
         _lib.check(self._L.abd_step(self._h, ctypes.byref(cst), _ptr(self.x_view), ctypes.byref(info)), "abd_step")
         self.last_info = info.as_dict()
         return self.last_info
+
+    # ------------------------------------------------------------------ frames
+    def export_frame(self, frame: int, folder: str | None = None):
+        """Write the current ``x_view`` (vertex positions of the last completed step) and the
+        bodies' DOFs to ``folder/frame_NNNN.npz`` (default ``output_seq_folder``); returns the
+        path.  Headless stand-in for the reference's bgeo export (simulator/base.py:70-75)."""
+        folder = self.output_seq_folder if folder is None else folder
+        os.makedirs(folder, exist_ok=True)
+        path = os.path.join(folder, f"frame_{frame:04d}.npz")
+        s = self.states
+        np.savez(path, frame=np.int64(frame), x=self.x_view.cpu().numpy(), A=s.A0.cpu().numpy(),
+                 p=s.p0.cpu().numpy(), vert_off=self.flat["voff"])
+        return path
+
+    def run(self, frame_in: int | None = None, frame_out: int | None = None, save_sequence: bool | None = None):
+        """Step the frames [frame_in, frame_out) (defaults from the config), exporting each
+        frame's positions when ``save_sequence``; returns the per-step infos.  This replaces
+        the viewer's callback loop (abd/abd.py:364-416), which calls ``step(frame)`` once per
+        frame."""
+        f0 = self.frame_in if frame_in is None else frame_in
+        f1 = self.frame_out if frame_out is None else frame_out
+        save = self.save_sequence if save_sequence is None else save_sequence
+        infos = []
+        for frame in range(f0, f1):
+            infos.append(self.step(frame))
+            if save:
+                self.export_frame(frame)
+            if self.verbose:
+                print(f"frame {frame}: {infos[-1]}")
+        return infos
 
     # ------------------------------------------------------------------ stages
     def update_mesh_vertex(self, field: str = "x"):
@@ -310,3 +368,15 @@ class AffineBodySimulator:
 
     def launch_count(self) -> int:
         return int(self._L.abd_launch_count(self._h))
+
+
+def load_trajectory(folder: str):
+    """Frames written by :meth:`AffineBodySimulator.export_frame`, in frame order: a dict of
+    ``frames`` [F], ``x`` [F, V, 3], ``A`` [F, n, 3, 3], ``p`` [F, n, 3] and ``vert_off``."""
+    names = sorted(f for f in os.listdir(folder) if f.startswith("frame_") and f.endswith(".npz"))
+    if not names:
+        raise FileNotFoundError(f"no frame_*.npz in {folder}")
+    data = [np.load(os.path.join(folder, f)) for f in names]
+    return {"frames": np.array([int(d["frame"]) for d in data]), "x": np.stack([d["x"] for d in data]),
+            "A": np.stack([d["A"] for d in data]), "p": np.stack([d["p"] for d in data]),
+            "vert_off": data[0]["vert_off"]}
