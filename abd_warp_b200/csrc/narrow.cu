@@ -118,6 +118,44 @@ struct Visits {
   unsigned internal = 0, leaf = 0;
 };
 
+// One visit: the child table of `node` (codes and rest boxes, indexed by the node itself);
+// every leaf child whose box overlaps q goes to f(prim), every internal one to push(node).
+template <class F, class P>
+__device__ inline void expand_node(const NodeBoxes& nb, int node, const Box& q, F&& f, P&& push, Visits& cnt) {
+  const Tree& tr = *nb.tr;
+  const int L0 = tr.N - 1;
+  const int4 cc = __ldg(&tr.ccode[node]);
+  Box R[4];
+  if (nb.m0) {
+#pragma unroll
+    for (int h = 0; h < 4; ++h) R[h] = load_box(&tr.crest[4 * node + h]);
+  }
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const int code = h == 0 ? cc.x : h == 1 ? cc.y : h == 2 ? cc.z : cc.w;
+    if (code == kNoChild) continue;
+    if (code < 0) {
+      const int prim = ~code;
+      ++cnt.leaf;
+      Box B;
+      if (!nb.m0) B = load_box(&tr.box[L0 + __ldg(&tr.prim_leaf[prim])]);
+      else if (nb.sup) B = affine_box2(R[h], nb.m0, nb.m1, nb.pad);
+      else B = nb.tri ? tri_leaf_box(nb.prims, nb.y0, nb.y1, prim) : edge_leaf_box(nb.prims, nb.y0, nb.y1, prim, nb.dhh);
+      if (overlap(B, q)) f(prim);
+    } else {
+      ++cnt.internal;
+      const Box B = nb.m0 ? affine_box2(R[h], nb.m0, nb.m1, nb.pad) : load_box(&tr.box[code]);
+      if (overlap(B, q)) push(code);
+    }
+  }
+}
+
+// every pushed node is visited later: start bringing its child table to L2 now
+__device__ inline void prefetch_node(const Tree& tr, int node) {
+  prefetch_l2(&tr.ccode[node]);
+  prefetch_l2(&tr.crest[4 * node]);
+}
+
 template <class F>
 __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int* dstat, F&& f) {
   Visits v;
@@ -142,41 +180,14 @@ __device__ inline void traverse(const NodeBoxes& nb, int root, const Box& q, int
   stack[sp++] = root;
   while (sp > 0) {
     const int node = stack[--sp];
-    const int4 cc = __ldg(&tr.ccode[node]);
-    Box R[4];
-    if (nb.m0) {
-#pragma unroll
-      for (int h = 0; h < 4; ++h) R[h] = load_box(&tr.crest[4 * node + h]);
-    }
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int code = h == 0 ? cc.x : h == 1 ? cc.y : h == 2 ? cc.z : cc.w;
-      if (code == kNoChild) continue;
-      if (code < 0) {
-        const int prim = ~code;
-        ++cnt.leaf;
-        Box B;
-        if (!nb.m0) B = load_box(&tr.box[L0 + __ldg(&tr.prim_leaf[prim])]);
-        else if (nb.sup) B = affine_box2(R[h], nb.m0, nb.m1, nb.pad);
-        else B = nb.tri ? tri_leaf_box(nb.prims, nb.y0, nb.y1, prim) : edge_leaf_box(nb.prims, nb.y0, nb.y1, prim, nb.dhh);
-        if (overlap(B, q)) f(prim);
+    expand_node(nb, node, q, f, [&](int c) {
+      if (sp < kTraversalStack) {
+        stack[sp++] = c;
+        if (nb.m0) prefetch_node(tr, c);
       } else {
-        ++cnt.internal;
-        const Box B = nb.m0 ? affine_box2(R[h], nb.m0, nb.m1, nb.pad) : load_box(&tr.box[code]);
-        if (overlap(B, q)) {
-          if (sp < kTraversalStack) {
-            stack[sp++] = code;
-            // every pushed node is popped later: start bringing its child table to L2 now
-            if (nb.m0) {
-              prefetch_l2(&tr.ccode[code]);
-              prefetch_l2(&tr.crest[4 * code]);
-            }
-          } else {
-            atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
-          }
-        }
+        atomicOr(&dstat[DS_STATUS], ST_STACK_OVERFLOW);
       }
-    }
+    }, cnt);
   }
 }
 
@@ -566,8 +577,9 @@ __device__ inline bool ee_owner(int I, int nEI, int J, int nEJ) { return nEI > n
 // candidates; the pairs that also pass the CCD pass's own boxes (body pair, query and leaf)
 // become CCD candidates, the same set as the CCD pass finds.
 constexpr int CW = 4 * CT;  // (query, neighbour) combinations tested per round
+constexpr int kFront = 512;  // entries of a breadth-first frontier
 template <int MODE>
-__global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
+__global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   constexpr bool ls = MODE == NARROW_CCD_LS;
   constexpr bool ccd = MODE == NARROW_CCD || ls, gh = MODE == NARROW_GH;
   const int c = blockIdx.x, tid = threadIdx.x;
@@ -583,6 +595,9 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
   __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB], nrel[NBB];
   __shared__ unsigned short work[CW];
   __shared__ int nwork;
+  __shared__ int2 front[2][kFront];  // breadth-first frontiers: (query | neighbour << 8, node)
+  __shared__ int nfr[2];
+  int fcur = 0;
   __shared__ XSum xe;
   __shared__ unsigned long long tkey;
   __shared__ Box cbx;  // the chunk's world box: every query box of the chunk lies inside
@@ -599,6 +614,7 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
       }
     }
   }
+  if (tid == 0) nfr[0] = nfr[1] = 0;
   if (ccd) {
     if (tid == 0) tkey = 0;
   } else {
@@ -703,56 +719,105 @@ __global__ void __launch_bounds__(CT) k_chunk_narrow(NarrowArgs a) {
         work[atomicAdd(&nwork, 1)] = (unsigned short)(q | (j << 8));
       }
       __syncthreads();
+      // the compacted (query, neighbour) combinations walk their neighbour's tree breadth
+      // first: each round every thread takes frontier entries (query, neighbour, node) and
+      // expands them into the next frontier, so the visits of a chunk in heavy contact spread
+      // over the CTA instead of queueing on the threads that drew its longest walks.  When the
+      // frontier is full a thread walks the subtree itself, depth first.
+      auto visit = [&](int q, int j, int type, int pa, int pb) {
+        if constexpr (gh) {
+          // evaluated by k_gh_eval, one thread per candidate.  PT: the point is I's, the
+          // pair's first body is min(I, J); EE: the lower body's edge comes first
+          const int swap = (type == 0 && I > nJ[j]) ? 1 : 0;
+          const int pos = append_slot(&a.dstat[DS_NCCD]);
+          if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(npair[j], type | (swap << 1), pa, pb);
+          else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+        } else if constexpr (ls) {
+          // line-search candidates; k_ccd_eval takes those that pass the CCD pass's boxes
+          const int pos = append_slot(&a.dstat[DS_NECAND]);
+          ++pf_cand;
+          if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
+          else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
+        } else if constexpr (ccd) {  // evaluated by k_ccd_eval, one thread per candidate
+          const int pos = append_slot(&a.dstat[DS_NCCD]);
+          if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
+          else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+        } else {
+          int ids[4];
+          d3 xs[4];
+          cand_vertices(a, type, pa, pb, ids);
+          fetch(a.y0, ids, xs);
+          const double e = contact_energy(type, xs, a.prm);
+          if (e != 0.0) xs_add_atomic(&xe, e);
+        }
+      };
+      // a leaf of J's tree reached by query q: PT (I's point, J's triangle) or EE (the lower
+      // body's edge first, as the per-pair lists)
+      auto hit = [&](int q, int j, int prim) {
+        const int qp = qprim[q];
+        if (qp >= 0) visit(q, j, 0, qp, prim);
+        else if (I < nJ[j]) visit(q, j, 1, ~qp, prim);
+        else visit(q, j, 1, prim, ~qp);
+      };
+      auto boxes_of = [&](int q, int j) {
+        const bool tri = qprim[q] >= 0;
+        NodeBoxes nbx = node_boxes(a, tri ? &a.tri : &a.edge, tri, ndof[j]);
+        nbx.sup = ls;
+        return nbx;
+      };
+      auto tally = [&](bool tri, const Visits& vc) {
+        pf_node += vc.internal;
+        if (tri) pf_tri += vc.leaf;
+        else pf_edge += vc.leaf;
+      };
+      // frontier entry: (q | j << 8, node); a full frontier makes the pusher walk the subtree
+      auto push = [&](int nxt, int q, int j, int node) {
+        const NodeBoxes nbx = boxes_of(q, j);
+        const int slot = atomicAdd(&nfr[nxt], 1);
+        if (slot < kFront) {
+          front[nxt][slot] = make_int2(q | (j << 8), node);
+          prefetch_node(*nbx.tr, node);
+        } else {
+          Visits vc;
+          traverse(nbx, node, qbox[q], a.dstat, [&](int prim) { hit(q, j, prim); }, vc);
+          tally(nbx.tri, vc);
+        }
+      };
+      // the roots
       for (int k = tid; k < nwork; k += CT) {
         const int q = work[k] & 0xff, j = work[k] >> 8;
-        const int qp = qprim[q];
-        const Box qb = qbox[q];
-        auto visit = [&](int type, int pa, int pb) {
-          if constexpr (gh) {
-            // evaluated by k_gh_eval, one thread per candidate.  PT: the point is I's, the
-            // pair's first body is min(I, J); EE: the lower body's edge comes first
-            const int swap = (type == 0 && I > nJ[j]) ? 1 : 0;
-            const int pos = append_slot(&a.dstat[DS_NCCD]);
-            if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(npair[j], type | (swap << 1), pa, pb);
-            else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
-          } else if constexpr (ls) {
-            // line-search candidates; k_ccd_eval takes those that pass the CCD pass's boxes
-            const int pos = append_slot(&a.dstat[DS_NECAND]);
-            ++pf_cand;
-            if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
-            else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
-          } else if constexpr (ccd) {  // evaluated by k_ccd_eval, one thread per candidate
-            const int pos = append_slot(&a.dstat[DS_NCCD]);
-            if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
-            else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
-          } else {
-            int ids[4];
-            d3 xs[4];
-            cand_vertices(a, type, pa, pb, ids);
-            fetch(a.y0, ids, xs);
-            const double e = contact_energy(type, xs, a.prm);
-            if (e != 0.0) xs_add_atomic(&xe, e);
-          }
-        };
-        if (qp >= 0) {
-          Visits vc;
-          NodeBoxes nbt = node_boxes(a, &a.tri, true, ndof[j]);
-          nbt.sup = ls;
-          traverse(nbt, ntri[j], qb, a.dstat, [&](int t) { visit(0, qp, t); }, vc);
-          pf_node += vc.internal;
-          pf_tri += vc.leaf;
-        } else {
-          // EE candidates are evaluated with the edge of the lower body first, as the per-pair lists
-          const bool lower = I < nJ[j];
-          Visits vc;
-          NodeBoxes nbe = node_boxes(a, &a.edge, false, ndof[j]);
-          nbe.sup = ls;
-          traverse(nbe, nedge[j], qb, a.dstat, [&](int e) { lower ? visit(1, ~qp, e) : visit(1, e, ~qp); }, vc);
-          pf_node += vc.internal;
-          pf_edge += vc.leaf;
+        const NodeBoxes nbx = boxes_of(q, j);
+        const int root = nbx.tri ? ntri[j] : nedge[j];
+        const int L0 = nbx.tr->N - 1;
+        Visits vc;
+        if (root >= L0) {  // a tree of one leaf
+          const int prim = __ldg(&nbx.tr->leaf_prim[root - L0]);
+          ++vc.leaf;
+          if (overlap(nbx.leaf(root, prim), qbox[q])) hit(q, j, prim);
+        } else if (root >= 0) {
+          ++vc.internal;
+          if (overlap(nbx.internal(root), qbox[q])) push(fcur, q, j, root);
         }
+        tally(nbx.tri, vc);
       }
-      __syncthreads();
+      // the rounds
+      for (;;) {
+        __syncthreads();
+        const int n = min(nfr[fcur], kFront);
+        if (n == 0) break;
+        const int nxt = fcur ^ 1;
+        for (int e = tid; e < n; e += CT) {
+          const int2 en = front[fcur][e];
+          const int q = en.x & 0xff, j = en.x >> 8;
+          const NodeBoxes nbx = boxes_of(q, j);
+          Visits vc;
+          expand_node(nbx, en.y, qbox[q], [&](int prim) { hit(q, j, prim); }, [&](int c) { push(nxt, q, j, c); }, vc);
+          tally(nbx.tri, vc);
+        }
+        __syncthreads();
+        if (tid == 0) nfr[fcur] = 0;
+        fcur = nxt;
+      }
     }
   }
   if constexpr (gh) return;
