@@ -253,10 +253,12 @@ struct Sim {
   double* dpar = nullptr;
   int* dint = nullptr;             // device integers: [0] preconditioner clusters
   int* hint = nullptr;             // pinned staging of dint
-  // captured passes: energy trial, CCD bound, GH, Krylov setup and one block of iterations
+  // captured passes: CCD bound (with events for profiling), GH, the Krylov solve, line-search
+  // batches (step lengths from the host or from the CCD pass on the device)
   cudaStream_t cap_stream = nullptr;
   cudaStream_t cap_stream2 = nullptr;  // captures the bodies of conditional (loop) nodes
-  GraphSlot g_energy, g_ccd, g_ccd_ev, g_gh, g_kinit, g_ls;
+  GraphSlot g_ccd, g_ccd_ev, g_gh, g_gh0, g_kinit, g_ls, g_ls_dev;
+  int gh_energy = 0;               // the GH pass also sums the energy at its DOFs
   unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
   // kernel profiling of the line-search candidate pass's narrow kernel: CUDA events around
   // it (recorded as graph nodes), its duration and algorithmic bytes accumulated per pass
@@ -437,9 +439,13 @@ cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, cons
 // [0, 1], from the candidates of the last CCD_LS pass between (A, p) and (A, p) - dq, into
 // the mailbox's ls_energy[k]
 cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p);
+// the trial count and step lengths of a batch (dpar) from the last CCD pass's time of impact
+cudaError_t ls_setup_from_ccd(Sim& s);
 
 // solver.cu
 int build_preconditioner(Sim& s);                 // returns ABD status
-int krylov_solve(Sim& s, double* x, int* iters);  // returns ABD status
+// returns ABD status; iters == null: enqueue only (krylov_outcome after the next mailbox read)
+int krylov_solve(Sim& s, double* x, int* iters);
+int krylov_outcome(Sim& s);                       // iterations of the last solve
 
 }  // namespace abd

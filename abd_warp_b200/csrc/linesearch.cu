@@ -192,7 +192,32 @@ __global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv) {
   }
 }
 
+// The trials of a batch from the CCD pass's minimum time of impact, on the device (one
+// thread): the step bound alpha = clamp(toi, 0, 1), times 0.9 below 1 (ccd, abd.py:278-303),
+// then alpha, alpha / 2, ... up to the first below alpha_min, at most kLsMax -- the same
+// arithmetic as the host's.
+__global__ void k_ls_setup(const unsigned long long* toi_key, double alpha_min, double* dpar) {
+  double toi = 1.0;
+  if (const unsigned long long key = *toi_key) toi = __longlong_as_double((long long)~key);
+  const double lo = toi < 1.0 ? toi : 1.0;  // std::min(1.0, toi), std::max(0.0, .)
+  double t = 0.0 < lo ? lo : 0.0;
+  if (t < 1.0) t *= 0.9;
+  int K = 0;
+  for (double al = t; K < kLsMax;) {
+    dpar[kParAlpha + K++] = al;
+    if (al < alpha_min) break;
+    al *= 0.5;
+  }
+  dpar[kParK] = K;
+}
+
 }  // namespace
+
+cudaError_t ls_setup_from_ccd(Sim& s) {
+  k_ls_setup<<<1, 1, 0, s.stream>>>(s.dmin, s.prm.alpha_min, s.dpar);
+  ++s.launches;
+  return cudaGetLastError();
+}
 
 cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p) {
   LsArgs a;

@@ -54,6 +54,7 @@ struct NarrowArgs {
   const int* adj_pair;
   int cap_ccd;
   int4* ccd_cand;
+  int gh_energy;                // GH: also sum the candidates' barrier energies into energy
   const Box* body_sup;          // CCD_LS: body boxes over every DOF set between the two
   const int* vbody;
   int cap_ecand;
@@ -884,11 +885,15 @@ __global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
 
 // Contacts of the GH pass's candidates, one thread per candidate: the active ones
 // (pt_ipc.py:13-22, 114; ee_ipc.py:13-23, 382) are appended for the per-pair assembly and
-// counted per pair; the candidates are counted per kind.
+// counted per pair; the candidates are counted per kind.  With gh_energy their barrier
+// energies join the pass's exact energy (k_body_gh adds the bodies' terms: the GH pass then
+// also gives the energy at its DOFs, the same sum as an energy pass there).
 __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
   if (a.dstat[DS_STATUS] & (ST_CCD_OVERFLOW | ST_PAIR_OVERFLOW)) return;
   const int n = min(a.dstat[DS_NCCD], a.cap_ccd);
   int cpt = 0, cee = 0;
+  XSum en;  // the candidates' barrier energy (ipcsk/energy.py:9-48)
+  xs_zero(en);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int4 c = a.ccd_cand[k];  // pair, type | swap << 1, primitive a, primitive b
     const int type = c.y & 1;
@@ -898,6 +903,10 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
     d3 xs[4];
     cand_vertices(a, type, c.z, c.w, ids);
     fetch(a.y0, ids, xs);
+    if (a.gh_energy) {
+      const double e = contact_energy(type, xs, a.prm);
+      if (e != 0.0) xs_add(en, e);
+    }
     Geo G;
     double d2;
     if (contact_active(type, xs, a.prm, &G, &d2)) {
@@ -912,9 +921,15 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
     cpt += __shfl_xor_sync(0xffffffffu, cpt, o);
     cee += __shfl_xor_sync(0xffffffffu, cee, o);
   }
+  if (a.gh_energy) xs_warp_sum(en);
   if ((threadIdx.x & 31) == 0) {
     if (cpt) atomicAdd(&a.dstat[DS_PT_COUNT], cpt);
     if (cee) atomicAdd(&a.dstat[DS_EE_COUNT], cee);
+    long long* d = reinterpret_cast<long long*>(a.energy);
+#pragma unroll
+    for (int i = 0; i < kXD; ++i)
+      if (en.d[i]) atomicAdd((unsigned long long*)&d[i], (unsigned long long)en.d[i]);
+    if (en.flags) atomicOr((unsigned long long*)&d[kXD], (unsigned long long)en.flags);
   }
 }
 
@@ -937,6 +952,7 @@ struct BodyArgs {
   int* dstat;
   int* vg_list;
   int cap_vg;
+  XSum* energy;  // or null; the pass's exact energy (GH: inertia + vertex-ground terms, added here)
 };
 
 __device__ inline void tilde(const BodyArgs& a, int b, double At[9], double pt[3]) {
@@ -954,19 +970,26 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   const double dt = a.prm.dt, ks = a.prm.stiffness;
   const double* A = a.A + 9 * b;
   double val = 0.0;
-  // vertex-ground sums, exact: g (4 y-components) and H (4x4 yy-components)
-  __shared__ XSum vx[20];
+  // vertex-ground sums, exact: g (4 y-components) and H (4x4 yy-components); vx[20]: the
+  // body's energy (vertex-ground barriers of every body, inertia + orthogonality of a free one)
+  __shared__ XSum vx[21];
   const bool vg_any = a.prm.ground_enabled && a.prm.enable_vg, vg_on = vg_any && !fixed;
-  for (int e = t; e < 20 * (kXD + 1); e += BT) reinterpret_cast<long long*>(vx)[e] = 0;
+  for (int e = t; e < 21 * (kXD + 1); e += BT) reinterpret_cast<long long*>(vx)[e] = 0;
   __syncthreads();
+  if (a.energy && t == 128 && !fixed)
+    xs_add_atomic(&vx[20], inertia_energy(a.prm, a.st, a.mass, a.I0, b, a.A + 9 * b, a.p + 3 * b));
   if (vg_any && t < 128) {
     const Box bb = load_box(&a.body_box[b]);
     int cnt = 0;  // the culling's vertex-ground pairs, fixed bodies included (culling.py:54-82)
     for (int v = a.voff[b] + t; v < a.voff[b + 1]; v += 128) {
       if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
       ++cnt;
-      if (!vg_on) continue;
       const double d = a.y[3 * v + 1] - a.prm.ground;
+      if (a.energy) {
+        const double e = barrier(d * d, a.prm);
+        if (e != 0.0) xs_add_atomic(&vx[20], e);
+      }
+      if (!vg_on) continue;
       const double d2b = barrier_d2(d * d, a.prm), db = barrier_d1(d * d, a.prm);
       const double th[4] = {1.0, a.x0[3 * v], a.x0[3 * v + 1], a.x0[3 * v + 2]};
 #pragma unroll
@@ -979,6 +1002,14 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
     if (cnt) atomicAdd(&a.dstat[DS_VG_COUNT], cnt);
   }
   __syncthreads();
+  if (a.energy && t <= kXD) {
+    const long long v = reinterpret_cast<const long long*>(&vx[20])[t];
+    long long* d = reinterpret_cast<long long*>(a.energy);
+    if (v) {
+      if (t < kXD) atomicAdd((unsigned long long*)&d[t], (unsigned long long)v);
+      else atomicOr((unsigned long long*)&d[t], (unsigned long long)v);
+    }
+  }
   if (t >= 156) return;
   if (!fixed) {
     double At[9], pt[3];
@@ -1174,6 +1205,7 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.cap_ccd = s.cap_ccd;
   a.ccd_cand = s.ccd_cand;
   a.body_sup = s.body_sup;
+  a.gh_energy = s.gh_energy;
   a.vbody = s.vbody;
   a.cap_ecand = s.cap_ecand;
   a.ecand = s.ecand;
@@ -1236,6 +1268,7 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
   a.dstat = s.dstat;
   a.vg_list = s.vg_list;
   a.cap_vg = s.cap_vg;
+  a.energy = s.gh_energy ? s.energy_acc : nullptr;
   return a;
 }
 

@@ -289,20 +289,17 @@ int energy_at(abd_sim* h, const abd_states& st, const double* Ak, const double* 
   return energy_of(h, st, direct(Ak, pk), E);
 }
 
-// Energy at q - alpha dq (written to Ak, pk): one trial of the line search (abd.py:146-160)
-int energy_trial(abd_sim* h, const abd_states& st, double alpha, double* E) {
-  Sim& s = h->s;
-  s.hpar[0] = alpha;  // copied to dpar[0] by the pass itself
-  return energy_of(h, st, updated(s, st.A, st.p, 0, st.Ak, st.pk), E, &s.g_energy, states_key(s, st));
-}
+
+int no_post() { return ABD_OK; }
 
 // CCD bound between DOFs d0 and d1 (ccd, abd.py:278-303); positions land in x, xk.  pre()
 // enqueues work that belongs to the same pass (the step's dot products, whose results ride
-// along in the mailbox).  mode NARROW_CCD_LS also collects the line-search candidates
-// between d0 and d1 for ls_batch.
-template <class Pre>
+// along in the mailbox); post() enqueues work that follows it before the host's wait (the
+// step's first line-search batch).  mode NARROW_CCD_LS also collects the line-search
+// candidates between d0 and d1.
+template <class Pre, class Post = int (*)()>
 int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, double* raw, Pre&& pre,
-           abd::GraphSlot* g = nullptr, uint64_t key = 0, int mode = abd::NARROW_CCD) {
+           abd::GraphSlot* g = nullptr, uint64_t key = 0, int mode = abd::NARROW_CCD, Post&& post = no_post) {
   Sim& s = h->s;
   auto issue = [&]() -> int {
     int r = pre();
@@ -322,7 +319,7 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
     abd::KeyHash k;
     k.add(key).add(s.cap_ccd).add(s.ccd_cand).add(mode).add(s.cap_ecand).add(s.ecand).add(s.prof_on).add(s.prof_events);
     int r = g ? abd::run_graph(s, *g, k.h, issue) : issue();
-    if (r) return r;
+    if (r || (r = post())) return r;
     CK(cudaStreamSynchronize(s.stream));
     std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
     if ((r = overflow(s)) > 0) return r;
@@ -356,25 +353,50 @@ int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const
   return ccd_of(h, direct(A, p), direct(A1, p1), alpha, raw, []() -> int { return ABD_OK; });
 }
 
-// Energies at (A, p) - al[k] dq, k < K <= kLsMax, 0 <= al[k] <= 1, from the candidates of the
-// last CCD_LS pass between (A, p) and (A, p) - dq: one replayed pass and one read.  Each is
-// bitwise the energy pass's at the same DOFs.
-int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p, const double* al, int K,
-             double* E, uint64_t key) {
+// Enqueues the energies at (A, p) - al[k] dq, k < K <= kLsMax, 0 <= al[k] <= 1, from the
+// candidates of the last CCD_LS pass between (A, p) and (A, p) - dq, with the mailbox copy: one
+// replayed pass.  al == null: the step lengths follow from that pass's time of impact on the
+// device (k_ls_setup).  Each energy is bitwise the energy pass's at the same DOFs.
+int ls_launch(abd_sim* h, const abd_states& st, const double* A, const double* p, const double* al, int K,
+              uint64_t key) {
   Sim& s = h->s;
-  if (K < 1 || K > abd::kLsMax) return ABD_ERR_INVALID;
-  s.hpar[abd::kParK] = K;
-  for (int k = 0; k < abd::kLsMax; ++k) s.hpar[abd::kParAlpha + k] = k < K ? al[k] : 0.0;
+  if (al && (K < 1 || K > abd::kLsMax)) return ABD_ERR_INVALID;
+  if (al) {
+    s.hpar[abd::kParK] = K;
+    for (int k = 0; k < abd::kLsMax; ++k) s.hpar[abd::kParAlpha + k] = k < K ? al[k] : 0.0;
+  }
   auto issue = [&]() -> int {
-    CK(cudaMemcpyAsync(s.dpar + abd::kParK, s.hpar + abd::kParK, sizeof(double) * (1 + abd::kLsMax),
-                       cudaMemcpyHostToDevice, s.stream));
+    if (al)
+      CK(cudaMemcpyAsync(s.dpar + abd::kParK, s.hpar + abd::kParK, sizeof(double) * (1 + abd::kLsMax),
+                         cudaMemcpyHostToDevice, s.stream));
+    else
+      CK(abd::ls_setup_from_ccd(s));
     CK(abd::ls_energies(s, st, A, p));
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
   abd::KeyHash kh;
   kh.add(key).add(A).add(p).add(s.cap_ecand).add(s.ecand);
-  int r = abd::run_graph(s, s.g_ls, kh.h, issue);
+  return abd::run_graph(s, al ? s.g_ls : s.g_ls_dev, kh.h, issue);
+}
+
+// The trial step lengths of a line search from the bound alpha: alpha, alpha / 2, ... up to
+// the first below alpha_min, at most kLsMax (the device's k_ls_setup makes the same list)
+int trial_steps(double alpha, double alpha_min, double* al) {
+  int K = 0;
+  for (double a_ = alpha; K < abd::kLsMax;) {
+    al[K++] = a_;
+    if (a_ < alpha_min) break;
+    a_ *= 0.5;
+  }
+  return K;
+}
+
+// ls_launch with the host's wait; the energies land in E[0, K)
+int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p, const double* al, int K,
+             double* E, uint64_t key) {
+  Sim& s = h->s;
+  int r = ls_launch(h, st, A, p, al, K, key);
   if (r) return r;
   CK(cudaStreamSynchronize(s.stream));
   std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
@@ -385,9 +407,10 @@ int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p,
 // Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner.
 // g: replay slot for the step (its key covers every capacity the captured grids depend on).
 int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active,
-          abd::GraphSlot* g = nullptr) {
+          abd::GraphSlot* g = nullptr, bool with_energy = false) {
   Sim& s = h->s;
   const abd::Dofs d = direct(A, p);
+  s.gh_energy = with_energy ? 1 : 0;  // read by the kernel arguments of this pass
   auto issue = [&]() -> int {
     int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
     if (r) return r;
@@ -405,7 +428,7 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
       k.add(states_key(s, st)).add(A).add(p).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
       k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
       k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.hact);
-      k.add(s.cap_ccd).add(s.ccd_cand);
+      k.add(s.cap_ccd).add(s.ccd_cand).add(s.gh_energy);
       r = abd::run_graph(s, *g, k.h, issue);
     } else {
       r = issue();
@@ -724,7 +747,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.body_sup, s.slice};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (abd::GraphSlot* g : {&s.g_energy, &s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_kinit, &s.g_ls})
+  for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev})
     if (g->exec) cudaGraphExecDestroy(g->exec);
   if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
   if (s.cap_stream2) cudaStreamDestroy(s.cap_stream2);
@@ -887,7 +910,10 @@ int abd_solve(abd_sim* h, double* dq, int* iters) {
   if (!h || !dq) return ABD_ERR_INVALID;
   int r = abd::build_preconditioner(h->s);
   if (r) return r;
-  return abd::krylov_solve(h->s, dq, iters);
+  int it = 0;
+  r = abd::krylov_solve(h->s, dq, &it);  // waits for the solve
+  if (iters) *iters = it;
+  return r;
 }
 
 int abd_compute_energy(abd_sim* h, const abd_states* st, const double* Ak, const double* pk, double* E) {
@@ -929,24 +955,24 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
   CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, s.stream));
   abd_step_info inf{};
   int r;
-  double E0;
-  if ((r = energy_trial(h, st, 0.0, &E0))) return r;  // Ak = A - 0 dq
+  double E0 = 0.0;
   int it = 0;
   for (;;) {
     int nact = 0;
-    if ((r = gh_of(h, st, st.A, st.p, &nact, &s.g_gh))) return r;
+    // the step's first GH pass also gives the energy at q0 (its own replay slot)
+    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0))) return r;
     if (it == 0) {
+      // the energy at q0 (abd.py:126-128): the GH pass at q0 sums the same terms as an
+      // energy pass there
+      E0 = xs_round_host(s.hbox->energy);
       inf.n_pt = s.hstat[abd::DS_PT_COUNT];
       inf.n_ee = s.hstat[abd::DS_EE_COUNT];
       inf.n_vg = s.hstat[abd::DS_VG_COUNT];
       inf.n_ij = s.n_pairs;
     }
     inf.n_active = nact;
-    int lin = 0;
     if ((r = abd::build_preconditioner(s))) return r;
-    if ((r = abd::krylov_solve(s, s.dq, &lin))) return r;
-    inf.linear_iters += lin;
-    // dq.g and g.g (abd.py:148, 265), read back together with the CCD bound
+    if ((r = abd::krylov_solve(s, s.dq, nullptr))) return r;  // outcome read with the CCD pass
     // dq.g, g.g (abd.py:148, 265) and the CCD bound between q and q - dq (abd.py:278-303),
     // one pass; Ak, pk = q - dq
     double alpha;
@@ -954,23 +980,27 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
       CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots));
       return ABD_OK;
     };
+    // the CCD pass and the line search's first batch (its step lengths from the pass's time of
+    // impact, on the device) before one wait
+    const uint64_t skey = states_key(s, st);
+    auto first_batch = [&]() -> int { return ls_launch(h, st, st.A, st.p, nullptr, 0, skey); };
     if ((r = ccd_of(h, direct(st.A, st.p), updated(s, st.A, st.p, 1, st.Ak, st.pk), &alpha, &inf.toi, dots,
-                    &s.g_ccd, states_key(s, st), abd::NARROW_CCD_LS)))
+                    &s.g_ccd, skey, abd::NARROW_CCD_LS, first_batch)))
       return r;
+    inf.linear_iters += abd::krylov_outcome(s);
     const double qTg = s.hbox->dots[0], gTg = s.hbox->dots[1];
     // backtracking line search (abd.py:146-160): the trials alpha, alpha / 2, ... up to the
     // first below alpha_min, kLsMax per batch; the first trial that passes is taken, as in
     // the sequential search
     double E1 = E0;
-    for (bool done = false; !done;) {
+    for (bool done = false, first = true; !done; first = false) {
       double al[abd::kLsMax], Eb[abd::kLsMax];
-      int K = 0;
-      for (double a_ = alpha; K < abd::kLsMax;) {
-        al[K++] = a_;
-        if (a_ < P.alpha_min) break;
-        a_ *= 0.5;
+      const int K = trial_steps(alpha, P.alpha_min, al);
+      if (first) {
+        for (int k = 0; k < K; ++k) Eb[k] = xs_round_host(s.hbox->ls_energy[k]);
+      } else if ((r = ls_batch(h, st, st.A, st.p, al, K, Eb, skey))) {
+        return r;
       }
-      if ((r = ls_batch(h, st, st.A, st.p, al, K, Eb, states_key(s, st)))) return r;
       for (int k = 0; k < K && !done; ++k) {
         alpha = al[k];
         E1 = Eb[k];

@@ -655,12 +655,14 @@ int build_preconditioner(Sim& s) {
 
 // Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  One replayed graph:
 // the setup kernels, then a WHILE node whose body is one iteration (its last kernel sets the
-// loop condition), then the mailbox copy; the host reads the outcome once.
+// loop condition).  With iters_out the host waits for it and reads the outcome; without, the
+// solve is only enqueued and its outcome stays in the mailbox's counters (krylov_outcome
+// reads it after the caller's next read of the mailbox).
 int krylov_solve(Sim& s, double* x, int* iters_out) {
   const SolverArgs a = solver_args(s);
   const double* bvec = s.g;
   const bool pcg = s.prm.solver == 1;
-  const int per_iter = pcg ? 5 : 10;  // kernels of one iteration
+  const int per_iter = pcg ? 5 : 10;  // kernels of one iteration (counted once at capture)
   KeyHash kh;
   kh.add(x).add(s.n).add(s.prm_version).add(s.prm.solver).add(s.prm.cg_max_iter).add(s.cl_inv).add(s.box);
   int r = run_graph(s, s.g_kinit, kh.h, [&]() -> int {
@@ -720,17 +722,25 @@ int krylov_solve(Sim& s, double* x, int* iters_out) {
     cudaGraph_t body_out = nullptr;
     const cudaError_t eb = cudaGetLastError();
     if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
-    if (cudaMemcpyAsync(s.hbox, s.box, sizeof(Mailbox), cudaMemcpyDeviceToHost, st)) return ABD_ERR_CUDA;
     return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
   });
-  if (r) return r;
-  if (cudaStreamSynchronize(s.stream) != cudaSuccess) return ABD_ERR_CUDA;
+  if (r || !iters_out) return r;
+  if (cudaMemcpyAsync(s.hbox, s.box, sizeof(Mailbox), cudaMemcpyDeviceToHost, s.stream) ||
+      cudaStreamSynchronize(s.stream) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  *iters_out = krylov_outcome(s);
+  return ABD_OK;
+}
+
+// The last solve's iterations, from the host's copy of the mailbox; non-convergence raises
+// ST_SOLVER_NOCONV in the host status bits.
+int krylov_outcome(Sim& s) {
   const int* ds = s.hbox->dstat;
+  const int per_iter = s.prm.solver == 1 ? 5 : 10;
   // the graph's launch count covers one iteration; the loop ran ds[DS_IT] - 1
   s.launches += (long long)per_iter * std::max(0, ds[DS_IT] - 2);
-  if (!(ds[DS_R_DONE] || ds[DS_S_DONE])) s.host_status |= ST_SOLVER_NOCONV;  // reported through the status bits
-  if (iters_out) *iters_out = ds[DS_SOLVER_ITERS];
-  return ABD_OK;
+  if (!(ds[DS_R_DONE] || ds[DS_S_DONE])) s.host_status |= ST_SOLVER_NOCONV;
+  return ds[DS_SOLVER_ITERS];
 }
 
 }  // namespace abd
