@@ -14,6 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libabd_b200.so")
 
 ABD_OK = 0
+ABD_ERR_CUDA, ABD_ERR_INVALID, ABD_ERR_OVERFLOW, ABD_ERR_DEVICE = 1, 2, 3, 4  # include/abd_b200.h
 STATUS_NAMES = {1: "pt_overflow", 2: "ee_overflow", 4: "pair_overflow", 8: "stack_overflow",
                 16: "solver_not_converged", 32: "nan", 64: "vg_overflow"}
 

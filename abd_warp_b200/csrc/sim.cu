@@ -480,7 +480,7 @@ const char* abd_status_string(int code) {
 
 int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream, abd_sim** out) {
   if (!d || !prm || !out || d->n_bodies <= 0 || !d->vert_off || !d->tri_off || !d->edge_off || !d->x0 ||
-      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed)
+      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed || prm->precision != 0)
     return ABD_ERR_INVALID;
   const int n = d->n_bodies;
   const int V = d->vert_off[n], T = d->tri_off[n], E = d->edge_off[n];
@@ -761,7 +761,7 @@ int abd_sim_destroy(abd_sim* h) {
 }
 
 int abd_sim_set_params(abd_sim* h, const abd_params* prm) {
-  if (!h || !prm) return ABD_ERR_INVALID;
+  if (!h || !prm || prm->precision != 0) return ABD_ERR_INVALID;
   h->s.prm = *prm;
   ++h->s.prm_version;  // parameters are kernel arguments of the captured passes
   return ABD_OK;

@@ -47,8 +47,10 @@ class SimParams:
     cluster_max: int = 12            # bodies per preconditioner cluster
     cg_tol: float = 1e-10            # stop when r^T M^-1 r <= cg_tol^2 b^T M^-1 b
     cg_max_iter: int = 2000
-    precision: int = PRECISION_FP64
-    refine_tol: float = 1e-10        # mixed precision: FP64 refinement target
+    precision: int = PRECISION_FP64  # the CUDA library accepts FP64 only; the oracle also runs
+                                     # PRECISION_MIXED (FP32 PCG inside FP64 refinement), which
+                                     # diverges once bodies touch (cond(H) ~ 1e10 > 1 / eps_FP32)
+    refine_tol: float = 1e-4         # oracle mixed precision: the FP32 inner solve's relative tolerance
 
     @property
     def d2hat(self) -> float:

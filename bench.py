@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64"],
+                    help="FP64 only: FP32 Krylov solves inside FP64 refinement diverge on the contact systems")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--start-state", type=int, default=None,
@@ -202,7 +203,6 @@ def main():
     import numpy as np
     import torch
     import torch.distributed as dist
-    from abd_warp_b200.params import PRECISION_MIXED
     from abd_warp_b200.simulator import AffineBodySimulator
 
     rank, world, local = dist_env()
@@ -213,8 +213,6 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     bodies, prm = make_scene()
-    if args.precision == "mixed":
-        prm.precision = PRECISION_MIXED
     sim = AffineBodySimulator(bodies=bodies, params=prm, device=f"cuda:{local}")
     s = sim.states
     stream = torch.cuda.current_stream(dev)

@@ -45,7 +45,9 @@ typedef struct abd_params {
   int enable_pt, enable_ee, enable_vg; /* const_params.py:41-43 */
   int solver;         /* 0: preconditioned BiCGSTAB (abd.py:244 uses bicgstab), 1: PCG (default) */
   int cg_max_iter;
-  int precision;      /* 0: FP64 throughout; 1: FP32 Krylov solve inside FP64 refinement */
+  int precision;      /* 0: FP64 throughout (the only accepted value).  1, an FP32 Krylov solve
+                         inside FP64 refinement, is rejected with ABD_ERR_INVALID: on contact
+                         systems (cond(H) ~ 1e10 > 1 / eps_FP32) the refinement diverges */
   int contact_psd;    /* 1: PSD projection of the barrier Hessian; 0: the reference's form */
   int precond;        /* 1: contact-cluster block Jacobi (clusters of <= cluster_max bodies); 0: per body */
   int cluster_max;    /* 1..12 */
@@ -77,7 +79,7 @@ typedef struct abd_step_info {
   int newton_iters, linear_iters, ls_trials, n_pt, n_ee, n_vg, n_ij, n_active;
   double alpha, toi, energy;
   int status;          /* device status bits seen during the step (0 = clean) */
-  int refine_iters;    /* precision == 1: FP64 refinement sweeps */
+  int refine_iters;    /* FP64 refinement sweeps (0: precision 1 is not accepted) */
 } abd_step_info;
 
 typedef struct abd_sim abd_sim;

@@ -74,7 +74,7 @@ class OrcInfo(ctypes.Structure):
     _fields_ = [("newton_iters", ctypes.c_int), ("linear_iters", ctypes.c_int), ("ls_trials", ctypes.c_int),
                 ("n_pt", ctypes.c_int), ("n_ee", ctypes.c_int), ("n_vg", ctypes.c_int), ("n_ij", ctypes.c_int),
                 ("n_active", ctypes.c_int), ("alpha", ctypes.c_double), ("toi", ctypes.c_double),
-                ("energy", ctypes.c_double)]
+                ("energy", ctypes.c_double), ("refine_iters", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

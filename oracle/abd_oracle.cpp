@@ -198,7 +198,8 @@ struct Oracle {
   std::vector<int> adj_ptr, adj;  // per body (neighbour, pair, side), neighbours increasing
   // stats
   int stat_newton = 0, stat_lin = 0, stat_ls = 0, stat_pt = 0, stat_ee = 0, stat_vg = 0, stat_ij = 0,
-      stat_active = 0;
+      stat_active = 0, stat_refine = 0;
+  int last_sweeps = 0;  // refinement sweeps of the last mixed-precision solve
   double stat_alpha = 0, stat_toi = 0, stat_energy = 0;
 };
 
@@ -1107,8 +1108,120 @@ void build_clusters(const Oracle& o, std::vector<int>& cl_ptr, std::vector<int>&
   }
 }
 
+// Mixed precision (precision == 1): FP64 iterative refinement around an FP32 PCG.  Each sweep
+// takes the FP64 residual r = b - H x and its preconditioned norm; the solve stops when that
+// norm meets the FP64 target (rz <= thr2, the FP64 solve's test), else an FP32 PCG solves
+// H e = r from e = 0 -- FP32 copies of the blocks and of the cluster inverses, FP32 vector
+// arithmetic in the FP64 solve's operation order, exact dot products of the FP32 products,
+// FP64 scalars -- until its own preconditioned norm falls by refine_tol, and x += e in FP64.
+// At most kMaxSweeps sweeps; cg_max_iter bounds the FP32 iterations of the whole solve.
+constexpr int kMaxSweeps = 16;
+template <class Prec>
+int solve_mixed(Oracle& o, const std::vector<double>& Kinv, const std::vector<size_t>& cl_off,
+                const std::vector<int>& cl_ptr, const std::vector<int>& cl_body, Prec&& prec, double thr2) {
+  const int n = o.n, N = 12 * n, ncl = (int)cl_ptr.size() - 1;
+  std::vector<float> d32(o.diag.size()), f32(o.off.size()), K32(Kinv.size());
+  for (size_t i = 0; i < d32.size(); ++i) d32[i] = (float)o.diag[i];
+  for (size_t i = 0; i < f32.size(); ++i) f32[i] = (float)o.off[i];
+  for (size_t i = 0; i < K32.size(); ++i) K32[i] = (float)Kinv[i];
+  // y = H32 x in the order of spmv
+  auto spmv32 = [&](const std::vector<float>& xv, std::vector<float>& yv) {
+    yv.assign(N, 0.f);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < n; ++b)
+      for (int r = 0; r < 12; ++r) {
+        float acc[2];
+        for (int h = 0; h < 2; ++h) {
+          float a = 0.f;
+          for (int c = 0; c < 6; ++c) a += d32[144 * b + r * 12 + 6 * h + c] * xv[12 * b + 6 * h + c];
+          if (!o.fixed[b])
+            for (int k = o.adj_ptr[b]; k < o.adj_ptr[b + 1]; ++k) {
+              const int J = o.adj[3 * (size_t)k], q = o.adj[3 * (size_t)k + 1], side = o.adj[3 * (size_t)k + 2];
+              if (o.pact[q] <= 0 || o.fixed[J]) continue;
+              const float* B = &f32[144 * (size_t)q];
+              for (int c = 0; c < 6; ++c) {
+                const int col = 6 * h + c;
+                const float O = side == 0 ? B[r * 12 + col] : B[col * 12 + r];
+                a += O * xv[12 * J + col];
+              }
+            }
+          acc[h] = a;
+        }
+        yv[12 * b + r] = acc[0] + acc[1];
+      }
+  };
+  // out = M32^-1 v in the order of prec
+  auto prec32 = [&](const std::vector<float>& v, std::vector<float>& out) {
+    out.assign(N, 0.f);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < ncl; ++c) {
+      const int sz = cl_ptr[c + 1] - cl_ptr[c], D = 12 * sz;
+      const float* K = &K32[cl_off[c]];
+      for (int i = 0; i < D; ++i) {
+        float acc = 0.f;
+        for (int j = 0; j < D; ++j) acc += K[(size_t)i * D + j] * v[12 * cl_body[cl_ptr[c] + j / 12] + j % 12];
+        out[12 * cl_body[cl_ptr[c] + i / 12] + i % 12] = acc;
+      }
+    }
+  };
+  // exact sum of the FP32 products, rounded once to FP64
+  auto dot32 = [&](const std::vector<float>& a, const std::vector<float>& b) {
+    XSum total;
+#pragma omp parallel
+    {
+      XSum part;
+#pragma omp for schedule(static) nowait
+      for (int i = 0; i < N; ++i) part.add((double)(a[i] * b[i]));
+#pragma omp critical
+      total.merge(part);
+    }
+    return total.round();
+  };
+  std::vector<double>& x = o.dq;
+  const std::vector<double>& bvec = o.g;
+  std::vector<double> r(N), Ax, z;
+  std::vector<float> r32(N), e32(N), z32, p32, Ap32;
+  int its = 0, sweeps = 0;
+  for (;;) {
+    spmv(o, x, Ax);
+    for (int i = 0; i < N; ++i) r[i] = bvec[i] - Ax[i];
+    prec(r, z);
+    if (ddot(r, z) <= thr2 || sweeps >= kMaxSweeps || its >= o.prm.cg_max_iter) break;
+    ++sweeps;
+    for (int i = 0; i < N; ++i) {
+      r32[i] = (float)r[i];
+      e32[i] = 0.f;
+    }
+    prec32(r32, z32);
+    double rz = dot32(r32, z32);
+    const double ithr = o.prm.refine_tol * o.prm.refine_tol * rz;
+    p32 = z32;
+    while (its < o.prm.cg_max_iter) {
+      spmv32(p32, Ap32);
+      const double pAp = dot32(p32, Ap32);
+      if (!(pAp > 0.0)) break;
+      ++its;
+      const float af = (float)(rz / pAp);
+      for (int i = 0; i < N; ++i) {
+        e32[i] = e32[i] + af * p32[i];
+        r32[i] = r32[i] - af * Ap32[i];
+      }
+      prec32(r32, z32);
+      const double rzn = dot32(r32, z32);
+      if (rzn <= ithr) break;
+      const float bf = (float)(rzn / rz);
+      for (int i = 0; i < N; ++i) p32[i] = z32[i] + bf * p32[i];
+      rz = rzn;
+    }
+    for (int i = 0; i < N; ++i) x[i] = x[i] + (double)e32[i];
+  }
+  o.last_sweeps = sweeps;
+  return its;
+}
+
 int solve(Oracle& o) {
   const int n = o.n, N = 12 * n, m = (int)o.ij.size() / 2;
+  o.last_sweeps = 0;
   // preconditioner: dense inverse of every cluster's block system
   std::vector<int> cl_ptr, cl_body;
   build_clusters(o, cl_ptr, cl_body);
@@ -1172,6 +1285,7 @@ int solve(Oracle& o) {
     return 0;
   }
   const double thr2 = o.prm.cg_tol * o.prm.cg_tol * bz;
+  if (o.prm.precision == 1) return solve_mixed(o, Kinv, cl_off, cl_ptr, cl_body, prec, thr2);
   std::vector<double> r(N), Ax;
   spmv(o, x, Ax);
   for (int i = 0; i < N; ++i) r[i] = bvec[i] - Ax[i];
@@ -1531,7 +1645,7 @@ void step(Oracle& o) {
   o.Ak = o.A0;
   o.pk = o.p0;
   double E0 = compute_energy(o, 0.0);
-  int it = 0, lin = 0, ls = 0;
+  int it = 0, lin = 0, ls = 0, sweeps = 0;
   for (;;) {
     transform(o, o.A.data(), o.p.data(), o.x.data());
     o.xk = o.x;
@@ -1547,6 +1661,7 @@ void step(Oracle& o) {
     }
     assemble(o, o.x.data(), bx, L);
     lin += solve(o);
+    sweeps += o.last_sweeps;
     // CCD (abd.py:278-303)
     update_qk(o, 1.0);
     transform(o, o.Ak.data(), o.pk.data(), o.xk.data());
@@ -1582,6 +1697,7 @@ void step(Oracle& o) {
   transform(o, o.A0.data(), o.p0.data(), o.xview.data());
   o.stat_newton = it;
   o.stat_lin = lin;
+  o.stat_refine = sweeps;
   o.stat_ls = ls;
   o.stat_energy = E0;
 }
@@ -1596,6 +1712,7 @@ extern "C" {
 struct orc_info {
   int newton_iters, linear_iters, ls_trials, n_pt, n_ee, n_vg, n_ij, n_active;
   double alpha, toi, energy;
+  int refine_iters;  // precision == 1: FP64 refinement sweeps of the step
 };
 
 void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const double* x0, const int* tris,
@@ -1668,6 +1785,7 @@ int orc_step(void* h, orc_info* info) {
     info->alpha = o->stat_alpha;
     info->toi = o->stat_toi;
     info->energy = o->stat_energy;
+    info->refine_iters = o->stat_refine;
   }
   return 0;
 }

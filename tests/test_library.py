@@ -46,3 +46,26 @@ def test_status_strings():
     L = _lib.load()
     assert L.abd_status_string(0) == b"ok"
     assert L.abd_status_string(3) == b"capacity could not be grown"
+
+
+def test_create_rejects_mixed_precision():
+    """precision 1 (FP32 Krylov inside FP64 refinement) is refused before any device work:
+    the refinement diverges on contact systems (tests/test_mixed_precision.py)."""
+    import numpy as np
+    from abd_warp_b200 import _lib, scenes
+    from abd_warp_b200.params import PRECISION_MIXED, SimParams
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libabd_b200.so not built")
+    L = _lib.load()
+    bodies, prm, _ = scenes.make_config(0)
+    f = scenes.flatten_bodies(bodies)
+    host = {k: np.ascontiguousarray(f[k], dtype=np.int32 if k in ("voff", "toff", "eoff", "tris", "edges", "fixed")
+                                    else np.float64)
+            for k in ("voff", "toff", "eoff", "x0", "tris", "edges", "mass", "I0", "fixed")}
+    hp = {k: v.ctypes.data_as(ctypes.c_void_p) for k, v in host.items()}
+    desc = _lib.SceneDesc(len(bodies), hp["voff"], hp["toff"], hp["eoff"], hp["x0"], hp["tris"], hp["edges"],
+                          hp["mass"], hp["I0"], hp["fixed"])
+    cprm = SimParams(precision=PRECISION_MIXED).to_c()
+    h = ctypes.c_void_p()
+    rc = L.abd_sim_create(ctypes.byref(desc), ctypes.byref(cprm), None, ctypes.byref(h))
+    assert rc == _lib.ABD_ERR_INVALID and not h.value
