@@ -251,7 +251,10 @@ struct Sim {
   // device pass parameters: [0] trial step, [1] = 1, [kParK] trials of a line-search batch,
   // [kParAlpha + k] their step lengths
   double* dpar = nullptr;
-  int* dint = nullptr;             // device integers: [0] preconditioner clusters
+  // device integers: [0] preconditioner clusters, [kSupHave] the line-search candidates of the
+  // last step's last CCD pass are kept, [kSupValid] they hold the current GH pass's candidates
+  int* dint = nullptr;
+  double* q_last = nullptr;        // [12 n] the DOFs (A, then p) the last step ended with
   int* hint = nullptr;             // pinned staging of dint
   // captured passes: CCD bound (with events for profiling), GH, the Krylov solve, line-search
   // batches (step lengths from the host or from the CCD pass on the device)
@@ -323,6 +326,8 @@ constexpr int kChunk = 128;       // items per chunk of the energy / CCD narrow 
 constexpr int kNbList = 32;       // neighbours per body listed by the pair mask
 constexpr int kRedSlots = 12;
 constexpr int kLsMax = 16;        // line-search trials evaluated per batch
+constexpr int kSupHave = 1;       // dint slots (see Sim::dint)
+constexpr int kSupValid = 2;
 constexpr int kSlice = 64;        // vertices per slice of the line-search bounds (two per lane)
 constexpr int kParK = 4;          // dpar slot of a batch's trial count
 constexpr int kParAlpha = 5;      // dpar slots of its step lengths
@@ -423,6 +428,10 @@ enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS
 cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
                    const double* y0, const double* y1, const abd_states* st = nullptr);
 cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y);
+// Whether the next GH pass may take its candidates from the kept line-search candidates
+// (dint[kSupValid]): mode 0 no, 2 yes (a later Newton iteration of the step), 1 when they
+// were kept (dint[kSupHave]) and the step starts from the DOFs the last step ended with.
+cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode);
 cudaError_t vg_list(Sim& s, const double* y0);
 // active pairs with their coupling weights (device list + count in dstat DS_NACTP)
 cudaError_t pair_weights(Sim& s);

@@ -55,6 +55,7 @@ struct NarrowArgs {
   int cap_ccd;
   int4* ccd_cand;
   int gh_energy;                // GH: also sum the candidates' barrier energies into energy
+  const int* sup_valid;         // GH: take the candidates from ecand instead of the traversal
   const Box* body_sup;          // CCD_LS: body boxes over every DOF set between the two
   const int* vbody;
   int cap_ecand;
@@ -583,6 +584,9 @@ template <int MODE>
 __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   constexpr bool ls = MODE == NARROW_CCD_LS;
   constexpr bool ccd = MODE == NARROW_CCD || ls, gh = MODE == NARROW_GH;
+  if constexpr (gh) {
+    if (*a.sup_valid) return;  // k_gh_scan takes the candidates from ecand
+  }
   const int c = blockIdx.x, tid = threadIdx.x;
   const int2 ch = a.chunk[c];
   const int I = ch.x;
@@ -881,6 +885,62 @@ __global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
     const double t = collision_time(c.x, x0, x1);
     if (t < 1.0) toi_min(a.toi_key, t);
   }
+}
+
+// The GH pass's candidates without a traversal, when the kept line-search candidates hold
+// every pair its culling can produce (sup_valid): the pass's DOFs lie on the segment the step's
+// last CCD pass covered (the accepted step q - alpha dq, 0 <= alpha <= 1).  Each candidate is
+// put to the GH pass's own culling predicate -- the exact body boxes overlap and the static
+// primitive boxes overlap (culling2.py:32-79, 213-227) -- and appended as the traversal would
+// append it, with its pair index from the adjacency of the point's (or lower edge's) body.
+__global__ void __launch_bounds__(128) k_gh_scan(NarrowArgs a) {
+  if (!*a.sup_valid || (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW)) return;
+  const int n = min(a.dstat[DS_NECAND], a.cap_ecand);
+  const float dhf = (float)a.prm.dhat;
+  const double dhh = 0.5 * a.prm.dhat;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int4 c = a.ecand[k];
+    const int type = c.x, pa = c.y, pb = c.z;
+    int ids[4];
+    cand_vertices(a, type, pa, pb, ids);
+    const int I = __ldg(&a.vbody[ids[0]]), J = __ldg(&a.vbody[ids[type == 0 ? 1 : 2]]);
+    if (!overlap(load_box(&a.body_box[I]), load_box(&a.body_box[J]))) continue;
+    const bool hit = type == 0 ? overlap(point_box(a.y0, nullptr, pa, dhf), tri_leaf_box(a.tris, a.y0, nullptr, pb))
+                               : overlap(edge_leaf_box(a.edges, a.y0, nullptr, pa, dhh),
+                                         edge_leaf_box(a.edges, a.y0, nullptr, pb, dhh));
+    if (!hit) continue;
+    // row I of the adjacency lists its neighbours in increasing order
+    int lo = a.row_ptr[I], hi = min(a.row_ptr[I + 1], a.cap_adj) - 1, pr = -1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1, col = a.adj_col[mid];
+      if (col == J) {
+        pr = a.adj_pair[mid];
+        break;
+      }
+      if (col < J) lo = mid + 1;
+      else hi = mid - 1;
+    }
+    if (pr < 0) continue;  // (the body boxes overlap, so the pair is listed)
+    const int swap = (type == 0 && I > J) ? 1 : 0;
+    const int pos = append_slot(&a.dstat[DS_NCCD]);
+    if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(pr, type | (swap << 1), pa, pb);
+    else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+  }
+}
+
+// Sets dint[kSupValid] (gh_superset_check); one CTA
+__global__ void k_sup_check(int n, const double* A0, const double* p0, const double* q_last, const int* have,
+                            int* valid, int mode) {
+  __shared__ int ok;
+  if (threadIdx.x == 0) ok = mode == 2 ? 1 : (mode == 1 ? (*have != 0) : 0);
+  __syncthreads();
+  if (mode == 1 && ok)
+    for (int i = threadIdx.x; i < 12 * n; i += blockDim.x) {
+      const double v = i < 9 * n ? A0[i] : p0[i - 9 * n];
+      if (__double_as_longlong(v) != __double_as_longlong(q_last[i])) ok = 0;
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) *valid = ok;
 }
 
 // Contacts of the GH pass's candidates, one thread per candidate: the active ones
@@ -1206,6 +1266,7 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.ccd_cand = s.ccd_cand;
   a.body_sup = s.body_sup;
   a.gh_energy = s.gh_energy;
+  a.sup_valid = s.dint + kSupValid;
   a.vbody = s.vbody;
   a.cap_ecand = s.cap_ecand;
   a.ecand = s.ecand;
@@ -1308,8 +1369,9 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, sizeof(int), s.stream);
       if (e != cudaSuccess) return e;
       k_chunk_narrow<NARROW_GH><<<s.nch, CT, 0, s.stream>>>(a);
+      k_gh_scan<<<kRedBlocks, 128, 0, s.stream>>>(a);
       k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
-      ++s.launches;
+      s.launches += 2;
       k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
       k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
                                                                            s.contacts_by_pair, s.dstat);
@@ -1322,6 +1384,13 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
     if (s.cap_pairs == 0) return cudaSuccess;
     k_pair_lists<<<s.cap_pairs, NT, 0, s.stream>>>(a);
   }
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode) {
+  k_sup_check<<<1, 1024, 0, s.stream>>>(s.n, st ? st->A0 : nullptr, st ? st->p0 : nullptr, s.q_last,
+                                         s.dint + kSupHave, s.dint + kSupValid, st ? mode : 0);
   ++s.launches;
   return cudaGetLastError();
 }

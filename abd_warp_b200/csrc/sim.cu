@@ -406,12 +406,16 @@ int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p,
 
 // Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner.
 // g: replay slot for the step (its key covers every capacity the captured grids depend on).
+// sup_mode (gh_superset_check): 0 the traversal finds the candidates; 1 the step's first GH
+// pass, which takes them from the kept line-search candidates when the step starts where the
+// last one ended; 2 a later Newton iteration's GH pass, which always does.
 int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active,
-          abd::GraphSlot* g = nullptr, bool with_energy = false) {
+          abd::GraphSlot* g = nullptr, bool with_energy = false, int sup_mode = 0) {
   Sim& s = h->s;
   const abd::Dofs d = direct(A, p);
   s.gh_energy = with_energy ? 1 : 0;  // read by the kernel arguments of this pass
   auto issue = [&]() -> int {
+    CK(abd::gh_superset_check(s, &st, sup_mode));
     int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
     if (r) return r;
     CK(abd::body_gh(s, st, A, p, s.x));
@@ -428,7 +432,7 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
       k.add(states_key(s, st)).add(A).add(p).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
       k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
       k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.hact);
-      k.add(s.cap_ccd).add(s.ccd_cand).add(s.gh_energy);
+      k.add(s.cap_ccd).add(s.ccd_cand).add(s.gh_energy).add(sup_mode).add(s.q_last).add(s.dint);
       r = abd::run_graph(s, *g, k.h, issue);
     } else {
       r = issue();
@@ -679,6 +683,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.dpar, abd::kNPar));
   ok(dalloc(&s.body_sup, n));
   ok(dalloc(&s.dint, 4));
+  ok(dalloc(&s.q_last, 12 * (size_t)n));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream2, cudaStreamNonBlocking);
   ok(dalloc(&s.row_cnt, n));
@@ -698,6 +703,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.kcount, 0, 4 * sizeof(int), s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.dint, 0, 4 * sizeof(int), s.stream);
   if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, ...}
     for (int k = 0; k < abd::kNPar; ++k) s.hpar[k] = 0.0;
     s.hpar[1] = 1.0;
@@ -744,7 +750,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
-                  s.body_sup, s.slice};
+                  s.body_sup, s.slice, s.q_last};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev})
@@ -760,8 +766,16 @@ int abd_sim_destroy(abd_sim* h) {
   return ABD_OK;
 }
 
+// The kept line-search candidates no longer hold the next step's first GH candidates (a pass
+// replaced them, or the parameters or states changed under them).
+static int drop_superset(abd_sim* h) {
+  CK(cudaMemsetAsync(h->s.dint + abd::kSupHave, 0, sizeof(int), h->s.stream));
+  return ABD_OK;
+}
+
 int abd_sim_set_params(abd_sim* h, const abd_params* prm) {
   if (!h || !prm || prm->precision != 0) return ABD_ERR_INVALID;
+  if (int r = drop_superset(h)) return r;
   h->s.prm = *prm;
   ++h->s.prm_version;  // parameters are kernel arguments of the captured passes
   return ABD_OK;
@@ -776,7 +790,7 @@ int abd_sim_set_stream(abd_sim* h, void* stream) {
 int abd_sim_reset(abd_sim* h) {
   if (!h) return ABD_ERR_INVALID;
   CK(cudaMemsetAsync(h->s.dq, 0, sizeof(double) * 12 * h->s.n, h->s.stream));
-  return ABD_OK;
+  return drop_superset(h);
 }
 
 static int copy_vec(abd_sim* h, double* dst, const double* src) {
@@ -868,12 +882,14 @@ extern "C" {
 
 int abd_collision_set(abd_sim* h, const double* y0, const double* y1, int counts[4]) {
   if (!h || !y0 || !counts) return ABD_ERR_INVALID;
+  if (int r = drop_superset(h)) return r;
   return cull_lists(h, nullptr, nullptr, nullptr, nullptr, const_cast<double*>(y0), const_cast<double*>(y1), counts);
 }
 
 int abd_collision_set_dofs(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1,
                            int counts[4]) {
   if (!h || !A || !p || !counts || (!A1) != (!p1)) return ABD_ERR_INVALID;
+  if (int r = drop_superset(h)) return r;
   Sim& s = h->s;
   return cull_lists(h, A, p, A1, p1, s.x, A1 ? s.xk : nullptr, counts);
 }
@@ -924,6 +940,7 @@ int abd_compute_energy(abd_sim* h, const abd_states* st, const double* Ak, const
 int abd_ccd(abd_sim* h, const double* A, const double* p, const double* A1, const double* p1, double* alpha,
             double* raw) {
   if (!h || !A || !p || !A1 || !p1 || !alpha) return ABD_ERR_INVALID;
+  if (int r = drop_superset(h)) return r;  // the CCD pass clears the candidate count
   return ccd_at(h, A, p, A1, p1, alpha, raw);
 }
 
@@ -933,6 +950,7 @@ int abd_energies_along(abd_sim* h, const abd_states* st, const double* A, const 
   for (int k = 0; k < K; ++k)
     if (!(alphas[k] >= 0.0 && alphas[k] <= 1.0)) return ABD_ERR_INVALID;
   if (K == 0) return ABD_OK;
+  if (int r = drop_superset(h)) return r;  // the pass replaces the kept candidates
   Sim& s = h->s;
   double a1 = 0.0, raw = 0.0;
   int r = ccd_of(h, direct(A, p), updated(s, A, p, 1, st->Ak, st->pk), &a1, &raw, []() -> int { return ABD_OK; },
@@ -959,8 +977,11 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
   int it = 0;
   for (;;) {
     int nact = 0;
-    // the step's first GH pass also gives the energy at q0 (its own replay slot)
-    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0))) return r;
+    // the step's first GH pass also gives the energy at q0 (its own replay slot); the GH
+    // passes take their candidates from the last CCD pass's line-search candidates (which the
+    // step's CCD passes then replace: the first pass's kept list is consumed)
+    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2))) return r;
+    if (it == 0) CK(cudaMemsetAsync(s.dint + abd::kSupHave, 0, sizeof(int), s.stream));
     if (it == 0) {
       // the energy at q0 (abd.py:126-128): the GH pass at q0 sums the same terms as an
       // energy pass there
@@ -1021,6 +1042,11 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     if (gTg < P.tol || it >= P.max_iter) break;
   }
   CK(abd::finish_step(s, st, x_view));
+  // the last CCD pass's line-search candidates hold the next step's first GH candidates when
+  // that step starts from these DOFs
+  CK(cudaMemcpyAsync(s.q_last, st.A, nA, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaMemcpyAsync(s.q_last + 9 * (size_t)s.n, st.p, np, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaMemsetAsync(s.dint + abd::kSupHave, 1, 1, s.stream));
   inf.newton_iters = it;
   inf.energy = E0;
   inf.status = take_status(h);
