@@ -344,7 +344,7 @@ enum : int {
   DS_SOLVER_ITERS = 6,
   DS_NPAIRS = 7,     // body pairs of the last culling pass
   DS_NADJ = 8,       // adjacency entries (2 x pairs)
-  DS_NACTP = 9,      // active pairs appended by pair_weights
+  DS_NACTP = 9,      // active pairs appended by the pair assembly
   DS_NCONTACT = 12,  // active contacts appended by the GH pass
   DS_IT = 13,        // Krylov iteration counter (device-side, for replayed blocks)
   DS_NCCD = 14,      // CCD candidates appended by the CCD pass
@@ -433,8 +433,6 @@ cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double*
 // were kept (dint[kSupHave]) and the step starts from the DOFs the last step ended with.
 cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode);
 cudaError_t vg_list(Sim& s, const double* y0);
-// active pairs with their coupling weights (device list + count in dstat DS_NACTP)
-cudaError_t pair_weights(Sim& s);
 cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
                         double* pout);

@@ -56,6 +56,8 @@ struct NarrowArgs {
   int4* ccd_cand;
   int gh_energy;                // GH: also sum the candidates' barrier energies into energy
   const int* sup_valid;         // GH: take the candidates from ecand instead of the traversal
+  int cap_act;
+  int4* act_pairs;              // GH: active pairs with their coupling weights (preconditioner)
   const Box* body_sup;          // CCD_LS: body boxes over every DOF set between the two
   const int* vbody;
   int cap_ecand;
@@ -505,6 +507,23 @@ __global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
         a.pdiag[(size_t)p * 288 + (e - 144)] = v;
       } else {
         a.pgrad[(size_t)p * 24 + (e - 432)] = v;
+      }
+    }
+    // an active pair of two free bodies joins the preconditioner's clustering with the
+    // Frobenius norm of H_IJ as its weight (summed in row order, then rounded to FP32)
+    __syncthreads();  // H_IJ is in global memory
+    if (tid == 0) {
+      const int2 ij = a.ij[p];
+      if (!a.fixed[ij.x] && !a.fixed[ij.y]) {
+        double f = 0.0;
+        const double* O = a.offdiag + (size_t)p * 288;
+        for (int k = 0; k < 144; ++k) f += O[k] * O[k];
+        const float w = (float)sqrt(f);
+        if (w > 0.f) {
+          const int pos = atomicAdd(&a.dstat[DS_NACTP], 1);
+          if (pos < a.cap_act) a.act_pairs[pos] = make_int4(p, ij.x, ij.y, __float_as_int(w));
+          else atomicOr(&a.dstat[DS_STATUS], ST_ACT_OVERFLOW);
+        }
       }
     }
   }
@@ -1267,6 +1286,8 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.body_sup = s.body_sup;
   a.gh_energy = s.gh_energy;
   a.sup_valid = s.dint + kSupValid;
+  a.cap_act = s.cap_act;
+  a.act_pairs = s.act_pairs;
   a.vbody = s.vbody;
   a.cap_ecand = s.cap_ecand;
   a.ecand = s.ecand;
@@ -1375,6 +1396,7 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
       k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
                                                                            s.contacts_by_pair, s.dstat);
+      if ((e = cudaMemsetAsync(s.dstat + DS_NACTP, 0, sizeof(int), s.stream)) != cudaSuccess) return e;
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
       static_assert(smem + sizeof(double) * PT_WARPS * 5 * 24 + 256 <= 48 * 1024, "pair assembly shared memory");
       k_pair_assemble<<<s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148, PT_THREADS, smem, s.stream>>>(a);

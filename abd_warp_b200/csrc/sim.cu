@@ -419,7 +419,6 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
     int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
     if (r) return r;
     CK(abd::body_gh(s, st, A, p, s.x));
-    CK(abd::pair_weights(s));
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     if (s.cap_act > 0)
       CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));

@@ -487,23 +487,6 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, c
   }
 }
 
-// Active pairs of the last GH pass (contacts, both bodies free) with the Frobenius norm of
-// their coupling block, appended to a list in any order (the host sorts it)
-__global__ void k_pair_weights(int cap_pairs, const int* dstat_np, const int2* ij, const int* pair_active,
-                               const int* fixed, const double* offdiag, int cap_act, int4* act, int* dstat) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= cap_pairs || p >= *dstat_np) return;
-  if (!(pair_active[p] > 0 && !fixed[ij[p].x] && !fixed[ij[p].y])) return;
-  double f = 0.0;
-  const double* O = offdiag + (size_t)p * 288;
-  for (int k = 0; k < 144; ++k) f += O[k] * O[k];
-  const float w = (float)sqrt(f);
-  if (!(w > 0.f)) return;
-  const int pos = atomicAdd(&dstat[DS_NACTP], 1);
-  if (pos < cap_act) act[pos] = make_int4(p, ij[p].x, ij[p].y, __float_as_int(w));
-  else atomicOr(&dstat[DS_STATUS], ST_ACT_OVERFLOW);
-}
-
 // Threshold thr^2 = tol^2 b^T M^-1 b and the recurrence scalars; b = 0 gives x = 0 and ends
 // the solve before its first iteration
 __global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, double* x) {
@@ -544,16 +527,6 @@ SolverArgs solver_args(Sim& s) {
 }
 
 }  // namespace
-
-cudaError_t pair_weights(Sim& s) {
-  cudaError_t e = cudaMemsetAsync(s.dstat + DS_NACTP, 0, sizeof(int), s.stream);
-  if (e != cudaSuccess || s.cap_pairs == 0) return e;
-  k_pair_weights<<<(s.cap_pairs + 255) / 256, 256, 0, s.stream>>>(s.cap_pairs, s.dstat + DS_NPAIRS, s.ij,
-                                                                  s.pair_active, s.fixed, s.offdiag, s.cap_act,
-                                                                  s.act_pairs, s.dstat);
-  ++s.launches;
-  return cudaGetLastError();
-}
 
 // Clusters and their dense inverses, from the active-pair list the host read at its last
 // sync (s.hact, count in the dstat mirror).  Same clustering rule as the oracle: greedy
