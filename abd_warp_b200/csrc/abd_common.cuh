@@ -269,6 +269,11 @@ struct Sim {
   int prof_events = 0;             // this pass records the events
   long long prof_tick = 0;
   cudaEvent_t prof_ev[2] = {nullptr, nullptr};
+  // recorded by the GH pass once the active-pair list is on the host (before the body terms)
+  cudaEvent_t act_ev = nullptr;
+  // fork / join of a side branch in a captured pass (the CCD pass's dot products)
+  cudaEvent_t fork_ev[2] = {nullptr, nullptr};
+  bool fork_open = false;
   double prof_ms = 0.0, prof_bytes = 0.0;
   long long prof_launches = 0;
   double* hpar = nullptr;          // pinned staging of dpar
@@ -303,9 +308,14 @@ struct Sim {
   // Krylov work vectors [n][12]
   double *r = nullptr, *rh = nullptr, *pv = nullptr, *v = nullptr, *y = nullptr, *s = nullptr, *z = nullptr,
          *t = nullptr, *ddq = nullptr;
-  // preconditioner clusters (contact-coupled bodies, <= cluster_max each)
+  // preconditioner clusters (contact-coupled bodies, <= cluster_max each): the tables live in
+  // one device block (ClusterTables layout) with a pinned copy in hstage
   int ncl = 0, max_cl = 1;
+  size_t cl_bytes = 0;                           // bytes of the tables in use
+  int cl_smem = 0;                               // dynamic shared memory opted in for the inverse
+  void* cl_tab = nullptr;
   int *cl_ptr = nullptr, *cl_body = nullptr;     // [ncl+1], [n]
+  int *body_cl = nullptr, *ncl_dev = nullptr;    // [n], [1]
   long long* cl_off = nullptr;                   // [ncl+1] offsets into cl_inv (doubles)
   double* cl_inv = nullptr;                      // dense inverses of the cluster systems
   size_t cap_cl_inv = 0;
@@ -316,10 +326,45 @@ struct Sim {
   int* dstat = nullptr;            // = box->dstat: [0] status, [1..] counters
   int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
   void* hstage = nullptr;          // pinned staging of the preconditioner's cluster tables
+                                   // (hint[2]: the GH pass's active-pair count, -1 until copied)
   size_t cap_hstage = 0;
   double* hval = nullptr;          // pinned host scalars
   unsigned long long* dmin = nullptr;  // = &box->toi_key
 };
+
+// Records ev on st: while st is capturing, as a graph node that records it on every replay
+// (which the host can wait for), else directly
+inline cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const cudaError_t e = cudaStreamIsCapturing(st, &cs);
+  if (e != cudaSuccess) return e;
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+                                             : cudaEventRecord(ev, st);
+}
+
+// The preconditioner's cluster tables, laid out the same in the pinned staging block and on
+// the device so that one copy moves them: the cluster count, cl_ptr [n+1], cl_body [n] and
+// body_cl [n] (ints), then cl_off [n+1] (long longs, 8-byte aligned)
+struct ClusterTables {
+  int *ncl, *cl_ptr, *cl_body, *body_cl;
+  long long* cl_off;
+  size_t off_bytes;  // byte offset of cl_off
+  size_t bytes_through(int ncl_) const { return off_bytes + sizeof(long long) * ((size_t)ncl_ + 1); }
+};
+inline size_t cluster_tables_bytes(int n) {
+  return ((sizeof(int) * (3 * (size_t)n + 3) + 7) & ~(size_t)7) + sizeof(long long) * ((size_t)n + 1);
+}
+inline ClusterTables cluster_tables_at(void* base, int n) {
+  ClusterTables t;
+  int* b = static_cast<int*>(base);
+  t.ncl = b;
+  t.cl_ptr = b + 2;
+  t.cl_body = b + 3 + n;
+  t.body_cl = b + 3 + 2 * (size_t)n;
+  t.off_bytes = (sizeof(int) * (3 * (size_t)n + 3) + 7) & ~(size_t)7;
+  t.cl_off = reinterpret_cast<long long*>(static_cast<char*>(base) + t.off_bytes);
+  return t;
+}
 
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs: fixed grid of every reduction kernel
 constexpr int kChunk = 128;       // items per chunk of the energy / CCD narrow passes
@@ -438,8 +483,9 @@ cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* 
                         double* pout);
 cudaError_t finish_step(Sim& s, const abd_states& st, double* xview);
 // exact dot products a.b (and c.d when c != null) of [n][12] vectors into out_dev[0], [1]
-// (reduction slots 10 and 11)
-cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev);
+// (reduction slots 10 and 11), on stream st (the pass's stream when null)
+cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev,
+                 cudaStream_t st = nullptr);
 
 // linesearch.cu
 // Energies at (A, p) - alpha_k dq for the dpar[kParK] step lengths dpar[kParAlpha + k] in
@@ -450,7 +496,13 @@ cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const dou
 cudaError_t ls_setup_from_ccd(Sim& s);
 
 // solver.cu
-int build_preconditioner(Sim& s);                 // returns ABD status
+// The preconditioner: cluster_tables forms the clusters on the host from the first nact
+// entries of the active-pair list (hact) into the pinned tables; cluster_inverse uploads them
+// and inverts each cluster's system on the device; build_preconditioner does both with the
+// count of the last mailbox read.  ABD status.
+int cluster_tables(Sim& s, int nact);
+int cluster_inverse(Sim& s);
+int build_preconditioner(Sim& s);
 // returns ABD status; iters == null: enqueue only (krylov_outcome after the next mailbox read)
 int krylov_solve(Sim& s, double* x, int* iters);
 int krylov_outcome(Sim& s);                       // iterations of the last solve

@@ -1373,10 +1373,10 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if (e != cudaSuccess) return e;
       if (mode == NARROW_CCD_LS) {
         if (!a.y1) return cudaErrorInvalidValue;
-        if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[0], s.stream, cudaEventRecordExternal))
+        if (s.prof_events && record_event(s.prof_ev[0], s.stream))
           return cudaErrorUnknown;
         k_chunk_narrow<NARROW_CCD_LS><<<s.nch, CT, 0, s.stream>>>(a);
-        if (s.prof_events && cudaEventRecordWithFlags(s.prof_ev[1], s.stream, cudaEventRecordExternal))
+        if (s.prof_events && record_event(s.prof_ev[1], s.stream))
           return cudaErrorUnknown;
         k_ccd_eval<true><<<kRedBlocks, 128, 0, s.stream>>>(a);
       } else {
@@ -1460,9 +1460,10 @@ cudaError_t finish_step(Sim& s, const abd_states& st, double* xview) {
   return transform(s, st.A0, st.p0, xview);
 }
 
-cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev) {
+cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, const double* d, double* out_dev,
+                 cudaStream_t st) {
   static_assert(2 * kRedDot <= 2 * kRedBlocks, "dot partials fit two reduction slots");
-  k_dots<<<kRedDot, 256, 0, s.stream>>>(12 * s.n, a, b, c, d, s.partials + 10 * (size_t)kRedBlocks,
+  k_dots<<<kRedDot, 256, 0, st ? st : s.stream>>>(12 * s.n, a, b, c, d, s.partials + 10 * (size_t)kRedBlocks,
                                         s.red_count + 10, out_dev);
   ++s.launches;
   return cudaGetLastError();

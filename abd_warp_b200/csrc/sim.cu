@@ -294,7 +294,8 @@ int no_post() { return ABD_OK; }
 
 // CCD bound between DOFs d0 and d1 (ccd, abd.py:278-303); positions land in x, xk.  pre()
 // enqueues work that belongs to the same pass (the step's dot products, whose results ride
-// along in the mailbox); post() enqueues work that follows it before the host's wait (the
+// along in the mailbox), possibly on a branch it forks (s.fork_open), joined before the
+// mailbox copy; post() enqueues work that follows it before the host's wait (the
 // step's first line-search batch).  mode NARROW_CCD_LS also collects the line-search
 // candidates between d0 and d1.
 template <class Pre, class Post = int (*)()>
@@ -302,9 +303,14 @@ int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, 
            abd::GraphSlot* g = nullptr, uint64_t key = 0, int mode = abd::NARROW_CCD, Post&& post = no_post) {
   Sim& s = h->s;
   auto issue = [&]() -> int {
+    s.fork_open = false;
     int r = pre();
     if (r) return r;
     if ((r = culling(h, &d0, &d1, s.x, s.xk, mode))) return r;
+    if (s.fork_open) {  // join the branch pre() forked
+      CK(cudaStreamWaitEvent(s.stream, s.fork_ev[1], 0));
+      s.fork_open = false;
+    }
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
@@ -405,12 +411,16 @@ int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p,
 }
 
 // Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner.
+// The list and its count (hint[2]) reach the host before the body terms are computed: the
+// pass records act_ev there, and mid() runs on the host after it while the device finishes
+// the pass (the step forms the preconditioner's clusters in it).
 // g: replay slot for the step (its key covers every capacity the captured grids depend on).
 // sup_mode (gh_superset_check): 0 the traversal finds the candidates; 1 the step's first GH
 // pass, which takes them from the kept line-search candidates when the step starts where the
 // last one ended; 2 a later Newton iteration's GH pass, which always does.
+template <class Mid = int (*)()>
 int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active,
-          abd::GraphSlot* g = nullptr, bool with_energy = false, int sup_mode = 0) {
+          abd::GraphSlot* g = nullptr, bool with_energy = false, int sup_mode = 0, Mid&& mid = no_post) {
   Sim& s = h->s;
   const abd::Dofs d = direct(A, p);
   s.gh_energy = with_energy ? 1 : 0;  // read by the kernel arguments of this pass
@@ -418,10 +428,12 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
     CK(abd::gh_superset_check(s, &st, sup_mode));
     int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
     if (r) return r;
-    CK(abd::body_gh(s, st, A, p, s.x));
-    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     if (s.cap_act > 0)
       CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
+    CK(cudaMemcpyAsync(s.hint + 2, s.dstat + abd::DS_NACTP, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    CK(abd::record_event(s.act_ev, s.stream));
+    CK(abd::body_gh(s, st, A, p, s.x));
+    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
   for (int tries = 0;; ++tries) {
@@ -432,11 +444,18 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
       k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
       k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.hact);
       k.add(s.cap_ccd).add(s.ccd_cand).add(s.gh_energy).add(sup_mode).add(s.q_last).add(s.dint);
+      s.hint[2] = -1;  // replaced by the pass's copy of the count
       r = abd::run_graph(s, *g, k.h, issue);
     } else {
+      s.hint[2] = -1;
       r = issue();
     }
     if (r) return r;
+    CK(cudaEventSynchronize(s.act_ev));
+    // the count's copy precedes the event and follows the list's: once it has landed, the list
+    // on the host is this pass's (otherwise wait for the whole pass)
+    if (*static_cast<volatile int*>(s.hint + 2) < 0) CK(cudaStreamSynchronize(s.stream));
+    if ((r = mid())) return r;
     CK(cudaStreamSynchronize(s.stream));
     std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
     s.n_pairs = s.hstat[abd::DS_NPAIRS];
@@ -664,9 +683,15 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.upper_ptr, n + 1));
   for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq, &s.zb})
     ok(dalloc(v, 12 * (size_t)n));
-  ok(dalloc(&s.cl_ptr, n + 1));
-  ok(dalloc(&s.cl_body, n));
-  ok(dalloc(&s.cl_off, n + 1));
+  s.cap_hstage = abd::cluster_tables_bytes(n);
+  if (ok(cudaMalloc(&s.cl_tab, s.cap_hstage))) {
+    const abd::ClusterTables t = abd::cluster_tables_at(s.cl_tab, n);
+    s.cl_ptr = t.cl_ptr;
+    s.cl_body = t.cl_body;
+    s.body_cl = t.body_cl;
+    s.ncl_dev = t.ncl;
+    s.cl_off = t.cl_off;
+  }
   ok(dalloc(&s.diag, 144 * (size_t)n));
   ok(dalloc(&s.Minv, 144 * (size_t)n));
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
@@ -685,6 +710,8 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.q_last, 12 * (size_t)n));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream2, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&s.act_ev, &s.fork_ev[0], &s.fork_ev[1]})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   ok(dalloc(&s.row_cnt, n));
   ok(dalloc(&s.nbr, (size_t)n * abd::kNbList));
   ok(dalloc(&s.fdof, 24 * (size_t)n));
@@ -695,14 +722,14 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, abd::kNPar * sizeof(double), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hint, 4 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 32 * sizeof(double), cudaHostAllocDefault);
-  // preconditioner tables: cl_ptr, cl_body, body_cl (ints), cl_off (8-byte aligned long longs)
-  s.cap_hstage = sizeof(int) * (3 * (size_t)n + 2) + sizeof(long long) * ((size_t)n + 2);
+  // the preconditioner's cluster tables (the device block's layout)
   if (e == cudaSuccess) e = cudaHostAlloc(&s.hstage, s.cap_hstage, cudaHostAllocDefault);
   if (e == cudaSuccess) e = abd::rest_boxes(s);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.kcount, 0, 4 * sizeof(int), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dint, 0, 4 * sizeof(int), s.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.cl_tab, 0, sizeof(int), s.stream);
   if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, ...}
     for (int k = 0; k < abd::kNPar; ++k) s.hpar[k] = 0.0;
     s.hpar[1] = 1.0;
@@ -747,7 +774,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.pair_active, s.pair_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.dint,
                   s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
-                  s.zb, s.cl_ptr, s.cl_body, s.cl_off, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
+                  s.zb, s.cl_tab, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
                   s.body_sup, s.slice, s.q_last};
   for (void* q : bufs)
@@ -756,7 +783,7 @@ int abd_sim_destroy(abd_sim* h) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
   if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
   if (s.cap_stream2) cudaStreamDestroy(s.cap_stream2);
-  for (cudaEvent_t ev : s.prof_ev)
+  for (cudaEvent_t ev : {s.prof_ev[0], s.prof_ev[1], s.act_ev, s.fork_ev[0], s.fork_ev[1]})
     if (ev) cudaEventDestroy(ev);
   for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar,
                   (void*)s.hint})
@@ -979,7 +1006,10 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     // the step's first GH pass also gives the energy at q0 (its own replay slot); the GH
     // passes take their candidates from the last CCD pass's line-search candidates (which the
     // step's CCD passes then replace: the first pass's kept list is consumed)
-    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2))) return r;
+    // the preconditioner's clusters are formed on the host while the pass's body terms run
+    auto clusters = [&]() -> int { return abd::cluster_tables(s, s.hint[2]); };
+    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2, clusters)))
+      return r;
     if (it == 0) CK(cudaMemsetAsync(s.dint + abd::kSupHave, 0, sizeof(int), s.stream));
     if (it == 0) {
       // the energy at q0 (abd.py:126-128): the GH pass at q0 sums the same terms as an
@@ -991,13 +1021,19 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
       inf.n_ij = s.n_pairs;
     }
     inf.n_active = nact;
-    if ((r = abd::build_preconditioner(s))) return r;
+    if ((r = abd::cluster_inverse(s))) return r;
     if ((r = abd::krylov_solve(s, s.dq, nullptr))) return r;  // outcome read with the CCD pass
     // dq.g, g.g (abd.py:148, 265) and the CCD bound between q and q - dq (abd.py:278-303),
     // one pass; Ak, pk = q - dq
     double alpha;
+    // (on a branch of their own beside the pass's culling, which neither reads g nor writes
+    // what they write)
     auto dots = [&]() -> int {
-      CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots));
+      CK(cudaEventRecord(s.fork_ev[0], s.stream));
+      CK(cudaStreamWaitEvent(s.cap_stream2, s.fork_ev[0], 0));
+      CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots, s.cap_stream2));
+      CK(cudaEventRecord(s.fork_ev[1], s.cap_stream2));
+      s.fork_open = true;
       return ABD_OK;
     };
     // the CCD pass and the line search's first batch (its step lengths from the pass's time of

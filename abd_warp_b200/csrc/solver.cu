@@ -513,7 +513,7 @@ SolverArgs solver_args(Sim& s) {
   a.fixed = s.fixed;
   a.ij = s.ij;
   a.ncl = s.ncl;
-  a.ncl_dev = s.dint;
+  a.ncl_dev = s.ncl_dev;
   a.maxit = s.prm.cg_max_iter;
   a.cl_ptr = s.cl_ptr;
   a.cl_body = s.cl_body;
@@ -528,35 +528,34 @@ SolverArgs solver_args(Sim& s) {
 
 }  // namespace
 
-// Clusters and their dense inverses, from the active-pair list the host read at its last
-// sync (s.hact, count in the dstat mirror).  Same clustering rule as the oracle: greedy
+// Clusters of the preconditioner from the first nact entries of the active-pair list on the
+// host (s.hact), into the pinned tables.  Same clustering rule as the oracle: greedy
 // union-find, strongest coupling first (FP32 Frobenius norm of H_IJ, ties by pair index), at
-// most cluster_max bodies per cluster.  Tables go up through pinned staging without a sync.
-int build_preconditioner(Sim& s) {
+// most cluster_max bodies per cluster.  Host work only: it may run while the device is busy.
+int cluster_tables(Sim& s, int nact) {
   const int n = s.n;
   const int cap = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
   std::vector<int> parent(n), size(n, 1);
   std::iota(parent.begin(), parent.end(), 0);
-  const int nact = std::min(s.hstat[DS_NACTP], s.cap_act);
+  nact = std::max(0, std::min(nact, s.cap_act));
   if (cap > 1 && nact > 0) {
-    std::vector<int> order(nact);
-    std::iota(order.begin(), order.end(), 0);
-    const int4* L = s.hact;
-    auto weight = [&](int k) {
-      float f;
-      std::memcpy(&f, &L[k].w, sizeof(float));
-      return f;
+    // (weight descending, pair ascending) as one 64-bit key: the weights are positive FP32
+    // values, whose bit patterns order like the values themselves
+    struct Entry {
+      unsigned long long key;
+      int k;
     };
-    std::sort(order.begin(), order.end(), [&](int x, int y) {
-      const float wx = weight(x), wy = weight(y);
-      return wx > wy || (wx == wy && L[x].x < L[y].x);
-    });
+    const int4* L = s.hact;
+    std::vector<Entry> order(nact);
+    for (int k = 0; k < nact; ++k)
+      order[k] = {((unsigned long long)(~(unsigned)L[k].w) << 32) | (unsigned)L[k].x, k};
+    std::sort(order.begin(), order.end(), [](const Entry& x, const Entry& y) { return x.key < y.key; });
     auto find = [&](int x) {
       while (parent[x] != x) x = parent[x] = parent[parent[x]];
       return x;
     };
-    for (int k : order) {
-      const int a = find(L[k].y), b = find(L[k].z);
+    for (const Entry& e : order) {
+      const int a = find(L[e.k].y), b = find(L[e.k].z);
       if (a == b || size[a] + size[b] > cap) continue;
       if (a < b) {
         parent[b] = a;
@@ -569,10 +568,7 @@ int build_preconditioner(Sim& s) {
     for (int b = 0; b < n; ++b) parent[b] = find(b);
   }
   // clusters ordered by their first body, members in increasing order
-  int* cl_ptr = reinterpret_cast<int*>(s.hstage);          // [n+1]
-  int* cl_body = cl_ptr + (n + 1);                          // [n]
-  int* body_cl = cl_body + n;                               // [n]
-  long long* cl_off = reinterpret_cast<long long*>(body_cl + n + ((3 * n + 1) & 1));  // [n+1], 8-aligned
+  const ClusterTables t = cluster_tables_at(s.hstage, n);
   std::vector<int> first(n, -1), csize;
   for (int b = 0; b < n; ++b) {
     const int r = parent[b];
@@ -583,47 +579,57 @@ int build_preconditioner(Sim& s) {
     ++csize[first[r]];
   }
   const int ncl = (int)csize.size();
-  cl_ptr[0] = 0;
-  cl_off[0] = 0;
+  t.cl_ptr[0] = 0;
+  t.cl_off[0] = 0;
   int max_cl = 1;
   for (int c = 0; c < ncl; ++c) {
-    cl_ptr[c + 1] = cl_ptr[c] + csize[c];
+    t.cl_ptr[c + 1] = t.cl_ptr[c] + csize[c];
     const long long d = 12LL * csize[c];
-    cl_off[c + 1] = cl_off[c] + d * d;
+    t.cl_off[c + 1] = t.cl_off[c] + d * d;
     max_cl = std::max(max_cl, csize[c]);
   }
   std::vector<int> fill(ncl, 0);
   for (int b = 0; b < n; ++b) {
     const int c = first[parent[b]];
-    cl_body[cl_ptr[c] + fill[c]++] = b;
-    body_cl[b] = c;
+    t.cl_body[t.cl_ptr[c] + fill[c]++] = b;
+    t.body_cl[b] = c;
   }
+  *t.ncl = ncl;
   s.ncl = ncl;
   s.max_cl = max_cl;
-  const size_t need = (size_t)cl_off[ncl];
+  s.cl_bytes = t.bytes_through(ncl);
+  return ABD_OK;
+}
+
+// Uploads the tables cluster_tables made (one copy) and inverts every cluster's dense system.
+// Enqueued without a sync.
+int cluster_inverse(Sim& s) {
+  const ClusterTables t = cluster_tables_at(s.hstage, s.n);
+  const size_t need = (size_t)t.cl_off[s.ncl];
   if (need > s.cap_cl_inv) {
     if (s.cl_inv) cudaFree(s.cl_inv);
+    s.cl_inv = nullptr;
     s.cap_cl_inv = std::max(need, 2 * s.cap_cl_inv);
     if (cudaMalloc(&s.cl_inv, sizeof(double) * s.cap_cl_inv) != cudaSuccess) return ABD_ERR_OVERFLOW;
   }
-  // body -> cluster map rides in the scratch vector zb (as ints) during the setup kernel
-  int* body_cl_dev = reinterpret_cast<int*>(s.zb);
-  s.hint[0] = ncl;
-  if (cudaMemcpyAsync(s.dint, s.hint, sizeof(int), cudaMemcpyHostToDevice, s.stream) ||
-      cudaMemcpyAsync(s.cl_ptr, cl_ptr, sizeof(int) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
-      cudaMemcpyAsync(s.cl_body, cl_body, sizeof(int) * n, cudaMemcpyHostToDevice, s.stream) ||
-      cudaMemcpyAsync(s.cl_off, cl_off, sizeof(long long) * (ncl + 1), cudaMemcpyHostToDevice, s.stream) ||
-      cudaMemcpyAsync(body_cl_dev, body_cl, sizeof(int) * n, cudaMemcpyHostToDevice, s.stream))
-    return ABD_ERR_CUDA;
+  if (cudaMemcpyAsync(s.cl_tab, s.hstage, s.cl_bytes, cudaMemcpyHostToDevice, s.stream)) return ABD_ERR_CUDA;
   SolverArgs a = solver_args(s);
-  const size_t smem = sizeof(double) * 144 * (size_t)max_cl * max_cl;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return ABD_ERR_CUDA;
+  const size_t smem = sizeof(double) * 144 * (size_t)s.max_cl * s.max_cl;
+  if (smem > 48 * 1024 && (int)smem > s.cl_smem) {
+    if (cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return ABD_ERR_CUDA;
+    s.cl_smem = (int)smem;
+  }
   const int grid = std::min(s.ncl, 4 * 148);
-  k_cluster_inverse<<<grid, IT, smem, s.stream>>>(a, 0, s.ncl, body_cl_dev);
+  k_cluster_inverse<<<grid, IT, smem, s.stream>>>(a, 0, s.ncl, s.body_cl);
   ++s.launches;
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+}
+
+int build_preconditioner(Sim& s) {
+  const int r = cluster_tables(s, s.hstat[DS_NACTP]);
+  return r ? r : cluster_inverse(s);
 }
 
 // Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  One replayed graph:
