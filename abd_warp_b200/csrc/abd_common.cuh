@@ -247,7 +247,6 @@ struct Sim {
   int* nbr = nullptr;              // [n][kNbList] first neighbours of each body (pair mask)
   float* fdof = nullptr;           // [n][2][12] FP32 DOFs of the last broad phase
   int* upper_cnt = nullptr;        // [n] neighbours J > I
-  int* kcount = nullptr;           // [4] last-CTA counters of single-pass kernels
   // device pass parameters: [0] trial step, [1] = 1, [kParK] trials of a line-search batch,
   // [kParAlpha + k] their step lengths
   double* dpar = nullptr;
@@ -303,8 +302,7 @@ struct Sim {
 
 
   // Newton system
-  double *g = nullptr, *dq = nullptr, *diag = nullptr, *Minv = nullptr;  // [n][12], [n][144]
-  float *diag32 = nullptr, *off32 = nullptr, *Minv32 = nullptr;          // mixed precision copies
+  double *g = nullptr, *dq = nullptr, *diag = nullptr;  // [n][12], [n][12], [n][144]
   // Krylov work vectors [n][12]
   double *r = nullptr, *rh = nullptr, *pv = nullptr, *v = nullptr, *y = nullptr, *s = nullptr, *z = nullptr,
          *t = nullptr, *ddq = nullptr;

@@ -693,7 +693,6 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     s.cl_off = t.cl_off;
   }
   ok(dalloc(&s.diag, 144 * (size_t)n));
-  ok(dalloc(&s.Minv, 144 * (size_t)n));
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
   ok(dalloc(&s.red_count, abd::kRedSlots));
   ok(dalloc(&s.scal, 32));
@@ -716,7 +715,6 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.nbr, (size_t)n * abd::kNbList));
   ok(dalloc(&s.fdof, 24 * (size_t)n));
   ok(dalloc(&s.upper_cnt, n));
-  ok(dalloc(&s.kcount, 4));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hbox, sizeof(abd::Mailbox), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, abd::kNPar * sizeof(double), cudaHostAllocDefault);
@@ -727,7 +725,6 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = abd::rest_boxes(s);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s.kcount, 0, 4 * sizeof(int), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dint, 0, 4 * sizeof(int), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.cl_tab, 0, sizeof(int), s.stream);
   if (e == cudaSuccess) {  // dpar = {trial step, 1 (the full step of the CCD bound), 0, ...}
@@ -771,9 +768,9 @@ int abd_sim_destroy(abd_sim* h) {
   void* bufs[] = {s.voff, s.toff, s.eoff, s.vbody, s.tbody, s.ebody, s.tris, s.edges, s.x0, s.mass, s.I0,
                   s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
-                  s.pair_active, s.pair_val, s.g, s.dq, s.diag, s.Minv, s.diag32, s.off32, s.Minv32,
+                  s.pair_active, s.pair_val, s.g, s.dq, s.diag,
                   s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.dint,
-                  s.row_cnt, s.upper_cnt, s.kcount, s.nbr, s.fdof, s.chunk_box, s.vperm,
+                  s.row_cnt, s.upper_cnt, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_tab, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
                   s.body_sup, s.slice, s.q_last};
