@@ -1,0 +1,245 @@
+"""The full IPC contact model (closest-feature classification, barrier on the classified
+distance, edge-edge mollifier, PSD projection, mapping to affine DOFs) in
+``abd_warp_b200/csrc/abd_ipc_full.cuh``, built for the host and checked against the numpy
+restatement ``oracle/ipc_full_ref.py``, brute-force sampling, central differences and, on
+interior contacts, the reference's own contact model (``oracle.contact_gh``).  CPU only."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import ipc_full_ref as R
+from abd_warp_b200.params import SimParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DH, KAPPA = 0.01, 1e3  # dhat^2 and stiffness of these unit-scale tests
+
+
+@pytest.fixture(scope="module")
+def L(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("ipcf") / "libipcf.so")
+    src = os.path.join(HERE, "native", "ipc_full_host.cpp")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-o", out, src], check=True)
+    lib = ctypes.CDLL(out)
+    v, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.ipcf_type.argtypes = [i, v]
+    lib.ipcf_type.restype = i
+    lib.ipcf_d2.argtypes = [i, i, v]
+    lib.ipcf_d2.restype = d
+    lib.ipcf_energy.argtypes = [i, v, v, d, d]
+    lib.ipcf_energy.restype = d
+    lib.ipcf_local_gh.argtypes = [i, v, v, d, d, v, v, v, v, v]
+    lib.ipcf_local_gh.restype = i
+    lib.ipcf_project_psd12.argtypes = [v]
+    lib.ipcf_to_affine.argtypes = [v, v, v, i, v, v, v, v]
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _x(a):
+    return np.ascontiguousarray(a, dtype=np.float64).ravel()
+
+
+def local_gh(L, kind, x, r):
+    x, r = _x(x), _x(r)
+    ty, d2, E = ctypes.c_int(0), ctypes.c_double(0), ctypes.c_double(0)
+    g, H = np.zeros(12), np.zeros(144)
+    ok = L.ipcf_local_gh(kind, _p(x), _p(r), DH, KAPPA, ctypes.byref(ty), ctypes.byref(d2), ctypes.byref(E), _p(g),
+                         _p(H))
+    return bool(ok), ty.value, d2.value, E.value, g, H.reshape(12, 12)
+
+
+def random_pair(rng, kind, scale=1.0):
+    """A random unit-scale triangle and point, or two edges."""
+    return rng.normal(size=(4, 3)) * scale
+
+
+def near_pair(rng, kind, dist):
+    """A random pair with its first group (point / edge a) moved along the separation of the
+    closest points until they are ``dist`` apart; the closest features stay the same."""
+    while True:
+        x = random_pair(rng, kind)
+        ty, d2 = R.classify(kind, x)
+        if d2 < 1e-6:
+            continue
+        ca, cb = R.separation(kind, x)
+        n = 1 if kind == 0 else 2
+        x[:n] += (ca - cb) / np.sqrt(d2) * (dist - np.sqrt(d2))
+        ty2, d22 = R.classify(kind, x)
+        if abs(np.sqrt(d22) - dist) < 1e-9 and ty2 == ty:
+            return x, ty
+
+
+def _tie_free(kind, x, tol=1e-7):
+    """No near-tie between feature types (so both classifications must agree)."""
+    for dx in (tol, -tol):
+        for c in range(12):
+            y = _x(x).copy()
+            y[c] += dx
+            if R.classify(kind, y)[0] != R.classify(kind, x)[0]:
+                return False
+    return True
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_types_and_distances_match_restatement(L, kind):
+    rng = np.random.default_rng(10 + kind)
+    seen = set()
+    checked = 0
+    for _ in range(3000):
+        x = random_pair(rng, kind)
+        ty_ref, d2_ref = R.classify(kind, x)
+        if not _tie_free(kind, x):
+            continue
+        xs = _x(x)
+        ty = L.ipcf_type(kind, _p(xs))
+        assert ty == ty_ref, (x, ty, ty_ref)
+        d2 = L.ipcf_d2(kind, ty, _p(xs))
+        assert d2 == pytest.approx(d2_ref, rel=1e-10, abs=1e-14)
+        seen.add(ty)
+        checked += 1
+    assert checked > 2500
+    assert seen == set(range(7 if kind == 0 else 9)), seen  # every feature pair occurs
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_distance_is_the_sampled_minimum(L, kind):
+    rng = np.random.default_rng(20 + kind)
+    for _ in range(60):
+        x = _x(random_pair(rng, kind))
+        ty = L.ipcf_type(kind, _p(x))
+        d2 = L.ipcf_d2(kind, ty, _p(x))
+        ds = R.sample_d2(kind, x, n=301)
+        assert d2 <= ds * (1 + 1e-12) + 1e-15  # the sampled points are on the primitives
+        assert np.sqrt(ds) - np.sqrt(d2) < 0.05  # and the grid comes close to the minimum
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_gradient_hessian_central_differences(L, kind):
+    rng = np.random.default_rng(30 + kind)
+    done = 0
+    while done < 40:
+        x, ty = near_pair(rng, kind, dist=0.06)
+        if not _tie_free(kind, x, tol=1e-4):
+            continue
+        r = random_pair(rng, kind)  # rest positions: the mollifier threshold only
+        ok, ty_h, d2, E, g, H = local_gh(L, kind, x, r)
+        assert ok and ty_h == ty
+        assert E == pytest.approx(R.energy(kind, x, r, DH, KAPPA), rel=1e-10)
+        gf, Hf = R.fd_gradient_hessian(kind, x, r, DH, KAPPA, 1e-5, ty)
+        assert np.linalg.norm(g - gf) <= 1e-6 * np.linalg.norm(gf) + 1e-9
+        assert np.linalg.norm(H - Hf) <= 1e-4 * np.linalg.norm(Hf)
+        assert np.array_equal(H, H.T)
+        done += 1
+
+
+def test_inactive_beyond_dhat(L):
+    rng = np.random.default_rng(40)
+    for kind in (0, 1):
+        x, _ = near_pair(rng, kind, dist=0.2)  # 0.2^2 > dhat^2 = 0.01
+        ok, _, d2, _, _, _ = local_gh(L, kind, x, x)
+        assert not ok and d2 == pytest.approx(0.04, rel=1e-8)
+        assert L.ipcf_energy(kind, _p(_x(x)), _p(_x(x)), DH, KAPPA) == 0.0
+
+
+def test_mollifier_parallel_edges(L):
+    """Near-parallel edges: the energy is scaled by m(|a x b|^2 / e_x), which is 0 for
+    parallel edges, 1 at and beyond e_x, and C1 there."""
+    a0, a1 = np.array([0.0, 0.0, 0.0]), np.array([1.0, 0.0, 0.0])
+    r = _x([a0, a1, [0.2, 0.05, 0.0], [0.8, 0.05, 0.0]])
+    ex = R.eps_x(r)
+    vals = []
+    for ang in (0.0, 1e-4, 1e-3, 1e-2, 0.05, 0.2):
+        b0 = np.array([0.2, 0.05, -0.3 * np.sin(ang)])
+        b1 = np.array([0.8, 0.05, 0.3 * np.sin(ang)])
+        x = _x([a0, a1, b0, b1])
+        e = L.ipcf_energy(1, _p(x), _p(r), DH, KAPPA)
+        assert e == pytest.approx(R.energy(1, x, r, DH, KAPPA), rel=1e-10, abs=1e-300)
+        c = np.linalg.norm(np.cross(a1 - a0, b1 - b0)) ** 2
+        m = R.mollifier(x, ex)
+        assert (m == 1.0) == (c >= ex)
+        vals.append(e)
+    assert vals[0] == 0.0  # exactly parallel: no contribution
+    assert vals == sorted(vals)  # grows as the edges turn apart (distance fixed at 0.05)
+
+
+def test_energy_continuous_across_feature_boundaries(L):
+    """A point sliding past a triangle edge and then past a vertex: the classified distance
+    and the energy change continuously although the feature pair changes."""
+    t = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]])
+    for path in (lambda s: [0.3, -0.2 + s, 0.06], lambda s: [-0.2 + s, -0.2 + s, 0.06]):
+        prev, types = None, set()
+        for s in np.linspace(0.0, 0.4, 4001):
+            x = _x(np.vstack([path(s), t]))
+            types.add(L.ipcf_type(0, _p(x)))
+            ok, _, d2, e, g, _ = local_gh(L, 0, x, x)
+            if not ok:
+                e, g = 0.0, np.zeros(12)
+            if prev is not None:
+                # no jump: the change stays within the gradient bound over the step
+                dx = np.linalg.norm(x - prev[0])
+                assert abs(e - prev[1]) <= 1.5 * max(np.linalg.norm(g), np.linalg.norm(prev[2])) * dx + 1e-15
+                assert abs(np.sqrt(d2) - np.sqrt(prev[3])) <= dx * (1 + 1e-9)  # distance is 1-Lipschitz
+            prev = (x, e, g, d2)
+        assert len(types) >= 2
+
+
+def test_psd_projection(L):
+    rng = np.random.default_rng(50)
+    for _ in range(50):
+        A = rng.normal(size=(12, 12))
+        H = _x(A + A.T)
+        L.ipcf_project_psd12(_p(H))
+        P = R.project_psd((A + A.T))
+        assert np.allclose(H.reshape(12, 12), P, rtol=0, atol=1e-11 * np.abs(P).max())
+        B = rng.normal(size=(12, 12))
+        S = _x(B @ B.T)  # already PSD: unchanged
+        S0 = S.copy()
+        L.ipcf_project_psd12(_p(S))
+        assert np.allclose(S, S0, rtol=0, atol=1e-11 * np.abs(S0).max())
+
+
+def test_to_affine(L):
+    rng = np.random.default_rng(60)
+    for nI in (1, 2):
+        gx, Hx, r = rng.normal(size=12), rng.normal(size=(12, 12)), rng.normal(size=12)
+        Hx = _x(Hx + Hx.T)
+        g24, Hi, Hj, Hij = np.zeros(24), np.zeros(144), np.zeros(144), np.zeros(144)
+        L.ipcf_to_affine(_p(gx), _p(Hx), _p(r), nI, _p(g24), _p(Hi), _p(Hj), _p(Hij))
+        rg, ri, rj, rij = R.to_affine(gx, Hx, r, nI)
+        for a, b in ((g24, rg), (Hi, ri), (Hj, rj), (Hij, rij)):
+            assert np.allclose(np.reshape(a, np.shape(b)), b, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_interior_contacts_reduce_to_the_reference_model(L, kind):
+    """On interior contacts (point over the triangle's interior; edges crossing, away from
+    parallel) the full model's distance, energy and affine gradient equal the reference's."""
+    prm = SimParams()
+    prm.dhat, prm.kappa = float(np.sqrt(DH)), KAPPA
+    assert prm.d2hat == pytest.approx(DH, rel=1e-15)
+    rng = np.random.default_rng(70 + kind)
+    done = 0
+    while done < 30:
+        x, ty = near_pair(rng, kind, dist=0.05)
+        if ty != 0 or not _tie_free(kind, x, tol=1e-4):
+            continue
+        r = x + rng.normal(size=(4, 3)) * 0.1
+        if kind == 1 and R.mollifier(x, R.eps_x(r)) != 1.0:
+            continue
+        active, d2_ref, g_ref, _, _, _ = oracle.contact_gh(kind, x, r, prm)
+        ok, _, d2, E, g, H = local_gh(L, kind, x, r)
+        assert active and ok
+        assert d2 == pytest.approx(d2_ref, rel=1e-10)
+        assert E == pytest.approx(oracle.contact_energy(kind, x, prm), rel=1e-10)
+        g24, Hi, Hj, Hij = np.zeros(24), np.zeros(144), np.zeros(144), np.zeros(144)
+        nI = 1 if kind == 0 else 2
+        L.ipcf_to_affine(_p(g), _p(_x(H)), _p(_x(r)), nI, _p(g24), _p(Hi), _p(Hj), _p(Hij))
+        assert np.linalg.norm(g24 - g_ref) <= 1e-8 * np.linalg.norm(g_ref)
+        done += 1
