@@ -254,7 +254,7 @@ struct Sim {
   // last step's last CCD pass are kept, [kSupValid] they hold the current GH pass's candidates
   int* dint = nullptr;
   double* q_last = nullptr;        // [12 n] the DOFs (A, then p) the last step ended with
-  int* hint = nullptr;             // pinned staging of dint
+  int* hint = nullptr;             // pinned: [2] the GH pass's active-pair count (-1 until copied)
   // captured passes: CCD bound (with events for profiling), GH, the Krylov solve, line-search
   // batches (step lengths from the host or from the CCD pass on the device)
   cudaStream_t cap_stream = nullptr;
@@ -324,7 +324,6 @@ struct Sim {
   int* dstat = nullptr;            // = box->dstat: [0] status, [1..] counters
   int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
   void* hstage = nullptr;          // pinned staging of the preconditioner's cluster tables
-                                   // (hint[2]: the GH pass's active-pair count, -1 until copied)
   size_t cap_hstage = 0;
   double* hval = nullptr;          // pinned host scalars
   unsigned long long* dmin = nullptr;  // = &box->toi_key
