@@ -58,6 +58,9 @@ def lib():
         L.orc_contact_energy.restype = d
         L.orc_collision_time.argtypes = [i, v, v]
         L.orc_collision_time.restype = d
+        L.orc_set_ipc_full.argtypes = [v, i]
+        L.orc_full_terms.argtypes = [i, v, v, v, i, v, v, v, v]
+        L.orc_full_terms.restype = i
         L.orc_cubic_roots.argtypes = [v, d, d, v]
         L.orc_cubic_roots.restype = i
         L.orc_solve.argtypes = [v, v]
@@ -112,6 +115,11 @@ class Oracle:
     def set_params(self, prm):
         self._prm = prm.to_c()
         lib().orc_set_params(self.h, ctypes.byref(self._prm))
+
+    def set_ipc_full(self, on: bool):
+        """The full IPC contact model (closest-feature types, edge-edge mollifier, inclusive
+        CCD) instead of the reference's interior-only model."""
+        lib().orc_set_ipc_full(self.h, 1 if on else 0)
 
     def set_state(self, A0, p0, Adot, pdot, dq=None):
         A0, p0, Adot, pdot = _c64(A0), _c64(p0), _c64(Adot), _c64(pdot)
@@ -201,6 +209,18 @@ def contact_terms(type_, x4, r4, prm):
     out = np.zeros(456)
     a = lib().orc_contact_terms(type_, _p(x4), _p(r4), ctypes.byref(c), _p(out))
     return bool(a), out[:144].reshape(12, 12), out[144:288].reshape(12, 12), out[288:432].reshape(12, 12), out[432:]
+
+
+def full_terms(kind, x4, r4, prm, swap=0):
+    """Full-model pair terms of one candidate: (active, E, d2, type, H_IJ, H_II, H_JJ, g24)."""
+    x4, r4 = _c64(x4), _c64(r4)
+    c = prm.to_c()
+    out = np.zeros(456)
+    E, d2, ty = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_int(0)
+    a = lib().orc_full_terms(kind, _p(x4), _p(r4), ctypes.byref(c), swap, _p(out), ctypes.byref(E), ctypes.byref(d2),
+                             ctypes.byref(ty))
+    return (bool(a), E.value, d2.value, ty.value, out[:144].reshape(12, 12), out[144:288].reshape(12, 12),
+            out[288:432].reshape(12, 12), out[432:])
 
 
 def abd_log(x: float) -> float:

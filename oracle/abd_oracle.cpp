@@ -200,6 +200,7 @@ struct Oracle {
   int stat_newton = 0, stat_lin = 0, stat_ls = 0, stat_pt = 0, stat_ee = 0, stat_vg = 0, stat_ij = 0,
       stat_active = 0, stat_refine = 0;
   int last_sweeps = 0;  // refinement sweeps of the last mixed-precision solve
+  bool ipc_full = false;  // full IPC contact model (closest-feature types, mollifier)
   double stat_alpha = 0, stat_toi = 0, stat_energy = 0;
 };
 
@@ -765,6 +766,313 @@ inline double contact_energy(int type, const V3 xs[4], const Params& P) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Full IPC contact model (opt-in, Oracle::ipc_full): the closest feature pair of a PT or EE
+// candidate (point-triangle / point-edge / point-point; line-line / point-edge /
+// point-point), the barrier on its squared distance, the edge-edge mollifier below
+// e_x = 1e-3 |a_rest|^2 |b_rest|^2, and the local 12x12 Hessian projected to PSD per contact
+// (Li et al., "Incremental Potential Contact", SIGGRAPH 2020).  The reference evaluates only
+// the interior cases (ipcsk/energy.py:20-22, 46-48; ccd.py:44-54).  Derivatives: forward-mode
+// automatic differentiation carrying the full gradient and Hessian through every operation.
+// ---------------------------------------------------------------------------------------
+struct D12 {
+  double v;
+  double g[12];
+  double H[144];
+};
+inline D12 d12_const(double x) {
+  D12 r;
+  r.v = x;
+  std::memset(r.g, 0, sizeof(r.g));
+  std::memset(r.H, 0, sizeof(r.H));
+  return r;
+}
+inline D12 d12_var(double x, int i) {
+  D12 r = d12_const(x);
+  r.g[i] = 1.0;
+  return r;
+}
+inline D12 operator+(const D12& a, const D12& b) {
+  D12 r;
+  r.v = a.v + b.v;
+  for (int i = 0; i < 12; ++i) r.g[i] = a.g[i] + b.g[i];
+  for (int i = 0; i < 144; ++i) r.H[i] = a.H[i] + b.H[i];
+  return r;
+}
+inline D12 operator-(const D12& a, const D12& b) {
+  D12 r;
+  r.v = a.v - b.v;
+  for (int i = 0; i < 12; ++i) r.g[i] = a.g[i] - b.g[i];
+  for (int i = 0; i < 144; ++i) r.H[i] = a.H[i] - b.H[i];
+  return r;
+}
+inline D12 operator*(const D12& a, const D12& b) {
+  D12 r;
+  r.v = a.v * b.v;
+  for (int i = 0; i < 12; ++i) r.g[i] = a.v * b.g[i] + b.v * a.g[i];
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 12; ++j)
+      r.H[12 * i + j] = a.v * b.H[12 * i + j] + b.v * a.H[12 * i + j] + a.g[i] * b.g[j] + b.g[i] * a.g[j];
+  return r;
+}
+inline D12 scale(const D12& a, double s) {
+  D12 r;
+  r.v = a.v * s;
+  for (int i = 0; i < 12; ++i) r.g[i] = a.g[i] * s;
+  for (int i = 0; i < 144; ++i) r.H[i] = a.H[i] * s;
+  return r;
+}
+// f(a) from f, f', f'' at a.v (chain rule)
+inline D12 apply(const D12& a, double f, double f1, double f2) {
+  D12 r;
+  r.v = f;
+  for (int i = 0; i < 12; ++i) r.g[i] = f1 * a.g[i];
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 12; ++j) r.H[12 * i + j] = f1 * a.H[12 * i + j] + f2 * a.g[i] * a.g[j];
+  return r;
+}
+inline D12 operator/(const D12& a, const D12& b) {
+  const double q = 1.0 / b.v;
+  return a * apply(b, q, -q * q, 2.0 * q * q * q);
+}
+struct V3D {
+  D12 x, y, z;
+};
+inline V3D vsub(const V3D& a, const V3D& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline D12 vdot(const V3D& a, const V3D& b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3D vcross(const V3D& a, const V3D& b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// closest-feature types (triangle edges E0 = t0t1, E1 = t1t2, E2 = t2t0; edge a = x0x1,
+// edge b = x2x3)
+enum { F_PT = 0, F_PE0, F_PE1, F_PE2, F_PV0, F_PV1, F_PV2 };
+enum { F_EE = 0, F_A0B, F_A1B, F_AB0, F_AB1, F_A0B0, F_A0B1, F_A1B0, F_A1B1 };
+
+// clamped parameter of the point of segment [a, b] nearest p, and the squared distance
+inline double seg_param(V3 p, V3 a, V3 b, double& d2) {
+  const V3 e = b - a;
+  const double ee = dot(e, e);
+  double s = ee > 0.0 ? dot(p - a, e) / ee : 0.0;
+  s = std::min(1.0, std::max(0.0, s));
+  const V3 c = a + e * s;
+  d2 = dot(p - c, p - c);
+  return s;
+}
+
+// Point-triangle: the interior when the point's projection has non-negative barycentric
+// coordinates (from sub-triangle areas); else the nearest edge as a segment (an edge or one
+// of its end points), ties to the first of E0, E1, E2.
+int full_pt_type(const V3 x[4]) {
+  const V3 p = x[0], t0 = x[1], t1 = x[2], t2 = x[3];
+  const V3 n = cross(t1 - t0, t2 - t0);
+  const double nn = dot(n, n);
+  if (nn > 0.0) {
+    const V3 q = p - n * (dot(p - t0, n) / nn);
+    const double u = dot(cross(t1 - q, t2 - q), n), v = dot(cross(t2 - q, t0 - q), n),
+                 w = dot(cross(t0 - q, t1 - q), n);
+    if (u >= 0.0 && v >= 0.0 && w >= 0.0) return F_PT;
+  }
+  const V3 tv[3] = {t0, t1, t2};
+  int best = 0;
+  double bd = 0.0, bs = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    double d2;
+    const double s = seg_param(p, tv[k], tv[(k + 1) % 3], d2);
+    if (k == 0 || d2 < bd) {
+      best = k;
+      bd = d2;
+      bs = s;
+    }
+  }
+  if (bs <= 0.0) return F_PV0 + best;
+  if (bs >= 1.0) return F_PV0 + (best + 1) % 3;
+  return F_PE0 + best;
+}
+
+// Edge-edge: line-line when the stationary point of the two lines' distance lies inside
+// both segments; else the nearest end point to segment distance (a0, a1 to b; b0, b1 to a),
+// ties to the first.
+int full_ee_type(const V3 x[4]) {
+  const V3 u = x[1] - x[0], v = x[3] - x[2], w = x[0] - x[2];
+  const double a = dot(u, u), b = dot(u, v), c = dot(v, v), d = dot(u, w), e = dot(v, w);
+  const double D = a * c - b * b;
+  if (D > 0.0) {
+    const double s = (b * e - c * d) / D, t = (a * e - b * d) / D;
+    if (s > 0.0 && s < 1.0 && t > 0.0 && t < 1.0) return F_EE;
+  }
+  double d2[4], s[4];
+  s[0] = seg_param(x[0], x[2], x[3], d2[0]);
+  s[1] = seg_param(x[1], x[2], x[3], d2[1]);
+  s[2] = seg_param(x[2], x[0], x[1], d2[2]);
+  s[3] = seg_param(x[3], x[0], x[1], d2[3]);
+  int k = 0;
+  for (int m = 1; m < 4; ++m)
+    if (d2[m] < d2[k]) k = m;
+  const int edge[4] = {F_A0B, F_A1B, F_AB0, F_AB1}, at0[4] = {F_A0B0, F_A1B0, F_A0B0, F_A0B1},
+            at1[4] = {F_A0B1, F_A1B1, F_A1B0, F_A1B1};
+  return s[k] <= 0.0 ? at0[k] : (s[k] >= 1.0 ? at1[k] : edge[k]);
+}
+
+inline D12 full_d2_point_line(const V3D& p, const V3D& a, const V3D& b) {
+  const V3D c = vcross(vsub(a, p), vsub(b, p)), e = vsub(b, a);
+  return vdot(c, c) / vdot(e, e);
+}
+inline D12 full_d2_pp(const V3D& p, const V3D& q) {
+  const V3D d = vsub(p, q);
+  return vdot(d, d);
+}
+inline D12 full_d2_plane(const V3D& p, const V3D& o, const V3D& n) {
+  const D12 s = vdot(vsub(p, o), n);
+  return (s * s) / vdot(n, n);
+}
+
+// squared distance of feature pair `type` (kind 0 PT, 1 EE) on AD variables
+D12 full_d2(int kind, int type, const V3D X[4]) {
+  if (kind == 0) {
+    switch (type) {
+      case F_PT: return full_d2_plane(X[0], X[1], vcross(vsub(X[2], X[1]), vsub(X[3], X[1])));
+      case F_PE0: return full_d2_point_line(X[0], X[1], X[2]);
+      case F_PE1: return full_d2_point_line(X[0], X[2], X[3]);
+      case F_PE2: return full_d2_point_line(X[0], X[3], X[1]);
+      default: return full_d2_pp(X[0], X[1 + type - F_PV0]);
+    }
+  }
+  switch (type) {
+    case F_EE: return full_d2_plane(X[2], X[0], vcross(vsub(X[1], X[0]), vsub(X[3], X[2])));
+    case F_A0B: return full_d2_point_line(X[0], X[2], X[3]);
+    case F_A1B: return full_d2_point_line(X[1], X[2], X[3]);
+    case F_AB0: return full_d2_point_line(X[2], X[0], X[1]);
+    case F_AB1: return full_d2_point_line(X[3], X[0], X[1]);
+    case F_A0B0: return full_d2_pp(X[0], X[2]);
+    case F_A0B1: return full_d2_pp(X[0], X[3]);
+    case F_A1B0: return full_d2_pp(X[1], X[2]);
+    default: return full_d2_pp(X[1], X[3]);
+  }
+}
+
+// energy of one candidate with its derivatives in the four points' coordinates; false when
+// the classified distance is not below dhat^2
+bool full_energy_d(int kind, const V3 xs[4], const V3 rs[4], const Params& P, D12& E, double* d2out = nullptr) {
+  const int type = kind == 0 ? full_pt_type(xs) : full_ee_type(xs);
+  V3D X[4];
+  for (int k = 0; k < 4; ++k) X[k] = {d12_var(xs[k].x, 3 * k), d12_var(xs[k].y, 3 * k + 1), d12_var(xs[k].z, 3 * k + 2)};
+  const D12 d = full_d2(kind, type, X);
+  if (d2out) *d2out = d.v;
+  if (!(d.v < P.d2hat)) return false;
+  // b(d) = -kappa (d / dh - 1)^2 log(d / dh) and its first two derivatives in d
+  const double dh = P.d2hat, s = d.v / dh, l = std::log(s);
+  const double f = -P.kappa * (s - 1.0) * (s - 1.0) * l;
+  const double f1 = -P.kappa * (2.0 * (s - 1.0) * l + (s - 1.0) * (s - 1.0) / s) / dh;
+  const double f2 = -P.kappa * (2.0 * l + 4.0 * (s - 1.0) / s - (s - 1.0) * (s - 1.0) / (s * s)) / (dh * dh);
+  E = apply(d, f, f1, f2);
+  if (kind == 1) {  // mollifier m(c) = (2 - c / e_x) c / e_x below e_x, c = |a x b|^2
+    const V3 ra = rs[1] - rs[0], rb = rs[3] - rs[2];
+    const double ex = 1e-3 * dot(ra, ra) * dot(rb, rb);
+    const V3D nv = vcross(vsub(X[1], X[0]), vsub(X[3], X[2]));
+    const D12 c = vdot(nv, nv);
+    if (c.v < ex) E = E * apply(c, (2.0 - c.v / ex) * c.v / ex, 2.0 / ex - 2.0 * c.v / (ex * ex), -2.0 / (ex * ex));
+  }
+  return true;
+}
+
+// symmetric 12x12 matrix onto the PSD cone (cyclic Jacobi, negative eigenvalues dropped)
+void psd12(double* H) {
+  double A[12][12], Q[12][12];
+  double fro = 0.0;
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 12; ++j) {
+      A[i][j] = 0.5 * (H[12 * i + j] + H[12 * j + i]);
+      Q[i][j] = i == j ? 1.0 : 0.0;
+      fro += A[i][j] * A[i][j];
+    }
+  if (!(fro > 0.0)) return;
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < 12; ++i)
+      for (int j = 0; j < 12; ++j)
+        if (i != j) off += A[i][j] * A[i][j];
+    if (off <= 1e-30 * fro) break;
+    for (int p = 0; p < 12; ++p)
+      for (int q = p + 1; q < 12; ++q) {
+        if (A[p][q] == 0.0) continue;
+        const double th = 0.5 * std::atan2(2.0 * A[p][q], A[q][q] - A[p][p]);
+        const double c = std::cos(th), s = std::sin(th);
+        for (int k = 0; k < 12; ++k) {
+          const double akp = A[k][p], akq = A[k][q];
+          A[k][p] = c * akp - s * akq;
+          A[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 12; ++k) {
+          const double apk = A[p][k], aqk = A[q][k];
+          A[p][k] = c * apk - s * aqk;
+          A[q][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 12; ++k) {
+          const double qkp = Q[k][p], qkq = Q[k][q];
+          Q[k][p] = c * qkp - s * qkq;
+          Q[k][q] = s * qkp + c * qkq;
+        }
+      }
+  }
+  for (int i = 0; i < 12; ++i)
+    for (int j = 0; j < 12; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < 12; ++k)
+        if (A[k][k] > 0.0) acc += Q[i][k] * A[k][k] * Q[j][k];
+      H[12 * i + j] = acc;
+    }
+}
+
+// The pair terms of one candidate under the full model, in contact_terms' layout: out[456] =
+// H_IJ, H_II, H_JJ, g (the pair's first body, then its second); `swap`: the candidate's
+// first group (point / edge a) belongs to the pair's second body.
+bool full_terms(int kind, const V3 xs[4], const V3 rs[4], int swap, const Params& P, double out[456]) {
+  D12 E;
+  if (!full_energy_d(kind, xs, rs, P, E)) return false;
+  double H[144];
+  std::memcpy(H, E.H, sizeof(H));
+  psd12(H);
+  const int nI = kind == 0 ? 1 : 2;  // points of the first group
+  // x_a = p_a + sum_k r_k A_ka: weights (1, r) of DOF group m for point v
+  double w[4][4];
+  for (int v = 0; v < 4; ++v) {
+    w[v][0] = 1.0;
+    w[v][1] = rs[v].x;
+    w[v][2] = rs[v].y;
+    w[v][3] = rs[v].z;
+  }
+  double G[2][12], B[2][2][144];
+  std::memset(G, 0, sizeof(G));
+  std::memset(B, 0, sizeof(B));
+  for (int u = 0; u < 4; ++u)
+    for (int m = 0; m < 4; ++m)
+      for (int a = 0; a < 3; ++a) {
+        const int gu = u < nI ? 0 : 1;
+        G[gu][3 * m + a] += w[u][m] * E.g[3 * u + a];
+        for (int v = 0; v < 4; ++v)
+          for (int n2 = 0; n2 < 4; ++n2)
+            for (int b = 0; b < 3; ++b)
+              B[gu][v < nI ? 0 : 1][12 * (3 * m + a) + 3 * n2 + b] += w[u][m] * H[12 * (3 * u + a) + 3 * v + b] * w[v][n2];
+      }
+  const int I = swap ? 1 : 0, J = 1 - I;  // groups of the pair's first and second body
+  for (int e = 0; e < 144; ++e) {
+    out[e] = B[I][J][e];
+    out[144 + e] = B[I][I][e];
+    out[288 + e] = B[J][J][e];
+  }
+  for (int e = 0; e < 12; ++e) {
+    out[432 + e] = G[I][e];
+    out[444 + e] = G[J][e];
+  }
+  return true;
+}
+
+double full_energy(int kind, const V3 xs[4], const V3 rs[4], const Params& P) {
+  D12 E;
+  return full_energy_d(kind, xs, rs, P, E) ? E.v : 0.0;
+}
+
+// ---------------------------------------------------------------------------------------
 // inertia + orthogonality (orthogonal_energy.py:24-135)
 // ---------------------------------------------------------------------------------------
 inline V3 row(const double* A, int k) { return {A[3 * k], A[3 * k + 1], A[3 * k + 2]}; }
@@ -892,7 +1200,9 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
       V3 xs[4], rs[4];
       fetch(o, y, C[i], type, xs, rs);
       const int swap = C[i].I != L.ij[2 * C[i].pair];
-      on[i] = contact_terms(type, xs, rs, swap, o.prm, R[i].v) ? 1 : 0;
+      on[i] = (o.ipc_full ? full_terms(type, xs, rs, swap, o.prm, R[i].v) : contact_terms(type, xs, rs, swap, o.prm, R[i].v))
+                  ? 1
+                  : 0;
       R[i].pair = C[i].pair;
     }
     for (int i = 0; i < nc; ++i)
@@ -1516,7 +1826,9 @@ inline void cols(V3 p, V3 q, V3 r, double m[3][3]) {
   m[0][2] = r.x; m[1][2] = r.y; m[2][2] = r.z;
 }
 
-double collision_time(int type, const V3 a0[4], const V3 a1[4]) {
+// inclusive: a root also counts on the closed triangle / segments (edge and vertex hits, which
+// the full contact model resolves), within 1e-9 of their parameter bounds
+double collision_time(int type, const V3 a0[4], const V3 a1[4], bool inclusive = false) {
   double A[4][3][3], B[4][3][3];
   const int sel[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
   for (int k = 0; k < 4; ++k) {
@@ -1538,7 +1850,12 @@ double collision_time(int type, const V3 a0[4], const V3 a1[4]) {
     V3 pt[4];
     for (int k = 0; k < 4; ++k) pt[k] = a0[k] * (1.0 - root) + a1[k] * root;  // wp.lerp
     Geo G = geometry(type, pt[0], pt[1], pt[2], pt[3]);
-    ok = valid_root(type, G.beta, G.gamma);
+    if (inclusive) {
+      const double t = 1e-9, b = G.beta, c = type == 0 ? G.gamma : -G.gamma;
+      ok = b >= -t && c >= -t && (type == 0 ? b + c <= 1.0 + t : (b <= 1.0 + t && c <= 1.0 + t));
+    } else {
+      ok = valid_root(type, G.beta, G.gamma);
+    }
     if (ok) break;
   }
   return ok ? root : 1.0;
@@ -1581,7 +1898,7 @@ double energy_at(Oracle& o, const double* y, const double* Akp, const double* pk
       for (int i = 0; i < nc; ++i) {
         V3 xs[4], rs[4];
         fetch(o, y, C[i], type, xs, rs);
-        part.add(contact_energy(type, xs, o.prm));
+        part.add(o.ipc_full ? full_energy(type, xs, rs, o.prm) : contact_energy(type, xs, o.prm));
       }
 #pragma omp critical
       total.merge(part);
@@ -1627,7 +1944,7 @@ double ccd_toi(Oracle& o, const double* x, const double* xk, double* raw) {
       V3 a0[4], a1[4], rs[4];
       fetch(o, x, C[i], type, a0, rs);
       fetch(o, xk, C[i], type, a1, rs);
-      const double t = collision_time(type, a0, a1);
+      const double t = collision_time(type, a0, a1, o.ipc_full);
       if (t < 1.0) tmin = std::min(tmin, t);
     }
     toi = std::min(toi, tmin);
@@ -1744,6 +2061,23 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
 
 void orc_destroy(void* h) { delete (Oracle*)h; }
 void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
+void orc_set_ipc_full(void* h, int on) { ((Oracle*)h)->ipc_full = on != 0; }
+
+// full-model pair terms of one candidate (swap as in the assembly): out[456] = H_IJ, H_II,
+// H_JJ, g; *E the energy, *d2 the classified squared distance, *type its feature pair
+int orc_full_terms(int kind, const double* xs12, const double* rs12, const Params* prm, int swap, double* out,
+                   double* E, double* d2, int* type) {
+  V3 xs[4], rs[4];
+  for (int k = 0; k < 4; ++k) {
+    xs[k] = {xs12[3 * k], xs12[3 * k + 1], xs12[3 * k + 2]};
+    rs[k] = {rs12[3 * k], rs12[3 * k + 1], rs12[3 * k + 2]};
+  }
+  *type = kind == 0 ? full_pt_type(xs) : full_ee_type(xs);
+  D12 e;
+  const bool on = full_energy_d(kind, xs, rs, *prm, e, d2);
+  *E = on ? e.v : 0.0;
+  return on && full_terms(kind, xs, rs, swap, *prm, out) ? 1 : 0;
+}
 void orc_set_threads(int t) { omp_set_num_threads(t); }
 int orc_max_threads() { return omp_get_max_threads(); }
 

@@ -243,3 +243,78 @@ def test_interior_contacts_reduce_to_the_reference_model(L, kind):
         L.ipcf_to_affine(_p(g), _p(_x(H)), _p(_x(r)), nI, _p(g24), _p(Hi), _p(Hj), _p(Hij))
         assert np.linalg.norm(g24 - g_ref) <= 1e-8 * np.linalg.norm(g_ref)
         done += 1
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_oracle_full_model_matches_the_header(L, kind):
+    """The C++ oracle's full model (forward-mode AD carrying the whole Hessian, its own
+    classification and Jacobi projection) against the header's (hyper-dual entries): same
+    feature pair, distance and energy; the projected affine terms to 1e-9, in both group
+    orders of the pair."""
+    prm = SimParams()
+    prm.dhat, prm.kappa = float(np.sqrt(DH)), KAPPA
+    rng = np.random.default_rng(80 + kind)
+    seen = set()
+    done = 0
+    while done < 60:
+        x, ty = near_pair(rng, kind, dist=0.07)
+        if not _tie_free(kind, x, tol=1e-6):
+            continue
+        r = x + rng.normal(size=(4, 3)) * (0.1 if done % 2 else 2.0)  # mollified and not
+        ok, ty_h, d2, E, g, H = local_gh(L, kind, x, r)
+        Hp = _x(H)
+        L.ipcf_project_psd12(_p(Hp))
+        g24, Hi, Hj, Hij = np.zeros(24), np.zeros(144), np.zeros(144), np.zeros(144)
+        L.ipcf_to_affine(_p(g), _p(Hp), _p(_x(r)), 1 if kind == 0 else 2, _p(g24), _p(Hi), _p(Hj), _p(Hij))
+        Hi, Hj, Hij = Hi.reshape(12, 12), Hj.reshape(12, 12), Hij.reshape(12, 12)
+        for swap in (0, 1):
+            a, Eo, d2o, tyo, HIJ, HII, HJJ, go = oracle.full_terms(kind, x, r, prm, swap)
+            assert a and ok and tyo == ty_h == ty
+            assert d2o == pytest.approx(d2, rel=1e-12) and Eo == pytest.approx(E, rel=1e-10)
+            want = (Hij, Hi, Hj, g24) if swap == 0 else (Hij.T, Hj, Hi, np.concatenate([g24[12:], g24[:12]]))
+            for got, ref in zip((HIJ, HII, HJJ, go), want):
+                assert np.linalg.norm(got - ref) <= 1e-9 * max(np.linalg.norm(ref), np.linalg.norm(Hi) * 1e-6)
+        seen.add(ty)
+        done += 1
+    assert len(seen) >= 4
+
+
+def _min_surface_distance(flat, x):
+    """Minimum distance between the two bodies' surfaces over every PT and EE pair."""
+    voff, toff, eoff = flat["voff"], flat["toff"], flat["eoff"]
+    tris, edges = flat["tris"].reshape(-1, 3), flat["edges"].reshape(-1, 2)
+    best = np.inf
+    for a, b in ((0, 1), (1, 0)):
+        for v in range(voff[a], voff[a + 1]):
+            for t in range(toff[b], toff[b + 1]):
+                best = min(best, R.classify(0, np.vstack([x[v], x[tris[t]]]))[1])
+    for e in range(eoff[0], eoff[1]):
+        for f in range(eoff[1], eoff[2]):
+            best = min(best, R.classify(1, np.vstack([x[edges[e]], x[edges[f]]]))[1])
+    return float(np.sqrt(best))
+
+
+def test_oracle_full_mode_steps():
+    """Two cubes (configuration 0: one falls onto the other, fixed) with the full contact
+    model in the oracle: identical to the reference model before the first contact; after
+    it the bodies stay apart (surface distance near dhat) with at least one active contact
+    every step.  The reference model loses every contact at steps 16-18 of this scene while
+    the bodies touch; only its CCD cap keeps them apart there."""
+    from abd_warp_b200 import scenes
+
+    bodies, prm, _ = scenes.make_config(0)
+    flat = scenes.flatten_bodies(bodies)
+    ref, full = oracle.Oracle(flat, prm), oracle.Oracle(flat, prm)
+    full.set_ipc_full(True)
+    contact, lost_ref = False, 0
+    for k in range(25):
+        a, b = ref.step(), full.step()
+        if not contact and b["n_active"] == 0:
+            assert a == b
+        contact = contact or b["n_active"] > 0
+        assert b["newton_iters"] <= prm.max_iter and np.isfinite(b["energy"])
+        if contact:
+            assert b["n_active"] > 0
+            lost_ref += a["n_active"] == 0
+            assert _min_surface_distance(flat, full.get_state()["x_view"]) > 0.5 * prm.dhat
+    assert contact and lost_ref > 0
