@@ -61,6 +61,8 @@ def lib():
         L.orc_set_ipc_full.argtypes = [v, i]
         L.orc_full_terms.argtypes = [i, v, v, v, i, v, v, v, v]
         L.orc_full_terms.restype = i
+        L.orc_full_hessian.argtypes = [v, v, v, v]
+        L.orc_full_hessian.restype = i
         L.orc_cubic_roots.argtypes = [v, d, d, v]
         L.orc_cubic_roots.restype = i
         L.orc_solve.argtypes = [v, v]
@@ -120,6 +122,15 @@ class Oracle:
         """The full IPC contact model (closest-feature types, edge-edge mollifier, inclusive
         CCD) instead of the reference's interior-only model."""
         lib().orc_set_ipc_full(self.h, 1 if on else 0)
+
+    def full_hessian(self, A, p):
+        """Exact, unprojected Hessian of the step's energy at (A, p) under the full contact
+        model: dense [12n, 12n], DOFs [p, A rows] per body, fixed bodies' rows zero."""
+        A, p = _c64(A), _c64(p)
+        H = np.zeros((12 * self.n, 12 * self.n))
+        if lib().orc_full_hessian(self.h, _p(A), _p(p), _p(H)) < 0:
+            raise RuntimeError("full_hessian needs set_ipc_full(True)")
+        return H
 
     def set_state(self, A0, p0, Adot, pdot, dq=None):
         A0, p0, Adot, pdot = _c64(A0), _c64(p0), _c64(Adot), _c64(pdot)

@@ -2178,6 +2178,59 @@ int orc_gh(void* h, const double* A, const double* p, double* g, double* diag, d
   return m;
 }
 
+// The exact Hessian of the step's energy at DOFs (A, p), dense [12n][12n] in the DOF order
+// [p, A row 0, row 1, row 2] per body, for the adjoint of a converged step: inertia and
+// orthogonality (exact in the assembly already) plus every candidate's unprojected
+// full-model contact Hessian.  Needs the full contact model (set_ipc_full).  Rows and columns
+// of fixed bodies are left zero.  Returns the number of active contacts, -1 without the model.
+int orc_full_hessian(void* h, const double* A, const double* p, double* Hd) {
+  Oracle* o = (Oracle*)h;
+  if (!o->ipc_full) return -1;
+  const int n = o->n;
+  const size_t N = 12 * (size_t)n;
+  std::fill(Hd, Hd + N * N, 0.0);
+  std::copy(A, A + 9 * n, o->A.begin());
+  std::copy(p, p + 3 * n, o->p.begin());
+  for (int b = 0; b < n; ++b) {
+    if (o->fixed[b]) continue;
+    double gb[12], Hb[144];
+    inertia_gh(*o, b, gb, Hb);
+    for (int r = 0; r < 12; ++r)
+      for (int c = 0; c < 12; ++c) Hd[(12 * (size_t)b + r) * N + 12 * (size_t)b + c] += Hb[12 * r + c];
+  }
+  transform(*o, o->A.data(), o->p.data(), o->x.data());
+  Boxes bx;
+  Lists L;
+  static_boxes(*o, o->x.data(), bx);
+  cull(*o, bx, L);
+  int active = 0;
+  for (int kind = 0; kind < 2; ++kind) {
+    const std::vector<Cand>& C = kind == 0 ? L.pt : L.ee;
+    for (const Cand& cd : C) {
+      V3 xs[4], rs[4];
+      fetch(*o, o->x.data(), cd, kind, xs, rs);
+      D12 E;
+      if (!full_energy_d(kind, xs, rs, o->prm, E)) continue;
+      ++active;
+      const int nI = kind == 0 ? 1 : 2;
+      const int body[2] = {cd.I, cd.J};  // the candidate's first group moves with cd.I
+      for (int u = 0; u < 4; ++u)
+        for (int v = 0; v < 4; ++v) {
+          const int bu = body[u < nI ? 0 : 1], bv = body[v < nI ? 0 : 1];
+          if (o->fixed[bu] || o->fixed[bv]) continue;
+          const double wu[4] = {1.0, rs[u].x, rs[u].y, rs[u].z}, wv[4] = {1.0, rs[v].x, rs[v].y, rs[v].z};
+          for (int m = 0; m < 4; ++m)
+            for (int a = 0; a < 3; ++a)
+              for (int n2 = 0; n2 < 4; ++n2)
+                for (int b2 = 0; b2 < 3; ++b2)
+                  Hd[(12 * (size_t)bu + 3 * m + a) * N + 12 * (size_t)bv + 3 * n2 + b2] +=
+                      wu[m] * E.H[12 * (3 * u + a) + 3 * v + b2] * wv[n2];
+        }
+    }
+  }
+  return active;
+}
+
 // Energy at trial DOFs (Ak, pk) against the state set by orc_set_state.
 double orc_energy(void* h, const double* Ak, const double* pk) {
   Oracle* o = (Oracle*)h;
