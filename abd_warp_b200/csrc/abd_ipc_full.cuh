@@ -10,7 +10,8 @@
 // e_x = 1e-3 |a_rest|^2 |b_rest|^2, and a per-contact PSD projection of the local Hessian.
 // Derivatives are exact to rounding: the local energy is evaluated on hyper-dual numbers
 // (Fike and Alonso 2011), one evaluation per Hessian entry.  The projection is the cyclic
-// Jacobi eigenvalue method (Golub and Van Loan, Matrix Computations, 8.5).
+// Jacobi eigenvalue method in round-robin (parallel) order (Golub and Van Loan, Matrix
+// Computations, 8.5).
 //
 // Everything here is plain arithmetic callable from host and device code.
 #pragma once
@@ -293,55 +294,93 @@ ABD_HD inline bool local_gh(int kind, const double x[12], const double r[12], do
   return true;
 }
 
-// Projects a symmetric 12x12 matrix onto the positive semidefinite cone: cyclic Jacobi
-// rotations until the off-diagonal part is below 1e-30 of the whole (or 32 sweeps), negative
-// eigenvalues set to 0, and the matrix rebuilt from the eigenpairs.
-ABD_HD inline void project_psd12(double H[144]) {
-  double A[144], Vm[144];
+// Eigen-decomposition of a symmetric 12x12 matrix H = V diag(lam) V^T (V's columns the
+// eigenvectors, row-major) by Jacobi rotations in round-robin order: each sweep is 11 rounds
+// of 6 rotations on disjoint index pairs (index 0 fixed, the others shifted one place per
+// round).  A round takes its 6 angles from the matrix as it enters the round, then applies the
+// 6 column updates, then the 6 row updates: the order a warp follows when its lanes share one
+// round.  Stops when the off-diagonal part is below 1e-30 of the whole, or after 32 sweeps.
+ABD_HD inline void eig_sym12(const double H[144], double lam[12], double V[144]) {
+  double A[144];
   double total = 0.0;
   for (int k = 0; k < 144; ++k) {
     A[k] = H[k];
-    Vm[k] = (k / 12 == k % 12) ? 1.0 : 0.0;
+    V[k] = (k / 12 == k % 12) ? 1.0 : 0.0;
     total += H[k] * H[k];
   }
-  if (!(total > 0.0)) return;
-  for (int sweep = 0; sweep < 32; ++sweep) {
+  int pos[12];
+  for (int k = 0; k < 12; ++k) pos[k] = k;
+  for (int sweep = 0; sweep < 32 && total > 0.0; ++sweep) {
     double off = 0.0;
     for (int p = 0; p < 12; ++p)
       for (int q = p + 1; q < 12; ++q) off += 2.0 * A[12 * p + q] * A[12 * p + q];
     if (!(off > 1e-30 * total)) break;
-    for (int p = 0; p < 11; ++p)
-      for (int q = p + 1; q < 12; ++q) {
-        const double apq = A[12 * p + q];
-        if (apq == 0.0) continue;
-        const double theta = (A[12 * q + q] - A[12 * p + p]) / (2.0 * apq);
-        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < 12; ++k) {  // A <- A J (columns p, q)
-          const double akp = A[12 * k + p], akq = A[12 * k + q];
-          A[12 * k + p] = c * akp - s * akq;
-          A[12 * k + q] = s * akp + c * akq;
+    for (int round = 0; round < 11; ++round) {
+      int P[6], Q[6];
+      double C[6], S[6];
+      for (int k = 0; k < 6; ++k) {
+        const int a = pos[k], b = pos[11 - k];
+        P[k] = a < b ? a : b;
+        Q[k] = a < b ? b : a;
+        const double apq = A[12 * P[k] + Q[k]];
+        if (apq == 0.0) {
+          C[k] = 1.0;
+          S[k] = 0.0;
+          continue;
         }
-        for (int k = 0; k < 12; ++k) {  // A <- J^T A (rows p, q)
-          const double apk = A[12 * p + k], aqk = A[12 * q + k];
-          A[12 * p + k] = c * apk - s * aqk;
-          A[12 * q + k] = s * apk + c * aqk;
-        }
-        for (int k = 0; k < 12; ++k) {  // V <- V J
-          const double vkp = Vm[12 * k + p], vkq = Vm[12 * k + q];
-          Vm[12 * k + p] = c * vkp - s * vkq;
-          Vm[12 * k + q] = s * vkp + c * vkq;
-        }
+        const double theta = (A[12 * Q[k] + Q[k]] - A[12 * P[k] + P[k]]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        C[k] = 1.0 / sqrt(t * t + 1.0);
+        S[k] = t * C[k];
       }
+      for (int k = 0; k < 6; ++k)  // A <- A J, V <- V J (columns P, Q)
+        for (int r = 0; r < 12; ++r) {
+          const double ap = A[12 * r + P[k]], aq = A[12 * r + Q[k]];
+          A[12 * r + P[k]] = C[k] * ap - S[k] * aq;
+          A[12 * r + Q[k]] = S[k] * ap + C[k] * aq;
+          const double vp = V[12 * r + P[k]], vq = V[12 * r + Q[k]];
+          V[12 * r + P[k]] = C[k] * vp - S[k] * vq;
+          V[12 * r + Q[k]] = S[k] * vp + C[k] * vq;
+        }
+      for (int k = 0; k < 6; ++k)  // A <- J^T A (rows P, Q)
+        for (int c = 0; c < 12; ++c) {
+          const double ap = A[12 * P[k] + c], aq = A[12 * Q[k] + c];
+          A[12 * P[k] + c] = C[k] * ap - S[k] * aq;
+          A[12 * Q[k] + c] = S[k] * ap + C[k] * aq;
+        }
+      const int last = pos[11];  // next round: shift indices 1..11 by one place
+      for (int k = 11; k > 1; --k) pos[k] = pos[k - 1];
+      pos[1] = last;
+    }
   }
-  double lam[12];
-  for (int k = 0; k < 12; ++k) lam[k] = A[13 * k] > 0.0 ? A[13 * k] : 0.0;
+  for (int k = 0; k < 12; ++k) lam[k] = A[13 * k];
+}
+
+// Projects a symmetric 12x12 matrix onto the positive semidefinite cone: its eigenpairs
+// (eig_sym12) with negative eigenvalues set to 0, the matrix rebuilt from them.
+ABD_HD inline void project_psd12(double H[144]) {
+  double lam[12], Vm[144];
+  eig_sym12(H, lam, Vm);
+  for (int k = 0; k < 12; ++k) lam[k] = lam[k] > 0.0 ? lam[k] : 0.0;
   for (int i = 0; i < 12; ++i)
     for (int j = i; j < 12; ++j) {
       double acc = 0.0;
       for (int k = 0; k < 12; ++k) acc += Vm[12 * i + k] * lam[k] * Vm[12 * j + k];
       H[12 * i + j] = H[12 * j + i] = acc;
     }
+}
+
+// A point-coordinate vector v[12] as a vector over the two bodies' affine DOFs u[24] (the
+// first body's 12, then the second's), with the weights of to_affine: a rank-one term
+// c v v^T of the projected contact Hessian becomes c u u^T in the DOFs.
+ABD_HD inline void to_affine_vec(const double v[12], const double r[12], int nI, double u[24]) {
+  for (int k = 0; k < 24; ++k) u[k] = 0.0;
+  for (int p = 0; p < 4; ++p) {
+    const int off = p < nI ? 0 : 12;
+    const double w[4] = {1.0, r[3 * p], r[3 * p + 1], r[3 * p + 2]};
+    for (int m = 0; m < 4; ++m)
+      for (int a = 0; a < 3; ++a) u[off + 3 * m + a] += w[m] * v[3 * p + a];
+  }
 }
 
 // Maps a contact's gradient and Hessian in point coordinates to the affine DOFs of its two

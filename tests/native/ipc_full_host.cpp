@@ -38,6 +38,10 @@ int ipcf_local_gh(int kind, const double* x, const double* r, double dh, double 
 
 void ipcf_project_psd12(double* H) { abd::ipc::project_psd12(H); }
 
+void ipcf_eig_sym12(const double* H, double* lam, double* V) { abd::ipc::eig_sym12(H, lam, V); }
+
+void ipcf_to_affine_vec(const double* v, const double* r, int nI, double* u) { abd::ipc::to_affine_vec(v, r, nI, u); }
+
 void ipcf_to_affine(const double* gx, const double* Hx, const double* r, int nI, double* g24, double* Hi, double* Hj,
                     double* Hij) {
   abd::ipc::to_affine(gx, Hx, r, nI, g24, Hi, Hj, Hij);

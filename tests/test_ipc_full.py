@@ -34,6 +34,8 @@ def L(tmp_path_factory):
     lib.ipcf_local_gh.argtypes = [i, v, v, d, d, v, v, v, v, v]
     lib.ipcf_local_gh.restype = i
     lib.ipcf_project_psd12.argtypes = [v]
+    lib.ipcf_eig_sym12.argtypes = [v, v, v]
+    lib.ipcf_to_affine_vec.argtypes = [v, v, i, v]
     lib.ipcf_to_affine.argtypes = [v, v, v, i, v, v, v, v]
     return lib
 
@@ -203,6 +205,51 @@ def test_psd_projection(L):
         S0 = S.copy()
         L.ipcf_project_psd12(_p(S))
         assert np.allclose(S, S0, rtol=0, atol=1e-11 * np.abs(S0).max())
+
+
+def test_eigen_decomposition(L):
+    """Round-robin Jacobi: H V = V diag(lam), V orthonormal, the spectrum of numpy's eigh."""
+    rng = np.random.default_rng(55)
+    mats = [rng.normal(size=(12, 12)) for _ in range(30)]
+    mats = [m + m.T for m in mats] + [np.diag(rng.normal(size=12)), np.zeros((12, 12))]
+    for A in mats:
+        lam, V = np.zeros(12), np.zeros(144)
+        L.ipcf_eig_sym12(_p(_x(A)), _p(lam), _p(V))
+        V = V.reshape(12, 12)
+        scale = max(np.abs(A).max(), 1e-300)
+        assert np.abs(A @ V - V * lam).max() <= 1e-12 * scale
+        assert np.abs(V.T @ V - np.eye(12)).max() <= 1e-13
+        assert np.allclose(np.sort(lam), np.linalg.eigvalsh(A), rtol=0, atol=1e-12 * scale)
+
+
+def test_rank_one_form_of_a_contact(L):
+    """The projected contact Hessian as rank-one terms lam_k u_k u_k^T over the affine DOFs
+    (u_k = to_affine_vec of eigenvector k): the assembly's form, equal to to_affine of the
+    projected matrix."""
+    rng = np.random.default_rng(57)
+    for kind in (0, 1):
+        x, _ = near_pair(rng, kind, dist=0.05)
+        r = x + rng.normal(size=(4, 3)) * 0.1
+        ok, _, _, _, g, H = local_gh(L, kind, x, r)
+        assert ok
+        lam, V = np.zeros(12), np.zeros(144)
+        L.ipcf_eig_sym12(_p(_x(H)), _p(lam), _p(V))
+        V = V.reshape(12, 12)
+        nI = 1 if kind == 0 else 2
+        H24 = np.zeros((24, 24))
+        for k in range(12):
+            if lam[k] > 0:
+                u = np.zeros(24)
+                L.ipcf_to_affine_vec(_p(np.ascontiguousarray(V[:, k])), _p(_x(r)), nI, _p(u))
+                H24 += lam[k] * np.outer(u, u)
+        Hp = _x(H)
+        L.ipcf_project_psd12(_p(Hp))
+        g24, Hi, Hj, Hij = np.zeros(24), np.zeros(144), np.zeros(144), np.zeros(144)
+        L.ipcf_to_affine(_p(g), _p(Hp), _p(_x(r)), nI, _p(g24), _p(Hi), _p(Hj), _p(Hij))
+        s = np.abs(H24).max()
+        assert np.abs(H24[:12, :12] - Hi.reshape(12, 12)).max() <= 1e-11 * s
+        assert np.abs(H24[12:, 12:] - Hj.reshape(12, 12)).max() <= 1e-11 * s
+        assert np.abs(H24[:12, 12:] - Hij.reshape(12, 12)).max() <= 1e-11 * s
 
 
 def test_to_affine(L):
