@@ -1,4 +1,5 @@
-"""Seeded synthetic scenes for the five benchmark configurations.
+"""Seeded synthetic scenes for the five benchmark configurations (configuration 3, the
+batched workload, is a list of scenes: ``config3``).
 
 The reference publishes no benchmark scenes and its assets are absent, so every scene
 is generated procedurally with ``numpy.random.default_rng(seed)`` (seed = config index
@@ -128,6 +129,36 @@ def config4(seed: int = 4):
         bodies.append(_body(f"icosphere:2:{r}", (x, r + 2 * prm.dhat, z),
                             R=random_rotation(rng), v=v))
     return bodies, prm, 100
+
+
+def config3(seed: int = 3, n_scenes: int = 512):
+    """The batched workload: ``n_scenes`` independent scenes, each with U{2..48} bodies over
+    its own ground box.  Bodies are cubes (edge U(0.15, 0.4)) or level-2 icospheres
+    (r U(0.1, 0.3)), half and half at random, with random rotations and velocities
+    N(0, 0.5^2).  They are placed without overlap (rejection on bounding spheres with a gap of
+    2 dhat) in a 3 x 3 x 3 m box on the ground.  100 steps.  Returns
+    ``(list of body lists, prm, steps)``; each body list is one scene, ground box first."""
+    prm = SimParams()
+    rng = np.random.default_rng(seed)
+    gap = 2 * prm.dhat
+    out = []
+    for _ in range(n_scenes):
+        nb = int(rng.integers(2, 49))
+        bodies = [ground_box()]
+        placed = []
+        while len(placed) < nb:
+            if rng.random() < 0.5:
+                e = float(rng.uniform(0.15, 0.4))
+                spec, rad = f"cube:{e}", 0.5 * np.sqrt(3.0) * e
+            else:
+                r = float(rng.uniform(0.1, 0.3))
+                spec, rad = f"icosphere:2:{r}", r
+            c = rng.uniform([-1.5 + rad, rad + gap, -1.5 + rad], [1.5 - rad, 3.0 - rad, 1.5 - rad])
+            if all(np.linalg.norm(c - c2) > rad + r2 + gap for c2, r2 in placed):
+                placed.append((c, rad))
+                bodies.append(_body(spec, c, R=random_rotation(rng), v=rng.normal(0.0, 0.5, size=3)))
+        out.append(bodies)
+    return out, prm, 100
 
 
 CONFIGS = {0: config0, 1: config1, 2: config2, 4: config4}

@@ -54,3 +54,27 @@ def test_scene_json_with_mesh_map(tmp_path):
     np.testing.assert_array_equal(a.Adot[0], [0.0, 0.5, 0.0])
     np.testing.assert_array_equal(b.A, np.identity(3))
     assert abs(a.mass - 1000.0) < 1e-9  # unit cube, density 1000
+
+
+def test_config3_batched_scenes():
+    """Configuration 3 (the batched workload): independent scenes of 2..48 bodies over their
+    own fixed ground box, deterministic for a seed, bodies apart (bounding spheres more than
+    2 dhat apart) and above the ground."""
+    import numpy as np
+    from abd_warp_b200 import scenes
+
+    sc, prm, steps = scenes.config3(n_scenes=12)
+    again, _, _ = scenes.config3(n_scenes=12)
+    assert steps == 100 and len(sc) == 12
+    for bodies, other in zip(sc, again):
+        assert 3 <= len(bodies) <= 49
+        assert bodies[0].fixed and not any(b.fixed for b in bodies[1:])
+        assert len(other) == len(bodies)
+        for b, c in zip(bodies, other):
+            np.testing.assert_array_equal(b.vertices_world(), c.vertices_world())
+        centres = [b.vertices_world().mean(axis=0) for b in bodies[1:]]
+        radii = [np.linalg.norm(b.vertices_world() - m, axis=1).max() for b, m in zip(bodies[1:], centres)]
+        for i in range(len(centres)):
+            assert bodies[1 + i].vertices_world()[:, 1].min() > 0.0
+            for j in range(i):
+                assert np.linalg.norm(centres[i] - centres[j]) > radii[i] + radii[j] + 2 * prm.dhat - 1e-9
