@@ -13,6 +13,8 @@
 // Jacobi eigenvalue method in round-robin (parallel) order (Golub and Van Loan, Matrix
 // Computations, 8.5).
 //
+// Friction follows the same paper's lagged dissipative potential (section 5).
+//
 // Everything here is plain arithmetic callable from host and device code.
 #pragma once
 
@@ -418,6 +420,148 @@ ABD_HD inline void to_affine(const double gx[12], const double Hx[144], const do
           Hj[12 * (3 * m + a) + 3 * n + b] = sJJ;
           Hij[12 * (3 * m + a) + 3 * n + b] = sIJ;
         }
+}
+
+// ---------------------------------------------------------------------------------------
+// Lagged friction (Li et al. 2020, section 5): at the step start x^t each contact fixes the
+// weights w of its closest points (c_a - c_b = sum_v w_v x_v: + for the first group, - for
+// the second), a tangent basis P (3x2) orthogonal to the separation n = c_a - c_b, and the
+// normal force lambda = -dE/dd of its barrier (mollified for EE).  The friction potential is
+// D(x) = mu lambda f0(|u|), u = P^T sum_v w_v (x_v - x^t_v) the tangential displacement over
+// the step, with f0' = f1(y) = 2 y / eps - y^2 / eps^2 below eps (static friction, eps =
+// eps_v dt) and 1 above (sliding).  Its Hessian is positive semidefinite by construction.
+// ---------------------------------------------------------------------------------------
+struct FrictionLag {
+  double w[4];    // closest-point weights of the four points
+  double P[6];    // tangent basis, row-major 3x2
+  double lambda;  // normal force
+};
+
+// closest-point weights of a classified pair at positions v[4]
+ABD_HD inline void closest_weights(int kind, int type, const V3<double> v[4], double w[4]) {
+  for (int k = 0; k < 4; ++k) w[k] = 0.0;
+  w[0] = 1.0;
+  if (kind == 0) {
+    if (type == PT_P_T) {
+      const V3<double> e1 = sub(v[2], v[1]), e2 = sub(v[3], v[1]), q = sub(v[0], v[1]);
+      const double a = dot(e1, e1), b = dot(e1, e2), c = dot(e2, e2), d = dot(e1, q), e = dot(e2, q);
+      const double det = a * c - b * b, s = (c * d - b * e) / det, t = (a * e - b * d) / det;
+      w[1] = -(1.0 - s - t);
+      w[2] = -s;
+      w[3] = -t;
+    } else if (type <= PT_P_E2) {
+      const int i = 1 + (type - PT_P_E0), j = 1 + (type - PT_P_E0 + 1) % 3;
+      double d2;
+      const double s = point_segment(v[0], v[i], v[j], &d2);
+      w[i] = -(1.0 - s);
+      w[j] = -s;
+    } else {
+      w[1 + type - PT_P_V0] = -1.0;
+    }
+    return;
+  }
+  const V3<double> u = sub(v[1], v[0]), e = sub(v[3], v[2]), q = sub(v[0], v[2]);
+  double s = 0.0, t = 0.0, d2;
+  switch (type) {
+    case EE_EA_EB: {
+      const double a = dot(u, u), b = dot(u, e), c = dot(e, e), d = dot(u, q), f = dot(e, q);
+      const double det = a * c - b * b;
+      s = (b * f - c * d) / det;
+      t = (a * f - b * d) / det;
+      break;
+    }
+    case EE_EA0_EB: t = point_segment(v[0], v[2], v[3], &d2); break;
+    case EE_EA1_EB: s = 1.0; t = point_segment(v[1], v[2], v[3], &d2); break;
+    case EE_EA_EB0: s = point_segment(v[2], v[0], v[1], &d2); break;
+    case EE_EA_EB1: s = point_segment(v[3], v[0], v[1], &d2); t = 1.0; break;
+    case EE_EA0_EB0: break;
+    case EE_EA0_EB1: t = 1.0; break;
+    case EE_EA1_EB0: s = 1.0; break;
+    default: s = 1.0; t = 1.0; break;
+  }
+  w[0] = 1.0 - s;
+  w[1] = s;
+  w[2] = -(1.0 - t);
+  w[3] = -t;
+}
+
+// The lagged quantities of one contact at the step start xt[12] (rest positions r for the
+// EE mollifier); false when the pair is not within dhat there.
+template <class LogFn>
+ABD_HD inline bool friction_lag(int kind, const double xt[12], const double r[12], double dh, double kappa, LogFn lg,
+                                FrictionLag* L) {
+  V3<double> v[4];
+  load(xt, v);
+  const int type = kind == 0 ? pt_type(v[0], v[1], v[2], v[3]) : ee_type(v[0], v[1], v[2], v[3]);
+  const double d2 = kind == 0 ? pt_d2(type, v) : ee_d2(type, v);
+  if (!(d2 < dh) || !(d2 > 0.0)) return false;
+  closest_weights(kind, type, v, L->w);
+  V3<double> n = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 4; ++k) {
+    n.x += L->w[k] * v[k].x;
+    n.y += L->w[k] * v[k].y;
+    n.z += L->w[k] * v[k].z;
+  }
+  const double nl = sqrt(dot(n, n));
+  n = {n.x / nl, n.y / nl, n.z / nl};
+  // tangent basis: the coordinate axis least aligned with n, made orthogonal to it
+  const double ax = fabs(n.x), ay = fabs(n.y), az = fabs(n.z);
+  const V3<double> axis = (ax <= ay && ax <= az) ? V3<double>{1.0, 0.0, 0.0}
+                          : (ay <= az)            ? V3<double>{0.0, 1.0, 0.0}
+                                                  : V3<double>{0.0, 0.0, 1.0};
+  V3<double> t1 = cross(n, axis);
+  const double tl = sqrt(dot(t1, t1));
+  t1 = {t1.x / tl, t1.y / tl, t1.z / tl};
+  const V3<double> t2 = cross(n, t1);
+  L->P[0] = t1.x, L->P[1] = t2.x, L->P[2] = t1.y, L->P[3] = t2.y, L->P[4] = t1.z, L->P[5] = t2.z;
+  // lambda = -dE/dd, E = m b(d^2): -2 d m b'(d^2) with b'(d^2) from the barrier's derivative
+  const double d = sqrt(d2);
+  HD dd = {d, 1.0, 0.0, 0.0};
+  const HD e = barrier_of(dd * dd, dh, kappa, lg);
+  const double m = kind == 1 ? ee_mollifier(v, ee_eps_x(r)) : 1.0;
+  L->lambda = -m * e.a;
+  return true;
+}
+
+// friction potential, gradient g[12] and Hessian H[144] at positions x (step start xt)
+ABD_HD inline double friction_gh(const FrictionLag& L, const double x[12], const double xt[12], double mu,
+                                 double eps, double g[12], double H[144]) {
+  double dx[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 4; ++k)
+    for (int a = 0; a < 3; ++a) dx[a] += L.w[k] * (x[3 * k + a] - xt[3 * k + a]);
+  const double u0 = L.P[0] * dx[0] + L.P[2] * dx[1] + L.P[4] * dx[2];
+  const double u1 = L.P[1] * dx[0] + L.P[3] * dx[1] + L.P[5] * dx[2];
+  const double y = sqrt(u0 * u0 + u1 * u1), c = mu * L.lambda;
+  double f0, f1y, M00, M01, M11;  // f1(y) / y and the 2x2 Hessian of f0(|u|)
+  if (y >= eps) {
+    f0 = y;
+    f1y = 1.0 / y;
+    const double h0 = u0 / y, h1 = u1 / y;
+    M00 = f1y * (1.0 - h0 * h0);
+    M01 = -f1y * h0 * h1;
+    M11 = f1y * (1.0 - h1 * h1);
+  } else {
+    f0 = -y * y * y / (3.0 * eps * eps) + y * y / eps + eps / 3.0;
+    f1y = 2.0 / eps - y / (eps * eps);
+    const double k = y > 0.0 ? 1.0 / (eps * eps * y) : 0.0;  // -(f1' - f1 / y) / y^2
+    M00 = f1y - k * u0 * u0;
+    M01 = -k * u0 * u1;
+    M11 = f1y - k * u1 * u1;
+  }
+  // per point v: d u / d x_v = w_v P^T, so g_v = c w_v P (f1 / y) u, H_vw = c w_v w_w P M P^T
+  const double gu0 = f1y * u0, gu1 = f1y * u1;
+  double PMP[9];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      PMP[3 * a + b] = L.P[2 * a] * (M00 * L.P[2 * b] + M01 * L.P[2 * b + 1]) +
+                       L.P[2 * a + 1] * (M01 * L.P[2 * b] + M11 * L.P[2 * b + 1]);
+  for (int v = 0; v < 4; ++v)
+    for (int a = 0; a < 3; ++a) {
+      g[3 * v + a] = c * L.w[v] * (L.P[2 * a] * gu0 + L.P[2 * a + 1] * gu1);
+      for (int q = 0; q < 4; ++q)
+        for (int b = 0; b < 3; ++b) H[12 * (3 * v + a) + 3 * q + b] = c * L.w[v] * L.w[q] * PMP[3 * a + b];
+    }
+  return c * f0;
 }
 
 }  // namespace ipc

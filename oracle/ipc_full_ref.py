@@ -211,3 +211,45 @@ def sample_d2(kind, x12, n=400):
         S, T = np.meshgrid(s, s, indexing="ij")
         d = (a0 + S.ravel()[:, None] * (a1 - a0)) - (b0 + T.ravel()[:, None] * (b1 - b0))
     return float(np.min(np.einsum("ij,ij->i", d, d)))
+
+
+# ---------------------------------------------------------------------------------------
+# lagged friction (Li et al. 2020, section 5)
+# ---------------------------------------------------------------------------------------
+def closest_weights(kind, x12):
+    """Weights w (4) with sum_v w_v x_v = c_a - c_b, the closest points of the pair's two groups
+    (+ on the first group, - on the second), from this module's own closest points."""
+    x = np.asarray(x12, dtype=np.float64).reshape(4, 3)
+    ca, cb = separation(kind, x)
+    w = np.zeros(4)
+    if kind == 0:
+        w[0] = 1.0
+        t0, t1, t2 = x[1:]
+        # barycentric coordinates of cb in the triangle (least squares on its plane)
+        M = np.stack([t1 - t0, t2 - t0], axis=1)
+        s, t = np.linalg.lstsq(M, cb - t0, rcond=None)[0]
+        w[1:] = -np.array([1.0 - s - t, s, t])
+        return w
+    a0, a1, b0, b1 = x
+    s = float(np.clip(np.linalg.lstsq((a1 - a0)[:, None], ca - a0, rcond=None)[0][0], 0.0, 1.0))
+    t = float(np.clip(np.linalg.lstsq((b1 - b0)[:, None], cb - b0, rcond=None)[0][0], 0.0, 1.0))
+    return np.array([1.0 - s, s, -(1.0 - t), -t])
+
+
+def friction_f0(y, eps):
+    return y if y >= eps else -y ** 3 / (3 * eps * eps) + y * y / eps + eps / 3.0
+
+
+def friction_potential(w, P, lam, x12, xt12, mu, eps):
+    """D(x) = mu lambda f0(|P^T sum_v w_v (x_v - xt_v)|)."""
+    d = np.asarray(w) @ (np.asarray(x12).reshape(4, 3) - np.asarray(xt12).reshape(4, 3))
+    u = np.asarray(P).reshape(3, 2).T @ d
+    return mu * lam * friction_f0(float(np.linalg.norm(u)), eps)
+
+
+def normal_force(kind, x12, r12, dh, kappa, h=1e-7):
+    """lambda = -dE/dd at the pair's distance, E = m b(d^2) (central difference in d)."""
+    _, d2 = classify(kind, x12)
+    d = np.sqrt(d2)
+    m = mollifier(x12, eps_x(r12)) if kind == 1 else 1.0
+    return -m * (barrier((d + h) ** 2, dh, kappa) - barrier((d - h) ** 2, dh, kappa)) / (2 * h)

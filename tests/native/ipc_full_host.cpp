@@ -42,6 +42,25 @@ void ipcf_eig_sym12(const double* H, double* lam, double* V) { abd::ipc::eig_sym
 
 void ipcf_to_affine_vec(const double* v, const double* r, int nI, double* u) { abd::ipc::to_affine_vec(v, r, nI, u); }
 
+int ipcf_friction_lag(int kind, const double* xt, const double* r, double dh, double kappa, double* w, double* P,
+                      double* lambda) {
+  abd::ipc::FrictionLag L;
+  if (!abd::ipc::friction_lag(kind, xt, r, dh, kappa, StdLog(), &L)) return 0;
+  for (int k = 0; k < 4; ++k) w[k] = L.w[k];
+  for (int k = 0; k < 6; ++k) P[k] = L.P[k];
+  *lambda = L.lambda;
+  return 1;
+}
+
+double ipcf_friction_gh(const double* w, const double* P, double lambda, const double* x, const double* xt, double mu,
+                        double eps, double* g, double* H) {
+  abd::ipc::FrictionLag L;
+  for (int k = 0; k < 4; ++k) L.w[k] = w[k];
+  for (int k = 0; k < 6; ++k) L.P[k] = P[k];
+  L.lambda = lambda;
+  return abd::ipc::friction_gh(L, x, xt, mu, eps, g, H);
+}
+
 void ipcf_to_affine(const double* gx, const double* Hx, const double* r, int nI, double* g24, double* Hi, double* Hj,
                     double* Hij) {
   abd::ipc::to_affine(gx, Hx, r, nI, g24, Hi, Hj, Hij);

@@ -365,3 +365,90 @@ def test_oracle_full_mode_steps():
             lost_ref += a["n_active"] == 0
             assert _min_surface_distance(flat, full.get_state()["x_view"]) > 0.5 * prm.dhat
     assert contact and lost_ref > 0
+
+
+def _friction_lag(L, kind, xt, r):
+    w, P, lam = np.zeros(4), np.zeros(6), ctypes.c_double(0)
+    ok = L.ipcf_friction_lag(kind, _p(_x(xt)), _p(_x(r)), DH, KAPPA, _p(w), _p(P), ctypes.byref(lam))
+    return bool(ok), w, P, lam.value
+
+
+def _friction_gh(L, w, P, lam, x, xt, mu, eps):
+    g, H = np.zeros(12), np.zeros(144)
+    D = L.ipcf_friction_gh(_p(w), _p(P), lam, _p(_x(x)), _p(_x(xt)), mu, eps, _p(g), _p(H))
+    return D, g, H.reshape(12, 12)
+
+
+@pytest.fixture(scope="module")
+def Lf(L):
+    v, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.ipcf_friction_lag.argtypes = [i, v, v, d, d, v, v, v]
+    L.ipcf_friction_lag.restype = i
+    L.ipcf_friction_gh.argtypes = [v, v, d, v, v, d, d, v, v]
+    L.ipcf_friction_gh.restype = d
+    return L
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_friction_lagged_quantities(Lf, kind):
+    """At the step start: the weights give the separation of the closest points (as this
+    module's restatement finds them), P is an orthonormal basis of the plane orthogonal to
+    it, and lambda is the barrier's -dE/dd."""
+    rng = np.random.default_rng(90 + kind)
+    seen = set()
+    done = 0
+    while done < 40:
+        xt, ty = near_pair(rng, kind, dist=0.05)
+        if not _tie_free(kind, xt, tol=1e-6):
+            continue
+        r = xt + rng.normal(size=(4, 3)) * (0.1 if done % 2 else 2.0)
+        ok, w, P, lam = _friction_lag(Lf, kind, xt, r)
+        assert ok
+        ca, cb = R.separation(kind, xt)
+        assert np.allclose(w @ xt, ca - cb, rtol=0, atol=1e-12)
+        assert np.allclose(w, R.closest_weights(kind, xt), rtol=0, atol=1e-9)
+        n = (ca - cb) / np.linalg.norm(ca - cb)
+        Pm = P.reshape(3, 2)
+        assert np.allclose(Pm.T @ Pm, np.eye(2), atol=1e-14) and np.allclose(Pm.T @ n, 0.0, atol=1e-10)
+        assert lam > 0 and lam == pytest.approx(R.normal_force(kind, xt, r, DH, KAPPA), rel=1e-6)
+        seen.add(ty)
+        done += 1
+    assert len(seen) >= 4
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("regime", ["static", "sliding"])
+def test_friction_gradient_hessian(Lf, kind, regime):
+    """D, its gradient (central differences, 1e-6) and Hessian (1e-4, positive semidefinite)
+    below eps (static friction) and above (sliding); the tangential force stays within the
+    Coulomb bound mu lambda and reaches it when sliding."""
+    mu, eps = 0.4, 1e-3
+    rng = np.random.default_rng(100 + kind + (2 if regime == "sliding" else 0))
+    done = 0
+    while done < 20:
+        xt, _ = near_pair(rng, kind, dist=0.05)
+        ok, w, P, lam = _friction_lag(Lf, kind, xt, xt)
+        if not ok:
+            continue
+        y_goal = 0.4 * eps if regime == "static" else 5 * eps
+        dx = rng.normal(size=(4, 3))
+        dx *= y_goal / max(np.linalg.norm(P.reshape(3, 2).T @ (w @ dx)), 1e-300)
+        x = xt + dx
+        D, g, H = _friction_gh(Lf, w, P, lam, x, xt, mu, eps)
+        f = lambda y: R.friction_potential(w, P, lam, y, xt, mu, eps)
+        assert D == pytest.approx(f(_x(x)), rel=1e-12)
+        h = 1e-4 * eps
+        I = np.eye(12) * h
+        xf = _x(x)
+        gf = np.array([(f(xf + I[i]) - f(xf - I[i])) / (2 * h) for i in range(12)])
+        Hf = np.array([[(f(xf + I[i] + I[j]) - f(xf + I[i] - I[j]) - f(xf - I[i] + I[j]) + f(xf - I[i] - I[j]))
+                        / (4 * h * h) for j in range(12)] for i in range(12)])
+        assert np.linalg.norm(g - gf) <= 1e-6 * np.linalg.norm(gf)
+        assert np.linalg.norm(H - Hf) <= 1e-4 * np.linalg.norm(Hf)
+        assert np.linalg.eigvalsh(H).min() >= -1e-12 * np.abs(H).max()
+        v = int(np.argmax(np.abs(w)))  # a point's share of the force, per unit weight
+        force = np.linalg.norm(g[3 * v:3 * v + 3]) / abs(w[v])
+        assert force <= mu * lam * (1 + 1e-12)
+        if regime == "sliding":
+            assert force == pytest.approx(mu * lam, rel=1e-12)
+        done += 1
