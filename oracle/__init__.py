@@ -61,6 +61,7 @@ def lib():
         L.orc_set_ipc_full.argtypes = [v, i]
         L.orc_full_terms.argtypes = [i, v, v, v, i, v, v, v, v]
         L.orc_full_terms.restype = i
+        L.orc_set_friction.argtypes = [v, d, d]
         L.orc_full_hessian.argtypes = [v, v, v, v]
         L.orc_full_hessian.restype = i
         L.orc_cubic_roots.argtypes = [v, d, d, v]
@@ -122,6 +123,11 @@ class Oracle:
         """The full IPC contact model (closest-feature types, edge-edge mollifier, inclusive
         CCD) instead of the reference's interior-only model."""
         lib().orc_set_ipc_full(self.h, 1 if on else 0)
+
+    def set_friction(self, mu: float, eps_v: float = 1e-3):
+        """Lagged friction (coefficient mu, slip velocity eps_v) on the full contact model's
+        contacts; 0 turns it off."""
+        lib().orc_set_friction(self.h, float(mu), float(eps_v))
 
     def full_hessian(self, A, p):
         """Exact, unprojected Hessian of the step's energy at (A, p) under the full contact

@@ -201,6 +201,15 @@ struct Oracle {
       stat_active = 0, stat_refine = 0;
   int last_sweeps = 0;  // refinement sweeps of the last mixed-precision solve
   bool ipc_full = false;  // full IPC contact model (closest-feature types, mollifier)
+  // lagged friction (with the full model): coefficient, slip velocity, and the contacts that
+  // the step fixed at its start
+  double fr_mu = 0.0, fr_epsv = 1e-3;
+  struct Fric {
+    int I, J, kind;  // the first group (point / edge a) moves with I
+    double w[4], P[6], lam, xt[12], rs[12];
+    int ids[4];
+  };
+  std::vector<Fric> fric;
   double stat_alpha = 0, stat_toi = 0, stat_energy = 0;
 };
 
@@ -1073,6 +1082,214 @@ double full_energy(int kind, const V3 xs[4], const V3 rs[4], const Params& P) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Lagged friction (Li et al. 2020, section 5), with the full contact model: at the step start
+// each contact within dhat fixes the weights w of its closest points (c_a - c_b =
+// sum_v w_v x_v), a basis P of the plane orthogonal to c_a - c_b, and its normal force
+// lambda = -dE/dd.  D(x) = mu lambda f0(|P^T sum_v w_v (x_v - x^t_v)|), f0' = 2y/eps -
+// y^2/eps^2 below eps = eps_v dt, 1 above.
+// ---------------------------------------------------------------------------------------
+void fric_weights(int kind, int type, const V3 x[4], double w[4]) {
+  for (int k = 0; k < 4; ++k) w[k] = 0.0;
+  w[0] = 1.0;
+  if (kind == 0) {
+    const V3 p = x[0], t0 = x[1], t1 = x[2], t2 = x[3];
+    if (type == F_PT) {  // barycentric coordinates of the projection from sub-triangle areas
+      const V3 n = cross(t1 - t0, t2 - t0);
+      const double nn = dot(n, n);
+      const V3 q = p - n * (dot(p - t0, n) / nn);
+      w[1] = -dot(cross(t1 - q, t2 - q), n) / nn;
+      w[2] = -dot(cross(t2 - q, t0 - q), n) / nn;
+      w[3] = -dot(cross(t0 - q, t1 - q), n) / nn;
+    } else if (type <= F_PE2) {
+      const int a = type - F_PE0, b = (a + 1) % 3;
+      double d2;
+      const double s = seg_param(p, x[1 + a], x[1 + b], d2);
+      w[1 + a] = -(1.0 - s);
+      w[1 + b] = -s;
+    } else {
+      w[1 + type - F_PV0] = -1.0;
+    }
+    return;
+  }
+  double s = 0.0, t = 0.0, d2;
+  if (type == F_EE) {
+    const V3 u = x[1] - x[0], v = x[3] - x[2], q = x[0] - x[2];
+    const double a = dot(u, u), b = dot(u, v), c = dot(v, v), d = dot(u, q), e = dot(v, q);
+    const double D = a * c - b * b;
+    s = (b * e - c * d) / D;
+    t = (a * e - b * d) / D;
+  } else if (type == F_A0B) {
+    t = seg_param(x[0], x[2], x[3], d2);
+  } else if (type == F_A1B) {
+    s = 1.0;
+    t = seg_param(x[1], x[2], x[3], d2);
+  } else if (type == F_AB0) {
+    s = seg_param(x[2], x[0], x[1], d2);
+  } else if (type == F_AB1) {
+    s = seg_param(x[3], x[0], x[1], d2);
+    t = 1.0;
+  } else {
+    s = (type == F_A1B0 || type == F_A1B1) ? 1.0 : 0.0;
+    t = (type == F_A0B1 || type == F_A1B1) ? 1.0 : 0.0;
+  }
+  w[0] = 1.0 - s;
+  w[1] = s;
+  w[2] = -(1.0 - t);
+  w[3] = -t;
+}
+
+// the contacts within dhat at DOFs (A0, p0), with their lagged quantities
+void friction_lag(Oracle& o) {
+  o.fric.clear();
+  if (!(o.fr_mu > 0.0) || !o.ipc_full) return;
+  std::vector<double> xt(3 * (size_t)o.V);
+  transform(o, o.A0.data(), o.p0.data(), xt.data());
+  Boxes bx;
+  Lists L;
+  static_boxes(o, xt.data(), bx);
+  cull(o, bx, L);
+  for (int kind = 0; kind < 2; ++kind)
+    for (const Cand& cd : kind == 0 ? L.pt : L.ee) {
+      V3 xs[4], rs[4];
+      fetch(o, xt.data(), cd, kind, xs, rs);
+      const int type = kind == 0 ? full_pt_type(xs) : full_ee_type(xs);
+      Oracle::Fric f;
+      fric_weights(kind, type, xs, f.w);
+      V3 n = {0.0, 0.0, 0.0};
+      for (int k = 0; k < 4; ++k) n = n + xs[k] * f.w[k];
+      const double d2 = dot(n, n);
+      if (!(d2 < o.prm.d2hat) || !(d2 > 0.0)) continue;
+      const double d = std::sqrt(d2);
+      n = n * (1.0 / d);
+      // basis: the coordinate axis least aligned with n, made orthogonal to it
+      const double an[3] = {std::fabs(n.x), std::fabs(n.y), std::fabs(n.z)};
+      const int ax = an[0] <= an[1] && an[0] <= an[2] ? 0 : (an[1] <= an[2] ? 1 : 2);
+      V3 e = {ax == 0 ? 1.0 : 0.0, ax == 1 ? 1.0 : 0.0, ax == 2 ? 1.0 : 0.0};
+      V3 t1 = cross(n, e);
+      t1 = t1 * (1.0 / std::sqrt(dot(t1, t1)));
+      const V3 t2 = cross(n, t1);
+      const double P[6] = {t1.x, t2.x, t1.y, t2.y, t1.z, t2.z};
+      std::memcpy(f.P, P, sizeof(P));
+      double m = 1.0;
+      if (kind == 1) {
+        const V3 ra = rs[1] - rs[0], rb = rs[3] - rs[2];
+        const double ex = 1e-3 * dot(ra, ra) * dot(rb, rb);
+        const V3 c = cross(xs[1] - xs[0], xs[3] - xs[2]);
+        const double cc = dot(c, c);
+        if (cc < ex) m = (2.0 - cc / ex) * cc / ex;
+      }
+      f.lam = -2.0 * d * m * barrier_d1(d2, o.prm);
+      f.kind = kind;
+      f.I = cd.I;
+      f.J = cd.J;
+      for (int k = 0; k < 4; ++k) {
+        const V3 v[2] = {xs[k], rs[k]};
+        f.xt[3 * k] = v[0].x, f.xt[3 * k + 1] = v[0].y, f.xt[3 * k + 2] = v[0].z;
+        f.rs[3 * k] = v[1].x, f.rs[3 * k + 1] = v[1].y, f.rs[3 * k + 2] = v[1].z;
+      }
+      // the vertex ids, for reading the current positions
+      if (kind == 0) {
+        f.ids[0] = o.voff[cd.I] + cd.pi;
+        const int t = o.toff[cd.J] + cd.pj;
+        for (int k = 0; k < 3; ++k) f.ids[1 + k] = o.tris[3 * t + k];
+      } else {
+        const int ea = o.eoff[cd.I] + cd.pi, eb = o.eoff[cd.J] + cd.pj;
+        f.ids[0] = o.edges[2 * ea];
+        f.ids[1] = o.edges[2 * ea + 1];
+        f.ids[2] = o.edges[2 * eb];
+        f.ids[3] = o.edges[2 * eb + 1];
+      }
+      o.fric.push_back(f);
+    }
+}
+
+// D, gradient g[12] and Hessian H[144] of one lagged contact at positions y (all vertices)
+double friction_gh(const Oracle& o, const Oracle::Fric& f, const double* y, double* g, double* H) {
+  const double eps = o.fr_epsv * o.prm.dt, c = o.fr_mu * f.lam;
+  double dx[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 4; ++k)
+    for (int a = 0; a < 3; ++a) dx[a] += f.w[k] * (y[3 * f.ids[k] + a] - f.xt[3 * k + a]);
+  const double u0 = f.P[0] * dx[0] + f.P[2] * dx[1] + f.P[4] * dx[2];
+  const double u1 = f.P[1] * dx[0] + f.P[3] * dx[1] + f.P[5] * dx[2];
+  const double yy = std::sqrt(u0 * u0 + u1 * u1);
+  double f0, f1y, M[3];
+  if (yy >= eps) {
+    f0 = yy;
+    f1y = 1.0 / yy;
+    M[0] = f1y * (1.0 - u0 * u0 / (yy * yy));
+    M[1] = -f1y * u0 * u1 / (yy * yy);
+    M[2] = f1y * (1.0 - u1 * u1 / (yy * yy));
+  } else {
+    f0 = -yy * yy * yy / (3.0 * eps * eps) + yy * yy / eps + eps / 3.0;
+    f1y = 2.0 / eps - yy / (eps * eps);
+    const double k = yy > 0.0 ? 1.0 / (eps * eps * yy) : 0.0;
+    M[0] = f1y - k * u0 * u0;
+    M[1] = -k * u0 * u1;
+    M[2] = f1y - k * u1 * u1;
+  }
+  if (g && H) {
+    for (int v = 0; v < 4; ++v)
+      for (int a = 0; a < 3; ++a) {
+        g[3 * v + a] = c * f.w[v] * f1y * (f.P[2 * a] * u0 + f.P[2 * a + 1] * u1);
+        for (int q = 0; q < 4; ++q)
+          for (int b = 0; b < 3; ++b) {
+            const double pmp = f.P[2 * a] * (M[0] * f.P[2 * b] + M[1] * f.P[2 * b + 1]) +
+                               f.P[2 * a + 1] * (M[1] * f.P[2 * b] + M[2] * f.P[2 * b + 1]);
+            H[12 * (3 * v + a) + 3 * q + b] = c * f.w[v] * f.w[q] * pmp;
+          }
+      }
+  }
+  return c * f0;
+}
+
+// point-coordinate gradient / Hessian of a contact (first nI points with the first group's
+// body) as the pair terms out[456] = H_IJ, H_II, H_JJ, g; swap as in contact_terms
+void affine_terms(const double rs12[12], int nI, const double* g12, const double* H12, int swap, double out[456]) {
+  double w[4][4];
+  for (int v = 0; v < 4; ++v) {
+    w[v][0] = 1.0;
+    for (int m = 1; m < 4; ++m) w[v][m] = rs12[3 * v + m - 1];
+  }
+  double G[2][12], B[2][2][144];
+  std::memset(G, 0, sizeof(G));
+  std::memset(B, 0, sizeof(B));
+  for (int u = 0; u < 4; ++u)
+    for (int m = 0; m < 4; ++m)
+      for (int a = 0; a < 3; ++a) {
+        const int gu = u < nI ? 0 : 1;
+        G[gu][3 * m + a] += w[u][m] * g12[3 * u + a];
+        for (int v = 0; v < 4; ++v)
+          for (int n2 = 0; n2 < 4; ++n2)
+            for (int b = 0; b < 3; ++b)
+              B[gu][v < nI ? 0 : 1][12 * (3 * m + a) + 3 * n2 + b] += w[u][m] * H12[12 * (3 * u + a) + 3 * v + b] * w[v][n2];
+      }
+  const int I = swap ? 1 : 0, J = 1 - I;
+  for (int e = 0; e < 144; ++e) {
+    out[e] = B[I][J][e];
+    out[144 + e] = B[I][I][e];
+    out[288 + e] = B[J][J][e];
+  }
+  for (int e = 0; e < 12; ++e) {
+    out[432 + e] = G[I][e];
+    out[444 + e] = G[J][e];
+  }
+}
+
+// the body pairs of the lagged contacts join the culled pairs (a contact may outlast the
+// overlap of its bodies' boxes during the step)
+void add_friction_pairs(const Oracle& o, Lists& L) {
+  for (const Oracle::Fric& f : o.fric) {
+    const int a = std::min(f.I, f.J), b = std::max(f.I, f.J);
+    bool have = false;
+    for (size_t q = 0; q + 1 < L.ij.size() && !have; q += 2) have = L.ij[q] == a && L.ij[q + 1] == b;
+    if (!have) {
+      L.ij.push_back(a);
+      L.ij.push_back(b);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // inertia + orthogonality (orthogonal_energy.py:24-135)
 // ---------------------------------------------------------------------------------------
 inline V3 row(const double* A, int k) { return {A[3 * k], A[3 * k + 1], A[3 * k + 2]}; }
@@ -1211,6 +1428,20 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
         ++o.pact[R[i].pair];
         ++active;
       }
+  }
+  for (const Oracle::Fric& f : o.fric) {  // lagged friction: terms of the contact's body pair
+    const int a = std::min(f.I, f.J), b = std::max(f.I, f.J);
+    int q = -1;
+    for (int k = 0; k < m && q < 0; ++k)
+      if (L.ij[2 * k] == a && L.ij[2 * k + 1] == b) q = k;
+    if (q < 0) continue;
+    double g12[12], H12[144];
+    friction_gh(o, f, y, g12, H12);
+    Act act;
+    act.pair = q;
+    affine_terms(f.rs, f.kind == 0 ? 1 : 2, g12, H12, f.I != L.ij[2 * q], act.v);
+    acts.push_back(act);
+    ++o.pact[q];
   }
   // per pair: exact sums of its contacts, rounded (H_IJ, contributions to diag I / J, g I / J)
   std::vector<double> pdiag(288 * (size_t)m, 0.0), pgrad(24 * (size_t)m, 0.0);
@@ -1908,6 +2139,7 @@ double energy_at(Oracle& o, const double* y, const double* Akp, const double* pk
     const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
     total.add(barrier(d * d, o.prm));
   }
+  for (const Oracle::Fric& f : o.fric) total.add(friction_gh(o, f, y, nullptr, nullptr));
   for (int b = 0; b < o.n; ++b)
     if (!o.fixed[b]) total.add(inertia_energy(o, b, Akp, pkp));
   return total.round();
@@ -1961,6 +2193,7 @@ void step(Oracle& o) {
   o.p = o.p0;
   o.Ak = o.A0;
   o.pk = o.p0;
+  friction_lag(o);
   double E0 = compute_energy(o, 0.0);
   int it = 0, lin = 0, ls = 0, sweeps = 0;
   for (;;) {
@@ -1976,6 +2209,7 @@ void step(Oracle& o) {
       o.stat_vg = (int)L.vg.size() / 2;
       o.stat_ij = (int)L.ij.size() / 2;
     }
+    add_friction_pairs(o, L);
     assemble(o, o.x.data(), bx, L);
     lin += solve(o);
     sweeps += o.last_sweeps;
@@ -2062,6 +2296,11 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
 void orc_destroy(void* h) { delete (Oracle*)h; }
 void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
 void orc_set_ipc_full(void* h, int on) { ((Oracle*)h)->ipc_full = on != 0; }
+// lagged friction with coefficient mu and slip velocity eps_v (needs the full contact model)
+void orc_set_friction(void* h, double mu, double eps_v) {
+  ((Oracle*)h)->fr_mu = mu;
+  ((Oracle*)h)->fr_epsv = eps_v;
+}
 
 // full-model pair terms of one candidate (swap as in the assembly): out[456] = H_IJ, H_II,
 // H_JJ, g; *E the energy, *d2 the classified squared distance, *type its feature pair

@@ -452,3 +452,31 @@ def test_friction_gradient_hessian(Lf, kind, regime):
         if regime == "sliding":
             assert force == pytest.approx(mu * lam, rel=1e-12)
         done += 1
+
+
+def test_oracle_friction_sliding_cube():
+    """A cube sliding on the ground box at 1 m/s (full contact model, lagged friction in the
+    oracle): without friction it keeps its speed; with mu = 0.5 it decelerates at mu g
+    (Coulomb) until it stops at t = v0 / (mu g), and static friction then holds it."""
+    from abd_warp_b200 import scenes
+
+    prm = SimParams()
+    prm.max_iter, prm.tol = 100, 1e-12  # converged steps
+    g = -prm.gravity
+    bodies = [scenes.ground_box(), scenes._body("cube:0.3", (0.0, 0.15 + 1.2 * prm.dhat, 0.0), v=(1.0, 0.0, 0.0))]
+    flat = scenes.flatten_bodies(bodies)
+    for mu in (0.0, 0.5):
+        o = oracle.Oracle(flat, prm)
+        o.set_ipc_full(True)
+        o.set_friction(mu, 1e-3)
+        for k in range(1, 31):
+            info = o.step()
+            vx = o.get_state()["pdot"][1, 0]
+            assert info["n_active"] > 0
+            if mu == 0.0:
+                assert vx == pytest.approx(1.0, abs=1e-6)
+            elif 3 <= k and k * prm.dt < 1.0 / (mu * g) - 2 * prm.dt:
+                # the cube lands in step 1; step 2 lags the landing's normal force
+                assert vx == pytest.approx(1.0 - mu * g * (k - 1) * prm.dt, abs=1e-3)
+            elif k * prm.dt > 1.0 / (mu * g) + 2 * prm.dt:
+                assert abs(vx) < 1e-6
