@@ -62,6 +62,8 @@ def lib():
         L.orc_full_terms.argtypes = [i, v, v, v, i, v, v, v, v]
         L.orc_full_terms.restype = i
         L.orc_set_friction.argtypes = [v, d, d]
+        L.orc_friction_contact.argtypes = [i, v, v, v, d, d, v, v, v, v, v, v]
+        L.orc_friction_contact.restype = i
         L.orc_full_hessian.argtypes = [v, v, v, v]
         L.orc_full_hessian.restype = i
         L.orc_cubic_roots.argtypes = [v, d, d, v]
@@ -238,6 +240,18 @@ def full_terms(kind, x4, r4, prm, swap=0):
                              ctypes.byref(ty))
     return (bool(a), E.value, d2.value, ty.value, out[:144].reshape(12, 12), out[144:288].reshape(12, 12),
             out[288:432].reshape(12, 12), out[432:])
+
+
+def friction_contact(kind, xt4, r4, prm, mu, eps, x4):
+    """One candidate's lagged friction, fixed at xt4 and evaluated at x4:
+    (active, D, g (12), H (12x12), weights (4), lambda)."""
+    xt4, r4, x4 = _c64(xt4), _c64(r4), _c64(x4)
+    c = prm.to_c()
+    D, lam = ctypes.c_double(0), ctypes.c_double(0)
+    g, H, w = np.zeros(12), np.zeros((12, 12)), np.zeros(4)
+    a = lib().orc_friction_contact(kind, _p(xt4), _p(r4), ctypes.byref(c), mu, eps, _p(x4), ctypes.byref(D), _p(g),
+                                   _p(H), _p(w), ctypes.byref(lam))
+    return bool(a), D.value, g, H, w, lam.value
 
 
 def abd_log(x: float) -> float:

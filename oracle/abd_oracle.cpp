@@ -1138,6 +1138,43 @@ void fric_weights(int kind, int type, const V3 x[4], double w[4]) {
   w[3] = -t;
 }
 
+// the lagged quantities of one candidate at its step-start positions xs (rest positions rs);
+// false when it is not within dhat there
+bool make_fric(int kind, const V3 xs[4], const V3 rs[4], const Params& P, Oracle::Fric& f) {
+  const int type = kind == 0 ? full_pt_type(xs) : full_ee_type(xs);
+  fric_weights(kind, type, xs, f.w);
+  V3 n = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 4; ++k) n = n + xs[k] * f.w[k];
+  const double d2 = dot(n, n);
+  if (!(d2 < P.d2hat) || !(d2 > 0.0)) return false;
+  const double d = std::sqrt(d2);
+  n = n * (1.0 / d);
+  // basis: the coordinate axis least aligned with n, made orthogonal to it
+  const double an[3] = {std::fabs(n.x), std::fabs(n.y), std::fabs(n.z)};
+  const int ax = an[0] <= an[1] && an[0] <= an[2] ? 0 : (an[1] <= an[2] ? 1 : 2);
+  const V3 e = {ax == 0 ? 1.0 : 0.0, ax == 1 ? 1.0 : 0.0, ax == 2 ? 1.0 : 0.0};
+  V3 t1 = cross(n, e);
+  t1 = t1 * (1.0 / std::sqrt(dot(t1, t1)));
+  const V3 t2 = cross(n, t1);
+  const double B[6] = {t1.x, t2.x, t1.y, t2.y, t1.z, t2.z};
+  std::memcpy(f.P, B, sizeof(B));
+  double m = 1.0;
+  if (kind == 1) {
+    const V3 ra = rs[1] - rs[0], rb = rs[3] - rs[2];
+    const double ex = 1e-3 * dot(ra, ra) * dot(rb, rb);
+    const V3 c = cross(xs[1] - xs[0], xs[3] - xs[2]);
+    const double cc = dot(c, c);
+    if (cc < ex) m = (2.0 - cc / ex) * cc / ex;
+  }
+  f.lam = -2.0 * d * m * barrier_d1(d2, P);
+  f.kind = kind;
+  for (int k = 0; k < 4; ++k) {
+    f.xt[3 * k] = xs[k].x, f.xt[3 * k + 1] = xs[k].y, f.xt[3 * k + 2] = xs[k].z;
+    f.rs[3 * k] = rs[k].x, f.rs[3 * k + 1] = rs[k].y, f.rs[3 * k + 2] = rs[k].z;
+  }
+  return true;
+}
+
 // the contacts within dhat at DOFs (A0, p0), with their lagged quantities
 void friction_lag(Oracle& o) {
   o.fric.clear();
@@ -1152,41 +1189,10 @@ void friction_lag(Oracle& o) {
     for (const Cand& cd : kind == 0 ? L.pt : L.ee) {
       V3 xs[4], rs[4];
       fetch(o, xt.data(), cd, kind, xs, rs);
-      const int type = kind == 0 ? full_pt_type(xs) : full_ee_type(xs);
       Oracle::Fric f;
-      fric_weights(kind, type, xs, f.w);
-      V3 n = {0.0, 0.0, 0.0};
-      for (int k = 0; k < 4; ++k) n = n + xs[k] * f.w[k];
-      const double d2 = dot(n, n);
-      if (!(d2 < o.prm.d2hat) || !(d2 > 0.0)) continue;
-      const double d = std::sqrt(d2);
-      n = n * (1.0 / d);
-      // basis: the coordinate axis least aligned with n, made orthogonal to it
-      const double an[3] = {std::fabs(n.x), std::fabs(n.y), std::fabs(n.z)};
-      const int ax = an[0] <= an[1] && an[0] <= an[2] ? 0 : (an[1] <= an[2] ? 1 : 2);
-      V3 e = {ax == 0 ? 1.0 : 0.0, ax == 1 ? 1.0 : 0.0, ax == 2 ? 1.0 : 0.0};
-      V3 t1 = cross(n, e);
-      t1 = t1 * (1.0 / std::sqrt(dot(t1, t1)));
-      const V3 t2 = cross(n, t1);
-      const double P[6] = {t1.x, t2.x, t1.y, t2.y, t1.z, t2.z};
-      std::memcpy(f.P, P, sizeof(P));
-      double m = 1.0;
-      if (kind == 1) {
-        const V3 ra = rs[1] - rs[0], rb = rs[3] - rs[2];
-        const double ex = 1e-3 * dot(ra, ra) * dot(rb, rb);
-        const V3 c = cross(xs[1] - xs[0], xs[3] - xs[2]);
-        const double cc = dot(c, c);
-        if (cc < ex) m = (2.0 - cc / ex) * cc / ex;
-      }
-      f.lam = -2.0 * d * m * barrier_d1(d2, o.prm);
-      f.kind = kind;
+      if (!make_fric(kind, xs, rs, o.prm, f)) continue;
       f.I = cd.I;
       f.J = cd.J;
-      for (int k = 0; k < 4; ++k) {
-        const V3 v[2] = {xs[k], rs[k]};
-        f.xt[3 * k] = v[0].x, f.xt[3 * k + 1] = v[0].y, f.xt[3 * k + 2] = v[0].z;
-        f.rs[3 * k] = v[1].x, f.rs[3 * k + 1] = v[1].y, f.rs[3 * k + 2] = v[1].z;
-      }
       // the vertex ids, for reading the current positions
       if (kind == 0) {
         f.ids[0] = o.voff[cd.I] + cd.pi;
@@ -1204,8 +1210,8 @@ void friction_lag(Oracle& o) {
 }
 
 // D, gradient g[12] and Hessian H[144] of one lagged contact at positions y (all vertices)
-double friction_gh(const Oracle& o, const Oracle::Fric& f, const double* y, double* g, double* H) {
-  const double eps = o.fr_epsv * o.prm.dt, c = o.fr_mu * f.lam;
+double friction_gh(double mu, double eps, const Oracle::Fric& f, const double* y, double* g, double* H) {
+  const double c = mu * f.lam;
   double dx[3] = {0.0, 0.0, 0.0};
   for (int k = 0; k < 4; ++k)
     for (int a = 0; a < 3; ++a) dx[a] += f.w[k] * (y[3 * f.ids[k] + a] - f.xt[3 * k + a]);
@@ -1436,7 +1442,7 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
       if (L.ij[2 * k] == a && L.ij[2 * k + 1] == b) q = k;
     if (q < 0) continue;
     double g12[12], H12[144];
-    friction_gh(o, f, y, g12, H12);
+    friction_gh(o.fr_mu, o.fr_epsv * o.prm.dt, f, y, g12, H12);
     Act act;
     act.pair = q;
     affine_terms(f.rs, f.kind == 0 ? 1 : 2, g12, H12, f.I != L.ij[2 * q], act.v);
@@ -2139,7 +2145,7 @@ double energy_at(Oracle& o, const double* y, const double* Akp, const double* pk
     const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
     total.add(barrier(d * d, o.prm));
   }
-  for (const Oracle::Fric& f : o.fric) total.add(friction_gh(o, f, y, nullptr, nullptr));
+  for (const Oracle::Fric& f : o.fric) total.add(friction_gh(o.fr_mu, o.fr_epsv * o.prm.dt, f, y, nullptr, nullptr));
   for (int b = 0; b < o.n; ++b)
     if (!o.fixed[b]) total.add(inertia_energy(o, b, Akp, pkp));
   return total.round();
@@ -2297,6 +2303,24 @@ void orc_destroy(void* h) { delete (Oracle*)h; }
 void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
 void orc_set_ipc_full(void* h, int on) { ((Oracle*)h)->ipc_full = on != 0; }
 // lagged friction with coefficient mu and slip velocity eps_v (needs the full contact model)
+// one candidate's lagged friction: fixed at step-start positions xt12 (rest rs12), evaluated at
+// x12 with coefficient mu and threshold eps (displacement); returns 0 when not within dhat
+int orc_friction_contact(int kind, const double* xt12, const double* rs12, const Params* prm, double mu, double eps,
+                         const double* x12, double* D, double* g12, double* H144, double* w, double* lam) {
+  V3 xs[4], rs[4];
+  for (int k = 0; k < 4; ++k) {
+    xs[k] = {xt12[3 * k], xt12[3 * k + 1], xt12[3 * k + 2]};
+    rs[k] = {rs12[3 * k], rs12[3 * k + 1], rs12[3 * k + 2]};
+  }
+  Oracle::Fric f;
+  if (!make_fric(kind, xs, rs, *prm, f)) return 0;
+  for (int k = 0; k < 4; ++k) f.ids[k] = k;
+  *D = friction_gh(mu, eps, f, x12, g12, H144);
+  for (int k = 0; k < 4; ++k) w[k] = f.w[k];
+  *lam = f.lam;
+  return 1;
+}
+
 void orc_set_friction(void* h, double mu, double eps_v) {
   ((Oracle*)h)->fr_mu = mu;
   ((Oracle*)h)->fr_epsv = eps_v;

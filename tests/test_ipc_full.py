@@ -480,3 +480,30 @@ def test_oracle_friction_sliding_cube():
                 assert vx == pytest.approx(1.0 - mu * g * (k - 1) * prm.dt, abs=1e-3)
             elif k * prm.dt > 1.0 / (mu * g) + 2 * prm.dt:
                 assert abs(vx) < 1e-6
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_oracle_friction_matches_the_header(Lf, kind):
+    """The oracle's lagged friction (its own weights from sub-triangle areas, its own basis)
+    against the header's per contact: weights, normal force, D, gradient and Hessian (which do
+    not depend on the choice of tangent basis), static and sliding."""
+    prm = SimParams()
+    prm.dhat, prm.kappa = float(np.sqrt(DH)), KAPPA
+    mu, eps = 0.3, 1e-3
+    rng = np.random.default_rng(120 + kind)
+    done = 0
+    while done < 30:
+        xt, _ = near_pair(rng, kind, dist=0.05)
+        if not _tie_free(kind, xt, tol=1e-6):
+            continue
+        r = xt + rng.normal(size=(4, 3)) * (0.1 if done % 2 else 2.0)
+        ok, w, P, lam = _friction_lag(Lf, kind, xt, r)
+        x = xt + rng.normal(size=(4, 3)) * (2e-4 if done % 3 else 3e-3)
+        D, g, H = _friction_gh(Lf, w, P, lam, x, xt, mu, eps)
+        a, Do, go, Ho, wo, lamo = oracle.friction_contact(kind, xt, r, prm, mu, eps, x)
+        assert ok and a
+        assert np.allclose(wo, w, rtol=0, atol=1e-10) and lamo == pytest.approx(lam, rel=1e-10)
+        assert Do == pytest.approx(D, rel=1e-10)
+        assert np.linalg.norm(go - g) <= 1e-9 * np.linalg.norm(g)
+        assert np.linalg.norm(Ho - H) <= 1e-9 * np.linalg.norm(H)
+        done += 1
