@@ -507,10 +507,17 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   const int n = d->n_bodies;
   const int V = d->vert_off[n], T = d->tri_off[n], E = d->edge_off[n];
   if (V <= 0 || T < 0 || E < 0) return ABD_ERR_INVALID;
+  if (d->vert_off[0] != 0 || d->tri_off[0] != 0 || d->edge_off[0] != 0) return ABD_ERR_INVALID;
   for (int b = 0; b < n; ++b)
     if (d->vert_off[b + 1] < d->vert_off[b] || d->tri_off[b + 1] < d->tri_off[b] ||
         d->edge_off[b + 1] < d->edge_off[b])
       return ABD_ERR_INVALID;
+  // free bodies need a positive, finite mass and I0; rest positions must be finite
+  for (int b = 0; b < n; ++b)
+    if (!d->fixed[b] && !(d->mass[b] > 0.0 && d->I0[b] > 0.0 && std::isfinite(d->mass[b]) && std::isfinite(d->I0[b])))
+      return ABD_ERR_INVALID;
+  for (long k = 0; k < 3L * V; ++k)
+    if (!std::isfinite(d->x0[k])) return ABD_ERR_INVALID;
   std::vector<int> vbody(V), tbody(T), ebody(E);
   int max_v = 0, max_t = 0, max_e = 0;
   for (int b = 0; b < n; ++b) {

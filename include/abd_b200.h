@@ -86,7 +86,11 @@ typedef struct abd_sim abd_sim;
 
 /* Create a simulator for one scene on the current CUDA device; stream may be NULL (legacy
  * default stream).  Builds the per-body LBVHs (Morton codes, radix sort, Karras build).
- * Replaces AffineBodySimulator.__init__'s device setup (abd/abd.py:21-95). */
+ * Replaces AffineBodySimulator.__init__'s device setup (abd/abd.py:21-95).
+ * Returns ABD_ERR_INVALID, before any device work, for a malformed scene: no bodies or no
+ * vertices, offsets that do not start at 0 or decrease, a triangle or edge index outside its
+ * body's vertices, a non-finite rest position, a free body without a positive finite mass
+ * and I0, or precision != 0. */
 int abd_sim_create(const abd_scene_desc* scene, const abd_params* prm, void* stream, abd_sim** out);
 int abd_sim_destroy(abd_sim* sim);
 int abd_sim_set_params(abd_sim* sim, const abd_params* prm);

@@ -69,3 +69,51 @@ def test_create_rejects_mixed_precision():
     h = ctypes.c_void_p()
     rc = L.abd_sim_create(ctypes.byref(desc), ctypes.byref(cprm), None, ctypes.byref(h))
     assert rc == _lib.ABD_ERR_INVALID and not h.value
+
+
+def test_create_rejects_malformed_scenes():
+    """A malformed scene is refused with ABD_ERR_INVALID before any device work: no bodies,
+    offsets not starting at 0 or decreasing, a triangle or edge index outside its body, a
+    non-finite rest position, a free body without positive mass or I0."""
+    import numpy as np
+    from abd_warp_b200 import _lib, scenes
+    from abd_warp_b200.params import SimParams
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libabd_b200.so not built")
+    L = _lib.load()
+    bodies, prm, _ = scenes.make_config(0)
+    f = scenes.flatten_bodies(bodies)
+    ints = ("voff", "toff", "eoff", "tris", "edges", "fixed")
+    base = {k: np.ascontiguousarray(f[k], dtype=np.int32 if k in ints else np.float64)
+            for k in ("voff", "toff", "eoff", "x0", "tris", "edges", "mass", "I0", "fixed")}
+    free = int(np.flatnonzero(base["fixed"] == 0)[0])
+
+    def create(mod, n=None):
+        host = {k: v.copy() for k, v in base.items()}
+        mod(host)
+        hp = {k: v.ctypes.data_as(ctypes.c_void_p) for k, v in host.items()}
+        desc = _lib.SceneDesc(len(bodies) if n is None else n, hp["voff"], hp["toff"], hp["eoff"], hp["x0"],
+                              hp["tris"], hp["edges"], hp["mass"], hp["I0"], hp["fixed"])
+        cprm = SimParams().to_c()
+        h = ctypes.c_void_p()
+        rc = L.abd_sim_create(ctypes.byref(desc), ctypes.byref(cprm), None, ctypes.byref(h))
+        return rc, h.value
+
+    def setter(key, idx, val):
+        def f_(h):
+            h[key].reshape(-1)[idx] = val
+        return f_
+
+    cases = [
+        (lambda h: None, 0),                                   # no bodies
+        (setter("voff", 0, 1), None),                           # offsets start past 0
+        (setter("toff", 1, int(base["toff"][0]) - 1), None),    # decreasing offsets
+        (setter("tris", 0, int(base["voff"][-1])), None),       # triangle index out of range
+        (setter("edges", 1, -1), None),                         # edge index out of range
+        (setter("x0", 4, float("nan")), None),                  # non-finite rest position
+        (setter("mass", free, 0.0), None),                      # free body without mass
+        (setter("I0", free, float("inf")), None),               # non-finite I0
+    ]
+    for mod, n in cases:
+        rc, h = create(mod, n)
+        assert rc == _lib.ABD_ERR_INVALID and not h
