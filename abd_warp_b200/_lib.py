@@ -16,7 +16,10 @@ LIB_PATH = os.path.join(_HERE, "libabd_b200.so")
 ABD_OK = 0
 ABD_ERR_CUDA, ABD_ERR_INVALID, ABD_ERR_OVERFLOW, ABD_ERR_DEVICE = 1, 2, 3, 4  # include/abd_b200.h
 STATUS_NAMES = {1: "pt_overflow", 2: "ee_overflow", 4: "pair_overflow", 8: "stack_overflow",
-                16: "solver_not_converged", 32: "nan", 64: "vg_overflow"}
+                16: "solver_not_converged", 32: "nan", 64: "vg_overflow", 128: "active_pair_overflow",
+                256: "contact_overflow", 512: "ccd_overflow", 1024: "ls_candidate_overflow",
+                2048: "line_search_needs_more_trials"}
+ST_STACK_OVERFLOW, ST_SOLVER_NOCONV, ST_NAN = 8, 16, 32
 
 c_int, c_double, c_void_p, c_longlong = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
 
@@ -77,6 +80,8 @@ def load():
         "abd_compute_energy": ([P, P, P, P, P], c_int),
         "abd_ccd": ([P, P, P, P, P, P, P], c_int),
         "abd_energies_along": ([P, P, P, P, P, c_int, P], c_int),
+        "abd_get_highlight": ([P, P], c_int),
+        "abd_adjoint_step": ([P, P, P, P, P, P, P, P, P], c_int),
         "abd_take_status": ([P, P], c_int),
         "abd_status_string": ([c_int], ctypes.c_char_p),
         "abd_launch_count": ([P], c_longlong),
@@ -97,7 +102,7 @@ def exported_symbols():
     return ["abd_sim_create", "abd_sim_destroy", "abd_sim_set_params", "abd_sim_set_stream", "abd_sim_reset",
             "abd_sim_get_dq", "abd_sim_set_dq", "abd_sim_get_g", "abd_sim_sizes", "abd_step", "abd_update_mesh_vertex",
             "abd_collision_set", "abd_collision_set_dofs", "abd_export_lists", "abd_ipc_gh", "abd_export_system", "abd_solve",
-            "abd_compute_energy", "abd_ccd", "abd_energies_along", "abd_take_status", "abd_status_string", "abd_launch_count",
+            "abd_compute_energy", "abd_ccd", "abd_energies_along", "abd_get_highlight", "abd_adjoint_step", "abd_take_status", "abd_status_string", "abd_launch_count",
             "abd_profile", "abd_profile_read"]
 
 

@@ -28,7 +28,11 @@ enum : int {
   ST_CONTACT_OVERFLOW = 256,  // active-contact list capacity exceeded (host grows and reruns)
   ST_CCD_OVERFLOW = 512,   // CCD candidate list capacity exceeded (host grows and reruns)
   ST_ECAND_OVERFLOW = 1024,  // line-search candidate list capacity exceeded (grow and rerun)
+  ST_LS_MORE = 2048,       // a line search needs more trials than one batch (the host finishes)
 };
+// the status bits after which the device-driven Newton loop stops and the host reruns the step
+constexpr int kRerunMask = ST_PT_OVERFLOW | ST_EE_OVERFLOW | ST_PAIR_OVERFLOW | ST_VG_OVERFLOW | ST_ACT_OVERFLOW |
+                           ST_CONTACT_OVERFLOW | ST_CCD_OVERFLOW | ST_ECAND_OVERFLOW | ST_LS_MORE;
 
 constexpr int kTraversalStack = 64;
 constexpr int kNoChild = (int)0x80000000;  // unused slot of a node's child table
@@ -143,6 +147,13 @@ __device__ inline Box point_box(const double* y0, const double* y1, int v, float
   return B;
 }
 
+// the GPU's global nanosecond timer (kernel timing inside graphs, where events cannot go)
+__device__ inline unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // order-preserving encoding of a non-negative double for atomicMin on 64-bit integers
 __device__ inline unsigned long long dkey(double v) { return (unsigned long long)__double_as_longlong(v); }
 
@@ -175,12 +186,34 @@ struct Tree {
   int* order = nullptr;       // [N-1]
   int* lvl = nullptr;         // [sum over bodies of (heights + 1)]
   int* body_lvl = nullptr;    // [n+1]
+  int max_height = 0;         // internal levels of the deepest body subtree (host)
 };
 
 // ---------------------------------------------------------------------------------------
 // the simulator
 // ---------------------------------------------------------------------------------------
 struct Mailbox;
+
+constexpr int kMaxCluster = 12;  // bodies per preconditioner cluster: 144 x 144 doubles fit in
+                                 // shared memory
+
+// scratch of the clustering kernel, [n] each
+struct ClusterWork {
+  int *label = nullptr, *size = nullptr, *to = nullptr, *cidx = nullptr, *fill = nullptr;
+  unsigned long long* best = nullptr;
+};
+inline size_t cluster_work_bytes(int n) { return (5 * sizeof(int) + sizeof(unsigned long long)) * (size_t)n; }
+inline ClusterWork cluster_work_at(void* base, int n) {
+  ClusterWork w;
+  w.best = static_cast<unsigned long long*>(base);
+  int* q = reinterpret_cast<int*>(w.best + n);
+  w.label = q;
+  w.size = q + n;
+  w.to = q + 2 * (size_t)n;
+  w.cidx = q + 3 * (size_t)n;
+  w.fill = q + 4 * (size_t)n;
+  return w;
+}
 
 // one captured pass (see abd_graph.cuh)
 struct GraphSlot {
@@ -225,10 +258,9 @@ struct Sim {
   int *adj_col = nullptr, *adj_pair = nullptr;   // [cap_adj]
   int n_pairs = 0, n_adj = 0;      // host copies, valid after a read of dstat
   // active pairs (contacts, both bodies free) with their coupling weight, for the
-  // preconditioner's clustering on the host: int4 (pair, I, J, weight bits)
+  // preconditioner's clustering on the device: int4 (pair, I, J, weight bits)
   int cap_act = 0;
   int4* act_pairs = nullptr;       // device [cap_act]
-  int4* hact = nullptr;            // pinned [cap_act]
 
   // per-body work chunks of the energy / CCD narrow passes: (body, first item) with items
   // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
@@ -254,22 +286,31 @@ struct Sim {
   // last step's last CCD pass are kept, [kSupValid] they hold the current GH pass's candidates
   int* dint = nullptr;
   double* q_last = nullptr;        // [12 n] the DOFs (A, then p) the last step ended with
-  int* hint = nullptr;             // pinned: [2] the GH pass's active-pair count (-1 until copied)
+  int* highlight = nullptr;        // [n] contact flags of the last GH pass (k_body_gh)
   // captured passes: CCD bound (with events for profiling), GH, the Krylov solve, line-search
   // batches (step lengths from the host or from the CCD pass on the device)
   cudaStream_t cap_stream = nullptr;
   cudaStream_t cap_stream2 = nullptr;  // captures the bodies of conditional (loop) nodes
   GraphSlot g_ccd, g_ccd_ev, g_gh, g_gh0, g_kinit, g_ls, g_ls_dev;
+  GraphSlot g_step;                // a whole time step as a device loop
+  GraphSlot g_kadj;                // the adjoint's Krylov solve
+  double* adj_x = nullptr;         // [12 n] the adjoint solve's unknown lambda
+  cudaStream_t cap_stream3 = nullptr, cap_stream4 = nullptr;  // capture the loop's bodies
+  double* dq_save = nullptr;       // [12 n] dq at the start of a device-loop step (for a rerun)
+  long long step_launch[3] = {0, 0, 0};  // kernels of a step graph: outside the loops, per
+                                         // Newton iteration, per Krylov iteration
   int gh_energy = 0;               // the GH pass also sums the energy at its DOFs
+  int exact_hessian = 0;           // the GH pass assembles the exact Hessian (the adjoint's)
+  const int* energy_gate = nullptr;  // device loop: the GH pass sums the energy only while this
+                                     // device counter (the Newton iteration) is 0
   unsigned prm_version = 0;        // bumped by set_params (parameters are kernel arguments)
+  unsigned cap_gen = 0;            // bumped by every capacity growth (buffers are kernel arguments)
   // kernel profiling of the line-search candidate pass's narrow kernel: CUDA events around
   // it (recorded as graph nodes), its duration and algorithmic bytes accumulated per pass
   int prof_on = 0;                 // 0 off, 1 time every kProfEvery-th pass, 2 time and count all
   int prof_events = 0;             // this pass records the events
   long long prof_tick = 0;
   cudaEvent_t prof_ev[2] = {nullptr, nullptr};
-  // recorded by the GH pass once the active-pair list is on the host (before the body terms)
-  cudaEvent_t act_ev = nullptr;
   // fork / join of a side branch in a captured pass (the CCD pass's dot products)
   cudaEvent_t fork_ev[2] = {nullptr, nullptr};
   bool fork_open = false;
@@ -306,25 +347,24 @@ struct Sim {
   // Krylov work vectors [n][12]
   double *r = nullptr, *rh = nullptr, *pv = nullptr, *v = nullptr, *y = nullptr, *s = nullptr, *z = nullptr,
          *t = nullptr, *ddq = nullptr;
-  // preconditioner clusters (contact-coupled bodies, <= cluster_max each): the tables live in
-  // one device block (ClusterTables layout) with a pinned copy in hstage
-  int ncl = 0, max_cl = 1;
-  size_t cl_bytes = 0;                           // bytes of the tables in use
+  // preconditioner clusters (contact-coupled bodies, <= cluster_max each), formed on the
+  // device: the tables live in one device block (ClusterTables layout)
   int cl_smem = 0;                               // dynamic shared memory opted in for the inverse
+  ClusterWork cl_work;                           // the clustering kernel's scratch ([n] each)
+  void* cl_work_buf = nullptr;
   void* cl_tab = nullptr;
   int *cl_ptr = nullptr, *cl_body = nullptr;     // [ncl+1], [n]
   int *body_cl = nullptr, *ncl_dev = nullptr;    // [n], [1]
   long long* cl_off = nullptr;                   // [ncl+1] offsets into cl_inv (doubles)
   double* cl_inv = nullptr;                      // dense inverses of the cluster systems
-  size_t cap_cl_inv = 0;
+                                                 // (144 kMaxCluster n doubles: the most any
+                                                 // clustering needs)
   double* zb = nullptr;                          // [n][12] scratch (M^-1 b)
   XSum* partials = nullptr; // exact reduction partials [kRedSlots][kRedBlocks]
   int* red_count = nullptr;        // [kRedSlots] CTAs done per reduction (last CTA finishes)
   double* scal = nullptr;          // solver scalars
   int* dstat = nullptr;            // = box->dstat: [0] status, [1..] counters
   int* hstat = nullptr;            // pinned: [0, 16) mirror of dstat, [16, 32) host scratch
-  void* hstage = nullptr;          // pinned staging of the preconditioner's cluster tables
-  size_t cap_hstage = 0;
   double* hval = nullptr;          // pinned host scalars
   unsigned long long* dmin = nullptr;  // = &box->toi_key
 };
@@ -373,7 +413,8 @@ constexpr int kSupValid = 2;
 constexpr int kSlice = 64;        // vertices per slice of the line-search bounds (two per lane)
 constexpr int kParK = 4;          // dpar slot of a batch's trial count
 constexpr int kParAlpha = 5;      // dpar slots of its step lengths
-constexpr int kNPar = kParAlpha + kLsMax;
+constexpr int kParAcc = kParAlpha + kLsMax;  // dpar slot of the accepted step length
+constexpr int kNPar = kParAcc + 1;
 
 // dstat layout
 enum : int {
@@ -394,6 +435,19 @@ enum : int {
   DS_NSLOTS = 16
 };
 
+// Counters of a time step run as a device loop (the step info, kept on the device), and the
+// kernel timing of the CCD pass's narrow kernel by the GPU's global timer.
+struct StepDev {
+  int it;            // Newton iterations done (the loop's counter)
+  int lin, ls;       // Krylov iterations, line-search trials
+  int n_pt, n_ee, n_vg, n_ij, n_active;
+  double E0;         // energy of the current iterate
+  double alpha, toi; // the last accepted step length and raw time of impact
+  unsigned long long t0, t1;       // first start and last end (ns) of the current narrow launch
+  unsigned long long prof_ns, prof_n;  // their accumulated durations and launches
+  double prof_bytes;               // algorithmic bytes of those launches (profiling mode 2)
+};
+
 // The host's view of a pass: status word and counters, the exact energy, the minimum time of
 // impact and the Newton dot products, contiguous so that one copy brings them all.
 struct Mailbox {
@@ -405,6 +459,7 @@ struct Mailbox {
   // work counters of the line-search candidate pass's narrow kernel (kernel profiling only),
   // spread over 32 rows against atomic contention: [row][PF_*]
   unsigned long long prof[32][8];
+  StepDev step;
 };
 
 // counters of the line-search candidate pass's narrow kernel (kernel profiling): the data it
@@ -470,10 +525,12 @@ enum NarrowMode { NARROW_GH = 0, NARROW_ENERGY = 1, NARROW_CCD = 2, NARROW_LISTS
 cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
                    const double* y0, const double* y1, const abd_states* st = nullptr);
 cudaError_t body_gh(Sim& s, const abd_states& st, const double* A, const double* p, const double* y);
+cudaError_t prepare_narrow(Sim& s);  // kernel attributes (once, at creation)
 // Whether the next GH pass may take its candidates from the kept line-search candidates
 // (dint[kSupValid]): mode 0 no, 2 yes (a later Newton iteration of the step), 1 when they
 // were kept (dint[kSupHave]) and the step starts from the DOFs the last step ended with.
 cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode);
+// mode 3 (the device loop): 1 at the step's first Newton iteration, else 2
 cudaError_t vg_list(Sim& s, const double* y0);
 cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap);
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
@@ -493,15 +550,33 @@ cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const dou
 cudaError_t ls_setup_from_ccd(Sim& s);
 
 // solver.cu
-// The preconditioner: cluster_tables forms the clusters on the host from the first nact
-// entries of the active-pair list (hact) into the pinned tables; cluster_inverse uploads them
-// and inverts each cluster's system on the device; build_preconditioner does both with the
-// count of the last mailbox read.  ABD status.
-int cluster_tables(Sim& s, int nact);
+// The preconditioner: cluster_tables forms the clusters on the device from the last GH pass's
+// active-pair list (on stream st, the pass's stream when null); cluster_inverse inverts each
+// cluster's system; build_preconditioner does both.  The last two return an ABD status.
+cudaError_t cluster_tables(Sim& s, cudaStream_t st);
 int cluster_inverse(Sim& s);
 int build_preconditioner(Sim& s);
+int prepare_solver(Sim& s);
 // returns ABD status; iters == null: enqueue only (krylov_outcome after the next mailbox read)
-int krylov_solve(Sim& s, double* x, int* iters);
+int krylov_solve(Sim& s, double* x, int* iters, GraphSlot* slot = nullptr);
 int krylov_outcome(Sim& s);                       // iterations of the last solve
+// Enqueues a solve (setup kernels and the WHILE node of its iterations) into the graph being
+// captured on s.stream, for the device-driven Newton loop; its outcome is added to the
+// mailbox's step counters by krylov_tally.
+int krylov_issue(Sim& s, double* x);
+cudaError_t krylov_tally(Sim& s);
+
+// newton.cu: the kernels of the device-driven Newton loop (abd_step when the parameters'
+// newton_loop is 0).  Each enqueues on s.stream.
+cudaError_t step_begin(Sim& s, cudaGraphConditionalHandle h);
+cudaError_t gate_no_overflow(Sim& s, cudaGraphConditionalHandle h);
+cudaError_t after_gh(Sim& s);
+cudaError_t ls_accept(Sim& s);
+cudaError_t update_dofs_dev(Sim& s, double* A, double* p);
+cudaError_t newton_end(Sim& s, cudaGraphConditionalHandle h);
+cudaError_t finish_step_dev(Sim& s, const abd_states& st, double* xview);
+// the adjoint step (abd_adjoint_step): its right-hand side into g, its outputs from lambda
+cudaError_t adjoint_rhs(Sim& s, const double* qb, const double* qdb);
+cudaError_t adjoint_out(Sim& s, const double* lam, const double* qdb, double* qb_out, double* qdb_out);
 
 }  // namespace abd

@@ -311,8 +311,12 @@ cudaError_t build_tree(Sim& s, Tree& tr, int N, const int* prim_body, const doub
     }
     std::vector<int> order, lvl, body_lvl(n + 1, 0);
     std::vector<std::vector<int>> per(n);
+    tr.max_height = 0;
     for (int i = 0; i < M; ++i)
-      if (owner[i] >= 0) per[owner[i]].push_back(i);
+      if (owner[i] >= 0) {
+        per[owner[i]].push_back(i);
+        tr.max_height = std::max(tr.max_height, height[i]);
+      }
     for (int b = 0; b < n; ++b) {
       std::vector<int>& v = per[b];
       std::stable_sort(v.begin(), v.end(), [&](int a, int c) { return height[a] < height[c]; });

@@ -25,6 +25,7 @@
 
 #include "abd_body.cuh"
 #include "abd_geometry.cuh"
+#include "abd_ipc_full.cuh"
 
 namespace abd {
 
@@ -55,6 +56,8 @@ struct NarrowArgs {
   int cap_ccd;
   int4* ccd_cand;
   int gh_energy;                // GH: also sum the candidates' barrier energies into energy
+  const int* energy_gate;       // GH in the device loop: the energy only while this counter is 0
+  unsigned long long* gtime;    // CCD_LS: first start / last end of the launch (global timer)
   const int* sup_valid;         // GH: take the candidates from ecand instead of the traversal
   int cap_act;
   int4* act_pairs;              // GH: active pairs with their coupling weights (preconditioner)
@@ -432,14 +435,86 @@ __global__ void k_contact_scatter(int cap_contacts, const int4* __restrict__ in,
 // CTAs loop over the body pairs: every active contact of a pair (pt_ipc.py:111-190,
 // ee_ipc.py:381-430) as 5 rank-one terms, one warp per contact; its 456 values (H_IJ, the
 // contributions to H_II and H_JJ, and to g_I, g_J; put.py:25-66) are added exactly.
+// EXACT (the adjoint's system): each contact's exact, unprojected Hessian instead -- the
+// barrier of the point-plane (PT) or line-line (EE) squared distance, the reference's interior
+// contacts, with every second-derivative term (also those of the closest-point coefficients
+// that the Newton Hessian leaves out, psd/vf.py:150-176, psd/ee.py:94-116): 78 hyper-dual
+// evaluations of the contact's energy per warp, one per Hessian entry, then mapped to the two
+// bodies' affine DOFs.
 constexpr int PT_THREADS = 256;  // threads of the pair assembly (a warp per contact)
+struct ExactLog {  // the hyper-dual log's value (its derivatives are 1 / x)
+  __device__ double operator()(double v) const { return log(v); }
+};
+// One contact's exact terms (EXACT pair assembly), by its warp: the local Hessian and gradient
+// in the four points' coordinates into h [156], then the 456 affine values added to xred.
+// Vertices 0 .. nI-1 are the first group (the point; edge a), the rest the second; the group
+// of side 0 (the pair's first body) is the first unless swapped.
+__device__ void exact_contact_terms(const NarrowArgs& a, int type, int swap, const int ids[4], double* h,
+                                    XSum* xred) {
+  const int lane = threadIdx.x & 31;
+  double x[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) x[k] = a.y0[3 * ids[k / 3] + k % 3];
+  for (int e = lane; e < 78; e += 32) {  // the upper triangle, row by row
+    int i = 0, rem = e;
+    while (rem >= 12 - i) {
+      rem -= 12 - i;
+      ++i;
+    }
+    const int j = i + rem;
+    ipc::V3<ipc::HD> v[4];
+    for (int k = 0; k < 4; ++k) {
+      ipc::HD c[3];
+      for (int m = 0; m < 3; ++m) {
+        const int q = 3 * k + m;
+        c[m] = {x[q], q == i ? 1.0 : 0.0, q == j ? 1.0 : 0.0, 0.0};
+      }
+      v[k] = {c[0], c[1], c[2]};
+    }
+    // the reference's interior types, no mollifier
+    const ipc::HD en = ipc::local_energy(type, 0, v, 0.0, a.prm.d2hat, a.prm.kappa, ExactLog());
+    h[12 * i + j] = en.ab;
+    h[12 * j + i] = en.ab;
+    if (i == j) h[144 + i] = en.a;
+  }
+  __syncwarp();
+  const int nI = type == 0 ? 1 : 2;
+  auto side = [&](int v) { return (v < nI ? 0 : 1) ^ swap; };
+  auto wt = [&](int v, int m) { return m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]); };
+  for (int e = lane; e < NOUT; e += 32) {
+    double val = 0.0;
+    if (e < 432) {
+      const int blk = e / 144, r = (e % 144) / 12, c = e % 12;
+      const int rs = blk == 2 ? 1 : 0, cs = blk == 1 ? 0 : 1;  // H_IJ, diag I, diag J
+      const int m = r / 3, ra = r % 3, n = c / 3, cb = c % 3;
+      for (int u = 0; u < 4; ++u) {
+        if (side(u) != rs) continue;
+        for (int w = 0; w < 4; ++w)
+          if (side(w) == cs) val += (wt(u, m) * h[12 * (3 * u + ra) + 3 * w + cb]) * wt(w, n);
+      }
+    } else {
+      const int k = e - 432, sd = k / 12, m = (k % 12) / 3, comp = k % 3;
+      for (int u = 0; u < 4; ++u)
+        if (side(u) == sd) val += wt(u, m) * h[144 + 3 * u + comp];
+    }
+    xs_add_atomic(&xred[e], val);
+  }
+  __syncwarp();
+}
+
 constexpr int PT_WARPS = PT_THREADS / 32;
+constexpr int kExactLocal = 156;  // EXACT: a warp's local Hessian (144) and gradient (12)
+// the exact pair assembly's shared memory: the sums and every warp's local Hessian (49 KB: the
+// kernel is opted in once, at creation, since its launches may be captured)
+constexpr int kExactSmem = NOUT * (int)sizeof(XSum) + PT_WARPS * kExactLocal * (int)sizeof(double);
+template <bool EXACT>
 __global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
   const int npairs = a.dstat[DS_NPAIRS];
-  __shared__ double ush[PT_WARPS][5][24];
-  extern __shared__ XSum xred[];  // [NOUT]
+  __shared__ double ush[EXACT ? 1 : PT_WARPS][5][24];
+  extern __shared__ XSum xred[];  // [NOUT], then (EXACT) [PT_WARPS][kExactLocal] doubles
+  double* hloc = reinterpret_cast<double*>(xred + NOUT) + warp * kExactLocal;
   for (int p = blockIdx.x; p < npairs; p += gridDim.x) {  // pairs, grid-stride
     const int cnt = a.pair_cand[4 * p + 1], off = a.pair_cand[4 * p];
     if (tid == 0) {
@@ -455,6 +530,10 @@ __global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
       const int type = rec.y & 1, swap = rec.y >> 1;
       int ids[4];
       cand_vertices(a, type, rec.z, rec.w, ids);
+      if constexpr (EXACT) {
+        exact_contact_terms(a, type, swap, ids, hloc, xred);
+        continue;
+      }
       d3 xs[4];
       fetch(a.y0, ids, xs);
       Geo G;
@@ -607,6 +686,7 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
     if (*a.sup_valid) return;  // k_gh_scan takes the candidates from ecand
   }
   const int c = blockIdx.x, tid = threadIdx.x;
+  if (ls && a.gtime && tid == 0) atomicMin(&a.gtime[0], globaltimer_ns());
   const int2 ch = a.chunk[c];
   const int I = ch.x;
   const int nEI = a.eoff[I + 1] - a.eoff[I];
@@ -622,6 +702,8 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   __shared__ int2 front[2][kFront];  // breadth-first frontiers: (query | neighbour << 8, node)
   __shared__ int nfr[2];
   int fcur = 0;
+  // frontier entries in use: all of them, or fewer when a test injects a small capacity
+  const int fcap = a.prm.min_capacity > 0 ? min(kFront, a.prm.min_capacity) : kFront;
   __shared__ XSum xe;
   __shared__ unsigned long long tkey;
   __shared__ Box cbx;  // the chunk's world box: every query box of the chunk lies inside
@@ -798,7 +880,7 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
       auto push = [&](int nxt, int q, int j, int node) {
         const NodeBoxes nbx = boxes_of(q, j);
         const int slot = atomicAdd(&nfr[nxt], 1);
-        if (slot < kFront) {
+        if (slot < fcap) {
           front[nxt][slot] = make_int2(q | (j << 8), node);
           prefetch_node(*nbx.tr, node);
         } else {
@@ -827,7 +909,7 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
       // the rounds
       for (;;) {
         __syncthreads();
-        const int n = min(nfr[fcur], kFront);
+        const int n = min(nfr[fcur], fcap);
         if (n == 0) break;
         const int nxt = fcur ^ 1;
         for (int e = tid; e < n; e += CT) {
@@ -864,6 +946,9 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   }
   __syncthreads();
   if (tid == 0) {
+    if constexpr (ls) {
+      if (a.gtime) atomicMax(&a.gtime[1], globaltimer_ns());
+    }
     if constexpr (ccd) {
       if (tkey) atomicMax(a.toi_key, tkey);
     } else {
@@ -949,7 +1034,8 @@ __global__ void __launch_bounds__(128) k_gh_scan(NarrowArgs a) {
 
 // Sets dint[kSupValid] (gh_superset_check); one CTA
 __global__ void k_sup_check(int n, const double* A0, const double* p0, const double* q_last, const int* have,
-                            int* valid, int mode) {
+                            int* valid, int mode, const int* it) {
+  if (mode == 3) mode = *it == 0 ? 1 : 2;
   __shared__ int ok;
   if (threadIdx.x == 0) ok = mode == 2 ? 1 : (mode == 1 ? (*have != 0) : 0);
   __syncthreads();
@@ -973,6 +1059,7 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
   int cpt = 0, cee = 0;
   XSum en;  // the candidates' barrier energy (ipcsk/energy.py:9-48)
   xs_zero(en);
+  const bool with_energy = a.gh_energy && (!a.energy_gate || *a.energy_gate == 0);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int4 c = a.ccd_cand[k];  // pair, type | swap << 1, primitive a, primitive b
     const int type = c.y & 1;
@@ -982,7 +1069,7 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
     d3 xs[4];
     cand_vertices(a, type, c.z, c.w, ids);
     fetch(a.y0, ids, xs);
-    if (a.gh_energy) {
+    if (with_energy) {
       const double e = contact_energy(type, xs, a.prm);
       if (e != 0.0) xs_add(en, e);
     }
@@ -1000,7 +1087,7 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
     cpt += __shfl_xor_sync(0xffffffffu, cpt, o);
     cee += __shfl_xor_sync(0xffffffffu, cee, o);
   }
-  if (a.gh_energy) xs_warp_sum(en);
+  if (with_energy) xs_warp_sum(en);
   if ((threadIdx.x & 31) == 0) {
     if (cpt) atomicAdd(&a.dstat[DS_PT_COUNT], cpt);
     if (cee) atomicAdd(&a.dstat[DS_EE_COUNT], cee);
@@ -1032,6 +1119,9 @@ struct BodyArgs {
   int* vg_list;
   int cap_vg;
   XSum* energy;  // or null; the pass's exact energy (GH: inertia + vertex-ground terms, added here)
+  const int* energy_gate;  // device loop: the energy is summed only while this counter is 0
+  int exact;     // the adjoint's system: the vertex-ground Hessian with its 2 B' term
+  int* highlight;  // [n] or null: the body takes part in an active PT / EE / vertex-ground contact
 };
 
 __device__ inline void tilde(const BodyArgs& a, int b, double At[9], double pt[3]) {
@@ -1045,6 +1135,7 @@ constexpr int BT = 160;
 
 __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   const int b = blockIdx.x, t = threadIdx.x;
+  XSum* const energy = (a.energy && (!a.energy_gate || *a.energy_gate == 0)) ? a.energy : nullptr;
   const bool fixed = a.fixed[b] != 0;
   const double dt = a.prm.dt, ks = a.prm.stiffness;
   const double* A = a.A + 9 * b;
@@ -1052,10 +1143,12 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
   // vertex-ground sums, exact: g (4 y-components) and H (4x4 yy-components); vx[20]: the
   // body's energy (vertex-ground barriers of every body, inertia + orthogonality of a free one)
   __shared__ XSum vx[21];
+  __shared__ int vg_hit;  // an active vertex-ground contact (d^2 < dhat^2)
   const bool vg_any = a.prm.ground_enabled && a.prm.enable_vg, vg_on = vg_any && !fixed;
   for (int e = t; e < 21 * (kXD + 1); e += BT) reinterpret_cast<long long*>(vx)[e] = 0;
+  if (t == 0) vg_hit = 0;
   __syncthreads();
-  if (a.energy && t == 128 && !fixed)
+  if (energy && t == 128 && !fixed)
     xs_add_atomic(&vx[20], inertia_energy(a.prm, a.st, a.mass, a.I0, b, a.A + 9 * b, a.p + 3 * b));
   if (vg_any && t < 128) {
     const Box bb = load_box(&a.body_box[b]);
@@ -1064,7 +1157,8 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
       if (!vg_candidate(a, bb, a.y, nullptr, v)) continue;
       ++cnt;
       const double d = a.y[3 * v + 1] - a.prm.ground;
-      if (a.energy) {
+      if (d * d < a.prm.d2hat) vg_hit = 1;
+      if (energy) {
         const double e = barrier(d * d, a.prm);
         if (e != 0.0) xs_add_atomic(&vx[20], e);
       }
@@ -1075,19 +1169,29 @@ __global__ void __launch_bounds__(BT) k_body_gh(BodyArgs a) {
       for (int ii = 0; ii < 4; ++ii) {
         xs_add_atomic(&vx[ii], ((d * 2.0) * th[ii]) * db);
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) xs_add_atomic(&vx[4 + 4 * ii + jj], (((th[ii] * th[jj]) * d2b) * 4.0) * d * d);
+        for (int jj = 0; jj < 4; ++jj) {
+          xs_add_atomic(&vx[4 + 4 * ii + jj], (((th[ii] * th[jj]) * d2b) * 4.0) * d * d);
+          if (a.exact) xs_add_atomic(&vx[4 + 4 * ii + jj], (th[ii] * th[jj]) * (2.0 * db));
+        }
       }
     }
     if (cnt) atomicAdd(&a.dstat[DS_VG_COUNT], cnt);
   }
   __syncthreads();
-  if (a.energy && t <= kXD) {
+  if (energy && t <= kXD) {
     const long long v = reinterpret_cast<const long long*>(&vx[20])[t];
-    long long* d = reinterpret_cast<long long*>(a.energy);
+    long long* d = reinterpret_cast<long long*>(energy);
     if (v) {
       if (t < kXD) atomicAdd((unsigned long long*)&d[t], (unsigned long long)v);
       else atomicOr((unsigned long long*)&d[t], (unsigned long long)v);
     }
+  }
+  // contact flags (abd.py:238): any active contact of the body's pairs, or vertex-ground
+  if (a.highlight && t == 156) {
+    int on = vg_hit;
+    const int k1 = (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW) ? a.row_ptr[b] : a.row_ptr[b + 1];
+    for (int k = a.row_ptr[b]; k < k1 && !on; ++k) on = a.pair_active[a.adj_pair[k]] > 0;
+    a.highlight[b] = on;
   }
   if (t >= 156) return;
   if (!fixed) {
@@ -1188,9 +1292,10 @@ __global__ void k_export_off(int np, const int* pair_active, const int* fixed, c
 }
 
 __global__ void k_update_dofs(int n, const double* A, const double* p, const double* dq, double alpha, double* Ao,
-                              double* po) {
+                              double* po, const double* alpha_dev) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
+  if (alpha_dev) alpha = *alpha_dev;
 #pragma unroll
   for (int k = 0; k < 3; ++k) po[3 * b + k] = p[3 * b + k] - dq[12 * b + k] * alpha;
 #pragma unroll
@@ -1285,6 +1390,8 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.ccd_cand = s.ccd_cand;
   a.body_sup = s.body_sup;
   a.gh_energy = s.gh_energy;
+  a.energy_gate = s.energy_gate;
+  a.gtime = s.prof_events < 0 ? &s.box->step.t0 : nullptr;
   a.sup_valid = s.dint + kSupValid;
   a.cap_act = s.cap_act;
   a.act_pairs = s.act_pairs;
@@ -1351,6 +1458,9 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
   a.vg_list = s.vg_list;
   a.cap_vg = s.cap_vg;
   a.energy = s.gh_energy ? s.energy_acc : nullptr;
+  a.energy_gate = s.energy_gate;
+  a.exact = s.exact_hessian;
+  a.highlight = s.highlight;
   return a;
 }
 
@@ -1373,10 +1483,10 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if (e != cudaSuccess) return e;
       if (mode == NARROW_CCD_LS) {
         if (!a.y1) return cudaErrorInvalidValue;
-        if (s.prof_events && record_event(s.prof_ev[0], s.stream))
+        if (s.prof_events > 0 && record_event(s.prof_ev[0], s.stream))
           return cudaErrorUnknown;
         k_chunk_narrow<NARROW_CCD_LS><<<s.nch, CT, 0, s.stream>>>(a);
-        if (s.prof_events && record_event(s.prof_ev[1], s.stream))
+        if (s.prof_events > 0 && record_event(s.prof_ev[1], s.stream))
           return cudaErrorUnknown;
         k_ccd_eval<true><<<kRedBlocks, 128, 0, s.stream>>>(a);
       } else {
@@ -1399,7 +1509,11 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if ((e = cudaMemsetAsync(s.dstat + DS_NACTP, 0, sizeof(int), s.stream)) != cudaSuccess) return e;
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
       static_assert(smem + sizeof(double) * PT_WARPS * 5 * 24 + 256 <= 48 * 1024, "pair assembly shared memory");
-      k_pair_assemble<<<s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148, PT_THREADS, smem, s.stream>>>(a);
+      const int grid = s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148;
+      if (s.exact_hessian)
+        k_pair_assemble<true><<<grid, PT_THREADS, kExactSmem, s.stream>>>(a);
+      else
+        k_pair_assemble<false><<<grid, PT_THREADS, smem, s.stream>>>(a);
       s.launches += 3;
     }
   } else {
@@ -1410,9 +1524,14 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
   return cudaGetLastError();
 }
 
+cudaError_t prepare_narrow(Sim& s) {
+  (void)s;
+  return cudaFuncSetAttribute(k_pair_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExactSmem);
+}
+
 cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode) {
   k_sup_check<<<1, 1024, 0, s.stream>>>(s.n, st ? st->A0 : nullptr, st ? st->p0 : nullptr, s.q_last,
-                                         s.dint + kSupHave, s.dint + kSupValid, st ? mode : 0);
+                                         s.dint + kSupHave, s.dint + kSupValid, st ? mode : 0, &s.box->step.it);
   ++s.launches;
   return cudaGetLastError();
 }
@@ -1447,9 +1566,43 @@ cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap) {
 
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
                         double* pout) {
-  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, dq, alpha, Aout, pout);
+  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, dq, alpha, Aout, pout, nullptr);
   ++s.launches;
   return cudaGetLastError();
+}
+
+cudaError_t update_dofs_dev(Sim& s, double* A, double* p) {
+  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, s.dq, 0.0, A, p, s.dpar + kParAcc);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+// k_finish, unless the device loop stopped for a rerun (the states are then left as they
+// were); the DOFs it ended with are kept for the next step's first GH pass
+__global__ void k_finish_dev(int n, double dt, abd_states st, const int* dstat, double* q_last, int* sup_have) {
+  if (dstat[DS_STATUS] & kRerunMask) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) {
+    for (int k = 0; k < 3; ++k) {
+      st.pdot[3 * b + k] = (st.p[3 * b + k] - st.p0[3 * b + k]) / dt;
+      st.p0[3 * b + k] = st.p[3 * b + k];
+      q_last[9 * (size_t)n + 3 * b + k] = st.p[3 * b + k];
+    }
+    for (int k = 0; k < 9; ++k) {
+      st.Adot[9 * b + k] = (st.A[9 * b + k] - st.A0[9 * b + k]) / dt;
+      st.A0[9 * b + k] = st.A[9 * b + k];
+      q_last[9 * b + k] = st.A[9 * b + k];
+    }
+  }
+  if (b == 0) *sup_have = 1;
+}
+
+cudaError_t finish_step_dev(Sim& s, const abd_states& st, double* xview) {
+  k_finish_dev<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, s.prm.dt, st, s.dstat, s.q_last, s.dint + kSupHave);
+  ++s.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !xview) return e;
+  return transform(s, st.A0, st.p0, xview);
 }
 
 cudaError_t finish_step(Sim& s, const abd_states& st, double* xview) {

@@ -16,7 +16,13 @@
 //
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current) and remembers it for later calls; make
-// that first call before any stream capture begins.
+// that first call before any stream capture begins.  The remembered address belongs to the
+// device's primary context: after cudaDeviceReset on that device it is stale, so a process
+// that resets a device must not call this entry point on it afterwards.
+//
+// The sum: each CTA adds its 256 bodies' energies by a fixed-order tree and the last kernel
+// adds the CTA partials the same way, so the result is deterministic but can differ in the
+// last bits from abd_compute_energy, whose sum is exact (rounded once).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -141,9 +147,15 @@ extern "C" int abd_inertia_energy_noalloc(const abd_params* prm, int n_bodies, c
   a.mass = mass_dev;
   a.I0 = I0_dev;
   a.fixed = fixed_dev;
-  const int nb = (n_bodies + kThreads - 1) / kThreads;
+  int nb = (n_bodies + kThreads - 1) / kThreads;
   cudaStream_t s = (cudaStream_t)stream;
-  k_energy_partials<<<nb, kThreads, 0, s>>>(a, partials);
-  k_energy_finish<<<1, 1024, 0, s>>>(partials, nb, E_dev);
-  return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+  // launched through cudaLaunchKernel so that each launch's own error is the one returned (an
+  // error left by an unrelated earlier call is not this call's)
+  void* pargs[] = {&a, &partials};
+  if (cudaLaunchKernel((const void*)k_energy_partials, dim3(nb), dim3(kThreads), pargs, 0, s) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  void* fargs[] = {&partials, &nb, &E_dev};
+  if (cudaLaunchKernel((const void*)k_energy_finish, dim3(1), dim3(1024), fargs, 0, s) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  return ABD_OK;
 }

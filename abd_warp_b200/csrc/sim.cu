@@ -95,6 +95,7 @@ void free_tree(abd::Tree& t) {
 }
 
 int grow_pairs(Sim& s, int need) {
+  ++s.cap_gen;  // every captured pass is keyed on it
   const int cap = std::max(need + need / 2, 2 * s.cap_pairs);
   const int cap_adj = 2 * cap;
   for (void* q : {(void*)s.ij, (void*)s.adj_col, (void*)s.adj_pair, (void*)s.pair_cand, (void*)s.offdiag,
@@ -116,6 +117,7 @@ int grow_pairs(Sim& s, int need) {
 }
 
 int grow_contacts(Sim& s, int need) {
+  ++s.cap_gen;  // every captured pass is keyed on it
   if (need <= s.cap_contacts) return ABD_OK;
   if (s.contacts) cudaFree(s.contacts);
   if (s.contacts_by_pair) cudaFree(s.contacts_by_pair);
@@ -126,6 +128,7 @@ int grow_contacts(Sim& s, int need) {
 }
 
 int grow_ccd(Sim& s, int need) {
+  ++s.cap_gen;  // every captured pass is keyed on it
   if (need <= s.cap_ccd) return ABD_OK;
   if (s.ccd_cand) cudaFree(s.ccd_cand);
   s.ccd_cand = nullptr;
@@ -135,6 +138,7 @@ int grow_ccd(Sim& s, int need) {
 }
 
 int grow_ecand(Sim& s, int need) {
+  ++s.cap_gen;  // every captured pass is keyed on it
   if (need <= s.cap_ecand) return ABD_OK;
   if (s.ecand) cudaFree(s.ecand);
   s.ecand = nullptr;
@@ -144,19 +148,17 @@ int grow_ecand(Sim& s, int need) {
 }
 
 int grow_act(Sim& s, int need) {
+  ++s.cap_gen;  // every captured pass is keyed on it
   if (need <= s.cap_act) return ABD_OK;
   if (s.act_pairs) cudaFree(s.act_pairs);
-  if (s.hact) cudaFreeHost(s.hact);
   s.act_pairs = nullptr;
-  s.hact = nullptr;
   s.cap_act = std::max(need + need / 2, 2 * s.cap_act);
-  if (dalloc(&s.act_pairs, s.cap_act) ||
-      cudaHostAlloc((void**)&s.hact, sizeof(int4) * s.cap_act, cudaHostAllocDefault) != cudaSuccess)
-    return ABD_ERR_OVERFLOW;
+  if (dalloc(&s.act_pairs, s.cap_act)) return ABD_ERR_OVERFLOW;
   return ABD_OK;
 }
 
 int grow_lists(Sim& s, int need_pt, int need_ee) {
+  ++s.cap_gen;  // every captured pass is keyed on it
   if (need_pt > s.cap_pt) {
     cudaFree(s.pt_list);
     s.cap_pt = std::max(need_pt + need_pt / 2, 2 * s.cap_pt);
@@ -206,12 +208,10 @@ abd::Dofs updated(Sim& s, const double* A, const double* p, int slot, double* Ao
   return d;
 }
 
-// One synchronisation: the mailbox (status, counters, energy, time of impact, dots) and,
-// when act is set, the active-pair list.  Updates the host mirror and pair counts.
-int sync_read(Sim& s, bool act = false) {
+// One synchronisation: the mailbox (status, counters, energy, time of impact, dots).
+// Updates the host mirror and pair counts.
+int sync_read(Sim& s) {
   CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
-  if (act && s.cap_act > 0)
-    CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
   CK(cudaStreamSynchronize(s.stream));
   std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
   s.n_pairs = s.hstat[abd::DS_NPAIRS];
@@ -236,6 +236,7 @@ int overflow(Sim& s) {
   if (!r && (bits & abd::ST_VG_OVERFLOW) && s.hstat[abd::DS_VG_COUNT] > s.cap_vg) {
     cudaFree(s.vg_list);
     s.vg_list = nullptr;
+    ++s.cap_gen;
     s.cap_vg = 2 * s.hstat[abd::DS_VG_COUNT];
     if (dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) r = ABD_ERR_OVERFLOW;
   }
@@ -257,7 +258,7 @@ constexpr int kMaxReruns = 6;
 uint64_t states_key(const Sim& s, const abd_states& st) {
   abd::KeyHash k;
   k.add(st.A).add(st.p).add(st.Ak).add(st.pk).add(st.A0).add(st.p0).add(st.Adot).add(st.pdot);
-  k.add(s.prm_version).add(s.dq).add(s.x).add(s.xk).add(s.box);
+  k.add(s.prm_version).add(s.dq).add(s.x).add(s.xk).add(s.box).add(s.cap_gen);
   return k.h;
 }
 
@@ -298,19 +299,27 @@ int no_post() { return ABD_OK; }
 // mailbox copy; post() enqueues work that follows it before the host's wait (the
 // step's first line-search batch).  mode NARROW_CCD_LS also collects the line-search
 // candidates between d0 and d1.
+// The kernels of a CCD pass (no copy to the host); pre() as in ccd_of
+template <class Pre>
+int ccd_issue(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, int mode, Pre&& pre) {
+  Sim& s = h->s;
+  s.fork_open = false;
+  int r = pre();
+  if (r) return r;
+  if ((r = culling(h, &d0, &d1, s.x, s.xk, mode))) return r;
+  if (s.fork_open) {  // join the branch pre() forked
+    CK(cudaStreamWaitEvent(s.stream, s.fork_ev[1], 0));
+    s.fork_open = false;
+  }
+  return ABD_OK;
+}
+
 template <class Pre, class Post = int (*)()>
 int ccd_of(abd_sim* h, const abd::Dofs& d0, const abd::Dofs& d1, double* alpha, double* raw, Pre&& pre,
            abd::GraphSlot* g = nullptr, uint64_t key = 0, int mode = abd::NARROW_CCD, Post&& post = no_post) {
   Sim& s = h->s;
   auto issue = [&]() -> int {
-    s.fork_open = false;
-    int r = pre();
-    if (r) return r;
-    if ((r = culling(h, &d0, &d1, s.x, s.xk, mode))) return r;
-    if (s.fork_open) {  // join the branch pre() forked
-      CK(cudaStreamWaitEvent(s.stream, s.fork_ev[1], 0));
-      s.fork_open = false;
-    }
+    if (int r = ccd_issue(h, d0, d1, mode, pre)) return r;
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
@@ -410,29 +419,35 @@ int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p,
   return ABD_OK;
 }
 
-// Gradient and Hessian blocks at (A, p), and the active-pair list for the preconditioner.
-// The list and its count (hint[2]) reach the host before the body terms are computed: the
-// pass records act_ev there, and mid() runs on the host after it while the device finishes
-// the pass (the step forms the preconditioner's clusters in it).
+// Gradient and Hessian blocks at (A, p), and the preconditioner's clusters: the pass forks
+// after the pair assembly and forms the clusters from its active-pair list on a side branch
+// while the body terms run (both on the device).
 // g: replay slot for the step (its key covers every capacity the captured grids depend on).
 // sup_mode (gh_superset_check): 0 the traversal finds the candidates; 1 the step's first GH
 // pass, which takes them from the kept line-search candidates when the step starts where the
 // last one ended; 2 a later Newton iteration's GH pass, which always does.
-template <class Mid = int (*)()>
-int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active,
-          abd::GraphSlot* g = nullptr, bool with_energy = false, int sup_mode = 0, Mid&& mid = no_post) {
+// The kernels of a GH pass (no copy to the host)
+int gh_issue(abd_sim* h, const abd_states& st, const double* A, const double* p, int sup_mode) {
   Sim& s = h->s;
   const abd::Dofs d = direct(A, p);
+  CK(abd::gh_superset_check(s, &st, sup_mode));
+  int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
+  if (r) return r;
+  CK(cudaEventRecord(s.fork_ev[0], s.stream));
+  CK(cudaStreamWaitEvent(s.cap_stream2, s.fork_ev[0], 0));
+  CK(abd::cluster_tables(s, s.cap_stream2));
+  CK(cudaEventRecord(s.fork_ev[1], s.cap_stream2));
+  CK(abd::body_gh(s, st, A, p, s.x));
+  CK(cudaStreamWaitEvent(s.stream, s.fork_ev[1], 0));
+  return ABD_OK;
+}
+
+int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, int* n_active,
+          abd::GraphSlot* g = nullptr, bool with_energy = false, int sup_mode = 0) {
+  Sim& s = h->s;
   s.gh_energy = with_energy ? 1 : 0;  // read by the kernel arguments of this pass
   auto issue = [&]() -> int {
-    CK(abd::gh_superset_check(s, &st, sup_mode));
-    int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
-    if (r) return r;
-    if (s.cap_act > 0)
-      CK(cudaMemcpyAsync(s.hact, s.act_pairs, sizeof(int4) * s.cap_act, cudaMemcpyDeviceToHost, s.stream));
-    CK(cudaMemcpyAsync(s.hint + 2, s.dstat + abd::DS_NACTP, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-    CK(abd::record_event(s.act_ev, s.stream));
-    CK(abd::body_gh(s, st, A, p, s.x));
+    if (int r = gh_issue(h, st, A, p, sup_mode)) return r;
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
@@ -442,20 +457,14 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
       abd::KeyHash k;
       k.add(states_key(s, st)).add(A).add(p).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
       k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
-      k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.hact);
+      k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active);
       k.add(s.cap_ccd).add(s.ccd_cand).add(s.gh_energy).add(sup_mode).add(s.q_last).add(s.dint);
-      s.hint[2] = -1;  // replaced by the pass's copy of the count
+      k.add(s.cap_ecand).add(s.ecand);  // k_gh_scan reads the kept line-search candidates
       r = abd::run_graph(s, *g, k.h, issue);
     } else {
-      s.hint[2] = -1;
       r = issue();
     }
     if (r) return r;
-    CK(cudaEventSynchronize(s.act_ev));
-    // the count's copy precedes the event and follows the list's: once it has landed, the list
-    // on the host is this pass's (otherwise wait for the whole pass)
-    if (*static_cast<volatile int*>(s.hint + 2) < 0) CK(cudaStreamSynchronize(s.stream));
-    if ((r = mid())) return r;
     CK(cudaStreamSynchronize(s.stream));
     std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
     s.n_pairs = s.hstat[abd::DS_NPAIRS];
@@ -502,14 +511,16 @@ const char* abd_status_string(int code) {
 
 int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream, abd_sim** out) {
   if (!d || !prm || !out || d->n_bodies <= 0 || !d->vert_off || !d->tri_off || !d->edge_off || !d->x0 ||
-      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed || prm->precision != 0)
+      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed || prm->precision != 0 || prm->min_capacity < 0)
     return ABD_ERR_INVALID;
   const int n = d->n_bodies;
   const int V = d->vert_off[n], T = d->tri_off[n], E = d->edge_off[n];
   if (V <= 0 || T < 0 || E < 0) return ABD_ERR_INVALID;
   if (d->vert_off[0] != 0 || d->tri_off[0] != 0 || d->edge_off[0] != 0) return ABD_ERR_INVALID;
+  // every body needs a vertex: a body without one would get a point box at the origin that
+  // the broad phase pairs against its neighbours
   for (int b = 0; b < n; ++b)
-    if (d->vert_off[b + 1] < d->vert_off[b] || d->tri_off[b + 1] < d->tri_off[b] ||
+    if (d->vert_off[b + 1] <= d->vert_off[b] || d->tri_off[b + 1] < d->tri_off[b] ||
         d->edge_off[b + 1] < d->edge_off[b])
       return ABD_ERR_INVALID;
   // free bodies need a positive, finite mass and I0; rest positions must be finite
@@ -585,6 +596,18 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(upload(&ecd, ec.data(), ec.size(), s.stream));
   if (e == cudaSuccess) ok(abd::build_tree(s, s.tri_tree, T, s.tbody, tcd, d->tri_off));
   if (e == cudaSuccess) ok(abd::build_tree(s, s.edge_tree, E, s.ebody, ecd, d->edge_off));
+  // a depth-first walk pops one node and pushes at most four (the node's descendants one or
+  // two levels down), so a subtree of H internal levels needs at most 3 ceil(H / 2) + 1
+  // stack entries; a deeper tree (many primitives sharing a Morton code) is refused
+  if (e == cudaSuccess) {
+    const int H = std::max(s.tri_tree.max_height, s.edge_tree.max_height);
+    if (3 * ((H + 1) / 2) + 1 > abd::kTraversalStack) {
+      if (tcd) cudaFree(tcd);
+      if (ecd) cudaFree(ecd);
+      abd_sim_destroy(h);
+      return ABD_ERR_INVALID;
+    }
+  }
   s.W = (n + 31) / 32;
   ok(dalloc(&s.x, 3 * (size_t)V));
   ok(dalloc(&s.xk, 3 * (size_t)V));
@@ -690,8 +713,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.upper_ptr, n + 1));
   for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq, &s.zb})
     ok(dalloc(v, 12 * (size_t)n));
-  s.cap_hstage = abd::cluster_tables_bytes(n);
-  if (ok(cudaMalloc(&s.cl_tab, s.cap_hstage))) {
+  if (ok(cudaMalloc(&s.cl_tab, abd::cluster_tables_bytes(n)))) {
     const abd::ClusterTables t = abd::cluster_tables_at(s.cl_tab, n);
     s.cl_ptr = t.cl_ptr;
     s.cl_body = t.cl_body;
@@ -700,6 +722,10 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     s.cl_off = t.cl_off;
   }
   ok(dalloc(&s.diag, 144 * (size_t)n));
+  // the clustering kernel's scratch, and room for the inverses of any clustering: a cluster of
+  // s bodies takes (12 s)^2 doubles, and the sum of s^2 over clusters is at most kMaxCluster n
+  if (ok(cudaMalloc(&s.cl_work_buf, abd::cluster_work_bytes(n)))) s.cl_work = abd::cluster_work_at(s.cl_work_buf, n);
+  ok(dalloc(&s.cl_inv, 144 * (size_t)abd::kMaxCluster * n));
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
   ok(dalloc(&s.red_count, abd::kRedSlots));
   ok(dalloc(&s.scal, 32));
@@ -714,9 +740,15 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.body_sup, n));
   ok(dalloc(&s.dint, 4));
   ok(dalloc(&s.q_last, 12 * (size_t)n));
+  ok(dalloc(&s.dq_save, 12 * (size_t)n));
+  ok(dalloc(&s.adj_x, 12 * (size_t)n));
+  ok(dalloc(&s.highlight, n));
+  if (e == cudaSuccess) e = cudaMemsetAsync(s.highlight, 0, sizeof(int) * n, s.stream);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream2, cudaStreamNonBlocking);
-  for (cudaEvent_t* ev : {&s.act_ev, &s.fork_ev[0], &s.fork_ev[1]})
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream3, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream4, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&s.fork_ev[0], &s.fork_ev[1]})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   ok(dalloc(&s.row_cnt, n));
   ok(dalloc(&s.nbr, (size_t)n * abd::kNbList));
@@ -725,11 +757,10 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hstat, 32 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hbox, sizeof(abd::Mailbox), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hpar, abd::kNPar * sizeof(double), cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hint, 4 * sizeof(int), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.hval, 32 * sizeof(double), cudaHostAllocDefault);
-  // the preconditioner's cluster tables (the device block's layout)
-  if (e == cudaSuccess) e = cudaHostAlloc(&s.hstage, s.cap_hstage, cudaHostAllocDefault);
   if (e == cudaSuccess) e = abd::rest_boxes(s);
+  if (e == cudaSuccess && abd::prepare_solver(s) != ABD_OK) e = cudaErrorUnknown;
+  if (e == cudaSuccess) e = abd::prepare_narrow(s);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dq, 0, sizeof(double) * 12 * n, s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.box, 0, sizeof(abd::Mailbox), s.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s.dint, 0, 4 * sizeof(int), s.stream);
@@ -747,16 +778,19 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     abd_sim_destroy(h);
     return ABD_ERR_CUDA;
   }
+  // initial capacities; min_capacity > 0 replaces them all (host-injected shortfalls)
+  const int mc = prm->min_capacity;
+  auto cap0 = [mc](int dflt) { return mc > 0 ? mc : dflt; };
   s.cap_pairs = 0;
-  int r = grow_pairs(s, std::max(256, 8 * n));
-  if (!r) r = grow_act(s, std::max(1024, n));
-  if (!r) r = grow_contacts(s, std::max(4096, 8 * n));
-  if (!r) r = grow_ccd(s, std::max(1 << 15, 32 * n));
-  if (!r) r = grow_ecand(s, std::max(1 << 15, 32 * n));
+  int r = grow_pairs(s, cap0(std::max(256, 8 * n)));
+  if (!r) r = grow_act(s, cap0(std::max(1024, n)));
+  if (!r) r = grow_contacts(s, cap0(std::max(4096, 8 * n)));
+  if (!r) r = grow_ccd(s, cap0(std::max(1 << 15, 32 * n)));
+  if (!r) r = grow_ecand(s, cap0(std::max(1 << 15, 32 * n)));
   s.cap_pt = 0;
   s.cap_ee = 0;
-  if (!r) r = grow_lists(s, std::max(1 << 14, V / 4), std::max(1 << 14, E / 4));
-  s.cap_vg = std::max(1024, V);
+  if (!r) r = grow_lists(s, cap0(std::max(1 << 14, V / 4)), cap0(std::max(1 << 14, E / 4)));
+  s.cap_vg = cap0(std::max(1024, V));
   if (!r && dalloc(&s.vg_list, 2 * (size_t)s.cap_vg)) r = ABD_ERR_OVERFLOW;
   if (r) {
     abd_sim_destroy(h);
@@ -780,17 +814,16 @@ int abd_sim_destroy(abd_sim* h) {
                   s.row_cnt, s.upper_cnt, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_tab, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
-                  s.body_sup, s.slice, s.q_last};
+                  s.body_sup, s.slice, s.q_last, s.highlight, s.cl_work_buf, s.dq_save, s.adj_x};
   for (void* q : bufs)
     if (q) cudaFree(q);
-  for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev})
+  for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev, &s.g_step, &s.g_kadj})
     if (g->exec) cudaGraphExecDestroy(g->exec);
-  if (s.cap_stream) cudaStreamDestroy(s.cap_stream);
-  if (s.cap_stream2) cudaStreamDestroy(s.cap_stream2);
-  for (cudaEvent_t ev : {s.prof_ev[0], s.prof_ev[1], s.act_ev, s.fork_ev[0], s.fork_ev[1]})
+  for (cudaStream_t q : {s.cap_stream, s.cap_stream2, s.cap_stream3, s.cap_stream4})
+    if (q) cudaStreamDestroy(q);
+  for (cudaEvent_t ev : {s.prof_ev[0], s.prof_ev[1], s.fork_ev[0], s.fork_ev[1]})
     if (ev) cudaEventDestroy(ev);
-  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hstage, (void*)s.hact, (void*)s.hbox, (void*)s.hpar,
-                  (void*)s.hint})
+  for (void* q : {(void*)s.hstat, (void*)s.hval, (void*)s.hbox, (void*)s.hpar})
     if (q) cudaFreeHost(q);
   delete h;
   return ABD_OK;
@@ -865,6 +898,14 @@ int abd_profile_read(const abd_sim* h, double* ms, long long* launches, double* 
   if (ms) *ms = h->s.prof_ms;
   if (launches) *launches = h->s.prof_launches;
   if (bytes) *bytes = h->s.prof_bytes;
+  return ABD_OK;
+}
+
+int abd_get_highlight(abd_sim* h, int* out) {
+  if (!h || !out) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  CK(cudaMemcpyAsync(out, s.highlight, sizeof(int) * s.n, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
   return ABD_OK;
 }
 
@@ -990,8 +1031,13 @@ int abd_energies_along(abd_sim* h, const abd_states* st, const double* A, const 
   return r;
 }
 
-int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
-  if (!h || !stp) return ABD_ERR_INVALID;
+}  // extern "C"
+
+namespace {
+
+// The step with the Newton iterations driven from the host (newton_loop = 1, and the fallback
+// of the device loop when a line search needs a second batch of trials).
+int step_host(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
   Sim& s = h->s;
   const abd_states& st = *stp;
   const abd_params& P = s.prm;
@@ -1010,9 +1056,8 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
     // the step's first GH pass also gives the energy at q0 (its own replay slot); the GH
     // passes take their candidates from the last CCD pass's line-search candidates (which the
     // step's CCD passes then replace: the first pass's kept list is consumed)
-    // the preconditioner's clusters are formed on the host while the pass's body terms run
-    auto clusters = [&]() -> int { return abd::cluster_tables(s, s.hint[2]); };
-    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2, clusters)))
+    // (the pass also forms the preconditioner's clusters)
+    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2)))
       return r;
     if (it == 0) CK(cudaMemsetAsync(s.dint + abd::kSupHave, 0, sizeof(int), s.stream));
     if (it == 0) {
@@ -1091,6 +1136,233 @@ int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* i
   inf.status = take_status(h);
   if (info) *info = inf;
   return (inf.status & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
+}
+
+// A conditional handle of the graph being captured on st (its value is set by kernels)
+int make_handle(cudaStream_t st, cudaGraphConditionalHandle* hc) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr));
+  if (cs != cudaStreamCaptureStatusActive) return ABD_ERR_CUDA;
+  CK(cudaGraphConditionalHandleCreate(hc, graph, 0, 0));
+  return ABD_OK;
+}
+
+// Adds a conditional node (hc, type) after the work captured on st so far; what st captures
+// next follows the node.  *body: the node's body graph.
+int add_conditional(cudaStream_t st, cudaGraphConditionalHandle hc, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+  if (cs != cudaStreamCaptureStatusActive) return ABD_ERR_CUDA;
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = hc;
+  np.conditional.type = type;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
+  *body = np.conditional.phGraph_out[0];
+  CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  return ABD_OK;
+}
+
+// Captures issue() into the body graph of a conditional node, on stream bs (the simulator's
+// stream points there meanwhile)
+template <class F>
+int capture_body(Sim& s, cudaGraph_t body, cudaStream_t bs, F&& issue) {
+  CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const cudaStream_t saved = s.stream;
+  s.stream = bs;
+  const int r = issue();
+  s.stream = saved;
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(bs, &out);
+  if (r) return r;
+  return e == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+}
+
+// The step with the Newton iterations as a device loop: one graph launch and one copy to the
+// host per step (newton.cu describes the loop)
+int step_device(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
+  Sim& s = h->s;
+  const abd_states& st = *stp;
+  const size_t nA = sizeof(double) * 9 * s.n, np = sizeof(double) * 3 * s.n, nq = sizeof(double) * 12 * s.n;
+  auto dots = [&]() -> int {  // dq.g, g.g on a branch beside the CCD pass's culling
+    CK(cudaEventRecord(s.fork_ev[0], s.stream));
+    CK(cudaStreamWaitEvent(s.cap_stream2, s.fork_ev[0], 0));
+    CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots, s.cap_stream2));
+    CK(cudaEventRecord(s.fork_ev[1], s.cap_stream2));
+    s.fork_open = true;
+    return ABD_OK;
+  };
+  auto iteration_tail = [&]() -> int {  // after a GH pass without overflow
+    CK(abd::after_gh(s));
+    if (int r = abd::cluster_inverse(s)) return r;
+    if (int r = abd::krylov_issue(s, s.dq)) return r;
+    CK(abd::krylov_tally(s));
+    // the CCD bound between q and q - dq with the line-search candidates (abd.py:278-303),
+    // Ak, pk = q - dq; the trials of the line search; the accepted step
+    const abd::Dofs d0 = direct(st.A, st.p), d1 = updated(s, st.A, st.p, 1, st.Ak, st.pk);
+    if (int r = ccd_issue(h, d0, d1, abd::NARROW_CCD_LS, dots)) return r;
+    CK(abd::ls_setup_from_ccd(s));
+    CK(abd::ls_energies(s, st, st.A, st.p));
+    CK(abd::ls_accept(s));
+    CK(abd::update_dofs_dev(s, st.A, st.p));
+    CK(cudaMemcpyAsync(st.Ak, st.A, nA, cudaMemcpyDeviceToDevice, s.stream));
+    CK(cudaMemcpyAsync(st.pk, st.p, np, cudaMemcpyDeviceToDevice, s.stream));
+    return ABD_OK;
+  };
+  auto issue = [&]() -> int {
+    const cudaStream_t top = s.stream;
+    // q <- q0 (abd.py:124-128); the warm start kept for a rerun
+    CK(cudaMemcpyAsync(st.A, st.A0, nA, cudaMemcpyDeviceToDevice, top));
+    CK(cudaMemcpyAsync(st.p, st.p0, np, cudaMemcpyDeviceToDevice, top));
+    CK(cudaMemcpyAsync(st.Ak, st.A0, nA, cudaMemcpyDeviceToDevice, top));
+    CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, top));
+    CK(cudaMemcpyAsync(s.dq_save, s.dq, nq, cudaMemcpyDeviceToDevice, top));
+    cudaGraphConditionalHandle hn;
+    if (int r = make_handle(top, &hn)) return r;
+    CK(abd::step_begin(s, hn));
+    cudaGraph_t nbody = nullptr;
+    if (int r = add_conditional(top, hn, cudaGraphCondTypeWhile, &nbody)) return r;
+    const long long l0 = s.launches;
+    int r = capture_body(s, nbody, s.cap_stream3, [&]() -> int {
+      if (int q = gh_issue(h, st, st.A, st.p, 3)) return q;
+      cudaGraphConditionalHandle hi;
+      if (int q = make_handle(s.stream, &hi)) return q;
+      CK(abd::gate_no_overflow(s, hi));
+      cudaGraph_t ibody = nullptr;
+      if (int q = add_conditional(s.stream, hi, cudaGraphCondTypeIf, &ibody)) return q;
+      if (int q = capture_body(s, ibody, s.cap_stream4, iteration_tail)) return q;
+      CK(abd::newton_end(s, hn));
+      return ABD_OK;
+    });
+    if (r) return r;
+    s.step_launch[1] = s.launches - l0;
+    CK(abd::finish_step_dev(s, st, x_view));
+    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, top));
+    return ABD_OK;
+  };
+  abd::KeyHash k;
+  k.add(states_key(s, st)).add(x_view).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
+  k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
+  k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.q_last).add(s.dint);
+  k.add(s.cap_ccd).add(s.ccd_cand).add(s.cap_ecand).add(s.ecand).add(s.prof_on).add(s.cl_inv).add(s.dq_save);
+  s.prof_events = s.prof_on ? -1 : 0;  // kernel timing by the global timer (no events in the loop)
+  s.gh_energy = 1;                     // the GH pass sums the energy at the first iteration only
+  s.energy_gate = &s.box->step.it;
+  int r = ABD_OK;
+  for (int tries = 0;; ++tries) {
+    const long long launches0 = s.launches;
+    r = abd::run_graph(s, s.g_step, k.h, issue);
+    if (r) break;
+    s.launches = launches0 + s.g_step.nlaunch - s.step_launch[1];  // counted below
+    if (cudaStreamSynchronize(s.stream) != cudaSuccess) {
+      r = ABD_ERR_CUDA;
+      break;
+    }
+    std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
+    const abd::StepDev& S = s.hbox->step;
+    s.launches += (long long)S.it * s.step_launch[1] + (long long)(S.lin + S.it) * s.step_launch[2];
+    s.n_pairs = s.hstat[abd::DS_NPAIRS];
+    s.n_adj = s.hstat[abd::DS_NADJ];
+    const int bits = s.hstat[abd::DS_STATUS];
+    if (!(bits & abd::kRerunMask)) break;
+    // a list overflowed or a line search needs more trials: the states are as they were;
+    // restore the warm start, drop the kept candidates and grow what was short
+    if (cudaMemcpyAsync(s.dq, s.dq_save, nq, cudaMemcpyDeviceToDevice, s.stream) != cudaSuccess) {
+      r = ABD_ERR_CUDA;
+      break;
+    }
+    if ((r = drop_superset(h))) break;
+    if ((r = overflow(s)) > 0) break;
+    if (bits & abd::ST_LS_MORE) {  // finished on the host
+      s.hstat[abd::DS_STATUS] &= ~abd::ST_LS_MORE;
+      if (cudaMemcpyAsync(s.dstat + abd::DS_STATUS, &s.hstat[abd::DS_STATUS], sizeof(int), cudaMemcpyHostToDevice,
+                          s.stream) != cudaSuccess ||
+          cudaStreamSynchronize(s.stream) != cudaSuccess) {
+        r = ABD_ERR_CUDA;
+        break;
+      }
+      s.energy_gate = nullptr;
+      s.prof_events = 0;
+      return step_host(h, stp, x_view, info);
+    }
+    r = ABD_OK;
+    if (tries >= kMaxReruns) {
+      r = ABD_ERR_OVERFLOW;
+      break;
+    }
+  }
+  s.energy_gate = nullptr;
+  s.prof_events = 0;
+  if (r) return r;
+  const abd::StepDev& S = s.hbox->step;
+  if (s.prof_on) {
+    s.prof_ms += 1e-6 * (double)S.prof_ns;
+    s.prof_launches += (long long)S.prof_n;
+    s.prof_bytes += S.prof_bytes;
+  }
+  abd_step_info inf{};
+  inf.newton_iters = S.it;
+  inf.linear_iters = S.lin;
+  inf.ls_trials = S.ls;
+  inf.n_pt = S.n_pt;
+  inf.n_ee = S.n_ee;
+  inf.n_vg = S.n_vg;
+  inf.n_ij = S.n_ij;
+  inf.n_active = S.n_active;
+  inf.alpha = S.alpha;
+  inf.toi = S.toi;
+  inf.energy = S.E0;
+  inf.status = take_status(h);
+  if (info) *info = inf;
+  return (inf.status & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int abd_adjoint_step(abd_sim* h, const abd_states* st, const double* A, const double* p, const double* qb,
+                     const double* qdb, double* qb_out, double* qdb_out, int* iters) {
+  if (!h || !st || !A || !p || !qb || !qdb || !qb_out || !qdb_out) return ABD_ERR_INVALID;
+  Sim& s = h->s;
+  // the exact Hessian at (A, p): the GH pass with the exact contact and vertex-ground terms
+  // (its candidates from the traversal: the kept line-search candidates are for the step)
+  if (int r = drop_superset(h)) return r;
+  s.exact_hessian = 1;
+  int r = gh_of(h, *st, A, p, nullptr, nullptr, false, 0);
+  s.exact_hessian = 0;
+  if (r) return r;
+  // H lambda = a by preconditioned BiCGSTAB from lambda = 0 (the exact Hessian need not be
+  // positive definite), to the step's Krylov tolerance
+  CK(abd::adjoint_rhs(s, qb, qdb));
+  CK(cudaMemsetAsync(s.adj_x, 0, sizeof(double) * 12 * s.n, s.stream));
+  if ((r = abd::cluster_inverse(s))) return r;
+  const int solver = s.prm.solver;
+  s.prm.solver = 0;
+  int it = 0;
+  r = abd::krylov_solve(s, s.adj_x, &it, &s.g_kadj);
+  s.prm.solver = solver;
+  if (r) return r;
+  if (iters) *iters = it;
+  CK(abd::adjoint_out(s, s.adj_x, qdb, qb_out, qdb_out));
+  CK(cudaStreamSynchronize(s.stream));
+  const int bits = take_status(h);
+  return (bits & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
+}
+
+int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
+  if (!h || !stp) return ABD_ERR_INVALID;
+  // the device loop takes every step whose line search ends within one batch of trials
+  // (alpha_min above 2^-15, the 16th halving of the largest step 1); else the host drives
+  const bool device = h->s.prm.newton_loop == 0 && h->s.prm.alpha_min > 0x1p-15;
+  return device ? step_device(h, stp, x_view, info) : step_host(h, stp, x_view, info);
 }
 
 }  // extern "C"

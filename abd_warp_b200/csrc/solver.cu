@@ -23,7 +23,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <numeric>
 #include <utility>
 #include <vector>
 
@@ -37,7 +36,6 @@ namespace {
 constexpr int WPB = 8;          // warps (body rows) per CTA of the row kernels
 constexpr int AT = 128;         // threads of the cluster apply kernel
 constexpr int IT = 512;         // threads of the cluster inverse kernel (one CTA per cluster)
-constexpr int kMaxCluster = 12; // bodies per cluster: 144 x 144 doubles fit in shared memory
 
 // slots of Sim::partials
 enum { SL_RZ0 = 0, SL_RZ1 = 1, SL_PAP = 2, SL_BZ = 3, SL_RHR = 4, SL_RHV = 5, SL_SZ = 6, SL_TS = 7, SL_TT = 8 };
@@ -51,8 +49,7 @@ struct SolverArgs {
   const double *diag, *offdiag;
   const int *row_ptr, *adj_col, *adj_pair, *pair_active, *fixed;
   const int2* ij;
-  int ncl;            // clusters (setup kernel)
-  const int* ncl_dev; // clusters (device copy: the replayed Krylov kernels read it)
+  const int* ncl_dev; // clusters (formed on the device)
   int maxit;
   const int *cl_ptr, *cl_body;
   const long long* cl_off;
@@ -175,9 +172,11 @@ __global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) 
 }
 
 // ---- preconditioner setup: assemble and invert each cluster's dense block system ----
-__global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, int c0, int c1, const int* body_cl) {
+constexpr int kInvGrid = 148;  // CTAs of the inverse kernel (one per SM at the largest clusters)
+__global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, const int* body_cl) {
   extern __shared__ double K[];
-  for (int c = c0 + blockIdx.x; c < c1; c += gridDim.x) {
+  const int ncl = *a.ncl_dev;
+  for (int c = blockIdx.x; c < ncl; c += gridDim.x) {
     const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
     for (int e = threadIdx.x; e < D * D; e += IT) K[e] = 0.0;
     __syncthreads();
@@ -206,24 +205,38 @@ __global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, int c0, in
       }
     }
     __syncthreads();
-    // in-place Gauss-Jordan inverse (SPD: no pivoting), same operation order as the oracle
-    __shared__ double f[12 * kMaxCluster];
+    // In-place Gauss-Jordan inverse (SPD: no pivoting) with the oracle's arithmetic: at pivot
+    // k, row k is scaled by 1 / K[k][k] (its diagonal becoming that reciprocal), then every
+    // other row i with f = K[i][k] != 0 becomes (j == k ? 0 : K[i][j]) - f K[k][j] (f == 0:
+    // only K[i][k] = 0).  Each row belongs to one warp for the whole inverse (rows warp,
+    // warp + 16, ...), which reads its own multiplier, and the owner of row k + 1 scales that
+    // row right after updating it at pivot k, so the next pivot row is ready at the one block
+    // barrier per pivot.
+    constexpr int NW = IT / 32;
+    const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+    auto scale_row = [&](int i) {  // row i / K[i][i], its diagonal the reciprocal
+      double* R = K + (size_t)i * D;
+      const double ip = 1.0 / R[i];
+      __syncwarp();
+      for (int j = lane; j < D; j += 32) R[j] = (j == i ? 1.0 : R[j]) * ip;
+      __syncwarp();
+    };
+    if (warp == 0) scale_row(0);
+    __syncthreads();
     for (int k = 0; k < D; ++k) {
-      const double p = K[(size_t)k * D + k];
-      __syncthreads();
-      const double ip = 1.0 / p;
-      if (threadIdx.x == 0) K[(size_t)k * D + k] = 1.0;
-      __syncthreads();
-      for (int j = threadIdx.x; j < D; j += IT) K[(size_t)k * D + j] *= ip;
-      for (int i = threadIdx.x; i < D; i += IT) f[i] = (i == k) ? 0.0 : K[(size_t)i * D + k];
-      __syncthreads();
-      for (int i = threadIdx.x; i < D; i += IT)
-        if (i != k) K[(size_t)i * D + k] = 0.0;
-      __syncthreads();
-      for (int i = (int)(threadIdx.x >> 5); i < D; i += IT / 32) {  // a warp per row
-        const double fi = f[i];
-        if (i == k || fi == 0.0) continue;
-        for (int j = (int)(threadIdx.x & 31); j < D; j += 32) K[(size_t)i * D + j] -= fi * K[(size_t)k * D + j];
+      const double* P = K + (size_t)k * D;
+      for (int i = warp; i < D; i += NW) {
+        if (i == k) continue;
+        double* R = K + (size_t)i * D;
+        const double f = R[k];
+        __syncwarp();
+        if (f != 0.0) {
+          for (int j = lane; j < D; j += 32) R[j] = (j == k ? 0.0 : R[j]) - f * P[j];
+        } else if (lane == 0) {
+          R[k] = 0.0;
+        }
+        __syncwarp();
+        if (i == k + 1) scale_row(i);
       }
       __syncthreads();
     }
@@ -489,7 +502,10 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, c
 
 // Threshold thr^2 = tol^2 b^T M^-1 b and the recurrence scalars; b = 0 gives x = 0 and ends
 // the solve before its first iteration
-__global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, double* x) {
+// (and the iteration loop's condition: enter it unless the solve is already done; the loop's
+// node may sit inside another conditional node, whose launches do not reset it)
+__global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, double* x,
+                                                     cudaGraphConditionalHandle h) {
   const double b = a.scal[SC_RED + SL_BZ];
   if (!(b > 0.0))
     for (int i = blockIdx.x * 256 + threadIdx.x; i < 12 * a.n; i += kRedBlocks * 256) x[i] = 0.0;
@@ -498,7 +514,16 @@ __global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, 
     a.scal[SC_THR2] = tol2 * b;
     a.dstat[DS_IT] = 1;
     if (!(b > 0.0)) a.dstat[DS_R_DONE] = 1;
+    cudaGraphSetConditional(h, (b > 0.0 && a.maxit >= 1) ? 1u : 0u);
   }
+}
+
+// The outcome of the last solve into the device loop's step counters: its iterations, and
+// the non-convergence bit when it stopped at cg_max_iter
+__global__ void k_krylov_tally(Mailbox* box) {
+  const int* ds = box->dstat;
+  box->step.lin += ds[DS_SOLVER_ITERS];
+  if (!(ds[DS_R_DONE] || ds[DS_S_DONE])) box->dstat[DS_STATUS] |= ST_SOLVER_NOCONV;
 }
 
 SolverArgs solver_args(Sim& s) {
@@ -512,7 +537,6 @@ SolverArgs solver_args(Sim& s) {
   a.pair_active = s.pair_active;
   a.fixed = s.fixed;
   a.ij = s.ij;
-  a.ncl = s.ncl;
   a.ncl_dev = s.ncl_dev;
   a.maxit = s.prm.cg_max_iter;
   a.cl_ptr = s.cl_ptr;
@@ -528,180 +552,260 @@ SolverArgs solver_args(Sim& s) {
 
 }  // namespace
 
-// Clusters of the preconditioner from the first nact entries of the active-pair list on the
-// host (s.hact), into the pinned tables.  Same clustering rule as the oracle: greedy
-// union-find, strongest coupling first (FP32 Frobenius norm of H_IJ, ties by pair index), at
-// most cluster_max bodies per cluster.  Host work only: it may run while the device is busy.
-int cluster_tables(Sim& s, int nact) {
-  const int n = s.n;
-  const int cap = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
-  std::vector<int> parent(n), size(n, 1);
-  std::iota(parent.begin(), parent.end(), 0);
-  nact = std::max(0, std::min(nact, s.cap_act));
-  if (cap > 1 && nact > 0) {
-    // (weight descending, pair ascending) as one 64-bit key: the weights are positive FP32
-    // values, whose bit patterns order like the values themselves
-    struct Entry {
-      unsigned long long key;
-      int k;
-    };
-    const int4* L = s.hact;
-    std::vector<Entry> order(nact);
-    for (int k = 0; k < nact; ++k)
-      order[k] = {((unsigned long long)(~(unsigned)L[k].w) << 32) | (unsigned)L[k].x, k};
-    std::sort(order.begin(), order.end(), [](const Entry& x, const Entry& y) { return x.key < y.key; });
-    auto find = [&](int x) {
-      while (parent[x] != x) x = parent[x] = parent[parent[x]];
-      return x;
-    };
-    for (const Entry& e : order) {
-      const int a = find(L[e.k].y), b = find(L[e.k].z);
-      if (a == b || size[a] + size[b] > cap) continue;
-      if (a < b) {
-        parent[b] = a;
-        size[a] += size[b];
-      } else {
-        parent[a] = b;
-        size[b] += size[a];
-      }
+// Exclusive prefix sum over the 1024 threads of a CTA (one value per thread); *total gets the
+// sum.  Every thread must call it.
+__device__ inline long long block_scan_excl(long long v, long long* total) {
+  __shared__ long long wsum[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    long long w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
     }
-    for (int b = 0; b < n; ++b) parent[b] = find(b);
+    wsum[lane] = w;  // inclusive prefix of the warp totals
   }
-  // clusters ordered by their first body, members in increasing order
-  const ClusterTables t = cluster_tables_at(s.hstage, n);
-  std::vector<int> first(n, -1), csize;
-  for (int b = 0; b < n; ++b) {
-    const int r = parent[b];
-    if (first[r] < 0) {
-      first[r] = (int)csize.size();
-      csize.push_back(0);
-    }
-    ++csize[first[r]];
-  }
-  const int ncl = (int)csize.size();
-  t.cl_ptr[0] = 0;
-  t.cl_off[0] = 0;
-  int max_cl = 1;
-  for (int c = 0; c < ncl; ++c) {
-    t.cl_ptr[c + 1] = t.cl_ptr[c] + csize[c];
-    const long long d = 12LL * csize[c];
-    t.cl_off[c + 1] = t.cl_off[c] + d * d;
-    max_cl = std::max(max_cl, csize[c]);
-  }
-  std::vector<int> fill(ncl, 0);
-  for (int b = 0; b < n; ++b) {
-    const int c = first[parent[b]];
-    t.cl_body[t.cl_ptr[c] + fill[c]++] = b;
-    t.body_cl[b] = c;
-  }
-  *t.ncl = ncl;
-  s.ncl = ncl;
-  s.max_cl = max_cl;
-  s.cl_bytes = t.bytes_through(ncl);
-  return ABD_OK;
+  __syncthreads();
+  const long long before = (warp > 0 ? wsum[warp - 1] : 0) + x - v;
+  *total = wsum[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before;
 }
 
-// Uploads the tables cluster_tables made (one copy) and inverts every cluster's dense system.
-// Enqueued without a sync.
-int cluster_inverse(Sim& s) {
-  const ClusterTables t = cluster_tables_at(s.hstage, s.n);
-  const size_t need = (size_t)t.cl_off[s.ncl];
-  if (need > s.cap_cl_inv) {
-    if (s.cl_inv) cudaFree(s.cl_inv);
-    s.cl_inv = nullptr;
-    s.cap_cl_inv = std::max(need, 2 * s.cap_cl_inv);
-    if (cudaMalloc(&s.cl_inv, sizeof(double) * s.cap_cl_inv) != cudaSuccess) return ABD_ERR_OVERFLOW;
+// The preconditioner's clusters, formed on the device by one CTA from the active-pair list
+// the pair assembly appended (pair, I, J, FP32 weight bits; in any order).  Rounds: every
+// cluster picks its strongest admissible pair to another cluster (weight, then the lower pair
+// index, as one 64-bit key; admissible: both clusters together within cap bodies) and two
+// clusters that pick the same pair merge under the lower label.  Every decision of a round
+// uses the labels and sizes from its start, so the result does not depend on the order in
+// which threads see the pairs.  Then the tables: clusters ordered by their first body (the
+// label), members in increasing order, the offsets of the dense inverses.  Skipped when the
+// list overflowed (the pass is rerun).
+constexpr int KT = 1024;  // threads of the clustering CTA
+__global__ void __launch_bounds__(KT) k_clusters(int n, int cap, const int4* __restrict__ act, int cap_act,
+                                                 int* dstat, ClusterTables t, ClusterWork w) {
+  const int tid = threadIdx.x;
+  if (dstat[DS_STATUS] & (ST_ACT_OVERFLOW | ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
+  const int m = min(dstat[DS_NACTP], cap_act);
+  for (int b = tid; b < n; b += KT) {
+    w.label[b] = b;
+    w.size[b] = 1;
   }
-  if (cudaMemcpyAsync(s.cl_tab, s.hstage, s.cl_bytes, cudaMemcpyHostToDevice, s.stream)) return ABD_ERR_CUDA;
+  __shared__ int merged;
+  __syncthreads();
+  for (int round = 0; cap > 1 && round < 4 * kMaxCluster; ++round) {
+    for (int b = tid; b < n; b += KT) {
+      w.best[b] = 0ULL;
+      w.to[b] = b;
+    }
+    if (tid == 0) merged = 0;
+    __syncthreads();
+    for (int e = tid; e < m; e += KT) {
+      const int4 q = act[e];
+      const int a = w.label[q.y], b = w.label[q.z];
+      if (a == b || w.size[a] + w.size[b] > cap) continue;
+      const unsigned long long key = ((unsigned long long)(unsigned)q.w << 32) | (0xffffffffULL - (unsigned)q.x);
+      atomicMax(&w.best[a], key);
+      atomicMax(&w.best[b], key);
+    }
+    __syncthreads();
+    // a cluster has one best pair, so it takes part in at most one merge of the round
+    for (int e = tid; e < m; e += KT) {
+      const int4 q = act[e];
+      const int a = w.label[q.y], b = w.label[q.z];
+      if (a == b) continue;
+      const unsigned long long key = ((unsigned long long)(unsigned)q.w << 32) | (0xffffffffULL - (unsigned)q.x);
+      if (w.best[a] != key || w.best[b] != key) continue;
+      const int r = min(a, b), o = max(a, b);
+      w.to[o] = r;
+      w.size[r] += w.size[o];
+      merged = 1;
+    }
+    __syncthreads();
+    for (int b = tid; b < n; b += KT) w.label[b] = w.to[w.label[b]];
+    __syncthreads();
+    if (!merged) break;
+  }
+  // cluster index of every label, cluster offsets and inverse offsets, in label order
+  long long ccarry = 0, pcarry = 0, ocarry = 0;
+  for (int b0 = 0; b0 < n; b0 += KT) {
+    const int b = b0 + tid;
+    const bool root = b < n && w.label[b] == b;
+    const int sz = root ? w.size[b] : 0;
+    long long tc, tp, to_;
+    const long long c = block_scan_excl(root ? 1 : 0, &tc) + ccarry;
+    const long long p = block_scan_excl(sz, &tp) + pcarry;
+    const long long o = block_scan_excl(root ? 144LL * sz * sz : 0, &to_) + ocarry;
+    if (root) {
+      w.cidx[b] = (int)c;
+      t.cl_ptr[c] = (int)p;
+      t.cl_off[c] = o;
+      w.fill[c] = 0;
+    }
+    ccarry += tc;
+    pcarry += tp;
+    ocarry += to_;
+  }
+  const int ncl = (int)ccarry;
+  if (tid == 0) {
+    *t.ncl = ncl;
+    t.cl_ptr[ncl] = n;
+    t.cl_off[ncl] = ocarry;
+  }
+  __syncthreads();
+  for (int b = tid; b < n; b += KT) {
+    const int c = w.cidx[w.label[b]];
+    t.body_cl[b] = c;
+    t.cl_body[t.cl_ptr[c] + atomicAdd(&w.fill[c], 1)] = b;
+  }
+  __syncthreads();
+  for (int c = tid; c < ncl; c += KT) {  // members in increasing order (at most cap of them)
+    int* mb = t.cl_body + t.cl_ptr[c];
+    const int k1 = t.cl_ptr[c + 1] - t.cl_ptr[c];
+    for (int i = 1; i < k1; ++i) {
+      const int v = mb[i];
+      int j = i - 1;
+      for (; j >= 0 && mb[j] > v; --j) mb[j + 1] = mb[j];
+      mb[j + 1] = v;
+    }
+  }
+}
+
+// Clusters of the preconditioner from the active-pair list of the last GH pass, on the device
+// (k_clusters); enqueued on stream st (the pass's stream when null).
+cudaError_t cluster_tables(Sim& s, cudaStream_t st) {
+  const int cap = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
+  k_clusters<<<1, KT, 0, st ? st : s.stream>>>(s.n, cap, s.act_pairs, s.cap_act, s.dstat,
+                                               cluster_tables_at(s.cl_tab, s.n), s.cl_work);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
+// Inverts every cluster's dense system (the tables k_clusters made; their count is read on the
+// device): a fixed grid, the shared memory of the largest cluster cluster_max allows.  Enqueued
+// without a sync.
+int cluster_inverse(Sim& s) {
   SolverArgs a = solver_args(s);
-  const size_t smem = sizeof(double) * 144 * (size_t)s.max_cl * s.max_cl;
+  const int cm = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
+  const size_t smem = sizeof(double) * 144 * (size_t)cm * cm;
   if (smem > 48 * 1024 && (int)smem > s.cl_smem) {
     if (cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
       return ABD_ERR_CUDA;
     s.cl_smem = (int)smem;
   }
-  const int grid = std::min(s.ncl, 4 * 148);
-  k_cluster_inverse<<<grid, IT, smem, s.stream>>>(a, 0, s.ncl, s.body_cl);
+  k_cluster_inverse<<<kInvGrid, IT, smem, s.stream>>>(a, s.body_cl);
   ++s.launches;
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
-int build_preconditioner(Sim& s) {
-  const int r = cluster_tables(s, s.hstat[DS_NACTP]);
-  return r ? r : cluster_inverse(s);
+// Opts the inverse kernel in to the shared memory of the largest cluster (once, at creation:
+// the passes that launch it may be under stream capture)
+int prepare_solver(Sim& s) {
+  const int smem = (int)(sizeof(double) * 144 * kMaxCluster * kMaxCluster);
+  if (cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  s.cl_smem = smem;
+  return ABD_OK;
 }
 
-// Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  One replayed graph:
-// the setup kernels, then a WHILE node whose body is one iteration (its last kernel sets the
-// loop condition).  With iters_out the host waits for it and reads the outcome; without, the
-// solve is only enqueued and its outcome stays in the mailbox's counters (krylov_outcome
-// reads it after the caller's next read of the mailbox).
-int krylov_solve(Sim& s, double* x, int* iters_out) {
+int build_preconditioner(Sim& s) {
+  if (cluster_tables(s, nullptr) != cudaSuccess) return ABD_ERR_CUDA;
+  return cluster_inverse(s);
+}
+
+// Enqueues a solve on s.stream, which must be capturing: the setup kernels, then a WHILE node
+// whose body is one iteration (its last kernel sets the loop condition), the body captured on
+// cap_stream2.  Counts the setup's launches and, in *per_iter, one iteration's.
+int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   const SolverArgs a = solver_args(s);
   const double* bvec = s.g;
   const bool pcg = s.prm.solver == 1;
-  const int per_iter = pcg ? 5 : 10;  // kernels of one iteration (counted once at capture)
+  cudaStream_t st = s.stream;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusActive)
+    return ABD_ERR_CUDA;
+  // the loop's handle first: k_solver_init sets its value
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) return ABD_ERR_CUDA;
+  // b^T M^-1 b sets the threshold
+  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
+  k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
+                                         pcg ? nullptr : s.v);
+  if (cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st) ||
+      cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st))
+    return ABD_ERR_CUDA;
+  k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x, h);
+  // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
+  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
+  s.launches += 4;
+  // the iteration loop: a WHILE node on the capture, its body captured on a second stream
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusActive)
+    return ABD_ERR_CUDA;
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t loop;
+  if (cudaGraphAddNode(&loop, graph, deps, ndeps, &np) != cudaSuccess) return ABD_ERR_CUDA;
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  if (cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  cudaStream_t bs = s.cap_stream2;
+  if (cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return ABD_ERR_CUDA;
+  if (pcg) {
+    k_pcg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v);
+    k_pcg_2<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v, x, s.r);
+    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.z, nullptr, kSlotRzNew);
+    k_pcg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.pv);
+  } else {
+    k_bicg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.pv, s.v);
+    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.pv, s.y, nullptr, -1);
+    k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
+    k_bicg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.v, s.s);
+    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
+    k_bicg_4<<<kRedBlocks, 256, 0, bs>>>(a, s.y, x);
+    k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
+    k_bicg_6<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
+    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
+  }
+  k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
+  if (per_iter_out) *per_iter_out = pcg ? 5 : 10;
+  cudaGraph_t body_out = nullptr;
+  const cudaError_t eb = cudaGetLastError();
+  if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+}
+
+// Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  One replayed graph
+// (krylov_capture).  With iters_out the host waits for it and reads the outcome; without, the
+// solve is only enqueued and its outcome stays in the mailbox's counters (krylov_outcome
+// reads it after the caller's next read of the mailbox).
+int krylov_solve(Sim& s, double* x, int* iters_out, GraphSlot* slot) {
   KeyHash kh;
   kh.add(x).add(s.n).add(s.prm_version).add(s.prm.solver).add(s.prm.cg_max_iter).add(s.cl_inv).add(s.box);
-  int r = run_graph(s, s.g_kinit, kh.h, [&]() -> int {
-    cudaStream_t st = s.stream;
-    // b^T M^-1 b sets the threshold
-    k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
-    k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
-                                           pcg ? nullptr : s.v);
-    if (cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st) ||
-        cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st))
-      return ABD_ERR_CUDA;
-    k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x);
-    // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
-    k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
-    s.launches += 4;
-    // the iteration loop: a WHILE node on the capture, its body captured on a second stream
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t graph = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
-        cs != cudaStreamCaptureStatusActive)
-      return ABD_ERR_CUDA;
-    cudaGraphConditionalHandle h;
-    if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) return ABD_ERR_CUDA;
-    cudaGraphNodeParams np = {};
-    np.type = cudaGraphNodeTypeConditional;
-    np.conditional.handle = h;
-    np.conditional.type = cudaGraphCondTypeWhile;
-    np.conditional.size = 1;
-    cudaGraphNode_t loop;
-    if (cudaGraphAddNode(&loop, graph, deps, ndeps, &np) != cudaSuccess) return ABD_ERR_CUDA;
-    cudaGraph_t body = np.conditional.phGraph_out[0];
-    if (cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
-      return ABD_ERR_CUDA;
-    cudaStream_t bs = s.cap_stream2;
-    if (cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-      return ABD_ERR_CUDA;
-    if (pcg) {
-      k_pcg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v);
-      k_pcg_2<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v, x, s.r);
-      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.z, nullptr, kSlotRzNew);
-      k_pcg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.pv);
-    } else {
-      k_bicg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.pv, s.v);
-      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.pv, s.y, nullptr, -1);
-      k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
-      k_bicg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.v, s.s);
-      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
-      k_bicg_4<<<kRedBlocks, 256, 0, bs>>>(a, s.y, x);
-      k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
-      k_bicg_6<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-      k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
-    }
-    k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
-    s.launches += per_iter;
-    cudaGraph_t body_out = nullptr;
-    const cudaError_t eb = cudaGetLastError();
-    if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
-    return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+  kh.add(s.cap_gen).add(s.adj_col).add(s.adj_pair).add(s.ij).add(s.offdiag).add(s.pair_active);
+  int r = run_graph(s, slot ? *slot : s.g_kinit, kh.h, [&]() -> int {
+    long long per_iter = 0;
+    const int q = krylov_capture(s, x, &per_iter);
+    s.launches += per_iter;  // the graph's count covers one iteration
+    return q;
   });
   if (r || !iters_out) return r;
   if (cudaMemcpyAsync(s.hbox, s.box, sizeof(Mailbox), cudaMemcpyDeviceToHost, s.stream) ||
@@ -709,6 +813,19 @@ int krylov_solve(Sim& s, double* x, int* iters_out) {
     return ABD_ERR_CUDA;
   *iters_out = krylov_outcome(s);
   return ABD_OK;
+}
+
+int krylov_issue(Sim& s, double* x) {
+  long long per_iter = 0;
+  const int r = krylov_capture(s, x, &per_iter);
+  s.step_launch[2] = per_iter;  // the setup's kernels are counted with the Newton iteration's
+  return r;
+}
+
+cudaError_t krylov_tally(Sim& s) {
+  k_krylov_tally<<<1, 1, 0, s.stream>>>(s.box);
+  ++s.launches;
+  return cudaGetLastError();
 }
 
 // The last solve's iterations, from the host's copy of the mailbox; non-convergence raises

@@ -51,6 +51,11 @@ class SimParams:
                                      # PRECISION_MIXED (FP32 PCG inside FP64 refinement), which
                                      # diverges once bodies touch (cond(H) ~ 1e10 > 1 / eps_FP32)
     refine_tol: float = 1e-4         # oracle mixed precision: the FP32 inner solve's relative tolerance
+    newton_loop: int = 0             # 0: the step's Newton iterations run as a device loop (one graph
+                                     # launch per step); 1: the host drives them (same results)
+    min_capacity: int = 0            # > 0: every list of the simulator starts this small and the
+                                     # traversal frontier holds at most this many nodes (tests force
+                                     # the grow-and-rerun paths and the depth-first fallback with it)
 
     @property
     def d2hat(self) -> float:
@@ -84,6 +89,8 @@ class SimParams:
         c.contact_psd = self.contact_psd
         c.precond = self.precond
         c.cluster_max = self.cluster_max
+        c.min_capacity = self.min_capacity
+        c.newton_loop = self.newton_loop
         return c
 
     def as_dict(self):
@@ -102,5 +109,5 @@ class CParams(ctypes.Structure):
         ("psd_ee", ctypes.c_int), ("enable_pt", ctypes.c_int), ("enable_ee", ctypes.c_int),
         ("enable_vg", ctypes.c_int), ("solver", ctypes.c_int), ("cg_max_iter", ctypes.c_int),
         ("precision", ctypes.c_int), ("contact_psd", ctypes.c_int), ("precond", ctypes.c_int),
-        ("cluster_max", ctypes.c_int),
+        ("cluster_max", ctypes.c_int), ("min_capacity", ctypes.c_int), ("newton_loop", ctypes.c_int),
     ]

@@ -111,7 +111,6 @@ class AffineBodySimulator:
                 id=i, x0=self.x0[v0:v1], x=self.x[v0:v1], xk=self.xk[v0:v1], x_view=self.x_view[v0:v1],
                 triangles=torch.as_tensor(b.F, dtype=torch.int32, device=dev),
                 edges=torch.as_tensor(b.edges, dtype=torch.int32, device=dev)))
-        self.highlight = np.zeros(n, dtype=bool)
         self.last_info = None
         # C ABI scene description (host arrays are copied by abd_sim_create)
         self._host = {k: np.ascontiguousarray(flat[k], dtype=np.int32 if k in ("voff", "toff", "eoff", "tris", "edges", "fixed") else np.float64)
@@ -329,6 +328,26 @@ class AffineBodySimulator:
         _lib.check(self._L.abd_energies_along(self._h, ctypes.byref(cst), _ptr(A), _ptr(p), al, len(alphas), E),
                    "abd_energies_along")
         return [E[k] for k in range(len(alphas))]
+
+    # ------------------------------------------------------------------ contact flags
+    @property
+    def highlight(self):
+        """Per-body contact flags of the last gradient / Hessian pass (the last step's last
+        Newton iteration), numpy bool [n]: the reference's ``sim.highlight``, which the step
+        sets from its contact pass (abd/abd.py:238) and the viewer colours bodies by
+        (abd/abd.py:412-413).  A body is flagged when it takes part in an active PT, EE or
+        vertex-ground contact.  Read from the device on access."""
+        t = self.torch
+        out = t.zeros(self.n_bodies, dtype=t.int32, device=self.device)
+        _lib.check(self._L.abd_get_highlight(self._h, _ptr(out)), "abd_get_highlight")
+        return out.cpu().numpy().astype(bool)
+
+    def take_status(self) -> int:
+        """Device status bits accumulated since the last call (and cleared); see
+        ``_lib.STATUS_NAMES``."""
+        st = ctypes.c_int(0)
+        _lib.check(self._L.abd_take_status(self._h, ctypes.byref(st)), "abd_take_status")
+        return st.value
 
     # ------------------------------------------------------------------ dq / g
     @property

@@ -1,29 +1,37 @@
 """Benchmark of the ABD implicit contact time step on B200.
 
 Workload: the 1024-body pile (512 cubes + 512 level-3 icospheres dropped on a fixed ground
-box; V = 332,808, T = 661,516, E = 992,274), a seeded synthetic scene.  A step is one
-implicit time step (Newton with CCD-bounded backtracking line search).  W untimed warm-up
-steps run first; the scene is then reset to its initial state and K steps of its trajectory
-are timed (K = 300, the whole trajectory, by default: the cost of a step grows as the pile
-settles into contact).  Each step is timed with CUDA events on the simulator's stream, and
-L2 is flushed before every step by writing a 256 MiB buffer.
+box; V = 332,808, T = 661,516, E = 992,274), a seeded synthetic scene, 300-step trajectory.
+A step is one implicit time step (Newton with CCD-bounded backtracking line search).
 
-value: steps/s on device-resident states.  e2e: the same trajectory again through the public
-API with host buffers -- every step copies its inputs (A0, p0, Adot, pdot) from pinned host
-memory and reads the new vertex positions back.
+Timed steps: the trajectory is covered in four stretches that start from the oracle's states
+at steps 0, 75, 150 and 225 (tests/golden/c2_states.npz; the GPU reproduces them bit for
+bit).  --steps K times K // 4 consecutive steps from each state (the remainder from the
+first ones), so that a short run samples the free fall, the landing and the settled pile
+alike; K = 300 (the default) is exactly the whole trajectory.  W untimed warm-up steps run
+first.  Each step is timed with CUDA events on the simulator's stream, and L2 is flushed
+before every step by writing a 256 MiB buffer.
+
+value: steps/s on device-resident states.  e2e: the same steps through the public API with
+host buffers: every step copies its inputs (A0, p0, Adot, pdot) in from pinned host memory,
+and copies the new vertex positions and the new states back, inside the timed region.
 
 roofline: the narrow-phase kernel of the CCD pass, which also collects the line-search
-candidates (the largest share of the step), timed with CUDA events around every 4th of its
-launches inside the timed region; the data it moves (algorithmic bytes) is counted by the
-kernel in a replay of the same (deterministic) trajectory, which makes the same launches.
+candidates (the largest share of the step).  The step runs as one CUDA graph whose Newton loop
+is a device-side WHILE node, where events cannot be recorded, so every launch of the kernel
+inside the timed region is timed by the GPU's global timer: the kernel records the start of
+its first CTA and the end of its last, on the stream it runs on.  The data it moves
+(algorithmic bytes) is counted by the kernel in a replay of the same (deterministic) steps,
+which makes the same launches.
 
 Multi-GPU: the step does not shard (one coupled Newton solve per scene), so N ranks run N
 independent replicas; value = N * K / max-over-ranks time.
 
 --impl reference times the CPU FP64 oracle (the restatement of the reference's step; the
-reference itself needs Warp and abdtk, absent here) on all host cores: steps from oracle
-states at steps 0, 75, 150 and 225 of the same trajectory (tests/golden/c2_states.npz),
-weighted equally.  The GPU arm's cpu_baseline is the same measurement on a smaller budget.
+reference itself needs Warp and abdtk, absent here) on all host cores, over the same
+schedule of steps (a bounded number per state when the full schedule would take too long;
+the line says which).  The GPU arm's cpu_baseline is the same measurement on a smaller
+budget.
 """
 from __future__ import annotations
 
@@ -39,10 +47,16 @@ sys.path.insert(0, ROOT)
 METRIC = "ABD steps/s vs plain FP64 on same B200 at \u22641e-6 rel pos err; adjoint grads/s"
 WORKLOAD = "pile of 1024 bodies (512 cubes + 512 level-3 icospheres) on a ground box, 300-step trajectory"
 STATES = os.path.join(ROOT, "tests", "golden", "c2_states.npz")
-# DRAM bytes per launch of the CCD pass's narrow kernel (dram__bytes_read.sum + write.sum)
-# from the ncu capture at trajectory step 225 summarised in
-# profiles/k_chunk_narrow_ccdls_pile1024_state225.md (the contact-rich end of the trajectory)
-NCU_TRAFFIC_PER_LAUNCH = 13.23e6
+STARTS = (0, 75, 150, 225)  # trajectory steps of the stored states
+
+
+def schedule(k):
+    """Steps timed from each stored state: k // 4 each, the remainder from the first ones."""
+    return [k // len(STARTS) + (1 if i < k % len(STARTS) else 0) for i in range(len(STARTS))]
+
+
+def schedule_text(per_state):
+    return ", ".join(f"{n} from step {s}" for s, n in zip(STARTS, per_state) if n)
 
 
 def measured_hbm_peak():
@@ -61,11 +75,14 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64"],
                     help="FP64 only: FP32 Krylov solves inside FP64 refinement diverge on the contact systems")
+    ap.add_argument("--newton-loop", default="device", choices=["device", "host"],
+                    help="the step's Newton iterations as a device loop (one graph launch per step) or driven "
+                         "from the host (two waits per iteration); the same results")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--start-state", type=int, default=None,
-                    help="start from the stored oracle state at this step of the trajectory (0, 75, 150 or 225; "
-                         "for profiling a contact-rich stretch) instead of the initial state")
+                    help="time all K steps from the stored oracle state at this step of the trajectory (0, 75, "
+                         "150 or 225; for profiling one stretch) instead of K / 4 from each")
     return ap.parse_args()
 
 
@@ -83,7 +100,7 @@ def make_scene():
 
 
 class ClockSampler:
-    """SM clocks, power and throttle reasons of the GPU sampled every 100 ms during the timed
+    """SM clocks, power and throttle reasons of the GPU sampled every 20 ms during the timed
     region, in-process through NVML (the data nvidia-smi reports; a polling nvidia-smi
     process would compete with the step's host synchronisations)."""
 
@@ -129,7 +146,7 @@ class ClockSampler:
                     self.rows.append((sm, mx, pw, [k for k, m in masks.items() if rs & m]))
                 except Exception as exc:
                     self.err = str(exc)
-                time.sleep(0.1)
+                time.sleep(0.02)
 
         self.thread = threading.Thread(target=run, daemon=True)
         self.thread.start()
@@ -144,13 +161,13 @@ class ClockSampler:
         sm = sorted(r[0] for r in self.rows)
         return {"sm_mhz": float(sm[len(sm) // 2]), "sm_max_mhz": float(max(r[1] for r in self.rows)),
                 "reasons": sorted({x for r in self.rows for x in r[3]}), "samples": len(self.rows),
-                "power_w_max": max(r[2] for r in self.rows), "source": "NVML, every 100 ms"}
+                "power_w_max": max(r[2] for r in self.rows), "source": "NVML, every 20 ms"}
 
 
-def oracle_sample(budget, max_steps=None):
-    """Oracle steps/s over the trajectory: from each stored state, steps for budget / 4
-    seconds (at least one), the mean time per step weighted equally over the states.
-    Returns (steps_per_s, steps, threads, description)."""
+def oracle_sample(per_state, budget):
+    """Oracle steps/s over the benchmark's schedule: from each stored state, up to per_state[i]
+    consecutive steps, stopping early at budget / 4 seconds per state (at least one step).
+    Returns (steps_per_s, steps done per state, threads, description)."""
     import numpy as np
 
     import oracle
@@ -159,22 +176,27 @@ def oracle_sample(budget, max_steps=None):
     o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
     threads = oracle.max_threads()
     z = np.load(STATES)
-    per_state, total = [], 0
-    for s in z["steps"]:
+    total_s, done = 0.0, []
+    for s, want in zip(STARTS, per_state):
+        if want == 0:
+            done.append(0)
+            continue
         o.set_state(*(z[f"s{s}_{k}"] for k in ("A0", "p0", "Adot", "pdot", "dq")))
         t0 = time.perf_counter()
         n = 0
-        while True:
+        while n < want:
             o.step()
             n += 1
-            if time.perf_counter() - t0 >= budget / len(z["steps"]) or (max_steps and n >= max_steps):
+            if time.perf_counter() - t0 >= budget / len(STARTS):
                 break
-        per_state.append((time.perf_counter() - t0) / n)
-        total += n
-    mean = sum(per_state) / len(per_state)
-    desc = (f"{total} oracle steps from the states at steps {', '.join(str(int(s)) for s in z['steps'])} of the "
-            f"trajectory, mean time per step weighted equally over the states")
-    return 1.0 / mean, total, threads, desc
+        total_s += (time.perf_counter() - t0) * (want / n)  # scaled to the whole stretch
+        done.append(n)
+    want_total = sum(per_state)
+    same = done == list(per_state)
+    desc = (f"oracle steps {schedule_text(done)} of the trajectory"
+            + ("" if same else f" (the first steps of each stretch of the schedule {schedule_text(per_state)}, "
+                               "each stretch's time scaled to its length)"))
+    return want_total / total_s, done, threads, desc
 
 
 def run_reference(args):
@@ -182,13 +204,15 @@ def run_reference(args):
     if rank != 0:
         return
     bodies, _ = make_scene()
-    # a bounded sample: about 2 minutes of host work
-    v, n, threads, desc = oracle_sample(budget=120.0)
+    per_state = schedule(args.steps)
+    # the same steps as the GPU arm, bounded to about 2 minutes of host work
+    v, done, threads, desc = oracle_sample(per_state, budget=120.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
-        "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": WORKLOAD, "bodies": len(bodies), "precision": "fp64"},
+        "config": {"workload": WORKLOAD, "bodies": len(bodies), "precision": "fp64",
+                   "timed_steps": schedule_text(per_state), "oracle_steps_run": schedule_text(done)},
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -213,50 +237,67 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     bodies, prm = make_scene()
+    prm.newton_loop = 0 if args.newton_loop == "device" else 1
     sim = AffineBodySimulator(bodies=bodies, params=prm, device=f"cuda:{local}")
     s = sim.states
     stream = torch.cuda.current_stream(dev)
     names = ("A0", "p0", "Adot", "pdot")
 
-    start = None
-    if args.start_state is not None:
-        z = np.load(STATES)
-        start = {k: torch.as_tensor(z[f"s{args.start_state}_{k}"], device=dev) for k in (*names, "dq")}
+    z = np.load(STATES)
+    per_state = schedule(args.steps)
+    if args.start_state is not None:  # profiling: all K steps from one stored state
+        if args.start_state not in STARTS:
+            raise SystemExit(f"--start-state must be one of {STARTS}")
+        per_state = [args.steps if st == args.start_state else 0 for st in STARTS]
+    starts = {st: {k: torch.as_tensor(z[f"s{st}_{k}"], device=dev) for k in (*names, "dq")} for st in STARTS}
 
-    def reset():  # back to the start state (the scene's initial state, dq warm start 0)
+    def start_at(st):  # the stored state at trajectory step st, with its dq warm start
         sim.reset()
-        if start is not None:
-            for k in names:
-                getattr(s, k).copy_(start[k])
-            s.A.copy_(s.A0)
-            s.p.copy_(s.p0)
-            sim.dq = start["dq"]
+        for k in names:
+            getattr(s, k).copy_(starts[st][k])
+        s.A.copy_(s.A0)
+        s.p.copy_(s.p0)
+        sim.dq = starts[st]["dq"]
         torch.cuda.synchronize(dev)
 
+    def run_schedule(counts, step_fn, at_start=None):
+        """counts[i] consecutive steps from each stored state; returns (total ms, infos)."""
+        total, infos = 0.0, []
+        for st, n in zip(STARTS, counts):
+            if n == 0:
+                continue
+            start_at(st)
+            if at_start:
+                at_start()
+            for _ in range(n):
+                ms, info = step_fn()
+                total += ms
+                infos.append(info)
+        return total, infos
+
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    reset()
-    for _ in range(max(args.warmup, 3)):
-        sim.step()
-    reset()
-    # ---- device-resident timing of K steps of the trajectory ----
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def device_step():
+        flush.zero_()
+        e0.record(stream)
+        info = sim.step()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), info
+
+    # warm-up: W steps spread over the stored states like the timed ones (untimed)
+    run_schedule(schedule(max(args.warmup, 3)), device_step)
+    # ---- device-resident timing of the K steps ----
     clocks = ClockSampler(dev)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
-    sim.profile(1)  # CUDA events around every 4th launch of the CCD pass's narrow kernel
+    sim.profile(1)  # the CCD pass's narrow kernel times its launches (global timer)
     launches0 = sim.launch_count()
-    total_ms = 0.0
-    infos = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        infos.append(sim.step())
-        e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
+    total_ms, infos = run_schedule(per_state, device_step)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
     launches = sim.launch_count() - launches0
@@ -269,39 +310,44 @@ def main():
     max_ms = float(t.item())
     value = world * args.steps / (max_ms / 1e3)
     # ---- end to end through the public API with host buffers ----
-    reset()
-    pin = {k: getattr(s, k).cpu().pin_memory() for k in names}
+    # the caller keeps its states in pinned host memory: each step copies them in, steps, and
+    # copies the new states and the vertex positions out (its next step's inputs)
+    host = {"in": {k: torch.empty(getattr(s, k).shape, dtype=torch.float64).pin_memory() for k in names},
+            "out": {k: torch.empty(getattr(s, k).shape, dtype=torch.float64).pin_memory() for k in names}}
     xv_host = torch.empty(sim.x_view.shape, dtype=torch.float64).pin_memory()
-    h2d = sum(v.numel() * 8 for v in pin.values())
-    d2h = xv_host.numel() * 8
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    e2e_ms = 0.0
-    for _ in range(args.steps):
+    h2d = sum(v.numel() * 8 for v in host["in"].values())
+    d2h = xv_host.numel() * 8 + sum(v.numel() * 8 for v in host["out"].values())
+
+    def e2e_begin():  # the stretch's start state, held by the caller on the host
+        for k in names:
+            host["in"][k].copy_(getattr(s, k))
+
+    def e2e_step():
         flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for k, v in pin.items():
+        for k, v in host["in"].items():
             getattr(s, k).copy_(v, non_blocking=True)
         sim.step()
         xv_host.copy_(sim.x_view, non_blocking=True)
+        for k, v in host["out"].items():
+            v.copy_(getattr(s, k), non_blocking=True)
         e1.record(stream)
         e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
-        for k in pin:  # the caller keeps the new state on the host for its next step
-            pin[k].copy_(getattr(s, k))
+        host["in"], host["out"] = host["out"], host["in"]
+        return e0.elapsed_time(e1), None
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e2e_ms, _ = run_schedule(per_state, e2e_step, e2e_begin)
     te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * args.steps / (float(te.item()) / 1e3)
-    # the algorithmic bytes of the same launches: the trajectory is deterministic, so a replay
-    # with the kernel counting what it reads has the same launches (not timed: counting slows it)
-    reset()
+    # the algorithmic bytes of the same launches: the steps are deterministic, so a replay with
+    # the kernel counting what it reads has the same launches (not timed: counting slows it)
     sim.profile(2)
-    for _ in range(args.steps):
-        sim.step()
+    run_schedule(per_state, lambda: (0.0, sim.step()))
     _, c_launches, c_bytes = sim.profile_read()
     sim.profile(0)
     peak, peak_kind = measured_hbm_peak()
@@ -313,10 +359,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded procedural scene)",
         "config": {"workload": WORKLOAD, "bodies": len(bodies), "verts": int(sim.n_verts),
-                   "timed_steps": (f"steps 1..{args.steps} of the trajectory from the initial state"
-                                   if start is None else
-                                   f"{args.steps} steps from the state at step {args.start_state} of the trajectory"),
+                   "timed_steps": schedule_text(per_state),
                    "precision": args.precision, "parallelism": f"replicas{world}",
+                   "newton_loop": args.newton_loop,
                    "l2": "flushed before every timed step (256 MiB write)",
                    "newton_iters_per_step": float(np.mean([i["newton_iters"] for i in infos])),
                    "linear_iters_per_step": float(np.mean([i["linear_iters"] for i in infos])),
@@ -329,12 +374,12 @@ def main():
                                "the line-search candidates)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                     "traffic": None,
                      "peak_kind": peak_kind, "timed_launches": k_launches, "counted_launches": c_launches,
                      "avg_launch_us": us_per_launch, "bytes_per_launch": bytes_per_launch},
     }
     if rank == 0 and not args.no_cpu_baseline:
-        v, n, threads, desc = oracle_sample(args.cpu_budget)
+        v, _, threads, desc = oracle_sample(per_state, args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)

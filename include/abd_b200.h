@@ -51,6 +51,17 @@ typedef struct abd_params {
   int contact_psd;    /* 1: PSD projection of the barrier Hessian; 0: the reference's form */
   int precond;        /* 1: contact-cluster block Jacobi (clusters of <= cluster_max bodies); 0: per body */
   int cluster_max;    /* 1..12 */
+  int min_capacity;   /* 0: default capacities.  n > 0: every list of the simulator (body
+                         pairs, candidates, contacts, active pairs, vertex-ground pairs) starts
+                         with n entries (read by abd_sim_create) and the breadth-first
+                         traversal frontier holds at most min(n, 512) nodes (read per pass),
+                         so that small scenes run every grow-and-rerun path and the traversal's
+                         depth-first fallback: a host-side way to inject capacity shortfalls */
+  int newton_loop;    /* 0 (default): abd_step runs its Newton iterations as a device loop, one
+                         CUDA graph launch and one copy to the host per step; 1: the host drives
+                         them, waiting for the device twice per iteration.  Both give the same
+                         results; the device loop hands a step over to the host loop when its
+                         line search needs more than 16 trials (alpha_min <= 2^-15) */
 } abd_params;
 
 /* Scene description (host arrays, copied at creation).  Bodies are concatenated:
@@ -87,10 +98,12 @@ typedef struct abd_sim abd_sim;
 /* Create a simulator for one scene on the current CUDA device; stream may be NULL (legacy
  * default stream).  Builds the per-body LBVHs (Morton codes, radix sort, Karras build).
  * Replaces AffineBodySimulator.__init__'s device setup (abd/abd.py:21-95).
- * Returns ABD_ERR_INVALID, before any device work, for a malformed scene: no bodies or no
- * vertices, offsets that do not start at 0 or decrease, a triangle or edge index outside its
- * body's vertices, a non-finite rest position, a free body without a positive finite mass
- * and I0, or precision != 0. */
+ * Returns ABD_ERR_INVALID, before any device work, for a malformed scene: no bodies, a body
+ * without vertices, offsets that do not start at 0 or decrease, a triangle or edge index
+ * outside its body's vertices, a non-finite rest position, a free body without a positive
+ * finite mass and I0, precision != 0 or min_capacity < 0; and, after the tree build, for a
+ * body whose primitive tree is deeper than the traversal stack holds (3 ceil(H / 2) + 1 > 64
+ * entries for H internal levels, which takes many primitives with one Morton code). */
 int abd_sim_create(const abd_scene_desc* scene, const abd_params* prm, void* stream, abd_sim** out);
 int abd_sim_destroy(abd_sim* sim);
 int abd_sim_set_params(abd_sim* sim, const abd_params* prm);
@@ -108,6 +121,26 @@ int abd_sim_sizes(const abd_sim* sim, int* n_bodies, int* n_verts, int* n_tris, 
  * inertia + orthogonality + IPC barrier energy with CCD-bounded backtracking line search,
  * then q0 <- q, qdot <- (q - q0)/dt and x_view_dev <- transform(q0).  x_view_dev may be NULL. */
 int abd_step(abd_sim* sim, const abd_states* st, double* x_view_dev, abd_step_info* info);
+
+/* One step of the adjoint of abd_step (the reference has none: hl_entry.py:4 sets
+ * enable_backward = False).  A converged step solves grad E(q; q~) = 0 for q_{t+1}, with the
+ * prediction q~ = q_t + dt qdot_t (+ dt^2 g on p), and qdot_{t+1} = (q_{t+1} - q_t) / dt.  Given
+ * the adjoints qb_dev, qdb_dev [n][12] of q_{t+1} and qdot_{t+1} (per body [p, A rows], the
+ * layout of g / dq), this returns those of q_t and qdot_t:
+ *   a = qb + qdb / dt,  H lambda = a,  qb_out = M lambda - qdb / dt,  qdb_out = dt M lambda,
+ * where H is the exact Hessian of the step's energy at q_{t+1} = (A_dev, p_dev) -- inertia,
+ * orthogonality, and each active contact's unprojected barrier Hessian with every
+ * second-derivative term (the Newton Hessian projects the barrier and, like the reference,
+ * leaves out the derivatives of the closest-point coefficients: psd/vf.py:150-176,
+ * psd/ee.py:94-116, and the vertex-ground 2 B' term: vg_ipc.py:28-33) -- and M the mass matrix
+ * (mass on p, I0 on A).  H is solved by preconditioned BiCGSTAB to cg_tol; iters (host, may be
+ * NULL) receives its iterations.  st supplies the inertia prediction (its A0 / p0 / Adot / pdot:
+ * any values; H does not depend on them).  Fixed bodies get zero adjoints.  Valid where the
+ * step converged (g.g below tol): the implicit-function derivative it computes is the
+ * derivative of the step only there. */
+int abd_adjoint_step(abd_sim* sim, const abd_states* st, const double* A_dev, const double* p_dev,
+                     const double* qb_dev, const double* qdb_dev, double* qb_out_dev, double* qdb_out_dev,
+                     int* iters);
 
 /* x = p + sum_k r_k a_k for every vertex (update_mesh_vertex, abd/abd.py:305-324). */
 int abd_update_mesh_vertex(abd_sim* sim, const double* A_dev, const double* p_dev, double* x_dev);
@@ -176,11 +209,25 @@ int abd_energies_along(abd_sim* sim, const abd_states* st, const double* A_dev, 
  * application owns all device memory).  It allocates nothing; its only scratch is a
  * fixed array inside the library (4096 doubles, so n_bodies <= 1,048,576, else
  * ABD_ERR_INVALID).  All calls share that array: calls that overlap on the GPU race.  The
- * first call on a device looks up the array's address (make it before any stream capture).
- * Fixed bodies contribute nothing.  Runs on `stream` (NULL: legacy default stream). */
+ * first call on a device looks up the array's address (make it before any stream capture);
+ * the address is kept for the process, so after cudaDeviceReset of a device this entry point
+ * must not be called on it again.  The sum is a fixed-order tree (per CTA of 256 bodies, then
+ * over the CTAs): deterministic, but it can differ in the last bits from abd_compute_energy,
+ * whose sum is exact.  Fixed bodies contribute nothing.  Runs on `stream` (NULL: legacy
+ * default stream). */
 int abd_inertia_energy_noalloc(const abd_params* prm, int n_bodies, const abd_states* st, const double* Ak_dev,
                                const double* pk_dev, const double* mass_dev, const double* I0_dev,
                                const int* fixed_dev, double* E_dev, void* stream);
+
+/* Per-body contact flags of the last gradient / Hessian pass (the step's last Newton
+ * iteration, or abd_ipc_gh) into highlight_dev [n] (int, device): 1 when the body takes part
+ * in an active PT or EE contact (d^2 < dhat^2 and a valid closest-point configuration) or has
+ * an active vertex-ground contact, else 0.  The reference's step sets sim.highlight from its
+ * contact pass every Newton iteration (abd/abd.py:238) and the viewer colours bodies by it
+ * (abd/abd.py:412-413); ipc.py:59-60 keeps only the EE result and marks one body per contact
+ * (pt_ipc.py:118, ee_ipc.py:98).  Here PT, EE and vertex-ground contacts all count, for both
+ * bodies of a contact. */
+int abd_get_highlight(abd_sim* sim, int* highlight_dev);
 
 /* Device status bits accumulated since the last call (and cleared). */
 int abd_take_status(abd_sim* sim, int* status);
@@ -191,9 +238,11 @@ long long abd_launch_count(const abd_sim* sim);
 
 /* Kernel profiling (no counterpart in the reference; used by the benchmark's roofline).
  * abd_profile(sim, mode) resets the counters; from then on the step's CCD passes (which also
- * collect the line-search candidates) record CUDA events around their narrow-phase kernel on
- * the simulator's stream -- every 4th pass in mode 1, every pass in mode 2, which also counts
- * the data the kernel moves (and slows it down).
+ * collect the line-search candidates) time their narrow-phase kernel: with the device Newton
+ * loop (newton_loop 0) every launch, by the GPU's global timer (the kernel records its first
+ * CTA's start and its last CTA's end); with the host loop by CUDA events on the simulator's
+ * stream, every 4th pass in mode 1 and every pass in mode 2.  Mode 2 also counts the data the
+ * kernel moves (and slows it down).
  * abd_profile_read returns the accumulated kernel time (ms), the number of launches and, for
  * mode 2, the algorithmic bytes (point queries 24 B, edge queries 36 B, (chunk, neighbour)
  * records 140 B, tree entries tested 36 B, candidates written 16 B).

@@ -31,6 +31,7 @@ def lib():
         L.orc_create.restype = v
         L.orc_create.argtypes = [i] + [v] * 10
         L.orc_destroy.argtypes = [v]
+        L.orc_get_highlight.argtypes = [v, v]
         L.orc_set_params.argtypes = [v, v]
         L.orc_set_threads.argtypes = [i]
         L.orc_max_threads.restype = i
@@ -54,6 +55,8 @@ def lib():
         L.orc_log.restype = d
         L.orc_exact_sum.argtypes = [v, ctypes.c_long]
         L.orc_exact_sum.restype = d
+        L.orc_inertia_energy_sum.argtypes = [i, v] + [v] * 9
+        L.orc_inertia_energy_sum.restype = d
         L.orc_contact_energy.argtypes = [i, v, v]
         L.orc_contact_energy.restype = d
         L.orc_collision_time.argtypes = [i, v, v]
@@ -64,7 +67,7 @@ def lib():
         L.orc_set_friction.argtypes = [v, d, d]
         L.orc_friction_contact.argtypes = [i, v, v, v, d, d, v, v, v, v, v, v]
         L.orc_friction_contact.restype = i
-        L.orc_full_hessian.argtypes = [v, v, v, v]
+        L.orc_full_hessian.argtypes = [v, v, v, v, i]
         L.orc_full_hessian.restype = i
         L.orc_cubic_roots.argtypes = [v, d, d, v]
         L.orc_cubic_roots.restype = i
@@ -131,12 +134,14 @@ class Oracle:
         contacts; 0 turns it off."""
         lib().orc_set_friction(self.h, float(mu), float(eps_v))
 
-    def full_hessian(self, A, p):
-        """Exact, unprojected Hessian of the step's energy at (A, p) under the full contact
-        model: dense [12n, 12n], DOFs [p, A rows] per body, fixed bodies' rows zero."""
+    def full_hessian(self, A, p, model="full"):
+        """Exact, unprojected Hessian of the step's energy at (A, p): dense [12n, 12n], DOFs
+        [p, A rows] per body, fixed bodies' rows zero.  model "full": the full contact model
+        (needs set_ipc_full(True)); "reference": the reference's interior PT / EE contacts with
+        their complete second derivatives."""
         A, p = _c64(A), _c64(p)
         H = np.zeros((12 * self.n, 12 * self.n))
-        if lib().orc_full_hessian(self.h, _p(A), _p(p), _p(H)) < 0:
+        if lib().orc_full_hessian(self.h, _p(A), _p(p), _p(H), 1 if model == "full" else 0) < 0:
             raise RuntimeError("full_hessian needs set_ipc_full(True)")
         return H
 
@@ -153,6 +158,12 @@ class Oracle:
         xv = np.zeros((self.V, 3))
         lib().orc_get_state(self.h, _p(A0), _p(p0), _p(Adot), _p(pdot), _p(dq), _p(xv))
         return {"A0": A0, "p0": p0, "Adot": Adot, "pdot": pdot, "dq": dq, "x_view": xv}
+
+    def highlight(self):
+        """Per-body contact flags of the last assembly (bool [n])."""
+        out = np.zeros(self.n, dtype=np.int32)
+        lib().orc_get_highlight(self.h, _p(out))
+        return out.astype(bool)
 
     def step(self):
         info = OrcInfo()
@@ -262,6 +273,14 @@ def abd_log(x: float) -> float:
 def exact_sum(values) -> float:
     v = _c64(np.ravel(values))
     return lib().orc_exact_sum(_p(v), len(v))
+
+
+def inertia_energy_sum(prm, Ak, pk, A0, p0, Adot, pdot, mass, I0, fixed):
+    """Exact sum of the bodies' inertia + orthogonality energies (fixed bodies: none)."""
+    arrs = [_c64(a) for a in (Ak, pk, A0, p0, Adot, pdot, mass, I0)]
+    fx = _c32(fixed)
+    c = prm.to_c()
+    return lib().orc_inertia_energy_sum(len(fx), ctypes.byref(c), *[_p(a) for a in arrs], _p(fx))
 
 
 def contact_energy(type_, x4, prm):

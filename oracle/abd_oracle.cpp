@@ -44,6 +44,8 @@ struct Params {
   double ls_noise_floor;
   int max_iter, armijo_sign, ground_enabled, psd_ee, enable_pt, enable_ee, enable_vg, solver,
       cg_max_iter, precision, contact_psd, precond, cluster_max;
+  int min_capacity;  // the CUDA library's capacity injection (the oracle has no capacities)
+  int newton_loop;   // the CUDA library's choice of Newton loop (the oracle has one)
 };
 
 struct V3 {
@@ -196,6 +198,7 @@ struct Oracle {
   std::vector<int> ij;            // [npairs][2]
   std::vector<int> pact;          // [npairs] active contacts
   std::vector<int> adj_ptr, adj;  // per body (neighbour, pair, side), neighbours increasing
+  std::vector<int> highlight;     // [n] body in an active PT / EE / vertex-ground contact (abd.py:238)
   // stats
   int stat_newton = 0, stat_lin = 0, stat_ls = 0, stat_pt = 0, stat_ee = 0, stat_vg = 0, stat_ij = 0,
       stat_active = 0, stat_refine = 0;
@@ -1502,6 +1505,16 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
     for (int k = 0; k < 144; ++k) o.diag[144 * b + k] = acc[k].round();
     for (int k = 0; k < 12; ++k) o.g[12 * b + k] = acc[144 + k].round();
   }
+  // contact flags (abd.py:238; ipc.py:59-60 keeps only EE, here PT, EE and vertex-ground all
+  // count, for both bodies of a contact)
+  o.highlight.assign(n, 0);
+  for (int q = 0; q < m; ++q)
+    if (o.pact[q] > 0) o.highlight[L.ij[2 * q]] = o.highlight[L.ij[2 * q + 1]] = 1;
+  if (o.prm.ground_enabled && o.prm.enable_vg)
+    for (size_t k = 0; k + 1 < L.vg.size(); k += 2) {
+      const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
+      if (d * d < o.prm.d2hat) o.highlight[L.vg[k]] = 1;
+    }
   // pairs touching a fixed (Dirichlet) body have no coupling block
   for (int q = 0; q < m; ++q)
     if (o.fixed[L.ij[2 * q]] || o.fixed[L.ij[2 * q + 1]])
@@ -1585,67 +1598,86 @@ void inv12(const double* Ain, double* out) {
     for (int c = 0; c < 12; ++c) out[r * 12 + c] = a[r][12 + c];
 }
 
-// In-place Gauss-Jordan inverse without pivoting of an SPD matrix (row-major N x N).
-void inv_spd_inplace(std::vector<double>& a, int N) {
+// In-place Gauss-Jordan inverse without pivoting of an SPD matrix (row-major N x N), in the
+// arithmetic of T (double; float for the mixed-precision preconditioner).
+template <class T>
+void inv_spd_inplace(std::vector<T>& a, int N) {
   for (int k = 0; k < N; ++k) {
-    const double p = a[(size_t)k * N + k];
-    a[(size_t)k * N + k] = 1.0;
-    const double ip = 1.0 / p;
+    const T p = a[(size_t)k * N + k];
+    a[(size_t)k * N + k] = T(1);
+    const T ip = T(1) / p;
     for (int j = 0; j < N; ++j) a[(size_t)k * N + j] *= ip;
     for (int i = 0; i < N; ++i) {
       if (i == k) continue;
-      const double f = a[(size_t)i * N + k];
-      a[(size_t)i * N + k] = 0.0;
-      if (f != 0.0)
+      const T f = a[(size_t)i * N + k];
+      a[(size_t)i * N + k] = T(0);
+      if (f != T(0))
         for (int j = 0; j < N; ++j) a[(size_t)i * N + j] -= f * a[(size_t)k * N + j];
     }
   }
 }
 
-// Contact clusters for the preconditioner: union-find over free body pairs with active
-// contacts, strongest coupling (Frobenius norm of the off-diagonal block, as float) first,
-// ties by pair index, merged only while the cluster stays within cluster_max bodies.
-// Clusters list their bodies in increasing order and are ordered by their first body.
+// Contact clusters for the preconditioner (the preconditioner is this project's, not the
+// reference's, whose bicgstab runs unpreconditioned): free body pairs with active contacts,
+// weighted by the Frobenius norm of their coupling block (as float), merged in rounds.  In a
+// round every cluster picks its strongest admissible pair to another cluster -- weight, then
+// the lower pair index; admissible: the two clusters together within cluster_max bodies --
+// and two clusters that pick the same pair merge, under the lower label (the lower first
+// body).  Rounds repeat until none merges.  Every decision of a round uses the labels and
+// sizes from its start, so the rule has the same result in any order of evaluation (the GPU
+// forms the clusters this way in parallel).  Clusters list their bodies in increasing order
+// and are ordered by their first body.
 void build_clusters(const Oracle& o, std::vector<int>& cl_ptr, std::vector<int>& cl_body) {
   const int n = o.n, m = (int)o.ij.size() / 2;
-  std::vector<std::pair<float, int>> w;
+  struct Edge {
+    unsigned long long key;
+    int I, J;
+  };
+  std::vector<Edge> w;
   for (int q = 0; q < m; ++q) {
     const int I = o.ij[2 * q], J = o.ij[2 * q + 1];
-    if (o.fixed[I] || o.fixed[J]) continue;
+    if (o.fixed[I] || o.fixed[J] || o.pact[q] <= 0) continue;
     double f = 0.0;
     for (int k = 0; k < 144; ++k) f += o.off[144 * (size_t)q + k] * o.off[144 * (size_t)q + k];
-    if (f > 0.0) w.push_back({(float)std::sqrt(f), q});
+    const float wf = (float)std::sqrt(f);
+    if (!(wf > 0.f)) continue;
+    unsigned wb;
+    std::memcpy(&wb, &wf, 4);
+    w.push_back({((unsigned long long)wb << 32) | (0xffffffffULL - (unsigned)q), I, J});
   }
-  std::sort(w.begin(), w.end(), [](const std::pair<float, int>& a, const std::pair<float, int>& b) {
-    return a.first > b.first || (a.first == b.first && a.second < b.second);
-  });
-  std::vector<int> parent(n), size(n, 1);
-  for (int b = 0; b < n; ++b) parent[b] = b;
-  auto find = [&](int x) {
-    while (parent[x] != x) x = parent[x] = parent[parent[x]];
-    return x;
-  };
   const int cap = o.prm.precond == 1 ? std::max(1, o.prm.cluster_max) : 1;
-  for (auto& e : w) {
-    const int a = find(o.ij[2 * e.second]), b = find(o.ij[2 * e.second + 1]);
-    if (a == b || size[a] + size[b] > cap) continue;
-    if (a < b) {
-      parent[b] = a;
-      size[a] += size[b];
-    } else {
-      parent[a] = b;
-      size[b] += size[a];
+  std::vector<int> label(n), size(n, 1), to(n);
+  for (int b = 0; b < n; ++b) label[b] = b;
+  std::vector<unsigned long long> best(n);
+  for (bool merged = cap > 1; merged;) {
+    merged = false;
+    std::fill(best.begin(), best.end(), 0ULL);
+    for (const Edge& e : w) {
+      const int a = label[e.I], b = label[e.J];
+      if (a == b || size[a] + size[b] > cap) continue;
+      best[a] = std::max(best[a], e.key);
+      best[b] = std::max(best[b], e.key);
     }
+    for (int b = 0; b < n; ++b) to[b] = b;
+    for (const Edge& e : w) {
+      const int a = label[e.I], b = label[e.J];
+      if (a == b || best[a] != e.key || best[b] != e.key) continue;
+      const int r = std::min(a, b), q = std::max(a, b);
+      to[q] = r;
+      size[r] += size[q];
+      merged = true;
+    }
+    for (int b = 0; b < n; ++b) label[b] = to[label[b]];
   }
-  std::vector<int> root_first(n, -1), order;
+  std::vector<int> first(n, -1);
   std::vector<std::vector<int>> members;
   for (int b = 0; b < n; ++b) {
-    const int r = find(b);
-    if (root_first[r] < 0) {
-      root_first[r] = (int)members.size();
+    const int r = label[b];
+    if (first[r] < 0) {
+      first[r] = (int)members.size();
       members.push_back({});
     }
-    members[root_first[r]].push_back(b);
+    members[first[r]].push_back(b);
   }
   cl_ptr.assign(1, 0);
   cl_body.clear();
@@ -1655,7 +1687,8 @@ void build_clusters(const Oracle& o, std::vector<int>& cl_ptr, std::vector<int>&
   }
 }
 
-// Mixed precision (precision == 1): FP64 iterative refinement around an FP32 PCG.  Each sweep
+// Refinement (precision == 2, kept as a measured negative result): FP64 iterative refinement
+// around an FP32 PCG.  Each sweep
 // takes the FP64 residual r = b - H x and its preconditioned norm; the solve stops when that
 // norm meets the FP64 target (rz <= thr2, the FP64 solve's test), else an FP32 PCG solves
 // H e = r from e = 0 -- FP32 copies of the blocks and of the cluster inverses, FP32 vector
@@ -1778,7 +1811,11 @@ int solve(Oracle& o) {
     const size_t s = cl_ptr[c + 1] - cl_ptr[c];
     cl_off[c + 1] = cl_off[c] + 144 * s * s;
   }
-  std::vector<double> Kinv(cl_off[ncl]);
+  // precision 1: the cluster systems rounded to FP32 and inverted in FP32 arithmetic; the
+  // preconditioner is then applied in FP32 (the Krylov iteration itself stays FP64)
+  const bool p32 = o.prm.precision == 1;
+  std::vector<double> Kinv(p32 ? 0 : cl_off[ncl]);
+  std::vector<float> Kinv32(p32 ? cl_off[ncl] : 0);
   std::vector<int> where(n, -1);
   for (int c = 0; c < ncl; ++c)
     for (int k = cl_ptr[c]; k < cl_ptr[c + 1]; ++k) where[cl_body[k]] = k - cl_ptr[c];
@@ -1806,14 +1843,33 @@ int solve(Oracle& o) {
             K[(size_t)(12 * b + cc) * D + 12 * a + r] = v;
           }
       }
-    inv_spd_inplace(K, D);
-    std::copy(K.begin(), K.end(), Kinv.begin() + cl_off[c]);
+    if (p32) {
+      std::vector<float> K32(K.size());
+      for (size_t e = 0; e < K.size(); ++e) K32[e] = (float)K[e];
+      inv_spd_inplace(K32, D);
+      std::copy(K32.begin(), K32.end(), Kinv32.begin() + cl_off[c]);
+    } else {
+      inv_spd_inplace(K, D);
+      std::copy(K.begin(), K.end(), Kinv.begin() + cl_off[c]);
+    }
   }
+  // out = M^-1 v: FP64, or (precision 1) the FP32 inverse times v rounded to FP32, summed in
+  // FP32 and widened
   auto prec = [&](const std::vector<double>& v, std::vector<double>& out) {
     out.assign(N, 0.0);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int c = 0; c < ncl; ++c) {
       const int s = cl_ptr[c + 1] - cl_ptr[c], D = 12 * s;
+      if (p32) {
+        const float* K = &Kinv32[cl_off[c]];
+        for (int i = 0; i < D; ++i) {
+          float acc = 0.f;
+          for (int j = 0; j < D; ++j)
+            acc += K[(size_t)i * D + j] * (float)v[12 * cl_body[cl_ptr[c] + j / 12] + j % 12];
+          out[12 * cl_body[cl_ptr[c] + i / 12] + i % 12] = (double)acc;
+        }
+        continue;
+      }
       const double* K = &Kinv[cl_off[c]];
       for (int i = 0; i < D; ++i) {
         double acc = 0.0;
@@ -1832,13 +1888,15 @@ int solve(Oracle& o) {
     return 0;
   }
   const double thr2 = o.prm.cg_tol * o.prm.cg_tol * bz;
-  if (o.prm.precision == 1) return solve_mixed(o, Kinv, cl_off, cl_ptr, cl_body, prec, thr2);
+  if (o.prm.precision == 2) return solve_mixed(o, Kinv, cl_off, cl_ptr, cl_body, prec, thr2);
   std::vector<double> r(N), Ax;
   spmv(o, x, Ax);
   for (int i = 0; i < N; ++i) r[i] = bvec[i] - Ax[i];
   int it = 0;
   if (o.prm.solver == 1) {  // PCG, converged when r^T M^-1 r <= tol^2 b^T M^-1 b
-    std::vector<double> z, pv, Ap;
+    // precision 1: flexible CG (Polak-Ribiere beta = z_new.(r_new - r_old) / z_old.r_old), which
+    // tolerates the FP32 preconditioner's rounding (not exactly a symmetric linear map)
+    std::vector<double> z, pv, Ap, rold;
     prec(r, z);
     double rz = ddot(r, z);
     if (rz <= thr2) return 0;
@@ -1851,6 +1909,7 @@ int solve(Oracle& o) {
         break;
       }
       const double alpha = rz / pAp;
+      if (p32) rold = r;
       for (int i = 0; i < N; ++i) {
         x[i] += alpha * pv[i];
         r[i] -= alpha * Ap[i];
@@ -1858,7 +1917,7 @@ int solve(Oracle& o) {
       prec(r, z);
       const double rzn = ddot(r, z);
       if (rzn <= thr2) break;
-      const double beta = rzn / rz;
+      const double beta = p32 ? (rzn - ddot(rold, z)) / rz : rzn / rz;
       for (int i = 0; i < N; ++i) pv[i] = z[i] + beta * pv[i];
       rz = rzn;
     }
@@ -2300,6 +2359,11 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
 }
 
 void orc_destroy(void* h) { delete (Oracle*)h; }
+// contact flags of the last assembly (the step's last Newton iteration, or orc_gh)
+void orc_get_highlight(void* h, int* out) {
+  const Oracle& o = *(Oracle*)h;
+  for (int b = 0; b < o.n; ++b) out[b] = (int)o.highlight.size() == o.n ? o.highlight[b] : 0;
+}
 void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
 void orc_set_ipc_full(void* h, int on) { ((Oracle*)h)->ipc_full = on != 0; }
 // lagged friction with coefficient mu and slip velocity eps_v (needs the full contact model)
@@ -2446,9 +2510,17 @@ int orc_gh(void* h, const double* A, const double* p, double* g, double* diag, d
 // orthogonality (exact in the assembly already) plus every candidate's unprojected
 // full-model contact Hessian.  Needs the full contact model (set_ipc_full).  Rows and columns
 // of fixed bodies are left zero.  Returns the number of active contacts, -1 without the model.
-int orc_full_hessian(void* h, const double* A, const double* p, double* Hd) {
+// Exact, unprojected Hessian of the step's energy at (A, p), dense [12n][12n].  model 1: the
+// full contact model (needs ipc_full); model 0: the reference's model -- the interior PT /
+// EE contacts the reference evaluates (d^2 < dhat^2 and a valid closest-point configuration,
+// pt_ipc.py:111-118, ee_ipc.py:93-97), each the barrier of the point-plane or line-line
+// squared distance with its full second derivative (the terms with the derivatives of the
+// closest-point coefficients that the reference's Newton Hessian leaves out, psd/vf.py:150-176,
+// psd/ee.py:94-116), and the vertex-ground barriers with their 2 B' term (vg_ipc.py:28-33
+// leaves it out).
+int orc_full_hessian(void* h, const double* A, const double* p, double* Hd, int model) {
   Oracle* o = (Oracle*)h;
-  if (!o->ipc_full) return -1;
+  if (model == 1 && !o->ipc_full) return -1;
   const int n = o->n;
   const size_t N = 12 * (size_t)n;
   std::fill(Hd, Hd + N * N, 0.0);
@@ -2466,6 +2538,18 @@ int orc_full_hessian(void* h, const double* A, const double* p, double* Hd) {
   Lists L;
   static_boxes(*o, o->x.data(), bx);
   cull(*o, bx, L);
+  // vertex-ground barriers, exact: d = y - ground, d2E/dy2 = 2 B'(d^2) + 4 d^2 B''(d^2)
+  if (o->prm.ground_enabled && o->prm.enable_vg)
+    for (size_t q = 0; q + 1 < L.vg.size(); q += 2) {
+      const int b = L.vg[q], v = L.vg[q + 1];
+      if (o->fixed[b]) continue;
+      const double d = o->x[3 * (size_t)v + 1] - o->prm.ground;
+      const double hy = 2.0 * barrier_d1(d * d, o->prm) + 4.0 * d * d * barrier_d2(d * d, o->prm);
+      const double th[4] = {1.0, o->x0[3 * v], o->x0[3 * v + 1], o->x0[3 * v + 2]};
+      for (int m = 0; m < 4; ++m)
+        for (int n2 = 0; n2 < 4; ++n2)
+          Hd[(12 * (size_t)b + 3 * m + 1) * N + 12 * (size_t)b + 3 * n2 + 1] += th[m] * th[n2] * hy;
+    }
   int active = 0;
   for (int kind = 0; kind < 2; ++kind) {
     const std::vector<Cand>& C = kind == 0 ? L.pt : L.ee;
@@ -2473,7 +2557,22 @@ int orc_full_hessian(void* h, const double* A, const double* p, double* Hd) {
       V3 xs[4], rs[4];
       fetch(*o, o->x.data(), cd, kind, xs, rs);
       D12 E;
-      if (!full_energy_d(kind, xs, rs, o->prm, E)) continue;
+      if (model == 1) {
+        if (!full_energy_d(kind, xs, rs, o->prm, E)) continue;
+      } else {
+        double terms[456];
+        if (!contact_terms(kind, xs, rs, 0, o->prm, terms)) continue;  // the reference's activity
+        V3D X[4];
+        for (int k = 0; k < 4; ++k)
+          X[k] = {d12_var(xs[k].x, 3 * k), d12_var(xs[k].y, 3 * k + 1), d12_var(xs[k].z, 3 * k + 2)};
+        const D12 d = full_d2(kind, kind == 0 ? (int)F_PT : (int)F_EE, X);
+        const double dh = o->prm.d2hat, sv = d.v / dh, l = std::log(sv);
+        const double f = -o->prm.kappa * (sv - 1.0) * (sv - 1.0) * l;
+        const double f1 = -o->prm.kappa * (2.0 * (sv - 1.0) * l + (sv - 1.0) * (sv - 1.0) / sv) / dh;
+        const double f2 =
+            -o->prm.kappa * (2.0 * l + 4.0 * (sv - 1.0) / sv - (sv - 1.0) * (sv - 1.0) / (sv * sv)) / (dh * dh);
+        E = apply(d, f, f1, f2);
+      }
       ++active;
       const int nI = kind == 0 ? 1 : 2;
       const int body[2] = {cd.I, cd.J};  // the candidate's first group moves with cd.I
@@ -2539,6 +2638,37 @@ double orc_exact_sum(const double* v, long n) {
   XSum s;
   for (long i = 0; i < n; ++i) s.add(v[i]);
   return s.round();
+}
+
+// Inertia + orthogonality energy of n free-standing bodies (orthogonal_energy.py:24-32, the
+// per-body term of inertia_energy above) at trial DOFs (Ak, pk) with the prediction from
+// (A0, p0, Adot, pdot), summed exactly; fixed bodies contribute nothing.  Checks the library's
+// allocation-free energy on synthetic states of any size.
+double orc_inertia_energy_sum(int n, const Params* prm, const double* Ak, const double* pk, const double* A0,
+                              const double* p0, const double* Adot, const double* pdot, const double* mass,
+                              const double* I0, const int* fixed) {
+  XSum total;
+  const double dt = prm->dt;
+  for (int b = 0; b < n; ++b) {
+    if (fixed[b]) continue;
+    double At[9], pt[3];
+    for (int k = 0; k < 9; ++k) At[k] = A0[9 * b + k] + dt * Adot[9 * b + k];
+    const double gv[3] = {0.0, prm->gravity, 0.0};
+    for (int k = 0; k < 3; ++k) pt[k] = (p0[3 * b + k] + dt * pdot[3 * b + k]) + (dt * dt) * gv[k];
+    const double* a = Ak + 9 * b;
+    double eo = 0.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const double t = dot(row(a, i), row(a, j)) - (i == j ? 1.0 : 0.0);
+        eo += t * t;
+      }
+    eo = eo * prm->stiffness;
+    V3 d0 = V3{pk[3 * b], pk[3 * b + 1], pk[3 * b + 2]} - V3{pt[0], pt[1], pt[2]};
+    V3 d1 = row(a, 0) - row(At, 0), d2 = row(a, 1) - row(At, 1), d3 = row(a, 2) - row(At, 2);
+    const double nm = dot(d0, d0) * mass[b] + (dot(d1, d1) + dot(d2, d2) + dot(d3, d3)) * I0[b];
+    total.add(eo * dt * dt + 0.5 * nm);
+  }
+  return total.round();
 }
 
 double orc_contact_energy(int type, const double* xs12, const Params* prm) {

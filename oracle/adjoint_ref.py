@@ -43,18 +43,19 @@ def com_loss(states, body, target):
     return float(d @ d), 2.0 * d
 
 
-def backward(o, flat, prm, states, qb_T):
-    """dL/dq_0 and dL/dqdot_0 ([n, 12] each) from the adjoint qb_T of the final DOFs."""
+def backward(o, flat, prm, states, qb_T, model="full", qdb_T=None):
+    """dL/dq_0 and dL/dqdot_0 ([n, 12] each) from the adjoints qb_T (and qdb_T) of the final
+    DOFs (and velocities); model: the contact model of the forward ("full" or "reference")."""
     n = o.n
     dt = prm.dt
     free = np.repeat(np.asarray(flat["fixed"]) == 0, 12)
     Mdiag = np.concatenate([np.repeat(np.asarray(flat["mass"])[:, None], 3, axis=1),
                             np.repeat(np.asarray(flat["I0"])[:, None], 9, axis=1)], axis=1).ravel()
     qb = np.asarray(qb_T, dtype=np.float64).reshape(n * 12).copy()
-    qdb = np.zeros(n * 12)
+    qdb = np.zeros(n * 12) if qdb_T is None else np.asarray(qdb_T, dtype=np.float64).reshape(n * 12).copy()
     for t in range(len(states) - 2, -1, -1):
         S = states[t + 1]
-        H = o.full_hessian(S["A0"], S["p0"])
+        H = o.full_hessian(S["A0"], S["p0"], model=model)
         a = qb + qdb / dt
         lam = np.zeros(n * 12)
         lam[free] = np.linalg.solve(H[np.ix_(free, free)], a[free])

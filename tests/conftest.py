@@ -10,7 +10,6 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libabd_b200.so")
-    config.addinivalue_line("markers", "gpu_full: needs a GPU; full-size workload parity, selected explicitly")
 
 
 def has_gpu():
@@ -26,5 +25,5 @@ def pytest_collection_modifyitems(config, items):
         return
     skip = pytest.mark.skip(reason="no CUDA device")
     for item in items:
-        if "gpu" in item.keywords or "gpu_full" in item.keywords:
+        if "gpu" in item.keywords:
             item.add_marker(skip)

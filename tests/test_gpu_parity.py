@@ -49,10 +49,19 @@ def _sorted_rows(a):
     return a[np.lexsort(a.T[::-1])]
 
 
+def _c1_state(step):
+    """The oracle's state of the 64-icosphere scene after `step` steps (golden fixture)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c1_trajectory.npz"))
+    return {k: z[f"s{step}_{k}"] for k in ("A0", "p0", "Adot", "pdot", "dq")}
+
+
 SCENES = {
     "c0_contact": lambda: (scenes.make_config(0)[0], SimParams(), 3),
     "pile_ground": lambda: (scenes.small_pile(2, 2, seed=7)[0], SimParams(), 30),
     "c1_start": lambda: (scenes.make_config(1)[0], SimParams(), 0),
+    # 64 icospheres piled on the ground box after 200 steps: 600 PT / 2361 EE culled pairs
+    "c1_contact": lambda: (scenes.make_config(1)[0], SimParams(), _c1_state(200)),
     "pile_plane": lambda: (*scenes.small_pile(2, 2, seed=7, plane=True), 30),
 }
 
@@ -60,7 +69,10 @@ SCENES = {
 @pytest.fixture(scope="module", params=sorted(SCENES))
 def scene_state(request):
     bodies, prm, steps = SCENES[request.param]()
-    o, st = _scene_after(bodies, prm, steps)
+    if isinstance(steps, dict):
+        o, st = oracle.Oracle(scenes.flatten_bodies(bodies), prm), steps
+    else:
+        o, st = _scene_after(bodies, prm, steps)
     sim = _sim(bodies, prm)
     _set_state(sim, st)
     o.set_state(st["A0"], st["p0"], st["Adot"], st["pdot"], st["dq"])
@@ -94,7 +106,7 @@ def test_culling_sets_bitexact(scene_state, swept):
     np.testing.assert_array_equal(got["ij"], ref["ij"])  # ij is sorted by construction on both sides
     for k in ("pt", "ee", "vg"):
         np.testing.assert_array_equal(_sorted_rows(got[k]), _sorted_rows(ref[k]), err_msg=f"{name} {k}")
-    if name != "c1_start":
+    if name != "c1_start":  # the 64 spheres start more than dhat apart
         assert len(ref["pt"]) + len(ref["ee"]) + len(ref["vg"]) > 0
 
 
@@ -130,8 +142,11 @@ def test_gradient_hessian(scene_state):
     np.testing.assert_array_equal(got["diag"].cpu().numpy(), ref["diag"])
     np.testing.assert_array_equal(got["ij"].cpu().numpy(), ref["ij"])
     np.testing.assert_array_equal(got["off"].cpu().numpy(), ref["off"])
-    if name == "pile_ground":
+    # per-body contact flags of this pass (the reference's sim.highlight, abd.py:238)
+    np.testing.assert_array_equal(sim.highlight, o.highlight())
+    if name in ("pile_ground", "c1_contact"):
         assert ref["n_active"] > 0  # the bodies rest on the ground and on each other
+        assert o.highlight().any()
 
 
 def test_energy(scene_state):
@@ -210,18 +225,21 @@ def test_solve(scene_state, solver):
         o.set_params(prm0)
 
 
+@pytest.mark.parametrize("loop", ["device", "host"])
 @pytest.mark.parametrize("case,nsteps", [("c0", 200), ("pile", 60), ("plane", 60)])
-def test_step_parity(case, nsteps):
+def test_step_parity(case, nsteps, loop):
     """Whole time steps against the oracle, bit for bit: positions, velocities, the dq warm
     start and every iteration count, at every step (c0: the two-cube configuration for its
     200 steps; pile: 8 bodies on the ground box, 60 steps through landing and contact;
-    plane: the same bodies landing on the vertex-ground plane)."""
+    plane: the same bodies landing on the vertex-ground plane), with the Newton iterations
+    run as a device loop (the default) and driven from the host."""
+    import dataclasses
     if case == "c0":
         bodies, prm, _ = scenes.make_config(0)
     else:
         bodies, prm = scenes.small_pile(2, 2, seed=7, plane=case == "plane")
     o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
-    sim = _sim(bodies, prm)
+    sim = _sim(bodies, dataclasses.replace(prm, newton_loop=0 if loop == "device" else 1))
     active = 0
     try:
         for s in range(nsteps):

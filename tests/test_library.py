@@ -88,13 +88,13 @@ def test_create_rejects_malformed_scenes():
             for k in ("voff", "toff", "eoff", "x0", "tris", "edges", "mass", "I0", "fixed")}
     free = int(np.flatnonzero(base["fixed"] == 0)[0])
 
-    def create(mod, n=None):
+    def create(mod, n=None, prm=None):
         host = {k: v.copy() for k, v in base.items()}
         mod(host)
         hp = {k: v.ctypes.data_as(ctypes.c_void_p) for k, v in host.items()}
         desc = _lib.SceneDesc(len(bodies) if n is None else n, hp["voff"], hp["toff"], hp["eoff"], hp["x0"],
                               hp["tris"], hp["edges"], hp["mass"], hp["I0"], hp["fixed"])
-        cprm = SimParams().to_c()
+        cprm = (prm or SimParams()).to_c()
         h = ctypes.c_void_p()
         rc = L.abd_sim_create(ctypes.byref(desc), ctypes.byref(cprm), None, ctypes.byref(h))
         return rc, h.value
@@ -114,6 +114,14 @@ def test_create_rejects_malformed_scenes():
         (setter("mass", free, 0.0), None),                      # free body without mass
         (setter("I0", free, float("inf")), None),               # non-finite I0
     ]
+    def empty_body(h):  # body 0 loses its vertices (they go to body 1), keeps no primitives
+        h["voff"][1] = 0
+        h["toff"][1] = 0
+        h["eoff"][1] = 0
+
+    cases.append((empty_body, None))                            # a body without vertices
     for mod, n in cases:
         rc, h = create(mod, n)
         assert rc == _lib.ABD_ERR_INVALID and not h
+    rc, h = create(lambda h: None, prm=SimParams(min_capacity=-1))  # negative injected capacity
+    assert rc == _lib.ABD_ERR_INVALID and not h
