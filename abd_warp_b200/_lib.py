@@ -82,8 +82,12 @@ def load():
         "abd_energies_along": ([P, P, P, P, P, c_int, P], c_int),
         "abd_get_highlight": ([P, P], c_int),
         "abd_adjoint_step": ([P, P, P, P, P, P, P, P, P], c_int),
+        "abd_batch_create": ([c_int, P, P, P], c_int),
+        "abd_batch_destroy": ([P], c_int),
+        "abd_batch_step": ([P, P, P, P], c_int),
         "abd_take_status": ([P, P], c_int),
         "abd_status_string": ([c_int], ctypes.c_char_p),
+        "abd_error_detail": ([], ctypes.c_char_p),
         "abd_launch_count": ([P], c_longlong),
         "abd_profile": ([P, c_int], c_int),
         "abd_profile_read": ([P, P, P, P], c_int),
@@ -102,13 +106,16 @@ def exported_symbols():
     return ["abd_sim_create", "abd_sim_destroy", "abd_sim_set_params", "abd_sim_set_stream", "abd_sim_reset",
             "abd_sim_get_dq", "abd_sim_set_dq", "abd_sim_get_g", "abd_sim_sizes", "abd_step", "abd_update_mesh_vertex",
             "abd_collision_set", "abd_collision_set_dofs", "abd_export_lists", "abd_ipc_gh", "abd_export_system", "abd_solve",
-            "abd_compute_energy", "abd_ccd", "abd_energies_along", "abd_get_highlight", "abd_adjoint_step", "abd_take_status", "abd_status_string", "abd_launch_count",
+            "abd_compute_energy", "abd_ccd", "abd_energies_along", "abd_get_highlight", "abd_adjoint_step", "abd_batch_create", "abd_batch_destroy", "abd_batch_step", "abd_take_status", "abd_status_string", "abd_error_detail", "abd_launch_count",
             "abd_profile", "abd_profile_read"]
 
 
 def check(rc: int, what: str = ""):
     if rc != ABD_OK:
-        msg = load().abd_status_string(rc).decode()
+        L = load()
+        msg = L.abd_status_string(rc).decode()
+        if rc == ABD_ERR_CUDA:
+            msg += f" [{L.abd_error_detail().decode()}]"
         raise AbdError(f"{what}: {msg} (code {rc})")
 
 

@@ -13,6 +13,12 @@
 
 namespace abd {
 
+// The last failed CUDA call of this thread, as "file:line: error name: description"
+// (abd_error_detail returns it); note_error records one and returns e.
+cudaError_t note_error(cudaError_t e, const char* file, int line);
+const char* error_detail();
+#define ABD_NOTE(x) ::abd::note_error((x), __FILE__, __LINE__)
+
 // ---------------------------------------------------------------------------------------
 // status bits written by kernels into the simulator's device status word
 // ---------------------------------------------------------------------------------------
@@ -296,6 +302,10 @@ struct Sim {
   GraphSlot g_kadj;                // the adjoint's Krylov solve
   double* adj_x = nullptr;         // [12 n] the adjoint solve's unknown lambda
   cudaStream_t cap_stream3 = nullptr, cap_stream4 = nullptr;  // capture the loop's bodies
+  // side branches of a pass (the GH pass's clustering, the CCD pass's dot products): a stream
+  // joins the capture it forks from until that capture ends, so the device loop gives each
+  // capture scope its own (fork_a: the Newton body, fork_b: its IF body); null: cap_stream2
+  cudaStream_t fork_a = nullptr, fork_b = nullptr, side = nullptr;
   double* dq_save = nullptr;       // [12 n] dq at the start of a device-loop step (for a rerun)
   long long step_launch[3] = {0, 0, 0};  // kernels of a step graph: outside the loops, per
                                          // Newton iteration, per Krylov iteration

@@ -16,6 +16,7 @@
 
 #include "abd_common.cuh"
 #include "abd_exact.cuh"
+#include "abd_ipc_full.cuh"
 
 namespace abd {
 
@@ -151,6 +152,44 @@ __device__ inline bool contact_active(int type, const d3 xs[4], const abd_params
   *Gout = G;
   *d2out = d2;
   return d2 < P.d2hat && valid;
+}
+
+// ---------------------------------------------------------------------------------------
+// The full IPC contact model (abd_params.ipc_full; abd_ipc_full.cuh): the closest feature pair
+// is classified and the barrier acts on its squared distance, with the edge-edge mollifier.
+// The logarithm is the shared one, so the oracle's full mode (which evaluates the same header)
+// gets the same bits.
+// ---------------------------------------------------------------------------------------
+struct SharedLog {
+  __device__ double operator()(double v) const { return abd_log(v); }
+};
+__device__ inline void points12(const d3 xs[4], double x[12]) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    x[3 * k] = xs[k].x;
+    x[3 * k + 1] = xs[k].y;
+    x[3 * k + 2] = xs[k].z;
+  }
+}
+// the candidate's classified squared distance (and its type): the contact is active below dhat^2
+__device__ inline double full_d2(int kind, const d3 xs[4], int* type) {
+  double x[12];
+  points12(xs, x);
+  ipc::V3<double> v[4];
+  ipc::load(x, v);
+  const int ty = ipc::contact_type(kind, x);
+  *type = ty;
+  return kind == 0 ? ipc::pt_d2(ty, v) : ipc::ee_d2(ty, v);
+}
+// its energy (0 beyond dhat); r: the four points' rest positions (the mollifier's scale)
+__device__ inline double full_contact_energy(int kind, const d3 xs[4], const double r[12], const abd_params& P) {
+  int ty;
+  if (!(full_d2(kind, xs, &ty) < P.d2hat)) return 0.0;
+  double x[12];
+  points12(xs, x);
+  ipc::V3<double> v[4];
+  ipc::load(x, v);
+  return ipc::local_energy(kind, ty, v, kind == 1 ? ipc::ee_eps_x(r) : 0.0, P.d2hat, P.kappa, SharedLog());
 }
 
 // Factored barrier Hessian of one active contact:
@@ -405,8 +444,9 @@ __device__ inline void cols3(d3 p, d3 q, d3 r, double m[9]) {
   m[2] = r.x; m[5] = r.y; m[8] = r.z;
 }
 
-// pt_collision_time / ee_collision_time (ccd.py:133-186)
-__device__ inline double collision_time(int type, const d3 a0[4], const d3 a1[4]) {
+// pt_collision_time / ee_collision_time (ccd.py:133-186).  inclusive (the full contact model):
+// a coplanarity root also counts on the closed triangle / segments, within 1e-9
+__device__ inline double collision_time(int type, const d3 a0[4], const d3 a1[4], bool inclusive = false) {
   const int sel[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
   double coef[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -431,7 +471,12 @@ __device__ inline double collision_time(int type, const d3 a0[4], const d3 a1[4]
 #pragma unroll
     for (int k = 0; k < 4; ++k) pt[k] = a0[k] * (1.0 - root) + a1[k] * root;  // wp.lerp
     Geo G = geometry(type, pt[0], pt[1], pt[2], pt[3]);
-    ok = valid_root(type, G.beta, G.gamma);
+    if (inclusive) {
+      const double t = 1e-9, b = G.beta, c = type == 0 ? G.gamma : -G.gamma;
+      ok = b >= -t && c >= -t && (type == 0 ? b + c <= 1.0 + t : (b <= 1.0 + t && c <= 1.0 + t));
+    } else {
+      ok = valid_root(type, G.beta, G.gamma);
+    }
     if (ok) break;
   }
   return ok ? root : 1.0;

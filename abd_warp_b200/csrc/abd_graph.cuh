@@ -42,13 +42,13 @@ int run_graph(Sim& s, GraphSlot& g, uint64_t key, F&& issue) {
     const cudaStream_t work = s.stream;
     const long long l0 = s.launches;
     s.stream = s.cap_stream;
-    cudaError_t e = cudaStreamBeginCapture(s.cap_stream, cudaStreamCaptureModeThreadLocal);
+    cudaError_t e = ABD_NOTE(cudaStreamBeginCapture(s.cap_stream, cudaStreamCaptureModeThreadLocal));
     int r = e == cudaSuccess ? issue() : ABD_ERR_CUDA;
     cudaGraph_t graph = nullptr;
-    const cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(s.cap_stream, &graph) : e;
+    const cudaError_t e2 = e == cudaSuccess ? ABD_NOTE(cudaStreamEndCapture(s.cap_stream, &graph)) : e;
     s.stream = work;
     if (r == ABD_OK && e2 != cudaSuccess) r = ABD_ERR_CUDA;
-    if (r == ABD_OK && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) r = ABD_ERR_CUDA;
+    if (r == ABD_OK && ABD_NOTE(cudaGraphInstantiate(&g.exec, graph, 0)) != cudaSuccess) r = ABD_ERR_CUDA;
     if (graph) cudaGraphDestroy(graph);
     g.nlaunch = s.launches - l0;
     s.launches = l0;
@@ -59,7 +59,7 @@ int run_graph(Sim& s, GraphSlot& g, uint64_t key, F&& issue) {
     }
     g.key = key;
   }
-  if (cudaGraphLaunch(g.exec, s.stream) != cudaSuccess) return ABD_ERR_CUDA;
+  if (ABD_NOTE(cudaGraphLaunch(g.exec, s.stream)) != cudaSuccess) return ABD_ERR_CUDA;
   s.launches += g.nlaunch;
   return ABD_OK;
 }

@@ -143,7 +143,15 @@ __global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv) {
       } else if (!overlap(edge_box_at(xs[0], xs[1], dhh), edge_box_at(xs[2], xs[3], dhh))) {
         continue;  // (the edge boxes lie inside their body boxes)
       }
-      const double e = contact_energy(type, xs, a.prm);
+      double e;
+      if (a.prm.ipc_full) {  // the full model; its mollifier's scale from the rest positions
+        double r[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) r[k] = __ldg(&a.x0[3 * ids[k / 3] + k % 3]);
+        e = full_contact_energy(type, xs, r, a.prm);
+      } else {
+        e = contact_energy(type, xs, a.prm);
+      }
       if (e != 0.0) xs_add_atomic(&acc, e);
     }
   } else if (bx < G + Gv) {

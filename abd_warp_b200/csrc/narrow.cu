@@ -442,19 +442,24 @@ __global__ void k_contact_scatter(int cap_contacts, const int4* __restrict__ in,
 // evaluations of the contact's energy per warp, one per Hessian entry, then mapped to the two
 // bodies' affine DOFs.
 constexpr int PT_THREADS = 256;  // threads of the pair assembly (a warp per contact)
-struct ExactLog {  // the hyper-dual log's value (its derivatives are 1 / x)
-  __device__ double operator()(double v) const { return log(v); }
-};
 // One contact's exact terms (EXACT pair assembly), by its warp: the local Hessian and gradient
 // in the four points' coordinates into h [156], then the 456 affine values added to xred.
 // Vertices 0 .. nI-1 are the first group (the point; edge a), the rest the second; the group
 // of side 0 (the pair's first body) is the first unless swapped.
+// full: the contact's classified feature pair and the edge-edge mollifier (the full model;
+// else the reference's interior types); project: the PSD projection of the local Hessian
+// (Jacobi, by the warp's first lane) before the map.
 __device__ void exact_contact_terms(const NarrowArgs& a, int type, int swap, const int ids[4], double* h,
-                                    XSum* xred) {
+                                    XSum* xred, bool full, bool project) {
   const int lane = threadIdx.x & 31;
-  double x[12];
+  double x[12], rr[12];
 #pragma unroll
-  for (int k = 0; k < 12; ++k) x[k] = a.y0[3 * ids[k / 3] + k % 3];
+  for (int k = 0; k < 12; ++k) {
+    x[k] = a.y0[3 * ids[k / 3] + k % 3];
+    rr[k] = __ldg(&a.x0[3 * ids[k / 3] + k % 3]);
+  }
+  const int ftype = full ? ipc::contact_type(type, x) : 0;
+  const double ex = full && type == 1 ? ipc::ee_eps_x(rr) : 0.0;
   for (int e = lane; e < 78; e += 32) {  // the upper triangle, row by row
     int i = 0, rem = e;
     while (rem >= 12 - i) {
@@ -471,12 +476,13 @@ __device__ void exact_contact_terms(const NarrowArgs& a, int type, int swap, con
       }
       v[k] = {c[0], c[1], c[2]};
     }
-    // the reference's interior types, no mollifier
-    const ipc::HD en = ipc::local_energy(type, 0, v, 0.0, a.prm.d2hat, a.prm.kappa, ExactLog());
+    const ipc::HD en = ipc::local_energy(type, ftype, v, ex, a.prm.d2hat, a.prm.kappa, SharedLog());
     h[12 * i + j] = en.ab;
     h[12 * j + i] = en.ab;
     if (i == j) h[144 + i] = en.a;
   }
+  __syncwarp();
+  if (project && lane == 0) ipc::project_psd12(h);
   __syncwarp();
   const int nI = type == 0 ? 1 : 2;
   auto side = [&](int v) { return (v < nI ? 0 : 1) ^ swap; };
@@ -507,8 +513,14 @@ constexpr int kExactLocal = 156;  // EXACT: a warp's local Hessian (144) and gra
 // the exact pair assembly's shared memory: the sums and every warp's local Hessian (49 KB: the
 // kernel is opted in once, at creation, since its launches may be captured)
 constexpr int kExactSmem = NOUT * (int)sizeof(XSum) + PT_WARPS * kExactLocal * (int)sizeof(double);
-template <bool EXACT>
+// MODE: kAsmRef the reference's model (5 rank-one terms); kAsmExact the adjoint's exact Hessian
+// of the reference's model; kAsmFull the full IPC model, its exact local Hessian projected onto
+// the PSD cone (the Newton system with ipc_full); kAsmFullExact the adjoint's exact Hessian of
+// the full model
+enum { kAsmRef = 0, kAsmExact = 1, kAsmFull = 2, kAsmFullExact = 3 };
+template <int MODE>
 __global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
+  constexpr bool EXACT = MODE != kAsmRef;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
   const int npairs = a.dstat[DS_NPAIRS];
@@ -531,7 +543,7 @@ __global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
       int ids[4];
       cand_vertices(a, type, rec.z, rec.w, ids);
       if constexpr (EXACT) {
-        exact_contact_terms(a, type, swap, ids, hloc, xred);
+        exact_contact_terms(a, type, swap, ids, hloc, xred, MODE >= kAsmFull, MODE == kAsmFull);
         continue;
       }
       d3 xs[4];
@@ -625,6 +637,16 @@ __device__ inline double vg_toi(const abd_params& P, const double* y0, const dou
     tt = d0 / (d0 - d1);
   }
   return tt;
+}
+
+// One candidate's barrier energy at positions xs: the reference's model (ipcsk/energy.py:9-48)
+// or, with ipc_full, the full model (its rest positions scale the edge-edge mollifier)
+__device__ inline double candidate_energy(const NarrowArgs& a, int type, const int ids[4], const d3 xs[4]) {
+  if (!a.prm.ipc_full) return contact_energy(type, xs, a.prm);
+  double r[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) r[k] = __ldg(&a.x0[3 * ids[k / 3] + k % 3]);
+  return full_contact_energy(type, xs, r, a.prm);
 }
 
 // minimum of non-negative doubles by atomicMax on the complemented bit patterns (0 = none)
@@ -853,7 +875,7 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
           d3 xs[4];
           cand_vertices(a, type, pa, pb, ids);
           fetch(a.y0, ids, xs);
-          const double e = contact_energy(type, xs, a.prm);
+          const double e = candidate_energy(a, type, ids, xs);
           if (e != 0.0) xs_add_atomic(&xe, e);
         }
       };
@@ -986,7 +1008,7 @@ __global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
     d3 x0[4], x1[4];
     fetch(a.y0, ids, x0);
     fetch(a.y1, ids, x1);
-    const double t = collision_time(c.x, x0, x1);
+    const double t = collision_time(c.x, x0, x1, a.prm.ipc_full != 0);
     if (t < 1.0) toi_min(a.toi_key, t);
   }
 }
@@ -1070,12 +1092,13 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
     cand_vertices(a, type, c.z, c.w, ids);
     fetch(a.y0, ids, xs);
     if (with_energy) {
-      const double e = contact_energy(type, xs, a.prm);
+      const double e = candidate_energy(a, type, ids, xs);
       if (e != 0.0) xs_add(en, e);
     }
     Geo G;
     double d2;
-    if (contact_active(type, xs, a.prm, &G, &d2)) {
+    int fty;
+    if (a.prm.ipc_full ? full_d2(type, xs, &fty) < a.prm.d2hat : contact_active(type, xs, a.prm, &G, &d2)) {
       const int pos = append_slot(&a.dstat[DS_NCONTACT]);
       if (pos < a.cap_contacts) a.contacts[pos] = c;
       else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
@@ -1510,10 +1533,14 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
       static_assert(smem + sizeof(double) * PT_WARPS * 5 * 24 + 256 <= 48 * 1024, "pair assembly shared memory");
       const int grid = s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148;
-      if (s.exact_hessian)
-        k_pair_assemble<true><<<grid, PT_THREADS, kExactSmem, s.stream>>>(a);
+      if (s.exact_hessian && s.prm.ipc_full)
+        k_pair_assemble<kAsmFullExact><<<grid, PT_THREADS, kExactSmem, s.stream>>>(a);
+      else if (s.exact_hessian)
+        k_pair_assemble<kAsmExact><<<grid, PT_THREADS, kExactSmem, s.stream>>>(a);
+      else if (s.prm.ipc_full)
+        k_pair_assemble<kAsmFull><<<grid, PT_THREADS, kExactSmem, s.stream>>>(a);
       else
-        k_pair_assemble<false><<<grid, PT_THREADS, smem, s.stream>>>(a);
+        k_pair_assemble<kAsmRef><<<grid, PT_THREADS, smem, s.stream>>>(a);
       s.launches += 3;
     }
   } else {
@@ -1526,7 +1553,12 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
 
 cudaError_t prepare_narrow(Sim& s) {
   (void)s;
-  return cudaFuncSetAttribute(k_pair_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExactSmem);
+  cudaError_t e = cudaFuncSetAttribute(k_pair_assemble<kAsmExact>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExactSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pair_assemble<kAsmFull>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExactSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pair_assemble<kAsmFullExact>, cudaFuncAttributeMaxDynamicSharedMemorySize, kExactSmem);
+  return e;
 }
 
 cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode) {

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -25,13 +26,47 @@ struct abd_sim {
   abd::Sim s;
 };
 
+// Independent scenes stepped together: one CUDA graph holds every scene's device-loop step as
+// a branch of its own (see abd_batch_step)
+struct abd_batch {
+  std::vector<abd_sim*> sims;
+  cudaStream_t stream = nullptr;      // the stream the steps are launched on
+  cudaStream_t cap = nullptr;         // captures the graph
+  std::vector<cudaStream_t> branch;   // one per scene, for the capture
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t key = 0;
+  std::vector<long long> top;         // kernels of each branch outside its loops
+};
+
+namespace abd {
+
+namespace {
+thread_local char g_error_detail[256] = "";
+}
+
+const char* error_detail() { return g_error_detail; }
+
+cudaError_t note_error(cudaError_t e, const char* file, int line) {
+  if (e != cudaSuccess) {
+    const char* base = std::strrchr(file, '/');
+    std::snprintf(g_error_detail, sizeof(g_error_detail), "%s:%d: %s: %s", base ? base + 1 : file, line,
+                  cudaGetErrorName(e), cudaGetErrorString(e));
+    (void)cudaGetLastError();  // the caller gets the error here; it must not reach later calls
+  }
+  return e;
+}
+
+}  // namespace abd
+
 namespace {
 
 using abd::Sim;
 
-#define CK(x)                                  \
-  do {                                         \
-    if ((x) != cudaSuccess) return ABD_ERR_CUDA; \
+#define CK(x)                                       \
+  do {                                              \
+    if (ABD_NOTE(x) != cudaSuccess) return ABD_ERR_CUDA; \
   } while (0)
 
 // The exact accumulator rounded to FP64 on the host (the same rounding as the device's).
@@ -253,7 +288,8 @@ int overflow(Sim& s) {
   return kRerun;
 }
 
-constexpr int kMaxReruns = 6;
+constexpr int kMaxReruns = 6;       // per pass of the host loop
+constexpr int kMaxStepReruns = 48;  // per step of the device loop
 
 uint64_t states_key(const Sim& s, const abd_states& st) {
   abd::KeyHash k;
@@ -433,10 +469,11 @@ int gh_issue(abd_sim* h, const abd_states& st, const double* A, const double* p,
   CK(abd::gh_superset_check(s, &st, sup_mode));
   int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
   if (r) return r;
+  const cudaStream_t side = s.side ? s.side : s.cap_stream2;
   CK(cudaEventRecord(s.fork_ev[0], s.stream));
-  CK(cudaStreamWaitEvent(s.cap_stream2, s.fork_ev[0], 0));
-  CK(abd::cluster_tables(s, s.cap_stream2));
-  CK(cudaEventRecord(s.fork_ev[1], s.cap_stream2));
+  CK(cudaStreamWaitEvent(side, s.fork_ev[0], 0));
+  CK(abd::cluster_tables(s, side));
+  CK(cudaEventRecord(s.fork_ev[1], side));
   CK(abd::body_gh(s, st, A, p, s.x));
   CK(cudaStreamWaitEvent(s.stream, s.fork_ev[1], 0));
   return ABD_OK;
@@ -497,6 +534,8 @@ int take_status(abd_sim* h) {
 }  // namespace
 
 extern "C" {
+
+const char* abd_error_detail(void) { return abd::error_detail(); }
 
 const char* abd_status_string(int code) {
   switch (code) {
@@ -748,6 +787,8 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream2, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream3, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream4, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.fork_a, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.fork_b, cudaStreamNonBlocking);
   for (cudaEvent_t* ev : {&s.fork_ev[0], &s.fork_ev[1]})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   ok(dalloc(&s.row_cnt, n));
@@ -819,7 +860,7 @@ int abd_sim_destroy(abd_sim* h) {
     if (q) cudaFree(q);
   for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev, &s.g_step, &s.g_kadj})
     if (g->exec) cudaGraphExecDestroy(g->exec);
-  for (cudaStream_t q : {s.cap_stream, s.cap_stream2, s.cap_stream3, s.cap_stream4})
+  for (cudaStream_t q : {s.cap_stream, s.cap_stream2, s.cap_stream3, s.cap_stream4, s.fork_a, s.fork_b})
     if (q) cudaStreamDestroy(q);
   for (cudaEvent_t ev : {s.prof_ev[0], s.prof_ev[1], s.fork_ev[0], s.fork_ev[1]})
     if (ev) cudaEventDestroy(ev);
@@ -1185,21 +1226,20 @@ int capture_body(Sim& s, cudaGraph_t body, cudaStream_t bs, F&& issue) {
   return e == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
-// The step with the Newton iterations as a device loop: one graph launch and one copy to the
-// host per step (newton.cu describes the loop)
-int step_device(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
+// Enqueues a step with the Newton iterations as a device loop on s.stream, which must be
+// capturing (newton.cu describes the loop); ends with the copy of the mailbox to the host
+int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
   Sim& s = h->s;
-  const abd_states& st = *stp;
   const size_t nA = sizeof(double) * 9 * s.n, np = sizeof(double) * 3 * s.n, nq = sizeof(double) * 12 * s.n;
   auto dots = [&]() -> int {  // dq.g, g.g on a branch beside the CCD pass's culling
     CK(cudaEventRecord(s.fork_ev[0], s.stream));
-    CK(cudaStreamWaitEvent(s.cap_stream2, s.fork_ev[0], 0));
-    CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots, s.cap_stream2));
-    CK(cudaEventRecord(s.fork_ev[1], s.cap_stream2));
+    CK(cudaStreamWaitEvent(s.fork_b, s.fork_ev[0], 0));
+    CK(abd::dots(s, s.dq, s.g, s.g, s.g, s.box->dots, s.fork_b));
+    CK(cudaEventRecord(s.fork_ev[1], s.fork_b));
     s.fork_open = true;
     return ABD_OK;
   };
-  auto iteration_tail = [&]() -> int {  // after a GH pass without overflow
+  auto iteration_tail = [&]() -> int {  // after a GH pass without overflow (the IF body)
     CK(abd::after_gh(s));
     if (int r = abd::cluster_inverse(s)) return r;
     if (int r = abd::krylov_issue(s, s.dq)) return r;
@@ -1216,91 +1256,89 @@ int step_device(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info
     CK(cudaMemcpyAsync(st.pk, st.p, np, cudaMemcpyDeviceToDevice, s.stream));
     return ABD_OK;
   };
-  auto issue = [&]() -> int {
-    const cudaStream_t top = s.stream;
-    // q <- q0 (abd.py:124-128); the warm start kept for a rerun
-    CK(cudaMemcpyAsync(st.A, st.A0, nA, cudaMemcpyDeviceToDevice, top));
-    CK(cudaMemcpyAsync(st.p, st.p0, np, cudaMemcpyDeviceToDevice, top));
-    CK(cudaMemcpyAsync(st.Ak, st.A0, nA, cudaMemcpyDeviceToDevice, top));
-    CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, top));
-    CK(cudaMemcpyAsync(s.dq_save, s.dq, nq, cudaMemcpyDeviceToDevice, top));
-    cudaGraphConditionalHandle hn;
-    if (int r = make_handle(top, &hn)) return r;
-    CK(abd::step_begin(s, hn));
-    cudaGraph_t nbody = nullptr;
-    if (int r = add_conditional(top, hn, cudaGraphCondTypeWhile, &nbody)) return r;
-    const long long l0 = s.launches;
-    int r = capture_body(s, nbody, s.cap_stream3, [&]() -> int {
-      if (int q = gh_issue(h, st, st.A, st.p, 3)) return q;
-      cudaGraphConditionalHandle hi;
-      if (int q = make_handle(s.stream, &hi)) return q;
-      CK(abd::gate_no_overflow(s, hi));
-      cudaGraph_t ibody = nullptr;
-      if (int q = add_conditional(s.stream, hi, cudaGraphCondTypeIf, &ibody)) return q;
-      if (int q = capture_body(s, ibody, s.cap_stream4, iteration_tail)) return q;
-      CK(abd::newton_end(s, hn));
-      return ABD_OK;
-    });
-    if (r) return r;
-    s.step_launch[1] = s.launches - l0;
-    CK(abd::finish_step_dev(s, st, x_view));
-    CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, top));
+  const cudaStream_t top = s.stream;
+  // q <- q0 (abd.py:124-128); the warm start kept for a rerun
+  CK(cudaMemcpyAsync(st.A, st.A0, nA, cudaMemcpyDeviceToDevice, top));
+  CK(cudaMemcpyAsync(st.p, st.p0, np, cudaMemcpyDeviceToDevice, top));
+  CK(cudaMemcpyAsync(st.Ak, st.A0, nA, cudaMemcpyDeviceToDevice, top));
+  CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, top));
+  CK(cudaMemcpyAsync(s.dq_save, s.dq, nq, cudaMemcpyDeviceToDevice, top));
+  cudaGraphConditionalHandle hn;
+  if (int r = make_handle(top, &hn)) return r;
+  CK(abd::step_begin(s, hn));
+  cudaGraph_t nbody = nullptr;
+  if (int r = add_conditional(top, hn, cudaGraphCondTypeWhile, &nbody)) return r;
+  const long long l0 = s.launches;
+  int r = capture_body(s, nbody, s.cap_stream3, [&]() -> int {
+    s.side = s.fork_a;
+    const int q0 = gh_issue(h, st, st.A, st.p, 3);
+    s.side = nullptr;
+    if (q0) return q0;
+    cudaGraphConditionalHandle hi;
+    if (int q = make_handle(s.stream, &hi)) return q;
+    CK(abd::gate_no_overflow(s, hi));
+    cudaGraph_t ibody = nullptr;
+    if (int q = add_conditional(s.stream, hi, cudaGraphCondTypeIf, &ibody)) return q;
+    if (int q = capture_body(s, ibody, s.cap_stream4, iteration_tail)) return q;
+    CK(abd::newton_end(s, hn));
     return ABD_OK;
-  };
+  });
+  if (r) return r;
+  s.step_launch[1] = s.launches - l0;
+  CK(abd::finish_step_dev(s, st, x_view));
+  CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, top));
+  return ABD_OK;
+}
+
+// The key of a device-loop step's graph: everything its captured kernels read by value
+uint64_t step_key(const Sim& s, const abd_states& st, const double* x_view) {
   abd::KeyHash k;
   k.add(states_key(s, st)).add(x_view).add(s.cap_pairs).add(s.cap_adj).add(s.cap_contacts).add(s.cap_act);
   k.add(s.ij).add(s.adj_col).add(s.adj_pair).add(s.contacts).add(s.contacts_by_pair).add(s.act_pairs);
   k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active).add(s.q_last).add(s.dint);
   k.add(s.cap_ccd).add(s.ccd_cand).add(s.cap_ecand).add(s.ecand).add(s.prof_on).add(s.cl_inv).add(s.dq_save);
-  s.prof_events = s.prof_on ? -1 : 0;  // kernel timing by the global timer (no events in the loop)
-  s.gh_energy = 1;                     // the GH pass sums the energy at the first iteration only
-  s.energy_gate = &s.box->step.it;
-  int r = ABD_OK;
-  for (int tries = 0;; ++tries) {
-    const long long launches0 = s.launches;
-    r = abd::run_graph(s, s.g_step, k.h, issue);
-    if (r) break;
-    s.launches = launches0 + s.g_step.nlaunch - s.step_launch[1];  // counted below
-    if (cudaStreamSynchronize(s.stream) != cudaSuccess) {
-      r = ABD_ERR_CUDA;
-      break;
-    }
-    std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
-    const abd::StepDev& S = s.hbox->step;
-    s.launches += (long long)S.it * s.step_launch[1] + (long long)(S.lin + S.it) * s.step_launch[2];
-    s.n_pairs = s.hstat[abd::DS_NPAIRS];
-    s.n_adj = s.hstat[abd::DS_NADJ];
-    const int bits = s.hstat[abd::DS_STATUS];
-    if (!(bits & abd::kRerunMask)) break;
-    // a list overflowed or a line search needs more trials: the states are as they were;
-    // restore the warm start, drop the kept candidates and grow what was short
-    if (cudaMemcpyAsync(s.dq, s.dq_save, nq, cudaMemcpyDeviceToDevice, s.stream) != cudaSuccess) {
-      r = ABD_ERR_CUDA;
-      break;
-    }
-    if ((r = drop_superset(h))) break;
-    if ((r = overflow(s)) > 0) break;
-    if (bits & abd::ST_LS_MORE) {  // finished on the host
-      s.hstat[abd::DS_STATUS] &= ~abd::ST_LS_MORE;
-      if (cudaMemcpyAsync(s.dstat + abd::DS_STATUS, &s.hstat[abd::DS_STATUS], sizeof(int), cudaMemcpyHostToDevice,
-                          s.stream) != cudaSuccess ||
-          cudaStreamSynchronize(s.stream) != cudaSuccess) {
-        r = ABD_ERR_CUDA;
-        break;
-      }
-      s.energy_gate = nullptr;
-      s.prof_events = 0;
-      return step_host(h, stp, x_view, info);
-    }
-    r = ABD_OK;
-    if (tries >= kMaxReruns) {
-      r = ABD_ERR_OVERFLOW;
-      break;
-    }
+  return k.h;
+}
+
+// The simulator's set-up around a device-loop step's capture and replay
+void step_modes(Sim& s, bool on) {
+  s.prof_events = on && s.prof_on ? -1 : 0;  // kernel timing by the global timer (no events)
+  s.gh_energy = on ? 1 : 0;                  // the GH pass sums the energy at the first iteration
+  s.energy_gate = on ? &s.box->step.it : nullptr;
+}
+
+constexpr int kHostFinish = -2;
+
+// After a device-loop step's graph ran (the mailbox on the host, the stream synchronised):
+// 0 when the step is complete; kRerun when a list overflowed (the warm start restored, the
+// kept candidates dropped, the list grown: run the step again); kHostFinish when a line search
+// needed more trials (likewise restored: the host loop finishes the step); or an ABD error.
+int step_outcome(abd_sim* h) {
+  Sim& s = h->s;
+  std::memcpy(s.hstat, s.hbox->dstat, sizeof(int) * abd::DS_NSLOTS);
+  const abd::StepDev& S = s.hbox->step;
+  s.launches += (long long)S.it * s.step_launch[1] + (long long)(S.lin + S.it) * s.step_launch[2];
+  s.n_pairs = s.hstat[abd::DS_NPAIRS];
+  s.n_adj = s.hstat[abd::DS_NADJ];
+  const int bits = s.hstat[abd::DS_STATUS];
+  if (!(bits & abd::kRerunMask)) return 0;
+  CK(cudaMemcpyAsync(s.dq, s.dq_save, sizeof(double) * 12 * s.n, cudaMemcpyDeviceToDevice, s.stream));
+  if (int r = drop_superset(h)) return r;
+  const int g = overflow(s);  // grows what was short; clears the overflow bits on the device
+  if (g > 0) return g;
+  if (bits & abd::ST_LS_MORE) {
+    s.hstat[abd::DS_STATUS] &= ~abd::ST_LS_MORE;
+    CK(cudaMemcpyAsync(s.dstat + abd::DS_STATUS, &s.hstat[abd::DS_STATUS], sizeof(int), cudaMemcpyHostToDevice,
+                       s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+    return kHostFinish;
   }
-  s.energy_gate = nullptr;
-  s.prof_events = 0;
-  if (r) return r;
+  return kRerun;
+}
+
+// The step info of a completed device-loop step, from the mailbox; the step's status taken
+int step_info(abd_sim* h, abd_step_info* info) {
+  Sim& s = h->s;
   const abd::StepDev& S = s.hbox->step;
   if (s.prof_on) {
     s.prof_ms += 1e-6 * (double)S.prof_ns;
@@ -1322,6 +1360,31 @@ int step_device(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info
   inf.status = take_status(h);
   if (info) *info = inf;
   return (inf.status & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
+}
+
+// The step with the Newton iterations as a device loop: one graph launch and one copy to the
+// host per step, a rerun from the step's start when a list overflowed
+int step_device(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {
+  Sim& s = h->s;
+  const abd_states& st = *stp;
+  int r = ABD_OK;
+  // a rerun restarts the whole step and meets the next short list, so a step gets the reruns of
+  // all its passes; each recaptures (the buffers and capacities are in the key)
+  for (int tries = 0;; ++tries) {
+    step_modes(s, true);
+    const long long launches0 = s.launches;
+    r = abd::run_graph(s, s.g_step, step_key(s, st, x_view), [&]() { return step_issue(h, st, x_view); });
+    step_modes(s, false);
+    if (r) return r;
+    s.launches = launches0 + s.g_step.nlaunch - s.step_launch[1];  // the loops: step_outcome
+    CK(cudaStreamSynchronize(s.stream));
+    r = step_outcome(h);
+    if (r == 0) break;
+    if (r == kHostFinish) return step_host(h, stp, x_view, info);
+    if (r > 0) return r;
+    if (tries >= kMaxStepReruns) return ABD_ERR_OVERFLOW;
+  }
+  return step_info(h, info);
 }
 
 }  // namespace
@@ -1355,6 +1418,105 @@ int abd_adjoint_step(abd_sim* h, const abd_states* st, const double* A, const do
   CK(cudaStreamSynchronize(s.stream));
   const int bits = take_status(h);
   return (bits & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
+}
+
+int abd_batch_create(int n, abd_sim* const* sims, void* stream, abd_batch** out) {
+  if (n <= 0 || !sims || !out) return ABD_ERR_INVALID;
+  for (int i = 0; i < n; ++i)
+    if (!sims[i]) return ABD_ERR_INVALID;
+  abd_batch* b = new (std::nothrow) abd_batch();
+  if (!b) return ABD_ERR_OVERFLOW;
+  b->sims.assign(sims, sims + n);
+  b->stream = (cudaStream_t)stream;
+  b->branch.assign(n, nullptr);
+  b->join.assign(n, nullptr);
+  b->top.assign(n, 0);
+  cudaError_t e = ABD_NOTE(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  if (e == cudaSuccess) e = ABD_NOTE(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    e = ABD_NOTE(cudaStreamCreateWithFlags(&b->branch[i], cudaStreamNonBlocking));
+    if (e == cudaSuccess) e = ABD_NOTE(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
+  }
+  if (e != cudaSuccess) {
+    abd_batch_destroy(b);
+    return ABD_ERR_CUDA;
+  }
+  *out = b;
+  return ABD_OK;
+}
+
+int abd_batch_destroy(abd_batch* b) {
+  if (!b) return ABD_ERR_INVALID;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (cudaStream_t q : b->branch)
+    if (q) cudaStreamDestroy(q);
+  for (cudaEvent_t ev : b->join)
+    if (ev) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  delete b;
+  return ABD_OK;
+}
+
+int abd_batch_step(abd_batch* b, const abd_states* st, double* const* x_view, abd_step_info* info) {
+  if (!b || !st) return ABD_ERR_INVALID;
+  const int n = (int)b->sims.size();
+  for (abd_sim* h : b->sims)  // the device loop takes every step (one batch of trials)
+    if (!(h->s.prm.alpha_min > 0x1p-15)) return ABD_ERR_INVALID;
+  abd::KeyHash k;
+  k.add(n);
+  for (int i = 0; i < n; ++i) k.add(step_key(b->sims[i]->s, st[i], x_view ? x_view[i] : nullptr)).add(b->sims[i]);
+  if (!b->exec || b->key != k.h) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    CK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    int r = ABD_NOTE(cudaEventRecord(b->fork, b->cap)) == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+    for (int i = 0; i < n && r == ABD_OK; ++i) {
+      Sim& s = b->sims[i]->s;
+      if (ABD_NOTE(cudaStreamWaitEvent(b->branch[i], b->fork, 0)) != cudaSuccess) {
+        r = ABD_ERR_CUDA;
+        break;
+      }
+      const cudaStream_t saved = s.stream;
+      const long long l0 = s.launches;
+      s.stream = b->branch[i];
+      step_modes(s, true);
+      r = step_issue(b->sims[i], st[i], x_view ? x_view[i] : nullptr);
+      step_modes(s, false);
+      s.stream = saved;
+      b->top[i] = s.launches - l0 - s.step_launch[1];
+      s.launches = l0;
+      if (r == ABD_OK && (ABD_NOTE(cudaEventRecord(b->join[i], b->branch[i])) != cudaSuccess ||
+                          ABD_NOTE(cudaStreamWaitEvent(b->cap, b->join[i], 0)) != cudaSuccess))
+        r = ABD_ERR_CUDA;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = ABD_NOTE(cudaStreamEndCapture(b->cap, &graph));
+    if (r == ABD_OK && e2 != cudaSuccess) r = ABD_ERR_CUDA;
+    if (r == ABD_OK && ABD_NOTE(cudaGraphInstantiate(&b->exec, graph, 0)) != cudaSuccess) r = ABD_ERR_CUDA;
+    if (graph) cudaGraphDestroy(graph);
+    if (r != ABD_OK) {
+      if (b->exec) cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+      return r;
+    }
+    b->key = k.h;
+  }
+  CK(cudaGraphLaunch(b->exec, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  int first_error = ABD_OK;
+  for (int i = 0; i < n; ++i) {
+    abd_sim* h = b->sims[i];
+    h->s.launches += b->top[i];
+    int r = step_outcome(h);
+    abd_step_info* inf = info ? info + i : nullptr;
+    if (r == 0) r = step_info(h, inf);
+    else if (r == kRerun) r = step_device(h, &st[i], x_view ? x_view[i] : nullptr, inf);  // alone, grown
+    else if (r == kHostFinish) r = step_host(h, &st[i], x_view ? x_view[i] : nullptr, inf);
+    if (r != ABD_OK && first_error == ABD_OK) first_error = r;
+  }
+  return first_error;
 }
 
 int abd_step(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* info) {

@@ -738,13 +738,13 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
     return ABD_ERR_CUDA;
   // the loop's handle first: k_solver_init sets its value
   cudaGraphConditionalHandle h;
-  if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) return ABD_ERR_CUDA;
+  if (ABD_NOTE(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return ABD_ERR_CUDA;
   // b^T M^-1 b sets the threshold
   k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
   k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
                                          pcg ? nullptr : s.v);
-  if (cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st) ||
-      cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st))
+  if (ABD_NOTE(cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st)) ||
+      ABD_NOTE(cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st)))
     return ABD_ERR_CUDA;
   k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x, h);
   // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
@@ -762,12 +762,12 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   np.conditional.type = cudaGraphCondTypeWhile;
   np.conditional.size = 1;
   cudaGraphNode_t loop;
-  if (cudaGraphAddNode(&loop, graph, deps, ndeps, &np) != cudaSuccess) return ABD_ERR_CUDA;
+  if (ABD_NOTE(cudaGraphAddNode(&loop, graph, deps, ndeps, &np)) != cudaSuccess) return ABD_ERR_CUDA;
   cudaGraph_t body = np.conditional.phGraph_out[0];
-  if (cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+  if (ABD_NOTE(cudaStreamUpdateCaptureDependencies(st, &loop, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
     return ABD_ERR_CUDA;
   cudaStream_t bs = s.cap_stream2;
-  if (cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+  if (ABD_NOTE(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return ABD_ERR_CUDA;
   if (pcg) {
     k_pcg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v);
@@ -788,9 +788,9 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
   if (per_iter_out) *per_iter_out = pcg ? 5 : 10;
   cudaGraph_t body_out = nullptr;
-  const cudaError_t eb = cudaGetLastError();
+  const cudaError_t eb = ABD_NOTE(cudaGetLastError());
   if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
-  return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+  return ABD_NOTE(cudaGetLastError()) == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
 // Solves H x = g (x: warm start, overwritten).  Returns an ABD_* status.  One replayed graph

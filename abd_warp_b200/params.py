@@ -53,6 +53,9 @@ class SimParams:
     refine_tol: float = 1e-4         # oracle mixed precision: the FP32 inner solve's relative tolerance
     newton_loop: int = 0             # 0: the step's Newton iterations run as a device loop (one graph
                                      # launch per step); 1: the host drives them (same results)
+    ipc_full: int = 0                # 1: the full IPC contact model (closest-feature types, edge-edge
+                                     # mollifier, per-contact PSD projection, inclusive CCD); 0: the
+                                     # reference's interior-only model
     min_capacity: int = 0            # > 0: every list of the simulator starts this small and the
                                      # traversal frontier holds at most this many nodes (tests force
                                      # the grow-and-rerun paths and the depth-first fallback with it)
@@ -91,6 +94,7 @@ class SimParams:
         c.cluster_max = self.cluster_max
         c.min_capacity = self.min_capacity
         c.newton_loop = self.newton_loop
+        c.ipc_full = self.ipc_full
         return c
 
     def as_dict(self):
@@ -110,4 +114,5 @@ class CParams(ctypes.Structure):
         ("enable_vg", ctypes.c_int), ("solver", ctypes.c_int), ("cg_max_iter", ctypes.c_int),
         ("precision", ctypes.c_int), ("contact_psd", ctypes.c_int), ("precond", ctypes.c_int),
         ("cluster_max", ctypes.c_int), ("min_capacity", ctypes.c_int), ("newton_loop", ctypes.c_int),
+        ("ipc_full", ctypes.c_int),
     ]

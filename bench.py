@@ -24,6 +24,16 @@ its first CTA and the end of its last, on the stream it runs on.  The data it mo
 (algorithmic bytes) is counted by the kernel in a replay of the same (deterministic) steps,
 which makes the same launches.
 
+batched: scene-steps/s of 512 independent scenes of 2 to 48 bodies (the batched
+configuration) stepped by one graph launch per step, beside the same scenes stepped one after
+another.  --no-batched skips it.
+
+adjoint: gradients/s of the differentiable configuration's loss (16 icospheres on the ground
+box, 100 steps, checkpoints every 10) with respect to all initial states, through the
+torch.autograd trajectory of abd_warp_b200/adjoint.py (forward, then the backward's segment
+recomputation and one adjoint step per step), with the oracle's forward and dense adjoint of
+the same gradient as its CPU baseline.  --no-adjoint skips it.
+
 Multi-GPU: the step does not shard (one coupled Newton solve per scene), so N ranks run N
 independent replicas; value = N * K / max-over-ranks time.
 
@@ -80,6 +90,8 @@ def parse():
                          "from the host (two waits per iteration); the same results")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint gradient throughput")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched scenes' throughput")
     ap.add_argument("--start-state", type=int, default=None,
                     help="time all K steps from the stored oracle state at this step of the trajectory (0, 75, "
                          "150 or 225; for profiling one stretch) instead of K / 4 from each")
@@ -97,6 +109,111 @@ def make_scene():
     from abd_warp_b200 import scenes
     bodies, prm, _ = scenes.make_config(2)
     return bodies, prm
+
+
+ADJ_BODY = 1
+
+
+def adjoint_scene():
+    """The differentiable configuration: 16 level-2 icospheres on the ground box, 100 steps,
+    loss ||com_1(T) - target||^2; the barrier stiffness lowered to 1e3 and Newton run to
+    g.g < 1e-22 (60 iterations at most) so that the steps converge and the derivative exists."""
+    import numpy as np
+    from abd_warp_b200 import scenes
+    bodies, prm, steps = scenes.make_config(4)
+    prm.kappa, prm.tol, prm.max_iter = 1e3, 1e-22, 60
+    flat = scenes.flatten_bodies(bodies)
+    target = np.asarray(flat["p"][ADJ_BODY]) + np.array([0.3, 0.0, -0.2])
+    return bodies, prm, steps, flat, target
+
+
+def batched_gpu(dev, n_scenes=512, steps=4, warmup=2):
+    """Scene-steps/s of the batched configuration (512 independent scenes of 2 to 48 bodies
+    over their own ground boxes): every scene stepped by one graph launch (abd_batch_step),
+    against the same scenes stepped one abd_step after another; the first steps of their
+    trajectory (warm-up steps first, then the timed ones, CUDA events around each)."""
+    import torch
+    from abd_warp_b200 import scenes
+    from abd_warp_b200.batch import BatchSimulator
+    sc, prm, _ = scenes.config3(n_scenes=n_scenes)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for mode in ("batched", "sequential"):
+        b = BatchSimulator(sc, prm, device=str(dev))
+        try:
+            fn = b.step if mode == "batched" else b.step_sequential
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize(dev)
+            ms = 0.0
+            contacts = 0
+            for _ in range(steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                infos = fn()
+                e1.record(stream)
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
+                contacts += sum(i["n_active"] for i in infos)
+            out[mode] = n_scenes * steps / (ms / 1e3)
+            out["active_contacts_per_step"] = contacts / steps
+        finally:
+            b.close()
+    bodies = sum(len(x) for x in sc)
+    return {"value": out["batched"], "unit": "scene-steps/s", "sequential": out["sequential"],
+            "speedup": out["batched"] / out["sequential"],
+            "workload": f"{n_scenes} scenes of 2-48 bodies ({bodies} bodies) over their own ground boxes, "
+                        f"steps {warmup + 1}-{warmup + steps} of their trajectories",
+            "active_contacts_per_step": out["active_contacts_per_step"], "dtype": "f64"}
+
+
+def adjoint_gpu(dev, reps=2):
+    """Gradients/s of the loss with respect to all initial states (positions, A, velocities)
+    through the 100-step trajectory: forward with checkpoints every 10 steps, then the backward
+    (segment recomputation and one adjoint step per step); the mean of reps gradients after one
+    untimed, CUDA events around each."""
+    import torch
+    from abd_warp_b200.adjoint import trajectory
+    from abd_warp_b200.simulator import AffineBodySimulator
+    bodies, prm, steps, _, target = adjoint_scene()
+    sim = AffineBodySimulator(bodies=bodies, params=prm, device=str(dev))
+    tgt = torch.as_tensor(target, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    times = []
+    try:
+        for r in range(reps + 1):
+            sim.reset()
+            x = [getattr(sim.states, k).clone().requires_grad_(True) for k in ("A0", "p0", "Adot", "pdot")]
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = trajectory(sim, *x, steps=steps, checkpoint=10)
+            d = out[1][ADJ_BODY] - tgt
+            (d * d).sum().backward()
+            e1.record(stream)
+            e1.synchronize()
+            if r:
+                times.append(e0.elapsed_time(e1) / 1e3)
+    finally:
+        sim.close()
+    return 1.0 / (sum(times) / len(times)), steps
+
+
+def adjoint_cpu():
+    """The oracle's forward and adjoint (dense exact Hessians) of the same gradient, timed once."""
+    import numpy as np
+
+    import oracle
+    from oracle import adjoint_ref as AJ
+    bodies, prm, steps, flat, target = adjoint_scene()
+    t0 = time.perf_counter()
+    o = oracle.Oracle(flat, prm)
+    states, _ = AJ.forward(o, steps)
+    _, gp = AJ.com_loss(states, ADJ_BODY, target)
+    qb = np.zeros((o.n, 12))
+    qb[ADJ_BODY, :3] = gp
+    AJ.backward(o, flat, prm, states, qb, model="reference")
+    return 1.0 / (time.perf_counter() - t0), oracle.max_threads()
 
 
 class ClockSampler:
@@ -378,6 +495,18 @@ def main():
                      "peak_kind": peak_kind, "timed_launches": k_launches, "counted_launches": c_launches,
                      "avg_launch_us": us_per_launch, "bytes_per_launch": bytes_per_launch},
     }
+    if not args.no_batched:
+        line["batched"] = batched_gpu(dev)
+    if not args.no_adjoint:
+        g, asteps = adjoint_gpu(dev)
+        line["adjoint"] = {"value": g, "unit": "grads/s",
+                           "workload": f"16 icospheres on a ground box, {asteps} steps, checkpoints every 10, "
+                                       "gradient of ||com_1(T) - target||^2 with respect to all initial states",
+                           "dtype": "f64"}
+        if rank == 0 and not args.no_cpu_baseline:
+            cg, cth = adjoint_cpu()
+            line["adjoint"]["cpu_baseline"] = {"value": cg, "unit": "grads/s", "cores": cth, "kind": "port",
+                                               "sample": "one gradient: oracle forward + dense exact-Hessian adjoint"}
     if rank == 0 and not args.no_cpu_baseline:
         v, _, threads, desc = oracle_sample(per_state, args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": desc}

@@ -62,6 +62,13 @@ typedef struct abd_params {
                          them, waiting for the device twice per iteration.  Both give the same
                          results; the device loop hands a step over to the host loop when its
                          line search needs more than 16 trials (alpha_min <= 2^-15) */
+  int ipc_full;       /* 0 (default): the reference's contact model -- interior point-triangle
+                         and edge-edge pairs only (ipcsk/energy.py:20-22, 46-48; ccd.py:44-54).
+                         1: the full IPC model -- the closest feature pair of every candidate
+                         (point-triangle / -edge / -point; edge-edge / point-edge / point-point),
+                         the barrier on its squared distance with the edge-edge mollifier, a
+                         per-contact PSD projection of the exact local Hessian, and CCD roots on
+                         the closed triangle / segments */
 } abd_params;
 
 /* Scene description (host arrays, copied at creation).  Bodies are concatenated:
@@ -94,6 +101,7 @@ typedef struct abd_step_info {
 } abd_step_info;
 
 typedef struct abd_sim abd_sim;
+typedef struct abd_batch abd_batch;
 
 /* Create a simulator for one scene on the current CUDA device; stream may be NULL (legacy
  * default stream).  Builds the per-body LBVHs (Morton codes, radix sort, Karras build).
@@ -121,6 +129,21 @@ int abd_sim_sizes(const abd_sim* sim, int* n_bodies, int* n_verts, int* n_tris, 
  * inertia + orthogonality + IPC barrier energy with CCD-bounded backtracking line search,
  * then q0 <- q, qdot <- (q - q0)/dt and x_view_dev <- transform(q0).  x_view_dev may be NULL. */
 int abd_step(abd_sim* sim, const abd_states* st, double* x_view_dev, abd_step_info* info);
+
+/* Batched scenes (the reference steps one scene per simulator).  abd_batch_create groups n
+ * simulators (one scene each, created by abd_sim_create and still owned by the caller, who
+ * destroys them after the batch); stream is where the batch's steps run (NULL: legacy default
+ * stream).  abd_batch_step steps every scene once: st[i] are scene i's states, x_view[i] its
+ * vertex positions out (x_view or any x_view[i] may be NULL), info[i] its step info (info may
+ * be NULL).  All scenes' device-loop steps are one CUDA graph, each scene a branch of its own
+ * that holds its Newton loop, so one launch runs every scene's iterations concurrently with
+ * each scene's own iteration counts, line search and convergence: each scene's result is the
+ * one abd_step gives it.  A scene whose list overflowed is stepped again alone after the
+ * list grew.  Needs alpha_min > 2^-15 in every scene (else ABD_ERR_INVALID).  Returns the
+ * first error of a scene, or ABD_OK. */
+int abd_batch_create(int n, abd_sim* const* sims, void* stream, abd_batch** out);
+int abd_batch_destroy(abd_batch* batch);
+int abd_batch_step(abd_batch* batch, const abd_states* st, double* const* x_view, abd_step_info* info);
 
 /* One step of the adjoint of abd_step (the reference has none: hl_entry.py:4 sets
  * enable_backward = False).  A converged step solves grad E(q; q~) = 0 for q_{t+1}, with the
@@ -228,6 +251,10 @@ int abd_inertia_energy_noalloc(const abd_params* prm, int n_bodies, const abd_st
  * (pt_ipc.py:118, ee_ipc.py:98).  Here PT, EE and vertex-ground contacts all count, for both
  * bodies of a contact. */
 int abd_get_highlight(abd_sim* sim, int* highlight_dev);
+
+/* Where the last CUDA runtime call that failed in this thread failed, for an ABD_ERR_CUDA:
+ * "file:line: error name: description" (empty if none has). */
+const char* abd_error_detail(void);
 
 /* Device status bits accumulated since the last call (and cleared). */
 int abd_take_status(abd_sim* sim, int* status);

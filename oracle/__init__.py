@@ -124,10 +124,12 @@ class Oracle:
         self._prm = prm.to_c()
         lib().orc_set_params(self.h, ctypes.byref(self._prm))
 
-    def set_ipc_full(self, on: bool):
+    def set_ipc_full(self, on: bool, independent: bool = False):
         """The full IPC contact model (closest-feature types, edge-edge mollifier, inclusive
-        CCD) instead of the reference's interior-only model."""
-        lib().orc_set_ipc_full(self.h, 1 if on else 0)
+        CCD) instead of the reference's interior-only model.  Per contact, the CUDA library's
+        arithmetic (its header, so that steps compare bit for bit) or, with independent, the
+        oracle's own forward-mode restatement.  SimParams.ipc_full = 1 also selects the first."""
+        lib().orc_set_ipc_full(self.h, (2 if independent else 1) if on else 0)
 
     def set_friction(self, mu: float, eps_v: float = 1e-3):
         """Lagged friction (coefficient mu, slip velocity eps_v) on the full contact model's

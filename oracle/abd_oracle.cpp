@@ -37,6 +37,11 @@
 #include <vector>
 #include <omp.h>
 
+// The full IPC model's per-contact arithmetic, shared with the CUDA library (plain C++): the
+// oracle's full mode evaluates it so that whole steps can be compared bit for bit, and checks
+// it against its own forward-mode restatement below (full_energy_d / full_terms).
+#include "../abd_warp_b200/csrc/abd_ipc_full.cuh"
+
 namespace {
 
 struct Params {
@@ -46,6 +51,7 @@ struct Params {
       cg_max_iter, precision, contact_psd, precond, cluster_max;
   int min_capacity;  // the CUDA library's capacity injection (the oracle has no capacities)
   int newton_loop;   // the CUDA library's choice of Newton loop (the oracle has one)
+  int ipc_full;      // the full contact model (the oracle's own switch, Oracle::ipc_full, decides)
 };
 
 struct V3 {
@@ -204,6 +210,7 @@ struct Oracle {
       stat_active = 0, stat_refine = 0;
   int last_sweeps = 0;  // refinement sweeps of the last mixed-precision solve
   bool ipc_full = false;  // full IPC contact model (closest-feature types, mollifier)
+  bool ipc_independent = false;  // full model in the oracle's own arithmetic (else the header's)
   // lagged friction (with the full model): coefficient, slip velocity, and the contacts that
   // the step fixed at its start
   double fr_mu = 0.0, fr_epsv = 1e-3;
@@ -1084,6 +1091,61 @@ double full_energy(int kind, const V3 xs[4], const V3 rs[4], const Params& P) {
   return full_energy_d(kind, xs, rs, P, E) ? E.v : 0.0;
 }
 
+// The full model in the CUDA library's arithmetic (abd_ipc_full.cuh with the shared log): the
+// energy, and a contact's 456 affine terms as the pair assembly forms them -- the local Hessian
+// and gradient from hyper-dual entries, projected onto the PSD cone, then each affine entry
+// summed over the contact's vertices in the kernel's order (vertex u, then w)
+inline void pts12(const V3 v[4], double x[12]) {
+  for (int k = 0; k < 4; ++k) {
+    x[3 * k] = v[k].x;
+    x[3 * k + 1] = v[k].y;
+    x[3 * k + 2] = v[k].z;
+  }
+}
+double full_energy_hd(int kind, const V3 xs[4], const V3 rs[4], const Params& P) {
+  double x[12], r[12];
+  pts12(xs, x);
+  pts12(rs, r);
+  abd::ipc::V3<double> v[4];
+  abd::ipc::load(x, v);
+  const int ty = abd::ipc::contact_type(kind, x);
+  const double d2 = kind == 0 ? abd::ipc::pt_d2(ty, v) : abd::ipc::ee_d2(ty, v);
+  if (!(d2 < P.d2hat)) return 0.0;
+  return abd::ipc::local_energy(kind, ty, v, kind == 1 ? abd::ipc::ee_eps_x(r) : 0.0, P.d2hat, P.kappa,
+                                [](double u) { return abd_log(u); });
+}
+bool full_terms_hd(int kind, const V3 xs[4], const V3 rs[4], int swap, const Params& P, double out[456]) {
+  double x[12], r[12], H[144], g[12], E, d2;
+  int ty;
+  pts12(xs, x);
+  pts12(rs, r);
+  if (!abd::ipc::local_gh(kind, x, r, P.d2hat, P.kappa, [](double u) { return abd_log(u); }, &ty, &d2, &E, g, H))
+    return false;
+  abd::ipc::project_psd12(H);
+  const int nI = kind == 0 ? 1 : 2;
+  auto side = [&](int v) { return (v < nI ? 0 : 1) ^ swap; };
+  auto wt = [&](int v, int m) { return m == 0 ? 1.0 : r[3 * v + m - 1]; };
+  for (int e = 0; e < 456; ++e) {
+    double val = 0.0;
+    if (e < 432) {
+      const int blk = e / 144, rw = (e % 144) / 12, c = e % 12;
+      const int rsd = blk == 2 ? 1 : 0, csd = blk == 1 ? 0 : 1;
+      const int m = rw / 3, ra = rw % 3, n = c / 3, cb = c % 3;
+      for (int u = 0; u < 4; ++u) {
+        if (side(u) != rsd) continue;
+        for (int w = 0; w < 4; ++w)
+          if (side(w) == csd) val += (wt(u, m) * H[12 * (3 * u + ra) + 3 * w + cb]) * wt(w, n);
+      }
+    } else {
+      const int k = e - 432, sd = k / 12, m = (k % 12) / 3, comp = k % 3;
+      for (int u = 0; u < 4; ++u)
+        if (side(u) == sd) val += wt(u, m) * g[3 * u + comp];
+    }
+    out[e] = val;
+  }
+  return true;
+}
+
 // ---------------------------------------------------------------------------------------
 // Lagged friction (Li et al. 2020, section 5), with the full contact model: at the step start
 // each contact within dhat fixes the weights w of its closest points (c_a - c_b =
@@ -1426,7 +1488,9 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
       V3 xs[4], rs[4];
       fetch(o, y, C[i], type, xs, rs);
       const int swap = C[i].I != L.ij[2 * C[i].pair];
-      on[i] = (o.ipc_full ? full_terms(type, xs, rs, swap, o.prm, R[i].v) : contact_terms(type, xs, rs, swap, o.prm, R[i].v))
+      on[i] = (o.ipc_full ? (o.ipc_independent ? full_terms(type, xs, rs, swap, o.prm, R[i].v)
+                                               : full_terms_hd(type, xs, rs, swap, o.prm, R[i].v))
+                          : contact_terms(type, xs, rs, swap, o.prm, R[i].v))
                   ? 1
                   : 0;
       R[i].pair = C[i].pair;
@@ -2194,7 +2258,8 @@ double energy_at(Oracle& o, const double* y, const double* Akp, const double* pk
       for (int i = 0; i < nc; ++i) {
         V3 xs[4], rs[4];
         fetch(o, y, C[i], type, xs, rs);
-        part.add(o.ipc_full ? full_energy(type, xs, rs, o.prm) : contact_energy(type, xs, o.prm));
+        part.add(o.ipc_full ? (o.ipc_independent ? full_energy(type, xs, rs, o.prm) : full_energy_hd(type, xs, rs, o.prm))
+                            : contact_energy(type, xs, o.prm));
       }
 #pragma omp critical
       total.merge(part);
@@ -2348,6 +2413,7 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
   o->I0.assign(I0, I0 + n);
   o->fixed.assign(fixed, fixed + n);
   o->prm = *prm;
+  o->ipc_full = prm->ipc_full != 0;
   for (auto* v : {&o->A, &o->Ak, &o->Adot, &o->A0}) v->assign(9 * (size_t)n, 0.0);
   for (auto* v : {&o->p, &o->pk, &o->pdot, &o->p0}) v->assign(3 * (size_t)n, 0.0);
   o->dq.assign(12 * (size_t)n, 0.0);
@@ -2364,8 +2430,17 @@ void orc_get_highlight(void* h, int* out) {
   const Oracle& o = *(Oracle*)h;
   for (int b = 0; b < o.n; ++b) out[b] = (int)o.highlight.size() == o.n ? o.highlight[b] : 0;
 }
-void orc_set_params(void* h, const Params* prm) { ((Oracle*)h)->prm = *prm; }
-void orc_set_ipc_full(void* h, int on) { ((Oracle*)h)->ipc_full = on != 0; }
+void orc_set_params(void* h, const Params* prm) {
+  Oracle* o = (Oracle*)h;
+  o->prm = *prm;
+  if (prm->ipc_full) o->ipc_full = true;
+}
+// on: 0 the reference's model, 1 the full model in the CUDA library's arithmetic, 2 the full
+// model in the oracle's own
+void orc_set_ipc_full(void* h, int on) {
+  ((Oracle*)h)->ipc_full = on != 0;
+  ((Oracle*)h)->ipc_independent = on == 2;
+}
 // lagged friction with coefficient mu and slip velocity eps_v (needs the full contact model)
 // one candidate's lagged friction: fixed at step-start positions xt12 (rest rs12), evaluated at
 // x12 with coefficient mu and threshold eps (displacement); returns 0 when not within dhat
