@@ -91,6 +91,7 @@ def load():
         "abd_launch_count": ([P], c_longlong),
         "abd_profile": ([P, c_int], c_int),
         "abd_profile_read": ([P, P, P, P], c_int),
+        "abd_fp64_peak": ([P], c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -107,7 +108,7 @@ def exported_symbols():
             "abd_sim_get_dq", "abd_sim_set_dq", "abd_sim_get_g", "abd_sim_sizes", "abd_step", "abd_update_mesh_vertex",
             "abd_collision_set", "abd_collision_set_dofs", "abd_export_lists", "abd_ipc_gh", "abd_export_system", "abd_solve",
             "abd_compute_energy", "abd_ccd", "abd_energies_along", "abd_get_highlight", "abd_adjoint_step", "abd_batch_create", "abd_batch_destroy", "abd_batch_step", "abd_take_status", "abd_status_string", "abd_error_detail", "abd_launch_count",
-            "abd_profile", "abd_profile_read"]
+            "abd_profile", "abd_profile_read", "abd_fp64_peak"]
 
 
 def check(rc: int, what: str = ""):

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libabd_b200.so")
-SOURCES = ["lbvh.cu", "broad.cu", "narrow.cu", "linesearch.cu", "solver.cu", "newton.cu", "sim.cu", "noalloc.cu"]
+SOURCES = ["lbvh.cu", "broad.cu", "narrow.cu", "linesearch.cu", "solver.cu", "newton.cu", "sim.cu", "noalloc.cu", "peak.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--expt-relaxed-constexpr",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]

@@ -495,6 +495,13 @@ def main():
                      "peak_kind": peak_kind, "timed_launches": k_launches, "counted_launches": c_launches,
                      "avg_launch_us": us_per_launch, "bytes_per_launch": bytes_per_launch},
     }
+    # the FP64 ceiling of the contact and solver kernels: the measured DFMA rate (their own
+    # multiplies and adds are separate instructions, so half of it bounds them)
+    import ctypes
+    from abd_warp_b200 import _lib
+    fp64 = ctypes.c_double(0.0)
+    if _lib.load().abd_fp64_peak(ctypes.byref(fp64)) == _lib.ABD_OK:
+        line["fp64_peak"] = {"value": fp64.value, "unit": "TFLOP/s", "how": "chains of DFMA on every SM, CUDA events"}
     if not args.no_batched:
         line["batched"] = batched_gpu(dev)
     if not args.no_adjoint:

@@ -275,6 +275,10 @@ long long abd_launch_count(const abd_sim* sim);
  * records 140 B, tree entries tested 36 B, candidates written 16 B).
  * abd_profile(sim, 0) stops. */
 int abd_profile(abd_sim* sim, int enable);
+/* The current device's FP64 throughput (TFLOP/s) measured by chains of fused multiply-adds
+ * (no counterpart in the reference; the benchmark's FP64 roofline).  The library's kernels
+ * are built without multiply-add contraction, so their own FP64 rate tops out at half of it. */
+int abd_fp64_peak(double* tflops);
 int abd_profile_read(const abd_sim* sim, double* ms, long long* launches, double* bytes);
 
 #ifdef __cplusplus
