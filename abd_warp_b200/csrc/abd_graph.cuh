@@ -64,4 +64,61 @@ int run_graph(Sim& s, GraphSlot& g, uint64_t key, F&& issue) {
   return ABD_OK;
 }
 
+// Conditional nodes built during stream capture: a handle of the graph being captured, a
+// WHILE or IF node after the work captured so far, and the capture of its body graph on a
+// stream of its own.
+#define GCK(x)                                         \
+  do {                                                 \
+    if (ABD_NOTE(x) != cudaSuccess) return ABD_ERR_CUDA; \
+  } while (0)
+
+// A conditional handle of the graph being captured on st (its value is set by kernels)
+inline int make_handle(cudaStream_t st, cudaGraphConditionalHandle* hc) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  GCK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr));
+  if (cs != cudaStreamCaptureStatusActive) return ABD_ERR_CUDA;
+  GCK(cudaGraphConditionalHandleCreate(hc, graph, 0, 0));
+  return ABD_OK;
+}
+
+// Adds a conditional node (hc, type) after the work captured on st so far; what st captures
+// next follows the node.  *body: the node's body graph.
+inline int add_conditional(cudaStream_t st, cudaGraphConditionalHandle hc, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  GCK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+  if (cs != cudaStreamCaptureStatusActive) return ABD_ERR_CUDA;
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = hc;
+  np.conditional.type = type;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  GCK(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
+  *body = np.conditional.phGraph_out[0];
+  GCK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  return ABD_OK;
+}
+
+// Captures issue() into the body graph of a conditional node, on stream bs (the simulator's
+// stream points there meanwhile)
+template <class F>
+inline int capture_body(Sim& s, cudaGraph_t body, cudaStream_t bs, F&& issue) {
+  GCK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const cudaStream_t saved = s.stream;
+  s.stream = bs;
+  const int r = issue();
+  s.stream = saved;
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(bs, &out);
+  if (r) return r;
+  return e == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+}
+
+#undef GCK
+
 }  // namespace abd

@@ -1179,53 +1179,6 @@ int step_host(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* 
   return (inf.status & (abd::ST_STACK_OVERFLOW | abd::ST_NAN)) ? ABD_ERR_DEVICE : ABD_OK;
 }
 
-// A conditional handle of the graph being captured on st (its value is set by kernels)
-int make_handle(cudaStream_t st, cudaGraphConditionalHandle* hc) {
-  cudaStreamCaptureStatus cs;
-  cudaGraph_t graph = nullptr;
-  CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr));
-  if (cs != cudaStreamCaptureStatusActive) return ABD_ERR_CUDA;
-  CK(cudaGraphConditionalHandleCreate(hc, graph, 0, 0));
-  return ABD_OK;
-}
-
-// Adds a conditional node (hc, type) after the work captured on st so far; what st captures
-// next follows the node.  *body: the node's body graph.
-int add_conditional(cudaStream_t st, cudaGraphConditionalHandle hc, cudaGraphConditionalNodeType type,
-                    cudaGraph_t* body) {
-  cudaStreamCaptureStatus cs;
-  cudaGraph_t graph = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t ndeps = 0;
-  CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
-  if (cs != cudaStreamCaptureStatusActive) return ABD_ERR_CUDA;
-  cudaGraphNodeParams np = {};
-  np.type = cudaGraphNodeTypeConditional;
-  np.conditional.handle = hc;
-  np.conditional.type = type;
-  np.conditional.size = 1;
-  cudaGraphNode_t node;
-  CK(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
-  *body = np.conditional.phGraph_out[0];
-  CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
-  return ABD_OK;
-}
-
-// Captures issue() into the body graph of a conditional node, on stream bs (the simulator's
-// stream points there meanwhile)
-template <class F>
-int capture_body(Sim& s, cudaGraph_t body, cudaStream_t bs, F&& issue) {
-  CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  const cudaStream_t saved = s.stream;
-  s.stream = bs;
-  const int r = issue();
-  s.stream = saved;
-  cudaGraph_t out = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(bs, &out);
-  if (r) return r;
-  return e == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
-}
-
 // Enqueues a step with the Newton iterations as a device loop on s.stream, which must be
 // capturing (newton.cu describes the loop); ends with the copy of the mailbox to the host
 int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
@@ -1264,22 +1217,22 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
   CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, top));
   CK(cudaMemcpyAsync(s.dq_save, s.dq, nq, cudaMemcpyDeviceToDevice, top));
   cudaGraphConditionalHandle hn;
-  if (int r = make_handle(top, &hn)) return r;
+  if (int r = abd::make_handle(top, &hn)) return r;
   CK(abd::step_begin(s, hn));
   cudaGraph_t nbody = nullptr;
-  if (int r = add_conditional(top, hn, cudaGraphCondTypeWhile, &nbody)) return r;
+  if (int r = abd::add_conditional(top, hn, cudaGraphCondTypeWhile, &nbody)) return r;
   const long long l0 = s.launches;
-  int r = capture_body(s, nbody, s.cap_stream3, [&]() -> int {
+  int r = abd::capture_body(s, nbody, s.cap_stream3, [&]() -> int {
     s.side = s.fork_a;
     const int q0 = gh_issue(h, st, st.A, st.p, 3);
     s.side = nullptr;
     if (q0) return q0;
     cudaGraphConditionalHandle hi;
-    if (int q = make_handle(s.stream, &hi)) return q;
+    if (int q = abd::make_handle(s.stream, &hi)) return q;
     CK(abd::gate_no_overflow(s, hi));
     cudaGraph_t ibody = nullptr;
-    if (int q = add_conditional(s.stream, hi, cudaGraphCondTypeIf, &ibody)) return q;
-    if (int q = capture_body(s, ibody, s.cap_stream4, iteration_tail)) return q;
+    if (int q = abd::add_conditional(s.stream, hi, cudaGraphCondTypeIf, &ibody)) return q;
+    if (int q = abd::capture_body(s, ibody, s.cap_stream4, iteration_tail)) return q;
     CK(abd::newton_end(s, hn));
     return ABD_OK;
   });
