@@ -272,6 +272,7 @@ struct Sim {
   // [0, nV) the body's points and [nV, nV + nE) its edges, kChunk items per chunk
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
+  int* chunk_act = nullptr;        // [nch + 1] the chunks of a narrow pass with work, then their count
   Box* chunk_box = nullptr;        // [nch] rest-frame box of each chunk's items
   int* vperm = nullptr;            // [V] vertices of each body in Morton order (chunk items)
   // vertex slices of the line-search bounds: (body, first vertex, count), count <= kSlice
@@ -306,6 +307,14 @@ struct Sim {
   // joins the capture it forks from until that capture ends, so the device loop gives each
   // capture scope its own (fork_a: the Newton body, fork_b: its IF body); null: cap_stream2
   cudaStream_t fork_a = nullptr, fork_b = nullptr, side = nullptr;
+  // A device-loop step (in_device_loop: its capture is in progress) puts the passes that most
+  // Newton iterations skip in IF nodes: the GH pass's tree traversal (needed only when the
+  // kept line-search candidates do not cover the pass; the superset check sets the condition)
+  // and the inverse of clusters of more than one body.  (The host loop launches them, and they
+  // return at once.)  gh_if_on: the GH handle belongs to the capture in progress
+  cudaStream_t cap_stream5 = nullptr;  // captures those IF nodes' bodies
+  cudaGraphConditionalHandle gh_if = 0;
+  bool in_device_loop = false, gh_if_on = false;
   double* dq_save = nullptr;       // [12 n] dq at the start of a device-loop step (for a rerun)
   long long step_launch[3] = {0, 0, 0};  // kernels of a step graph: outside the loops, per
                                          // Newton iteration, per Krylov iteration

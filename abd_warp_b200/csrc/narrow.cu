@@ -24,6 +24,7 @@
 #include <cooperative_groups.h>
 
 #include "abd_body.cuh"
+#include "abd_graph.cuh"
 #include "abd_geometry.cuh"
 #include "abd_ipc_full.cuh"
 
@@ -55,6 +56,8 @@ struct NarrowArgs {
   const int* adj_pair;
   int cap_ccd;
   int4* ccd_cand;
+  int nch;
+  int* chunk_act;               // [nch + 1] the chunks of a pass with work (k_chunk_active), then their count
   int gh_energy;                // GH: also sum the candidates' barrier energies into energy
   const int* energy_gate;       // GH in the device loop: the energy only while this counter is 0
   unsigned long long* gtime;    // CCD_LS: first start / last end of the launch (global timer)
@@ -698,8 +701,77 @@ __device__ inline bool ee_owner(int I, int nEI, int J, int nEJ) { return nEI > n
 // queries' and leaves' rest boxes) and appends every pair found to the line-search
 // candidates; the pairs that also pass the CCD pass's own boxes (body pair, query and leaf)
 // become CCD candidates, the same set as the CCD pass finds.
+// The world box of chunk c of body I: the affine image of its rest box at the pass's DOFs
+// (with y1: the union over both DOF sets), dilated by dhat.  Every query box of the chunk lies
+// inside.
+__device__ inline Box chunk_world_box(const NarrowArgs& a, int c, int I) {
+  const Box R = load_box(&a.chunk_box[c]);
+  const float pad = __double2float_ru(a.prm.dhat);
+  Box b = affine_box(R, a.fdof + 24 * (size_t)I, pad);
+  if (a.y1) {
+    const Box B1 = affine_box(R, a.fdof + 24 * (size_t)I + 12, pad);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      b.lo[k] = fminf(b.lo[k], B1.lo[k]);
+      b.hi[k] = fmaxf(b.hi[k], B1.hi[k]);
+    }
+  }
+  return b;
+}
+
+// The chunks of a pass with work, one warp per chunk: those whose world box overlaps the body
+// box of a neighbour (CCD_LS: the box over the DOF range), and a body's first chunk when the
+// pass adds the body's own terms there (ENERGY; CCD with vertex-ground contacts).  They are
+// appended to chunk_act, whose entry nch counts them; k_chunk_narrow's first CTAs take them.
+// In a resting pile most chunks face no neighbour, and finding that out costs a chunk CTA a
+// chain of dependent loads; here it costs a warp.  (The tests are k_chunk_narrow's own: a
+// chunk that is left out would have found no neighbour there.)
+constexpr int KA = 256;  // threads of the chunk filter
+template <int MODE>
+__global__ void __launch_bounds__(KA) k_chunk_active(NarrowArgs a) {
+  constexpr bool ls = MODE == NARROW_CCD_LS;
+  constexpr bool ccd = MODE == NARROW_CCD || ls, gh = MODE == NARROW_GH;
+  if constexpr (gh) {
+    if (*a.sup_valid) return;
+  }
+  if (ls && a.gtime && threadIdx.x == 0) atomicMin(&a.gtime[0], globaltimer_ns());
+  const int lane = (int)(threadIdx.x & 31);
+  const int c = (int)((blockIdx.x * KA + threadIdx.x) >> 5);
+  if (c >= a.nch) return;
+  const int2 ch = a.chunk[c];
+  const int I = ch.x;
+  const int nEI = a.eoff[I + 1] - a.eoff[I];
+  const int nV = a.voff[I + 1] - a.voff[I];
+  const int Q = max(0, min(CT, nV + nEI - ch.y));
+  bool need = !gh && ch.y == 0 && (!ccd || (a.prm.ground_enabled && a.prm.enable_vg));
+  int r0 = 0, deg;
+  if constexpr (gh) {
+    r0 = a.row_ptr[I];
+    deg = (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW) ? 0 : min(a.row_ptr[I + 1], a.cap_adj) - r0;
+  } else {
+    deg = a.row_cnt[I];
+  }
+  if (Q == 0) deg = 0;
+  if (ls && a.prof && lane == 0 && deg > 0)
+    atomicAdd(&a.prof_rows[8 * (c & 31) + PF_NEIGHBOUR], (unsigned long long)deg);
+  if (!need && deg > 0) {
+    const Box cbx = chunk_world_box(a, c, I);
+    for (int k0 = 0; k0 < deg && !need; k0 += 32) {
+      const int k = k0 + lane;
+      bool rel = false;
+      if (k < deg) {
+        const int J = gh ? a.adj_col[r0 + k] : (k < kNbList ? a.nbr[(size_t)I * kNbList + k] : kth_neighbour(a, I, k));
+        rel = overlap(cbx, load_box(&(ls ? a.body_sup : a.body_box)[J]));
+      }
+      need = __any_sync(0xffffffffu, rel);
+    }
+  }
+  if (need && lane == 0) a.chunk_act[atomicAdd(&a.chunk_act[a.nch], 1)] = c;
+}
+
 constexpr int CW = 4 * CT;  // (query, neighbour) combinations tested per round
 constexpr int kFront = 512;  // entries of a breadth-first frontier
+constexpr int kCandBuf = 256;  // candidates a chunk CTA gathers before it writes them out
 template <int MODE>
 __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   constexpr bool ls = MODE == NARROW_CCD_LS;
@@ -707,8 +779,12 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   if constexpr (gh) {
     if (*a.sup_valid) return;  // k_gh_scan takes the candidates from ecand
   }
-  const int c = blockIdx.x, tid = threadIdx.x;
-  if (ls && a.gtime && tid == 0) atomicMin(&a.gtime[0], globaltimer_ns());
+  const int tid = threadIdx.x;
+  if ((int)blockIdx.x >= a.chunk_act[a.nch]) {  // more CTAs than chunks with work
+    if (ls && a.gtime && tid == 0) atomicMax(&a.gtime[1], globaltimer_ns());
+    return;
+  }
+  const int c = a.chunk_act[blockIdx.x];
   const int2 ch = a.chunk[c];
   const int I = ch.x;
   const int nEI = a.eoff[I + 1] - a.eoff[I];
@@ -729,19 +805,41 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   __shared__ XSum xe;
   __shared__ unsigned long long tkey;
   __shared__ Box cbx;  // the chunk's world box: every query box of the chunk lies inside
-  if (tid == 0 && Q > 0) {
-    const Box R = load_box(&a.chunk_box[c]);
-    const float pad = __double2float_ru(a.prm.dhat);
-    cbx = affine_box(R, a.fdof + 24 * (size_t)I, pad);
-    if (a.y1) {
-      const Box B1 = affine_box(R, a.fdof + 24 * (size_t)I + 12, pad);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        cbx.lo[k] = fminf(cbx.lo[k], B1.lo[k]);
-        cbx.hi[k] = fmaxf(cbx.hi[k], B1.hi[k]);
-      }
+  if (tid == 0 && Q > 0) cbx = chunk_world_box(a, c, I);
+  // The candidates (GH, CCD, CCD_LS) gather in shared memory and go to their list in blocks,
+  // one global atomic per block: a hit does not wait on the list's counter, which every CTA
+  // of the launch shares.  A full buffer sends the rest straight to the list.
+  constexpr bool lists = gh || ccd;
+  __shared__ int4 cbuf[kCandBuf];
+  __shared__ int ncb, cbase;
+  int* const ccount = &a.dstat[ls ? DS_NECAND : DS_NCCD];
+  int4* const cdst = ls ? a.ecand : a.ccd_cand;
+  const int ccap = ls ? a.cap_ecand : a.cap_ccd;
+  const int cflag = ls ? ST_ECAND_OVERFLOW : ST_CCD_OVERFLOW;
+  auto emit = [&](int4 rec) {
+    const int k = atomicAdd(&ncb, 1);
+    if (k < kCandBuf) {
+      cbuf[k] = rec;
+    } else {
+      const int pos = append_slot(ccount);
+      if (pos < ccap) cdst[pos] = rec;
+      else atomicOr(&a.dstat[DS_STATUS], cflag);
     }
-  }
+  };
+  // the buffer to the list: every thread, after a barrier that follows the emits
+  auto flush = [&]() {
+    const int n = min(ncb, kCandBuf);
+    if (n == 0) return;
+    if (tid == 0) cbase = atomicAdd(ccount, n);
+    __syncthreads();
+    for (int e = tid; e < n; e += CT) {
+      if (cbase + e < ccap) cdst[cbase + e] = cbuf[e];
+      else atomicOr(&a.dstat[DS_STATUS], cflag);
+    }
+    __syncthreads();
+    if (tid == 0) ncb = 0;  // the next barrier orders it before the next emit
+  };
+  if (tid == 0) ncb = 0;
   if (tid == 0) nfr[0] = nfr[1] = 0;
   if (ccd) {
     if (tid == 0) tkey = 0;
@@ -857,19 +955,13 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
           // evaluated by k_gh_eval, one thread per candidate.  PT: the point is I's, the
           // pair's first body is min(I, J); EE: the lower body's edge comes first
           const int swap = (type == 0 && I > nJ[j]) ? 1 : 0;
-          const int pos = append_slot(&a.dstat[DS_NCCD]);
-          if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(npair[j], type | (swap << 1), pa, pb);
-          else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+          emit(make_int4(npair[j], type | (swap << 1), pa, pb));
         } else if constexpr (ls) {
           // line-search candidates; k_ccd_eval takes those that pass the CCD pass's boxes
-          const int pos = append_slot(&a.dstat[DS_NECAND]);
           ++pf_cand;
-          if (pos < a.cap_ecand) a.ecand[pos] = make_int4(type, pa, pb, 0);
-          else atomicOr(&a.dstat[DS_STATUS], ST_ECAND_OVERFLOW);
+          emit(make_int4(type, pa, pb, 0));
         } else if constexpr (ccd) {  // evaluated by k_ccd_eval, one thread per candidate
-          const int pos = append_slot(&a.dstat[DS_NCCD]);
-          if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(type, pa, pb, 0);
-          else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
+          emit(make_int4(type, pa, pb, 0));
         } else {
           int ids[4];
           d3 xs[4];
@@ -943,10 +1035,15 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
           tally(nbx.tri, vc);
         }
         __syncthreads();
+        if (lists && ncb >= kCandBuf / 2) flush();
         if (tid == 0) nfr[fcur] = 0;
         fcur = nxt;
       }
     }
+  }
+  if constexpr (lists) {
+    __syncthreads();
+    flush();
   }
   if constexpr (gh) return;
   if (ls && a.prof) {  // kernel profiling: the data this chunk read and wrote
@@ -964,7 +1061,6 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
       atomicAdd(&row[PF_EDGELEAF], (unsigned long long)pf_edge);
       atomicAdd(&row[PF_CAND], (unsigned long long)pf_cand);
     }
-    if (tid == 0 && deg > 0) atomicAdd(&row[PF_NEIGHBOUR], (unsigned long long)deg);
   }
   __syncthreads();
   if (tid == 0) {
@@ -1054,9 +1150,10 @@ __global__ void __launch_bounds__(128) k_gh_scan(NarrowArgs a) {
   }
 }
 
-// Sets dint[kSupValid] (gh_superset_check); one CTA
+// Sets dint[kSupValid] (gh_superset_check) and, in a captured pass (use_hc), the condition of
+// the IF node around the tree traversal: 1 when the traversal must run; one CTA
 __global__ void k_sup_check(int n, const double* A0, const double* p0, const double* q_last, const int* have,
-                            int* valid, int mode, const int* it) {
+                            int* valid, int mode, const int* it, cudaGraphConditionalHandle hc, int use_hc) {
   if (mode == 3) mode = *it == 0 ? 1 : 2;
   __shared__ int ok;
   if (threadIdx.x == 0) ok = mode == 2 ? 1 : (mode == 1 ? (*have != 0) : 0);
@@ -1067,7 +1164,10 @@ __global__ void k_sup_check(int n, const double* A0, const double* p0, const dou
       if (__double_as_longlong(v) != __double_as_longlong(q_last[i])) ok = 0;
     }
   __syncthreads();
-  if (threadIdx.x == 0) *valid = ok;
+  if (threadIdx.x == 0) {
+    *valid = ok;
+    if (use_hc) cudaGraphSetConditional(hc, ok ? 0u : 1u);
+  }
 }
 
 // Contacts of the GH pass's candidates, one thread per candidate: the active ones
@@ -1405,6 +1505,8 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.W = s.W;
   a.body_box = s.body_box;
   a.chunk = s.chunk;
+  a.nch = s.nch;
+  a.chunk_act = s.chunk_act;
   a.energy = s.energy_acc;
   a.prof = s.prof_on == 2;
   a.prof_rows = &s.box->prof[0][0];
@@ -1487,6 +1589,19 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
   return a;
 }
 
+// A chunk pass: the chunk filter, then the chunk kernel over the chunks with work (a grid of
+// every chunk; the CTAs past the count return at once).  Counts the filter's launch.
+template <int MODE>
+cudaError_t chunk_pass(Sim& s, const NarrowArgs& a) {
+  cudaError_t e = cudaMemsetAsync(s.chunk_act + s.nch, 0, sizeof(int), s.stream);
+  if (e != cudaSuccess) return e;
+  constexpr int per = KA / 32;
+  k_chunk_active<MODE><<<(s.nch + per - 1) / per, KA, 0, s.stream>>>(a);
+  k_chunk_narrow<MODE><<<s.nch, CT, 0, s.stream>>>(a);
+  ++s.launches;
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const double* A1, const double* p1,
@@ -1498,7 +1613,7 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       return cudaErrorInvalidValue;
     if (s.nch == 0) return cudaSuccess;
     if (mode == NARROW_ENERGY) {
-      k_chunk_narrow<NARROW_ENERGY><<<s.nch, CT, 0, s.stream>>>(a);
+      if (cudaError_t e = chunk_pass<NARROW_ENERGY>(s, a)) return e;
     } else if (mode == NARROW_CCD || mode == NARROW_CCD_LS) {
       // DS_NCCD and DS_NECAND are adjacent
       static_assert(DS_NECAND == DS_NCCD + 1, "candidate counters");
@@ -1508,12 +1623,12 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
         if (!a.y1) return cudaErrorInvalidValue;
         if (s.prof_events > 0 && record_event(s.prof_ev[0], s.stream))
           return cudaErrorUnknown;
-        k_chunk_narrow<NARROW_CCD_LS><<<s.nch, CT, 0, s.stream>>>(a);
+        if ((e = chunk_pass<NARROW_CCD_LS>(s, a)) != cudaSuccess) return e;
         if (s.prof_events > 0 && record_event(s.prof_ev[1], s.stream))
           return cudaErrorUnknown;
         k_ccd_eval<true><<<kRedBlocks, 128, 0, s.stream>>>(a);
       } else {
-        k_chunk_narrow<NARROW_CCD><<<s.nch, CT, 0, s.stream>>>(a);
+        if ((e = chunk_pass<NARROW_CCD>(s, a)) != cudaSuccess) return e;
         k_ccd_eval<false><<<kRedBlocks, 128, 0, s.stream>>>(a);
       }
       ++s.launches;
@@ -1522,7 +1637,20 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCONTACT, 0, sizeof(int), s.stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, sizeof(int), s.stream);
       if (e != cudaSuccess) return e;
-      k_chunk_narrow<NARROW_GH><<<s.nch, CT, 0, s.stream>>>(a);
+      if (s.gh_if_on) {
+        // captured: the traversal in an IF node (k_sup_check sets its condition); the
+        // kernels in the body are not counted among the pass's launches (they rarely run)
+        s.gh_if_on = false;
+        cudaGraph_t body = nullptr;
+        if (add_conditional(s.stream, s.gh_if, cudaGraphCondTypeIf, &body) != ABD_OK) return cudaErrorUnknown;
+        const int r = capture_body(s, body, s.cap_stream5, [&]() -> int {
+          return chunk_pass<NARROW_GH>(s, a) == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+        });
+        if (r != ABD_OK) return cudaErrorUnknown;
+        s.launches -= 2;
+      } else {
+        if ((e = chunk_pass<NARROW_GH>(s, a)) != cudaSuccess) return e;
+      }
       k_gh_scan<<<kRedBlocks, 128, 0, s.stream>>>(a);
       k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
       s.launches += 2;
@@ -1562,8 +1690,19 @@ cudaError_t prepare_narrow(Sim& s) {
 }
 
 cudaError_t gh_superset_check(Sim& s, const abd_states* st, int mode) {
+  // a device-loop step's capture: a handle for the IF node narrow() puts around the GH tree
+  // traversal
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s.stream, &cs);
+  if (e != cudaSuccess) return e;
+  s.gh_if_on = false;
+  if (s.in_device_loop && cs == cudaStreamCaptureStatusActive) {
+    if (make_handle(s.stream, &s.gh_if) != ABD_OK) return cudaErrorUnknown;
+    s.gh_if_on = true;
+  }
   k_sup_check<<<1, 1024, 0, s.stream>>>(s.n, st ? st->A0 : nullptr, st ? st->p0 : nullptr, s.q_last,
-                                         s.dint + kSupHave, s.dint + kSupValid, st ? mode : 0, &s.box->step.it);
+                                         s.dint + kSupHave, s.dint + kSupValid, st ? mode : 0, &s.box->step.it,
+                                         s.gh_if, s.gh_if_on ? 1 : 0);
   ++s.launches;
   return cudaGetLastError();
 }

@@ -744,6 +744,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     s.nslice = (int)slices.size();
     ok(upload(&s.slice, slices.data(), slices.size(), s.stream));
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
+    ok(dalloc(&s.chunk_act, ch.size() + 1));
     ok(upload(&s.chunk_box, cbox.data(), cbox.size(), s.stream));
     ok(upload(&s.vperm, vperm.data(), vperm.size(), s.stream));
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // host temporaries
@@ -789,6 +790,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream4, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.fork_a, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.fork_b, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.cap_stream5, cudaStreamNonBlocking);
   for (cudaEvent_t* ev : {&s.fork_ev[0], &s.fork_ev[1]})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   ok(dalloc(&s.row_cnt, n));
@@ -855,12 +857,13 @@ int abd_sim_destroy(abd_sim* h) {
                   s.row_cnt, s.upper_cnt, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.zb, s.cl_tab, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
-                  s.body_sup, s.slice, s.q_last, s.highlight, s.cl_work_buf, s.dq_save, s.adj_x};
+                  s.body_sup, s.slice, s.q_last, s.highlight, s.cl_work_buf, s.dq_save, s.adj_x,
+                  s.chunk_act};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev, &s.g_step, &s.g_kadj})
     if (g->exec) cudaGraphExecDestroy(g->exec);
-  for (cudaStream_t q : {s.cap_stream, s.cap_stream2, s.cap_stream3, s.cap_stream4, s.fork_a, s.fork_b})
+  for (cudaStream_t q : {s.cap_stream, s.cap_stream2, s.cap_stream3, s.cap_stream4, s.cap_stream5, s.fork_a, s.fork_b})
     if (q) cudaStreamDestroy(q);
   for (cudaEvent_t ev : {s.prof_ev[0], s.prof_ev[1], s.fork_ev[0], s.fork_ev[1]})
     if (ev) cudaEventDestroy(ev);
@@ -1258,6 +1261,7 @@ void step_modes(Sim& s, bool on) {
   s.prof_events = on && s.prof_on ? -1 : 0;  // kernel timing by the global timer (no events)
   s.gh_energy = on ? 1 : 0;                  // the GH pass sums the energy at the first iteration
   s.energy_gate = on ? &s.box->step.it : nullptr;
+  s.in_device_loop = on;                     // passes that usually skip in IF nodes
 }
 
 constexpr int kHostFinish = -2;

@@ -5,10 +5,11 @@
 //
 // Preconditioner: contact-cluster block Jacobi.  Barrier stiffness between touching bodies is
 // 1e8-1e10 times their mass, so a per-body block Jacobi leaves the Krylov method facing that
-// condition number.  Bodies coupled by active contacts are grouped (union-find on the host,
-// strongest coupling first, at most cluster_max bodies); each cluster's dense system is
-// assembled and inverted in shared memory by one CTA (Gauss-Jordan, SPD, no pivoting), and
-// applied as a dense product.  Clusters of one body reduce to the per-body 12x12 block.
+// condition number.  Bodies coupled by active contacts are grouped on the device (mutual
+// strongest couplings merge in rounds, at most cluster_max bodies: k_clusters); each
+// cluster's dense system is assembled and inverted (Gauss-Jordan, SPD, no pivoting) by one
+// warp in registers (one or two bodies) or one CTA in shared memory (more), and applied as a
+// dense product.  Clusters of one body reduce to the per-body 12x12 block.
 //
 // Krylov: PCG (default; the projected Hessian is SPD) or right-preconditioned BiCGSTAB (the
 // reference's choice).  Convergence is measured in the preconditioned norm,
@@ -172,12 +173,75 @@ __global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) 
 }
 
 // ---- preconditioner setup: assemble and invert each cluster's dense block system ----
+// Clusters of one body (in a resting pile nearly every cluster: most bodies touch only the
+// fixed ground) are inverted by one warp each, in registers: lane j + 12 h (j < 12, h < 2)
+// holds rows 6h .. 6h + 5 of column j, and the pivot values and multipliers travel by
+// shuffles, so no shared memory and no barrier.  The arithmetic of every entry is the CTA
+// kernel's, in the same order: at pivot k row k becomes (j == k ? 1 : K[k][j]) times the
+// reciprocal of K[k][k], then every other row i with f = K[i][k] != 0 becomes
+// (j == k ? 0 : K[i][j]) - f K[k][j] (f == 0: only K[i][k] = 0).
+constexpr int WIT = 256;           // threads of the one-body inverse kernel
+constexpr int kWarpInvGrid = 148;  // its CTAs: one wave, a warp per cluster (grid-stride past 1184)
+__device__ inline void warp_inverse1(const SolverArgs& a, int c, int b, int lane) {
+  const int j = lane % 12, h = lane / 12;  // lanes 24..31 (h = 2) carry values that no one reads
+  double col[6];
+  const double* B = a.diag + (size_t)b * 144;
+#pragma unroll
+  for (int t = 0; t < 6; ++t) col[t] = h < 2 ? B[(6 * h + t) * 12 + j] : 0.0;
+  // The pivot loop stays rolled (the code stays small); the rows are unrolled so that they
+  // live in registers, and the updates are branch-free so that the rows' shuffles overlap.
+#pragma unroll 1
+  for (int k = 0; k < 12; ++k) {
+    const int hk = k / 6, tk = k % 6;
+    double ck = 0.0;  // this lane's entry of row k (meaningful in half hk)
+#pragma unroll
+    for (int t = 0; t < 6; ++t)
+      if (t == tk) ck = col[t];
+    const double ip = 1.0 / __shfl_sync(0xffffffffu, ck, k + 12 * hk);
+    const double rk = __shfl_sync(0xffffffffu, ck, j + 12 * hk);  // K[k][j]
+    const double pk = (j == k ? 1.0 : rk) * ip;                     // row k scaled
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      const double f = __shfl_sync(0xffffffffu, col[t], k + 12 * h);  // K[6h + t][k]
+      const double base = j == k ? 0.0 : col[t];
+      const double upd = base - f * pk;
+      col[t] = (h == hk && t == tk) ? pk : (f != 0.0 ? upd : base);
+    }
+  }
+  if (h < 2) {
+    double* out = a.cl_inv + a.cl_off[c];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) out[(6 * h + t) * 12 + j] = col[t];
+  }
+}
+
+// use_hc: CTA 0 also sets the condition of the IF node around k_cluster_inverse (a
+// device-loop step): 1 when a cluster has more than one body
+__global__ void __launch_bounds__(WIT) k_cluster_inverse_small(SolverArgs a, cudaGraphConditionalHandle hc,
+                                                               int use_hc) {
+  const int ncl = *a.ncl_dev;
+  if (use_hc && blockIdx.x == 0) {
+    int big = 0;
+    for (int c = threadIdx.x; c < ncl && !big; c += WIT) big = a.cl_ptr[c + 1] - a.cl_ptr[c] > 1;
+    big = __syncthreads_or(big);
+    if (threadIdx.x == 0) cudaGraphSetConditional(hc, big ? 1u : 0u);
+  }
+  const int lane = (int)(threadIdx.x & 31);
+  const int nw = gridDim.x * (WIT / 32);
+  for (int c = (int)((blockIdx.x * WIT + threadIdx.x) >> 5); c < ncl; c += nw) {
+    const int base = a.cl_ptr[c];
+    if (a.cl_ptr[c + 1] - base == 1) warp_inverse1(a, c, a.cl_body[base], lane);
+  }
+}
+
+// Clusters of two bodies or more: one CTA each, the system in shared memory.
 constexpr int kInvGrid = 148;  // CTAs of the inverse kernel (one per SM at the largest clusters)
 __global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, const int* body_cl) {
   extern __shared__ double K[];
   const int ncl = *a.ncl_dev;
   for (int c = blockIdx.x; c < ncl; c += gridDim.x) {
     const int base = a.cl_ptr[c], s = a.cl_ptr[c + 1] - base, D = 12 * s;
+    if (s == 1) continue;  // k_cluster_inverse_small's
     for (int e = threadIdx.x; e < D * D; e += IT) K[e] = 0.0;
     __syncthreads();
     // block row of every member: its diagonal block and the blocks of active pairs whose
@@ -691,20 +755,41 @@ cudaError_t cluster_tables(Sim& s, cudaStream_t st) {
 }
 
 // Inverts every cluster's dense system (the tables k_clusters made; their count is read on the
-// device): a fixed grid, the shared memory of the largest cluster cluster_max allows.  Enqueued
-// without a sync.
+// device): clusters of one body a warp each, larger ones (when cluster_max allows them) a CTA
+// each with the shared memory of the largest.  Fixed grids; enqueued without a sync.
 int cluster_inverse(Sim& s) {
   SolverArgs a = solver_args(s);
   const int cm = s.prm.precond == 1 ? std::max(1, std::min(kMaxCluster, s.prm.cluster_max)) : 1;
-  const size_t smem = sizeof(double) * 144 * (size_t)cm * cm;
-  if (smem > 48 * 1024 && (int)smem > s.cl_smem) {
-    if (cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-      return ABD_ERR_CUDA;
-    s.cl_smem = (int)smem;
-  }
-  k_cluster_inverse<<<kInvGrid, IT, smem, s.stream>>>(a, s.body_cl);
+  // a device-loop step (in_device_loop, under capture) puts the CTA kernel in an IF node:
+  // most Newton iterations of a resting pile have no cluster of more than one body
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (ABD_NOTE(cudaStreamIsCapturing(s.stream, &cs)) != cudaSuccess) return ABD_ERR_CUDA;
+  const bool use_if = cm > 1 && s.in_device_loop && cs == cudaStreamCaptureStatusActive;
+  cudaGraphConditionalHandle hc = 0;
+  if (use_if && make_handle(s.stream, &hc) != ABD_OK) return ABD_ERR_CUDA;
+  k_cluster_inverse_small<<<kWarpInvGrid, WIT, 0, s.stream>>>(a, hc, use_if ? 1 : 0);
   ++s.launches;
+  if (cm > 1) {
+    const size_t smem = sizeof(double) * 144 * (size_t)cm * cm;
+    if (smem > 48 * 1024 && (int)smem > s.cl_smem) {
+      if (cudaFuncSetAttribute(k_cluster_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+        return ABD_ERR_CUDA;
+      s.cl_smem = (int)smem;
+    }
+    if (use_if) {  // the body's kernel is not counted among the launches (it runs now and then)
+      cudaGraph_t body = nullptr;
+      if (int r = add_conditional(s.stream, hc, cudaGraphCondTypeIf, &body)) return r;
+      if (int r = capture_body(s, body, s.cap_stream5, [&]() -> int {
+            k_cluster_inverse<<<kInvGrid, IT, smem, s.stream>>>(a, s.body_cl);
+            return ABD_NOTE(cudaGetLastError()) == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+          }))
+        return r;
+    } else {
+      k_cluster_inverse<<<kInvGrid, IT, smem, s.stream>>>(a, s.body_cl);
+      ++s.launches;
+    }
+  }
   return cudaGetLastError() == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
 }
 
