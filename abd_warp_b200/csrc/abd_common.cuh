@@ -429,7 +429,7 @@ constexpr int kRedSlots = 12;
 constexpr int kLsMax = 16;        // line-search trials evaluated per batch
 constexpr int kSupHave = 1;       // dint slots (see Sim::dint)
 constexpr int kSupValid = 2;
-constexpr int kSlice = 64;        // vertices per slice of the line-search bounds (two per lane)
+constexpr int kSlice = 96;        // vertices per warp of k_vertex_broad (three per lane)
 constexpr int kParK = 4;          // dpar slot of a batch's trial count
 constexpr int kParAlpha = 5;      // dpar slots of its step lengths
 constexpr int kParAcc = kParAlpha + kLsMax;  // dpar slot of the accepted step length

@@ -66,14 +66,14 @@ __device__ inline unsigned long long warp_max_key(unsigned long long key) {
   return ((unsigned long long)hm << 32) | lm;
 }
 
-// One warp per vertex slice (at most kSlice = 64 vertices of one body, two per lane):
+// One warp per vertex slice (at most kSlice vertices of one body, kSlice / 32 per lane):
 // y0 = x(d[0]) (and y1 = x(d[1])) with the arithmetic of k_transform, and the body bounds:
 // each lane takes the min / max of its vertices' coordinates, the warp reduces their
 // order-preserving keys (the maximum key is the exact min / max) and lane 0 updates the
 // body's keys atomically.  Then one thread per body: the body's DOFs of each set (written
 // out when updated, and as FP32 copies for the traversal's node boxes).  Block 0 clears the
 // pass's accumulators.
-__global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
+__global__ void __launch_bounds__(256, 4) k_vertex_broad(VertexArgs a) {
   const int w = (int)((blockIdx.x * 256 + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (blockIdx.x == 0) {
     if (threadIdx.x <= kXD) reinterpret_cast<long long*>(&a.box->energy)[threadIdx.x] = 0;
@@ -85,12 +85,15 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
   if (w < a.nslice) {
     const int4 sl = a.slice[w];  // body, first vertex, vertices
     const int b = sl.x;
-    const bool has[2] = {lane < sl.z, lane + 32 < sl.z};
-    double r[2][3];
+    constexpr int VPL = kSlice / 32;
+    bool has[VPL];
+    double r[VPL][3];
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+    for (int h = 0; h < VPL; ++h) {
+      has[h] = lane + 32 * h < sl.z;
 #pragma unroll
       for (int j = 0; j < 3; ++j) r[h][j] = has[h] ? a.x0[3 * (sl.y + lane + 32 * h) + j] : 0.0;
+    }
     for (int k = 0; k < nset; ++k) {
       double M[12];
       body_dofs(a.d[k], b, M);
@@ -100,7 +103,7 @@ __global__ void __launch_bounds__(256) k_vertex_broad(VertexArgs a) {
       for (int j = 0; j < 3; ++j) {
         double lo = INFINITY, hi = -INFINITY;
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < VPL; ++h)
           if (has[h]) {
             const double c = xform(M, r[h][0], r[h][1], r[h][2], j);
             y[3 * (sl.y + lane + 32 * h) + j] = c;
@@ -158,53 +161,66 @@ __global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double d
 // ---------------------------------------------------------------------------------------
 // body pairs: overlap bit matrix, per-row prefix counts, then O(1) placement of every pair
 // ---------------------------------------------------------------------------------------
-constexpr int PR_THREADS = 512;  // one warp per row of the overlap matrix
-constexpr int PR_TILE = 1024;    // body boxes staged in shared memory per tile (32 KB)
+constexpr int PR_THREADS = 128;  // one CTA per row of the overlap matrix, its 4 warps share the words
+constexpr int PR_WORDS = 128;    // words of a row per round (one scan)
 
-// Row I of the overlap matrix, one warp: lane l tests J = 32 w + l and the ballot is word w
-// (word w covers J in [32w, 32w + 32)).  The warp also keeps the per-row exclusive prefix
-// of the word popcounts (wpre), the row counts -- all neighbours (rcnt) and neighbours J > I
-// (ucnt) -- and the first kNbList neighbours in increasing order (nbr).
+// Row I of the overlap matrix, one CTA: word w (J in [32 w, 32 w + 32)) is one warp's ballot
+// of the box tests of its lanes (lane l tests J = 32 w + l, a coalesced load of the boxes),
+// the CTA's warps taking the row's words in turn.  A block scan of the words' popcounts gives
+// the per-row exclusive prefix (wpre); the CTA also writes the row counts -- all neighbours
+// (rcnt) and neighbours J > I (ucnt) -- and the first kNbList neighbours in increasing order
+// (nbr).
 __global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const Box* __restrict__ body_box,
                                                           uint32_t* mask, int* wpre, int* rcnt, int* ucnt,
                                                           int* nbr) {
-  __shared__ float4 tile[2 * PR_TILE];
-  const int I = (int)((blockIdx.x * (unsigned)PR_THREADS + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  const bool row = I < n;
-  const Box a = row ? load_box(&body_box[I]) : Box{};
-  const float4* src = reinterpret_cast<const float4*>(body_box);
-  int pre = 0, low = 0;
-  for (int j0 = 0; j0 < n; j0 += PR_TILE) {
-    const int jn = min(PR_TILE, n - j0);
-    __syncthreads();
-    for (int k = threadIdx.x; k < 2 * jn; k += PR_THREADS) tile[k] = __ldg(&src[2 * (size_t)j0 + k]);
-    __syncthreads();
-    if (!row) continue;
-    for (int wl = 0; wl < (jn + 31) / 32; ++wl) {
-      const int jl = 32 * wl + lane, J = j0 + jl;
-      bool hit = false;
-      if (jl < jn && J != I) {
-        const float4 lo = tile[2 * jl], hi = tile[2 * jl + 1];
-        hit = !(a.lo[0] > hi.x || lo.x > a.hi[0] || a.lo[1] > hi.y || lo.y > a.hi[1] || a.lo[2] > hi.z ||
-                lo.z > a.hi[2]);
-      }
+  __shared__ uint32_t sb[PR_WORDS];
+  __shared__ int wsum[PR_THREADS / 32];
+  __shared__ int slow;
+  const int I = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const Box a = load_box(&body_box[I]);
+  if (tid == 0) slow = 0;
+  int carry = 0;
+  for (int w0 = 0; w0 < W; w0 += PR_WORDS) {
+    const int nw = min(PR_WORDS, W - w0);
+#pragma unroll 4
+    for (int wl = warp; wl < nw; wl += PR_THREADS / 32) {
+      const int J = 32 * (w0 + wl) + lane;
+      const bool hit = J < n && J != I && overlap(a, load_box(&body_box[J]));
       const uint32_t bits = __ballot_sync(0xffffffffu, hit);
-      const int w = (j0 >> 5) + wl;
-      if (lane == 0) {
-        mask[(size_t)I * W + w] = bits;
-        wpre[(size_t)I * W + w] = pre;
-      }
-      if (hit) {
-        const int pos = pre + __popc(bits & ((1u << lane) - 1u));
-        if (pos < kNbList) nbr[(size_t)I * kNbList + pos] = J;
-      }
-      if (w == (I >> 5)) low = pre + __popc(bits & ((1u << (I & 31)) - 1u));
-      pre += __popc(bits);
+      if (lane == 0) sb[wl] = bits;
     }
+    __syncthreads();
+    // exclusive scan of the words' popcounts (thread t: word w0 + t)
+    const uint32_t bits = tid < nw ? sb[tid] : 0u;
+    const int pc = __popc(bits);
+    int incl = pc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int before = 0, total = 0;
+#pragma unroll
+    for (int k = 0; k < PR_THREADS / 32; ++k) {
+      before += k < warp ? wsum[k] : 0;
+      total += wsum[k];
+    }
+    if (tid < nw) {
+      const int w = w0 + tid, pre = carry + before + incl - pc;
+      mask[(size_t)I * W + w] = bits;
+      wpre[(size_t)I * W + w] = pre;
+      for (uint32_t m = bits; m && pre + (pc - __popc(m)) < kNbList; m &= m - 1)
+        nbr[(size_t)I * kNbList + pre + (pc - __popc(m))] = 32 * w + __ffs(m) - 1;
+      if (w == (I >> 5)) slow = pre + __popc(bits & ((1u << (I & 31)) - 1u));
+    }
+    carry += total;
+    __syncthreads();  // sb and wsum are reused
   }
-  if (row && lane == 0) {
-    rcnt[I] = pre;
-    ucnt[I] = pre - low;  // bit I itself is never set
+  if (tid == 0) {
+    rcnt[I] = carry;
+    ucnt[I] = carry - slow;  // bit I itself is never set
   }
 }
 
@@ -577,7 +593,7 @@ cudaError_t body_pairs(Sim& s, bool full, bool sup) {
   const int n = s.n, W = s.W;
   k_body_boxes<<<blocks(n, 128), 128, 0, s.stream>>>(n, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box,
                                                      s.body_rest, s.fdof, sup ? s.body_sup : nullptr);
-  k_pair_mask<<<blocks(32LL * n, PR_THREADS), PR_THREADS, 0, s.stream>>>(n, W, sup ? s.body_sup : s.body_box,
+  k_pair_mask<<<n, PR_THREADS, 0, s.stream>>>(n, W, sup ? s.body_sup : s.body_box,
                                                                          s.pair_mask, s.pair_wpre, s.row_cnt,
                                                                          s.upper_cnt, s.nbr);
   s.launches += 2;

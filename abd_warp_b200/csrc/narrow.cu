@@ -660,7 +660,8 @@ __device__ inline void toi_min(unsigned long long* key, double t) {
 // ---------------------------------------------------------------------------------------
 // energy / CCD passes: one CTA per chunk of one body's points and edges
 // ---------------------------------------------------------------------------------------
-constexpr int CT = kChunk;  // threads per chunk CTA
+constexpr int CT = 128;  // threads per chunk CTA
+static_assert(kChunk <= CT && kChunk <= 256, "a chunk's queries: one thread each when loaded, 8-bit ids");
 constexpr int kNoQuery = INT_MIN;  // a chunk item whose primitive kind is disabled
 constexpr int NBB = 64;     // neighbours staged per batch
 
@@ -680,10 +681,13 @@ __device__ inline int kth_neighbour(const NarrowArgs& a, int I, int k) {
 }
 
 // Which body of a pair {I, J} queries the other's edge tree for the EE candidates: the one
-// with more edges (ties: the higher index), so that a body with few edges and many
-// neighbours (a ground box) does not serialise them.  The candidate set does not depend on
-// the choice (the box predicate is symmetric).
-__device__ inline bool ee_owner(int I, int nEI, int J, int nEJ) { return nEI > nEJ || (nEI == nEJ && I > J); }
+// with more edges; at equal edge counts the one with fewer neighbours (dI, dJ: the pass's row
+// counts), then the higher index.  A body with many neighbours (a ground box among cubes of
+// as many edges) would otherwise query every neighbour's tree from its one chunk, in series.
+// The candidate set does not depend on the choice (the box predicate is symmetric).
+__device__ inline bool ee_owner(int I, int nEI, int dI, int J, int nEJ, int dJ) {
+  return nEI > nEJ || (nEI == nEJ && (dI < dJ || (dI == dJ && I > J)));
+}
 
 // Body I's points against the triangle trees of all its neighbours J (PT pairs (I, J); the
 // pairs (J, I) come from J's chunks), and its edges against the edge trees of the neighbours
@@ -742,7 +746,7 @@ __global__ void __launch_bounds__(KA) k_chunk_active(NarrowArgs a) {
   const int I = ch.x;
   const int nEI = a.eoff[I + 1] - a.eoff[I];
   const int nV = a.voff[I + 1] - a.voff[I];
-  const int Q = max(0, min(CT, nV + nEI - ch.y));
+  const int Q = max(0, min(kChunk, nV + nEI - ch.y));
   bool need = !gh && ch.y == 0 && (!ccd || (a.prm.ground_enabled && a.prm.enable_vg));
   int r0 = 0, deg;
   if constexpr (gh) {
@@ -789,9 +793,9 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   const int I = ch.x;
   const int nEI = a.eoff[I + 1] - a.eoff[I];
   const int nV = a.voff[I + 1] - a.voff[I];  // items: the body's points, then its edges
-  const int Q = max(0, min(CT, nV + nEI - ch.y));
-  __shared__ Box qbox[CT];  // query boxes (CCD_LS: over the DOF range)
-  __shared__ int qprim[CT];  // point id, ~edge id, or kNoQuery (primitive kind disabled)
+  const int Q = max(0, min(kChunk, nV + nEI - ch.y));
+  __shared__ Box qbox[kChunk];  // query boxes (CCD_LS: over the DOF range)
+  __shared__ int qprim[kChunk];  // point id, ~edge id, or kNoQuery (primitive kind disabled)
   __shared__ Box nbox[NBB];
   __shared__ __align__(16) float ndof[NBB][24];
   __shared__ int nJ[NBB], ntri[NBB], nedge[NBB], nown[NBB], npair[NBB], nrel[NBB];
@@ -880,17 +884,31 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
   for (int b0 = 0; b0 < deg; b0 += NBB) {
     const int nb = min(NBB, deg - b0);
     __syncthreads();
+    // ENERGY / CCD past the listed neighbours: the CTA decodes the batch from the row's overlap
+    // words (their prefix counts place each word's bits), one round of loads for the batch
+    const bool decode = !gh && b0 + nb > kNbList;
+    if (decode) {
+      for (int w = tid; w < a.W; w += CT) {
+        const int pre = a.pair_wpre[(size_t)I * a.W + w];
+        if (pre >= b0 + nb) continue;
+        uint32_t m = a.pair_mask[(size_t)I * a.W + w];
+        if (pre + __popc(m) <= b0) continue;
+        for (int k = pre; m; m &= m - 1, ++k)
+          if (k >= b0 && k < b0 + nb) nJ[k - b0] = 32 * w + __ffs(m) - 1;
+      }
+      __syncthreads();
+    }
     int rel = 0;
     if (tid < nb) {
       const int k = b0 + tid;
-      const int J = gh ? a.adj_col[r0 + k] : (k < kNbList ? a.nbr[(size_t)I * kNbList + k] : kth_neighbour(a, I, k));
+      const int J = gh ? a.adj_col[r0 + k] : (decode ? nJ[tid] : a.nbr[(size_t)I * kNbList + k]);
       nJ[tid] = J;
       nbox[tid] = load_box(&(ls ? a.body_sup : a.body_box)[J]);
       rel = overlap(cbx, nbox[tid]) ? 1 : 0;
       nrel[tid] = rel;
       ntri[tid] = a.tri.body_root[J];
       nedge[tid] = a.edge.body_root[J];
-      nown[tid] = ee_owner(I, nEI, J, a.eoff[J + 1] - a.eoff[J]);
+      nown[tid] = ee_owner(I, nEI, a.row_cnt[I], J, a.eoff[J + 1] - a.eoff[J], a.row_cnt[J]);
       if (gh) npair[tid] = a.adj_pair[r0 + b0 + tid];
     }
     if (!__syncthreads_or(rel)) continue;  // the chunk touches none of these neighbours
