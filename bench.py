@@ -56,6 +56,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "ABD steps/s vs plain FP64 on same B200 at \u22641e-6 rel pos err; adjoint grads/s"
 WORKLOAD = "pile of 1024 bodies (512 cubes + 512 level-3 icospheres) on a ground box, 300-step trajectory"
+# DRAM bytes (read + write) per launch of k_chunk_narrow<CCD_LS> over the algorithmic bytes of
+# the same launches, measured by ncu over the 20-step schedule (5 steps from each stored state,
+# 176 launches, cold cache): 10.170 MB against 13.742 MB.  Below 1: tree nodes that several
+# queries visit hit in L2.
+NARROW_DRAM_PER_ALG_BYTE = 0.740
 STATES = os.path.join(ROOT, "tests", "golden", "c2_states.npz")
 STARTS = (0, 75, 150, 225)  # trajectory steps of the stored states
 
@@ -491,7 +496,10 @@ def main():
                                "the line-search candidates)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "traffic": None,
+                     "traffic": bytes_per_launch * NARROW_DRAM_PER_ALG_BYTE,
+                     "traffic_how": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch over the "
+                                    "20-step schedule, as a ratio to the kernel's algorithmic bytes "
+                                    f"({NARROW_DRAM_PER_ALG_BYTE}), times this run's algorithmic bytes",
                      "peak_kind": peak_kind, "timed_launches": k_launches, "counted_launches": c_launches,
                      "avg_launch_us": us_per_launch, "bytes_per_launch": bytes_per_launch},
     }
