@@ -589,9 +589,9 @@ cudaError_t krylov_tally(Sim& s);
 // newton_loop is 0).  Each enqueues on s.stream.
 cudaError_t step_begin(Sim& s, cudaGraphConditionalHandle h);
 cudaError_t gate_no_overflow(Sim& s, cudaGraphConditionalHandle h);
-cudaError_t after_gh(Sim& s);
 cudaError_t ls_accept(Sim& s);
-cudaError_t update_dofs_dev(Sim& s, double* A, double* p);
+// (A, p) -= alpha dq with the accepted alpha on the device; also into (Ak, pk)
+cudaError_t update_dofs_dev(Sim& s, double* A, double* p, double* Ak, double* pk);
 cudaError_t newton_end(Sim& s, cudaGraphConditionalHandle h);
 cudaError_t finish_step_dev(Sim& s, const abd_states& st, double* xview);
 // the adjoint step (abd_adjoint_step): its right-hand side into g, its outputs from lambda

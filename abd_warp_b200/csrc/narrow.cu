@@ -1432,17 +1432,27 @@ __global__ void k_export_off(int np, const int* pair_active, const int* fixed, c
   }
 }
 
+// (Ao, po) = (A, p) - alpha dq (alpha_dev: the step length on the device); also into (Ao2, po2)
+// when given
 __global__ void k_update_dofs(int n, const double* A, const double* p, const double* dq, double alpha, double* Ao,
-                              double* po, const double* alpha_dev) {
+                              double* po, const double* alpha_dev, double* Ao2, double* po2) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   if (alpha_dev) alpha = *alpha_dev;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) po[3 * b + k] = p[3 * b + k] - dq[12 * b + k] * alpha;
+  for (int k = 0; k < 3; ++k) {
+    const double v = p[3 * b + k] - dq[12 * b + k] * alpha;
+    po[3 * b + k] = v;
+    if (po2) po2[3 * b + k] = v;
+  }
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) Ao[9 * b + 3 * r + k] = A[9 * b + 3 * r + k] - dq[12 * b + 3 * (r + 1) + k] * alpha;
+    for (int k = 0; k < 3; ++k) {
+      const double v = A[9 * b + 3 * r + k] - dq[12 * b + 3 * (r + 1) + k] * alpha;
+      Ao[9 * b + 3 * r + k] = v;
+      if (Ao2) Ao2[9 * b + 3 * r + k] = v;
+    }
 }
 
 __global__ void k_finish(int n, double dt, abd_states st) {
@@ -1755,13 +1765,13 @@ cudaError_t export_system(Sim& s, double* off_dev, int* ij_dev, int cap) {
 
 cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* dq, double alpha, double* Aout,
                         double* pout) {
-  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, dq, alpha, Aout, pout, nullptr);
+  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, dq, alpha, Aout, pout, nullptr, nullptr, nullptr);
   ++s.launches;
   return cudaGetLastError();
 }
 
-cudaError_t update_dofs_dev(Sim& s, double* A, double* p) {
-  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, s.dq, 0.0, A, p, s.dpar + kParAcc);
+cudaError_t update_dofs_dev(Sim& s, double* A, double* p, double* Ak, double* pk) {
+  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, s.dq, 0.0, A, p, s.dpar + kParAcc, Ak, pk);
   ++s.launches;
   return cudaGetLastError();
 }

@@ -41,17 +41,16 @@ __global__ void k_step_begin(Mailbox* box, cudaGraphConditionalHandle h) {
   cudaGraphSetConditional(h, 1u);
 }
 
-// the IF node after the GH pass: taken unless a list of the pass overflowed
-__global__ void k_gate(const Mailbox* box, cudaGraphConditionalHandle h) {
-  cudaGraphSetConditional(h, (box->dstat[DS_STATUS] & kRerunMask) ? 0u : 1u);
-}
-
-// After the GH pass: the active contacts of the iteration; at the first iteration the energy
-// at q0 (the pass summed it: abd.py:126-128), the culling counts, and the kept line-search
-// candidates are consumed (the step's CCD passes replace them)
-__global__ void k_after_gh(Mailbox* box, int* sup_have) {
-  StepDev& S = box->step;
+// The IF node after the GH pass: taken unless a list of the pass overflowed.  When it is
+// taken, also the pass's outcome for the step: the active contacts of the iteration; at the
+// first iteration the energy at q0 (the pass summed it: abd.py:126-128), the culling counts,
+// and the kept line-search candidates are consumed (the step's CCD passes replace them).
+__global__ void k_gate(Mailbox* box, cudaGraphConditionalHandle h, int* sup_have) {
   const int* ds = box->dstat;
+  const bool ok = !(ds[DS_STATUS] & kRerunMask);
+  cudaGraphSetConditional(h, ok ? 1u : 0u);
+  if (!ok) return;
+  StepDev& S = box->step;
   S.n_active = ds[DS_ACTIVE];
   if (S.it == 0) {
     S.E0 = xs_round(box->energy);
@@ -160,13 +159,7 @@ cudaError_t step_begin(Sim& s, cudaGraphConditionalHandle h) {
 }
 
 cudaError_t gate_no_overflow(Sim& s, cudaGraphConditionalHandle h) {
-  k_gate<<<1, 1, 0, s.stream>>>(s.box, h);
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t after_gh(Sim& s) {
-  k_after_gh<<<1, 1, 0, s.stream>>>(s.box, s.dint + kSupHave);
+  k_gate<<<1, 1, 0, s.stream>>>(s.box, h, s.dint + kSupHave);
   ++s.launches;
   return cudaGetLastError();
 }

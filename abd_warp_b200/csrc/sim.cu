@@ -1196,7 +1196,6 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
     return ABD_OK;
   };
   auto iteration_tail = [&]() -> int {  // after a GH pass without overflow (the IF body)
-    CK(abd::after_gh(s));
     if (int r = abd::cluster_inverse(s)) return r;
     if (int r = abd::krylov_issue(s, s.dq)) return r;
     CK(abd::krylov_tally(s));
@@ -1207,9 +1206,7 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
     CK(abd::ls_setup_from_ccd(s));
     CK(abd::ls_energies(s, st, st.A, st.p));
     CK(abd::ls_accept(s));
-    CK(abd::update_dofs_dev(s, st.A, st.p));
-    CK(cudaMemcpyAsync(st.Ak, st.A, nA, cudaMemcpyDeviceToDevice, s.stream));
-    CK(cudaMemcpyAsync(st.pk, st.p, np, cudaMemcpyDeviceToDevice, s.stream));
+    CK(abd::update_dofs_dev(s, st.A, st.p, st.Ak, st.pk));
     return ABD_OK;
   };
   const cudaStream_t top = s.stream;
