@@ -18,7 +18,7 @@ ABD_ERR_CUDA, ABD_ERR_INVALID, ABD_ERR_OVERFLOW, ABD_ERR_DEVICE = 1, 2, 3, 4  # 
 STATUS_NAMES = {1: "pt_overflow", 2: "ee_overflow", 4: "pair_overflow", 8: "stack_overflow",
                 16: "solver_not_converged", 32: "nan", 64: "vg_overflow", 128: "active_pair_overflow",
                 256: "contact_overflow", 512: "ccd_overflow", 1024: "ls_candidate_overflow",
-                2048: "line_search_needs_more_trials"}
+                2048: "line_search_needs_more_trials", 4096: "friction_contact_overflow"}
 ST_STACK_OVERFLOW, ST_SOLVER_NOCONV, ST_NAN = 8, 16, 32
 
 c_int, c_double, c_void_p, c_longlong = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong

@@ -35,10 +35,12 @@ enum : int {
   ST_CCD_OVERFLOW = 512,   // CCD candidate list capacity exceeded (host grows and reruns)
   ST_ECAND_OVERFLOW = 1024,  // line-search candidate list capacity exceeded (grow and rerun)
   ST_LS_MORE = 2048,       // a line search needs more trials than one batch (the host finishes)
+  ST_FRIC_OVERFLOW = 4096, // lagged friction contact capacity exceeded (host grows and reruns)
 };
 // the status bits after which the device-driven Newton loop stops and the host reruns the step
 constexpr int kRerunMask = ST_PT_OVERFLOW | ST_EE_OVERFLOW | ST_PAIR_OVERFLOW | ST_VG_OVERFLOW | ST_ACT_OVERFLOW |
-                           ST_CONTACT_OVERFLOW | ST_CCD_OVERFLOW | ST_ECAND_OVERFLOW | ST_LS_MORE;
+                           ST_CONTACT_OVERFLOW | ST_CCD_OVERFLOW | ST_ECAND_OVERFLOW | ST_LS_MORE |
+                           ST_FRIC_OVERFLOW;
 
 constexpr int kTraversalStack = 64;
 constexpr int kNoChild = (int)0x80000000;  // unused slot of a node's child table
@@ -221,6 +223,16 @@ inline ClusterWork cluster_work_at(void* base, int n) {
   return w;
 }
 
+// A lagged friction contact: the step start's closest-point weights w, tangent basis P (3x2,
+// row-major) and normal force lam, the four points there (xt) and their vertex ids; the first
+// group (the point; edge a) moves with body I.
+struct FricRec {
+  double w[4], P[6], lam;
+  double xt[12];
+  int ids[4];
+  int I, J, kind, pad;
+};
+
 // one captured pass (see abd_graph.cuh)
 struct GraphSlot {
   cudaGraphExec_t exec = nullptr;
@@ -273,6 +285,13 @@ struct Sim {
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
   int* chunk_act = nullptr;        // [nch + 1] the chunks of a narrow pass with work, then their count
+  // lagged friction (friction_mu > 0): the step's contacts, and its body pairs as bits of the
+  // overlap matrix that every GH pass of the step adds; fric_lag: the host loop's first GH pass
+  // of a step (the device loop lags at its first Newton iteration)
+  FricRec* fric = nullptr;
+  int cap_fric = 0;
+  uint32_t* fric_mask = nullptr;   // [n][W]
+  int fric_lag = 0;
   Box* chunk_box = nullptr;        // [nch] rest-frame box of each chunk's items
   int* vperm = nullptr;            // [V] vertices of each body in Morton order (chunk items)
   // vertex slices of the line-search bounds: (body, first vertex, count), count <= kSlice
@@ -451,8 +470,10 @@ enum : int {
   DS_IT = 13,        // Krylov iteration counter (device-side, for replayed blocks)
   DS_NCCD = 14,      // CCD candidates appended by the CCD pass
   DS_NECAND = 15,    // line-search candidates appended by the CCD pass
-  DS_NSLOTS = 16
+  DS_NFRIC = 16,     // lagged friction contacts of the step (its first GH pass appends them)
+  DS_NSLOTS = 17
 };
+
 
 // Counters of a time step run as a device loop (the step info, kept on the device), and the
 // kernel timing of the CCD pass's narrow kernel by the GPU's global timer.
@@ -529,7 +550,8 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
 // body pairs: full (mask, scan, fill: the sorted pair list and the adjacency with pair
 // indices) or mask only (row counts and the bit matrix, all the energy and CCD passes need)
 // sup: cull with the boxes over every DOF set between the two of a swept pass (body_sup)
-cudaError_t body_pairs(Sim& s, bool full, bool sup = false);
+// forced: [n][W] bits added to the overlap matrix (the step's friction pairs), or null
+cudaError_t body_pairs(Sim& s, bool full, bool sup = false, const uint32_t* forced = nullptr);
 // rest-frame internal node boxes of both trees (once, at creation)
 cudaError_t rest_boxes(Sim& s);
 

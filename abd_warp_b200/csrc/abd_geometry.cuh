@@ -482,4 +482,13 @@ __device__ inline double collision_time(int type, const d3 a0[4], const d3 a1[4]
   return ok ? root : 1.0;
 }
 
+// the lagged quantities of a friction record, as the full-model header's type
+__device__ inline ipc::FrictionLag lag_of(const FricRec& f) {
+  ipc::FrictionLag L;
+  for (int k = 0; k < 4; ++k) L.w[k] = f.w[k];
+  for (int k = 0; k < 6; ++k) L.P[k] = f.P[k];
+  L.lambda = f.lam;
+  return L;
+}
+
 }  // namespace abd

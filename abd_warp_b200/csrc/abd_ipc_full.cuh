@@ -564,5 +564,17 @@ ABD_HD inline double friction_gh(const FrictionLag& L, const double x[12], const
   return c * f0;
 }
 
+// the friction potential alone, with friction_gh's arithmetic (the same value, bit for bit)
+ABD_HD inline double friction_d(const FrictionLag& L, const double x[12], const double xt[12], double mu, double eps) {
+  double dx[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 4; ++k)
+    for (int a = 0; a < 3; ++a) dx[a] += L.w[k] * (x[3 * k + a] - xt[3 * k + a]);
+  const double u0 = L.P[0] * dx[0] + L.P[2] * dx[1] + L.P[4] * dx[2];
+  const double u1 = L.P[1] * dx[0] + L.P[3] * dx[1] + L.P[5] * dx[2];
+  const double y = sqrt(u0 * u0 + u1 * u1), c = mu * L.lambda;
+  const double f0 = y >= eps ? y : -y * y * y / (3.0 * eps * eps) + y * y / eps + eps / 3.0;
+  return c * f0;
+}
+
 }  // namespace ipc
 }  // namespace abd

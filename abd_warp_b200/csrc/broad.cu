@@ -169,10 +169,10 @@ constexpr int PR_WORDS = 128;    // words of a row per round (one scan)
 // the CTA's warps taking the row's words in turn.  A block scan of the words' popcounts gives
 // the per-row exclusive prefix (wpre); the CTA also writes the row counts -- all neighbours
 // (rcnt) and neighbours J > I (ucnt) -- and the first kNbList neighbours in increasing order
-// (nbr).
+// (nbr).  forced (or null): bits added to the row (the step's friction pairs).
 __global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const Box* __restrict__ body_box,
-                                                          uint32_t* mask, int* wpre, int* rcnt, int* ucnt,
-                                                          int* nbr) {
+                                                          const uint32_t* __restrict__ forced, uint32_t* mask,
+                                                          int* wpre, int* rcnt, int* ucnt, int* nbr) {
   __shared__ uint32_t sb[PR_WORDS];
   __shared__ int wsum[PR_THREADS / 32];
   __shared__ int slow;
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(PR_THREADS) k_pair_mask(int n, int W, const Bo
       const int J = 32 * (w0 + wl) + lane;
       const bool hit = J < n && J != I && overlap(a, load_box(&body_box[J]));
       const uint32_t bits = __ballot_sync(0xffffffffu, hit);
-      if (lane == 0) sb[wl] = bits;
+      if (lane == 0) sb[wl] = forced ? bits | forced[(size_t)I * W + w0 + wl] : bits;
     }
     __syncthreads();
     // exclusive scan of the words' popcounts (thread t: word w0 + t)
@@ -589,13 +589,12 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
 // the pair index of {I, J}).  Counts stay on the device (dstat DS_NPAIRS / DS_NADJ); a short
 // capacity raises ST_PAIR_OVERFLOW and leaves the lists incomplete, for the host to grow and
 // rerun at its next read of dstat.
-cudaError_t body_pairs(Sim& s, bool full, bool sup) {
+cudaError_t body_pairs(Sim& s, bool full, bool sup, const uint32_t* forced) {
   const int n = s.n, W = s.W;
   k_body_boxes<<<blocks(n, 128), 128, 0, s.stream>>>(n, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box,
                                                      s.body_rest, s.fdof, sup ? s.body_sup : nullptr);
-  k_pair_mask<<<n, PR_THREADS, 0, s.stream>>>(n, W, sup ? s.body_sup : s.body_box,
-                                                                         s.pair_mask, s.pair_wpre, s.row_cnt,
-                                                                         s.upper_cnt, s.nbr);
+  k_pair_mask<<<n, PR_THREADS, 0, s.stream>>>(n, W, sup ? s.body_sup : s.body_box, forced, s.pair_mask,
+                                               s.pair_wpre, s.row_cnt, s.upper_cnt, s.nbr);
   s.launches += 2;
   if (full) {
     k_pair_scan<<<1, 1024, 0, s.stream>>>(n, s.row_cnt, s.upper_cnt, s.row_ptr, s.upper_ptr, s.cap_pairs, s.cap_adj,

@@ -49,6 +49,8 @@ struct LsArgs {
   int cap_ecand;
   const int* dstat;
   XSum* energy;                 // [kLsMax] exact energies of the trials
+  const FricRec* fric;          // the step's lagged friction contacts (null: friction off)
+  int cap_fric;
 };
 
 __device__ inline int ls_trials(const LsArgs& a) { return (int)a.dpar[kParK]; }
@@ -99,8 +101,9 @@ __device__ inline d3 position_at(const LsArgs& a, const double M[12], int v) {
 }
 
 // Trial blockIdx.y: blocks [0, G) evaluate the candidates, blocks [G, G + Gv) the
-// vertex-ground terms, the rest the bodies' inertia + orthogonality terms.
-__global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv) {
+// vertex-ground terms, blocks [G + Gv, G + Gv + Gf) the lagged friction contacts, the rest the
+// bodies' inertia + orthogonality terms.
+__global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv, int Gf) {
   const int k = blockIdx.y;
   if (k >= ls_trials(a)) return;
   const double al = a.dpar[kParAlpha + k];
@@ -170,9 +173,24 @@ __global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv) {
       const double e = barrier(d * d, a.prm);
       if (e != 0.0) xs_add_atomic(&acc, e);
     }
+  } else if (bx < G + Gv + Gf) {  // friction potentials at the trial's positions
+    const int nf = min(a.dstat[DS_NFRIC], a.cap_fric);
+    const double mu = a.prm.friction_mu, eps = a.prm.friction_epsv * a.prm.dt;
+    for (int i = (bx - G - Gv) * 128 + threadIdx.x; i < nf; i += Gf * 128) {
+      const FricRec& f = a.fric[i];
+      double x12[12];
+      for (int q = 0; q < 4; ++q) {
+        double M[12];
+        dofs_at(a.A, a.p, a.dq, __ldg(&a.vbody[f.ids[q]]), al, M);
+        const d3 y = position_at(a, M, f.ids[q]);
+        x12[3 * q] = y.x, x12[3 * q + 1] = y.y, x12[3 * q + 2] = y.z;
+      }
+      const double e = ipc::friction_d(lag_of(f), x12, f.xt, mu, eps);
+      if (e != 0.0) xs_add_atomic(&acc, e);
+    }
   } else {
     const int lane = threadIdx.x & 31;
-    const int t = (bx - G - Gv) * 128 + threadIdx.x;
+    const int t = (bx - G - Gv - Gf) * 128 + threadIdx.x;
     XSum r;
     xs_zero(r);
     if (t < a.n && !a.fixed[t]) {
@@ -251,10 +269,13 @@ cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const dou
   a.energy = s.box->ls_energy;
   cudaError_t e = cudaMemsetAsync(a.energy, 0, sizeof(XSum) * kLsMax, s.stream);
   if (e != cudaSuccess) return e;
+  a.fric = s.prm.friction_mu > 0.0 ? s.fric : nullptr;
+  a.cap_fric = s.cap_fric;
   const int G = kRedBlocks;
   const int Gv = (s.prm.ground_enabled && s.prm.enable_vg) ? kRedBlocks : 0;
+  const int Gf = a.fric ? 148 : 0;
   const int Gi = (int)blocks(s.n, 128);
-  k_ls_eval<<<dim3(G + Gv + Gi, kLsMax), 128, 0, s.stream>>>(a, G, Gv);
+  k_ls_eval<<<dim3(G + Gv + Gf + Gi, kLsMax), 128, 0, s.stream>>>(a, G, Gv, Gf);
   s.launches += 1;
   return cudaGetLastError();
 }

@@ -64,6 +64,11 @@ struct NarrowArgs {
   const int* sup_valid;         // GH: take the candidates from ecand instead of the traversal
   int cap_act;
   int4* act_pairs;              // GH: active pairs with their coupling weights (preconditioner)
+  FricRec* fric;                // lagged friction contacts (null: friction off)
+  int cap_fric;
+  uint32_t* fric_mask;          // their body pairs, as bits of the overlap matrix
+  int fric_lag;                 // GH: this pass fixes the step's friction contacts (gated by
+                                // energy_gate in the device loop: its first iteration)
   const Box* body_sup;          // CCD_LS: body boxes over every DOF set between the two
   const int* vbody;
   int cap_ecand;
@@ -89,6 +94,8 @@ struct NarrowArgs {
   double *offdiag, *pdiag, *pgrad, *pair_val;
   int* pair_active;
 };
+
+constexpr int kFricContact = 8;  // contact record y of a lagged friction contact (k_fric_pairs)
 
 // start bringing the line at p into L2
 __device__ inline void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
@@ -452,6 +459,8 @@ constexpr int PT_THREADS = 256;  // threads of the pair assembly (a warp per con
 // full: the contact's classified feature pair and the edge-edge mollifier (the full model;
 // else the reference's interior types); project: the PSD projection of the local Hessian
 // (Jacobi, by the warp's first lane) before the map.
+__device__ void affine_map_terms(const NarrowArgs& a, int type, int swap, const int ids[4], const double* h,
+                                 XSum* xred);
 __device__ void exact_contact_terms(const NarrowArgs& a, int type, int swap, const int ids[4], double* h,
                                     XSum* xred, bool full, bool project) {
   const int lane = threadIdx.x & 31;
@@ -487,6 +496,16 @@ __device__ void exact_contact_terms(const NarrowArgs& a, int type, int swap, con
   __syncwarp();
   if (project && lane == 0) ipc::project_psd12(h);
   __syncwarp();
+  affine_map_terms(a, type, swap, ids, h, xred);
+}
+
+// A contact's local gradient and Hessian h [156] (Hessian, then gradient, in the four points'
+// coordinates) as its 456 affine values, added to xred by the calling warp: vertices 0 .. nI-1
+// are the first group (the point; edge a), the rest the second; the group of side 0 (the
+// pair's first body) is the first unless swapped.
+__device__ void affine_map_terms(const NarrowArgs& a, int type, int swap, const int ids[4], const double* h,
+                                 XSum* xred) {
+  const int lane = threadIdx.x & 31;
   const int nI = type == 0 ? 1 : 2;
   auto side = [&](int v) { return (v < nI ? 0 : 1) ^ swap; };
   auto wt = [&](int v, int m) { return m == 0 ? 1.0 : __ldg(&a.x0[3 * ids[v] + (m - 1)]); };
@@ -542,6 +561,20 @@ __global__ void __launch_bounds__(PT_THREADS) k_pair_assemble(NarrowArgs a) {
     __syncthreads();
     for (int ci = warp; ci < cnt; ci += PT_WARPS) {
       const int4 rec = a.contacts_by_pair[off + ci];
+      if constexpr (EXACT) {
+        if (rec.y == kFricContact) {  // a lagged friction contact: its potential's exact terms
+          const FricRec& f = a.fric[rec.z];
+          if (lane == 0) {
+            double x12[12];
+            for (int q = 0; q < 12; ++q) x12[q] = a.y0[3 * f.ids[q / 3] + q % 3];
+            ipc::friction_gh(lag_of(f), x12, f.xt, a.prm.friction_mu, a.prm.friction_epsv * a.prm.dt, hloc + 144,
+                             hloc);
+          }
+          __syncwarp();
+          affine_map_terms(a, f.kind, f.I != a.ij[p].x ? 1 : 0, f.ids, hloc, xred);
+          continue;
+        }
+      }
       const int type = rec.y & 1, swap = rec.y >> 1;
       int ids[4];
       cand_vertices(a, type, rec.z, rec.w, ids);
@@ -1188,6 +1221,86 @@ __global__ void k_sup_check(int n, const double* A0, const double* p0, const dou
   }
 }
 
+// Lagged friction (friction_mu > 0, with the full model; Li et al. 2020, section 5): at the
+// step's first GH pass every contact within dhat fixes its lagged quantities (the header's
+// friction_lag at the step-start positions xs) and its body pair joins the step's pair lists;
+// returns the contact's friction potential there (mu lambda eps / 3: no displacement yet).
+__device__ inline double friction_lag_contact(const NarrowArgs& a, int kind, const int ids[4], const d3 xs[4]) {
+  double x12[12], r12[12];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    x12[3 * k] = xs[k].x, x12[3 * k + 1] = xs[k].y, x12[3 * k + 2] = xs[k].z;
+    for (int m = 0; m < 3; ++m) r12[3 * k + m] = __ldg(&a.x0[3 * ids[k] + m]);
+  }
+  ipc::FrictionLag L;
+  if (!ipc::friction_lag(kind, x12, r12, a.prm.d2hat, a.prm.kappa, SharedLog(), &L)) return 0.0;
+  const int I = __ldg(&a.vbody[ids[0]]), J = __ldg(&a.vbody[ids[kind == 0 ? 1 : 2]]);
+  const int pos = atomicAdd(&a.dstat[DS_NFRIC], 1);
+  if (pos < a.cap_fric) {
+    FricRec& f = a.fric[pos];
+    for (int k = 0; k < 4; ++k) f.w[k] = L.w[k];
+    for (int k = 0; k < 6; ++k) f.P[k] = L.P[k];
+    f.lam = L.lambda;
+    for (int k = 0; k < 12; ++k) f.xt[k] = x12[k];
+    for (int k = 0; k < 4; ++k) f.ids[k] = ids[k];
+    f.I = I;
+    f.J = J;
+    f.kind = kind;
+  } else {
+    atomicOr(&a.dstat[DS_STATUS], ST_FRIC_OVERFLOW);
+  }
+  if (I != J) {
+    atomicOr(&a.fric_mask[(size_t)I * a.W + (J >> 5)], 1u << (J & 31));
+    atomicOr(&a.fric_mask[(size_t)J * a.W + (I >> 5)], 1u << (I & 31));
+  }
+  return ipc::friction_d(L, x12, x12, a.prm.friction_mu, a.prm.friction_epsv * a.prm.dt);
+}
+
+// The friction contacts of the GH pass, one thread per lagged contact: each joins its body
+// pair's contact list (found in the adjacency) as a pseudo-contact (y = kFricContact, z = its
+// record); the pair assembly adds its friction terms to the pair's exact sums.  They are not
+// active contacts (DS_ACTIVE is compensated for the pair assembly's count).
+__global__ void __launch_bounds__(128) k_fric_pairs(NarrowArgs a) {
+  if (a.dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW | ST_FRIC_OVERFLOW)) return;
+  const int n = min(a.dstat[DS_NFRIC], a.cap_fric);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int I = a.fric[k].I, J = a.fric[k].J, lo = min(I, J), hi = max(I, J);
+    int pr = -1;
+    const int k1 = min(a.row_ptr[lo + 1], a.cap_adj);
+    for (int q = a.row_ptr[lo]; q < k1 && pr < 0; ++q)
+      if (a.adj_col[q] == hi) pr = a.adj_pair[q];
+    if (pr < 0) continue;
+    const int pos = atomicAdd(&a.dstat[DS_NCONTACT], 1);
+    if (pos < a.cap_contacts) a.contacts[pos] = make_int4(pr, kFricContact, k, 0);
+    else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
+    atomicAdd(&a.pair_cand[4 * pr + 1], 1);
+    atomicSub(&a.dstat[DS_ACTIVE], 1);
+  }
+}
+
+// The friction potential of every lagged contact at the pass's positions y0, into the pass's
+// exact energy (the energy pass), one thread per contact
+__global__ void __launch_bounds__(128) k_fric_energy(NarrowArgs a) {
+  const int n = min(a.dstat[DS_NFRIC], a.cap_fric);
+  XSum en;
+  xs_zero(en);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const FricRec& f = a.fric[k];
+    double x12[12];
+    for (int q = 0; q < 12; ++q) x12[q] = a.y0[3 * f.ids[q / 3] + q % 3];
+    const double e = ipc::friction_d(lag_of(f), x12, f.xt, a.prm.friction_mu, a.prm.friction_epsv * a.prm.dt);
+    if (e != 0.0) xs_add(en, e);
+  }
+  xs_warp_sum(en);
+  if ((threadIdx.x & 31) == 0) {
+    long long* d = reinterpret_cast<long long*>(a.energy);
+#pragma unroll
+    for (int i = 0; i < kXD; ++i)
+      if (en.d[i]) atomicAdd((unsigned long long*)&d[i], (unsigned long long)en.d[i]);
+    if (en.flags) atomicOr((unsigned long long*)&d[kXD], (unsigned long long)en.flags);
+  }
+}
+
 // Contacts of the GH pass's candidates, one thread per candidate: the active ones
 // (pt_ipc.py:13-22, 114; ee_ipc.py:13-23, 382) are appended for the per-pair assembly and
 // counted per pair; the candidates are counted per kind.  With gh_energy their barrier
@@ -1200,6 +1313,7 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
   XSum en;  // the candidates' barrier energy (ipcsk/energy.py:9-48)
   xs_zero(en);
   const bool with_energy = a.gh_energy && (!a.energy_gate || *a.energy_gate == 0);
+  const bool lag = a.fric_lag && (!a.energy_gate || *a.energy_gate == 0);  // the step's first GH pass
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const int4 c = a.ccd_cand[k];  // pair, type | swap << 1, primitive a, primitive b
     const int type = c.y & 1;
@@ -1221,6 +1335,10 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
       if (pos < a.cap_contacts) a.contacts[pos] = c;
       else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
       atomicAdd(&a.pair_cand[4 * c.x + 1], 1);
+      if (lag) {
+        const double e = friction_lag_contact(a, type, ids, xs);
+        if (with_energy && e != 0.0) xs_add(en, e);
+      }
     }
   }
 #pragma unroll
@@ -1548,6 +1666,11 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.sup_valid = s.dint + kSupValid;
   a.cap_act = s.cap_act;
   a.act_pairs = s.act_pairs;
+  const bool fr = s.prm.friction_mu > 0.0;
+  a.fric = fr ? s.fric : nullptr;
+  a.cap_fric = s.cap_fric;
+  a.fric_mask = fr ? s.fric_mask : nullptr;
+  a.fric_lag = fr ? (s.energy_gate ? 1 : s.fric_lag) : 0;
   a.vbody = s.vbody;
   a.cap_ecand = s.cap_ecand;
   a.ecand = s.ecand;
@@ -1642,6 +1765,10 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
     if (s.nch == 0) return cudaSuccess;
     if (mode == NARROW_ENERGY) {
       if (cudaError_t e = chunk_pass<NARROW_ENERGY>(s, a)) return e;
+      if (a.fric) {  // the friction potential of the step's lagged contacts
+        k_fric_energy<<<kRedBlocks, 128, 0, s.stream>>>(a);
+        ++s.launches;
+      }
     } else if (mode == NARROW_CCD || mode == NARROW_CCD_LS) {
       // DS_NCCD and DS_NECAND are adjacent
       static_assert(DS_NECAND == DS_NCCD + 1, "candidate counters");
@@ -1682,6 +1809,10 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       k_gh_scan<<<kRedBlocks, 128, 0, s.stream>>>(a);
       k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
       s.launches += 2;
+      if (a.fric) {
+        k_fric_pairs<<<kRedBlocks, 128, 0, s.stream>>>(a);
+        ++s.launches;
+      }
       k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
       k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
                                                                            s.contacts_by_pair, s.dstat);

@@ -162,6 +162,16 @@ int grow_contacts(Sim& s, int need) {
   return ABD_OK;
 }
 
+int grow_fric(Sim& s, int need) {
+  ++s.cap_gen;  // every captured pass is keyed on it
+  if (need <= s.cap_fric) return ABD_OK;
+  if (s.fric) cudaFree(s.fric);
+  s.fric = nullptr;
+  s.cap_fric = std::max(need + need / 2, 2 * s.cap_fric);
+  if (dalloc(&s.fric, s.cap_fric)) return ABD_ERR_OVERFLOW;
+  return ABD_OK;
+}
+
 int grow_ccd(Sim& s, int need) {
   ++s.cap_gen;  // every captured pass is keyed on it
   if (need <= s.cap_ccd) return ABD_OK;
@@ -218,7 +228,9 @@ int culling(abd_sim* h, const abd::Dofs* d0, const abd::Dofs* d1, double* y0, do
   if (d0) CK(abd::body_broad(s, d0, d1, y0, y1));
   else CK(abd::body_broad(s, nullptr, nullptr, nullptr, nullptr, y0, y1));
   const bool full = mode == abd::NARROW_GH || mode == abd::NARROW_LISTS;
-  CK(abd::body_pairs(s, full, mode == abd::NARROW_CCD_LS));
+  // the GH pass's pairs also hold the body pairs of the step's lagged friction contacts
+  const uint32_t* forced = mode == abd::NARROW_GH && s.prm.friction_mu > 0.0 ? s.fric_mask : nullptr;
+  CK(abd::body_pairs(s, full, mode == abd::NARROW_CCD_LS, forced));
   CK(abd::narrow(s, mode, d0 ? d0->Aeff() : nullptr, d0 ? d0->peff() : nullptr, d1 ? d1->Aeff() : nullptr,
                  d1 ? d1->peff() : nullptr, y0, y1, st));
   return ABD_OK;
@@ -262,7 +274,7 @@ int overflow(Sim& s) {
   const int bits = s.hstat[abd::DS_STATUS];
   const int mask = abd::ST_PAIR_OVERFLOW | abd::ST_PT_OVERFLOW | abd::ST_EE_OVERFLOW | abd::ST_VG_OVERFLOW |
                    abd::ST_ACT_OVERFLOW | abd::ST_CONTACT_OVERFLOW | abd::ST_CCD_OVERFLOW |
-                   abd::ST_ECAND_OVERFLOW;
+                   abd::ST_ECAND_OVERFLOW | abd::ST_FRIC_OVERFLOW;
   if (!(bits & mask)) return 0;
   int r = ABD_OK;
   if (bits & abd::ST_PAIR_OVERFLOW) r = grow_pairs(s, std::max(s.n_pairs, s.n_adj / 2 + 1));
@@ -279,6 +291,7 @@ int overflow(Sim& s) {
   if (!r && (bits & abd::ST_CONTACT_OVERFLOW)) r = grow_contacts(s, s.hstat[abd::DS_NCONTACT]);
   if (!r && (bits & abd::ST_CCD_OVERFLOW)) r = grow_ccd(s, s.hstat[abd::DS_NCCD]);
   if (!r && (bits & abd::ST_ECAND_OVERFLOW)) r = grow_ecand(s, s.hstat[abd::DS_NECAND]);
+  if (!r && (bits & abd::ST_FRIC_OVERFLOW)) r = grow_fric(s, s.hstat[abd::DS_NFRIC]);
   if (r) return r;
   const int clear = bits & ~mask;
   s.hstat[abd::DS_STATUS] = clear;
@@ -463,9 +476,19 @@ int ls_batch(abd_sim* h, const abd_states& st, const double* A, const double* p,
 // pass, which takes them from the kept line-search candidates when the step starts where the
 // last one ended; 2 a later Newton iteration's GH pass, which always does.
 // The kernels of a GH pass (no copy to the host)
+// The step's lagged friction contacts start empty (the first GH pass of a step fixes them)
+int clear_friction(Sim& s) {
+  if (!(s.prm.friction_mu > 0.0)) return ABD_OK;
+  CK(cudaMemsetAsync(s.fric_mask, 0, sizeof(uint32_t) * (size_t)s.n * s.W, s.stream));
+  CK(cudaMemsetAsync(s.dstat + abd::DS_NFRIC, 0, sizeof(int), s.stream));
+  return ABD_OK;
+}
+
 int gh_issue(abd_sim* h, const abd_states& st, const double* A, const double* p, int sup_mode) {
   Sim& s = h->s;
   const abd::Dofs d = direct(A, p);
+  if (s.fric_lag)  // the host loop's first GH pass of a step (a rerun of it starts over)
+    if (int r = clear_friction(s)) return r;
   CK(abd::gh_superset_check(s, &st, sup_mode));
   int r = culling(h, &d, nullptr, s.x, nullptr, abd::NARROW_GH);
   if (r) return r;
@@ -497,6 +520,7 @@ int gh_of(abd_sim* h, const abd_states& st, const double* A, const double* p, in
       k.add(s.pair_cand).add(s.offdiag).add(s.pdiag).add(s.pgrad).add(s.pair_active);
       k.add(s.cap_ccd).add(s.ccd_cand).add(s.gh_energy).add(sup_mode).add(s.q_last).add(s.dint);
       k.add(s.cap_ecand).add(s.ecand);  // k_gh_scan reads the kept line-search candidates
+      k.add(s.fric_lag);                 // the pass that fixes the step's friction contacts
       r = abd::run_graph(s, *g, k.h, issue);
     } else {
       r = issue();
@@ -548,9 +572,16 @@ const char* abd_status_string(int code) {
   }
 }
 
+// parameters the library refuses: mixed precision, negative capacities, friction without the
+// full contact model or with a negative coefficient or a non-positive slip velocity
+static bool bad_params(const abd_params* prm) {
+  return prm->precision != 0 || prm->min_capacity < 0 || !(prm->friction_mu >= 0.0) ||
+         (prm->friction_mu > 0.0 && (!prm->ipc_full || !(prm->friction_epsv > 0.0)));
+}
+
 int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream, abd_sim** out) {
   if (!d || !prm || !out || d->n_bodies <= 0 || !d->vert_off || !d->tri_off || !d->edge_off || !d->x0 ||
-      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed || prm->precision != 0 || prm->min_capacity < 0)
+      !d->tris || !d->edges || !d->mass || !d->I0 || !d->fixed || bad_params(prm))
     return ABD_ERR_INVALID;
   const int n = d->n_bodies;
   const int V = d->vert_off[n], T = d->tri_off[n], E = d->edge_off[n];
@@ -745,6 +776,8 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
     ok(upload(&s.slice, slices.data(), slices.size(), s.stream));
     ok(upload(&s.chunk, ch.data(), ch.size(), s.stream));
     ok(dalloc(&s.chunk_act, ch.size() + 1));
+    ok(dalloc(&s.fric_mask, (size_t)n * s.W));
+    ok(cudaMemsetAsync(s.fric_mask, 0, sizeof(uint32_t) * (size_t)n * s.W, s.stream));
     ok(upload(&s.chunk_box, cbox.data(), cbox.size(), s.stream));
     ok(upload(&s.vperm, vperm.data(), vperm.size(), s.stream));
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);  // host temporaries
@@ -828,6 +861,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   int r = grow_pairs(s, cap0(std::max(256, 8 * n)));
   if (!r) r = grow_act(s, cap0(std::max(1024, n)));
   if (!r) r = grow_contacts(s, cap0(std::max(4096, 8 * n)));
+  if (!r) r = grow_fric(s, cap0(std::max(1024, 2 * n)));
   if (!r) r = grow_ccd(s, cap0(std::max(1 << 15, 32 * n)));
   if (!r) r = grow_ecand(s, cap0(std::max(1 << 15, 32 * n)));
   s.cap_pt = 0;
@@ -858,7 +892,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.zb, s.cl_tab, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,
                   s.body_sup, s.slice, s.q_last, s.highlight, s.cl_work_buf, s.dq_save, s.adj_x,
-                  s.chunk_act};
+                  s.chunk_act, s.fric, s.fric_mask};
   for (void* q : bufs)
     if (q) cudaFree(q);
   for (abd::GraphSlot* g : {&s.g_ccd, &s.g_ccd_ev, &s.g_gh, &s.g_gh0, &s.g_kinit, &s.g_ls, &s.g_ls_dev, &s.g_step, &s.g_kadj})
@@ -881,7 +915,7 @@ static int drop_superset(abd_sim* h) {
 }
 
 int abd_sim_set_params(abd_sim* h, const abd_params* prm) {
-  if (!h || !prm || prm->precision != 0) return ABD_ERR_INVALID;
+  if (!h || !prm || bad_params(prm)) return ABD_ERR_INVALID;
   if (int r = drop_superset(h)) return r;
   h->s.prm = *prm;
   ++h->s.prm_version;  // parameters are kernel arguments of the captured passes
@@ -1101,7 +1135,10 @@ int step_host(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* 
     // passes take their candidates from the last CCD pass's line-search candidates (which the
     // step's CCD passes then replace: the first pass's kept list is consumed)
     // (the pass also forms the preconditioner's clusters)
-    if ((r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2)))
+    s.fric_lag = it == 0 && s.prm.friction_mu > 0.0 ? 1 : 0;
+    r = gh_of(h, st, st.A, st.p, &nact, it == 0 ? &s.g_gh0 : &s.g_gh, it == 0, it == 0 ? 1 : 2);
+    s.fric_lag = 0;
+    if (r)
       return r;
     if (it == 0) CK(cudaMemsetAsync(s.dint + abd::kSupHave, 0, sizeof(int), s.stream));
     if (it == 0) {
@@ -1216,6 +1253,7 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
   CK(cudaMemcpyAsync(st.Ak, st.A0, nA, cudaMemcpyDeviceToDevice, top));
   CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, top));
   CK(cudaMemcpyAsync(s.dq_save, s.dq, nq, cudaMemcpyDeviceToDevice, top));
+  if (int r = clear_friction(s)) return r;  // the first Newton iteration's GH pass fixes them
   cudaGraphConditionalHandle hn;
   if (int r = abd::make_handle(top, &hn)) return r;
   CK(abd::step_begin(s, hn));

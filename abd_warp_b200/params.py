@@ -59,6 +59,9 @@ class SimParams:
     min_capacity: int = 0            # > 0: every list of the simulator starts this small and the
                                      # traversal frontier holds at most this many nodes (tests force
                                      # the grow-and-rerun paths and the depth-first fallback with it)
+    friction_mu: float = 0.0         # lagged IPC friction (not in the reference; needs ipc_full = 1):
+                                     # the Coulomb coefficient, 0 = off
+    friction_epsv: float = 1e-3      # its static-friction slip velocity (eps = friction_epsv dt)
 
     @property
     def d2hat(self) -> float:
@@ -95,6 +98,8 @@ class SimParams:
         c.min_capacity = self.min_capacity
         c.newton_loop = self.newton_loop
         c.ipc_full = self.ipc_full
+        c.friction_mu = self.friction_mu
+        c.friction_epsv = self.friction_epsv
         return c
 
     def as_dict(self):
@@ -114,5 +119,5 @@ class CParams(ctypes.Structure):
         ("enable_vg", ctypes.c_int), ("solver", ctypes.c_int), ("cg_max_iter", ctypes.c_int),
         ("precision", ctypes.c_int), ("contact_psd", ctypes.c_int), ("precond", ctypes.c_int),
         ("cluster_max", ctypes.c_int), ("min_capacity", ctypes.c_int), ("newton_loop", ctypes.c_int),
-        ("ipc_full", ctypes.c_int),
+        ("ipc_full", ctypes.c_int), ("friction_mu", ctypes.c_double), ("friction_epsv", ctypes.c_double),
     ]

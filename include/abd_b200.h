@@ -69,6 +69,14 @@ typedef struct abd_params {
                          the barrier on its squared distance with the edge-edge mollifier, a
                          per-contact PSD projection of the exact local Hessian, and CCD roots on
                          the closed triangle / segments */
+  double friction_mu;   /* lagged IPC friction (not in the reference; needs ipc_full = 1): the
+                           Coulomb coefficient, 0 (default) = off.  At a step's start every
+                           contact within dhat fixes its closest-point weights, a tangent basis
+                           and its normal force; the step then adds mu lambda f0(|u|) per contact
+                           (u: the tangential displacement over the step) to the energy, the
+                           gradient and the Hessian, and keeps the contact's body pair in the
+                           pair lists for the whole step */
+  double friction_epsv; /* the slip velocity below which friction is static (eps = friction_epsv dt) */
 } abd_params;
 
 /* Scene description (host arrays, copied at creation).  Bodies are concatenated:

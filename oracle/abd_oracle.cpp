@@ -52,6 +52,8 @@ struct Params {
   int min_capacity;  // the CUDA library's capacity injection (the oracle has no capacities)
   int newton_loop;   // the CUDA library's choice of Newton loop (the oracle has one)
   int ipc_full;      // the full contact model (the oracle's own switch, Oracle::ipc_full, decides)
+  double friction_mu;     // lagged friction (with the full model): coefficient, 0 = off
+  double friction_epsv;   // its slip velocity (eps = friction_epsv dt)
 };
 
 struct V3 {
@@ -218,6 +220,7 @@ struct Oracle {
     int I, J, kind;  // the first group (point / edge a) moves with I
     double w[4], P[6], lam, xt[12], rs[12];
     int ids[4];
+    abd::ipc::FrictionLag hl;  // the header's lagged quantities (the default arithmetic)
   };
   std::vector<Fric> fric;
   double stat_alpha = 0, stat_toi = 0, stat_energy = 0;
@@ -1114,6 +1117,7 @@ double full_energy_hd(int kind, const V3 xs[4], const V3 rs[4], const Params& P)
   return abd::ipc::local_energy(kind, ty, v, kind == 1 ? abd::ipc::ee_eps_x(r) : 0.0, P.d2hat, P.kappa,
                                 [](double u) { return abd_log(u); });
 }
+void affine_map_hd(int kind, const double r[12], int swap, const double* H, const double* g, double out[456]);
 bool full_terms_hd(int kind, const V3 xs[4], const V3 rs[4], int swap, const Params& P, double out[456]) {
   double x[12], r[12], H[144], g[12], E, d2;
   int ty;
@@ -1122,6 +1126,15 @@ bool full_terms_hd(int kind, const V3 xs[4], const V3 rs[4], int swap, const Par
   if (!abd::ipc::local_gh(kind, x, r, P.d2hat, P.kappa, [](double u) { return abd_log(u); }, &ty, &d2, &E, g, H))
     return false;
   abd::ipc::project_psd12(H);
+  affine_map_hd(kind, r, swap, H, g, out);
+  return true;
+}
+
+// A contact's point-coordinate gradient g[12] and Hessian H[144] as the pair terms out[456]
+// (H_IJ, H_II, H_JJ, g_I, g_J) of its two bodies' affine DOFs, with the CUDA library's
+// summation order: the first nI points (the point; edge a) move with the first group's body,
+// which is the pair's first body unless swapped; r: the points' rest positions.
+void affine_map_hd(int kind, const double r[12], int swap, const double* H, const double* g, double out[456]) {
   const int nI = kind == 0 ? 1 : 2;
   auto side = [&](int v) { return (v < nI ? 0 : 1) ^ swap; };
   auto wt = [&](int v, int m) { return m == 0 ? 1.0 : r[3 * v + m - 1]; };
@@ -1143,7 +1156,6 @@ bool full_terms_hd(int kind, const V3 xs[4], const V3 rs[4], int swap, const Par
     }
     out[e] = val;
   }
-  return true;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1255,7 +1267,19 @@ void friction_lag(Oracle& o) {
       V3 xs[4], rs[4];
       fetch(o, xt.data(), cd, kind, xs, rs);
       Oracle::Fric f;
-      if (!make_fric(kind, xs, rs, o.prm, f)) continue;
+      if (o.ipc_independent) {
+        if (!make_fric(kind, xs, rs, o.prm, f)) continue;
+      } else {  // the header's (the CUDA library's arithmetic)
+        double x12[12], r12[12];
+        pts12(xs, x12);
+        pts12(rs, r12);
+        if (!abd::ipc::friction_lag(kind, x12, r12, o.prm.d2hat, o.prm.kappa, [](double u) { return abd_log(u); },
+                                    &f.hl))
+          continue;
+        f.kind = kind;
+        std::memcpy(f.xt, x12, sizeof(x12));
+        std::memcpy(f.rs, r12, sizeof(r12));
+      }
       f.I = cd.I;
       f.J = cd.J;
       // the vertex ids, for reading the current positions
@@ -1344,6 +1368,14 @@ void affine_terms(const double rs12[12], int nI, const double* g12, const double
     out[432 + e] = G[I][e];
     out[444 + e] = G[J][e];
   }
+}
+
+// one lagged contact's friction potential at positions y (all vertices)
+double friction_energy(const Oracle& o, const Oracle::Fric& f, const double* y) {
+  if (o.ipc_independent) return friction_gh(o.fr_mu, o.fr_epsv * o.prm.dt, f, y, nullptr, nullptr);
+  double x12[12], g12[12], H12[144];
+  for (int k = 0; k < 12; ++k) x12[k] = y[3 * f.ids[k / 3] + k % 3];
+  return abd::ipc::friction_gh(f.hl, x12, f.xt, o.fr_mu, o.fr_epsv * o.prm.dt, g12, H12);
 }
 
 // the body pairs of the lagged contacts join the culled pairs (a contact may outlast the
@@ -1509,10 +1541,17 @@ void assemble(Oracle& o, const double* y, const Boxes& bx, const Lists& L) {
       if (L.ij[2 * k] == a && L.ij[2 * k + 1] == b) q = k;
     if (q < 0) continue;
     double g12[12], H12[144];
-    friction_gh(o.fr_mu, o.fr_epsv * o.prm.dt, f, y, g12, H12);
     Act act;
     act.pair = q;
-    affine_terms(f.rs, f.kind == 0 ? 1 : 2, g12, H12, f.I != L.ij[2 * q], act.v);
+    if (o.ipc_independent) {
+      friction_gh(o.fr_mu, o.fr_epsv * o.prm.dt, f, y, g12, H12);
+      affine_terms(f.rs, f.kind == 0 ? 1 : 2, g12, H12, f.I != L.ij[2 * q], act.v);
+    } else {
+      double x12[12];
+      for (int k = 0; k < 12; ++k) x12[k] = y[3 * f.ids[k / 3] + k % 3];
+      abd::ipc::friction_gh(f.hl, x12, f.xt, o.fr_mu, o.fr_epsv * o.prm.dt, g12, H12);
+      affine_map_hd(f.kind, f.rs, f.I != L.ij[2 * q], H12, g12, act.v);
+    }
     acts.push_back(act);
     ++o.pact[q];
   }
@@ -2269,7 +2308,7 @@ double energy_at(Oracle& o, const double* y, const double* Akp, const double* pk
     const double d = y[3 * L.vg[k + 1] + 1] - o.prm.ground;
     total.add(barrier(d * d, o.prm));
   }
-  for (const Oracle::Fric& f : o.fric) total.add(friction_gh(o.fr_mu, o.fr_epsv * o.prm.dt, f, y, nullptr, nullptr));
+  for (const Oracle::Fric& f : o.fric) total.add(friction_energy(o, f, y));
   for (int b = 0; b < o.n; ++b)
     if (!o.fixed[b]) total.add(inertia_energy(o, b, Akp, pkp));
   return total.round();
@@ -2414,6 +2453,10 @@ void* orc_create(int n, const int* voff, const int* toff, const int* eoff, const
   o->fixed.assign(fixed, fixed + n);
   o->prm = *prm;
   o->ipc_full = prm->ipc_full != 0;
+  if (prm->friction_mu > 0.0) {
+    o->fr_mu = prm->friction_mu;
+    o->fr_epsv = prm->friction_epsv;
+  }
   for (auto* v : {&o->A, &o->Ak, &o->Adot, &o->A0}) v->assign(9 * (size_t)n, 0.0);
   for (auto* v : {&o->p, &o->pk, &o->pdot, &o->p0}) v->assign(3 * (size_t)n, 0.0);
   o->dq.assign(12 * (size_t)n, 0.0);
@@ -2434,6 +2477,10 @@ void orc_set_params(void* h, const Params* prm) {
   Oracle* o = (Oracle*)h;
   o->prm = *prm;
   if (prm->ipc_full) o->ipc_full = true;
+  if (prm->friction_mu > 0.0) {
+    o->fr_mu = prm->friction_mu;
+    o->fr_epsv = prm->friction_epsv;
+  }
 }
 // on: 0 the reference's model, 1 the full model in the CUDA library's arithmetic, 2 the full
 // model in the oracle's own
