@@ -2614,6 +2614,7 @@ int orc_gh(void* h, const double* A, const double* p, double* g, double* diag, d
   Lists L;
   static_boxes(*o, o->x.data(), bx);
   cull(*o, bx, L);
+  add_friction_pairs(*o, L);  // as the step's GH passes (no-op without friction)
   assemble(*o, o->x.data(), bx, L);
   std::copy(o->g.begin(), o->g.end(), g);
   std::copy(o->diag.begin(), o->diag.end(), diag);

@@ -90,3 +90,30 @@ def test_friction_needs_the_full_model():
             sim.set_params(dataclasses.replace(prm, ipc_full=0))
     finally:
         sim.close()
+
+
+def test_friction_energy_and_gradient_hessian_apis():
+    """After friction steps the energy pass and the GH pass of the API carry the last step's
+    lagged friction contacts, as the oracle's: energies at two DOF sets and the assembled
+    gradient and blocks at the current DOFs, bit for bit."""
+    import torch
+    from abd_warp_b200.simulator import AffineBodySimulator
+    bodies, prm = _sliding_cube(0)
+    o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
+    sim = AffineBodySimulator(bodies=bodies, params=prm)
+    try:
+        for _ in range(8):
+            o.step()
+            sim.step()
+        st = o.get_state()
+        cu = lambda v: torch.as_tensor(v, device="cuda")
+        for shift in (0.0, 2e-4):
+            A, p = st["A0"], st["p0"] + np.array([shift, 0.0, 0.0])
+            assert sim.compute_energy(cu(A), cu(p)) == o.energy(A, p), shift
+        ref = o.gh(st["A0"], st["p0"])
+        got = sim.gradient_hessian(cu(st["A0"]), cu(st["p0"]))
+        assert got["n_active"] == ref["n_active"] > 0
+        for k in ("g", "diag", "off", "ij"):
+            np.testing.assert_array_equal(got[k].cpu().numpy(), ref[k], err_msg=k)
+    finally:
+        sim.close()
