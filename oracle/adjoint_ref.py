@@ -12,9 +12,9 @@ Newton uses does not enter.  With qdot_{t+1} = (q_{t+1} - q_t) / dt, the adjoint
     a = qb + qdb / dt,   lambda = H^-1 a,   qb_t = M lambda - qdb / dt,   qdb_t = dt M lambda.
 DOFs per body: [p, A row 0, row 1, row 2] (12).  Fixed bodies carry no adjoint.
 
-The reference has no adjoint.  This follows the differentiable-simulation form of the
-north star (checkpointed forward, transposed Hessian solve per step), restated for the
-oracle: every state is kept, since the scenes it checks are small.
+The reference has no adjoint.  This is the differentiable-simulation form of the library
+(checkpointed forward, transposed Hessian solve per step), restated for the oracle: every
+state is kept, since the scenes it checks are small.
 """
 from __future__ import annotations
 
