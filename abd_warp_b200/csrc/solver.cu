@@ -8,8 +8,8 @@
 // condition number.  Bodies coupled by active contacts are grouped on the device (mutual
 // strongest couplings merge in rounds, at most cluster_max bodies: k_clusters); each
 // cluster's dense system is assembled and inverted (Gauss-Jordan, SPD, no pivoting) by one
-// warp in registers (one or two bodies) or one CTA in shared memory (more), and applied as a
-// dense product.  Clusters of one body reduce to the per-body 12x12 block.
+// warp in registers (one body) or one CTA in shared memory (more), and applied as a dense
+// product.  Clusters of one body reduce to the per-body 12x12 block.
 //
 // Krylov: PCG (default; the projected Hessian is SPD) or right-preconditioned BiCGSTAB (the
 // reference's choice).  Convergence is measured in the preconditioned norm,
@@ -136,7 +136,7 @@ __device__ inline double row_product(const SolverArgs& a, int b, const double* x
   return acc;  // valid on lanes 0..11
 }
 
-#define FOR_BODIES(b) for (int b = blockIdx.x * WPB + (int)(threadIdx.x >> 5); b < a.n; b += kRedBlocks * WPB)
+#define FOR_BODIES(b) for (int b = blockIdx.x * WPB + (int)(threadIdx.x >> 5); b < a.n; b += (int)gridDim.x * WPB)
 
 __device__ inline bool solver_done(const int* dstat) {
   return ((volatile const int*)dstat)[DS_R_DONE] != 0 || ((volatile const int*)dstat)[DS_S_DONE] != 0;
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, 
                                                      cudaGraphConditionalHandle h) {
   const double b = a.scal[SC_RED + SL_BZ];
   if (!(b > 0.0))
-    for (int i = blockIdx.x * 256 + threadIdx.x; i < 12 * a.n; i += kRedBlocks * 256) x[i] = 0.0;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < 12 * a.n; i += (int)gridDim.x * 256) x[i] = 0.0;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
     a.scal[SC_THR2] = tol2 * b;
@@ -825,15 +825,15 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   cudaGraphConditionalHandle h;
   if (ABD_NOTE(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return ABD_ERR_CUDA;
   // b^T M^-1 b sets the threshold
-  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
-  k_residual<<<kRedBlocks, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
+  k_apply<<<s.red_grid, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
+  k_residual<<<s.red_grid, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
                                          pcg ? nullptr : s.v);
   if (ABD_NOTE(cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st)) ||
       ABD_NOTE(cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st)))
     return ABD_ERR_CUDA;
-  k_solver_init<<<kRedBlocks, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x, h);
+  k_solver_init<<<s.red_grid, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x, h);
   // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
-  k_apply<<<kRedBlocks, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
+  k_apply<<<s.red_grid, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
   s.launches += 4;
   // the iteration loop: a WHILE node on the capture, its body captured on a second stream
   const cudaGraphNode_t* deps = nullptr;
@@ -855,20 +855,20 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   if (ABD_NOTE(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return ABD_ERR_CUDA;
   if (pcg) {
-    k_pcg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v);
-    k_pcg_2<<<kRedBlocks, 256, 0, bs>>>(a, s.pv, s.v, x, s.r);
-    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.z, nullptr, kSlotRzNew);
-    k_pcg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.pv);
+    k_pcg_1<<<s.red_grid, 256, 0, bs>>>(a, s.pv, s.v);
+    k_pcg_2<<<s.red_grid, 256, 0, bs>>>(a, s.pv, s.v, x, s.r);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.z, nullptr, kSlotRzNew);
+    k_pcg_3<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.pv);
   } else {
-    k_bicg_1<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.pv, s.v);
-    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.pv, s.y, nullptr, -1);
-    k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
-    k_bicg_3<<<kRedBlocks, 256, 0, bs>>>(a, s.r, s.v, s.s);
-    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
-    k_bicg_4<<<kRedBlocks, 256, 0, bs>>>(a, s.y, x);
-    k_spmv<<<kRedBlocks, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
-    k_bicg_6<<<kRedBlocks, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-    k_apply<<<kRedBlocks, AT, 0, bs>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
+    k_bicg_1<<<s.red_grid, 256, 0, bs>>>(a, s.r, s.pv, s.v);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.pv, s.y, nullptr, -1);
+    k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
+    k_bicg_3<<<s.red_grid, 256, 0, bs>>>(a, s.r, s.v, s.s);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
+    k_bicg_4<<<s.red_grid, 256, 0, bs>>>(a, s.y, x);
+    k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
+    k_bicg_6<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
   }
   k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
   if (per_iter_out) *per_iter_out = pcg ? 5 : 10;
