@@ -110,6 +110,24 @@ def dist_env():
     return rank, world, local
 
 
+def slowest_ms(ms: float, world: int, device) -> float:
+    """The replicas' time for their timed steps: the maximum of each rank's device time (after
+    a barrier, so that every rank has finished them); a single rank's own time."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.barrier()
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, steps: int, max_ms: float) -> float:
+    """Steps per second of all replicas together: each rank ran `steps` steps in at most max_ms."""
+    return world * steps / (max_ms / 1e3)
+
+
 def make_scene():
     from abd_warp_b200 import scenes
     bodies, prm, _ = scenes.make_config(2)
@@ -425,12 +443,8 @@ def main():
     launches = sim.launch_count() - launches0
     k_ms, k_launches, _ = sim.profile_read()
     sim.profile(0)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms / 1e3)
+    max_ms = slowest_ms(total_ms, world, dev)
+    value = whole_job_rate(world, args.steps, max_ms)
     # ---- end to end through the public API with host buffers ----
     # the caller keeps its states in pinned host memory: each step copies them in, steps, and
     # copies the new states and the vertex positions out (its next step's inputs)
@@ -462,10 +476,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize(dev)
     e2e_ms, _ = run_schedule(per_state, e2e_step, e2e_begin)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / (float(te.item()) / 1e3)
+    e2e_value = whole_job_rate(world, args.steps, slowest_ms(e2e_ms, world, dev))
     # the algorithmic bytes of the same launches: the steps are deterministic, so a replay with
     # the kernel counting what it reads has the same launches (not timed: counting slows it)
     sim.profile(2)
