@@ -125,3 +125,35 @@ def test_create_rejects_malformed_scenes():
         assert rc == _lib.ABD_ERR_INVALID and not h
     rc, h = create(lambda h: None, prm=SimParams(min_capacity=-1))  # negative injected capacity
     assert rc == _lib.ABD_ERR_INVALID and not h
+
+
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and field offsets of a struct of include/abd_b200.h, from a C program built here."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    lines = ['#include <stddef.h>', '#include <stdio.h>', f'#include "{HEADER}"', "int main(void) {",
+             f'  printf("%zu\\n", sizeof({struct}));']
+    lines += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-o", str(exe), str(src)], check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    return out[0], out[1:]
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The Python mirrors of abd_params, abd_scene_desc, abd_states and abd_step_info have the
+    C header's field offsets and sizes (the library reads them by the C layout)."""
+    from abd_warp_b200 import _lib
+    from abd_warp_b200.params import CParams
+    for struct, cls in (("abd_params", CParams), ("abd_scene_desc", _lib.SceneDesc), ("abd_states", _lib.States),
+                        ("abd_step_info", _lib.StepInfo)):
+        names = [f[0] for f in cls._fields_]
+        size, offs = _c_layout(tmp_path, struct, names)
+        assert ctypes.sizeof(cls) == size, struct
+        assert [getattr(cls, n).offset for n in names] == offs, struct
