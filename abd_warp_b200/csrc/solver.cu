@@ -577,7 +577,10 @@ __global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, 
     a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
     a.scal[SC_THR2] = tol2 * b;
     a.dstat[DS_IT] = 1;
-    if (!(b > 0.0)) a.dstat[DS_R_DONE] = 1;
+    // the solve's outcome flags start clear (the iterations that follow set and read them)
+    a.dstat[DS_R_DONE] = b > 0.0 ? 0 : 1;
+    a.dstat[DS_S_DONE] = 0;
+    a.dstat[DS_SOLVER_ITERS] = 0;
     cudaGraphSetConditional(h, (b > 0.0 && a.maxit >= 1) ? 1u : 0u);
   }
 }
@@ -828,9 +831,6 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   k_apply<<<s.red_grid, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
   k_residual<<<s.red_grid, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
                                          pcg ? nullptr : s.v);
-  if (ABD_NOTE(cudaMemsetAsync(s.dstat + DS_R_DONE, 0, 2 * sizeof(int), st)) ||
-      ABD_NOTE(cudaMemsetAsync(s.dstat + DS_SOLVER_ITERS, 0, sizeof(int), st)))
-    return ABD_ERR_CUDA;
   k_solver_init<<<s.red_grid, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x, h);
   // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
   k_apply<<<s.red_grid, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
