@@ -553,8 +553,9 @@ cudaError_t body_broad(Sim& s, const double* A, const double* p, const double* A
 // body pairs: full (mask, scan, fill: the sorted pair list and the adjacency with pair
 // indices) or mask only (row counts and the bit matrix, all the energy and CCD passes need)
 // sup: cull with the boxes over every DOF set between the two of a swept pass (body_sup)
-// forced: [n][W] bits added to the overlap matrix (the step's friction pairs), or null
-cudaError_t body_pairs(Sim& s, bool full, bool sup = false, const uint32_t* forced = nullptr);
+// forced: [n][W] bits added to the overlap matrix (the step's friction pairs), or null;
+// ccd: a CCD pass follows (its candidate counters are cleared)
+cudaError_t body_pairs(Sim& s, bool full, bool sup = false, const uint32_t* forced = nullptr, bool ccd = false);
 // rest-frame internal node boxes of both trees (once, at creation)
 cudaError_t rest_boxes(Sim& s);
 

@@ -141,10 +141,17 @@ __global__ void __launch_bounds__(256, 4) k_vertex_broad(VertexArgs a) {
 // FP32 body boxes from the bounds (one thread per body), which are cleared for the next pass.
 // With body_sup: also the affine images of the body's rest box under both DOF sets, dilated
 // by dhat / 2, which hold the body's box at every DOF set between the two.
+// Also clears, for the narrow pass that follows, its chunk filter's count (chunk_count) and,
+// in a CCD pass, its candidate counters (cand_count: DS_NCCD, DS_NECAND).
 __global__ void k_body_boxes(int n, unsigned long long* bnd, int swept, double dhh, Box* body_box,
-                             const Box* body_rest, const float* fdof, Box* body_sup) {
+                             const Box* body_rest, const float* fdof, Box* body_sup, int* chunk_count,
+                             int* cand_count) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
+  if (b == 0) {
+    *chunk_count = 0;
+    if (cand_count) cand_count[0] = cand_count[1] = 0;
+  }
   unsigned long long k[12];
 #pragma unroll
   for (int i = 0; i < 12; ++i) {
@@ -278,6 +285,8 @@ __global__ void __launch_bounds__(1024) k_pair_scan(int n, const int* rcnt, cons
     dstat[DS_NPAIRS] = npairs;
     dstat[DS_PT_COUNT] = dstat[DS_EE_COUNT] = dstat[DS_VG_COUNT] = dstat[DS_ACTIVE] = 0;
     dstat[DS_NCONTACT] = 0;
+    dstat[DS_NCCD] = 0;   // the GH pass's candidates
+    dstat[DS_NACTP] = 0;  // its active pairs
     if (npairs > cap_pairs || carry[0] > cap_adj) atomicOr(&dstat[DS_STATUS], ST_PAIR_OVERFLOW);
   }
 }
@@ -589,10 +598,12 @@ cudaError_t transform(Sim& s, const double* A, const double* p, double* x) {
 // the pair index of {I, J}).  Counts stay on the device (dstat DS_NPAIRS / DS_NADJ); a short
 // capacity raises ST_PAIR_OVERFLOW and leaves the lists incomplete, for the host to grow and
 // rerun at its next read of dstat.
-cudaError_t body_pairs(Sim& s, bool full, bool sup, const uint32_t* forced) {
+cudaError_t body_pairs(Sim& s, bool full, bool sup, const uint32_t* forced, bool ccd) {
   const int n = s.n, W = s.W;
+  static_assert(DS_NECAND == DS_NCCD + 1, "candidate counters");
   k_body_boxes<<<blocks(n, 128), 128, 0, s.stream>>>(n, s.body_bnd, s.swept, 0.5 * s.prm.dhat, s.body_box,
-                                                     s.body_rest, s.fdof, sup ? s.body_sup : nullptr);
+                                                     s.body_rest, s.fdof, sup ? s.body_sup : nullptr,
+                                                     s.chunk_act + s.nch, ccd ? s.dstat + DS_NCCD : nullptr);
   k_pair_mask<<<n, PR_THREADS, 0, s.stream>>>(n, W, sup ? s.body_sup : s.body_box, forced, s.pair_mask,
                                                s.pair_wpre, s.row_cnt, s.upper_cnt, s.nbr);
   s.launches += 2;

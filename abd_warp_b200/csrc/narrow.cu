@@ -1744,8 +1744,7 @@ BodyArgs body_args(Sim& s, const abd_states* st, const double* A, const double* 
 // every chunk; the CTAs past the count return at once).  Counts the filter's launch.
 template <int MODE>
 cudaError_t chunk_pass(Sim& s, const NarrowArgs& a) {
-  cudaError_t e = cudaMemsetAsync(s.chunk_act + s.nch, 0, sizeof(int), s.stream);
-  if (e != cudaSuccess) return e;
+  // (the body-box kernel of the pass cleared the filter's count)
   constexpr int per = KA / 32;
   k_chunk_active<MODE><<<(s.nch + per - 1) / per, KA, 0, s.stream>>>(a);
   k_chunk_narrow<MODE><<<s.nch, CT, 0, s.stream>>>(a);
@@ -1770,10 +1769,8 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
         ++s.launches;
       }
     } else if (mode == NARROW_CCD || mode == NARROW_CCD_LS) {
-      // DS_NCCD and DS_NECAND are adjacent
-      static_assert(DS_NECAND == DS_NCCD + 1, "candidate counters");
-      cudaError_t e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, 2 * sizeof(int), s.stream);
-      if (e != cudaSuccess) return e;
+      // (the body-box kernel of the pass cleared DS_NCCD and DS_NECAND)
+      cudaError_t e = cudaSuccess;
       if (mode == NARROW_CCD_LS) {
         if (!a.y1) return cudaErrorInvalidValue;
         if (s.prof_events > 0 && record_event(s.prof_ev[0], s.stream))
@@ -1788,10 +1785,9 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       }
       ++s.launches;
     } else {
-      cudaError_t e = cudaMemsetAsync(s.pair_cand, 0, sizeof(int) * 4 * (size_t)s.cap_pairs, s.stream);
-      if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCONTACT, 0, sizeof(int), s.stream);
-      if (e == cudaSuccess) e = cudaMemsetAsync(s.dstat + DS_NCCD, 0, sizeof(int), s.stream);
-      if (e != cudaSuccess) return e;
+      // (the pass's pair scan cleared the per-pair contact counts, DS_NCONTACT, DS_NCCD and
+      // DS_NACTP; the contact scan sets the offsets and scatter counters)
+      cudaError_t e = cudaSuccess;
       if (s.gh_if_on) {
         // captured: the traversal in an IF node (k_sup_check sets its condition); the
         // kernels in the body are not counted among the pass's launches (they rarely run)
@@ -1816,7 +1812,6 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
       k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
                                                                            s.contacts_by_pair, s.dstat);
-      if ((e = cudaMemsetAsync(s.dstat + DS_NACTP, 0, sizeof(int), s.stream)) != cudaSuccess) return e;
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
       static_assert(smem + sizeof(double) * PT_WARPS * 5 * 24 + 256 <= 48 * 1024, "pair assembly shared memory");
       const int grid = s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148;

@@ -230,7 +230,8 @@ int culling(abd_sim* h, const abd::Dofs* d0, const abd::Dofs* d1, double* y0, do
   const bool full = mode == abd::NARROW_GH || mode == abd::NARROW_LISTS;
   // the GH pass's pairs also hold the body pairs of the step's lagged friction contacts
   const uint32_t* forced = mode == abd::NARROW_GH && s.prm.friction_mu > 0.0 ? s.fric_mask : nullptr;
-  CK(abd::body_pairs(s, full, mode == abd::NARROW_CCD_LS, forced));
+  CK(abd::body_pairs(s, full, mode == abd::NARROW_CCD_LS, forced,
+                     mode == abd::NARROW_CCD || mode == abd::NARROW_CCD_LS));
   CK(abd::narrow(s, mode, d0 ? d0->Aeff() : nullptr, d0 ? d0->peff() : nullptr, d1 ? d1->Aeff() : nullptr,
                  d1 ? d1->peff() : nullptr, y0, y1, st));
   return ABD_OK;
