@@ -1160,47 +1160,6 @@ __global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
   }
 }
 
-// The GH pass's candidates without a traversal, when the kept line-search candidates hold
-// every pair its culling can produce (sup_valid): the pass's DOFs lie on the segment the step's
-// last CCD pass covered (the accepted step q - alpha dq, 0 <= alpha <= 1).  Each candidate is
-// put to the GH pass's own culling predicate -- the exact body boxes overlap and the static
-// primitive boxes overlap (culling2.py:32-79, 213-227) -- and appended as the traversal would
-// append it, with its pair index from the adjacency of the point's (or lower edge's) body.
-__global__ void __launch_bounds__(128) k_gh_scan(NarrowArgs a) {
-  if (!*a.sup_valid || (a.dstat[DS_STATUS] & ST_PAIR_OVERFLOW)) return;
-  const int n = min(a.dstat[DS_NECAND], a.cap_ecand);
-  const float dhf = (float)a.prm.dhat;
-  const double dhh = 0.5 * a.prm.dhat;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int4 c = a.ecand[k];
-    const int type = c.x, pa = c.y, pb = c.z;
-    int ids[4];
-    cand_vertices(a, type, pa, pb, ids);
-    const int I = __ldg(&a.vbody[ids[0]]), J = __ldg(&a.vbody[ids[type == 0 ? 1 : 2]]);
-    if (!overlap(load_box(&a.body_box[I]), load_box(&a.body_box[J]))) continue;
-    const bool hit = type == 0 ? overlap(point_box(a.y0, nullptr, pa, dhf), tri_leaf_box(a.tris, a.y0, nullptr, pb))
-                               : overlap(edge_leaf_box(a.edges, a.y0, nullptr, pa, dhh),
-                                         edge_leaf_box(a.edges, a.y0, nullptr, pb, dhh));
-    if (!hit) continue;
-    // row I of the adjacency lists its neighbours in increasing order
-    int lo = a.row_ptr[I], hi = min(a.row_ptr[I + 1], a.cap_adj) - 1, pr = -1;
-    while (lo <= hi) {
-      const int mid = (lo + hi) >> 1, col = a.adj_col[mid];
-      if (col == J) {
-        pr = a.adj_pair[mid];
-        break;
-      }
-      if (col < J) lo = mid + 1;
-      else hi = mid - 1;
-    }
-    if (pr < 0) continue;  // (the body boxes overlap, so the pair is listed)
-    const int swap = (type == 0 && I > J) ? 1 : 0;
-    const int pos = append_slot(&a.dstat[DS_NCCD]);
-    if (pos < a.cap_ccd) a.ccd_cand[pos] = make_int4(pr, type | (swap << 1), pa, pb);
-    else atomicOr(&a.dstat[DS_STATUS], ST_CCD_OVERFLOW);
-  }
-}
-
 // Sets dint[kSupValid] (gh_superset_check) and, in a captured pass (use_hc), the condition of
 // the IF node around the tree traversal: 1 when the traversal must run; one CTA
 __global__ void k_sup_check(int n, const double* A0, const double* p0, const double* q_last, const int* have,
@@ -1301,46 +1260,42 @@ __global__ void __launch_bounds__(128) k_fric_energy(NarrowArgs a) {
   }
 }
 
-// Contacts of the GH pass's candidates, one thread per candidate: the active ones
-// (pt_ipc.py:13-22, 114; ee_ipc.py:13-23, 382) are appended for the per-pair assembly and
-// counted per pair; the candidates are counted per kind.  With gh_energy their barrier
-// energies join the pass's exact energy (k_body_gh adds the bodies' terms: the GH pass then
-// also gives the energy at its DOFs, the same sum as an energy pass there).
-__global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
-  if (a.dstat[DS_STATUS] & (ST_CCD_OVERFLOW | ST_PAIR_OVERFLOW)) return;
-  const int n = min(a.dstat[DS_NCCD], a.cap_ccd);
-  int cpt = 0, cee = 0;
-  XSum en;  // the candidates' barrier energy (ipcsk/energy.py:9-48)
-  xs_zero(en);
-  const bool with_energy = a.gh_energy && (!a.energy_gate || *a.energy_gate == 0);
-  const bool lag = a.fric_lag && (!a.energy_gate || *a.energy_gate == 0);  // the step's first GH pass
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int4 c = a.ccd_cand[k];  // pair, type | swap << 1, primitive a, primitive b
-    const int type = c.y & 1;
-    if (type == 0) ++cpt;
-    else ++cee;
-    int ids[4];
-    d3 xs[4];
-    cand_vertices(a, type, c.z, c.w, ids);
-    fetch(a.y0, ids, xs);
-    if (with_energy) {
-      const double e = candidate_energy(a, type, ids, xs);
-      if (e != 0.0) xs_add(en, e);
-    }
-    Geo G;
-    double d2;
-    int fty;
-    if (a.prm.ipc_full ? full_d2(type, xs, &fty) < a.prm.d2hat : contact_active(type, xs, a.prm, &G, &d2)) {
-      const int pos = append_slot(&a.dstat[DS_NCONTACT]);
-      if (pos < a.cap_contacts) a.contacts[pos] = c;
-      else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
-      atomicAdd(&a.pair_cand[4 * c.x + 1], 1);
-      if (lag) {
-        const double e = friction_lag_contact(a, type, ids, xs);
-        if (with_energy && e != 0.0) xs_add(en, e);
-      }
+// One candidate of the GH pass, c = (pair, type | swap << 1, primitive a, primitive b): counted
+// by kind; when active (pt_ipc.py:13-22, 114; ee_ipc.py:13-23, 382) appended for the per-pair
+// assembly and counted for its pair, and at the step's first GH pass (lag) its lagged friction
+// is fixed.  With gh_energy its barrier energy joins the pass's exact energy (k_body_gh adds
+// the bodies' terms: the GH pass then also gives the energy at its DOFs, the same sum as an
+// energy pass there).
+__device__ inline void gh_candidate(const NarrowArgs& a, const int4 c, bool with_energy, bool lag, int& cpt,
+                                    int& cee, XSum& en) {
+  const int type = c.y & 1;
+  if (type == 0) ++cpt;
+  else ++cee;
+  int ids[4];
+  d3 xs[4];
+  cand_vertices(a, type, c.z, c.w, ids);
+  fetch(a.y0, ids, xs);
+  if (with_energy) {
+    const double e = candidate_energy(a, type, ids, xs);
+    if (e != 0.0) xs_add(en, e);
+  }
+  Geo G;
+  double d2;
+  int fty;
+  if (a.prm.ipc_full ? full_d2(type, xs, &fty) < a.prm.d2hat : contact_active(type, xs, a.prm, &G, &d2)) {
+    const int pos = append_slot(&a.dstat[DS_NCONTACT]);
+    if (pos < a.cap_contacts) a.contacts[pos] = c;
+    else atomicOr(&a.dstat[DS_STATUS], ST_CONTACT_OVERFLOW);
+    atomicAdd(&a.pair_cand[4 * c.x + 1], 1);
+    if (lag) {
+      const double e = friction_lag_contact(a, type, ids, xs);
+      if (with_energy && e != 0.0) xs_add(en, e);
     }
   }
+}
+
+// the per-kind counts and the energy of a CTA's candidates into the pass's totals (every thread)
+__device__ inline void gh_flush(const NarrowArgs& a, int cpt, int cee, XSum& en, bool with_energy) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     cpt += __shfl_xor_sync(0xffffffffu, cpt, o);
@@ -1356,6 +1311,70 @@ __global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
       if (en.d[i]) atomicAdd((unsigned long long*)&d[i], (unsigned long long)en.d[i]);
     if (en.flags) atomicOr((unsigned long long*)&d[kXD], (unsigned long long)en.flags);
   }
+}
+
+// the energy and the friction lag ride on the step's first GH pass
+__device__ inline bool gh_with_energy(const NarrowArgs& a) {
+  return a.gh_energy && (!a.energy_gate || *a.energy_gate == 0);
+}
+__device__ inline bool gh_lag(const NarrowArgs& a) { return a.fric_lag && (!a.energy_gate || *a.energy_gate == 0); }
+
+// The candidates of the tree traversal (when the kept line-search candidates did not cover the
+// pass; k_gh_scan evaluates them otherwise), one thread per candidate
+__global__ void __launch_bounds__(128) k_gh_eval(NarrowArgs a) {
+  if (*a.sup_valid || (a.dstat[DS_STATUS] & (ST_CCD_OVERFLOW | ST_PAIR_OVERFLOW))) return;
+  const int n = min(a.dstat[DS_NCCD], a.cap_ccd);
+  int cpt = 0, cee = 0;
+  XSum en;  // the candidates' barrier energy (ipcsk/energy.py:9-48)
+  xs_zero(en);
+  const bool with_energy = gh_with_energy(a), lag = gh_lag(a);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    gh_candidate(a, a.ccd_cand[k], with_energy, lag, cpt, cee, en);
+  gh_flush(a, cpt, cee, en, with_energy);
+}
+
+// The GH pass's candidates without a traversal, when the kept line-search candidates hold
+// every pair its culling can produce (sup_valid): the pass's DOFs lie on the segment the step's
+// last CCD pass covered (the accepted step q - alpha dq, 0 <= alpha <= 1).  Each candidate is
+// put to the GH pass's own culling predicate -- the exact body boxes overlap and the static
+// primitive boxes overlap (culling2.py:32-79, 213-227) -- and evaluated as the traversal's
+// candidates are, with its pair index from the adjacency of the point's (or lower edge's) body.
+__global__ void __launch_bounds__(128) k_gh_scan(NarrowArgs a) {
+  if (!*a.sup_valid || (a.dstat[DS_STATUS] & (ST_CCD_OVERFLOW | ST_PAIR_OVERFLOW))) return;
+  const int n = min(a.dstat[DS_NECAND], a.cap_ecand);
+  const float dhf = (float)a.prm.dhat;
+  const double dhh = 0.5 * a.prm.dhat;
+  int cpt = 0, cee = 0;
+  XSum en;
+  xs_zero(en);
+  const bool with_energy = gh_with_energy(a), lag = gh_lag(a);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int4 c = a.ecand[k];
+    const int type = c.x, pa = c.y, pb = c.z;
+    int ids[4];
+    cand_vertices(a, type, pa, pb, ids);
+    const int I = __ldg(&a.vbody[ids[0]]), J = __ldg(&a.vbody[ids[type == 0 ? 1 : 2]]);
+    if (!overlap(load_box(&a.body_box[I]), load_box(&a.body_box[J]))) continue;
+    const bool hit = type == 0 ? overlap(point_box(a.y0, nullptr, pa, dhf), tri_leaf_box(a.tris, a.y0, nullptr, pb))
+                               : overlap(edge_leaf_box(a.edges, a.y0, nullptr, pa, dhh),
+                                         edge_leaf_box(a.edges, a.y0, nullptr, pb, dhh));
+    if (!hit) continue;
+    // row I of the adjacency lists its neighbours in increasing order
+    int lo = a.row_ptr[I], hi = min(a.row_ptr[I + 1], a.cap_adj) - 1, pr = -1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1, col = a.adj_col[mid];
+      if (col == J) {
+        pr = a.adj_pair[mid];
+        break;
+      }
+      if (col < J) lo = mid + 1;
+      else hi = mid - 1;
+    }
+    if (pr < 0) continue;  // (the body boxes overlap, so the pair is listed)
+    const int swap = (type == 0 && I > J) ? 1 : 0;
+    gh_candidate(a, make_int4(pr, type | (swap << 1), pa, pb), with_energy, lag, cpt, cee, en);
+  }
+  gh_flush(a, cpt, cee, en, with_energy);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1789,22 +1808,26 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
       // DS_NACTP; the contact scan sets the offsets and scatter counters)
       cudaError_t e = cudaSuccess;
       if (s.gh_if_on) {
-        // captured: the traversal in an IF node (k_sup_check sets its condition); the
-        // kernels in the body are not counted among the pass's launches (they rarely run)
+        // captured: the traversal and the evaluation of its candidates in an IF node
+        // (k_sup_check sets its condition); the kernels in the body are not counted among the
+        // pass's launches (they rarely run)
         s.gh_if_on = false;
         cudaGraph_t body = nullptr;
         if (add_conditional(s.stream, s.gh_if, cudaGraphCondTypeIf, &body) != ABD_OK) return cudaErrorUnknown;
         const int r = capture_body(s, body, s.cap_stream5, [&]() -> int {
-          return chunk_pass<NARROW_GH>(s, a) == cudaSuccess ? ABD_OK : ABD_ERR_CUDA;
+          if (chunk_pass<NARROW_GH>(s, a) != cudaSuccess) return ABD_ERR_CUDA;
+          k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
+          return ABD_OK;
         });
         if (r != ABD_OK) return cudaErrorUnknown;
         s.launches -= 2;
       } else {
         if ((e = chunk_pass<NARROW_GH>(s, a)) != cudaSuccess) return e;
+        k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
+        ++s.launches;
       }
       k_gh_scan<<<kRedBlocks, 128, 0, s.stream>>>(a);
-      k_gh_eval<<<kRedBlocks, 128, 0, s.stream>>>(a);
-      s.launches += 2;
+      ++s.launches;
       if (a.fric) {
         k_fric_pairs<<<kRedBlocks, 128, 0, s.stream>>>(a);
         ++s.launches;
