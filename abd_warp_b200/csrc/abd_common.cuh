@@ -400,7 +400,6 @@ struct Sim {
   double* cl_inv = nullptr;                      // dense inverses of the cluster systems
                                                  // (144 kMaxCluster n doubles: the most any
                                                  // clustering needs)
-  double* zb = nullptr;                          // [n][12] scratch (M^-1 b)
   XSum* partials = nullptr; // exact reduction partials [kRedSlots][kRedBlocks]
   int* red_count = nullptr;        // [kRedSlots] CTAs done per reduction (last CTA finishes)
   double* scal = nullptr;          // solver scalars

@@ -68,44 +68,51 @@ __device__ inline void cta_scalars(const SolverArgs& a, const int* slots, int ns
   for (int k = 0; k < ns; ++k) out[k] = a.scal[SC_RED + slots[k]];
 }
 
+// The CTA's exact partial of a dot product into part[slot] (every thread passes its accumulator)
+__device__ inline void cta_partial(const SolverArgs& a, XSum& x, int slot, XSum* sh) {
+  xs_block_sum(x, sh);
+  if (threadIdx.x == 0) a.part[slot * kRedBlocks + blockIdx.x] = x;
+}
+
+// After a CTA's partials: true in the last CTA to deliver (the launch's single counter cslot,
+// reset here for the next launch), which then sees every CTA's partials
+__device__ inline bool cta_last(const SolverArgs& a, int cslot) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&a.red_count[cslot], 1) == (int)gridDim.x - 1;
+    if (last) a.red_count[cslot] = 0;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// In the last CTA: the sum of every CTA's partial of `slot`, rounded into scal[SC_RED + slot]
+__device__ inline void total_of(const SolverArgs& a, int slot, XSum* sh) {
+  XSum t;
+  xs_zero(t);
+  const XSum* P = a.part + slot * kRedBlocks;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+    const long long* q = reinterpret_cast<const long long*>(P + i);
+#pragma unroll
+    for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
+    t.flags |= __ldcg(q + kXD);
+  }
+  xs_block_sum(t, sh);
+  if (threadIdx.x == 0) a.scal[SC_RED + slot] = xs_round(t);
+}
+
 // Exact per-CTA partials of up to two dot products (every thread passes its accumulators);
 // the last CTA to deliver sums the partials of all CTAs and stores the rounded totals in
 // scal[SC_RED + slot] (a single counter per launch: slot0 if >= 0, else slot1).
 __device__ inline void cta_partials(const SolverArgs& a, XSum& x0, XSum& x1, int slot0, int slot1) {
   __shared__ XSum sh[8];
-  __shared__ bool last;
-  if (slot0 >= 0) {
-    xs_block_sum(x0, sh);
-    if (threadIdx.x == 0) a.part[slot0 * kRedBlocks + blockIdx.x] = x0;
-  }
-  if (slot1 >= 0) {
-    xs_block_sum(x1, sh);
-    if (threadIdx.x == 0) a.part[slot1 * kRedBlocks + blockIdx.x] = x1;
-  }
-  const int cslot = slot0 >= 0 ? slot0 : slot1;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(&a.red_count[cslot], 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int k = 0; k < 2; ++k) {
-    const int slot = k ? slot1 : slot0;
-    if (slot < 0) continue;
-    XSum t;
-    xs_zero(t);
-    const XSum* P = a.part + slot * kRedBlocks;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-      const long long* q = reinterpret_cast<const long long*>(P + i);
-#pragma unroll
-      for (int j = 0; j < kXD; ++j) t.d[j] += __ldcg(q + j);
-      t.flags |= __ldcg(q + kXD);
-    }
-    xs_block_sum(t, sh);
-    if (threadIdx.x == 0) a.scal[SC_RED + slot] = xs_round(t);
-  }
-  if (threadIdx.x == 0) a.red_count[cslot] = 0;
+  if (slot0 >= 0) cta_partial(a, x0, slot0, sh);
+  if (slot1 >= 0) cta_partial(a, x1, slot1, sh);
+  if (!cta_last(a, slot0 >= 0 ? slot0 : slot1)) return;
+  if (slot0 >= 0) total_of(a, slot0, sh);
+  if (slot1 >= 0) total_of(a, slot1, sh);
 }
 
 // y_b (lanes 0..11 hold row lane) = (A x)_b for block row b
@@ -145,8 +152,6 @@ __device__ inline bool solver_done(const int* dstat) {
 // the current Krylov iteration (device counter, 1 at the first iteration, advanced by
 // k_loop_end); iterations beyond the limit do nothing
 __device__ inline int iteration(const SolverArgs& a) { return a.dstat[DS_IT]; }
-
-constexpr int kSlotRzNew = -2;  // k_apply: the r.z slot of the current iteration's new value
 
 // Last kernel of a loop iteration (one thread): advances the iteration counter, makes the
 // convergence test of the next iteration's first kernel (PCG: r.z against the threshold;
@@ -312,11 +317,9 @@ __global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, const int*
 
 // out = M^-1 in, one warp per cluster: lane i computes rows i, i + 32, ... of the cluster's
 // dense inverse times the gathered input, summing over the columns in order; partial in.out
-// into slot (if >= 0); also copies out into copy (if not null)
-__global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out,
-                                              double* copy, int slot) {
+// into slot (if >= 0)
+__global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out, int slot) {
   if (it_guard && (solver_done(a.dstat) || iteration(a) > a.maxit)) return;
-  if (slot == kSlotRzNew) slot = (iteration(a) & 1) ? SL_RZ1 : SL_RZ0;
   constexpr int NWA = AT / 32;
   __shared__ double vs[NWA][12 * kMaxCluster];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -335,7 +338,6 @@ __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const 
       for (int j = 0; j < D; ++j) acc += row[j] * vs[warp][j];
       const size_t gi = (size_t)a.cl_body[base + i / 12] * 12 + i % 12;
       out[gi] = acc;
-      if (copy) copy[gi] = acc;
       if (slot >= 0) xs_add(d0, vs[warp][i] * acc);
     }
     __syncwarp();
@@ -343,26 +345,83 @@ __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const 
   if (slot >= 0) cta_partials(a, d0, d1, slot, -1);
 }
 
-// ---- r = b - A x (+ rh = r, p = v = 0 for BiCGSTAB) ----
-__global__ void __launch_bounds__(256) k_residual(SolverArgs a, const double* bvec, const double* x, double* r,
-                                                  double* rh, double* pv, double* v) {
-  const int lane = threadIdx.x & 31;
-  XSum d0, d1;
-  xs_zero(d0);
-  xs_zero(d1);
-  FOR_BODIES(b) {
-    const double ax = row_product(a, b, x);
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      const double ri = bvec[i] - ax;
-      r[i] = ri;
-      if (rh) rh[i] = ri;
-      if (pv) pv[i] = 0.0;
-      if (v) v[i] = 0.0;
-      xs_add(d0, ri * ri);
+// ---- the solve's set-up ----
+// One launch, one warp per cluster (every body is in exactly one): the residual r = b - A x of
+// the cluster's bodies (BiCGSTAB: also rh = r, p = v = 0), z = M^-1 r (PCG: also p = z) and
+// M^-1 b, with the exact partials of b.M^-1 b, r.r and r.z -- the arithmetic of the row
+// kernels and of k_apply, entry for entry.  The last CTA rounds the three totals and starts
+// the solve: the threshold tol^2 b.M^-1 b, the scalars, the iteration counter, the outcome
+// flags and the WHILE node's condition (set at every solve: the loop's node may sit inside
+// another conditional node, whose launches do not reset it).  With b.M^-1 b <= 0 the solution
+// is 0 (x is cleared) and no iteration runs.
+__global__ void __launch_bounds__(AT) k_krylov_setup(SolverArgs a, const double* bvec, double* x, double* r,
+                                                     double* z, double* pz, double* rh, double* p0, double* v0,
+                                                     double tol2, cudaGraphConditionalHandle h) {
+  constexpr int NWA = AT / 32;
+  __shared__ double vr[NWA][12 * kMaxCluster], vb[NWA][12 * kMaxCluster];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  XSum bz, rr, rz;
+  xs_zero(bz);
+  xs_zero(rr);
+  xs_zero(rz);
+  const int ncl = *a.ncl_dev;
+  for (int c = blockIdx.x * NWA + warp; c < ncl; c += gridDim.x * NWA) {
+    const int base = a.cl_ptr[c], sz = a.cl_ptr[c + 1] - base, D = 12 * sz;
+    for (int m = 0; m < sz; ++m) {
+      const int b = a.cl_body[base + m];
+      const double ax = row_product(a, b, x);
+      if (lane < 12) {
+        const size_t i = (size_t)b * 12 + lane;
+        const double bi = bvec[i], ri = bi - ax;
+        r[i] = ri;
+        if (rh) rh[i] = ri;
+        if (p0) p0[i] = 0.0;
+        if (v0) v0[i] = 0.0;
+        xs_add(rr, ri * ri);
+        vr[warp][12 * m + lane] = ri;
+        vb[warp][12 * m + lane] = bi;
+      }
     }
+    __syncwarp();
+    const double* Kc = a.cl_inv + a.cl_off[c];
+    for (int i = lane; i < D; i += 32) {
+      double ar = 0.0, ab = 0.0;
+      const double* row = Kc + (size_t)i * D;
+      for (int j = 0; j < D; ++j) {
+        const double k = row[j];
+        ar += k * vr[warp][j];
+        ab += k * vb[warp][j];
+      }
+      const size_t gi = (size_t)a.cl_body[base + i / 12] * 12 + i % 12;
+      z[gi] = ar;
+      if (pz) pz[gi] = ar;
+      xs_add(rz, vr[warp][i] * ar);
+      xs_add(bz, vb[warp][i] * ab);
+    }
+    __syncwarp();
   }
-  cta_partials(a, d0, d1, SL_RHR, -1);
+  __shared__ XSum sh[NWA];
+  cta_partial(a, bz, SL_BZ, sh);
+  cta_partial(a, rr, SL_RHR, sh);
+  cta_partial(a, rz, SL_RZ0, sh);
+  if (!cta_last(a, SL_BZ)) return;
+  total_of(a, SL_BZ, sh);
+  total_of(a, SL_RHR, sh);
+  total_of(a, SL_RZ0, sh);
+  __syncthreads();  // the totals, stored by thread 0
+  const double b = a.scal[SC_RED + SL_BZ];
+  if (!(b > 0.0))
+    for (int i = threadIdx.x; i < 12 * a.n; i += AT) x[i] = 0.0;
+  if (threadIdx.x == 0) {
+    a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
+    a.scal[SC_THR2] = tol2 * b;
+    a.dstat[DS_IT] = 1;
+    // the solve's outcome flags start clear (the iterations that follow set and read them)
+    a.dstat[DS_R_DONE] = b > 0.0 ? 0 : 1;
+    a.dstat[DS_S_DONE] = 0;
+    a.dstat[DS_SOLVER_ITERS] = 0;
+    cudaGraphSetConditional(h, (b > 0.0 && a.maxit >= 1) ? 1u : 0u);
+  }
 }
 
 // ---- PCG ----
@@ -396,9 +455,11 @@ __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, const double* pv, d
   cta_partials(a, d0, d1, SL_PAP, -1);
 }
 
-// K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature)
-__global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, const double* pv, const double* Ap, double* x,
-                                               double* r) {
+// K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature); then
+// z = M^-1 r with the partial r.z into the new slot.  One warp per cluster: the update of the
+// cluster's bodies, then the product of k_apply over the updated r.
+__global__ void __launch_bounds__(AT) k_pcg_2(SolverArgs a, const double* pv, const double* Ap, double* x, double* r,
+                                              double* z) {
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
@@ -413,18 +474,39 @@ __global__ void __launch_bounds__(256) k_pcg_2(SolverArgs a, const double* pv, c
     return;
   }
   const double alpha = sc[0] / sc[1];
-  const int lane = threadIdx.x & 31;
-  FOR_BODIES(b) {
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      x[i] += alpha * pv[i];
-      r[i] -= alpha * Ap[i];
+  constexpr int NWA = AT / 32;
+  __shared__ double vs[NWA][12 * kMaxCluster];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
+  const int ncl = *a.ncl_dev;
+  for (int c = blockIdx.x * NWA + warp; c < ncl; c += gridDim.x * NWA) {
+    const int base = a.cl_ptr[c], sz = a.cl_ptr[c + 1] - base, D = 12 * sz;
+    if (lane < 12)
+      for (int m = 0; m < sz; ++m) {
+        const size_t i = (size_t)a.cl_body[base + m] * 12 + lane;
+        x[i] += alpha * pv[i];
+        const double ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        vs[warp][12 * m + lane] = ri;
+      }
+    __syncwarp();
+    const double* Kc = a.cl_inv + a.cl_off[c];
+    for (int i = lane; i < D; i += 32) {
+      double acc = 0.0;
+      const double* row = Kc + (size_t)i * D;
+      for (int j = 0; j < D; ++j) acc += row[j] * vs[warp][j];
+      z[(size_t)a.cl_body[base + i / 12] * 12 + i % 12] = acc;
+      xs_add(d0, vs[warp][i] * acc);
     }
+    __syncwarp();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.dstat[DS_SOLVER_ITERS] = it;
+  cta_partials(a, d0, d1, (it & 1) ? SL_RZ1 : SL_RZ0, -1);
 }
 
-// K3 (after z = M r with partial r.z into the new slot): beta = rz_new / rz_old; p = z + beta p
+// K3 (after K2's z = M^-1 r and r.z in the new slot): beta = rz_new / rz_old; p = z + beta p
 __global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, const double* z, double* pv) {
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
@@ -561,27 +643,6 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, c
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scal[SC_OMEGA] = omega;
     a.dstat[DS_SOLVER_ITERS] = it;
-  }
-}
-
-// Threshold thr^2 = tol^2 b^T M^-1 b and the recurrence scalars; b = 0 gives x = 0 and ends
-// the solve before its first iteration
-// (and the iteration loop's condition: enter it unless the solve is already done; the loop's
-// node may sit inside another conditional node, whose launches do not reset it)
-__global__ void __launch_bounds__(256) k_solver_init(SolverArgs a, double tol2, double* x,
-                                                     cudaGraphConditionalHandle h) {
-  const double b = a.scal[SC_RED + SL_BZ];
-  if (!(b > 0.0))
-    for (int i = blockIdx.x * 256 + threadIdx.x; i < 12 * a.n; i += (int)gridDim.x * 256) x[i] = 0.0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
-    a.scal[SC_THR2] = tol2 * b;
-    a.dstat[DS_IT] = 1;
-    // the solve's outcome flags start clear (the iterations that follow set and read them)
-    a.dstat[DS_R_DONE] = b > 0.0 ? 0 : 1;
-    a.dstat[DS_S_DONE] = 0;
-    a.dstat[DS_SOLVER_ITERS] = 0;
-    cudaGraphSetConditional(h, (b > 0.0 && a.maxit >= 1) ? 1u : 0u);
   }
 }
 
@@ -824,17 +885,12 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
   if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr) != cudaSuccess ||
       cs != cudaStreamCaptureStatusActive)
     return ABD_ERR_CUDA;
-  // the loop's handle first: k_solver_init sets its value
+  // the loop's handle first: k_krylov_setup sets its value
   cudaGraphConditionalHandle h;
   if (ABD_NOTE(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return ABD_ERR_CUDA;
-  // b^T M^-1 b sets the threshold
-  k_apply<<<s.red_grid, AT, 0, st>>>(a, 0, bvec, s.zb, nullptr, SL_BZ);
-  k_residual<<<s.red_grid, 256, 0, st>>>(a, bvec, x, s.r, pcg ? nullptr : s.rh, pcg ? nullptr : s.pv,
-                                         pcg ? nullptr : s.v);
-  k_solver_init<<<s.red_grid, 256, 0, st>>>(a, s.prm.cg_tol * s.prm.cg_tol, x, h);
-  // z = M^-1 r (and p = z for PCG) with r.z into the slot K1 of iteration 1 reads
-  k_apply<<<s.red_grid, AT, 0, st>>>(a, 0, s.r, s.z, pcg ? s.pv : nullptr, SL_RZ0);
-  s.launches += 4;
+  k_krylov_setup<<<s.red_grid, AT, 0, st>>>(a, bvec, x, s.r, s.z, pcg ? s.pv : nullptr, pcg ? nullptr : s.rh,
+                                           pcg ? nullptr : s.pv, pcg ? nullptr : s.v, s.prm.cg_tol * s.prm.cg_tol, h);
+  ++s.launches;
   // the iteration loop: a WHILE node on the capture, its body captured on a second stream
   const cudaGraphNode_t* deps = nullptr;
   size_t ndeps = 0;
@@ -856,22 +912,21 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
     return ABD_ERR_CUDA;
   if (pcg) {
     k_pcg_1<<<s.red_grid, 256, 0, bs>>>(a, s.pv, s.v);
-    k_pcg_2<<<s.red_grid, 256, 0, bs>>>(a, s.pv, s.v, x, s.r);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.z, nullptr, kSlotRzNew);
+    k_pcg_2<<<s.red_grid, AT, 0, bs>>>(a, s.pv, s.v, x, s.r, s.z);
     k_pcg_3<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.pv);
   } else {
     k_bicg_1<<<s.red_grid, 256, 0, bs>>>(a, s.r, s.pv, s.v);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.pv, s.y, nullptr, -1);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.pv, s.y, -1);
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
     k_bicg_3<<<s.red_grid, 256, 0, bs>>>(a, s.r, s.v, s.s);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.s, s.z, nullptr, SL_SZ);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.s, s.z, SL_SZ);
     k_bicg_4<<<s.red_grid, 256, 0, bs>>>(a, s.y, x);
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
     k_bicg_6<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.ddq, nullptr, SL_RZ0);
+    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.ddq, SL_RZ0);
   }
   k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
-  if (per_iter_out) *per_iter_out = pcg ? 5 : 10;
+  if (per_iter_out) *per_iter_out = pcg ? 4 : 10;
   cudaGraph_t body_out = nullptr;
   const cudaError_t eb = ABD_NOTE(cudaGetLastError());
   if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
