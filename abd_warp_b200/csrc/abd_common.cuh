@@ -588,10 +588,9 @@ cudaError_t dots(Sim& s, const double* a, const double* b, const double* c, cons
 // linesearch.cu
 // Energies at (A, p) - alpha_k dq for the dpar[kParK] step lengths dpar[kParAlpha + k] in
 // [0, 1], from the candidates of the last CCD_LS pass between (A, p) and (A, p) - dq, into
-// the mailbox's ls_energy[k]
-cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p);
-// the trial count and step lengths of a batch (dpar) from the last CCD pass's time of impact
-cudaError_t ls_setup_from_ccd(Sim& s);
+// the mailbox's ls_energy[k].  from_ccd: directly after that pass, which cleared ls_energy;
+// the trials then come from its time of impact and are written to dpar.
+cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p, bool from_ccd);
 
 // solver.cu
 // The preconditioner: cluster_tables forms the clusters on the device from the last GH pass's
@@ -604,11 +603,10 @@ int prepare_solver(Sim& s);
 // returns ABD status; iters == null: enqueue only (krylov_outcome after the next mailbox read)
 int krylov_solve(Sim& s, double* x, int* iters, GraphSlot* slot = nullptr);
 int krylov_outcome(Sim& s);                       // iterations of the last solve
-// Enqueues a solve (setup kernels and the WHILE node of its iterations) into the graph being
-// captured on s.stream, for the device-driven Newton loop; its outcome is added to the
-// mailbox's step counters by krylov_tally.
+// Enqueues a solve (its set-up kernel and the WHILE node of its iterations) into the graph
+// being captured on s.stream, for the device-driven Newton loop; the solve adds its outcome to
+// the mailbox's step counters where it ends.
 int krylov_issue(Sim& s, double* x);
-cudaError_t krylov_tally(Sim& s);
 
 // newton.cu: the kernels of the device-driven Newton loop (abd_step when the parameters'
 // newton_loop is 0).  Each enqueues on s.stream.

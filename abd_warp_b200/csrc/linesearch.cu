@@ -39,7 +39,10 @@ struct LsArgs {
   const int* vbody;
   const double* x0;
   const double *A, *p, *dq;     // the iterate and the search direction
-  const double* dpar;           // [kParK] trial count, [kParAlpha + k] step lengths
+  double* dpar;                 // [kParK] trial count, [kParAlpha + k] step lengths
+  const unsigned long long* toi_key;  // the CCD pass's minimum time of impact: the trials are
+                                      // derived from it (and written to dpar), or null: given
+  double alpha_min;
   abd_states st;
   const double *mass, *I0;
   const int* fixed;
@@ -53,7 +56,25 @@ struct LsArgs {
   int cap_fric;
 };
 
-__device__ inline int ls_trials(const LsArgs& a) { return (int)a.dpar[kParK]; }
+// The trials of a batch from the CCD pass's minimum time of impact (its complemented bits,
+// 0: none below 1): the step bound alpha = clamp(toi, 0, 1), times 0.9 below 1 (ccd,
+// abd.py:278-303), then alpha, alpha / 2, ... up to the first below alpha_min, at most kLsMax
+// -- the host's trial_steps.  Returns the step length of trial k (< *K) and the count *K.
+__device__ inline double trial_from_toi(unsigned long long key, double alpha_min, int k, int* K) {
+  double toi = 1.0;
+  if (key) toi = __longlong_as_double((long long)~key);
+  const double lo = toi < 1.0 ? toi : 1.0;  // std::min(1.0, toi), std::max(0.0, .)
+  double t = 0.0 < lo ? lo : 0.0;
+  if (t < 1.0) t *= 0.9;
+  double al = t;
+  int n = 1;
+  for (double s = t; n < kLsMax && !(s < alpha_min); ++n) {
+    s *= 0.5;
+    if (n == k) al = s;
+  }
+  *K = n;
+  return al;
+}
 
 // The exact FP32 box of body b at (A, p) - al dq (culling2.py:278-334): FP64 min / max of
 // its vertices, dilated by dhat / 2 in FP64, rounded to FP32 (one thread, rare case)
@@ -105,8 +126,21 @@ __device__ inline d3 position_at(const LsArgs& a, const double M[12], int v) {
 // bodies' inertia + orthogonality terms.
 __global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv, int Gf) {
   const int k = blockIdx.y;
-  if (k >= ls_trials(a)) return;
-  const double al = a.dpar[kParAlpha + k];
+  double al;
+  if (a.toi_key) {  // every CTA derives its trial; CTA (0, 0) writes the batch out for the accept
+    const unsigned long long key = *a.toi_key;
+    int K;
+    al = trial_from_toi(key, a.alpha_min, k, &K);
+    if (blockIdx.x == 0 && k == 0 && (int)threadIdx.x <= K) {
+      const double aj = trial_from_toi(key, a.alpha_min, (int)threadIdx.x - 1, &K);
+      if (threadIdx.x == 0) a.dpar[kParK] = K;
+      else a.dpar[kParAlpha + threadIdx.x - 1] = aj;
+    }
+    if (k >= K) return;
+  } else {
+    if (k >= (int)a.dpar[kParK]) return;
+    al = a.dpar[kParAlpha + k];
+  }
   __shared__ XSum acc;
   if (threadIdx.x <= kXD) reinterpret_cast<long long*>(&acc)[threadIdx.x] = 0;
   __syncthreads();
@@ -218,34 +252,9 @@ __global__ void __launch_bounds__(128) k_ls_eval(LsArgs a, int G, int Gv, int Gf
   }
 }
 
-// The trials of a batch from the CCD pass's minimum time of impact, on the device (one
-// thread): the step bound alpha = clamp(toi, 0, 1), times 0.9 below 1 (ccd, abd.py:278-303),
-// then alpha, alpha / 2, ... up to the first below alpha_min, at most kLsMax -- the same
-// arithmetic as the host's.
-__global__ void k_ls_setup(const unsigned long long* toi_key, double alpha_min, double* dpar) {
-  double toi = 1.0;
-  if (const unsigned long long key = *toi_key) toi = __longlong_as_double((long long)~key);
-  const double lo = toi < 1.0 ? toi : 1.0;  // std::min(1.0, toi), std::max(0.0, .)
-  double t = 0.0 < lo ? lo : 0.0;
-  if (t < 1.0) t *= 0.9;
-  int K = 0;
-  for (double al = t; K < kLsMax;) {
-    dpar[kParAlpha + K++] = al;
-    if (al < alpha_min) break;
-    al *= 0.5;
-  }
-  dpar[kParK] = K;
-}
-
 }  // namespace
 
-cudaError_t ls_setup_from_ccd(Sim& s) {
-  k_ls_setup<<<1, 1, 0, s.stream>>>(s.dmin, s.prm.alpha_min, s.dpar);
-  ++s.launches;
-  return cudaGetLastError();
-}
-
-cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p) {
+cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const double* p, bool from_ccd) {
   LsArgs a;
   a.prm = s.prm;
   a.n = s.n;
@@ -267,8 +276,12 @@ cudaError_t ls_energies(Sim& s, const abd_states& st, const double* A, const dou
   a.cap_ecand = s.cap_ecand;
   a.dstat = s.dstat;
   a.energy = s.box->ls_energy;
-  cudaError_t e = cudaMemsetAsync(a.energy, 0, sizeof(XSum) * kLsMax, s.stream);
-  if (e != cudaSuccess) return e;
+  a.toi_key = from_ccd ? s.dmin : nullptr;
+  a.alpha_min = s.prm.alpha_min;
+  if (!from_ccd) {  // (the CCD_LS pass clears them otherwise)
+    const cudaError_t e = cudaMemsetAsync(a.energy, 0, sizeof(XSum) * kLsMax, s.stream);
+    if (e != cudaSuccess) return e;
+  }
   a.fric = s.prm.friction_mu > 0.0 ? s.fric : nullptr;
   a.cap_fric = s.cap_fric;
   const int G = kRedBlocks;

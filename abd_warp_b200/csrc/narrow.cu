@@ -75,9 +75,10 @@ struct NarrowArgs {
   int4* ecand;                  // CCD_LS: line-search candidates
   int cap_contacts;
   int4 *contacts, *contacts_by_pair;
-  XSum* energy;
+  XSum* energy;                  // exact energy of the pass
+  XSum* ls_energy;               // CCD_LS: the energies of the line-search batch that follows
   int prof;                     // kernel profiling: count the data read into prof rows
-  unsigned long long* prof_rows;                       // exact energy of the pass
+  unsigned long long* prof_rows;
   unsigned long long* toi_key;        // complemented bits of the minimum time of impact
   abd_states st;
   const double *mass, *I0;
@@ -1133,9 +1134,15 @@ __global__ void __launch_bounds__(CT, 5) k_chunk_narrow(NarrowArgs a) {
 // Times of impact of the CCD candidates, one thread per candidate (ccd.py:20-40, 133-186);
 // the minimum below 1 goes to the mailbox key.  LS: the candidates are the line-search
 // candidates of a CCD_LS pass, and each is first put to the CCD pass's own culling
-// predicate: the exact swept body boxes overlap and the two swept primitive boxes overlap.
+// predicate: the exact swept body boxes overlap and the two swept primitive boxes overlap;
+// block 0 also clears the energies of the line-search batch that follows the pass.
 template <bool LS>
 __global__ void __launch_bounds__(128) k_ccd_eval(NarrowArgs a) {
+  if (LS && blockIdx.x == 0) {
+    static_assert(sizeof(XSum) == (kXD + 1) * sizeof(long long), "XSum layout");
+    for (int i = threadIdx.x; i < kLsMax * (kXD + 1); i += blockDim.x)
+      reinterpret_cast<long long*>(a.ls_energy)[i] = 0;
+  }
   const int n = LS ? min(a.dstat[DS_NECAND], a.cap_ecand) : min(a.dstat[DS_NCCD], a.cap_ccd);
   if (a.dstat[DS_STATUS] & (LS ? ST_ECAND_OVERFLOW : ST_CCD_OVERFLOW)) return;
   const int4* cand = LS ? a.ecand : a.ccd_cand;
@@ -1697,6 +1704,7 @@ NarrowArgs narrow_args(Sim& s, int mode, const double* A, const double* p, const
   a.contacts = s.contacts;
   a.contacts_by_pair = s.contacts_by_pair;
   a.toi_key = s.dmin;
+  a.ls_energy = s.box->ls_energy;
   a.st = st ? *st : abd_states{};
   a.mass = s.mass;
   a.I0 = s.I0;

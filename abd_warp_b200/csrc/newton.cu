@@ -62,7 +62,7 @@ __global__ void k_gate(Mailbox* box, cudaGraphConditionalHandle h, int* sup_have
   }
 }
 
-// Backtracking line search (abd.py:146-160) over the trials of the batch (k_ls_setup's step
+// Backtracking line search (abd.py:146-160) over the trials of the batch (k_ls_eval's step
 // lengths alpha, alpha / 2, ... to the first below alpha_min): the first trial that passes
 // the Armijo test, or the first below alpha_min, is taken, as the sequential search takes it.
 // A batch whose trials all fail while none is below alpha_min raises ST_LS_MORE (the host

@@ -421,7 +421,7 @@ int ccd_at(abd_sim* h, const double* A, const double* p, const double* A1, const
 // Enqueues the energies at (A, p) - al[k] dq, k < K <= kLsMax, 0 <= al[k] <= 1, from the
 // candidates of the last CCD_LS pass between (A, p) and (A, p) - dq, with the mailbox copy: one
 // replayed pass.  al == null: the step lengths follow from that pass's time of impact on the
-// device (k_ls_setup).  Each energy is bitwise the energy pass's at the same DOFs.
+// device (k_ls_eval derives them).  Each energy is bitwise the energy pass's at the same DOFs.
 int ls_launch(abd_sim* h, const abd_states& st, const double* A, const double* p, const double* al, int K,
               uint64_t key) {
   Sim& s = h->s;
@@ -434,9 +434,7 @@ int ls_launch(abd_sim* h, const abd_states& st, const double* A, const double* p
     if (al)
       CK(cudaMemcpyAsync(s.dpar + abd::kParK, s.hpar + abd::kParK, sizeof(double) * (1 + abd::kLsMax),
                          cudaMemcpyHostToDevice, s.stream));
-    else
-      CK(abd::ls_setup_from_ccd(s));
-    CK(abd::ls_energies(s, st, A, p));
+    CK(abd::ls_energies(s, st, A, p, !al));
     CK(cudaMemcpyAsync(s.hbox, s.box, sizeof(abd::Mailbox), cudaMemcpyDeviceToHost, s.stream));
     return ABD_OK;
   };
@@ -446,7 +444,7 @@ int ls_launch(abd_sim* h, const abd_states& st, const double* A, const double* p
 }
 
 // The trial step lengths of a line search from the bound alpha: alpha, alpha / 2, ... up to
-// the first below alpha_min, at most kLsMax (the device's k_ls_setup makes the same list)
+// the first below alpha_min, at most kLsMax (the device's k_ls_eval makes the same list)
 int trial_steps(double alpha, double alpha_min, double* al) {
   int K = 0;
   for (double a_ = alpha; K < abd::kLsMax;) {
@@ -1237,13 +1235,11 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
   auto iteration_tail = [&]() -> int {  // after a GH pass without overflow (the IF body)
     if (int r = abd::cluster_inverse(s)) return r;
     if (int r = abd::krylov_issue(s, s.dq)) return r;
-    CK(abd::krylov_tally(s));
     // the CCD bound between q and q - dq with the line-search candidates (abd.py:278-303),
     // Ak, pk = q - dq; the trials of the line search; the accepted step
     const abd::Dofs d0 = direct(st.A, st.p), d1 = updated(s, st.A, st.p, 1, st.Ak, st.pk);
     if (int r = ccd_issue(h, d0, d1, abd::NARROW_CCD_LS, dots)) return r;
-    CK(abd::ls_setup_from_ccd(s));
-    CK(abd::ls_energies(s, st, st.A, st.p));
+    CK(abd::ls_energies(s, st, st.A, st.p, true));
     CK(abd::ls_accept(s));
     CK(abd::update_dofs_dev(s, st.A, st.p, st.Ak, st.pk));
     return ABD_OK;

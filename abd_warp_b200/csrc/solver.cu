@@ -59,6 +59,7 @@ struct SolverArgs {
   int* red_count;    // [kRedSlots] CTAs that delivered their partial
   double* scal;
   int* dstat;
+  Mailbox* tally;    // device loop: the solve's outcome goes to the step's counters (else null)
 };
 
 constexpr int SC_RED = 16;  // scal[SC_RED + slot]: the rounded total of reduction `slot`
@@ -153,10 +154,19 @@ __device__ inline bool solver_done(const int* dstat) {
 // k_loop_end); iterations beyond the limit do nothing
 __device__ inline int iteration(const SolverArgs& a) { return a.dstat[DS_IT]; }
 
+// The outcome of a finished solve into the device loop's step counters (a.tally): its
+// iterations, and the non-convergence bit when it stopped at cg_max_iter (one thread)
+__device__ inline void tally_solve(const SolverArgs& a) {
+  if (!a.tally) return;
+  a.tally->step.lin += a.dstat[DS_SOLVER_ITERS];
+  if (!(a.dstat[DS_R_DONE] || a.dstat[DS_S_DONE])) atomicOr(&a.dstat[DS_STATUS], ST_SOLVER_NOCONV);
+}
+
 // Last kernel of a loop iteration (one thread): advances the iteration counter, makes the
 // convergence test of the next iteration's first kernel (PCG: r.z against the threshold;
 // BiCGSTAB: r.M^-1 r and rho = rh.r), records a stop as that kernel would, and sets the
-// WHILE node's condition.  The loop ends at convergence or after maxit iterations.
+// WHILE node's condition.  The loop ends at convergence or after maxit iterations (and the
+// solve's outcome is tallied).
 __global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) {
   const int it = a.dstat[DS_IT];
   bool stop = solver_done(a.dstat) || it + 1 > a.maxit;
@@ -174,6 +184,7 @@ __global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) 
     }
   }
   a.dstat[DS_IT] = it + 1;
+  if (stop) tally_solve(a);
   cudaGraphSetConditional(h, stop ? 0u : 1u);
 }
 
@@ -353,7 +364,7 @@ __global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const 
 // the solve: the threshold tol^2 b.M^-1 b, the scalars, the iteration counter, the outcome
 // flags and the WHILE node's condition (set at every solve: the loop's node may sit inside
 // another conditional node, whose launches do not reset it).  With b.M^-1 b <= 0 the solution
-// is 0 (x is cleared) and no iteration runs.
+// is 0 (x is cleared) and no iteration runs; a solve without iterations is tallied here.
 __global__ void __launch_bounds__(AT) k_krylov_setup(SolverArgs a, const double* bvec, double* x, double* r,
                                                      double* z, double* pz, double* rh, double* p0, double* v0,
                                                      double tol2, cudaGraphConditionalHandle h) {
@@ -420,7 +431,9 @@ __global__ void __launch_bounds__(AT) k_krylov_setup(SolverArgs a, const double*
     a.dstat[DS_R_DONE] = b > 0.0 ? 0 : 1;
     a.dstat[DS_S_DONE] = 0;
     a.dstat[DS_SOLVER_ITERS] = 0;
-    cudaGraphSetConditional(h, (b > 0.0 && a.maxit >= 1) ? 1u : 0u);
+    const bool loop = b > 0.0 && a.maxit >= 1;
+    if (!loop) tally_solve(a);
+    cudaGraphSetConditional(h, loop ? 1u : 0u);
   }
 }
 
@@ -646,16 +659,9 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, c
   }
 }
 
-// The outcome of the last solve into the device loop's step counters: its iterations, and
-// the non-convergence bit when it stopped at cg_max_iter
-__global__ void k_krylov_tally(Mailbox* box) {
-  const int* ds = box->dstat;
-  box->step.lin += ds[DS_SOLVER_ITERS];
-  if (!(ds[DS_R_DONE] || ds[DS_S_DONE])) box->dstat[DS_STATUS] |= ST_SOLVER_NOCONV;
-}
-
 SolverArgs solver_args(Sim& s) {
   SolverArgs a;
+  a.tally = nullptr;
   a.n = s.n;
   a.diag = s.diag;
   a.offdiag = s.offdiag;
@@ -872,11 +878,15 @@ int build_preconditioner(Sim& s) {
   return cluster_inverse(s);
 }
 
+// kernels of one iteration of the loop's body: PCG or BiCGSTAB, k_loop_end included
+constexpr int iteration_kernels(bool pcg) { return pcg ? 4 : 10; }
+
 // Enqueues a solve on s.stream, which must be capturing: the setup kernels, then a WHILE node
 // whose body is one iteration (its last kernel sets the loop condition), the body captured on
 // cap_stream2.  Counts the setup's launches and, in *per_iter, one iteration's.
-int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
-  const SolverArgs a = solver_args(s);
+int krylov_capture(Sim& s, double* x, long long* per_iter_out, bool tally) {
+  SolverArgs a = solver_args(s);
+  a.tally = tally ? s.box : nullptr;
   const double* bvec = s.g;
   const bool pcg = s.prm.solver == 1;
   cudaStream_t st = s.stream;
@@ -926,7 +936,7 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out) {
     k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.ddq, SL_RZ0);
   }
   k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
-  if (per_iter_out) *per_iter_out = pcg ? 4 : 10;
+  if (per_iter_out) *per_iter_out = iteration_kernels(pcg);
   cudaGraph_t body_out = nullptr;
   const cudaError_t eb = ABD_NOTE(cudaGetLastError());
   if (cudaStreamEndCapture(bs, &body_out) != cudaSuccess || eb != cudaSuccess) return ABD_ERR_CUDA;
@@ -943,7 +953,7 @@ int krylov_solve(Sim& s, double* x, int* iters_out, GraphSlot* slot) {
   kh.add(s.cap_gen).add(s.adj_col).add(s.adj_pair).add(s.ij).add(s.offdiag).add(s.pair_active);
   int r = run_graph(s, slot ? *slot : s.g_kinit, kh.h, [&]() -> int {
     long long per_iter = 0;
-    const int q = krylov_capture(s, x, &per_iter);
+    const int q = krylov_capture(s, x, &per_iter, false);
     s.launches += per_iter;  // the graph's count covers one iteration
     return q;
   });
@@ -957,22 +967,16 @@ int krylov_solve(Sim& s, double* x, int* iters_out, GraphSlot* slot) {
 
 int krylov_issue(Sim& s, double* x) {
   long long per_iter = 0;
-  const int r = krylov_capture(s, x, &per_iter);
+  const int r = krylov_capture(s, x, &per_iter, true);
   s.step_launch[2] = per_iter;  // the setup's kernels are counted with the Newton iteration's
   return r;
-}
-
-cudaError_t krylov_tally(Sim& s) {
-  k_krylov_tally<<<1, 1, 0, s.stream>>>(s.box);
-  ++s.launches;
-  return cudaGetLastError();
 }
 
 // The last solve's iterations, from the host's copy of the mailbox; non-convergence raises
 // ST_SOLVER_NOCONV in the host status bits.
 int krylov_outcome(Sim& s) {
   const int* ds = s.hbox->dstat;
-  const int per_iter = s.prm.solver == 1 ? 5 : 10;
+  const int per_iter = iteration_kernels(s.prm.solver == 1);
   // the graph's launch count covers one iteration; the loop ran ds[DS_IT] - 1
   s.launches += (long long)per_iter * std::max(0, ds[DS_IT] - 2);
   if (!(ds[DS_R_DONE] || ds[DS_S_DONE])) s.host_status |= ST_SOLVER_NOCONV;
