@@ -392,9 +392,24 @@ __global__ void __launch_bounds__(NT) k_pair_lists(NarrowArgs a) {
 // ---------------------------------------------------------------------------------------
 // GH assembly: the active contacts found by the chunk pass, grouped by body pair
 // ---------------------------------------------------------------------------------------
+// contacts into their pair's segment, thread k taking contacts k, k + stride, ... (the order
+// inside a segment does not matter: the assembly sums exactly)
+__device__ inline void scatter_contacts(int k, int stride, int cap_contacts, const int4* __restrict__ in,
+                                        int* pair_cand, int4* out, const int* dstat) {
+  for (const int m = min(dstat[DS_NCONTACT], cap_contacts); k < m; k += stride) {
+    const int4 c = in[k];
+    out[pair_cand[4 * c.x] + atomicAdd(&pair_cand[4 * c.x + 2], 1)] = c;
+  }
+}
+
+// Lists of at most this many contacts are scattered by the scan's CTA itself
+constexpr int kScanScatter = 16384;
+
 // single CTA: per-pair offsets of the contact lists (pair_cand[4p] = offset, [4p+1] = count,
-// [4p+2] = fill cursor); skipped when the pass overflowed (the host reruns it)
-__global__ void __launch_bounds__(1024) k_contact_scan(int cap_pairs, int* pair_cand, int* dstat) {
+// [4p+2] = fill cursor); with `in` (a list of at most kScanScatter), then the contacts into
+// their segments.  Skipped when the pass overflowed (the host reruns it).
+__global__ void __launch_bounds__(1024) k_contact_scan(int cap_pairs, int* pair_cand, int* dstat, int cap_contacts,
+                                                       const int4* __restrict__ in, int4* out) {
   if (dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
   const int np = min(dstat[DS_NPAIRS], cap_pairs);
   __shared__ int sh[33];
@@ -430,17 +445,16 @@ __global__ void __launch_bounds__(1024) k_contact_scan(int cap_pairs, int* pair_
     if (threadIdx.x == 0) carry = sh[32];
     __syncthreads();
   }
+  // (the barrier above makes the CTA's offsets and cleared cursors visible to all its threads)
+  if (in) scatter_contacts(threadIdx.x, 1024, cap_contacts, in, pair_cand, out, dstat);
 }
 
-// contacts into their pair's segment (the order inside a segment does not matter: the
-// assembly sums exactly)
+// the contacts into their segments, one thread per contact (lists above kScanScatter)
 __global__ void k_contact_scatter(int cap_contacts, const int4* __restrict__ in, int* pair_cand, int4* out,
                                   const int* dstat) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (dstat[DS_STATUS] & (ST_PAIR_OVERFLOW | ST_CONTACT_OVERFLOW)) return;
-  if (k >= min(dstat[DS_NCONTACT], cap_contacts)) return;
-  const int4 c = in[k];
-  out[pair_cand[4 * c.x] + atomicAdd(&pair_cand[4 * c.x + 2], 1)] = c;
+  scatter_contacts(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, cap_contacts, in, pair_cand, out,
+                   dstat);
 }
 
 // CTAs loop over the body pairs: every active contact of a pair (pt_ipc.py:111-190,
@@ -1840,9 +1854,14 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
         k_fric_pairs<<<kRedBlocks, 128, 0, s.stream>>>(a);
         ++s.launches;
       }
-      k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat);
-      k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts, s.pair_cand,
-                                                                           s.contacts_by_pair, s.dstat);
+      const bool one_cta = s.cap_contacts <= kScanScatter;
+      k_contact_scan<<<1, 1024, 0, s.stream>>>(s.cap_pairs, s.pair_cand, s.dstat, s.cap_contacts,
+                                               one_cta ? s.contacts : nullptr, s.contacts_by_pair);
+      if (!one_cta) {
+        k_contact_scatter<<<blocks(s.cap_contacts, 256), 256, 0, s.stream>>>(s.cap_contacts, s.contacts,
+                                                                             s.pair_cand, s.contacts_by_pair, s.dstat);
+        ++s.launches;
+      }
       constexpr int smem = NOUT * (int)sizeof(XSum);  // 40 KB, under the 48 KB default
       static_assert(smem + sizeof(double) * PT_WARPS * 5 * 24 + 256 <= 48 * 1024, "pair assembly shared memory");
       const int grid = s.cap_pairs < 4 * 148 ? s.cap_pairs : 4 * 148;
@@ -1854,7 +1873,7 @@ cudaError_t narrow(Sim& s, int mode, const double* A, const double* p, const dou
         k_pair_assemble<kAsmFull><<<grid, PT_THREADS, kExactSmem, s.stream>>>(a);
       else
         k_pair_assemble<kAsmRef><<<grid, PT_THREADS, smem, s.stream>>>(a);
-      s.launches += 3;
+      s.launches += 2;
     }
   } else {
     if (s.cap_pairs == 0) return cudaSuccess;

@@ -12,7 +12,8 @@
 * Injected capacity shortfalls (``SimParams.min_capacity``): every list of the simulator starts
   with 16 entries and the breadth-first traversal frontier holds 16 nodes, so each pass runs its
   grow-and-rerun paths and the traversal's depth-first fallback; the steps still equal the
-  oracle's bit for bit.
+  oracle's bit for bit.  Lists started above the contact scan's one-CTA scatter bound take the
+  separate scatter kernel, with the same result.
 * Edge cases: a single free body with no pairs (implicit-Euler free fall in closed form), and a
   scene of fixed bodies only."""
 import os
@@ -133,6 +134,18 @@ def test_injected_capacity_shortfalls(scene):
         st = {k: z[f"s225_{k}"] for k in (*FIELDS, "dq")}
     tiny = dataclasses.replace(prm, min_capacity=16)
     assert _steps_against_oracle(bodies, prm, st, 3, sim_prm=tiny) == 0
+
+
+def test_contact_lists_beyond_the_scan_scatter():
+    """Lists that start with 20,000 entries, more than the 16,384 contacts the contact scan's
+    CTA scatters itself: the GH passes group their contacts with the one-thread-per-contact
+    scatter kernel, and the steps are still the oracle's, bit for bit."""
+    import dataclasses
+    z = np.load(os.path.join(GOLDEN, "c1_trajectory.npz"))
+    bodies, prm, _ = scenes.make_config(1)
+    st = {k: z[f"s200_{k}"] for k in (*FIELDS, "dq")}
+    large = dataclasses.replace(prm, min_capacity=20000)
+    assert _steps_against_oracle(bodies, prm, st, 3, sim_prm=large) == 0
 
 
 def _oracle_and_gpu(bodies, prm):
