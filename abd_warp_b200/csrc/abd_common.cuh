@@ -387,7 +387,7 @@ struct Sim {
   double *g = nullptr, *dq = nullptr, *diag = nullptr;  // [n][12], [n][12], [n][144]
   // Krylov work vectors [n][12]
   double *r = nullptr, *rh = nullptr, *pv = nullptr, *v = nullptr, *y = nullptr, *s = nullptr, *z = nullptr,
-         *t = nullptr, *ddq = nullptr;
+         *t = nullptr;
   // preconditioner clusters (contact-coupled bodies, <= cluster_max each), formed on the
   // device: the tables live in one device block (ClusterTables layout)
   int cl_smem = 0;                               // dynamic shared memory opted in for the inverse

@@ -783,7 +783,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   }
   ok(dalloc(&s.row_ptr, n + 1));
   ok(dalloc(&s.upper_ptr, n + 1));
-  for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t, &s.ddq})
+  for (double** v : {&s.g, &s.dq, &s.r, &s.rh, &s.pv, &s.v, &s.y, &s.s, &s.z, &s.t})
     ok(dalloc(v, 12 * (size_t)n));
   if (ok(cudaMalloc(&s.cl_tab, abd::cluster_tables_bytes(n)))) {
     const abd::ClusterTables t = abd::cluster_tables_at(s.cl_tab, n);
@@ -887,7 +887,7 @@ int abd_sim_destroy(abd_sim* h) {
                   s.fixed, s.x, s.xk, s.body_box, s.pair_mask, s.row_ptr, s.upper_ptr, s.ij, s.adj_col,
                   s.adj_pair, s.pt_list, s.ee_list, s.vg_list, s.pair_cand, s.offdiag, s.pdiag, s.pgrad,
                   s.pair_active, s.pair_val, s.g, s.dq, s.diag,
-                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.ddq, s.partials, s.scal, s.box, s.dpar, s.dint,
+                  s.r, s.rh, s.pv, s.v, s.y, s.s, s.z, s.t, s.partials, s.scal, s.box, s.dpar, s.dint,
                   s.row_cnt, s.upper_cnt, s.nbr, s.fdof, s.chunk_box, s.vperm,
                   s.cl_tab, s.cl_inv, s.pair_wpre, s.act_pairs, s.chunk,
                   s.red_count, s.body_bnd, s.contacts, s.contacts_by_pair, s.ccd_cand, s.ecand, s.body_rest,

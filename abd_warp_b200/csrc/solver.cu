@@ -326,42 +326,41 @@ __global__ void __launch_bounds__(IT) k_cluster_inverse(SolverArgs a, const int*
   }
 }
 
-// out = M^-1 in, one warp per cluster: lane i computes rows i, i + 32, ... of the cluster's
-// dense inverse times the gathered input, summing over the columns in order; partial in.out
-// into slot (if >= 0)
-__global__ void __launch_bounds__(AT) k_apply(SolverArgs a, int it_guard, const double* in, double* out, int slot) {
-  if (it_guard && (solver_done(a.dstat) || iteration(a) > a.maxit)) return;
+// One warp per cluster: the input's entries of the cluster's body rows, in = row_in(i) for the
+// entry i of a member body (lanes 0..11: the row's 12 entries; row_in may also update the
+// body's own entries of other vectors), then out = M^-1 in over the cluster -- lane i
+// computes rows i, i + 32, ... of the cluster's dense inverse times the gathered input,
+// summing over the columns in order -- with the partial in.out added to *dot (if not null);
+// out null: the product only feeds the dot.
+template <class RowIn>
+__device__ inline void cluster_apply(const SolverArgs& a, double* out, XSum* dot, RowIn&& row_in) {
   constexpr int NWA = AT / 32;
   __shared__ double vs[NWA][12 * kMaxCluster];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  XSum d0, d1;
-  xs_zero(d0);
-  xs_zero(d1);
   const int ncl = *a.ncl_dev;
   for (int c = blockIdx.x * NWA + warp; c < ncl; c += gridDim.x * NWA) {
     const int base = a.cl_ptr[c], sz = a.cl_ptr[c + 1] - base, D = 12 * sz;
-    for (int i = lane; i < D; i += 32) vs[warp][i] = in[(size_t)a.cl_body[base + i / 12] * 12 + i % 12];
+    if (lane < 12)
+      for (int m = 0; m < sz; ++m) vs[warp][12 * m + lane] = row_in((size_t)a.cl_body[base + m] * 12 + lane);
     __syncwarp();
     const double* Kc = a.cl_inv + a.cl_off[c];
     for (int i = lane; i < D; i += 32) {
       double acc = 0.0;
       const double* row = Kc + (size_t)i * D;
       for (int j = 0; j < D; ++j) acc += row[j] * vs[warp][j];
-      const size_t gi = (size_t)a.cl_body[base + i / 12] * 12 + i % 12;
-      out[gi] = acc;
-      if (slot >= 0) xs_add(d0, vs[warp][i] * acc);
+      if (out) out[(size_t)a.cl_body[base + i / 12] * 12 + i % 12] = acc;
+      if (dot) xs_add(*dot, vs[warp][i] * acc);
     }
     __syncwarp();
   }
-  if (slot >= 0) cta_partials(a, d0, d1, slot, -1);
 }
 
 // ---- the solve's set-up ----
 // One launch, one warp per cluster (every body is in exactly one): the residual r = b - A x of
 // the cluster's bodies (BiCGSTAB: also rh = r, p = v = 0), z = M^-1 r (PCG: also p = z) and
 // M^-1 b, with the exact partials of b.M^-1 b, r.r and r.z -- the arithmetic of the row
-// kernels and of k_apply, entry for entry.  The last CTA rounds the three totals and starts
-// the solve: the threshold tol^2 b.M^-1 b, the scalars, the iteration counter, the outcome
+// kernels and of cluster_apply, entry for entry.  The last CTA rounds the three totals and
+// starts the solve: the threshold tol^2 b.M^-1 b, the scalars, the iteration counter, the outcome
 // flags and the WHILE node's condition (set at every solve: the loop's node may sit inside
 // another conditional node, whose launches do not reset it).  With b.M^-1 b <= 0 the solution
 // is 0 (x is cleared) and no iteration runs; a solve without iterations is tallied here.
@@ -469,8 +468,8 @@ __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, const double* pv, d
 }
 
 // K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature); then
-// z = M^-1 r with the partial r.z into the new slot.  One warp per cluster: the update of the
-// cluster's bodies, then the product of k_apply over the updated r.
+// z = M^-1 r with the partial r.z into the new slot, one warp per cluster (cluster_apply: the
+// update of the cluster's bodies, then the product over the updated r).
 __global__ void __launch_bounds__(AT) k_pcg_2(SolverArgs a, const double* pv, const double* Ap, double* x, double* r,
                                               double* z) {
   const int it = iteration(a);
@@ -487,34 +486,15 @@ __global__ void __launch_bounds__(AT) k_pcg_2(SolverArgs a, const double* pv, co
     return;
   }
   const double alpha = sc[0] / sc[1];
-  constexpr int NWA = AT / 32;
-  __shared__ double vs[NWA][12 * kMaxCluster];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   XSum d0, d1;
   xs_zero(d0);
   xs_zero(d1);
-  const int ncl = *a.ncl_dev;
-  for (int c = blockIdx.x * NWA + warp; c < ncl; c += gridDim.x * NWA) {
-    const int base = a.cl_ptr[c], sz = a.cl_ptr[c + 1] - base, D = 12 * sz;
-    if (lane < 12)
-      for (int m = 0; m < sz; ++m) {
-        const size_t i = (size_t)a.cl_body[base + m] * 12 + lane;
-        x[i] += alpha * pv[i];
-        const double ri = r[i] - alpha * Ap[i];
-        r[i] = ri;
-        vs[warp][12 * m + lane] = ri;
-      }
-    __syncwarp();
-    const double* Kc = a.cl_inv + a.cl_off[c];
-    for (int i = lane; i < D; i += 32) {
-      double acc = 0.0;
-      const double* row = Kc + (size_t)i * D;
-      for (int j = 0; j < D; ++j) acc += row[j] * vs[warp][j];
-      z[(size_t)a.cl_body[base + i / 12] * 12 + i % 12] = acc;
-      xs_add(d0, vs[warp][i] * acc);
-    }
-    __syncwarp();
-  }
+  cluster_apply(a, z, &d0, [&](size_t i) {
+    x[i] += alpha * pv[i];
+    const double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    return ri;
+  });
   if (blockIdx.x == 0 && threadIdx.x == 0) a.dstat[DS_SOLVER_ITERS] = it;
   cta_partials(a, d0, d1, (it & 1) ? SL_RZ1 : SL_RZ0, -1);
 }
@@ -539,8 +519,10 @@ __global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, const double* z, do
 }
 
 // ---- BiCGSTAB (right preconditioned) ----
-// K1: converged if r.M^-1 r small; rho = rh.r; p = r + beta (p - omega v)
-__global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, const double* r, double* pv, const double* v) {
+// K1: converged if r.M^-1 r small; rho = rh.r; p = r + beta (p - omega v); then y = M^-1 p,
+// one warp per cluster (cluster_apply)
+__global__ void __launch_bounds__(AT) k_bicg_1(SolverArgs a, const double* r, double* pv, const double* v,
+                                               double* y) {
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[2] = {SL_RZ0, SL_RHR};
@@ -557,13 +539,11 @@ __global__ void __launch_bounds__(256) k_bicg_1(SolverArgs a, const double* r, d
   const double rho_old = a.scal[(it + 1) & 1];
   const double alpha = a.scal[SC_ALPHA], omega = a.scal[SC_OMEGA];
   const double beta = (rho / rho_old) * (alpha / omega);
-  const int lane = threadIdx.x & 31;
-  FOR_BODIES(b) {
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      pv[i] = it == 1 ? r[i] : r[i] + beta * (pv[i] - omega * v[i]);
-    }
-  }
+  cluster_apply(a, y, nullptr, [&](size_t i) {
+    const double pi = it == 1 ? r[i] : r[i] + beta * (pv[i] - omega * v[i]);
+    pv[i] = pi;
+    return pi;
+  });
   if (blockIdx.x == 0 && threadIdx.x == 0) a.scal[it & 1] = rho;
 }
 
@@ -587,25 +567,29 @@ __global__ void __launch_bounds__(256) k_spmv(SolverArgs a, const double* in, do
   cta_partials(a, d0, d1, slot0, slot1);
 }
 
-// K3: alpha = rho / rh.v; s = r - alpha v
-__global__ void __launch_bounds__(256) k_bicg_3(SolverArgs a, const double* r, const double* v, double* s) {
+// K3: alpha = rho / rh.v; s = r - alpha v; then z = M^-1 s with the partial s.z, one warp per
+// cluster (cluster_apply)
+__global__ void __launch_bounds__(AT) k_bicg_3(SolverArgs a, const double* r, const double* v, double* s,
+                                               double* z) {
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[1] = {SL_RHV};
   double sc[1];
   cta_scalars(a, slots, 1, sc);
   const double alpha = a.scal[it & 1] / sc[0];
-  const int lane = threadIdx.x & 31;
-  FOR_BODIES(b) {
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      s[i] = r[i] - alpha * v[i];
-    }
-  }
+  XSum d0, d1;
+  xs_zero(d0);
+  xs_zero(d1);
+  cluster_apply(a, z, &d0, [&](size_t i) {
+    const double si = r[i] - alpha * v[i];
+    s[i] = si;
+    return si;
+  });
   if (blockIdx.x == 0 && threadIdx.x == 0) a.scal[SC_ALPHA] = alpha;
+  cta_partials(a, d0, d1, SL_SZ, -1);
 }
 
-// K4 (after z = M s with partial s.z): if small, x += alpha y and stop
+// K4 (after K3's z = M^-1 s and s.z): if small, x += alpha y and stop
 __global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, const double* y, double* x) {
   const int it = iteration(a);
   const volatile int* ds = a.dstat;
@@ -628,10 +612,10 @@ __global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, const double* y, d
   }
 }
 
-// K6: omega = t.s / t.t; x += alpha y + omega z; r = s - omega t; partial rh.r
-__global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, const double* z,
-                                                const double* s, const double* t, const double* rh, double* x,
-                                                double* r) {
+// K6: omega = t.s / t.t; x += alpha y + omega z; r = s - omega t; partial rh.r; then the
+// partial r.M^-1 r, one warp per cluster (cluster_apply; the product itself is not kept)
+__global__ void __launch_bounds__(AT) k_bicg_6(SolverArgs a, const double* y, const double* z, const double* s,
+                                               const double* t, const double* rh, double* x, double* r) {
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[2] = {SL_TS, SL_TT};
@@ -639,20 +623,17 @@ __global__ void __launch_bounds__(256) k_bicg_6(SolverArgs a, const double* y, c
   cta_scalars(a, slots, 2, sc);
   const double omega = sc[0] / sc[1];
   const double alpha = a.scal[SC_ALPHA];
-  const int lane = threadIdx.x & 31;
-  XSum d0, d1;
-  xs_zero(d0);
-  xs_zero(d1);
-  FOR_BODIES(b) {
-    if (lane < 12) {
-      const size_t i = (size_t)b * 12 + lane;
-      x[i] += alpha * y[i] + omega * z[i];
-      const double ri = s[i] - omega * t[i];
-      r[i] = ri;
-      xs_add(d1, rh[i] * ri);
-    }
-  }
-  cta_partials(a, d0, d1, -1, SL_RHR);
+  XSum rz, rhr;
+  xs_zero(rz);
+  xs_zero(rhr);
+  cluster_apply(a, nullptr, &rz, [&](size_t i) {
+    x[i] += alpha * y[i] + omega * z[i];
+    const double ri = s[i] - omega * t[i];
+    r[i] = ri;
+    xs_add(rhr, rh[i] * ri);
+    return ri;
+  });
+  cta_partials(a, rz, rhr, SL_RZ0, SL_RHR);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.scal[SC_OMEGA] = omega;
     a.dstat[DS_SOLVER_ITERS] = it;
@@ -879,7 +860,7 @@ int build_preconditioner(Sim& s) {
 }
 
 // kernels of one iteration of the loop's body: PCG or BiCGSTAB, k_loop_end included
-constexpr int iteration_kernels(bool pcg) { return pcg ? 4 : 10; }
+constexpr int iteration_kernels(bool pcg) { return pcg ? 4 : 7; }
 
 // Enqueues a solve on s.stream, which must be capturing: the setup kernels, then a WHILE node
 // whose body is one iteration (its last kernel sets the loop condition), the body captured on
@@ -925,15 +906,12 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out, bool tally) {
     k_pcg_2<<<s.red_grid, AT, 0, bs>>>(a, s.pv, s.v, x, s.r, s.z);
     k_pcg_3<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.pv);
   } else {
-    k_bicg_1<<<s.red_grid, 256, 0, bs>>>(a, s.r, s.pv, s.v);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.pv, s.y, -1);
+    k_bicg_1<<<s.red_grid, AT, 0, bs>>>(a, s.r, s.pv, s.v, s.y);
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
-    k_bicg_3<<<s.red_grid, 256, 0, bs>>>(a, s.r, s.v, s.s);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.s, s.z, SL_SZ);
+    k_bicg_3<<<s.red_grid, AT, 0, bs>>>(a, s.r, s.v, s.s, s.z);
     k_bicg_4<<<s.red_grid, 256, 0, bs>>>(a, s.y, x);
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
-    k_bicg_6<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
-    k_apply<<<s.red_grid, AT, 0, bs>>>(a, 1, s.r, s.ddq, SL_RZ0);
+    k_bicg_6<<<s.red_grid, AT, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
   }
   k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
   if (per_iter_out) *per_iter_out = iteration_kernels(pcg);
