@@ -610,7 +610,9 @@ int krylov_issue(Sim& s, double* x);
 
 // newton.cu: the kernels of the device-driven Newton loop (abd_step when the parameters'
 // newton_loop is 0).  Each enqueues on s.stream.
-cudaError_t step_begin(Sim& s, cudaGraphConditionalHandle h);
+// the step's start: q and the line-search origin from q0, the warm start kept for a rerun,
+// the step's counters cleared, the Newton loop's condition set
+cudaError_t step_begin(Sim& s, const abd_states& st, cudaGraphConditionalHandle h);
 cudaError_t gate_no_overflow(Sim& s, cudaGraphConditionalHandle h);
 cudaError_t ls_accept(Sim& s);
 // (A, p) -= alpha dq with the accepted alpha on the device; also into (Ak, pk)

@@ -28,7 +28,18 @@ static_assert(PF_N == 7 && kProfBytes[0] == 24.0 && kProfBytes[1] == 36.0 && kPr
 
 namespace {
 
-__global__ void k_step_begin(Mailbox* box, cudaGraphConditionalHandle h) {
+// The step's start, one thread per body: q <- q0 and the line-search origin (Ak, pk) <- q0
+// (abd.py:124-128), and the warm start dq kept for a rerun; thread 0 clears the step's
+// counters and enters the Newton loop.
+__global__ void k_step_begin(Mailbox* box, cudaGraphConditionalHandle h, int n, abd_states st, const double* dq,
+                             double* dq_save) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) {
+    for (int k = 0; k < 9; ++k) st.A[9 * b + k] = st.Ak[9 * b + k] = st.A0[9 * b + k];
+    for (int k = 0; k < 3; ++k) st.p[3 * b + k] = st.pk[3 * b + k] = st.p0[3 * b + k];
+    for (int k = 0; k < 12; ++k) dq_save[12 * b + k] = dq[12 * b + k];
+  }
+  if (b != 0) return;
   StepDev& S = box->step;
   S.it = S.lin = S.ls = 0;
   S.n_pt = S.n_ee = S.n_vg = S.n_ij = S.n_active = 0;
@@ -152,8 +163,8 @@ cudaError_t adjoint_out(Sim& s, const double* lam, const double* qdb, double* qb
   return cudaGetLastError();
 }
 
-cudaError_t step_begin(Sim& s, cudaGraphConditionalHandle h) {
-  k_step_begin<<<1, 1, 0, s.stream>>>(s.box, h);
+cudaError_t step_begin(Sim& s, const abd_states& st, cudaGraphConditionalHandle h) {
+  k_step_begin<<<(s.n + 127) / 128, 128, 0, s.stream>>>(s.box, h, s.n, st, s.dq, s.dq_save);
   ++s.launches;
   return cudaGetLastError();
 }

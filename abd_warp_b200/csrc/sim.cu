@@ -1223,7 +1223,6 @@ int step_host(abd_sim* h, const abd_states* stp, double* x_view, abd_step_info* 
 // capturing (newton.cu describes the loop); ends with the copy of the mailbox to the host
 int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
   Sim& s = h->s;
-  const size_t nA = sizeof(double) * 9 * s.n, np = sizeof(double) * 3 * s.n, nq = sizeof(double) * 12 * s.n;
   auto dots = [&]() -> int {  // dq.g, g.g on a branch beside the CCD pass's culling
     CK(cudaEventRecord(s.fork_ev[0], s.stream));
     CK(cudaStreamWaitEvent(s.fork_b, s.fork_ev[0], 0));
@@ -1245,16 +1244,11 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
     return ABD_OK;
   };
   const cudaStream_t top = s.stream;
-  // q <- q0 (abd.py:124-128); the warm start kept for a rerun
-  CK(cudaMemcpyAsync(st.A, st.A0, nA, cudaMemcpyDeviceToDevice, top));
-  CK(cudaMemcpyAsync(st.p, st.p0, np, cudaMemcpyDeviceToDevice, top));
-  CK(cudaMemcpyAsync(st.Ak, st.A0, nA, cudaMemcpyDeviceToDevice, top));
-  CK(cudaMemcpyAsync(st.pk, st.p0, np, cudaMemcpyDeviceToDevice, top));
-  CK(cudaMemcpyAsync(s.dq_save, s.dq, nq, cudaMemcpyDeviceToDevice, top));
   if (int r = clear_friction(s)) return r;  // the first Newton iteration's GH pass fixes them
   cudaGraphConditionalHandle hn;
   if (int r = abd::make_handle(top, &hn)) return r;
-  CK(abd::step_begin(s, hn));
+  // q <- q0 (abd.py:124-128); the warm start kept for a rerun
+  CK(abd::step_begin(s, st, hn));
   cudaGraph_t nbody = nullptr;
   if (int r = abd::add_conditional(top, hn, cudaGraphCondTypeWhile, &nbody)) return r;
   const long long l0 = s.launches;
