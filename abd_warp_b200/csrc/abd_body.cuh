@@ -19,6 +19,23 @@ __device__ inline void dofs_at(const double* A, const double* p, const double* d
     for (int k = 0; k < 3; ++k) M[3 * r + k] = A[9 * b + 3 * r + k] - dq[12 * b + 3 * (r + 1) + k] * al;
 }
 
+// (Ao, po) = (A, p) - al dq for body b, also into (Ao2, po2) when given (in place when Ao is A)
+__device__ inline void update_body_dofs(int b, const double* A, const double* p, const double* dq, double al,
+                                        double* Ao, double* po, double* Ao2, double* po2) {
+  double M[12];
+  dofs_at(A, p, dq, b, al, M);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    Ao[9 * b + k] = M[k];
+    if (Ao2) Ao2[9 * b + k] = M[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    po[3 * b + k] = M[9 + k];
+    if (po2) po2[3 * b + k] = M[9 + k];
+  }
+}
+
 // coordinate j of x = A^T r + p (update_mesh_vertex, abd.py:305-324)
 __device__ inline double xform(const double M[12], double r0, double r1, double r2, int j) {
   return ((M[j] * r0 + M[3 + j] * r1) + M[6 + j] * r2) + M[9 + j];

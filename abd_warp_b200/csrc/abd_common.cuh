@@ -615,9 +615,9 @@ int krylov_issue(Sim& s, double* x);
 cudaError_t step_begin(Sim& s, const abd_states& st, cudaGraphConditionalHandle h);
 cudaError_t gate_no_overflow(Sim& s, cudaGraphConditionalHandle h);
 cudaError_t ls_accept(Sim& s);
-// (A, p) -= alpha dq with the accepted alpha on the device; also into (Ak, pk)
-cudaError_t update_dofs_dev(Sim& s, double* A, double* p, double* Ak, double* pk);
-cudaError_t newton_end(Sim& s, cudaGraphConditionalHandle h);
+// the loop's end: (A, p) -= alpha dq with the accepted alpha on the device, also into (Ak, pk),
+// then the convergence test
+cudaError_t newton_end(Sim& s, const abd_states& st, cudaGraphConditionalHandle h);
 cudaError_t finish_step_dev(Sim& s, const abd_states& st, double* xview);
 // the adjoint step (abd_adjoint_step): its right-hand side into g, its outputs from lambda
 cudaError_t adjoint_rhs(Sim& s, const double* qb, const double* qdb);

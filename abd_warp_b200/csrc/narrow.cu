@@ -1596,21 +1596,7 @@ __global__ void k_update_dofs(int n, const double* A, const double* p, const dou
                               double* po, const double* alpha_dev, double* Ao2, double* po2) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
-  if (alpha_dev) alpha = *alpha_dev;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const double v = p[3 * b + k] - dq[12 * b + k] * alpha;
-    po[3 * b + k] = v;
-    if (po2) po2[3 * b + k] = v;
-  }
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const double v = A[9 * b + 3 * r + k] - dq[12 * b + 3 * (r + 1) + k] * alpha;
-      Ao[9 * b + 3 * r + k] = v;
-      if (Ao2) Ao2[9 * b + 3 * r + k] = v;
-    }
+  update_body_dofs(b, A, p, dq, alpha_dev ? *alpha_dev : alpha, Ao, po, Ao2, po2);
 }
 
 __global__ void k_finish(int n, double dt, abd_states st) {
@@ -1946,11 +1932,6 @@ cudaError_t update_dofs(Sim& s, const double* A, const double* p, const double* 
   return cudaGetLastError();
 }
 
-cudaError_t update_dofs_dev(Sim& s, double* A, double* p, double* Ak, double* pk) {
-  k_update_dofs<<<blocks(s.n, 128), 128, 0, s.stream>>>(s.n, A, p, s.dq, 0.0, A, p, s.dpar + kParAcc, Ak, pk);
-  ++s.launches;
-  return cudaGetLastError();
-}
 
 // k_finish, unless the device loop stopped for a rerun (the states are then left as they
 // were); the DOFs it ended with are kept for the next step's first GH pass

@@ -18,7 +18,7 @@
 // follow the same rules.
 #include <cuda_runtime.h>
 
-#include "abd_common.cuh"
+#include "abd_body.cuh"
 
 namespace abd {
 
@@ -112,10 +112,17 @@ __global__ void k_ls_accept(Mailbox* box, double* dpar, abd_params P, int prof_b
   S.t1 = 0ULL;
 }
 
-// The loop's last kernel: the iteration count and the convergence test (abd.py:259-271:
-// g.g < tol on the gradient the iteration solved with, or max_iter iterations); a list
-// overflow or a line search that needs more trials also ends the loop
-__global__ void k_newton_end(Mailbox* box, double tol, int max_iter, cudaGraphConditionalHandle h) {
+// The loop's last kernel, one thread per body: the accepted step q <- q - alpha dq, also
+// into the line-search origin (Ak, pk) (update_qk, abd.py:154-157); then thread 0: the
+// iteration count and the convergence test (abd.py:259-271: g.g < tol on the gradient the
+// iteration solved with, or max_iter iterations).  A list overflow or a line search that needs
+// more trials ends the loop without the update (the step is then made again from its start).
+__global__ void k_newton_end(Mailbox* box, double tol, int max_iter, cudaGraphConditionalHandle h, int n,
+                             abd_states st, const double* dq, const double* alpha) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n && !(box->dstat[DS_STATUS] & kRerunMask))
+    update_body_dofs(b, st.A, st.p, dq, *alpha, st.A, st.p, st.Ak, st.pk);
+  if (b != 0) return;
   StepDev& S = box->step;
   ++S.it;
   const double gTg = box->dots[1];
@@ -181,8 +188,9 @@ cudaError_t ls_accept(Sim& s) {
   return cudaGetLastError();
 }
 
-cudaError_t newton_end(Sim& s, cudaGraphConditionalHandle h) {
-  k_newton_end<<<1, 1, 0, s.stream>>>(s.box, s.prm.tol, s.prm.max_iter, h);
+cudaError_t newton_end(Sim& s, const abd_states& st, cudaGraphConditionalHandle h) {
+  k_newton_end<<<(s.n + 127) / 128, 128, 0, s.stream>>>(s.box, s.prm.tol, s.prm.max_iter, h, s.n, st, s.dq,
+                                                        s.dpar + kParAcc);
   ++s.launches;
   return cudaGetLastError();
 }

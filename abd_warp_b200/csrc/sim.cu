@@ -1235,12 +1235,12 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
     if (int r = abd::cluster_inverse(s)) return r;
     if (int r = abd::krylov_issue(s, s.dq)) return r;
     // the CCD bound between q and q - dq with the line-search candidates (abd.py:278-303),
-    // Ak, pk = q - dq; the trials of the line search; the accepted step
+    // Ak, pk = q - dq; the trials of the line search and the acceptance (the loop's last kernel
+    // takes the accepted step)
     const abd::Dofs d0 = direct(st.A, st.p), d1 = updated(s, st.A, st.p, 1, st.Ak, st.pk);
     if (int r = ccd_issue(h, d0, d1, abd::NARROW_CCD_LS, dots)) return r;
     CK(abd::ls_energies(s, st, st.A, st.p, true));
     CK(abd::ls_accept(s));
-    CK(abd::update_dofs_dev(s, st.A, st.p, st.Ak, st.pk));
     return ABD_OK;
   };
   const cudaStream_t top = s.stream;
@@ -1263,7 +1263,7 @@ int step_issue(abd_sim* h, const abd_states& st, double* x_view) {
     cudaGraph_t ibody = nullptr;
     if (int q = abd::add_conditional(s.stream, hi, cudaGraphCondTypeIf, &ibody)) return q;
     if (int q = abd::capture_body(s, ibody, s.cap_stream4, iteration_tail)) return q;
-    CK(abd::newton_end(s, hn));
+    CK(abd::newton_end(s, st, hn));  // (with the accepted step's DOF update)
     return ABD_OK;
   });
   if (r) return r;
