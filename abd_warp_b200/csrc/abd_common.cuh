@@ -463,7 +463,7 @@ enum : int {
   DS_EE_COUNT = 2,
   DS_VG_COUNT = 3,
   DS_ACTIVE = 4,
-  DS_SOLVER_DONE = 5,
+  DS_KRYLOV_RUNS = 5,  // Krylov loop body executions of the current solve (a watchdog)
   DS_SOLVER_ITERS = 6,
   DS_NPAIRS = 7,     // body pairs of the last culling pass
   DS_NADJ = 8,       // adjacency entries (2 x pairs)

@@ -17,9 +17,10 @@
 // of such stiff systems has a rounding floor near eps * cond.  The SpMV is warp per block row
 // (24 lanes = 12 rows x 2 half-rows).  Dot products are exact (per-CTA partials summed in
 // fixed point), so the solve is bitwise reproducible.  The iterations run as the body of a
-// CUDA graph WHILE node: the last kernel of an iteration advances the device iteration
-// counter, makes the convergence test that the next iteration would make, and sets the
-// loop's condition, so a solve runs exactly its iterations with no host round trip.
+// CUDA graph WHILE node: the kernel that completes an iteration's last dot product also ends
+// the iteration -- it advances the device iteration counter, makes the convergence test that
+// the next iteration would make, and sets the loop's condition -- so a solve runs exactly its
+// iterations with no host round trip.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +61,7 @@ struct SolverArgs {
   double* scal;
   int* dstat;
   Mailbox* tally;    // device loop: the solve's outcome goes to the step's counters (else null)
+  cudaGraphConditionalHandle loop;  // the iteration loop's WHILE node
 };
 
 constexpr int SC_RED = 16;  // scal[SC_RED + slot]: the rounded total of reduction `slot`
@@ -107,13 +109,15 @@ __device__ inline void total_of(const SolverArgs& a, int slot, XSum* sh) {
 // Exact per-CTA partials of up to two dot products (every thread passes its accumulators);
 // the last CTA to deliver sums the partials of all CTAs and stores the rounded totals in
 // scal[SC_RED + slot] (a single counter per launch: slot0 if >= 0, else slot1).
-__device__ inline void cta_partials(const SolverArgs& a, XSum& x0, XSum& x1, int slot0, int slot1) {
+// Returns true in the last CTA, whose thread 0 wrote the totals.
+__device__ inline bool cta_partials(const SolverArgs& a, XSum& x0, XSum& x1, int slot0, int slot1) {
   __shared__ XSum sh[8];
   if (slot0 >= 0) cta_partial(a, x0, slot0, sh);
   if (slot1 >= 0) cta_partial(a, x1, slot1, sh);
-  if (!cta_last(a, slot0 >= 0 ? slot0 : slot1)) return;
+  if (!cta_last(a, slot0 >= 0 ? slot0 : slot1)) return false;
   if (slot0 >= 0) total_of(a, slot0, sh);
   if (slot1 >= 0) total_of(a, slot1, sh);
+  return true;
 }
 
 // y_b (lanes 0..11 hold row lane) = (A x)_b for block row b
@@ -151,7 +155,7 @@ __device__ inline bool solver_done(const int* dstat) {
 }
 
 // the current Krylov iteration (device counter, 1 at the first iteration, advanced by
-// k_loop_end); iterations beyond the limit do nothing
+// loop_end); iterations beyond the limit do nothing
 __device__ inline int iteration(const SolverArgs& a) { return a.dstat[DS_IT]; }
 
 // The outcome of a finished solve into the device loop's step counters (a.tally): its
@@ -162,14 +166,15 @@ __device__ inline void tally_solve(const SolverArgs& a) {
   if (!(a.dstat[DS_R_DONE] || a.dstat[DS_S_DONE])) atomicOr(&a.dstat[DS_STATUS], ST_SOLVER_NOCONV);
 }
 
-// Last kernel of a loop iteration (one thread): advances the iteration counter, makes the
-// convergence test of the next iteration's first kernel (PCG: r.z against the threshold;
-// BiCGSTAB: r.M^-1 r and rho = rh.r), records a stop as that kernel would, and sets the
-// WHILE node's condition.  The loop ends at convergence or after maxit iterations (and the
-// solve's outcome is tallied).
-__global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) {
+// The end of a loop iteration (one thread, in the iteration's last kernel once its last
+// reduction is final): advances the iteration counter, makes the convergence test of the next
+// iteration's first kernel (PCG: r.z against the threshold; BiCGSTAB: r.M^-1 r and
+// rho = rh.r), records a stop as that kernel would, and sets the WHILE node's condition.  The
+// loop ends at convergence or after maxit iterations (and the solve's outcome is tallied); a
+// body that ran more than maxit times also ends it.
+__device__ inline void loop_end(const SolverArgs& a, int pcg) {
   const int it = a.dstat[DS_IT];
-  bool stop = solver_done(a.dstat) || it + 1 > a.maxit;
+  bool stop = solver_done(a.dstat) || it + 1 > a.maxit || a.dstat[DS_KRYLOV_RUNS] > a.maxit;
   if (!stop) {
     const double thr2 = a.scal[SC_THR2];
     if (pcg) {
@@ -185,7 +190,14 @@ __global__ void k_loop_end(SolverArgs a, int pcg, cudaGraphConditionalHandle h) 
   }
   a.dstat[DS_IT] = it + 1;
   if (stop) tally_solve(a);
-  cudaGraphSetConditional(h, stop ? 0u : 1u);
+  cudaGraphSetConditional(a.loop, stop ? 0u : 1u);
+}
+
+// The first kernel of an iteration counts the loop body's runs (thread 0 of CTA 0); a body
+// that runs more than maxit times ends the loop (a safeguard: loop_end ends it at maxit)
+__device__ inline void count_run(const SolverArgs& a) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && ++a.dstat[DS_KRYLOV_RUNS] > a.maxit)
+    cudaGraphSetConditional(a.loop, 0u);
 }
 
 // ---- preconditioner setup: assemble and invert each cluster's dense block system ----
@@ -426,6 +438,7 @@ __global__ void __launch_bounds__(AT) k_krylov_setup(SolverArgs a, const double*
     a.scal[SC_RHO0] = a.scal[SC_RHO1] = a.scal[SC_ALPHA] = a.scal[SC_OMEGA] = 1.0;
     a.scal[SC_THR2] = tol2 * b;
     a.dstat[DS_IT] = 1;
+    a.dstat[DS_KRYLOV_RUNS] = 0;
     // the solve's outcome flags start clear (the iterations that follow set and read them)
     a.dstat[DS_R_DONE] = b > 0.0 ? 0 : 1;
     a.dstat[DS_S_DONE] = 0;
@@ -439,6 +452,7 @@ __global__ void __launch_bounds__(AT) k_krylov_setup(SolverArgs a, const double*
 // ---- PCG ----
 // K1: converged if r.z <= thr^2; else Ap = A p with partial p.Ap
 __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, const double* pv, double* Ap) {
+  count_run(a);
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
@@ -469,19 +483,25 @@ __global__ void __launch_bounds__(256) k_pcg_1(SolverArgs a, const double* pv, d
 
 // K2: alpha = rz / p.Ap; x += alpha p; r -= alpha Ap (stops on a non-positive curvature); then
 // z = M^-1 r with the partial r.z into the new slot, one warp per cluster (cluster_apply: the
-// update of the cluster's bodies, then the product over the updated r).
+// update of the cluster's bodies, then the product over the updated r).  The iteration's end
+// (loop_end): by the last CTA, or by CTA 0 when the solve stops here or has stopped.
 __global__ void __launch_bounds__(AT) k_pcg_2(SolverArgs a, const double* pv, const double* Ap, double* x, double* r,
                                               double* z) {
   const int it = iteration(a);
-  if (solver_done(a.dstat) || it > a.maxit) return;
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  if (solver_done(a.dstat) || it > a.maxit) {
+    if (lead) loop_end(a, 1);
+    return;
+  }
   const int rz = (it & 1) ? SL_RZ0 : SL_RZ1;
   const int slots[2] = {rz, SL_PAP};
   double sc[2];
   cta_scalars(a, slots, 2, sc);
   if (!(sc[1] > 0.0)) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (lead) {
       a.dstat[DS_R_DONE] = it;
       a.dstat[DS_SOLVER_ITERS] = it - 1;
+      loop_end(a, 1);
     }
     return;
   }
@@ -495,13 +515,15 @@ __global__ void __launch_bounds__(AT) k_pcg_2(SolverArgs a, const double* pv, co
     r[i] = ri;
     return ri;
   });
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.dstat[DS_SOLVER_ITERS] = it;
-  cta_partials(a, d0, d1, (it & 1) ? SL_RZ1 : SL_RZ0, -1);
+  if (cta_partials(a, d0, d1, (it & 1) ? SL_RZ1 : SL_RZ0, -1) && threadIdx.x == 0) {
+    a.dstat[DS_SOLVER_ITERS] = it;
+    loop_end(a, 1);  // (the new r.z is final)
+  }
 }
 
 // K3 (after K2's z = M^-1 r and r.z in the new slot): beta = rz_new / rz_old; p = z + beta p
 __global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, const double* z, double* pv) {
-  const int it = iteration(a);
+  const int it = iteration(a) - 1;  // (K2 ended the iteration: the counter is one ahead)
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int rz_old = (it & 1) ? SL_RZ0 : SL_RZ1, rz_new = (it & 1) ? SL_RZ1 : SL_RZ0;
   const int slots[2] = {rz_new, rz_old};
@@ -523,6 +545,7 @@ __global__ void __launch_bounds__(256) k_pcg_3(SolverArgs a, const double* z, do
 // one warp per cluster (cluster_apply)
 __global__ void __launch_bounds__(AT) k_bicg_1(SolverArgs a, const double* r, double* pv, const double* v,
                                                double* y) {
+  count_run(a);
   const int it = iteration(a);
   if (solver_done(a.dstat) || it > a.maxit) return;
   const int slots[2] = {SL_RZ0, SL_RHR};
@@ -613,11 +636,15 @@ __global__ void __launch_bounds__(256) k_bicg_4(SolverArgs a, const double* y, d
 }
 
 // K6: omega = t.s / t.t; x += alpha y + omega z; r = s - omega t; partial rh.r; then the
-// partial r.M^-1 r, one warp per cluster (cluster_apply; the product itself is not kept)
+// partial r.M^-1 r, one warp per cluster (cluster_apply; the product itself is not kept).  The
+// iteration's end (loop_end): by the last CTA, or by CTA 0 when the solve has stopped.
 __global__ void __launch_bounds__(AT) k_bicg_6(SolverArgs a, const double* y, const double* z, const double* s,
                                                const double* t, const double* rh, double* x, double* r) {
   const int it = iteration(a);
-  if (solver_done(a.dstat) || it > a.maxit) return;
+  if (solver_done(a.dstat) || it > a.maxit) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) loop_end(a, 0);
+    return;
+  }
   const int slots[2] = {SL_TS, SL_TT};
   double sc[2];
   cta_scalars(a, slots, 2, sc);
@@ -633,16 +660,17 @@ __global__ void __launch_bounds__(AT) k_bicg_6(SolverArgs a, const double* y, co
     xs_add(rhr, rh[i] * ri);
     return ri;
   });
-  cta_partials(a, rz, rhr, SL_RZ0, SL_RHR);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (cta_partials(a, rz, rhr, SL_RZ0, SL_RHR) && threadIdx.x == 0) {
     a.scal[SC_OMEGA] = omega;
     a.dstat[DS_SOLVER_ITERS] = it;
+    loop_end(a, 0);  // (r.M^-1 r and rh.r are final)
   }
 }
 
 SolverArgs solver_args(Sim& s) {
   SolverArgs a;
   a.tally = nullptr;
+  a.loop = 0;
   a.n = s.n;
   a.diag = s.diag;
   a.offdiag = s.offdiag;
@@ -859,8 +887,8 @@ int build_preconditioner(Sim& s) {
   return cluster_inverse(s);
 }
 
-// kernels of one iteration of the loop's body: PCG or BiCGSTAB, k_loop_end included
-constexpr int iteration_kernels(bool pcg) { return pcg ? 4 : 7; }
+// kernels of one iteration of the loop's body: PCG or BiCGSTAB
+constexpr int iteration_kernels(bool pcg) { return pcg ? 3 : 6; }
 
 // Enqueues a solve on s.stream, which must be capturing: the setup kernels, then a WHILE node
 // whose body is one iteration (its last kernel sets the loop condition), the body captured on
@@ -879,6 +907,7 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out, bool tally) {
   // the loop's handle first: k_krylov_setup sets its value
   cudaGraphConditionalHandle h;
   if (ABD_NOTE(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return ABD_ERR_CUDA;
+  a.loop = h;
   k_krylov_setup<<<s.red_grid, AT, 0, st>>>(a, bvec, x, s.r, s.z, pcg ? s.pv : nullptr, pcg ? nullptr : s.rh,
                                            pcg ? nullptr : s.pv, pcg ? nullptr : s.v, s.prm.cg_tol * s.prm.cg_tol, h);
   ++s.launches;
@@ -913,7 +942,6 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out, bool tally) {
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
     k_bicg_6<<<s.red_grid, AT, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
   }
-  k_loop_end<<<1, 1, 0, bs>>>(a, pcg ? 1 : 0, h);
   if (per_iter_out) *per_iter_out = iteration_kernels(pcg);
   cudaGraph_t body_out = nullptr;
   const cudaError_t eb = ABD_NOTE(cudaGetLastError());
