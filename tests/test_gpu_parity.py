@@ -225,19 +225,10 @@ def test_solve(scene_state, solver):
         o.set_params(prm0)
 
 
-@pytest.mark.parametrize("loop", ["device", "host"])
-@pytest.mark.parametrize("case,nsteps", [("c0", 200), ("pile", 60), ("plane", 60)])
-def test_step_parity(case, nsteps, loop):
-    """Whole time steps against the oracle, bit for bit: positions, velocities, the dq warm
-    start and every iteration count, at every step (c0: the two-cube configuration for its
-    200 steps; pile: 8 bodies on the ground box, 60 steps through landing and contact;
-    plane: the same bodies landing on the vertex-ground plane), with the Newton iterations
-    run as a device loop (the default) and driven from the host."""
+def _steps_match_the_oracle(bodies, prm, nsteps, loop):
+    """nsteps whole steps on the GPU (device or host Newton loop) and on the oracle, bit for
+    bit at every step; the trajectory goes through contact."""
     import dataclasses
-    if case == "c0":
-        bodies, prm, _ = scenes.make_config(0)
-    else:
-        bodies, prm = scenes.small_pile(2, 2, seed=7, plane=case == "plane")
     o = oracle.Oracle(scenes.flatten_bodies(bodies), prm)
     sim = _sim(bodies, dataclasses.replace(prm, newton_loop=0 if loop == "device" else 1))
     active = 0
@@ -258,6 +249,31 @@ def test_step_parity(case, nsteps, loop):
         assert active > 0  # the trajectory went through contact
     finally:
         sim.close()
+
+
+@pytest.mark.parametrize("loop", ["device", "host"])
+@pytest.mark.parametrize("case,nsteps", [("c0", 200), ("pile", 60), ("plane", 60)])
+def test_step_parity(case, nsteps, loop):
+    """Whole time steps against the oracle, bit for bit: positions, velocities, the dq warm
+    start and every iteration count, at every step (c0: the two-cube configuration for its
+    200 steps; pile: 8 bodies on the ground box, 60 steps through landing and contact;
+    plane: the same bodies landing on the vertex-ground plane), with the Newton iterations
+    run as a device loop (the default) and driven from the host."""
+    if case == "c0":
+        bodies, prm, _ = scenes.make_config(0)
+    else:
+        bodies, prm = scenes.small_pile(2, 2, seed=7, plane=case == "plane")
+    _steps_match_the_oracle(bodies, prm, nsteps, loop)
+
+
+@pytest.mark.parametrize("loop", ["device", "host"])
+def test_step_parity_bicgstab(loop):
+    """The pile's 60 steps with the reference's solver, right-preconditioned BiCGSTAB
+    (solver = 0), against the oracle's BiCGSTAB steps, bit for bit at every step (the Krylov
+    iterations end inside the kernel that completes their last dot products)."""
+    import dataclasses
+    bodies, prm = scenes.small_pile(2, 2, seed=7)
+    _steps_match_the_oracle(bodies, dataclasses.replace(prm, solver=0), 60, loop)
 
 
 def test_step_deterministic():
