@@ -285,9 +285,10 @@ struct Sim {
   int nch = 0;
   int2* chunk = nullptr;           // [nch]
   int* chunk_act = nullptr;        // [nch + 1] the chunks of a narrow pass with work, then their count
-  // CTAs of the solver's kernels: one per 8 body rows, at most kRedBlocks (their dot products
-  // are exact sums of per-CTA partials, the same for any grid)
-  int red_grid = 1;
+  // CTAs of the solver's kernels, at most kRedBlocks (their dot products are exact sums of
+  // per-CTA partials, the same for any grid): the row kernels one per 8 body rows (a warp per
+  // row), the cluster kernels one per 4 bodies (a warp per cluster, at most one each)
+  int red_grid = 1, cl_grid = 1;
   // lagged friction (friction_mu > 0): the step's contacts, and its body pairs as bits of the
   // overlap matrix that every GH pass of the step adds; fric_lag: the host loop's first GH pass
   // of a step (the device loop lags at its first Newton iteration)

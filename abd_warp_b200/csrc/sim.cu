@@ -800,6 +800,7 @@ int abd_sim_create(const abd_scene_desc* d, const abd_params* prm, void* stream,
   ok(dalloc(&s.cl_inv, 144 * (size_t)abd::kMaxCluster * n));
   ok(dalloc(&s.partials, abd::kRedSlots * (size_t)abd::kRedBlocks));
   s.red_grid = std::max(1, std::min(abd::kRedBlocks, (n + 7) / 8));
+  s.cl_grid = std::max(1, std::min(abd::kRedBlocks, (n + 3) / 4));
   ok(dalloc(&s.red_count, abd::kRedSlots));
   ok(dalloc(&s.scal, 32));
 

@@ -908,7 +908,7 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out, bool tally) {
   cudaGraphConditionalHandle h;
   if (ABD_NOTE(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return ABD_ERR_CUDA;
   a.loop = h;
-  k_krylov_setup<<<s.red_grid, AT, 0, st>>>(a, bvec, x, s.r, s.z, pcg ? s.pv : nullptr, pcg ? nullptr : s.rh,
+  k_krylov_setup<<<s.cl_grid, AT, 0, st>>>(a, bvec, x, s.r, s.z, pcg ? s.pv : nullptr, pcg ? nullptr : s.rh,
                                            pcg ? nullptr : s.pv, pcg ? nullptr : s.v, s.prm.cg_tol * s.prm.cg_tol, h);
   ++s.launches;
   // the iteration loop: a WHILE node on the capture, its body captured on a second stream
@@ -932,15 +932,15 @@ int krylov_capture(Sim& s, double* x, long long* per_iter_out, bool tally) {
     return ABD_ERR_CUDA;
   if (pcg) {
     k_pcg_1<<<s.red_grid, 256, 0, bs>>>(a, s.pv, s.v);
-    k_pcg_2<<<s.red_grid, AT, 0, bs>>>(a, s.pv, s.v, x, s.r, s.z);
+    k_pcg_2<<<s.cl_grid, AT, 0, bs>>>(a, s.pv, s.v, x, s.r, s.z);
     k_pcg_3<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.pv);
   } else {
-    k_bicg_1<<<s.red_grid, AT, 0, bs>>>(a, s.r, s.pv, s.v, s.y);
+    k_bicg_1<<<s.cl_grid, AT, 0, bs>>>(a, s.r, s.pv, s.v, s.y);
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.y, s.v, s.rh, SL_RHV, nullptr, -1);
-    k_bicg_3<<<s.red_grid, AT, 0, bs>>>(a, s.r, s.v, s.s, s.z);
+    k_bicg_3<<<s.cl_grid, AT, 0, bs>>>(a, s.r, s.v, s.s, s.z);
     k_bicg_4<<<s.red_grid, 256, 0, bs>>>(a, s.y, x);
     k_spmv<<<s.red_grid, 256, 0, bs>>>(a, s.z, s.t, s.s, SL_TS, s.t, SL_TT);
-    k_bicg_6<<<s.red_grid, AT, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
+    k_bicg_6<<<s.cl_grid, AT, 0, bs>>>(a, s.y, s.z, s.s, s.t, s.rh, x, s.r);
   }
   if (per_iter_out) *per_iter_out = iteration_kernels(pcg);
   cudaGraph_t body_out = nullptr;
